@@ -1,0 +1,260 @@
+"""ctypes binding of the C ABI in include/brian_b200.h.
+
+`Runtime` wraps one network handle of a library that exports the bg_net
+function table.  The product library is ``libbrian_b200.so`` (CUDA, sm_100a);
+loading fails loudly when it is missing or no CUDA device is present -- there
+is no CPU path in the product.
+"""
+import ctypes as ct
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbrian_b200.so")
+
+_i32, _i64, _dbl, _u64, _vp = ct.c_int32, ct.c_int64, ct.c_double, ct.c_uint64, ct.c_void_p
+_P = ct.POINTER
+
+# name -> (argtypes) ; every function returns int32 status
+SIGNATURES = {
+    "version": [],
+    "last_error": [ct.c_char_p, _i64],
+    "net_create": [ct.c_int, ct.c_int, ct.c_int, _dbl, _P(_vp)],
+    "net_destroy": [_vp],
+    "group_add": [_vp, _i64, ct.c_int, _vp, _P(_i32)],
+    "group_set_linear": [_vp, _i32, _vp, _vp],
+    "group_set_threshold": [_vp, _i32, ct.c_int, ct.c_int, _dbl, ct.c_int],
+    "group_set_poisson": [_vp, _i32, ct.c_int, _u64],
+    "group_set_generator": [_vp, _i32, _i64, _vp, _vp],
+    "group_set_reset": [_vp, _i32, ct.c_int, ct.c_int, _dbl, ct.c_int],
+    "group_set_refractory": [_vp, _i32, _dbl, _i32, ct.c_int, _dbl],
+    "conn_add": [_vp, _i32, _i64, _i64, _i32, _i64, _i64, ct.c_int, _i64, _vp, _vp, _vp, ct.c_int,
+                 _i32, _vp, _i32, ct.c_int, _P(_i32)],
+    "conn_add_dense": [_vp, _i32, _i64, _i64, _i32, _i64, _i64, ct.c_int, _vp, ct.c_int, _i32, ct.c_int,
+                       _P(_i32)],
+    "conn_get_weights": [_vp, _i32, _vp],
+    "conn_set_weights": [_vp, _i32, _vp],
+    "stdp_add": [_vp, _i32, _vp, _dbl, _dbl, _dbl, _dbl, ct.c_int, _i32, _i32, _P(_i32)],
+    "stdp_get_traces": [_vp, _i32, _vp, _vp],
+    "spikemon_add": [_vp, _i32, _i64, _i64, _i32, _P(_i32)],
+    "statemon_add": [_vp, _i32, ct.c_int, _i64, _vp, _i32, _P(_i32)],
+    "spikemon_count": [_vp, _i32, _P(_i64)],
+    "spikemon_read": [_vp, _i32, _vp, _vp, _i64, _P(_i64)],
+    "statemon_count": [_vp, _i32, _P(_i64)],
+    "statemon_read": [_vp, _i32, _vp, _vp, _i64, _P(_i64)],
+    "monitor_clear": [_vp, _i32],
+    "net_prepare": [_vp],
+    "net_run": [_vp, _i64, _i64],
+    "group_get_state": [_vp, _i32, ct.c_int, _vp],
+    "group_set_state": [_vp, _i32, ct.c_int, _vp],
+    "net_reinit": [_vp],
+    "net_stats": [_vp, _P(_i64), _P(_i64), _P(_dbl)],
+}
+
+
+class EngineError(RuntimeError):
+    pass
+
+
+class FunctionTable(object):
+    """Typed view of one library's entry points under a name prefix."""
+
+    def __init__(self, path, prefix, signatures=SIGNATURES):
+        if not os.path.exists(path):
+            raise EngineError("engine library not found: %s (run `python -m brian_b200.build`)" % path)
+        self.path = path
+        self.prefix = prefix
+        self.lib = ct.CDLL(path)
+        for name, args in signatures.items():
+            fn = getattr(self.lib, prefix + name)
+            fn.argtypes = args
+            fn.restype = ct.c_int
+            setattr(self, name, fn)
+
+    def check(self, status, what):
+        if status != 0:
+            buf = ct.create_string_buffer(1024)
+            self.last_error(buf, 1024)
+            raise EngineError("%s failed (%d): %s" % (what, status, buf.value.decode(errors="replace")))
+
+
+_product = None
+
+
+def product_table():
+    """The CUDA engine (libbrian_b200.so).  Raises if it cannot be loaded."""
+    global _product
+    if _product is None:
+        if not os.path.exists(LIB_PATH):
+            from . import build
+            build.build()
+        _product = FunctionTable(LIB_PATH, "bg_")
+    return _product
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ct.c_void_p) if a is not None else None
+
+
+class Runtime(object):
+    """One network handle on a function table."""
+
+    def __init__(self, table=None, device=0, precision=64, deterministic=True, dt=1e-4):
+        self.t = table if table is not None else product_table()
+        self.h = ct.c_void_p()
+        self.precision = precision
+        self.t.check(self.t.net_create(device, precision, 1 if deterministic else 0, float(dt),
+                                       ct.byref(self.h)), "net_create")
+
+    def close(self):
+        if self.h:
+            self.t.net_destroy(self.h)
+            self.h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _c(self, st, what):
+        self.t.check(st, what)
+
+    # ------------------------------------------------------------ building
+    def group_add(self, S0):
+        S0 = np.ascontiguousarray(S0, dtype=np.float64)
+        nvar, n = S0.shape
+        gid = _i32()
+        self._c(self.t.group_add(self.h, n, nvar, _ptr(S0), ct.byref(gid)), "group_add")
+        return gid.value
+
+    def group_set_linear(self, gid, A, C):
+        A = np.ascontiguousarray(A, dtype=np.float64)
+        C = None if C is None else np.ascontiguousarray(C, dtype=np.float64)
+        self._c(self.t.group_set_linear(self.h, gid, _ptr(A), _ptr(C)), "group_set_linear")
+
+    def group_set_threshold(self, gid, kind, var=0, value=0.0, var2=0):
+        self._c(self.t.group_set_threshold(self.h, gid, kind, var, float(value), var2), "group_set_threshold")
+
+    def group_set_poisson(self, gid, rate_var, seed):
+        self._c(self.t.group_set_poisson(self.h, gid, rate_var, int(seed) & ((1 << 64) - 1)),
+                "group_set_poisson")
+
+    def group_set_generator(self, gid, steps, idx):
+        steps = np.ascontiguousarray(steps, dtype=np.int64)
+        idx = np.ascontiguousarray(idx, dtype=np.int32)
+        self._c(self.t.group_set_generator(self.h, gid, len(steps), _ptr(steps), _ptr(idx)),
+                "group_set_generator")
+
+    def group_set_reset(self, gid, kind, var=0, value=0.0, var2=0):
+        self._c(self.t.group_set_reset(self.h, gid, kind, var, float(value), var2), "group_set_reset")
+
+    def group_set_refractory(self, gid, refractory_time, period, var, value):
+        self._c(self.t.group_set_refractory(self.h, gid, float(refractory_time), int(period), var,
+                                            float(value)), "group_set_refractory")
+
+    def conn_add(self, src, so, sn, tgt, to, tn, var, rowptr, cols, w, delay_steps=0, delays=None,
+                 ring_depth=0, mod_var=-1):
+        rowptr = np.ascontiguousarray(rowptr, dtype=np.int64)
+        cols = np.ascontiguousarray(cols, dtype=np.int32)
+        w = np.ascontiguousarray(w)
+        if w.dtype not in (np.float32, np.float64):
+            w = w.astype(np.float64)
+        wbits = 32 if w.dtype == np.float32 else 64
+        d = None if delays is None else np.ascontiguousarray(delays, dtype=np.uint8)
+        cid = _i32()
+        self._c(self.t.conn_add(self.h, src, so, sn, tgt, to, tn, var, len(cols), _ptr(rowptr), _ptr(cols),
+                                _ptr(w), wbits, int(delay_steps), _ptr(d), int(ring_depth), int(mod_var),
+                                ct.byref(cid)), "conn_add")
+        return cid.value
+
+    def conn_add_dense(self, src, so, sn, tgt, to, tn, var, W, delay_steps=0, mod_var=-1):
+        W = np.ascontiguousarray(W)
+        if W.dtype not in (np.float32, np.float64):
+            W = W.astype(np.float64)
+        wbits = 32 if W.dtype == np.float32 else 64
+        cid = _i32()
+        self._c(self.t.conn_add_dense(self.h, src, so, sn, tgt, to, tn, var, _ptr(W), wbits, int(delay_steps),
+                                      int(mod_var), ct.byref(cid)), "conn_add_dense")
+        return cid.value
+
+    def conn_get_weights(self, cid, count):
+        out = np.empty(count, dtype=np.float64)
+        self._c(self.t.conn_get_weights(self.h, cid, _ptr(out)), "conn_get_weights")
+        return out
+
+    def conn_set_weights(self, cid, w):
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        self._c(self.t.conn_set_weights(self.h, cid, _ptr(w)), "conn_set_weights")
+
+    def stdp_add(self, cid, decay, Ap, Am, wmin, wmax, interactions, pre_delay, post_delay):
+        decay = np.ascontiguousarray(decay, dtype=np.float64)
+        sid = _i32()
+        self._c(self.t.stdp_add(self.h, cid, _ptr(decay), float(Ap), float(Am), float(wmin), float(wmax),
+                                int(interactions), int(pre_delay), int(post_delay), ct.byref(sid)), "stdp_add")
+        return sid.value
+
+    def stdp_get_traces(self, sid, npre, npost):
+        a = np.empty(npre)
+        b = np.empty(npost)
+        self._c(self.t.stdp_get_traces(self.h, sid, _ptr(a), _ptr(b)), "stdp_get_traces")
+        return a, b
+
+    def spikemon_add(self, gid, origin, n, delay=0):
+        mid = _i32()
+        self._c(self.t.spikemon_add(self.h, gid, origin, n, delay, ct.byref(mid)), "spikemon_add")
+        return mid.value
+
+    def statemon_add(self, gid, var, idx, timestep=1):
+        idx = None if idx is None else np.ascontiguousarray(idx, dtype=np.int32)
+        mid = _i32()
+        self._c(self.t.statemon_add(self.h, gid, var, 0 if idx is None else len(idx), _ptr(idx), timestep,
+                                    ct.byref(mid)), "statemon_add")
+        return mid.value
+
+    def spikemon_read(self, mid):
+        n = _i64()
+        self._c(self.t.spikemon_count(self.h, mid, ct.byref(n)), "spikemon_count")
+        steps = np.empty(n.value, dtype=np.int64)
+        idx = np.empty(n.value, dtype=np.int32)
+        got = _i64()
+        self._c(self.t.spikemon_read(self.h, mid, _ptr(steps), _ptr(idx), n.value, ct.byref(got)), "spikemon_read")
+        return steps[:got.value], idx[:got.value]
+
+    def statemon_read(self, mid, width):
+        n = _i64()
+        self._c(self.t.statemon_count(self.h, mid, ct.byref(n)), "statemon_count")
+        vals = np.empty((n.value, width), dtype=np.float64)
+        steps = np.empty(n.value, dtype=np.int64)
+        got = _i64()
+        self._c(self.t.statemon_read(self.h, mid, _ptr(vals), _ptr(steps), n.value, ct.byref(got)),
+                "statemon_read")
+        return steps[:got.value], vals[:got.value]
+
+    def monitor_clear(self, mid):
+        self._c(self.t.monitor_clear(self.h, mid), "monitor_clear")
+
+    # ------------------------------------------------------------- running
+    def prepare(self):
+        self._c(self.t.net_prepare(self.h), "net_prepare")
+
+    def run(self, nsteps, clock_step0):
+        self._c(self.t.net_run(self.h, int(nsteps), int(clock_step0)), "net_run")
+
+    def get_state(self, gid, var, n):
+        out = np.empty(n, dtype=np.float64)
+        self._c(self.t.group_get_state(self.h, gid, var, _ptr(out)), "group_get_state")
+        return out
+
+    def set_state(self, gid, var, values):
+        values = np.ascontiguousarray(values, dtype=np.float64)
+        self._c(self.t.group_set_state(self.h, gid, var, _ptr(values)), "group_set_state")
+
+    def reinit(self):
+        self._c(self.t.net_reinit(self.h), "net_reinit")
+
+    def stats(self):
+        s, l, ms = _i64(), _i64(), _dbl()
+        self._c(self.t.net_stats(self.h, ct.byref(s), ct.byref(l), ct.byref(ms)), "net_stats")
+        return {"steps": s.value, "launches": l.value, "last_run_ms": ms.value}

@@ -1,0 +1,554 @@
+// bg_kernels.cuh -- sm_100a kernels of the clock-driven loop.
+//
+// Spike history layout: one bit per neuron and step.  hist[slot][word] holds
+// the spikes of neurons 32*word .. 32*word+31 emitted at the step whose
+// counter is congruent to `slot` modulo `depth`.  The warp ballot of the
+// threshold test IS the history word, so compaction needs no scan, and
+// ascending neuron order (threshold.py:191) is the natural bit order.
+#pragma once
+#include "bg_common.cuh"
+
+namespace bg {
+
+constexpr int kHeadThreads = 256;
+constexpr int kMaxVars = 8;
+constexpr int kMaxDeliv = 4;
+constexpr int kMaxRec = 4;
+
+template <typename T> struct Deliv {   // DelayConnection ring delivered into this group
+    T *ring; int64_t tn, to; int md; int var;
+};
+struct RecDev {                        // StateMonitor recorded in this group
+    int var; int nidx; const int32_t *idx; const int32_t *pos; const int32_t *blk_lo;
+    void *buf; const long long *row_base; int timestep; long long start;
+};
+
+template <typename T> struct HeadArgs {
+    DevCtl *ctl;
+    T *S; int64_t n, npad; int nvar;
+    int linear, useC;
+    T A[kMaxVars * kMaxVars]; T C[kMaxVars];
+    int thr_kind, thr_var, thr_var2; T thr_val; double dt;
+    uint64_t seed; int rate_var;
+    const int64_t *gen_steps; const int32_t *gen_idx; int64_t gen_n;
+    int reset_kind, reset_var, reset_var2; T reset_val;
+    int refr; double refr_time; int period; int clamp_var; T clamp_val;
+    double *next_allowed; int32_t *last_spike;
+    uint32_t *hist; int depth; int64_t nwords;
+    int ndeliv; Deliv<T> deliv[kMaxDeliv];
+    int nrec; RecDev rec[kMaxRec];
+    int tail, update, last;
+};
+
+template <typename T, int NV>
+__device__ __forceinline__ void set_var(T (&s)[NV], int var, T v) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) if (k == var) s[k] = v;
+}
+template <typename T, int NV>
+__device__ __forceinline__ T get_var(const T (&s)[NV], int var) {
+    T r = T(0);
+#pragma unroll
+    for (int k = 0; k < NV; ++k) if (k == var) r = s[k];
+    return r;
+}
+
+// One thread per neuron.  tail: finish the previous step (delayed-ring
+// delivery, reset, refractory clamp, state monitors) -- the
+// 'after_connections', 'resets' and 'end' slots; update: this step's
+// 'groups' slot (state update, threshold, refractory filter, history push).
+template <typename T, int NV>
+__global__ void __launch_bounds__(kHeadThreads) k_head(const HeadArgs<T> a) {
+    const int64_t i = (int64_t)blockIdx.x * kHeadThreads + threadIdx.x;
+    const bool act = i < a.n;
+    const long long nstep = a.ctl->nstep;
+    const long long cs = nstep + a.ctl->clock_off;
+    T s[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) s[k] = act ? a.S[k * a.npad + i] : T(0);
+
+    if (a.tail) {
+        const long long ps = nstep - 1;
+        for (int d = 0; d < a.ndeliv; ++d) {
+            const Deliv<T> &dv = a.deliv[d];
+            if (act && i >= dv.to && i < dv.to + dv.tn) {
+                T *r = dv.ring + (int64_t)(ps % dv.md) * dv.tn + (i - dv.to);
+                const T v = *r;
+                set_var<T, NV>(s, dv.var, rn<T>::add(get_var<T, NV>(s, dv.var), v));
+                if (v != T(0)) *r = T(0);
+            }
+        }
+        if (a.period > 0) {
+            if (act && ps - (long long)a.last_spike[i] < a.period) set_var<T, NV>(s, a.clamp_var, a.clamp_val);
+        } else if (a.reset_kind) {
+            const uint32_t w = a.hist[(int64_t)(ps % a.depth) * a.nwords + (i >> 5)];
+            if (act && ((w >> (i & 31)) & 1u)) {
+                if (a.reset_kind == 1) set_var<T, NV>(s, a.reset_var, a.reset_val);
+                else set_var<T, NV>(s, a.reset_var, get_var<T, NV>(s, a.reset_var2));
+            }
+        }
+        if (a.nrec) {
+            __shared__ T stash[kMaxRec][kHeadThreads];
+            for (int r = 0; r < a.nrec; ++r) stash[r][threadIdx.x] = get_var<T, NV>(s, a.rec[r].var);
+            __syncthreads();
+            for (int r = 0; r < a.nrec; ++r) {
+                const RecDev &m = a.rec[r];
+                const long long rel = ps - m.start;
+                if (rel < 0 || rel % m.timestep) continue;
+                const long long row = rel / m.timestep - *m.row_base;
+                const int e0 = m.blk_lo[blockIdx.x], e1 = m.blk_lo[blockIdx.x + 1];
+                for (int e = e0 + threadIdx.x; e < e1; e += kHeadThreads) {
+                    const int li = m.idx[e] - (int)(blockIdx.x * kHeadThreads);
+                    ((T *)m.buf)[row * m.nidx + m.pos[e]] = stash[r][li];
+                }
+            }
+        }
+    }
+
+    if (a.update) {
+        if (a.linear) {
+            T x[NV];
+#pragma unroll
+            for (int j = 0; j < NV; ++j) {
+                T acc = rn<T>::mul(a.A[j * NV + 0], s[0]);
+#pragma unroll
+                for (int k = 1; k < NV; ++k) acc = rn<T>::add(acc, rn<T>::mul(a.A[j * NV + k], s[k]));
+                if (a.useC) acc = rn<T>::add(acc, a.C[j]);
+                x[j] = acc;
+            }
+#pragma unroll
+            for (int j = 0; j < NV; ++j) s[j] = x[j];
+        }
+        bool spk = false;
+        if (act) {
+            switch (a.thr_kind) {
+            case 1: spk = get_var<T, NV>(s, a.thr_var) > a.thr_val; break;
+            case 2: spk = get_var<T, NV>(s, a.thr_var) > get_var<T, NV>(s, a.thr_var2); break;
+            case 3: {
+                const double rate = (double)get_var<T, NV>(s, a.rate_var);
+                spk = bg_philox_uniform(a.seed, cs, i) < __dmul_rn(rate, a.dt);
+                break;
+            }
+            case 4: {
+                // spikes of this clock step: [lo, hi) of the (step, index)-sorted list
+                int64_t lo = 0, hi = a.gen_n;
+                while (lo < hi) { int64_t m = (lo + hi) >> 1; if (a.gen_steps[m] < cs) lo = m + 1; else hi = m; }
+                int64_t e = lo, hi2 = a.gen_n;
+                while (e < hi2) { int64_t m = (e + hi2) >> 1; if (a.gen_steps[m] <= cs) e = m + 1; else hi2 = m; }
+                int64_t l2 = lo, h2 = e;
+                while (l2 < h2) { int64_t m = (l2 + h2) >> 1; if (a.gen_idx[m] < i) l2 = m + 1; else h2 = m; }
+                spk = l2 < e && a.gen_idx[l2] == i;
+                break;
+            }
+            default: break;
+            }
+            if (spk && a.refr) {
+                const double t = __dmul_rn((double)cs, a.dt);
+                if (a.next_allowed[i] <= t) a.next_allowed[i] = __dadd_rn(t, a.refr_time);
+                else spk = false;
+            }
+            if (spk && a.period > 0) a.last_spike[i] = (int32_t)nstep;
+        }
+        const uint32_t ball = __ballot_sync(0xffffffffu, spk);
+        if ((threadIdx.x & 31) == 0 && i < a.npad)
+            a.hist[(int64_t)(nstep % a.depth) * a.nwords + (i >> 5)] = ball;
+    }
+    if (act && (a.update || a.tail)) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) a.S[k * a.npad + i] = s[k];
+    }
+    bg_finish_step(a.ctl, a.last);
+}
+
+// ---------------------------------------------------------------------------
+// Spike iteration over a history slot restricted to [origin, origin+cnt).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t masked_word(const uint32_t *H, int64_t wi, int64_t origin, int64_t end) {
+    uint32_t w = H[wi];
+    const int64_t base = wi << 5;
+    if (base < origin) { const int sh = (int)(origin - base); w = sh >= 32 ? 0u : (w & (0xffffffffu << sh)); }
+    if (base + 32 > end) { const int keep = (int)(end - base); w = keep <= 0 ? 0u : (keep >= 32 ? w : (w & ((1u << keep) - 1u))); }
+    return w;
+}
+
+template <typename T> struct PropArgs {
+    DevCtl *ctl;
+    const uint32_t *hist; int depth; int64_t nwords; int delay;
+    int64_t so, sn;                 // source range in the source group
+    int64_t to, tn;                 // target range in the target group
+    T *sv;                          // target state row + to (zero-delay path)
+    T *ring; int md;                // DelayConnection ring [md][tn]
+    const int64_t *rowptr; const int32_t *cols; const void *w; const uint8_t *d;
+    int dense;
+    const T *mod;                   // source modulation row + so, or null
+    int parts;                      // row split for the atomic path
+    // fused presynaptic STDP (stdp.py:370-414): w[i,:] += A_post; clip
+    int stdp; double *A_pre; const double *A_post; double Ap; int pre_set; double wmin, wmax;
+    int last;
+};
+
+template <typename T, typename WT>
+__device__ __forceinline__ void stdp_w(WT *w, int64_t k, double add, double wmin, double wmax) {
+    if (sizeof(WT) == 4) {
+        float x = __double2float_rn(__dadd_rn((double)w[k], add));
+        const float lo = __double2float_rn(wmin), hi = __double2float_rn(wmax);
+        x = x < lo ? lo : (x > hi ? hi : x);
+        w[k] = (WT)x;
+    } else {
+        double x = __dadd_rn((double)w[k], add);
+        x = x < wmin ? wmin : (x > wmax ? wmax : x);
+        w[k] = (WT)x;
+    }
+}
+
+// Shared-weight path (every addend of one accumulator is the same number, so
+// the order of the atomic adds cannot change the result): warp items are
+// (32 history words, row part).
+template <typename T, typename WT, bool RING>
+__global__ void __launch_bounds__(256) k_prop_atomic(const PropArgs<T> a) {
+    const long long nstep = a.ctl->nstep;
+    if (nstep >= a.delay) {
+        const int lane = threadIdx.x & 31;
+        const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+        const uint32_t *H = a.hist + (int64_t)((nstep - a.delay) % a.depth) * a.nwords;
+        const int64_t end = a.so + a.sn;
+        const int64_t w0 = a.so >> 5, w1 = (end + 31) >> 5;
+        const int64_t nch = (w1 - w0 + 31) >> 5;
+        const int P = a.parts;
+        const int cur = RING ? (int)(nstep % a.md) : 0;
+        const WT *W = (const WT *)a.w;
+        for (int64_t item = warp; item < nch * P; item += nwarps) {
+            const int64_t c = item / P; const int p = (int)(item - c * P);
+            const int64_t wi = w0 + c * 32 + lane;
+            const uint32_t word = wi < w1 ? masked_word(H, wi, a.so, end) : 0u;
+            uint32_t nz = __ballot_sync(0xffffffffu, word != 0u);
+            while (nz) {
+                const int l = __ffs(nz) - 1; nz &= nz - 1;
+                uint32_t wd = __shfl_sync(0xffffffffu, word, l);
+                const int64_t base = (w0 + c * 32 + l) << 5;
+                while (wd) {
+                    const int b = __ffs(wd) - 1; wd &= wd - 1;
+                    const int64_t i = base + b - a.so;
+                    const int64_t r0 = a.rowptr[i], r1 = a.rowptr[i + 1], len = r1 - r0;
+                    const int64_t q0 = r0 + len * p / P, q1 = r0 + len * (p + 1) / P;
+                    for (int64_t k = q0 + lane; k < q1; k += 32) {
+                        const int32_t j = a.cols[k];
+                        const T wv = (T)W[k];
+                        if (RING) atomicAdd(&a.ring[(int64_t)((cur + a.d[k]) % a.md) * a.tn + j], wv);
+                        else atomicAdd(&a.sv[j], wv);
+                        if (a.stdp) stdp_w<T, WT>((WT *)a.w, k, a.A_post[j], a.wmin, a.wmax);
+                    }
+                    if (a.stdp && p == 0 && lane == 0)
+                        a.A_pre[i] = a.pre_set ? a.Ap : __dadd_rn(a.A_pre[i], a.Ap);
+                }
+            }
+        }
+    }
+    bg_finish_step(a.ctl, a.last);
+}
+
+// Ordered path (general weights): block b owns targets [b*TB, b*TB+TB) and
+// walks the spikes in ascending order, so every accumulator sees its addends
+// in the reference order (connection.py:239-241, delayconnection.py:152-153).
+constexpr int kOrdThreads = 256;
+constexpr int kOrdTB = 1024;
+constexpr int kOrdBatch = 1024;
+
+template <typename T, typename WT, bool RING>
+__global__ void __launch_bounds__(kOrdThreads) k_prop_ordered(const PropArgs<T> a) {
+    __shared__ int32_t sp[kOrdBatch];
+    __shared__ int32_t slo[kOrdBatch], shi[kOrdBatch];
+    __shared__ int32_t wcnt[kOrdThreads + 1];
+    __shared__ int nb;
+    const long long nstep = a.ctl->nstep;
+    const int64_t t0 = (int64_t)blockIdx.x * kOrdTB, t1 = min(t0 + (int64_t)kOrdTB, a.tn);
+    if (nstep >= a.delay && t0 < a.tn) {
+        const uint32_t *H = a.hist + (int64_t)((nstep - a.delay) % a.depth) * a.nwords;
+        const int64_t end = a.so + a.sn;
+        const int64_t w0 = a.so >> 5, w1 = (end + 31) >> 5;
+        const int cur = RING ? (int)(nstep % a.md) : 0;
+        WT *W = (WT *)a.w;
+        const int tid = threadIdx.x;
+        // process the source range in chunks of kOrdThreads words
+        for (int64_t cw = w0; cw < w1; cw += kOrdThreads) {
+            const int64_t wi = cw + tid;
+            const uint32_t word = wi < w1 ? masked_word(H, wi, a.so, end) : 0u;
+            // exclusive scan of popcounts (simple two-level scan)
+            const int pc = __popc(word);
+            int incl = pc;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) { int v = __shfl_up_sync(0xffffffffu, incl, o); if ((tid & 31) >= o) incl += v; }
+            if ((tid & 31) == 31) wcnt[tid >> 5] = incl;
+            __syncthreads();
+            if (tid == 0) { int acc = 0; for (int q = 0; q < kOrdThreads / 32; ++q) { int v = wcnt[q]; wcnt[q] = acc; acc += v; } wcnt[kOrdThreads / 32] = acc; }
+            __syncthreads();
+            const int total = wcnt[kOrdThreads / 32];
+            int off = wcnt[tid >> 5] + incl - pc;
+            // emit in batches of kOrdBatch spikes
+            for (int bstart = 0; bstart < total; bstart += kOrdBatch) {
+                {
+                    uint32_t wd = word; int o = off;
+                    while (wd) {
+                        const int b = __ffs(wd) - 1; wd &= wd - 1;
+                        if (o >= bstart && o < bstart + kOrdBatch) sp[o - bstart] = (int32_t)(((wi << 5) + b) - a.so);
+                        ++o;
+                    }
+                }
+                if (tid == 0) nb = min(kOrdBatch, total - bstart);
+                __syncthreads();
+                const int n = nb;
+                // locate each spike's sub-range of targets in [t0, t1)
+                for (int s = tid; s < n; s += kOrdThreads) {
+                    const int64_t i = sp[s];
+                    if (a.dense) { slo[s] = (int32_t)t0; shi[s] = (int32_t)t1; continue; }
+                    const int64_t r0 = a.rowptr[i], r1 = a.rowptr[i + 1];
+                    int64_t lo = r0, hi = r1;
+                    while (lo < hi) { int64_t m = (lo + hi) >> 1; if (a.cols[m] < t0) lo = m + 1; else hi = m; }
+                    int64_t lo2 = lo, hi2 = r1;
+                    while (lo2 < hi2) { int64_t m = (lo2 + hi2) >> 1; if (a.cols[m] < t1) lo2 = m + 1; else hi2 = m; }
+                    slo[s] = (int32_t)(lo - r0); shi[s] = (int32_t)(lo2 - r0);
+                }
+                __syncthreads();
+                for (int s = 0; s < n; ++s) {
+                    const int64_t i = sp[s];
+                    const int64_t r0 = a.dense ? i * a.tn : a.rowptr[i];
+                    const T mul = a.mod ? a.mod[i] : T(1);
+                    for (int64_t q = slo[s] + tid; q < shi[s]; q += kOrdThreads) {
+                        const int64_t k = a.dense ? r0 + q : r0 + q;
+                        const int64_t j = a.dense ? q : a.cols[k];
+                        T wv = (T)W[k];
+                        if (a.mod) wv = rn<T>::mul(wv, mul);
+                        if (RING) {
+                            T *r = &a.ring[(int64_t)((cur + a.d[k]) % a.md) * a.tn + j];
+                            *r = rn<T>::add(*r, wv);
+                        } else {
+                            a.sv[j] = rn<T>::add(a.sv[j], wv);
+                        }
+                        if (a.stdp) stdp_w<T, WT>(W, k, a.A_post[j], a.wmin, a.wmax);
+                    }
+                    if (a.stdp && blockIdx.x == 0 && tid == 0)
+                        a.A_pre[i] = a.pre_set ? a.Ap : __dadd_rn(a.A_pre[i], a.Ap);
+                    __syncthreads();
+                }
+            }
+            __syncthreads();
+        }
+    }
+    bg_finish_step(a.ctl, a.last);
+}
+
+// Dense connection, one thread per target column, spikes in ascending order
+// from a shared-memory list (connection.py:256-262: sv += row).
+constexpr int kDenseThreads = 256;
+constexpr int kDenseList = 4096;
+template <typename T, typename WT>
+__global__ void __launch_bounds__(kDenseThreads) k_prop_dense(const PropArgs<T> a) {
+    __shared__ int32_t sp[kDenseList];
+    __shared__ int32_t wcnt[kDenseThreads / 32 + 1];
+    const long long nstep = a.ctl->nstep;
+    const int64_t j = (int64_t)blockIdx.x * kDenseThreads + threadIdx.x;
+    if (nstep >= a.delay) {
+        const uint32_t *H = a.hist + (int64_t)((nstep - a.delay) % a.depth) * a.nwords;
+        const int64_t end = a.so + a.sn;
+        const int64_t w0 = a.so >> 5, w1 = (end + 31) >> 5;
+        WT *W = (WT *)a.w;
+        const int tid = threadIdx.x;
+        T acc = j < a.tn ? a.sv[j] : T(0);
+        const double apost = (a.stdp && j < a.tn) ? a.A_post[j] : 0.0;
+        for (int64_t cw = w0; cw < w1; cw += kDenseThreads) {
+            const int64_t wi = cw + tid;
+            const uint32_t word = wi < w1 ? masked_word(H, wi, a.so, end) : 0u;
+            const int pc = __popc(word);
+            int incl = pc;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) { int v = __shfl_up_sync(0xffffffffu, incl, o); if ((tid & 31) >= o) incl += v; }
+            if ((tid & 31) == 31) wcnt[tid >> 5] = incl;
+            __syncthreads();
+            if (tid == 0) { int s = 0; for (int q = 0; q < kDenseThreads / 32; ++q) { int v = wcnt[q]; wcnt[q] = s; s += v; } wcnt[kDenseThreads / 32] = s; }
+            __syncthreads();
+            const int total = wcnt[kDenseThreads / 32];
+            const int off = wcnt[tid >> 5] + incl - pc;
+            for (int bstart = 0; bstart < total; bstart += kDenseList) {
+                { uint32_t wd = word; int o = off;
+                  while (wd) { const int b = __ffs(wd) - 1; wd &= wd - 1;
+                               if (o >= bstart && o < bstart + kDenseList) sp[o - bstart] = (int32_t)(((wi << 5) + b) - a.so);
+                               ++o; } }
+                __syncthreads();
+                const int n = min(kDenseList, total - bstart);
+                if (j < a.tn) {
+                    for (int s = 0; s < n; ++s) {
+                        const int64_t i = sp[s];
+                        const int64_t k = i * a.tn + j;
+                        T wv = (T)W[k];
+                        if (a.mod) wv = rn<T>::mul(wv, a.mod[i]);
+                        acc = rn<T>::add(acc, wv);
+                        if (a.stdp) stdp_w<T, WT>(W, k, apost, a.wmin, a.wmax);
+                    }
+                }
+                if (a.stdp && blockIdx.x == 0)
+                    for (int s = tid; s < n; s += kDenseThreads) {
+                        const int64_t i = sp[s];
+                        a.A_pre[i] = a.pre_set ? a.Ap : __dadd_rn(a.A_pre[i], a.Ap);
+                    }
+                __syncthreads();
+            }
+        }
+        if (j < a.tn) a.sv[j] = acc;
+    }
+    bg_finish_step(a.ctl, a.last);
+}
+
+// STDP trace decay (the G_pre/G_post groups' 1x1 linear updaters).
+struct DecayArgs { double *A_pre; int64_t npre; double a_pre, c_pre; double *A_post; int64_t npost; double a_post, c_post; DevCtl *ctl; int last; };
+__global__ void k_stdp_decay(const DecayArgs a) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < a.npre) a.A_pre[i] = __dadd_rn(__dmul_rn(a.a_pre, a.A_pre[i]), a.c_pre);
+    else if (i < a.npre + a.npost) { const int64_t j = i - a.npre; a.A_post[j] = __dadd_rn(__dmul_rn(a.a_post, a.A_post[j]), a.c_post); }
+    bg_finish_step(a.ctl, a.last);
+}
+
+// Standalone presynaptic STDP update (used when it cannot ride on the
+// connection's propagation kernel).
+template <typename WT>
+__global__ void __launch_bounds__(256) k_stdp_pre(const PropArgs<double> a) {
+    const long long nstep = a.ctl->nstep;
+    if (nstep >= a.delay) {
+        const int lane = threadIdx.x & 31;
+        const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+        const uint32_t *H = a.hist + (int64_t)((nstep - a.delay) % a.depth) * a.nwords;
+        const int64_t end = a.so + a.sn;
+        const int64_t w0 = a.so >> 5, w1 = (end + 31) >> 5;
+        WT *W = (WT *)a.w;
+        for (int64_t wi0 = w0 + warp * 32; wi0 < w1; wi0 += nwarps * 32) {
+            const int64_t wi = wi0 + lane;
+            const uint32_t word = wi < w1 ? masked_word(H, wi, a.so, end) : 0u;
+            uint32_t nz = __ballot_sync(0xffffffffu, word != 0u);
+            while (nz) {
+                const int l = __ffs(nz) - 1; nz &= nz - 1;
+                uint32_t wd = __shfl_sync(0xffffffffu, word, l);
+                const int64_t base = (wi0 + l) << 5;
+                while (wd) {
+                    const int b = __ffs(wd) - 1; wd &= wd - 1;
+                    const int64_t i = base + b - a.so;
+                    const int64_t r0 = a.dense ? i * a.tn : a.rowptr[i];
+                    const int64_t r1 = a.dense ? r0 + a.tn : a.rowptr[i + 1];
+                    for (int64_t k = r0 + lane; k < r1; k += 32) {
+                        const int64_t j = a.dense ? k - r0 : a.cols[k];
+                        stdp_w<double, WT>(W, k, a.A_post[j], a.wmin, a.wmax);
+                    }
+                    if (lane == 0) a.A_pre[i] = a.pre_set ? a.Ap : __dadd_rn(a.A_pre[i], a.Ap);
+                }
+            }
+        }
+    }
+    bg_finish_step(a.ctl, a.last);
+}
+
+// Postsynaptic STDP update: for each target spike j, A_post[j] (+)= Am and
+// w[:,j] += A_pre, clipped.  Columns of different spikes are disjoint.
+struct PostArgs {
+    DevCtl *ctl;
+    const uint32_t *hist; int depth; int64_t nwords; int delay;
+    int64_t to, tn, sn;
+    void *w; int dense;
+    const int64_t *colptr; const int64_t *colk; const int32_t *colsrc;
+    double *A_post; const double *A_pre; double Am; int post_set; double wmin, wmax;
+    int last;
+};
+template <typename WT>
+__global__ void __launch_bounds__(256) k_stdp_post(const PostArgs a) {
+    __shared__ int32_t sp[1024];
+    __shared__ int ns;
+    const long long nstep = a.ctl->nstep;
+    if (nstep >= a.delay) {
+        const uint32_t *H = a.hist + (int64_t)((nstep - a.delay) % a.depth) * a.nwords;
+        const int64_t end = a.to + a.tn;
+        const int64_t w0 = a.to >> 5, w1 = (end + 31) >> 5;
+        WT *W = (WT *)a.w;
+        for (int64_t cw = w0; cw < w1; cw += 32) {
+            if (threadIdx.x == 0) ns = 0;
+            __syncthreads();
+            if (threadIdx.x < 32) {
+                const int64_t wi = cw + threadIdx.x;
+                uint32_t word = wi < w1 ? masked_word(H, wi, a.to, end) : 0u;
+                const int pc = __popc(word);
+                int incl = pc;
+                for (int o = 1; o < 32; o <<= 1) { int v = __shfl_up_sync(0xffffffffu, incl, o); if ((int)threadIdx.x >= o) incl += v; }
+                int o = incl - pc;
+                while (word) { const int b = __ffs(word) - 1; word &= word - 1; sp[o++] = (int32_t)(((wi << 5) + b) - a.to); }
+                if (threadIdx.x == 31) ns = incl;
+            }
+            __syncthreads();
+            const int n = ns;
+            for (int s = 0; s < n; ++s) {
+                const int64_t j = sp[s];
+                if (a.dense) {
+                    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.sn; i += (int64_t)gridDim.x * blockDim.x)
+                        stdp_w<double, WT>(W, i * a.tn + j, a.A_pre[i], a.wmin, a.wmax);
+                } else {
+                    for (int64_t p = a.colptr[j] + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < a.colptr[j + 1];
+                         p += (int64_t)gridDim.x * blockDim.x)
+                        stdp_w<double, WT>(W, a.colk[p], a.A_pre[a.colsrc[p]], a.wmin, a.wmax);
+                }
+            }
+            if (blockIdx.x == 0)
+                for (int s = threadIdx.x; s < n; s += blockDim.x) {
+                    const int64_t j = sp[s];
+                    a.A_post[j] = a.post_set ? a.Am : __dadd_rn(a.A_post[j], a.Am);
+                }
+            __syncthreads();
+        }
+    }
+    bg_finish_step(a.ctl, a.last);
+}
+
+// SpikeMonitor (monitor.py:156-166): one block appends the step's spikes in
+// ascending order.
+struct MonArgs {
+    DevCtl *ctl;
+    const uint32_t *hist; int depth; int64_t nwords; int delay;
+    int64_t origin, n;
+    long long *cnt; int64_t cap; int32_t *idx; int32_t *steps;   // steps relative to the chunk base
+    const long long *step_base;
+    int last;
+};
+constexpr int kMonThreads = 1024;
+__global__ void __launch_bounds__(kMonThreads) k_spikemon(const MonArgs a) {
+    __shared__ int wcnt[kMonThreads / 32 + 1];
+    const long long nstep = a.ctl->nstep;
+    if (nstep >= a.delay && blockIdx.x == 0) {
+        const long long cs = nstep + a.ctl->clock_off;
+        const uint32_t *H = a.hist + (int64_t)((nstep - a.delay) % a.depth) * a.nwords;
+        const int64_t end = a.origin + a.n;
+        const int64_t w0 = a.origin >> 5, w1 = (end + 31) >> 5;
+        long long base = *a.cnt;
+        const int tid = threadIdx.x;
+        for (int64_t cw = w0; cw < w1; cw += kMonThreads) {
+            const int64_t wi = cw + tid;
+            uint32_t word = wi < w1 ? masked_word(H, wi, a.origin, end) : 0u;
+            const int pc = __popc(word);
+            int incl = pc;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) { int v = __shfl_up_sync(0xffffffffu, incl, o); if ((tid & 31) >= o) incl += v; }
+            if ((tid & 31) == 31) wcnt[tid >> 5] = incl;
+            __syncthreads();
+            if (tid == 0) { int s = 0; for (int q = 0; q < kMonThreads / 32; ++q) { int v = wcnt[q]; wcnt[q] = s; s += v; } wcnt[kMonThreads / 32] = s; }
+            __syncthreads();
+            long long o = base + wcnt[tid >> 5] + incl - pc;
+            while (word) {
+                const int b = __ffs(word) - 1; word &= word - 1;
+                if (o < a.cap) { a.idx[o] = (int32_t)(((wi << 5) + b) - a.origin); a.steps[o] = (int32_t)(cs - *a.step_base); }
+                else bg_raise(a.ctl, BG_DERR_MONITOR_OVERFLOW, o);
+                ++o;
+            }
+            base += wcnt[kMonThreads / 32];
+            __syncthreads();
+        }
+        if (tid == 0) *a.cnt = base;
+    }
+    bg_finish_step(a.ctl, a.last);
+}
+
+}  // namespace bg

@@ -1,0 +1,975 @@
+// bg_net.cu -- host runtime of the clock-driven network engine (C ABI).
+//
+// A bg_net holds the device image of a Brian Network: per-group state
+// matrices, bit-per-neuron spike history rings, CSR connection matrices,
+// DelayConnection rings, STDP traces and monitor buffers.  bg_net_prepare
+// freezes the schedule into a per-step list of kernel launches; bg_net_run
+// replays it from a CUDA graph of kGraphSteps steps, draining monitor
+// buffers to host memory between chunks.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <string>
+#include <vector>
+
+#include "bg_kernels.cuh"
+#include "../../include/brian_b200.h"
+
+namespace {
+
+thread_local std::string g_err;
+int fail(int code, const std::string &m) { g_err = m; return code; }
+
+#define BG_CUDA(call)                                                                    \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return fail(BG_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_));   \
+    } while (0)
+
+constexpr int kGraphSteps = 32;
+constexpr int64_t kChunkSteps = 1024;
+
+struct HGroup {
+    int64_t n = 0, npad = 0; int nvar = 0;
+    std::vector<double> S0;
+    bool linear = false, useC = false; std::vector<double> A, C;
+    int thr_kind = 0, thr_var = 0, thr_var2 = 0; double thr_val = 0;
+    int rate_var = 0; uint64_t seed = 0;
+    std::vector<int64_t> gen_steps; std::vector<int32_t> gen_idx;
+    int reset_kind = 0, reset_var = 0, reset_var2 = 0; double reset_val = 0;
+    bool refr = false; double refr_time = 0; int period = 0; int clamp_var = 0; double clamp_val = 0;
+    int depth = 1;
+    void *dS = nullptr; uint32_t *dHist = nullptr; double *dNext = nullptr; int32_t *dLast = nullptr;
+    int64_t *dGenSteps = nullptr; int32_t *dGenIdx = nullptr;
+    std::vector<int> delivs, recs;
+};
+struct HConn {
+    int32_t src = 0, tgt = 0; int64_t so = 0, sn = 0, to = 0, tn = 0; int var = 0;
+    bool dense = false; int64_t nnz = 0;
+    std::vector<int64_t> rowptr; std::vector<int32_t> cols; std::vector<char> w; int w_bits = 64;
+    int32_t delay = 0; bool hetero = false; std::vector<uint8_t> d; int md = 0; int mod_var = -1;
+    bool homogeneous = false; int parts = 1; int stdp = -1;
+    int64_t *dRow = nullptr; int32_t *dCols = nullptr; void *dW = nullptr; uint8_t *dD = nullptr; void *dRing = nullptr;
+    int64_t *dColptr = nullptr, *dColk = nullptr; int32_t *dColsrc = nullptr;
+    int64_t wcount() const { return dense ? sn * tn : nnz; }
+};
+struct HStdp {
+    int cid; double a_pre, c_pre, a_post, c_post, Ap, Am, wmin, wmax; int inter; int pre_delay, post_delay;
+    double *dApre = nullptr, *dApost = nullptr; bool fused = false;
+};
+struct HSpikeMon {
+    int gid; int64_t origin, n; int delay;
+    long long *dCnt = nullptr, *dBase = nullptr; int32_t *dIdx = nullptr, *dSteps = nullptr; int64_t cap = 0;
+    std::vector<int64_t> steps; std::vector<int32_t> idx;
+};
+struct HStateMon {
+    int gid; int var; std::vector<int32_t> idx; int timestep; long long start = 0;
+    std::vector<int32_t> sorted, pos, blk_lo;
+    int32_t *dIdx = nullptr, *dPos = nullptr, *dBlk = nullptr; void *dBuf = nullptr; long long *dRowBase = nullptr;
+    int64_t cap_rows = 0; long long rows_done = 0;
+    std::vector<double> vals; std::vector<int64_t> steps;
+};
+enum { IT_CONN = 0, IT_SPIKEMON = 1, IT_STDP_PRE = 2, IT_STDP_POST = 3 };
+struct Item { int kind; int id; };
+
+using Launch = std::function<cudaError_t(cudaStream_t, int tail, int last)>;
+
+}  // namespace
+
+struct bg_net {
+    int device = 0, precision = 64, deterministic = 1; double dt = 1e-4;
+    cudaStream_t stream = nullptr;
+    std::vector<HGroup> groups; std::vector<HConn> conns; std::vector<HStdp> stdps;
+    std::vector<HSpikeMon> smons; std::vector<HStateMon> stmons; std::vector<Item> items;
+    std::vector<int> mon_kind, mon_idx;
+    DevCtl *dCtl = nullptr;
+    bool prepared = false; long long nstep = 0;
+    std::vector<Launch> step_launches;     // per-step kernels in schedule order
+    std::vector<Launch> finalize_launches; // tail-only head kernels
+    cudaGraphExec_t gexec = nullptr;
+    int64_t launches = 0; double last_ms = 0;
+    std::vector<void *> allocs;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int64_t chunk_steps = kChunkSteps;
+
+    template <typename P> cudaError_t alloc(P **p, size_t bytes) {
+        void *q = nullptr;
+        cudaError_t e = cudaMalloc(&q, bytes ? bytes : 16);
+        if (e == cudaSuccess) { allocs.push_back(q); *p = (P *)q; }
+        return e;
+    }
+};
+
+namespace {
+
+size_t tsize(const bg_net *n) { return n->precision == 64 ? 8 : 4; }
+
+bool gid_ok(const bg_net *n, int32_t g) { return n && g >= 0 && g < (int32_t)n->groups.size(); }
+
+// ------------------------------------------------------------------ launches
+template <typename T, int NV>
+cudaError_t launch_head_nv(const bg::HeadArgs<T> &a, int64_t blocks, cudaStream_t s) {
+    bg::k_head<T, NV><<<(unsigned)blocks, bg::kHeadThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+template <typename T>
+cudaError_t launch_head(const bg::HeadArgs<T> &a, int nvar, int64_t blocks, cudaStream_t s) {
+    switch (nvar) {
+    case 0: case 1: return launch_head_nv<T, 1>(a, blocks, s);
+    case 2: return launch_head_nv<T, 2>(a, blocks, s);
+    case 3: return launch_head_nv<T, 3>(a, blocks, s);
+    case 4: return launch_head_nv<T, 4>(a, blocks, s);
+    case 5: return launch_head_nv<T, 5>(a, blocks, s);
+    case 6: return launch_head_nv<T, 6>(a, blocks, s);
+    case 7: return launch_head_nv<T, 7>(a, blocks, s);
+    default: return launch_head_nv<T, 8>(a, blocks, s);
+    }
+}
+
+template <typename T>
+int build_group(bg_net *net, int gid) {
+    HGroup &g = net->groups[gid];
+    bg::HeadArgs<T> a;
+    std::memset(&a, 0, sizeof(a));
+    a.ctl = net->dCtl; a.S = (T *)g.dS; a.n = g.n; a.npad = g.npad; a.nvar = g.nvar;
+    a.linear = g.linear; a.useC = g.useC;
+    for (int j = 0; j < g.nvar && g.linear; ++j) {
+        for (int k = 0; k < g.nvar; ++k) a.A[j * g.nvar + k] = (T)g.A[j * g.nvar + k];
+        a.C[j] = g.useC ? (T)g.C[j] : T(0);
+    }
+    a.thr_kind = g.thr_kind; a.thr_var = g.thr_var; a.thr_var2 = g.thr_var2; a.thr_val = (T)g.thr_val;
+    a.dt = net->dt; a.seed = g.seed; a.rate_var = g.rate_var;
+    a.gen_steps = g.dGenSteps; a.gen_idx = g.dGenIdx; a.gen_n = (int64_t)g.gen_steps.size();
+    a.reset_kind = g.reset_kind; a.reset_var = g.reset_var; a.reset_var2 = g.reset_var2; a.reset_val = (T)g.reset_val;
+    a.refr = g.refr; a.refr_time = g.refr_time; a.period = g.period; a.clamp_var = g.clamp_var; a.clamp_val = (T)g.clamp_val;
+    a.next_allowed = g.dNext; a.last_spike = g.dLast;
+    a.hist = g.dHist; a.depth = g.depth; a.nwords = g.npad / 32;
+    if ((int)g.delivs.size() > bg::kMaxDeliv) return fail(BG_ENOSYS, "too many DelayConnections into one group");
+    a.ndeliv = (int)g.delivs.size();
+    for (int k = 0; k < a.ndeliv; ++k) {
+        const HConn &c = net->conns[g.delivs[k]];
+        a.deliv[k].ring = (T *)c.dRing; a.deliv[k].tn = c.tn; a.deliv[k].to = c.to; a.deliv[k].md = c.md; a.deliv[k].var = c.var;
+    }
+    if ((int)g.recs.size() > bg::kMaxRec) return fail(BG_ENOSYS, "too many StateMonitors on one group");
+    a.nrec = (int)g.recs.size();
+    for (int k = 0; k < a.nrec; ++k) {
+        const HStateMon &m = net->stmons[g.recs[k]];
+        bg::RecDev &r = a.rec[k];
+        r.var = m.var; r.nidx = (int)m.idx.size(); r.idx = m.dIdx; r.pos = m.dPos; r.blk_lo = m.dBlk;
+        r.buf = m.dBuf; r.row_base = m.dRowBase; r.timestep = m.timestep; r.start = m.start;
+    }
+    const int64_t blocks = g.npad / bg::kHeadThreads;
+    const int nvar = g.nvar;
+    if (nvar > bg::kMaxVars) return fail(BG_ENOSYS, "more than 8 state variables in a linear group");
+    const bool has_tail = a.ndeliv || g.reset_kind || g.period > 0 || a.nrec;
+    net->step_launches.push_back([a, nvar, blocks](cudaStream_t s, int tail, int last) {
+        bg::HeadArgs<T> b = a; b.tail = tail; b.update = 1; b.last = last;
+        return launch_head<T>(b, nvar, blocks, s);
+    });
+    if (has_tail)
+        net->finalize_launches.push_back([a, nvar, blocks](cudaStream_t s, int, int) {
+            bg::HeadArgs<T> b = a; b.tail = 1; b.update = 0; b.last = 0;
+            return launch_head<T>(b, nvar, blocks, s);
+        });
+    return BG_OK;
+}
+
+template <typename T, typename WT>
+cudaError_t launch_prop(const bg::PropArgs<T> &a, int mode, int64_t grid, cudaStream_t s) {
+    switch (mode) {
+    case 0: bg::k_prop_atomic<T, WT, false><<<(unsigned)grid, 256, 0, s>>>(a); break;
+    case 1: bg::k_prop_atomic<T, WT, true><<<(unsigned)grid, 256, 0, s>>>(a); break;
+    case 2: bg::k_prop_ordered<T, WT, false><<<(unsigned)grid, bg::kOrdThreads, 0, s>>>(a); break;
+    case 3: bg::k_prop_ordered<T, WT, true><<<(unsigned)grid, bg::kOrdThreads, 0, s>>>(a); break;
+    default: bg::k_prop_dense<T, WT><<<(unsigned)grid, bg::kDenseThreads, 0, s>>>(a); break;
+    }
+    return cudaGetLastError();
+}
+
+int sm_count() {
+    static int n = 0;
+    if (!n) { int dev = 0; cudaGetDevice(&dev); cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev); if (n <= 0) n = 148; }
+    return n;
+}
+
+template <typename T>
+int build_conn(bg_net *net, int cid) {
+    HConn &c = net->conns[cid];
+    const HGroup &gs = net->groups[c.src];
+    HGroup &gt = net->groups[c.tgt];
+    bg::PropArgs<T> a;
+    std::memset(&a, 0, sizeof(a));
+    a.ctl = net->dCtl; a.hist = gs.dHist; a.depth = gs.depth; a.nwords = gs.npad / 32;
+    a.delay = c.hetero ? 0 : c.delay; a.so = c.so; a.sn = c.sn; a.to = c.to; a.tn = c.tn;
+    a.sv = (T *)gt.dS + (int64_t)c.var * gt.npad + c.to;
+    a.ring = (T *)c.dRing; a.md = c.md;
+    a.rowptr = c.dRow; a.cols = c.dCols; a.w = c.dW; a.d = c.dD; a.dense = c.dense;
+    a.mod = c.mod_var >= 0 ? (const T *)gs.dS + (int64_t)c.mod_var * gs.npad + c.so : nullptr;
+    const double avg = c.sn ? (double)c.nnz / (double)c.sn : 0.0;
+    c.parts = std::max(1, std::min(32, (int)((avg + 63.0) / 64.0)));
+    a.parts = c.parts;
+    if (c.stdp >= 0 && net->stdps[c.stdp].fused) {
+        HStdp &s = net->stdps[c.stdp];
+        a.stdp = 1; a.A_pre = s.dApre; a.A_post = s.dApost; a.Ap = s.Ap;
+        a.pre_set = (s.inter == BG_STDP_NEAREST || s.inter == BG_STDP_NEAREST_PRE);
+        a.wmin = s.wmin; a.wmax = s.wmax;
+    }
+    int mode; int64_t grid;
+    const bool use_atomic = !c.dense && c.mod_var < 0 && (c.homogeneous || !net->deterministic) && !a.stdp;
+    if (c.dense) { mode = 4; grid = (c.tn + bg::kDenseThreads - 1) / bg::kDenseThreads; }
+    else if (use_atomic) {
+        mode = c.hetero ? 1 : 0;
+        const int64_t nch = ((c.so + c.sn + 31) / 32 - c.so / 32 + 31) / 32;
+        const int64_t warps = std::max<int64_t>(1, nch * c.parts);
+        grid = std::min<int64_t>((warps + 7) / 8, (int64_t)sm_count() * 8);
+    } else {
+        mode = c.hetero ? 3 : 2;
+        grid = std::max<int64_t>(1, (c.tn + bg::kOrdTB - 1) / bg::kOrdTB);
+    }
+    const int wb = c.w_bits;
+    net->step_launches.push_back([a, mode, grid, wb](cudaStream_t s, int, int last) {
+        bg::PropArgs<T> b = a; b.last = last;
+        return wb == 64 ? launch_prop<T, double>(b, mode, grid, s) : launch_prop<T, float>(b, mode, grid, s);
+    });
+    return BG_OK;
+}
+
+int build_stdp_pre(bg_net *net, int sid) {
+    HStdp &s = net->stdps[sid];
+    if (s.fused) return BG_OK;
+    HConn &c = net->conns[s.cid];
+    const HGroup &gs = net->groups[c.src];
+    bg::PropArgs<double> a;
+    std::memset(&a, 0, sizeof(a));
+    a.ctl = net->dCtl; a.hist = gs.dHist; a.depth = gs.depth; a.nwords = gs.npad / 32; a.delay = s.pre_delay;
+    a.so = c.so; a.sn = c.sn; a.to = c.to; a.tn = c.tn; a.rowptr = c.dRow; a.cols = c.dCols; a.w = c.dW; a.dense = c.dense;
+    a.stdp = 1; a.A_pre = s.dApre; a.A_post = s.dApost; a.Ap = s.Ap;
+    a.pre_set = (s.inter == BG_STDP_NEAREST || s.inter == BG_STDP_NEAREST_PRE); a.wmin = s.wmin; a.wmax = s.wmax;
+    const int64_t nwords = (c.so + c.sn + 31) / 32 - c.so / 32;
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((nwords + 255) / 256, (int64_t)sm_count() * 4));
+    const int wb = c.w_bits;
+    net->step_launches.push_back([a, grid, wb](cudaStream_t st, int, int last) {
+        bg::PropArgs<double> b = a; b.last = last;
+        if (wb == 64) bg::k_stdp_pre<double><<<(unsigned)grid, 256, 0, st>>>(b);
+        else bg::k_stdp_pre<float><<<(unsigned)grid, 256, 0, st>>>(b);
+        return cudaGetLastError();
+    });
+    return BG_OK;
+}
+
+int build_stdp_post(bg_net *net, int sid) {
+    HStdp &s = net->stdps[sid];
+    HConn &c = net->conns[s.cid];
+    const HGroup &gt = net->groups[c.tgt];
+    bg::PostArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.ctl = net->dCtl; a.hist = gt.dHist; a.depth = gt.depth; a.nwords = gt.npad / 32; a.delay = s.post_delay;
+    a.to = c.to; a.tn = c.tn; a.sn = c.sn; a.w = c.dW; a.dense = c.dense;
+    a.colptr = c.dColptr; a.colk = c.dColk; a.colsrc = c.dColsrc;
+    a.A_post = s.dApost; a.A_pre = s.dApre; a.Am = s.Am;
+    a.post_set = (s.inter != BG_STDP_ALL);   // 'nearest_pre' writes A_post=+Am (stdp.py:500-502)
+    a.wmin = s.wmin; a.wmax = s.wmax;
+    const int64_t grid = c.dense ? std::max<int64_t>(1, std::min<int64_t>((c.sn + 255) / 256, (int64_t)sm_count() * 2)) : 8;
+    const int wb = c.w_bits;
+    net->step_launches.push_back([a, grid, wb](cudaStream_t st, int, int last) {
+        bg::PostArgs b = a; b.last = last;
+        if (wb == 64) bg::k_stdp_post<double><<<(unsigned)grid, 256, 0, st>>>(b);
+        else bg::k_stdp_post<float><<<(unsigned)grid, 256, 0, st>>>(b);
+        return cudaGetLastError();
+    });
+    return BG_OK;
+}
+
+int build_spikemon(bg_net *net, int k) {
+    HSpikeMon &m = net->smons[k];
+    const HGroup &g = net->groups[m.gid];
+    bg::MonArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.ctl = net->dCtl; a.hist = g.dHist; a.depth = g.depth; a.nwords = g.npad / 32; a.delay = m.delay;
+    a.origin = m.origin; a.n = m.n; a.cnt = m.dCnt; a.cap = m.cap; a.idx = m.dIdx; a.steps = m.dSteps; a.step_base = m.dBase;
+    net->step_launches.push_back([a](cudaStream_t st, int, int last) {
+        bg::MonArgs b = a; b.last = last;
+        bg::k_spikemon<<<1, bg::kMonThreads, 0, st>>>(b);
+        return cudaGetLastError();
+    });
+    return BG_OK;
+}
+
+int build_decay(bg_net *net, int sid) {
+    HStdp &s = net->stdps[sid];
+    const HConn &c = net->conns[s.cid];
+    bg::DecayArgs a;
+    a.A_pre = s.dApre; a.npre = c.sn; a.a_pre = s.a_pre; a.c_pre = s.c_pre;
+    a.A_post = s.dApost; a.npost = c.tn; a.a_post = s.a_post; a.c_post = s.c_post; a.ctl = net->dCtl; a.last = 0;
+    const int64_t grid = std::max<int64_t>(1, (c.sn + c.tn + 255) / 256);
+    net->step_launches.push_back([a, grid](cudaStream_t st, int, int last) {
+        bg::DecayArgs b = a; b.last = last;
+        bg::k_stdp_decay<<<(unsigned)grid, 256, 0, st>>>(b);
+        return cudaGetLastError();
+    });
+    return BG_OK;
+}
+
+int upload(bg_net *net, void *dst, const void *src, size_t bytes) {
+    BG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, net->stream));
+    return BG_OK;
+}
+
+int upload_state(bg_net *net, HGroup &g, int var, const double *in) {
+    if (net->precision == 64) return upload(net, (double *)g.dS + (size_t)var * g.npad, in, g.n * 8);
+    std::vector<float> tmp(g.n);
+    for (int64_t i = 0; i < g.n; ++i) tmp[i] = (float)in[i];
+    int st = upload(net, (float *)g.dS + (size_t)var * g.npad, tmp.data(), g.n * 4);
+    if (st) return st;
+    BG_CUDA(cudaStreamSynchronize(net->stream));
+    return BG_OK;
+}
+
+int reset_dynamic(bg_net *net) {
+    for (auto &g : net->groups) {
+        BG_CUDA(cudaMemsetAsync(g.dHist, 0, (size_t)g.depth * (g.npad / 32) * 4, net->stream));
+        if (g.dNext) {
+            std::vector<double> m1(g.npad, -1.0);
+            BG_CUDA(cudaMemcpyAsync(g.dNext, m1.data(), g.npad * 8, cudaMemcpyHostToDevice, net->stream));
+            BG_CUDA(cudaStreamSynchronize(net->stream));
+        }
+        if (g.dLast) {
+            std::vector<int32_t> m(g.npad, -(1 << 30));
+            BG_CUDA(cudaMemcpyAsync(g.dLast, m.data(), g.npad * 4, cudaMemcpyHostToDevice, net->stream));
+            BG_CUDA(cudaStreamSynchronize(net->stream));
+        }
+    }
+    for (auto &c : net->conns)
+        if (c.dRing) BG_CUDA(cudaMemsetAsync(c.dRing, 0, (size_t)c.md * c.tn * tsize(net), net->stream));
+    for (auto &s : net->stdps) {
+        const HConn &c = net->conns[s.cid];
+        BG_CUDA(cudaMemsetAsync(s.dApre, 0, c.sn * 8, net->stream));
+        BG_CUDA(cudaMemsetAsync(s.dApost, 0, c.tn * 8, net->stream));
+    }
+    return BG_OK;
+}
+
+int check_device_error(bg_net *net) {
+    DevCtl h;
+    BG_CUDA(cudaMemcpyAsync(&h, net->dCtl, sizeof(h), cudaMemcpyDeviceToHost, net->stream));
+    BG_CUDA(cudaStreamSynchronize(net->stream));
+    if (h.err == BG_DERR_MONITOR_OVERFLOW) return fail(BG_ESTATE, "spike monitor buffer overflow");
+    if (h.err) return fail(BG_ESTATE, "device error " + std::to_string(h.err));
+    return BG_OK;
+}
+
+// Copy monitor records of the finished chunk to host memory.
+// `tail_done_upto`: last step whose 'end' slot has run.
+int drain(bg_net *net, long long chunk_base_cs, long long tail_done_upto, long long off) {
+    BG_CUDA(cudaStreamSynchronize(net->stream));
+    for (auto &m : net->smons) {
+        long long cnt = 0;
+        BG_CUDA(cudaMemcpy(&cnt, m.dCnt, 8, cudaMemcpyDeviceToHost));
+        if (cnt > m.cap) return fail(BG_ESTATE, "spike monitor buffer overflow");
+        if (cnt > 0) {
+            std::vector<int32_t> idx(cnt), st(cnt);
+            BG_CUDA(cudaMemcpy(idx.data(), m.dIdx, cnt * 4, cudaMemcpyDeviceToHost));
+            BG_CUDA(cudaMemcpy(st.data(), m.dSteps, cnt * 4, cudaMemcpyDeviceToHost));
+            for (long long k = 0; k < cnt; ++k) { m.idx.push_back(idx[k]); m.steps.push_back(chunk_base_cs + st[k]); }
+            long long z = 0;
+            BG_CUDA(cudaMemcpy(m.dCnt, &z, 8, cudaMemcpyHostToDevice));
+        }
+    }
+    for (auto &m : net->stmons) {
+        // records exist for ps in [start, tail_done_upto] with (ps-start) % timestep == 0
+        long long total = tail_done_upto < m.start ? 0 : (tail_done_upto - m.start) / m.timestep + 1;
+        long long fresh = total - m.rows_done;
+        if (fresh <= 0) continue;
+        if (fresh > m.cap_rows) return fail(BG_ESTATE, "state monitor buffer overflow");
+        const size_t w = m.idx.size();
+        const size_t ts = tsize(net);
+        std::vector<char> buf(fresh * w * ts);
+        if (buf.size()) BG_CUDA(cudaMemcpy(buf.data(), m.dBuf, buf.size(), cudaMemcpyDeviceToHost));
+        for (long long r = 0; r < fresh; ++r) {
+            for (size_t j = 0; j < w; ++j)
+                m.vals.push_back(ts == 8 ? ((double *)buf.data())[r * w + j] : (double)((float *)buf.data())[r * w + j]);
+            const long long ps = m.start + (m.rows_done + r) * m.timestep;
+            m.steps.push_back(ps + off);   // clock step of the record
+        }
+        m.rows_done = total;
+        BG_CUDA(cudaMemcpy(m.dRowBase, &m.rows_done, 8, cudaMemcpyHostToDevice));
+    }
+    return BG_OK;
+}
+
+}  // namespace
+
+// ============================================================== C ABI
+extern "C" {
+
+int bg_version(void) { return 1; }
+
+int bg_last_error(char *buf, int64_t len) {
+    if (!buf || len <= 0) return BG_EINVAL;
+    std::strncpy(buf, g_err.c_str(), (size_t)len - 1);
+    buf[len - 1] = 0;
+    return BG_OK;
+}
+
+int bg_net_create(int device, int precision, int deterministic, double dt, bg_net **out) {
+    if (!out || !(dt > 0)) return fail(BG_EINVAL, "bg_net_create: bad dt or out");
+    if (precision != 64 && precision != 32) return fail(BG_EINVAL, "precision must be 64 or 32");
+    int ndev = 0;
+    BG_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return fail(BG_EINVAL, "no such CUDA device");
+    BG_CUDA(cudaSetDevice(device));
+    bg_net *n = new bg_net();
+    n->device = device; n->precision = precision; n->deterministic = deterministic; n->dt = dt;
+    cudaError_t e = cudaStreamCreateWithFlags(&n->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { delete n; return fail(BG_ECUDA, cudaGetErrorString(e)); }
+    if (n->alloc(&n->dCtl, sizeof(DevCtl)) != cudaSuccess) { delete n; return fail(BG_ENOMEM, "ctl"); }
+    cudaMemset(n->dCtl, 0, sizeof(DevCtl));
+    cudaEventCreate(&n->ev0); cudaEventCreate(&n->ev1);
+    *out = n;
+    return BG_OK;
+}
+
+int bg_net_destroy(bg_net *n) {
+    if (!n) return BG_OK;
+    cudaSetDevice(n->device);
+    if (n->stream) cudaStreamSynchronize(n->stream);
+    if (n->gexec) cudaGraphExecDestroy(n->gexec);
+    for (void *p : n->allocs) cudaFree(p);
+    if (n->ev0) cudaEventDestroy(n->ev0);
+    if (n->ev1) cudaEventDestroy(n->ev1);
+    if (n->stream) cudaStreamDestroy(n->stream);
+    delete n;
+    return BG_OK;
+}
+
+int bg_group_add(bg_net *n, int64_t N, int nvar, const double *S0, int32_t *gid) {
+    if (!n || N < 0 || nvar < 0 || (N > 0 && nvar > 0 && !S0) || !gid) return fail(BG_EINVAL, "bg_group_add");
+    if (n->prepared) return fail(BG_ESTATE, "network already prepared");
+    if (nvar > bg::kMaxVars) return fail(BG_ENOSYS, "at most 8 state variables per group");
+    HGroup g; g.n = N; g.nvar = nvar;
+    g.npad = std::max<int64_t>(bg::kHeadThreads, (N + bg::kHeadThreads - 1) / bg::kHeadThreads * bg::kHeadThreads);
+    g.S0.assign(S0, S0 + (size_t)N * nvar);
+    n->groups.push_back(std::move(g));
+    *gid = (int32_t)n->groups.size() - 1;
+    return BG_OK;
+}
+
+int bg_group_set_linear(bg_net *n, int32_t gid, const double *A, const double *C) {
+    if (!gid_ok(n, gid) || !A) return fail(BG_EINVAL, "bg_group_set_linear");
+    if (n->prepared) return fail(BG_ESTATE, "network already prepared");
+    HGroup &g = n->groups[gid];
+    g.linear = true; g.A.assign(A, A + g.nvar * g.nvar);
+    g.useC = C != nullptr; if (C) g.C.assign(C, C + g.nvar);
+    return BG_OK;
+}
+
+int bg_group_set_threshold(bg_net *n, int32_t gid, int kind, int var, double value, int var2) {
+    if (!gid_ok(n, gid) || kind < 0 || kind > 2) return fail(BG_EINVAL, "bg_group_set_threshold");
+    HGroup &g = n->groups[gid];
+    if (kind && (var < 0 || var >= g.nvar)) return fail(BG_EINVAL, "threshold variable out of range");
+    if (kind == 2 && (var2 < 0 || var2 >= g.nvar)) return fail(BG_EINVAL, "threshold variable out of range");
+    g.thr_kind = kind; g.thr_var = var; g.thr_val = value; g.thr_var2 = var2;
+    return BG_OK;
+}
+
+int bg_group_set_poisson(bg_net *n, int32_t gid, int rate_var, uint64_t seed) {
+    if (!gid_ok(n, gid)) return fail(BG_EINVAL, "bg_group_set_poisson");
+    HGroup &g = n->groups[gid];
+    if (rate_var < 0 || rate_var >= g.nvar) return fail(BG_EINVAL, "rate variable out of range");
+    g.thr_kind = BG_THR_POISSON; g.rate_var = rate_var; g.seed = seed;
+    return BG_OK;
+}
+
+int bg_group_set_generator(bg_net *n, int32_t gid, int64_t ns, const int64_t *steps, const int32_t *idx) {
+    if (!gid_ok(n, gid) || ns < 0 || (ns > 0 && (!steps || !idx))) return fail(BG_EINVAL, "bg_group_set_generator");
+    HGroup &g = n->groups[gid];
+    for (int64_t k = 0; k < ns; ++k) {
+        if (idx[k] < 0 || idx[k] >= g.n) return fail(BG_EINVAL, "generator index out of range");
+        if (k && (steps[k] < steps[k - 1] || (steps[k] == steps[k - 1] && idx[k] < idx[k - 1])))
+            return fail(BG_EINVAL, "generator spikes not sorted by (step, index)");
+    }
+    g.thr_kind = BG_THR_GENERATOR; g.gen_steps.assign(steps, steps + ns); g.gen_idx.assign(idx, idx + ns);
+    return BG_OK;
+}
+
+int bg_group_set_reset(bg_net *n, int32_t gid, int kind, int var, double value, int var2) {
+    if (!gid_ok(n, gid) || kind < 0 || kind > 2) return fail(BG_EINVAL, "bg_group_set_reset");
+    HGroup &g = n->groups[gid];
+    if (kind && (var < 0 || var >= g.nvar)) return fail(BG_EINVAL, "reset variable out of range");
+    if (kind == 2 && (var2 < 0 || var2 >= g.nvar)) return fail(BG_EINVAL, "reset variable out of range");
+    g.reset_kind = kind; g.reset_var = var; g.reset_val = value; g.reset_var2 = var2;
+    return BG_OK;
+}
+
+int bg_group_set_refractory(bg_net *n, int32_t gid, double rt, int32_t period, int var, double value) {
+    if (!gid_ok(n, gid) || period < 0) return fail(BG_EINVAL, "bg_group_set_refractory");
+    HGroup &g = n->groups[gid];
+    if (period > 0 && (var < 0 || var >= g.nvar)) return fail(BG_EINVAL, "clamp variable out of range");
+    // rt <= 0: no spike filter (refractory < 0.9*dt), clamp only
+    g.refr = rt > 0; g.refr_time = rt; g.period = period; g.clamp_var = var; g.clamp_val = value;
+    return BG_OK;
+}
+
+static int conn_common(bg_net *n, int32_t src, int64_t so, int64_t sn, int32_t tgt, int64_t to, int64_t tn,
+                       int var, int32_t delay, int mod_var, HConn &c) {
+    if (!gid_ok(n, src) || !gid_ok(n, tgt)) return fail(BG_EINVAL, "connection group id");
+    if (n->prepared) return fail(BG_ESTATE, "network already prepared");
+    const HGroup &gs = n->groups[src], &gt = n->groups[tgt];
+    if (so < 0 || sn < 0 || so + sn > gs.n || to < 0 || tn < 0 || to + tn > gt.n) return fail(BG_EINVAL, "connection ranges");
+    if (var < 0 || var >= gt.nvar) return fail(BG_EINVAL, "connection target variable");
+    if (delay < 0 || delay > 1 << 20) return fail(BG_EINVAL, "connection delay");
+    if (mod_var >= gs.nvar) return fail(BG_EINVAL, "modulation variable");
+    c.src = src; c.tgt = tgt; c.so = so; c.sn = sn; c.to = to; c.tn = tn; c.var = var; c.delay = delay; c.mod_var = mod_var;
+    return BG_OK;
+}
+
+int bg_conn_add(bg_net *n, int32_t src, int64_t so, int64_t sn, int32_t tgt, int64_t to, int64_t tn, int var,
+                int64_t nnz, const int64_t *rowptr, const int32_t *cols, const void *w, int w_bits, int32_t delay,
+                const uint8_t *delays, int32_t ring_depth, int mod_var, int32_t *cid) {
+    HConn c;
+    int st = conn_common(n, src, so, sn, tgt, to, tn, var, delay, mod_var, c);
+    if (st) return st;
+    if (w_bits != 32 && w_bits != 64) return fail(BG_EINVAL, "w_bits must be 32 or 64");
+    if (!rowptr || nnz < 0 || (nnz > 0 && (!cols || !w)) || !cid) return fail(BG_EINVAL, "CSR arrays");
+    if (rowptr[0] != 0 || rowptr[sn] != nnz) return fail(BG_EINVAL, "rowptr must start at 0 and end at nnz");
+    for (int64_t i = 0; i < sn; ++i) {
+        if (rowptr[i + 1] < rowptr[i]) return fail(BG_EINVAL, "rowptr not monotone");
+        for (int64_t k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+            if (cols[k] < 0 || cols[k] >= tn) return fail(BG_EINVAL, "column index out of range");
+            if (k > rowptr[i] && cols[k] <= cols[k - 1]) return fail(BG_EINVAL, "columns not strictly ascending in a row");
+        }
+    }
+    c.nnz = nnz; c.rowptr.assign(rowptr, rowptr + sn + 1); c.cols.assign(cols, cols + nnz);
+    c.w_bits = w_bits;
+    c.w.assign((const char *)w, (const char *)w + nnz * (w_bits / 8));
+    c.homogeneous = true;
+    for (int64_t k = 1; k < nnz && c.homogeneous; ++k)
+        c.homogeneous = std::memcmp(&c.w[0], &c.w[k * (w_bits / 8)], w_bits / 8) == 0;
+    if (delays) {
+        if (ring_depth < 1 || ring_depth > 255) return fail(BG_EINVAL, "ring depth must be in [1, 255]");
+        for (int64_t k = 0; k < nnz; ++k) if (delays[k] >= ring_depth) return fail(BG_EINVAL, "delay >= ring depth");
+        c.hetero = true; c.md = ring_depth; c.d.assign(delays, delays + nnz);
+    }
+    n->conns.push_back(std::move(c));
+    *cid = (int32_t)n->conns.size() - 1;
+    n->items.push_back({IT_CONN, *cid});
+    return BG_OK;
+}
+
+int bg_conn_add_dense(bg_net *n, int32_t src, int64_t so, int64_t sn, int32_t tgt, int64_t to, int64_t tn, int var,
+                      const void *W, int w_bits, int32_t delay, int mod_var, int32_t *cid) {
+    HConn c;
+    int st = conn_common(n, src, so, sn, tgt, to, tn, var, delay, mod_var, c);
+    if (st) return st;
+    if ((w_bits != 32 && w_bits != 64) || (!W && sn * tn > 0) || !cid) return fail(BG_EINVAL, "dense weights");
+    c.dense = true; c.w_bits = w_bits; c.nnz = sn * tn;
+    c.w.assign((const char *)W, (const char *)W + sn * tn * (w_bits / 8));
+    n->conns.push_back(std::move(c));
+    *cid = (int32_t)n->conns.size() - 1;
+    n->items.push_back({IT_CONN, *cid});
+    return BG_OK;
+}
+
+int bg_conn_get_weights(bg_net *n, int32_t cid, double *out) {
+    if (!n || cid < 0 || cid >= (int32_t)n->conns.size() || !out) return fail(BG_EINVAL, "bg_conn_get_weights");
+    HConn &c = n->conns[cid];
+    const int64_t cnt = c.wcount();
+    if (n->prepared) {
+        BG_CUDA(cudaStreamSynchronize(n->stream));
+        BG_CUDA(cudaMemcpy(c.w.data(), c.dW, c.w.size(), cudaMemcpyDeviceToHost));
+    }
+    for (int64_t k = 0; k < cnt; ++k)
+        out[k] = c.w_bits == 64 ? ((const double *)c.w.data())[k] : (double)((const float *)c.w.data())[k];
+    return BG_OK;
+}
+
+int bg_conn_set_weights(bg_net *n, int32_t cid, const double *in) {
+    if (!n || cid < 0 || cid >= (int32_t)n->conns.size() || !in) return fail(BG_EINVAL, "bg_conn_set_weights");
+    HConn &c = n->conns[cid];
+    const int64_t cnt = c.wcount();
+    for (int64_t k = 0; k < cnt; ++k) {
+        if (c.w_bits == 64) ((double *)c.w.data())[k] = in[k];
+        else ((float *)c.w.data())[k] = (float)in[k];
+    }
+    if (n->prepared) {
+        BG_CUDA(cudaStreamSynchronize(n->stream));
+        BG_CUDA(cudaMemcpy(c.dW, c.w.data(), c.w.size(), cudaMemcpyHostToDevice));
+    }
+    return BG_OK;
+}
+
+int bg_stdp_add(bg_net *n, int32_t cid, const double *decay, double Ap, double Am, double wmin, double wmax, int inter,
+                int32_t pre_delay, int32_t post_delay, int32_t *sid) {
+    if (!n || cid < 0 || cid >= (int32_t)n->conns.size() || !decay || !sid) return fail(BG_EINVAL, "bg_stdp_add");
+    if (n->prepared) return fail(BG_ESTATE, "network already prepared");
+    HConn &c = n->conns[cid];
+    if (c.hetero) return fail(BG_ENOSYS, "STDP on a DelayConnection is not supported");
+    if (c.stdp >= 0) return fail(BG_ENOSYS, "one STDP rule per connection");
+    if (pre_delay < 0 || post_delay < 0 || inter < 0 || inter > 3) return fail(BG_EINVAL, "STDP parameters");
+    HStdp s; s.cid = cid; s.a_pre = decay[0]; s.c_pre = decay[1]; s.a_post = decay[2]; s.c_post = decay[3];
+    s.Ap = Ap; s.Am = Am; s.wmin = wmin; s.wmax = wmax; s.inter = inter; s.pre_delay = pre_delay; s.post_delay = post_delay;
+    n->stdps.push_back(s);
+    *sid = (int32_t)n->stdps.size() - 1;
+    c.stdp = *sid;
+    n->items.push_back({IT_STDP_PRE, *sid});
+    n->items.push_back({IT_STDP_POST, *sid});
+    return BG_OK;
+}
+
+int bg_stdp_get_traces(bg_net *n, int32_t sid, double *a_pre, double *a_post) {
+    if (!n || sid < 0 || sid >= (int32_t)n->stdps.size()) return fail(BG_EINVAL, "bg_stdp_get_traces");
+    if (!n->prepared) return fail(BG_ESTATE, "network not prepared");
+    const HStdp &s = n->stdps[sid]; const HConn &c = n->conns[s.cid];
+    BG_CUDA(cudaStreamSynchronize(n->stream));
+    if (a_pre) BG_CUDA(cudaMemcpy(a_pre, s.dApre, c.sn * 8, cudaMemcpyDeviceToHost));
+    if (a_post) BG_CUDA(cudaMemcpy(a_post, s.dApost, c.tn * 8, cudaMemcpyDeviceToHost));
+    return BG_OK;
+}
+
+int bg_spikemon_add(bg_net *n, int32_t gid, int64_t origin, int64_t cnt, int32_t delay, int32_t *mid) {
+    if (!gid_ok(n, gid) || origin < 0 || cnt < 0 || origin + cnt > n->groups[gid].n || delay < 0 || !mid)
+        return fail(BG_EINVAL, "bg_spikemon_add");
+    if (n->prepared) return fail(BG_ESTATE, "network already prepared");
+    HSpikeMon m; m.gid = gid; m.origin = origin; m.n = cnt; m.delay = delay;
+    n->smons.push_back(m);
+    n->items.push_back({IT_SPIKEMON, (int)n->smons.size() - 1});
+    n->mon_kind.push_back(0); n->mon_idx.push_back((int)n->smons.size() - 1);
+    *mid = (int32_t)n->mon_kind.size() - 1;
+    return BG_OK;
+}
+
+int bg_statemon_add(bg_net *n, int32_t gid, int var, int64_t nidx, const int32_t *idx, int32_t timestep, int32_t *mid) {
+    if (!gid_ok(n, gid) || var < 0 || var >= n->groups[gid].nvar || timestep < 1 || nidx < 0 || !mid)
+        return fail(BG_EINVAL, "bg_statemon_add");
+    if (n->prepared) return fail(BG_ESTATE, "network already prepared");
+    HStateMon m; m.gid = gid; m.var = var; m.timestep = timestep;
+    const HGroup &g = n->groups[gid];
+    if (idx) m.idx.assign(idx, idx + nidx);
+    else { m.idx.resize(g.n); for (int64_t i = 0; i < g.n; ++i) m.idx[i] = (int32_t)i; }
+    for (int32_t i : m.idx) if (i < 0 || i >= g.n) return fail(BG_EINVAL, "state monitor index out of range");
+    n->stmons.push_back(std::move(m));
+    n->mon_kind.push_back(1); n->mon_idx.push_back((int)n->stmons.size() - 1);
+    *mid = (int32_t)n->mon_kind.size() - 1;
+    return BG_OK;
+}
+
+static bool mon_ok(const bg_net *n, int32_t mid, int kind) {
+    return n && mid >= 0 && mid < (int32_t)n->mon_kind.size() && n->mon_kind[mid] == kind;
+}
+
+int bg_spikemon_count(bg_net *n, int32_t mid, int64_t *cnt) {
+    if (!mon_ok(n, mid, 0) || !cnt) return fail(BG_EINVAL, "spike monitor id");
+    *cnt = (int64_t)n->smons[n->mon_idx[mid]].idx.size();
+    return BG_OK;
+}
+
+int bg_spikemon_read(bg_net *n, int32_t mid, int64_t *steps, int32_t *idx, int64_t cap, int64_t *cnt) {
+    if (!mon_ok(n, mid, 0) || !cnt || cap < 0) return fail(BG_EINVAL, "spike monitor id");
+    const HSpikeMon &m = n->smons[n->mon_idx[mid]];
+    const int64_t k = std::min<int64_t>(cap, (int64_t)m.idx.size());
+    if (k > 0) {
+        if (steps) std::memcpy(steps, m.steps.data(), k * 8);
+        if (idx) std::memcpy(idx, m.idx.data(), k * 4);
+    }
+    *cnt = k;
+    return BG_OK;
+}
+
+int bg_statemon_count(bg_net *n, int32_t mid, int64_t *rows) {
+    if (!mon_ok(n, mid, 1) || !rows) return fail(BG_EINVAL, "state monitor id");
+    *rows = (int64_t)n->stmons[n->mon_idx[mid]].steps.size();
+    return BG_OK;
+}
+
+int bg_statemon_read(bg_net *n, int32_t mid, double *vals, int64_t *steps, int64_t cap, int64_t *rows) {
+    if (!mon_ok(n, mid, 1) || !rows || cap < 0) return fail(BG_EINVAL, "state monitor id");
+    const HStateMon &m = n->stmons[n->mon_idx[mid]];
+    const int64_t r = std::min<int64_t>(cap, (int64_t)m.steps.size());
+    const int64_t w = (int64_t)m.idx.size();
+    if (r > 0) {
+        if (vals) std::memcpy(vals, m.vals.data(), r * w * 8);
+        if (steps) std::memcpy(steps, m.steps.data(), r * 8);
+    }
+    *rows = r;
+    return BG_OK;
+}
+
+int bg_monitor_clear(bg_net *n, int32_t mid) {
+    if (!n || mid < 0 || mid >= (int32_t)n->mon_kind.size()) return fail(BG_EINVAL, "monitor id");
+    if (n->mon_kind[mid] == 0) {
+        HSpikeMon &m = n->smons[n->mon_idx[mid]]; m.steps.clear(); m.idx.clear();
+    } else {
+        HStateMon &m = n->stmons[n->mon_idx[mid]];
+        if (n->prepared) return fail(BG_ENOSYS, "clearing a state monitor after prepare is not supported; create a new network");
+        m.steps.clear(); m.vals.clear();
+    }
+    return BG_OK;
+}
+
+int bg_net_prepare(bg_net *n) {
+    if (!n) return fail(BG_EINVAL, "net");
+    if (n->prepared) return BG_OK;
+    BG_CUDA(cudaSetDevice(n->device));
+    const size_t ts = tsize(n);
+    // spike-history depth per group (neurongroup.py:459-473)
+    for (auto &g : n->groups) g.depth = std::max(1, g.period);
+    for (auto &c : n->conns) { HGroup &g = n->groups[c.src]; g.depth = std::max(g.depth, (c.hetero ? 0 : c.delay) + 1); }
+    for (auto &s : n->stdps) {
+        const HConn &c = n->conns[s.cid];
+        n->groups[c.src].depth = std::max(n->groups[c.src].depth, s.pre_delay + 1);
+        n->groups[c.tgt].depth = std::max(n->groups[c.tgt].depth, s.post_delay + 1);
+    }
+    for (auto &m : n->smons) { HGroup &g = n->groups[m.gid]; g.depth = std::max(g.depth, m.delay + 1); }
+    // chunk length bounded by monitor buffer sizes
+    int64_t chunk = kChunkSteps;
+    for (auto &m : n->smons) chunk = std::min<int64_t>(chunk, std::max<int64_t>(kGraphSteps, (int64_t)(1 << 25) / std::max<int64_t>(1, m.n)));
+    for (auto &m : n->stmons) chunk = std::min<int64_t>(chunk, std::max<int64_t>(kGraphSteps, (int64_t)(1 << 26) / std::max<int64_t>(1, (int64_t)m.idx.size())));
+    chunk = std::max<int64_t>(kGraphSteps, chunk / kGraphSteps * kGraphSteps);
+    n->chunk_steps = chunk;
+    // ---- device allocations
+    for (auto &g : n->groups) {
+        if (n->alloc(&g.dS, (size_t)std::max(1, g.nvar) * g.npad * ts) != cudaSuccess) return fail(BG_ENOMEM, "group state");
+        BG_CUDA(cudaMemsetAsync(g.dS, 0, (size_t)std::max(1, g.nvar) * g.npad * ts, n->stream));
+        for (int v = 0; v < g.nvar; ++v) { int st = upload_state(n, g, v, g.S0.data() + (size_t)v * g.n); if (st) return st; }
+        if (n->alloc(&g.dHist, (size_t)g.depth * (g.npad / 32) * 4) != cudaSuccess) return fail(BG_ENOMEM, "spike history");
+        if (g.refr && n->alloc(&g.dNext, g.npad * 8) != cudaSuccess) return fail(BG_ENOMEM, "refractory");
+        if (g.period > 0 && n->alloc(&g.dLast, g.npad * 4) != cudaSuccess) return fail(BG_ENOMEM, "refractory");
+        if (!g.gen_steps.empty()) {
+            if (n->alloc(&g.dGenSteps, g.gen_steps.size() * 8) != cudaSuccess || n->alloc(&g.dGenIdx, g.gen_idx.size() * 4) != cudaSuccess)
+                return fail(BG_ENOMEM, "generator");
+            int st = upload(n, g.dGenSteps, g.gen_steps.data(), g.gen_steps.size() * 8); if (st) return st;
+            st = upload(n, g.dGenIdx, g.gen_idx.data(), g.gen_idx.size() * 4); if (st) return st;
+        }
+    }
+    for (size_t ci = 0; ci < n->conns.size(); ++ci) {
+        HConn &c = n->conns[ci];
+        if (n->alloc(&c.dW, c.w.size()) != cudaSuccess) return fail(BG_ENOMEM, "weights");
+        int st = upload(n, c.dW, c.w.data(), c.w.size()); if (st) return st;
+        if (!c.dense) {
+            if (n->alloc(&c.dRow, (c.sn + 1) * 8) != cudaSuccess || n->alloc(&c.dCols, c.nnz * 4) != cudaSuccess)
+                return fail(BG_ENOMEM, "CSR");
+            st = upload(n, c.dRow, c.rowptr.data(), (c.sn + 1) * 8); if (st) return st;
+            st = upload(n, c.dCols, c.cols.data(), c.nnz * 4); if (st) return st;
+        }
+        if (c.hetero) {
+            if (n->alloc(&c.dD, c.nnz) != cudaSuccess) return fail(BG_ENOMEM, "delays");
+            st = upload(n, c.dD, c.d.data(), c.nnz); if (st) return st;
+            if (n->alloc(&c.dRing, (size_t)c.md * c.tn * ts) != cudaSuccess) return fail(BG_ENOMEM, "delay ring");
+            n->groups[c.tgt].delivs.push_back((int)ci);
+        }
+        if (c.stdp >= 0 && !c.dense) {
+            // column access (connectionmatrix.py:317-333): ascending source per target column
+            std::vector<int64_t> colptr(c.tn + 1, 0), colk(c.nnz); std::vector<int32_t> colsrc(c.nnz);
+            for (int32_t j : c.cols) colptr[j + 1]++;
+            for (int64_t j = 0; j < c.tn; ++j) colptr[j + 1] += colptr[j];
+            std::vector<int64_t> fill(colptr.begin(), colptr.end() - 1);
+            for (int64_t i = 0; i < c.sn; ++i)
+                for (int64_t k = c.rowptr[i]; k < c.rowptr[i + 1]; ++k) { int64_t p = fill[c.cols[k]]++; colk[p] = k; colsrc[p] = (int32_t)i; }
+            if (n->alloc(&c.dColptr, (c.tn + 1) * 8) != cudaSuccess || n->alloc(&c.dColk, c.nnz * 8) != cudaSuccess ||
+                n->alloc(&c.dColsrc, c.nnz * 4) != cudaSuccess) return fail(BG_ENOMEM, "column index");
+            st = upload(n, c.dColptr, colptr.data(), (c.tn + 1) * 8); if (st) return st;
+            st = upload(n, c.dColk, colk.data(), c.nnz * 8); if (st) return st;
+            st = upload(n, c.dColsrc, colsrc.data(), c.nnz * 4); if (st) return st;
+            BG_CUDA(cudaStreamSynchronize(n->stream));
+        }
+    }
+    for (auto &s : n->stdps) {
+        const HConn &c = n->conns[s.cid];
+        if (n->alloc(&s.dApre, std::max<int64_t>(1, c.sn) * 8) != cudaSuccess || n->alloc(&s.dApost, std::max<int64_t>(1, c.tn) * 8) != cudaSuccess)
+            return fail(BG_ENOMEM, "STDP traces");
+        // the presynaptic update rides on the propagation kernel when it reads
+        // the same spikes and the items are adjacent (connection, then updater)
+        s.fused = (s.pre_delay == c.delay);
+        if (s.fused) {
+            for (size_t k = 0; k + 1 < n->items.size(); ++k)
+                if (n->items[k + 1].kind == IT_STDP_PRE && n->items[k + 1].id == (int)(&s - &n->stdps[0])) {
+                    s.fused = n->items[k].kind == IT_CONN && n->items[k].id == s.cid;
+                    break;
+                }
+        }
+    }
+    for (auto &m : n->smons) {
+        m.cap = std::max<int64_t>(1024, m.n * (n->chunk_steps + 1));
+        if (n->alloc(&m.dCnt, 8) != cudaSuccess || n->alloc(&m.dBase, 8) != cudaSuccess ||
+            n->alloc(&m.dIdx, m.cap * 4) != cudaSuccess || n->alloc(&m.dSteps, m.cap * 4) != cudaSuccess)
+            return fail(BG_ENOMEM, "spike monitor");
+        BG_CUDA(cudaMemsetAsync(m.dCnt, 0, 8, n->stream));
+        BG_CUDA(cudaMemsetAsync(m.dBase, 0, 8, n->stream));
+    }
+    for (size_t k = 0; k < n->stmons.size(); ++k) {
+        HStateMon &m = n->stmons[k];
+        HGroup &g = n->groups[m.gid];
+        const int64_t w = (int64_t)m.idx.size();
+        std::vector<int32_t> order(w);
+        for (int64_t e = 0; e < w; ++e) order[e] = (int32_t)e;
+        std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return m.idx[a] < m.idx[b]; });
+        m.sorted.resize(w); m.pos.resize(w);
+        for (int64_t e = 0; e < w; ++e) { m.sorted[e] = m.idx[order[e]]; m.pos[e] = order[e]; }
+        const int64_t nb = g.npad / bg::kHeadThreads;
+        m.blk_lo.assign(nb + 1, 0);
+        for (int64_t b = 0, e = 0; b <= nb; ++b) {
+            while (e < w && m.sorted[e] < b * bg::kHeadThreads) ++e;
+            m.blk_lo[b] = (int32_t)e;
+        }
+        m.cap_rows = n->chunk_steps / m.timestep + 2;
+        m.start = n->nstep;
+        if (n->alloc(&m.dIdx, std::max<int64_t>(1, w) * 4) != cudaSuccess || n->alloc(&m.dPos, std::max<int64_t>(1, w) * 4) != cudaSuccess ||
+            n->alloc(&m.dBlk, (nb + 1) * 4) != cudaSuccess || n->alloc(&m.dBuf, std::max<int64_t>(1, w) * m.cap_rows * ts) != cudaSuccess ||
+            n->alloc(&m.dRowBase, 8) != cudaSuccess)
+            return fail(BG_ENOMEM, "state monitor");
+        int st;
+        if (w) { st = upload(n, m.dIdx, m.sorted.data(), w * 4); if (st) return st; st = upload(n, m.dPos, m.pos.data(), w * 4); if (st) return st; }
+        st = upload(n, m.dBlk, m.blk_lo.data(), (nb + 1) * 4); if (st) return st;
+        BG_CUDA(cudaMemsetAsync(m.dRowBase, 0, 8, n->stream));
+        g.recs.push_back((int)k);
+    }
+    BG_CUDA(cudaStreamSynchronize(n->stream));
+    int st = reset_dynamic(n);
+    if (st) return st;
+    // ---- per-step launch list: groups, trace decay, connections slot
+    for (size_t gi = 0; gi < n->groups.size(); ++gi) {
+        st = n->precision == 64 ? build_group<double>(n, (int)gi) : build_group<float>(n, (int)gi);
+        if (st) return st;
+    }
+    for (size_t si = 0; si < n->stdps.size(); ++si) { st = build_decay(n, (int)si); if (st) return st; }
+    for (const Item &it : n->items) {
+        switch (it.kind) {
+        case IT_CONN: st = n->precision == 64 ? build_conn<double>(n, it.id) : build_conn<float>(n, it.id); break;
+        case IT_SPIKEMON: st = build_spikemon(n, it.id); break;
+        case IT_STDP_PRE:
+            if (n->precision != 64) return fail(BG_ENOSYS, "STDP runs on the FP64 network path");
+            st = build_stdp_pre(n, it.id); break;
+        case IT_STDP_POST: st = build_stdp_post(n, it.id); break;
+        }
+        if (st) return st;
+    }
+    if (n->step_launches.empty()) return fail(BG_EINVAL, "empty network");
+    BG_CUDA(cudaStreamSynchronize(n->stream));
+    n->prepared = true;
+    return BG_OK;
+}
+
+static int launch_step(bg_net *n, int tail) {
+    const size_t k = n->step_launches.size();
+    for (size_t i = 0; i < k; ++i) {
+        cudaError_t e = n->step_launches[i](n->stream, tail, i + 1 == k);
+        if (e != cudaSuccess) return fail(BG_ECUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    }
+    n->launches += (int64_t)k;
+    return BG_OK;
+}
+
+static int ensure_graph(bg_net *n) {
+    if (n->gexec) return BG_OK;
+    cudaGraph_t graph;
+    BG_CUDA(cudaStreamBeginCapture(n->stream, cudaStreamCaptureModeThreadLocal));
+    int st = BG_OK;
+    for (int s = 0; s < kGraphSteps && st == BG_OK; ++s) st = launch_step(n, 1);
+    cudaError_t e = cudaStreamEndCapture(n->stream, &graph);
+    n->launches -= (int64_t)kGraphSteps * (int64_t)n->step_launches.size();
+    if (st) return st;
+    if (e != cudaSuccess) return fail(BG_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&n->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(BG_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    return BG_OK;
+}
+
+int bg_net_run(bg_net *n, int64_t nsteps, int64_t cs0) {
+    if (!n || nsteps < 0) return fail(BG_EINVAL, "bg_net_run");
+    if (!n->prepared) { int st = bg_net_prepare(n); if (st) return st; }
+    if (nsteps == 0) return BG_OK;
+    BG_CUDA(cudaSetDevice(n->device));
+    int st = ensure_graph(n);
+    if (st) return st;
+    long long off = cs0 - n->nstep;
+    BG_CUDA(cudaMemcpyAsync(&n->dCtl->clock_off, &off, 8, cudaMemcpyHostToDevice, n->stream));
+    BG_CUDA(cudaStreamSynchronize(n->stream));
+    BG_CUDA(cudaEventRecord(n->ev0, n->stream));
+    float total_ms = 0;
+    int64_t done = 0;
+    while (done < nsteps) {
+        const int64_t c = std::min<int64_t>(n->chunk_steps, nsteps - done);
+        const long long chunk_cs = cs0 + done;
+        for (auto &m : n->smons) BG_CUDA(cudaMemcpyAsync(m.dBase, &chunk_cs, 8, cudaMemcpyHostToDevice, n->stream));
+        BG_CUDA(cudaStreamSynchronize(n->stream));
+        int64_t k = 0;
+        if (done == 0) { st = launch_step(n, 0); if (st) return st; k = 1; }
+        while (c - k >= kGraphSteps) {
+            BG_CUDA(cudaGraphLaunch(n->gexec, n->stream));
+            n->launches += (int64_t)kGraphSteps * (int64_t)n->step_launches.size();
+            k += kGraphSteps;
+        }
+        for (; k < c; ++k) { st = launch_step(n, 1); if (st) return st; }
+        done += c;
+        n->nstep += c;
+        const bool last_chunk = done == nsteps;
+        if (last_chunk) {
+            for (auto &f : n->finalize_launches) {
+                cudaError_t e = f(n->stream, 1, 0);
+                if (e != cudaSuccess) return fail(BG_ECUDA, cudaGetErrorString(e));
+                n->launches++;
+            }
+        }
+        BG_CUDA(cudaEventRecord(n->ev1, n->stream));
+        BG_CUDA(cudaEventSynchronize(n->ev1));
+        float ms = 0;
+        BG_CUDA(cudaEventElapsedTime(&ms, n->ev0, n->ev1));
+        total_ms += ms;
+        st = check_device_error(n);
+        if (st) return st;
+        // 'end' slot has run for steps < nstep-1, and for nstep-1 after finalize
+        st = drain(n, chunk_cs, last_chunk ? n->nstep - 1 : n->nstep - 2, off);
+        if (st) return st;
+        BG_CUDA(cudaEventRecord(n->ev0, n->stream));
+    }
+    n->last_ms = total_ms;
+    return BG_OK;
+}
+
+int bg_group_get_state(bg_net *n, int32_t gid, int var, double *out) {
+    if (!gid_ok(n, gid) || var < 0 || var >= n->groups[gid].nvar || !out) return fail(BG_EINVAL, "bg_group_get_state");
+    HGroup &g = n->groups[gid];
+    if (!n->prepared) { std::memcpy(out, g.S0.data() + (size_t)var * g.n, g.n * 8); return BG_OK; }
+    BG_CUDA(cudaStreamSynchronize(n->stream));
+    if (n->precision == 64) BG_CUDA(cudaMemcpy(out, (double *)g.dS + (size_t)var * g.npad, g.n * 8, cudaMemcpyDeviceToHost));
+    else {
+        std::vector<float> tmp(g.n);
+        BG_CUDA(cudaMemcpy(tmp.data(), (float *)g.dS + (size_t)var * g.npad, g.n * 4, cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < g.n; ++i) out[i] = tmp[i];
+    }
+    return BG_OK;
+}
+
+int bg_group_set_state(bg_net *n, int32_t gid, int var, const double *in) {
+    if (!gid_ok(n, gid) || var < 0 || var >= n->groups[gid].nvar || !in) return fail(BG_EINVAL, "bg_group_set_state");
+    HGroup &g = n->groups[gid];
+    if (!n->prepared) { std::memcpy(g.S0.data() + (size_t)var * g.n, in, g.n * 8); return BG_OK; }
+    BG_CUDA(cudaStreamSynchronize(n->stream));
+    int st = upload_state(n, g, var, in);
+    if (st) return st;
+    BG_CUDA(cudaStreamSynchronize(n->stream));
+    return BG_OK;
+}
+
+int bg_net_reinit(bg_net *n) {
+    if (!n) return fail(BG_EINVAL, "net");
+    if (!n->prepared) return BG_OK;
+    BG_CUDA(cudaStreamSynchronize(n->stream));
+    int st = reset_dynamic(n);
+    if (st) return st;
+    BG_CUDA(cudaStreamSynchronize(n->stream));
+    return BG_OK;
+}
+
+int bg_net_stats(bg_net *n, int64_t *steps, int64_t *launches, double *ms) {
+    if (!n) return fail(BG_EINVAL, "net");
+    if (steps) *steps = n->nstep;
+    if (launches) *launches = n->launches;
+    if (ms) *ms = n->last_ms;
+    return BG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,198 @@
+/*
+ * brian_b200.h -- C ABI of the B200 clock-driven spiking-network engine.
+ *
+ * The engine replaces Brian 1.4.4's clock-driven simulation loop
+ * (NeuronGroup.update / Connection.propagate / DelayConnection /
+ * ExponentialSTDP / SpikeMonitor / StateMonitor / Network.run) and the GPU
+ * model-fitting kernel (GPUModelFitting).  Every entry point is plain C:
+ * pointers, sizes, and an int status.  Nothing here throws; a negative
+ * status carries an error class and bg_last_error() returns the message
+ * of the calling thread's last failure.
+ *
+ * Ownership: handles (bg_net, bg_fit) own every device buffer they
+ * allocate and free them in bg_*_destroy.  Host arrays passed in are
+ * copied before the call returns.  One handle = one CUDA stream; calls on
+ * different handles may come from different threads, calls on one handle
+ * must be serialised by the caller.
+ *
+ * Units: all values are SI floats (volt, second, ...), the same numbers
+ * Brian holds in its state matrix when units are stripped.
+ */
+#ifndef BRIAN_B200_H
+#define BRIAN_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define BG_API __attribute__((visibility("default")))
+#else
+#define BG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define BG_OK        0
+#define BG_EINVAL   (-1)   /* bad argument (size, index, kind)              */
+#define BG_ENOMEM   (-2)   /* device or host allocation failed              */
+#define BG_ECUDA    (-3)   /* a CUDA runtime/driver call failed             */
+#define BG_ETIMEOUT (-4)   /* a bounded device-side wait gave up            */
+#define BG_ENUMERIC (-5)   /* non-finite value detected                     */
+#define BG_ESTATE   (-6)   /* call not valid in the handle's current state  */
+#define BG_ENOSYS   (-7)   /* feature combination not implemented           */
+#define BG_ECOMPILE (-8)   /* runtime compilation of generated code failed  */
+
+/* threshold kinds: Threshold (threshold.py:129-200), VariableThreshold
+ * (threshold.py:337-406), PoissonThreshold (threshold.py:461-471),
+ * SpikeGeneratorGroup (directcontrol.py:63-217). */
+#define BG_THR_NONE      0
+#define BG_THR_CONST     1   /* S[var] >  value                                */
+#define BG_THR_VAR       2   /* S[var] >  S[var2]                              */
+#define BG_THR_POISSON   3   /* u(seed,step,i) < S[var]*dt  (Philox4x32-10)    */
+#define BG_THR_GENERATOR 4   /* explicit (step, index) list                    */
+
+/* reset kinds: Reset (reset.py:115-152), VariableReset (reset.py:220-257) */
+#define BG_RESET_NONE  0
+#define BG_RESET_CONST 1     /* S[var] = value                                 */
+#define BG_RESET_VAR   2     /* S[var] = S[var2]                               */
+
+/* STDP interaction kinds (stdp.py:495-509) */
+#define BG_STDP_ALL          0
+#define BG_STDP_NEAREST      1
+#define BG_STDP_NEAREST_PRE  2
+#define BG_STDP_NEAREST_POST 3
+
+typedef struct bg_net bg_net;
+typedef struct bg_fit bg_fit;
+
+/* ---- library ----------------------------------------------------------- */
+BG_API int bg_version(void);
+/* Copies the calling thread's last error message (NUL-terminated). */
+BG_API int bg_last_error(char *buf, int64_t len);
+
+/* ---- network handle ------------------------------------------------------
+ * Replaces Network (network.py:62-679): groups, connections and monitors are
+ * registered, bg_net_prepare freezes the schedule, bg_net_run advances it.
+ * precision: 64 (bit-exact FP64 path) or 32 (FP32 state/accumulation).
+ * deterministic: 1 = accumulation order of the reference for every
+ * connection; 0 = atomics allowed where the result may then differ in the
+ * last bit (FP32 studies).  Connections with one shared weight use atomics
+ * in both modes, which is exact because every addend is identical. */
+BG_API int bg_net_create(int device, int precision, int deterministic, double dt,
+                  bg_net **out);
+BG_API int bg_net_destroy(bg_net *net);
+
+/* ---- neuron groups --------------------------------------------------------
+ * NeuronGroup.__init__ (neurongroup.py:258-456): state matrix _S of shape
+ * (nvar, n), row-major, rows in the model's variable order. */
+BG_API int bg_group_add(bg_net *net, int64_t n, int nvar, const double *S0,
+                 int32_t *gid);
+/* LinearStateUpdater (stateupdater.py:328-417): S <- A.S (+ C when C is not
+ * NULL).  A is nvar x nvar row-major; the sum runs left to right over the
+ * columns without fused multiply-add. */
+BG_API int bg_group_set_linear(bg_net *net, int32_t gid, const double *A,
+                        const double *C);
+/* Threshold / VariableThreshold (threshold.py:160-191, 373-396). */
+BG_API int bg_group_set_threshold(bg_net *net, int32_t gid, int kind, int var,
+                           double value, int var2);
+/* PoissonGroup (directcontrol.py:406-447) + PoissonThreshold
+ * (threshold.py:461-471): spike when u < S[rate_var]*dt, u from a
+ * counter-based Philox4x32-10 stream keyed by (seed, clock step, index). */
+BG_API int bg_group_set_poisson(bg_net *net, int32_t gid, int rate_var,
+                         uint64_t seed);
+/* SpikeGeneratorGroup (directcontrol.py:63-217): spikes given as clock
+ * steps, sorted by (step, index). */
+BG_API int bg_group_set_generator(bg_net *net, int32_t gid, int64_t nspikes,
+                           const int64_t *steps, const int32_t *idx);
+/* Reset / VariableReset (reset.py:139-147, 241-254), applied in the
+ * 'resets' slot to the neurons that spiked in this step. */
+BG_API int bg_group_set_reset(bg_net *net, int32_t gid, int kind, int var,
+                       double value, int var2);
+/* Refractoriness (neurongroup.py:506-515, reset.py:311-332).
+ * refractory_time = T - dt/2 (next allowed spike time offset; <= 0 turns
+ * the spike filter off, as for T < 0.9*dt);
+ * period = int(T/dt)+1 bins during which S[var] is clamped to value
+ * (period 0: no clamp, only the spike filter). */
+BG_API int bg_group_set_refractory(bg_net *net, int32_t gid, double refractory_time,
+                            int32_t period, int var, double value);
+
+/* ---- connections ----------------------------------------------------------
+ * Connection (connection.py:224-296) with SparseConnectionMatrix rows
+ * (connectionmatrix.py:196-387) and, when delays != NULL, DelayConnection
+ * (delayconnection.py:132-206): emission-time scatter into a ring of
+ * ring_depth rows, delivered in the 'after_connections' slot.
+ * rowptr has src_n+1 entries; cols are target indices (relative to
+ * tgt_origin), ascending within a row; w has w_bits 32 or 64.
+ * delay_steps is the homogeneous presynaptic delay of a plain Connection
+ * (spikes read from the source history delay_steps bins back).
+ * mod_var >= 0 multiplies each weight by the source's S[mod_var][i]. */
+BG_API int bg_conn_add(bg_net *net, int32_t src_gid, int64_t src_origin,
+                int64_t src_n, int32_t tgt_gid, int64_t tgt_origin,
+                int64_t tgt_n, int tgt_var, int64_t nnz,
+                const int64_t *rowptr, const int32_t *cols, const void *w,
+                int w_bits, int32_t delay_steps, const uint8_t *delays,
+                int32_t ring_depth, int mod_var, int32_t *cid);
+/* DenseConnectionMatrix (connectionmatrix.py:141-193): W[src_n][tgt_n]. */
+BG_API int bg_conn_add_dense(bg_net *net, int32_t src_gid, int64_t src_origin,
+                      int64_t src_n, int32_t tgt_gid, int64_t tgt_origin,
+                      int64_t tgt_n, int tgt_var, const void *W, int w_bits,
+                      int32_t delay_steps, int mod_var, int32_t *cid);
+/* Weights in the connection's own order (CSR data order, or row-major for
+ * dense), widened to double. */
+BG_API int bg_conn_get_weights(bg_net *net, int32_t cid, double *out);
+BG_API int bg_conn_set_weights(bg_net *net, int32_t cid, const double *in);
+
+/* ExponentialSTDP / STDP (stdp.py:181-539) on a non-delayed connection.
+ * decay = {a_pre, c_pre, a_post, c_post}: the 1x1 linear updaters of the
+ * separated trace groups (A <- a*A + c).  Pre spike i: A_pre[i] (+)= Ap;
+ * w[i,:] += A_post; clip.  Post spike j: A_post[j] (+)= Am; w[:,j] +=
+ * A_pre; clip.  pre_delay/post_delay in bins.  Two items are appended to
+ * the connections slot: the presynaptic then the postsynaptic updater. */
+BG_API int bg_stdp_add(bg_net *net, int32_t cid, const double *decay, double Ap,
+                double Am, double wmin, double wmax, int interactions,
+                int32_t pre_delay, int32_t post_delay, int32_t *sid);
+BG_API int bg_stdp_get_traces(bg_net *net, int32_t sid, double *a_pre,
+                       double *a_post);
+
+/* ---- monitors ------------------------------------------------------------
+ * SpikeMonitor (monitor.py:84-218): appends (clock step, index - origin) in
+ * the connections slot; StateMonitor (monitor.py:683-989): records S[var] at
+ * idx every `timestep` steps after the resets (when='end'). */
+BG_API int bg_spikemon_add(bg_net *net, int32_t gid, int64_t origin, int64_t n,
+                    int32_t delay, int32_t *mid);
+BG_API int bg_statemon_add(bg_net *net, int32_t gid, int var, int64_t nidx,
+                    const int32_t *idx, int32_t timestep, int32_t *mid);
+/* Number of spikes recorded so far. */
+BG_API int bg_spikemon_count(bg_net *net, int32_t mid, int64_t *n);
+/* Copies up to cap recorded spikes; *n receives the number copied. */
+BG_API int bg_spikemon_read(bg_net *net, int32_t mid, int64_t *steps, int32_t *idx,
+                     int64_t cap, int64_t *n);
+BG_API int bg_statemon_count(bg_net *net, int32_t mid, int64_t *nrows);
+/* values: row-major [row][nidx]; steps: clock step of each row. */
+BG_API int bg_statemon_read(bg_net *net, int32_t mid, double *values,
+                     int64_t *steps, int64_t cap_rows, int64_t *nrows);
+/* Clears a monitor's records (SpikeMonitor.reinit / StateMonitor.reinit). */
+BG_API int bg_monitor_clear(bg_net *net, int32_t mid);
+
+/* ---- schedule -------------------------------------------------------------
+ * Network.prepare + Network.run (network.py:313-363, 541-586): each step is
+ * groups -> connections slot (items in registration order) ->
+ * after_connections (ring delivery) -> resets -> end (state monitors). */
+BG_API int bg_net_prepare(bg_net *net);
+BG_API int bg_net_run(bg_net *net, int64_t nsteps, int64_t clock_step0);
+BG_API int bg_group_get_state(bg_net *net, int32_t gid, int var, double *out);
+BG_API int bg_group_set_state(bg_net *net, int32_t gid, int var, const double *in);
+/* Clears spike history, rings, refractory state and trace variables
+ * (NeuronGroup.reinit / Connection.reinit); states are set by the caller. */
+BG_API int bg_net_reinit(bg_net *net);
+/* steps run, kernel launches issued, device milliseconds of the last run. */
+BG_API int bg_net_stats(bg_net *net, int64_t *steps, int64_t *launches,
+                 double *last_run_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BRIAN_B200_H */

@@ -1,0 +1,568 @@
+/*
+ * oracle.cpp -- CPU restatement of Brian 1.4.4's clock-driven loop.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA engine
+ * in brian_b200/csrc: tests, __graft_entry__.smoke() and bench.py's CPU
+ * baseline leg load it; the product never does.
+ *
+ * It exports the same C ABI as include/brian_b200.h with the prefix
+ * `or_` instead of `bg_`, so one network description can be replayed into
+ * both.  Single-threaded, compiled with -O2 -ffp-contract=off: every
+ * floating-point operation is one IEEE rounding in the order written.
+ *
+ * Semantics followed (file:line in the Brian 1.4.4 tree):
+ *   step loop / schedule ......... network.py:365-380, 516-586; clock.py:162-212
+ *   linear update S <- A.S + C ... stateupdater.py:404-417 (sum fixed left to
+ *                                   right over columns, no FMA)
+ *   threshold ..................... threshold.py:160-191 (v > Vt, ascending)
+ *   variable threshold ............ threshold.py:373-396
+ *   Poisson threshold ............. threshold.py:461-471 (u < rate*dt)
+ *   spike generator ............... directcontrol.py:231-268
+ *   refractory filter ............. neurongroup.py:495-516
+ *   spike history ring ............ utils/circular.py:171-250
+ *   reset / variable reset ........ reset.py:139-147, 241-254
+ *   Refractoriness clamp .......... reset.py:311-332 (LS[0:period])
+ *   sparse propagation ............ connection.py:224-256
+ *   dense propagation ............. connection.py:256-262
+ *   delayed propagation ........... delayconnection.py:132-206 (ring row
+ *                                   (cur + d) % md), delivery :112-121
+ *   STDP pre/post updaters ........ stdp.py:31-54, 370-414, 452-539
+ *   SpikeMonitor .................. monitor.py:156-166
+ *   StateMonitor .................. monitor.py:824-842
+ */
+#include <cstdint>
+#include <cstring>
+#include <cmath>
+#include <string>
+#include <vector>
+#include <deque>
+#include <algorithm>
+
+#define OR_OK 0
+#define OR_EINVAL (-1)
+#define OR_ESTATE (-6)
+#define OR_ENOSYS (-7)
+
+static thread_local std::string g_err;
+static int fail(int code, const std::string &m) { g_err = m; return code; }
+
+/* ---------------- Philox4x32-10 (Salmon et al., SC'11) ------------------ */
+static inline void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+    for (int r = 0; r < 10; ++r) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
+        uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ c[1] ^ k0, n1 = lo1, n2 = hi0 ^ c[3] ^ k1, n3 = lo0;
+        c[0] = n0; c[1] = n1; c[2] = n2; c[3] = n3;
+        k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+    }
+}
+/* uniform double in [0,1) with 53 random bits, keyed by (seed, step, i) */
+static inline double philox_uniform(uint64_t seed, int64_t step, int64_t i) {
+    uint32_t c[4] = {(uint32_t)step, (uint32_t)((uint64_t)step >> 32),
+                     (uint32_t)i, (uint32_t)((uint64_t)i >> 32)};
+    philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    uint64_t a = c[0] >> 5, b = c[1] >> 6;
+    return (double)(a * 67108864ull + b) * (1.0 / 9007199254740992.0);
+}
+
+/* ---------------- data ---------------------------------------------------- */
+struct Group {
+    int64_t n = 0; int nvar = 0;
+    std::vector<double> S;           /* [nvar][n] */
+    std::vector<double> S0;
+    bool linear = false, useC = false;
+    std::vector<double> A, C;
+    int thr_kind = 0, thr_var = 0, thr_var2 = 0; double thr_val = 0;
+    int rate_var = 0; uint64_t seed = 0;
+    std::vector<int64_t> gen_steps; std::vector<int32_t> gen_idx;
+    int reset_kind = 0, reset_var = 0, reset_var2 = 0; double reset_val = 0;
+    bool refr = false; double refr_time = 0; int32_t period = 0; int clamp_var = 0; double clamp_val = 0;
+    std::vector<double> next_allowed;
+    std::deque<std::vector<int32_t>> hist;   /* hist[0] = current step */
+    int32_t depth = 1;
+};
+struct Conn {
+    int32_t src, tgt; int64_t so, sn, to, tn; int var;
+    bool dense = false;
+    std::vector<int64_t> rowptr; std::vector<int32_t> cols;
+    int w_bits = 64; std::vector<double> w64; std::vector<float> w32;
+    int32_t delay = 0; bool hetero = false; std::vector<uint8_t> d;
+    int32_t md = 0, cur = 0; std::vector<double> ring;
+    int mod_var = -1;
+    /* column index (built at prepare when STDP needs it) */
+    std::vector<int64_t> colptr; std::vector<int64_t> colk; std::vector<int32_t> colsrc;
+    double getw(int64_t k) const { return w_bits == 64 ? w64[k] : (double)w32[k]; }
+};
+struct Stdp {
+    int32_t cid; double a_pre, c_pre, a_post, c_post, Ap, Am, wmin, wmax;
+    int inter; int32_t pre_delay, post_delay;
+    std::vector<double> A_pre, A_post;
+};
+struct SpikeMon { int32_t gid; int64_t origin, n; int32_t delay; std::vector<int64_t> steps; std::vector<int32_t> idx; };
+struct StateMon { int32_t gid; int var; std::vector<int32_t> idx; int32_t timestep; int64_t start;
+                  std::vector<double> vals; std::vector<int64_t> steps; };
+enum { IT_CONN = 0, IT_SPIKEMON = 1, IT_STDP_PRE = 2, IT_STDP_POST = 3 };
+struct Item { int kind; int32_t id; };
+
+struct or_net {
+    double dt; int precision;
+    std::vector<Group> groups; std::vector<Conn> conns; std::vector<Stdp> stdps;
+    std::vector<SpikeMon> smons; std::vector<StateMon> stmons; std::vector<Item> items;
+    std::vector<int32_t> mon_kind;   /* monitor id -> 0 spike, 1 state (index into vector in mon_idx) */
+    std::vector<int32_t> mon_idx;
+    bool prepared = false; int64_t nstep = 0;
+};
+
+extern "C" {
+
+int or_version(void) { return 1; }
+int or_last_error(char *buf, int64_t len) {
+    if (!buf || len <= 0) return OR_EINVAL;
+    std::strncpy(buf, g_err.c_str(), (size_t)len - 1); buf[len - 1] = 0; return OR_OK;
+}
+int or_net_create(int device, int precision, int deterministic, double dt, or_net **out) {
+    (void)device; (void)deterministic;
+    if (!out || !(dt > 0)) return fail(OR_EINVAL, "bad dt/out");
+    if (precision != 64) return fail(OR_ENOSYS, "oracle runs the FP64 path only");
+    or_net *n = new or_net(); n->dt = dt; n->precision = precision; *out = n; return OR_OK;
+}
+int or_net_destroy(or_net *n) { delete n; return OR_OK; }
+
+static bool gid_ok(or_net *n, int32_t g) { return n && g >= 0 && g < (int32_t)n->groups.size(); }
+
+int or_group_add(or_net *n, int64_t N, int nvar, const double *S0, int32_t *gid) {
+    if (!n || N < 0 || nvar < 0 || (N > 0 && nvar > 0 && !S0)) return fail(OR_EINVAL, "group_add");
+    if (n->prepared) return fail(OR_ESTATE, "network already prepared");
+    Group g; g.n = N; g.nvar = nvar;
+    g.S.assign(S0, S0 + (size_t)N * nvar); g.S0 = g.S;
+    n->groups.push_back(std::move(g)); *gid = (int32_t)n->groups.size() - 1; return OR_OK;
+}
+int or_group_set_linear(or_net *n, int32_t gid, const double *A, const double *C) {
+    if (!gid_ok(n, gid) || !A) return fail(OR_EINVAL, "set_linear");
+    Group &g = n->groups[gid]; int m = g.nvar;
+    g.linear = true; g.A.assign(A, A + m * m);
+    g.useC = C != nullptr; if (C) g.C.assign(C, C + m);
+    return OR_OK;
+}
+int or_group_set_threshold(or_net *n, int32_t gid, int kind, int var, double value, int var2) {
+    if (!gid_ok(n, gid)) return fail(OR_EINVAL, "set_threshold");
+    Group &g = n->groups[gid];
+    if ((kind == 1 || kind == 2) && (var < 0 || var >= g.nvar)) return fail(OR_EINVAL, "threshold var");
+    if (kind == 2 && (var2 < 0 || var2 >= g.nvar)) return fail(OR_EINVAL, "threshold var2");
+    g.thr_kind = kind; g.thr_var = var; g.thr_val = value; g.thr_var2 = var2; return OR_OK;
+}
+int or_group_set_poisson(or_net *n, int32_t gid, int rate_var, uint64_t seed) {
+    if (!gid_ok(n, gid)) return fail(OR_EINVAL, "set_poisson");
+    Group &g = n->groups[gid];
+    if (rate_var < 0 || rate_var >= g.nvar) return fail(OR_EINVAL, "rate var");
+    g.thr_kind = 3; g.rate_var = rate_var; g.seed = seed; return OR_OK;
+}
+int or_group_set_generator(or_net *n, int32_t gid, int64_t ns, const int64_t *steps, const int32_t *idx) {
+    if (!gid_ok(n, gid) || ns < 0) return fail(OR_EINVAL, "set_generator");
+    Group &g = n->groups[gid]; g.thr_kind = 4;
+    g.gen_steps.assign(steps, steps + ns); g.gen_idx.assign(idx, idx + ns);
+    for (int64_t k = 0; k < ns; ++k) {
+        if (idx[k] < 0 || idx[k] >= g.n) return fail(OR_EINVAL, "generator index");
+        if (k && (steps[k] < steps[k - 1] || (steps[k] == steps[k - 1] && idx[k] < idx[k - 1])))
+            return fail(OR_EINVAL, "generator spikes not sorted by (step, index)");
+    }
+    return OR_OK;
+}
+int or_group_set_reset(or_net *n, int32_t gid, int kind, int var, double value, int var2) {
+    if (!gid_ok(n, gid)) return fail(OR_EINVAL, "set_reset");
+    Group &g = n->groups[gid];
+    if (kind && (var < 0 || var >= g.nvar)) return fail(OR_EINVAL, "reset var");
+    if (kind == 2 && (var2 < 0 || var2 >= g.nvar)) return fail(OR_EINVAL, "reset var2");
+    g.reset_kind = kind; g.reset_var = var; g.reset_val = value; g.reset_var2 = var2; return OR_OK;
+}
+int or_group_set_refractory(or_net *n, int32_t gid, double rt, int32_t period, int var, double value) {
+    if (!gid_ok(n, gid) || period < 0) return fail(OR_EINVAL, "set_refractory");
+    Group &g = n->groups[gid];
+    if (period > 0 && (var < 0 || var >= g.nvar)) return fail(OR_EINVAL, "clamp var");
+    /* rt <= 0: no spike filter (refractory < 0.9*dt), clamp only */
+    g.refr = rt > 0; g.refr_time = rt; g.period = period; g.clamp_var = var; g.clamp_val = value; return OR_OK;
+}
+
+static int add_conn_common(or_net *n, int32_t src, int64_t so, int64_t sn, int32_t tgt, int64_t to,
+                           int64_t tn, int var, int32_t delay, int mod_var, Conn &c) {
+    if (!gid_ok(n, src) || !gid_ok(n, tgt)) return fail(OR_EINVAL, "conn groups");
+    if (n->prepared) return fail(OR_ESTATE, "network already prepared");
+    const Group &gs = n->groups[src], &gt = n->groups[tgt];
+    if (so < 0 || sn < 0 || so + sn > gs.n || to < 0 || tn < 0 || to + tn > gt.n) return fail(OR_EINVAL, "conn ranges");
+    if (var < 0 || var >= gt.nvar) return fail(OR_EINVAL, "conn target var");
+    if (delay < 0) return fail(OR_EINVAL, "conn delay");
+    if (mod_var >= gs.nvar) return fail(OR_EINVAL, "modulation var");
+    c.src = src; c.tgt = tgt; c.so = so; c.sn = sn; c.to = to; c.tn = tn; c.var = var;
+    c.delay = delay; c.mod_var = mod_var;
+    return OR_OK;
+}
+int or_conn_add(or_net *n, int32_t src, int64_t so, int64_t sn, int32_t tgt, int64_t to, int64_t tn,
+                int var, int64_t nnz, const int64_t *rowptr, const int32_t *cols, const void *w, int w_bits,
+                int32_t delay, const uint8_t *delays, int32_t ring_depth, int mod_var, int32_t *cid) {
+    Conn c; int st = add_conn_common(n, src, so, sn, tgt, to, tn, var, delay, mod_var, c);
+    if (st) return st;
+    if (w_bits != 32 && w_bits != 64) return fail(OR_EINVAL, "w_bits");
+    if (!rowptr || nnz < 0 || (nnz > 0 && (!cols || !w))) return fail(OR_EINVAL, "csr arrays");
+    if (rowptr[0] != 0 || rowptr[sn] != nnz) return fail(OR_EINVAL, "rowptr bounds");
+    c.rowptr.assign(rowptr, rowptr + sn + 1); c.cols.assign(cols, cols + nnz);
+    for (int64_t i = 0; i < sn; ++i) {
+        if (rowptr[i + 1] < rowptr[i]) return fail(OR_EINVAL, "rowptr not monotone");
+        for (int64_t k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+            if (cols[k] < 0 || cols[k] >= tn) return fail(OR_EINVAL, "column index out of range");
+            if (k > rowptr[i] && cols[k] <= cols[k - 1]) return fail(OR_EINVAL, "columns not strictly ascending in a row");
+        }
+    }
+    c.w_bits = w_bits;
+    if (w_bits == 64) c.w64.assign((const double *)w, (const double *)w + nnz);
+    else c.w32.assign((const float *)w, (const float *)w + nnz);
+    if (delays) {
+        if (ring_depth < 1 || ring_depth > 255) return fail(OR_EINVAL, "ring depth");
+        c.hetero = true; c.d.assign(delays, delays + nnz); c.md = ring_depth;
+        for (int64_t k = 0; k < nnz; ++k) if (delays[k] >= ring_depth) return fail(OR_EINVAL, "delay >= ring depth");
+        c.ring.assign((size_t)ring_depth * tn, 0.0);
+    }
+    n->conns.push_back(std::move(c)); *cid = (int32_t)n->conns.size() - 1;
+    n->items.push_back({IT_CONN, *cid});
+    return OR_OK;
+}
+int or_conn_add_dense(or_net *n, int32_t src, int64_t so, int64_t sn, int32_t tgt, int64_t to, int64_t tn,
+                      int var, const void *W, int w_bits, int32_t delay, int mod_var, int32_t *cid) {
+    Conn c; int st = add_conn_common(n, src, so, sn, tgt, to, tn, var, delay, mod_var, c);
+    if (st) return st;
+    if ((w_bits != 32 && w_bits != 64) || (!W && sn * tn > 0)) return fail(OR_EINVAL, "dense weights");
+    c.dense = true; c.w_bits = w_bits;
+    size_t nn = (size_t)sn * tn;
+    if (w_bits == 64) c.w64.assign((const double *)W, (const double *)W + nn);
+    else c.w32.assign((const float *)W, (const float *)W + nn);
+    n->conns.push_back(std::move(c)); *cid = (int32_t)n->conns.size() - 1;
+    n->items.push_back({IT_CONN, *cid});
+    return OR_OK;
+}
+static size_t conn_size(const Conn &c) { return c.w_bits == 64 ? c.w64.size() : c.w32.size(); }
+int or_conn_get_weights(or_net *n, int32_t cid, double *out) {
+    if (!n || cid < 0 || cid >= (int32_t)n->conns.size() || !out) return fail(OR_EINVAL, "get_weights");
+    const Conn &c = n->conns[cid];
+    for (size_t k = 0; k < conn_size(c); ++k) out[k] = c.getw((int64_t)k);
+    return OR_OK;
+}
+int or_conn_set_weights(or_net *n, int32_t cid, const double *in) {
+    if (!n || cid < 0 || cid >= (int32_t)n->conns.size() || !in) return fail(OR_EINVAL, "set_weights");
+    Conn &c = n->conns[cid];
+    for (size_t k = 0; k < conn_size(c); ++k) { if (c.w_bits == 64) c.w64[k] = in[k]; else c.w32[k] = (float)in[k]; }
+    return OR_OK;
+}
+int or_stdp_add(or_net *n, int32_t cid, const double *decay, double Ap, double Am, double wmin, double wmax,
+                int inter, int32_t pre_delay, int32_t post_delay, int32_t *sid) {
+    if (!n || cid < 0 || cid >= (int32_t)n->conns.size() || !decay) return fail(OR_EINVAL, "stdp_add");
+    if (n->prepared) return fail(OR_ESTATE, "network already prepared");
+    Conn &c = n->conns[cid];
+    if (c.hetero) return fail(OR_ENOSYS, "STDP on a DelayConnection is not supported");
+    if (pre_delay < 0 || post_delay < 0) return fail(OR_EINVAL, "stdp delays");
+    Stdp s; s.cid = cid; s.a_pre = decay[0]; s.c_pre = decay[1]; s.a_post = decay[2]; s.c_post = decay[3];
+    s.Ap = Ap; s.Am = Am; s.wmin = wmin; s.wmax = wmax; s.inter = inter;
+    s.pre_delay = pre_delay; s.post_delay = post_delay;
+    s.A_pre.assign(c.sn, 0.0); s.A_post.assign(c.tn, 0.0);
+    n->stdps.push_back(std::move(s)); *sid = (int32_t)n->stdps.size() - 1;
+    n->items.push_back({IT_STDP_PRE, *sid}); n->items.push_back({IT_STDP_POST, *sid});
+    return OR_OK;
+}
+int or_stdp_get_traces(or_net *n, int32_t sid, double *a_pre, double *a_post) {
+    if (!n || sid < 0 || sid >= (int32_t)n->stdps.size()) return fail(OR_EINVAL, "stdp id");
+    const Stdp &s = n->stdps[sid];
+    if (a_pre) std::copy(s.A_pre.begin(), s.A_pre.end(), a_pre);
+    if (a_post) std::copy(s.A_post.begin(), s.A_post.end(), a_post);
+    return OR_OK;
+}
+int or_spikemon_add(or_net *n, int32_t gid, int64_t origin, int64_t cnt, int32_t delay, int32_t *mid) {
+    if (!gid_ok(n, gid) || origin < 0 || cnt < 0 || origin + cnt > n->groups[gid].n || delay < 0)
+        return fail(OR_EINVAL, "spikemon_add");
+    if (n->prepared) return fail(OR_ESTATE, "network already prepared");
+    SpikeMon m; m.gid = gid; m.origin = origin; m.n = cnt; m.delay = delay;
+    n->smons.push_back(m);
+    n->items.push_back({IT_SPIKEMON, (int32_t)n->smons.size() - 1});
+    n->mon_kind.push_back(0); n->mon_idx.push_back((int32_t)n->smons.size() - 1);
+    *mid = (int32_t)n->mon_kind.size() - 1; return OR_OK;
+}
+int or_statemon_add(or_net *n, int32_t gid, int var, int64_t nidx, const int32_t *idx, int32_t timestep, int32_t *mid) {
+    if (!gid_ok(n, gid) || var < 0 || var >= n->groups[gid].nvar || timestep < 1 || nidx < 0)
+        return fail(OR_EINVAL, "statemon_add");
+    if (n->prepared) return fail(OR_ESTATE, "network already prepared");
+    StateMon m; m.gid = gid; m.var = var; m.timestep = timestep; m.start = 0;
+    if (idx) m.idx.assign(idx, idx + nidx);
+    else { m.idx.resize(n->groups[gid].n); for (int64_t i = 0; i < n->groups[gid].n; ++i) m.idx[i] = (int32_t)i; }
+    for (int32_t i : m.idx) if (i < 0 || i >= n->groups[gid].n) return fail(OR_EINVAL, "statemon index");
+    n->stmons.push_back(std::move(m));
+    n->mon_kind.push_back(1); n->mon_idx.push_back((int32_t)n->stmons.size() - 1);
+    *mid = (int32_t)n->mon_kind.size() - 1; return OR_OK;
+}
+static bool mon_ok(or_net *n, int32_t mid, int kind) {
+    return n && mid >= 0 && mid < (int32_t)n->mon_kind.size() && n->mon_kind[mid] == kind;
+}
+int or_spikemon_count(or_net *n, int32_t mid, int64_t *cnt) {
+    if (!mon_ok(n, mid, 0)) return fail(OR_EINVAL, "spikemon id");
+    *cnt = (int64_t)n->smons[n->mon_idx[mid]].idx.size(); return OR_OK;
+}
+int or_spikemon_read(or_net *n, int32_t mid, int64_t *steps, int32_t *idx, int64_t cap, int64_t *cnt) {
+    if (!mon_ok(n, mid, 0)) return fail(OR_EINVAL, "spikemon id");
+    const SpikeMon &m = n->smons[n->mon_idx[mid]];
+    int64_t k = std::min<int64_t>(cap, (int64_t)m.idx.size());
+    for (int64_t i = 0; i < k; ++i) { steps[i] = m.steps[i]; idx[i] = m.idx[i]; }
+    *cnt = k; return OR_OK;
+}
+int or_statemon_count(or_net *n, int32_t mid, int64_t *rows) {
+    if (!mon_ok(n, mid, 1)) return fail(OR_EINVAL, "statemon id");
+    *rows = (int64_t)n->stmons[n->mon_idx[mid]].steps.size(); return OR_OK;
+}
+int or_statemon_read(or_net *n, int32_t mid, double *vals, int64_t *steps, int64_t cap, int64_t *rows) {
+    if (!mon_ok(n, mid, 1)) return fail(OR_EINVAL, "statemon id");
+    const StateMon &m = n->stmons[n->mon_idx[mid]];
+    int64_t r = std::min<int64_t>(cap, (int64_t)m.steps.size()), w = (int64_t)m.idx.size();
+    for (int64_t i = 0; i < r; ++i) {
+        steps[i] = m.steps[i];
+        for (int64_t j = 0; j < w; ++j) vals[i * w + j] = m.vals[i * w + j];
+    }
+    *rows = r; return OR_OK;
+}
+int or_monitor_clear(or_net *n, int32_t mid) {
+    if (!n || mid < 0 || mid >= (int32_t)n->mon_kind.size()) return fail(OR_EINVAL, "monitor id");
+    if (n->mon_kind[mid] == 0) { SpikeMon &m = n->smons[n->mon_idx[mid]]; m.steps.clear(); m.idx.clear(); }
+    else { StateMon &m = n->stmons[n->mon_idx[mid]]; m.steps.clear(); m.vals.clear(); m.start = n->nstep; }
+    return OR_OK;
+}
+
+int or_net_prepare(or_net *n) {
+    if (!n) return fail(OR_EINVAL, "net");
+    if (n->prepared) return OR_OK;
+    /* history depth: max delay read from each group, + 1 for the current bin,
+     * and the refractory period (neurongroup.py:459-473). */
+    for (auto &g : n->groups) g.depth = std::max<int32_t>(1, g.period);
+    for (auto &c : n->conns) {
+        Group &g = n->groups[c.src]; g.depth = std::max(g.depth, c.delay + 1);
+    }
+    for (auto &s : n->stdps) {
+        Conn &c = n->conns[s.cid];
+        n->groups[c.src].depth = std::max(n->groups[c.src].depth, s.pre_delay + 1);
+        n->groups[c.tgt].depth = std::max(n->groups[c.tgt].depth, s.post_delay + 1);
+        if (!c.dense && c.colptr.empty()) {
+            /* column access order: ascending source within each target column
+             * (connectionmatrix.py:317-333 coldataindices) */
+            c.colptr.assign(c.tn + 1, 0);
+            for (int32_t j : c.cols) c.colptr[j + 1]++;
+            for (int64_t j = 0; j < c.tn; ++j) c.colptr[j + 1] += c.colptr[j];
+            std::vector<int64_t> fill(c.colptr.begin(), c.colptr.end() - 1);
+            c.colk.resize(c.cols.size()); c.colsrc.resize(c.cols.size());
+            for (int64_t i = 0; i < c.sn; ++i)
+                for (int64_t k = c.rowptr[i]; k < c.rowptr[i + 1]; ++k) {
+                    int64_t p = fill[c.cols[k]]++; c.colk[p] = k; c.colsrc[p] = (int32_t)i;
+                }
+        }
+    }
+    for (auto &m : n->smons) { Group &g = n->groups[m.gid]; g.depth = std::max(g.depth, m.delay + 1); }
+    for (auto &g : n->groups) {
+        g.hist.assign(g.depth, std::vector<int32_t>());
+        if (g.refr) g.next_allowed.assign(g.n, -1.0);
+    }
+    n->prepared = true; return OR_OK;
+}
+
+int or_net_reinit(or_net *n) {
+    if (!n) return fail(OR_EINVAL, "net");
+    for (auto &g : n->groups) { for (auto &h : g.hist) h.clear(); if (g.refr) std::fill(g.next_allowed.begin(), g.next_allowed.end(), -1.0); }
+    for (auto &c : n->conns) std::fill(c.ring.begin(), c.ring.end(), 0.0);
+    for (auto &s : n->stdps) { std::fill(s.A_pre.begin(), s.A_pre.end(), 0.0); std::fill(s.A_post.begin(), s.A_post.end(), 0.0); }
+    return OR_OK;
+}
+
+/* spikes of group g `delay` bins back, restricted to [origin, origin+cnt),
+ * returned relative to origin (utils/circular.py:232-238 get_spikes). */
+static void get_spikes(const Group &g, int32_t delay, int64_t origin, int64_t cnt, std::vector<int32_t> &out) {
+    out.clear();
+    for (int32_t i : g.hist[delay]) if (i >= origin && i < origin + cnt) out.push_back((int32_t)(i - origin));
+}
+
+static inline float clipf(float x, float lo, float hi) { return x < lo ? lo : (x > hi ? hi : x); }
+static inline double clipd(double x, double lo, double hi) { return x < lo ? lo : (x > hi ? hi : x); }
+
+static void step(or_net *n, int64_t cs) {
+    const double dt = n->dt;
+    const double t = (double)cs * dt;
+    std::vector<int32_t> spk;
+    /* ---- groups slot ---- */
+    for (auto &g : n->groups) {
+        const int64_t N = g.n; const int m = g.nvar;
+        if (g.linear) {
+            std::vector<double> x(m), s(m);
+            for (int64_t i = 0; i < N; ++i) {
+                for (int k = 0; k < m; ++k) s[k] = g.S[(size_t)k * N + i];
+                for (int j = 0; j < m; ++j) {
+                    double acc = g.A[j * m + 0] * s[0];
+                    for (int k = 1; k < m; ++k) acc = acc + g.A[j * m + k] * s[k];
+                    if (g.useC) acc = acc + g.C[j];
+                    x[j] = acc;
+                }
+                for (int k = 0; k < m; ++k) g.S[(size_t)k * N + i] = x[k];
+            }
+        }
+        std::vector<int32_t> spikes;
+        switch (g.thr_kind) {
+        case 1: { const double *v = &g.S[(size_t)g.thr_var * N];
+                  for (int64_t i = 0; i < N; ++i) if (v[i] > g.thr_val) spikes.push_back((int32_t)i); break; }
+        case 2: { const double *v = &g.S[(size_t)g.thr_var * N], *vt = &g.S[(size_t)g.thr_var2 * N];
+                  for (int64_t i = 0; i < N; ++i) if (v[i] > vt[i]) spikes.push_back((int32_t)i); break; }
+        case 3: { const double *r = &g.S[(size_t)g.rate_var * N];
+                  for (int64_t i = 0; i < N; ++i) if (philox_uniform(g.seed, cs, i) < r[i] * dt) spikes.push_back((int32_t)i); break; }
+        case 4: { auto lo = std::lower_bound(g.gen_steps.begin(), g.gen_steps.end(), cs);
+                  for (auto it = lo; it != g.gen_steps.end() && *it == cs; ++it) {
+                      int32_t i = g.gen_idx[it - g.gen_steps.begin()];
+                      if (spikes.empty() || spikes.back() != i) spikes.push_back(i);
+                  } break; }
+        default: break;
+        }
+        if (g.refr) {
+            std::vector<int32_t> kept;
+            for (int32_t i : spikes) if (g.next_allowed[i] <= t) kept.push_back(i);
+            for (int32_t i : kept) g.next_allowed[i] = t + g.refr_time;
+            spikes.swap(kept);
+        }
+        g.hist.pop_back(); g.hist.push_front(std::move(spikes));
+    }
+    for (auto &s : n->stdps) {   /* trace groups G_pre / G_post (stdp.py:282-293) */
+        for (auto &a : s.A_pre) a = s.a_pre * a + s.c_pre;
+        for (auto &a : s.A_post) a = s.a_post * a + s.c_post;
+    }
+    /* ---- connections slot ---- */
+    for (const Item &it : n->items) {
+        if (it.kind == IT_CONN) {
+            Conn &c = n->conns[it.id];
+            const Group &gs = n->groups[c.src]; Group &gt = n->groups[c.tgt];
+            get_spikes(gs, c.hetero ? 0 : c.delay, c.so, c.sn, spk);
+            double *sv = &gt.S[(size_t)c.var * gt.n + c.to];
+            const double *mod = c.mod_var >= 0 ? &gs.S[(size_t)c.mod_var * gs.n + c.so] : nullptr;
+            for (int32_t i : spk) {
+                if (c.dense) {
+                    for (int64_t j = 0; j < c.tn; ++j) {
+                        double w = c.getw((int64_t)i * c.tn + j);
+                        if (mod) w = w * mod[i];
+                        sv[j] = sv[j] + w;
+                    }
+                } else if (!c.hetero) {
+                    for (int64_t k = c.rowptr[i]; k < c.rowptr[i + 1]; ++k) {
+                        double w = c.getw(k); if (mod) w = w * mod[i];
+                        sv[c.cols[k]] = sv[c.cols[k]] + w;
+                    }
+                } else {
+                    for (int64_t k = c.rowptr[i]; k < c.rowptr[i + 1]; ++k) {
+                        double w = c.getw(k); if (mod) w = w * mod[i];
+                        size_t slot = (size_t)((c.cur + c.d[k]) % c.md);
+                        double &r = c.ring[slot * c.tn + c.cols[k]];
+                        r = r + w;
+                    }
+                }
+            }
+        } else if (it.kind == IT_SPIKEMON) {
+            SpikeMon &m = n->smons[it.id];
+            get_spikes(n->groups[m.gid], m.delay, m.origin, m.n, spk);
+            for (int32_t i : spk) { m.steps.push_back(cs); m.idx.push_back(i); }
+        } else if (it.kind == IT_STDP_PRE) {
+            Stdp &s = n->stdps[it.id]; Conn &c = n->conns[s.cid];
+            get_spikes(n->groups[c.src], s.pre_delay, c.so, c.sn, spk);
+            for (int32_t i : spk) {
+                if (s.inter == 0 || s.inter == 3) s.A_pre[i] = s.A_pre[i] + s.Ap; else s.A_pre[i] = s.Ap;
+                if (c.dense) {
+                    for (int64_t j = 0; j < c.tn; ++j) {
+                        size_t k = (size_t)i * c.tn + j;
+                        if (c.w_bits == 64) c.w64[k] = clipd(c.w64[k] + s.A_post[j], s.wmin, s.wmax);
+                        else c.w32[k] = clipf((float)((double)c.w32[k] + s.A_post[j]), (float)s.wmin, (float)s.wmax);
+                    }
+                } else {
+                    for (int64_t k = c.rowptr[i]; k < c.rowptr[i + 1]; ++k) {
+                        int32_t j = c.cols[k];
+                        if (c.w_bits == 64) c.w64[k] = clipd(c.w64[k] + s.A_post[j], s.wmin, s.wmax);
+                        else c.w32[k] = clipf((float)((double)c.w32[k] + s.A_post[j]), (float)s.wmin, (float)s.wmax);
+                    }
+                }
+            }
+        } else if (it.kind == IT_STDP_POST) {
+            Stdp &s = n->stdps[it.id]; Conn &c = n->conns[s.cid];
+            get_spikes(n->groups[c.tgt], s.post_delay, c.to, c.tn, spk);
+            for (int32_t j : spk) {
+                if (s.inter == 0) s.A_post[j] = s.A_post[j] + s.Am; else s.A_post[j] = s.Am;   /* 'nearest_pre' is A_post=+Am */
+                if (c.dense) {
+                    for (int64_t i = 0; i < c.sn; ++i) {
+                        size_t k = (size_t)i * c.tn + j;
+                        if (c.w_bits == 64) c.w64[k] = clipd(c.w64[k] + s.A_pre[i], s.wmin, s.wmax);
+                        else c.w32[k] = clipf((float)((double)c.w32[k] + s.A_pre[i]), (float)s.wmin, (float)s.wmax);
+                    }
+                } else {
+                    for (int64_t p = c.colptr[j]; p < c.colptr[j + 1]; ++p) {
+                        int64_t k = c.colk[p]; int32_t i = c.colsrc[p];
+                        if (c.w_bits == 64) c.w64[k] = clipd(c.w64[k] + s.A_pre[i], s.wmin, s.wmax);
+                        else c.w32[k] = clipf((float)((double)c.w32[k] + s.A_pre[i]), (float)s.wmin, (float)s.wmax);
+                    }
+                }
+            }
+        }
+    }
+    /* ---- after_connections: DelayConnection.delayed_propagate ---- */
+    for (auto &c : n->conns) {
+        if (!c.hetero) continue;
+        Group &gt = n->groups[c.tgt];
+        double *sv = &gt.S[(size_t)c.var * gt.n + c.to];
+        double *row = &c.ring[(size_t)c.cur * c.tn];
+        for (int64_t j = 0; j < c.tn; ++j) { sv[j] = sv[j] + row[j]; row[j] = 0.0; }
+        c.cur = (c.cur + 1) % c.md;
+    }
+    /* ---- resets ---- */
+    for (auto &g : n->groups) {
+        const int64_t N = g.n;
+        if (g.refr && g.period > 0) {
+            double *v = &g.S[(size_t)g.clamp_var * N];
+            for (int32_t b = 0; b < g.period && b < g.depth; ++b)
+                for (int32_t i : g.hist[b]) v[i] = g.clamp_val;
+        } else if (g.reset_kind == 1) {
+            double *v = &g.S[(size_t)g.reset_var * N];
+            for (int32_t i : g.hist[0]) v[i] = g.reset_val;
+        } else if (g.reset_kind == 2) {
+            double *v = &g.S[(size_t)g.reset_var * N]; const double *r = &g.S[(size_t)g.reset_var2 * N];
+            for (int32_t i : g.hist[0]) v[i] = r[i];
+        }
+    }
+    /* ---- end: state monitors ---- */
+    for (auto &m : n->stmons) {
+        if ((n->nstep - m.start) % m.timestep != 0) continue;
+        const Group &g = n->groups[m.gid];
+        const double *v = &g.S[(size_t)m.var * g.n];
+        for (int32_t i : m.idx) m.vals.push_back(v[i]);
+        m.steps.push_back(cs);
+    }
+    n->nstep++;
+}
+
+int or_net_run(or_net *n, int64_t nsteps, int64_t cs0) {
+    if (!n || nsteps < 0) return fail(OR_EINVAL, "run");
+    if (!n->prepared) { int st = or_net_prepare(n); if (st) return st; }
+    for (int64_t k = 0; k < nsteps; ++k) step(n, cs0 + k);
+    return OR_OK;
+}
+int or_group_get_state(or_net *n, int32_t gid, int var, double *out) {
+    if (!gid_ok(n, gid) || var < 0 || var >= n->groups[gid].nvar || !out) return fail(OR_EINVAL, "get_state");
+    const Group &g = n->groups[gid];
+    std::copy(g.S.begin() + (size_t)var * g.n, g.S.begin() + (size_t)(var + 1) * g.n, out); return OR_OK;
+}
+int or_group_set_state(or_net *n, int32_t gid, int var, const double *in) {
+    if (!gid_ok(n, gid) || var < 0 || var >= n->groups[gid].nvar || !in) return fail(OR_EINVAL, "set_state");
+    Group &g = n->groups[gid];
+    std::copy(in, in + g.n, g.S.begin() + (size_t)var * g.n); return OR_OK;
+}
+int or_net_stats(or_net *n, int64_t *steps, int64_t *launches, double *ms) {
+    if (!n) return fail(OR_EINVAL, "net");
+    if (steps) *steps = n->nstep; if (launches) *launches = 0; if (ms) *ms = 0; return OR_OK;
+}
+
+/* Uniform draw shared with the device Poisson source; exported so tests can
+ * pin the stream against known answers. */
+double or_philox_uniform(uint64_t seed, int64_t step, int64_t i) { return philox_uniform(seed, step, i); }
+
+}  /* extern "C" */

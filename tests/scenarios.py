@@ -1,0 +1,174 @@
+"""Network scenarios shared by the oracle tests and the GPU parity tests.
+
+Each function builds a network with the public API, runs it on whatever
+engine is active (``brian_b200.network.engine``) and returns plain arrays.
+"""
+import numpy as np
+
+import brian_b200 as b
+from brian_b200 import ms, mV, second, Hz
+from brian_b200.connections import fixed_indegree_csr
+
+
+def _result(net, groups=(), spikemons=(), statemons=(), conns=(), stdps=()):
+    out = {}
+    for k, g in enumerate(groups):
+        for v in g._names:
+            out["g%d.%s" % (k, v)] = np.array(getattr(g, v))
+    for k, m in enumerate(spikemons):
+        s, i = m._record()
+        out["spk%d.steps" % k] = s.copy()
+        out["spk%d.idx" % k] = i.copy()
+    for k, m in enumerate(statemons):
+        s, v = m._record()
+        out["st%d.steps" % k] = s.copy()
+        out["st%d.vals" % k] = v.copy()
+    for k, c in enumerate(conns):
+        out["w%d" % k] = c._weights().astype(np.float64).copy()
+    for k, s in enumerate(stdps):
+        a, p = s._traces()
+        out["stdp%d.pre" % k] = a.copy()
+        out["stdp%d.post" % k] = p.copy()
+    return out
+
+
+def cuba(N=4000, steps=10000, seed=1, p=0.02, record=10, refractory=0.0):
+    """Config 1: CUBA-4000, FP64, zero delay (examples/misc/CUBA.py:25-74)."""
+    taum, taue, taui = 20 * ms, 5 * ms, 10 * ms
+    Vt, Vr, El = -50 * mV, -60 * mV, -49 * mV
+    eqs = b.Equations("""
+    dv/dt  = (ge+gi-(v-El))/taum : volt
+    dge/dt = -ge/taue : volt
+    dgi/dt = -gi/taui : volt
+    """, taum=taum, taue=taue, taui=taui, El=El)
+    P = b.NeuronGroup(N, model=eqs, threshold=Vt, reset=Vr, refractory=refractory)
+    Ne = int(0.8 * N)
+    Pe = P.subgroup(Ne)
+    Pi = P.subgroup(N - Ne)
+    we, wi = 1.62 * mV, -9 * mV
+    Ce = b.Connection(Pe, P, "ge")
+    Ce.connect_random(Pe, P, p, weight=we, seed=seed)
+    Ci = b.Connection(Pi, P, "gi")
+    Ci.connect_random(Pi, P, p, weight=wi, seed=seed + 1)
+    rng = np.random.Generator(np.random.PCG64(seed + 2))
+    P.v = Vr + rng.random(N) * (Vt - Vr)
+    M = b.SpikeMonitor(P)
+    S = b.StateMonitor(P, "v", record=list(range(record)))
+    net = b.Network(P, Ce, Ci, M, S)
+    net.run(steps * 0.1 * ms)
+    return _result(net, groups=[P], spikemons=[M], statemons=[S])
+
+
+def cuba_delay(N=3000, indegree=100, steps=2000, seed=3, wdtype=np.float32, we=0.162e-2, wi=-0.9e-2,
+               hetero_weights=False):
+    """Config 2 in miniature: fixed in-degree (80% exc / 20% inh), integer
+    delays uniform in 1..50 steps, DelayConnections into ge and gi."""
+    taum, taue, taui = 20 * ms, 5 * ms, 10 * ms
+    Vt, Vr, El = -50 * mV, -60 * mV, -49 * mV
+    eqs = b.Equations("""
+    dv/dt  = (ge+gi-(v-El))/taum : volt
+    dge/dt = -ge/taue : volt
+    dgi/dt = -gi/taui : volt
+    """, taum=taum, taue=taue, taui=taui, El=El)
+    P = b.NeuronGroup(N, model=eqs, threshold=Vt, reset=Vr)
+    Ne = int(0.8 * N)
+    Pe, Pi = P.subgroup(Ne), P.subgroup(N - Ne)
+    ke = int(0.8 * indegree)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    conns = []
+    for src, n, k, w, var, sd in ((Pe, Ne, ke, we, "ge", seed + 10), (Pi, N - Ne, indegree - ke, wi, "gi", seed + 20)):
+        rowptr, cols = fixed_indegree_csr(n, N, k, seed=sd)
+        d = rng.integers(1, 51, size=len(cols)).astype(np.uint8)
+        C = b.DelayConnection(src, P, var, max_delay=5 * ms, dtype=wdtype)
+        wv = (w * (0.5 + rng.random(len(cols)))) if hetero_weights else w
+        C.connect_csr(rowptr, cols, wv, delay_steps=d)
+        conns.append(C)
+    P.v = Vr + rng.random(N) * (Vt - Vr)
+    M = b.SpikeMonitor(P)
+    S = b.StateMonitor(P, "v", record=[0, 1, N - 1])
+    net = b.Network(P, conns[0], conns[1], M, S)
+    net.run(steps * 0.1 * ms)
+    return _result(net, groups=[P], spikemons=[M], statemons=[S])
+
+
+def stdp(Nin=400, Nout=32, steps=3000, seed=5, dense=True, rate_lo=5.0, rate_hi=25.0, wdtype=np.float32):
+    """Config 3 in miniature: Poisson inputs -> LIF outputs, all-to-all,
+    ExponentialSTDP (examples/plasticity/STDP1.py)."""
+    taum, taue = 10 * ms, 5 * ms
+    Ee, vt, vr, El = 0 * mV, -54 * mV, -60 * mV, -74 * mV
+    gmax = 0.01
+    eqs = b.Equations("""
+    dv/dt=(ge*(Ee-vr)+El-v)/taum : volt
+    dge/dt=-ge/taue : 1
+    """, taum=taum, taue=taue, Ee=Ee, vr=vr, El=El)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    inp = b.PoissonGroup(Nin, rates=rng.uniform(rate_lo, rate_hi, Nin) * 20, seed=seed)
+    out = b.NeuronGroup(Nout, model=eqs, threshold=vt, reset=vr)
+    out.v = vr
+    W0 = rng.uniform(0, gmax, (Nin, Nout))
+    C = b.Connection(inp, out, "ge", structure="dense" if dense else "sparse", dtype=wdtype)
+    if dense:
+        C.connect(W=W0)
+    else:
+        mask = rng.random((Nin, Nout)) < 0.5
+        C.connect(W=W0 * mask)
+    S = b.ExponentialSTDP(C, 20 * ms, 20 * ms, 0.01, -0.0105, wmax=gmax)
+    M = b.SpikeMonitor(out)
+    Mi = b.SpikeMonitor(inp)
+    net = b.Network(inp, out, C, S, M, Mi)
+    net.run(steps * 0.1 * ms)
+    return _result(net, groups=[out], spikemons=[M, Mi], conns=[C], stdps=[S])
+
+
+def kitchen_sink(steps=400, seed=7):
+    """Refractoriness, variable threshold/reset, homogeneous delays,
+    modulation, dense structure, generators and subgroup monitors."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    N = 300
+    eqs = b.Equations("""
+    dv/dt = (I - v)/tau : volt
+    dI/dt = -I/taus : volt
+    dvt/dt = (vt0 - vt)/taut : volt
+    """, tau=10 * ms, taus=3 * ms, taut=30 * ms, vt0=-50 * mV)
+    G = b.NeuronGroup(N, model=eqs, threshold=b.VariableThreshold("vt", "v"), reset=-65 * mV,
+                      refractory=2 * ms)
+    G.v = -65 * mV + rng.random(N) * 20 * mV
+    G.vt = -50 * mV
+    G.I = rng.random(N) * 40 * mV
+    spk = [(int(i), float(t)) for i, t in zip(rng.integers(0, 50, 600), rng.random(600) * steps * 0.1 * ms)]
+    gen = b.SpikeGeneratorGroup(50, spk)
+    H = b.NeuronGroup(40, model="dx/dt = -x/(5*ms) : 1\nm : 1", threshold=0.5, reset=b.VariableReset("m", "x"))
+    H.x = rng.random(40)
+    H.m = rng.random(40) * 0.1
+    C1 = b.Connection(gen, G, "I", weight=3 * mV, sparseness=0.3)
+    C2 = b.Connection(G, G, "v", delay=1.5 * ms)
+    C2.connect_random(G, G, 0.05, weight=lambda i, j: 0.1 * mV * (1 + (i % 7) + (j % 5)), seed=seed)
+    C3 = b.Connection(gen, H, "x", structure="dense", weight=rng.random((50, 40)) * 0.2)
+    C4 = b.Connection(H, G[100:200], "vt", modulation="m", weight=0.5 * mV, sparseness=0.2)
+    C5 = b.DelayConnection(G[:150], H, "x", max_delay=3 * ms)
+    C5.connect_random(G[:150], H, 0.1, weight=0.05, seed=seed + 1, delay=(0.1 * ms, 2.9 * ms))
+    M1 = b.SpikeMonitor(G)
+    M2 = b.SpikeMonitor(G[50:120])
+    M3 = b.SpikeMonitor(H, delay=1 * ms)
+    S1 = b.StateMonitor(G, "v", record=[3, 0, 250], timestep=3)
+    S2 = b.StateMonitor(H, "x", record=True)
+    net = b.Network(G, gen, H, C1, C2, C3, C4, C5, M1, M2, M3, S1, S2)
+    net.run(steps * 0.05 * ms)
+    net.run(steps * 0.05 * ms)
+    return _result(net, groups=[G, H], spikemons=[M1, M2, M3], statemons=[S1, S2], conns=[C1, C2, C3, C4, C5])
+
+
+def compare(a, b_, exact=True):
+    """Assert two scenario results agree: identical spikes and steps,
+    states equal bit for bit (+0 == -0)."""
+    assert set(a) == set(b_), (set(a) ^ set(b_))
+    for k in sorted(a):
+        x, y = np.asarray(a[k]), np.asarray(b_[k])
+        assert x.shape == y.shape, (k, x.shape, y.shape)
+        if exact or x.dtype.kind in "iu":
+            if not np.array_equal(x, y):
+                bad = np.argwhere(x != y)
+                raise AssertionError("%s differs at %d positions, first %s: %r vs %r"
+                                     % (k, len(bad), bad[0], x[tuple(bad[0])], y[tuple(bad[0])]))
+        else:
+            np.testing.assert_allclose(x, y, rtol=1e-12, atol=0, err_msg=k)

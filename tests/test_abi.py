@@ -1,0 +1,47 @@
+"""The C ABI: every function declared in include/*.h is exported by the
+engine library (and, under the or_ prefix, by the oracle)."""
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared():
+    names = []
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names += re.findall(r"^\s*(?:BG_API\s+)?(?:int|double|void)\s+\**(bg_\w+)\s*\(", src, flags=re.M)
+    return sorted(set(names))
+
+
+def test_header_declares_entry_points():
+    names = declared()
+    assert "bg_net_create" in names and "bg_net_run" in names
+    assert len(names) >= 30
+
+
+def test_engine_library_exports_all():
+    from brian_b200 import build
+    lib_path = build.build()
+    lib = ctypes.CDLL(lib_path)
+    missing = [n for n in declared() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_oracle_exports_network_abi():
+    import oracle
+    from brian_b200._lib import SIGNATURES
+    lib = oracle.table().lib
+    missing = ["or_" + n for n in SIGNATURES if not hasattr(lib, "or_" + n)]
+    assert not missing, missing
+
+
+def test_product_table_has_typed_signatures():
+    from brian_b200._lib import SIGNATURES
+    names = set("bg_" + n for n in SIGNATURES)
+    assert names <= set(declared())
