@@ -1,0 +1,397 @@
+"""Benchmark: synaptic events/s on CUBA-262k (FP64 state, delays 1..50 steps).
+
+Workload (the scaled CUBA network): 262,144 LIF neurons (80% exc / 20% inh),
+dv/dt=(ge+gi-(v-El))/taum, dge/dt=-ge/taue, dgi/dt=-gi/taui, taum=20 ms,
+taue=5 ms, taui=10 ms, El=-49 mV, Vt=-50 mV, Vr=-60 mV; fixed in-degree 1000
+(800 exc + 200 inh), int32 targets, float32 weights we=0.162 mV,
+wi=-0.9 mV, uint8 delays uniform in {1..50} steps, dt=0.1 ms, seeded uniform
+v0 in [Vr, Vt].  One bench step = 1000 simulation steps (0.1 s simulated);
+the default 100 timed steps cover the config's 10 s.
+
+value  = synaptic events (sum over spiking sources of their out-degree) /
+         device seconds of the timed steps (CUDA events on the engine stream,
+         max over ranks; N>1 runs independent replicas).
+e2e    = the same metric through the public API from host arrays: network
+         construction + upload + 10 s run + spike record read back.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_NEURONS = 262144
+INDEGREE = 1000
+SIM_STEPS_PER_BENCH_STEP = 1000
+DT = 1e-4
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def make_inputs(seed, n=N_NEURONS, indegree=INDEGREE, builder=None):
+    """Host arrays of the network: CSR of both connections, delays, v0."""
+    ne = int(0.8 * n)
+    ni = n - ne
+    ke = int(0.8 * indegree)
+    ki = indegree - ke
+    if builder is None:
+        from brian_b200._lib import fixed_indegree_csr_native as builder
+    rng = np.random.Generator(np.random.PCG64(seed))
+    exc = builder(ne, n, ke, seed * 2 + 1)
+    inh = builder(ni, n, ki, seed * 2 + 2)
+    d_exc = rng.integers(1, 51, size=len(exc[1]), dtype=np.uint8)
+    d_inh = rng.integers(1, 51, size=len(inh[1]), dtype=np.uint8)
+    v0 = -60e-3 + rng.random(n) * (-50e-3 - -60e-3)
+    return dict(n=n, ne=ne, exc=exc, inh=inh, d_exc=d_exc, d_inh=d_inh, v0=v0)
+
+
+def build_network(inp, with_monitor=False):
+    import brian_b200 as b
+    from brian_b200 import ms, mV
+    eqs = b.Equations("""
+    dv/dt  = (ge+gi-(v-El))/taum : volt
+    dge/dt = -ge/taue : volt
+    dgi/dt = -gi/taui : volt
+    """, taum=20 * ms, taue=5 * ms, taui=10 * ms, El=-49 * mV)
+    P = b.NeuronGroup(inp["n"], model=eqs, threshold=-50 * mV, reset=-60 * mV)
+    Pe = P.subgroup(inp["ne"])
+    Pi = P.subgroup(inp["n"] - inp["ne"])
+    Ce = b.DelayConnection(Pe, P, "ge", max_delay=5 * ms, dtype=np.float32)
+    Ce.connect_csr(inp["exc"][0], inp["exc"][1], np.float32(0.162e-3), delay_steps=inp["d_exc"])
+    Ci = b.DelayConnection(Pi, P, "gi", max_delay=5 * ms, dtype=np.float32)
+    Ci.connect_csr(inp["inh"][0], inp["inh"][1], np.float32(-0.9e-3), delay_steps=inp["d_inh"])
+    P.v = inp["v0"]
+    objs = [P, Ce, Ci]
+    M = None
+    if with_monitor:
+        M = b.SpikeMonitor(P)
+        objs.append(M)
+    net = b.Network(*objs)
+    return net, P, (Ce, Ci), M
+
+
+def out_degree_events(inp, steps, idx):
+    """Events of recorded spikes: out-degree of each spiking source."""
+    deg = np.concatenate([np.diff(inp["exc"][0]), np.diff(inp["inh"][0])])
+    return int(deg[idx].sum())
+
+
+class ClockSampler(object):
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allreduce_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allreduce_sum(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def traffic_from_profiles(kernel_name):
+    """Per-launch DRAM bytes of `kernel_name` from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "cuba262k_kernels.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d.get("dram_bytes_per_launch", {}).get(kernel_name)
+    except Exception:
+        return None
+
+
+def cpu_baseline(inp, nsteps):
+    """The oracle (single-threaded C restatement) on the same network."""
+    import oracle
+    import brian_b200 as b
+    from brian_b200.network import engine
+    b.clear()
+    b.reinit_default_clock()
+    with engine(oracle.table()):
+        net, P, conns, _ = build_network(inp)
+        net.prepare()
+        rt = net._binding.rt
+        _, ev0 = rt.counters(1, 2)
+        t0 = time.perf_counter()
+        net.run(nsteps * DT)
+        wall = time.perf_counter() - t0
+        _, ev1 = rt.counters(1, 2)
+        events = int(ev1.sum() - ev0.sum())
+    net._invalidate()
+    return {"value": events / wall, "unit": "events/s", "cores": 1, "kind": "port",
+            "sample": "CUBA-262k, first %d simulation steps (%.2f s simulated) from the same initial state, "
+                      "%d events in %.1f s wall" % (nsteps, nsteps * DT, events, wall)}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    inp = make_inputs(args.seed, n=args.neurons, builder=_numpy_free_builder())
+    import oracle
+    import brian_b200 as b
+    from brian_b200.network import engine
+    with engine(oracle.table()):
+        net, P, conns, _ = build_network(inp)
+        net.prepare()
+        rt = net._binding.rt
+        per = args.ref_sim_steps
+        for _ in range(args.warmup):
+            net.run(per * DT)
+        _, ev0 = rt.counters(1, 2)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            net.run(per * DT)
+        wall = time.perf_counter() - t0
+        _, ev1 = rt.counters(1, 2)
+    events = int(ev1.sum() - ev0.sum())
+    value = events / wall
+    line = {"impl": "reference", "metric": "synaptic events/s (CUBA-262k)", "value": value, "unit": "events/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "CUBA-262k", "neurons": inp["n"], "indegree": INDEGREE,
+                       "sim_steps_per_step": per, "dt": DT},
+            "cpu_baseline": {"value": value, "unit": "events/s", "cores": 1, "kind": "port",
+                             "sample": "each step = %d simulation steps of CUBA-262k on the CPU restatement "
+                                       "(the reference is Python 2 and cannot run here)" % per},
+            "e2e": {"value": value, "unit": "events/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def _numpy_free_builder():
+    from brian_b200._lib import fixed_indegree_csr_native
+    return fixed_indegree_csr_native
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", type=int, default=64, choices=[64, 32])
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--profile-steps", type=int, default=300)
+    ap.add_argument("--cpu-steps", type=int, default=1000)
+    ap.add_argument("--ref-sim-steps", type=int, default=50)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--neurons", type=int, default=N_NEURONS)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    world, rank, local = dist_setup(args)
+    import brian_b200 as b
+    b.set_global_preferences(precision=args.precision, device=local)
+    inp = make_inputs(args.seed + rank, n=args.neurons)
+    net, P, conns, _ = build_network(inp)
+    net.prepare()
+    rt = net._binding.rt
+    per = SIM_STEPS_PER_BENCH_STEP
+    for _ in range(args.warmup):
+        net.run(per * DT)
+    _, ev0 = rt.counters(1, 2)
+    sp0, _ = rt.counters(1, 2)
+    l0 = rt.stats()["launches"]
+    dev_ms = 0.0
+    barrier(world)
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            net.run(per * DT)
+            dev_ms += rt.stats()["last_run_ms"]
+        wall = time.perf_counter() - t0
+    barrier(world)
+    sp1, ev1 = rt.counters(1, 2)
+    launches = rt.stats()["launches"] - l0
+    events = int(ev1.sum() - ev0.sum())
+    spikes = int(sp1.sum() - sp0.sum())
+    dev_s = allreduce_max(dev_ms / 1e3, world)
+    total_events = allreduce_sum(events, world)
+    value = total_events / dev_s
+    rate_hz = spikes / (inp["n"] * args.steps * per * DT)
+
+    # ---- per-kernel durations (CUDA events between launches) and roofline
+    evp0 = rt.counters(1, 2)[1]
+    prof = rt.profile(args.profile_steps, net.clock.step)
+    net.clock._n += args.profile_steps
+    evp = rt.counters(1, 2)[1] - evp0
+    peak, peak_kind = peaks()
+    n = inp["n"]
+    # algorithmic bytes: per neuron 3 state vars read+written (48 B) and two
+    # ring rows read+cleared (32 B) plus one history bit; per synaptic event
+    # a target index (4 B), an f32 weight (4 B), a delay (1 B) and the ring
+    # read-modify-write (16 B).  Pushes fused into head[g0] are counted there.
+    s_state = 8 if args.precision == 64 else 4
+    per_neuron = 3 * s_state * 2 + 2 * s_state * 2 + 1.0 / 8
+    per_event = 4 + 4 + 1 + 2 * s_state
+    names = [nm for nm, _ in prof]
+    kernels = []
+    for name, ms in prof:
+        if name.startswith("head"):
+            fused = [c for c in (0, 1) if not any(("c%d]" % c) in nm for nm in names)]
+            ev = sum(evp[c] for c in fused) / args.profile_steps
+            nbytes = n * per_neuron + ev * per_event
+        else:
+            c = 0 if "c0" in name else 1
+            nbytes = evp[c] / args.profile_steps * per_event
+        kernels.append({"kernel": name, "ms": ms, "alg_bytes": nbytes, "gbs": nbytes / (ms * 1e-3) / 1e9})
+    dom = max(kernels, key=lambda k: k["ms"])
+    traffic = traffic_from_profiles(dom["kernel"])
+    roofline = {"bound": "hbm", "kernel": dom["kernel"], "achieved": dom["gbs"], "peak": peak, "unit": "GB/s",
+                "frac": dom["gbs"] / peak, "peak_source": peak_kind, "traffic": traffic,
+                "per_kernel": [{k: (round(v, 6) if isinstance(v, float) else v) for k, v in kk.items()}
+                               for kk in kernels],
+                "step_alg_gbs": sum(k["alg_bytes"] for k in kernels) / (sum(k["ms"] for k in kernels) * 1e-3) / 1e9}
+    # the same algorithmic bytes over the graph-replayed timed region
+    step_bytes = n * per_neuron + events / (args.steps * per) * per_event
+    step_s = dev_ms / 1e3 / (args.steps * per)
+    roofline["timed_region"] = {"alg_bytes_per_sim_step": step_bytes, "us_per_sim_step": step_s * 1e6,
+                                "achieved": step_bytes / step_s / 1e9, "frac": step_bytes / step_s / 1e9 / peak}
+    net._invalidate()
+
+    # ---- end to end through the public API from host arrays
+    e2e = None
+    if not args.no_e2e:
+        b.clear()
+        t0 = time.perf_counter()
+        net2, P2, conns2, M2 = build_network(inp, with_monitor=True)
+        net2.prepare()
+        net2.run(args.steps * per * DT)
+        steps_rec, idx_rec = M2._record()
+        wall_e2e = time.perf_counter() - t0
+        ev_e2e = out_degree_events(inp, steps_rec, idx_rec)
+        h2d = (inp["exc"][0].nbytes + inp["exc"][1].nbytes + inp["inh"][0].nbytes + inp["inh"][1].nbytes +
+               inp["d_exc"].nbytes + inp["d_inh"].nbytes + len(inp["exc"][1]) * 4 + len(inp["inh"][1]) * 4 +
+               3 * n * 8)
+        d2h = len(idx_rec) * 8
+        wall_e2e = allreduce_max(wall_e2e, world)
+        e2e = {"value": allreduce_sum(ev_e2e, world) / wall_e2e, "unit": "events/s",
+               "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
+               "wall_s": wall_e2e, "includes": "network upload (CSR, weights, delays, state), run, spike read-back"}
+        net2._invalidate()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(inp, args.cpu_steps)
+
+    if rank == 0:
+        line = {"metric": "synaptic events/s (CUBA-262k)", "value": value, "unit": "events/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.precision == 64 else "f32", "data": "synthetic",
+                "config": {"workload": "CUBA-262k: 262144 LIF, in-degree 1000 (800 exc/200 inh), f32 weights, "
+                                       "u8 delays 1..50 steps, FP%d state, dt 0.1 ms" % args.precision,
+                           "neurons": n, "synapses": int(len(inp["exc"][1]) + len(inp["inh"][1])),
+                           "sim_steps_per_step": per, "simulated_s": args.steps * per * DT,
+                           "parallelism": "replicas" if world > 1 else "single",
+                           "l2": "inputs larger than L2 (2.4 GB of connectivity streamed per simulated second)"},
+                "mean_rate_hz": rate_hz, "events_timed": total_events, "wall_s": wall,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+                "clocks": clk.summary()}
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -50,6 +50,15 @@ SIGNATURES = {
     "group_set_state": [_vp, _i32, ct.c_int, _vp],
     "net_reinit": [_vp],
     "net_stats": [_vp, _P(_i64), _P(_i64), _P(_dbl)],
+    "net_counters": [_vp, _vp, _vp],
+}
+
+# entry points of the CUDA engine only
+ENGINE_ONLY = {
+    "net_profile": [_vp, _i64, _i64, _vp, _i64, _P(_i64)],
+    "net_item_name": [_vp, _i64, ct.c_char_p, _i64],
+    "fixed_indegree_csr": [_i64, _i64, _i64, _u64, _vp, _vp],
+    "net_set_persistent": [_vp, ct.c_int],
 }
 
 
@@ -89,7 +98,7 @@ def product_table():
         if not os.path.exists(LIB_PATH):
             from . import build
             build.build()
-        _product = FunctionTable(LIB_PATH, "bg_")
+        _product = FunctionTable(LIB_PATH, "bg_", dict(SIGNATURES, **ENGINE_ONLY))
     return _product
 
 
@@ -100,12 +109,14 @@ def _ptr(a):
 class Runtime(object):
     """One network handle on a function table."""
 
-    def __init__(self, table=None, device=0, precision=64, deterministic=True, dt=1e-4):
+    def __init__(self, table=None, device=0, precision=64, deterministic=True, dt=1e-4, persistent=True):
         self.t = table if table is not None else product_table()
         self.h = ct.c_void_p()
         self.precision = precision
         self.t.check(self.t.net_create(device, precision, 1 if deterministic else 0, float(dt),
                                        ct.byref(self.h)), "net_create")
+        if not persistent and hasattr(self.t, "net_set_persistent"):
+            self.t.check(self.t.net_set_persistent(self.h, 0), "net_set_persistent")
 
     def close(self):
         if self.h:
@@ -254,7 +265,37 @@ class Runtime(object):
     def reinit(self):
         self._c(self.t.net_reinit(self.h), "net_reinit")
 
+    def counters(self, ngroups, nconns):
+        g = np.zeros(max(1, ngroups), dtype=np.int64)
+        c = np.zeros(max(1, nconns), dtype=np.int64)
+        self._c(self.t.net_counters(self.h, _ptr(g), _ptr(c)), "net_counters")
+        return g[:ngroups], c[:nconns]
+
+    def profile(self, nsteps, clock_step0):
+        # mean device ms of each launch of a step, with the launch names
+        cap = 256
+        ms = np.zeros(cap)
+        n = _i64()
+        self._c(self.t.net_profile(self.h, int(nsteps), int(clock_step0), _ptr(ms), cap, ct.byref(n)), "net_profile")
+        out = []
+        buf = ct.create_string_buffer(128)
+        for i in range(n.value):
+            self._c(self.t.net_item_name(self.h, i, buf, 128), "net_item_name")
+            out.append((buf.value.decode(), float(ms[i])))
+        return out
+
     def stats(self):
         s, l, ms = _i64(), _i64(), _dbl()
         self._c(self.t.net_stats(self.h, ct.byref(s), ct.byref(l), ct.byref(ms)), "net_stats")
         return {"steps": s.value, "launches": l.value, "last_run_ms": ms.value}
+
+
+def fixed_indegree_csr_native(n_src, n_tgt, k, seed):
+    """Native construction of a fixed in-degree connectivity (see
+    include/brian_b200.h bg_fixed_indegree_csr)."""
+    t = product_table()
+    rowptr = np.empty(n_src + 1, dtype=np.int64)
+    cols = np.empty(n_tgt * k, dtype=np.int32)
+    t.check(t.fixed_indegree_csr(n_src, n_tgt, k, int(seed) & ((1 << 64) - 1), _ptr(rowptr), _ptr(cols)),
+            "fixed_indegree_csr")
+    return rowptr, cols

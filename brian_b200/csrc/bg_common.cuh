@@ -81,6 +81,10 @@ struct DevCtl {
 
 #define BG_DERR_MONITOR_OVERFLOW 1
 #define BG_DERR_RANGE 2
+#define BG_DERR_TIMEOUT 3      // a bounded inter-block wait gave up
+
+// Spin limit of inter-block waits: about a second of polling.
+#define BG_SPIN_LIMIT (1u << 22)
 
 __device__ __forceinline__ void bg_finish_step(DevCtl *ctl, int last) {
     if (!last) return;

@@ -11,6 +11,10 @@
 namespace bg {
 
 constexpr int kHeadThreads = 256;
+constexpr int kNPT = 4;                                  // neurons per thread
+constexpr int kBlockNeurons = kHeadThreads * kNPT;       // neurons per block
+constexpr int kPushBatch = 64;                           // spikes per push batch
+constexpr int kPushUnroll = 4;                           // elements per thread per pass
 constexpr int kMaxVars = 8;
 constexpr int kMaxDeliv = 4;
 constexpr int kMaxRec = 4;
@@ -18,6 +22,18 @@ constexpr int kMaxRec = 4;
 template <typename T> struct Deliv {   // DelayConnection ring delivered into this group
     T *ring; int64_t tn, to; int md; int var;
 };
+// DelayConnection whose spikes are pushed by the SOURCE group's head kernel
+// right after the threshold (shared-weight / atomic path).  The ring has
+// md >= max delay + 2 rows, so the rows written at step t, (t + d) mod md with
+// d <= max delay, never include row (t - 1) mod md that the tail of this
+// same kernel delivers and clears: no grid-wide ordering is needed.
+template <typename T> struct Push {
+    T *ring; int md; int64_t so, sn, tn;
+    const int64_t *rowptr; const int32_t *cols; const void *w; int w_bits; const uint8_t *d;
+    unsigned long long *events;
+};
+constexpr int kMaxPush = 4;
+
 struct RecDev {                        // StateMonitor recorded in this group
     int var; int nidx; const int32_t *idx; const int32_t *pos; const int32_t *blk_lo;
     void *buf; const long long *row_base; int timestep; long long start;
@@ -37,8 +53,20 @@ template <typename T> struct HeadArgs {
     uint32_t *hist; int depth; int64_t nwords;
     int ndeliv; Deliv<T> deliv[kMaxDeliv];
     int nrec; RecDev rec[kMaxRec];
+    int npush; Push<T> push[kMaxPush];
+    unsigned long long *spikes;    // running spike count of the group
     int tail, update, last;
 };
+
+// Block-aggregated counter update (one global atomic per block).
+__device__ __forceinline__ void block_count(unsigned long long *g, unsigned long long v) {
+    __shared__ unsigned long long acc;
+    if (threadIdx.x == 0) acc = 0ull;
+    __syncthreads();
+    if (v) atomicAdd(&acc, v);
+    __syncthreads();
+    if (threadIdx.x == 0 && acc && g) atomicAdd(g, acc);
+}
 
 template <typename T, int NV>
 __device__ __forceinline__ void set_var(T (&s)[NV], int var, T v) {
@@ -53,109 +81,223 @@ __device__ __forceinline__ T get_var(const T (&s)[NV], int var) {
     return r;
 }
 
-// One thread per neuron.  tail: finish the previous step (delayed-ring
-// delivery, reset, refractory clamp, state monitors) -- the
-// 'after_connections', 'resets' and 'end' slots; update: this step's
-// 'groups' slot (state update, threshold, refractory filter, history push).
+// Push the spikes of one block (ascending, from the history words in shared
+// memory) into the rings of its outgoing delayed connections.  The
+// (spike, synapse) pairs of a batch of spikes are flattened over the block's
+// threads; each thread first loads kPushUnroll independent synapses, then
+// issues their atomic adds, so a batch costs two dependent memory latencies
+// (row pointers, then synapses) however many spikes it holds.
+template <typename T, typename HA>
+__device__ __forceinline__ void push_block_spikes(const HA &a, const uint32_t *words, int64_t base, int nstep) {
+    __shared__ int32_t sl[kBlockNeurons];
+    __shared__ int64_t srow[kPushBatch];
+    __shared__ int32_t spref[kPushBatch + 1];
+    __shared__ int nsp;
+    const int tid = threadIdx.x, lane = tid & 31;
+    if (tid < 32) {
+        uint32_t w = words[lane];
+        const int c = __popc(w);
+        int incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) { const int v = __shfl_up_sync(0xffffffffu, incl, o); if (lane >= o) incl += v; }
+        int off = incl - c;
+        while (w) { const int b = __ffs(w) - 1; w &= w - 1; sl[off++] = lane * 32 + b; }
+        if (lane == 31) nsp = incl;
+    }
+    __syncthreads();
+    const int n = nsp;
+    if (n == 0) return;                      // block-uniform
+    for (int p = 0; p < a.npush; ++p) {
+        const Push<T> &q = a.push[p];
+        const int cur = nstep % q.md;
+        unsigned long long ev = 0;
+        for (int b0 = 0; b0 < n; b0 += kPushBatch) {
+            const int nb = min(kPushBatch, n - b0);
+            if (tid < nb) {
+                const int64_t gi = base + sl[b0 + tid];
+                int64_t r0 = 0, len = 0;
+                if (gi >= q.so && gi < q.so + q.sn) { r0 = __ldg(q.rowptr + (gi - q.so)); len = __ldg(q.rowptr + (gi - q.so) + 1) - r0; }
+                srow[tid] = r0;
+                spref[tid + 1] = (int32_t)len;
+            }
+            __syncthreads();
+            if (tid == 0) { spref[0] = 0; for (int k = 1; k <= nb; ++k) spref[k] += spref[k - 1]; }
+            __syncthreads();
+            const int total = spref[nb];
+            ev += (unsigned long long)total;
+            for (int e0 = 0; e0 < total; e0 += kHeadThreads * kPushUnroll) {
+                int32_t col[kPushUnroll]; T wv[kPushUnroll]; int slot[kPushUnroll];
+#pragma unroll
+                for (int u = 0; u < kPushUnroll; ++u) {
+                    const int e = e0 + u * kHeadThreads + tid;
+                    col[u] = -1;
+                    if (e < total) {
+                        int lo = 0, hi = nb;             // last s with spref[s] <= e
+                        while (hi - lo > 1) { const int m = (lo + hi) >> 1; if (spref[m] <= e) lo = m; else hi = m; }
+                        const int64_t k = srow[lo] + (e - spref[lo]);
+                        col[u] = __ldg(q.cols + k);
+                        wv[u] = q.w_bits == 32 ? (T)__ldg((const float *)q.w + k) : (T)__ldg((const double *)q.w + k);
+                        int sl2 = cur + (int)__ldg(q.d + k);
+                        slot[u] = sl2 >= q.md ? sl2 - q.md : sl2;
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kPushUnroll; ++u)
+                    if (col[u] >= 0) atomicAdd(&q.ring[(int64_t)slot[u] * q.tn + col[u]], wv[u]);
+            }
+            __syncthreads();
+        }
+        if (tid == 0 && ev && q.events) atomicAdd(q.events, ev);
+    }
+}
+
+// Step counters are below 2^31 (checked by the host), so slot arithmetic
+// runs in 32 bits.
+//
+// One block = kBlockNeurons consecutive neurons, kNPT per thread (neuron
+// base + u*kHeadThreads + tid), so every warp instruction touches one
+// 32-neuron history word and a 262k-neuron group fits in one wave.
+//   tail:   finish the previous step -- delayed-ring delivery
+//           ('after_connections'), reset / refractory clamp ('resets') and
+//           state monitors ('end');
+//   update: this step's 'groups' slot -- state update, threshold, refractory
+//           filter, history push -- then the pushes of this block's spikes
+//           into the rings of outgoing delayed connections.
 template <typename T, int NV>
-__global__ void __launch_bounds__(kHeadThreads) k_head(const HeadArgs<T> a) {
-    const int64_t i = (int64_t)blockIdx.x * kHeadThreads + threadIdx.x;
-    const bool act = i < a.n;
+__global__ void __launch_bounds__(kHeadThreads, 2) k_head(const HeadArgs<T> a) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int64_t base = (int64_t)blockIdx.x * kBlockNeurons;
     const long long nstep = a.ctl->nstep;
     const long long cs = nstep + a.ctl->clock_off;
-    T s[NV];
+    T s[kNPT][NV];
 #pragma unroll
-    for (int k = 0; k < NV; ++k) s[k] = act ? a.S[k * a.npad + i] : T(0);
+    for (int u = 0; u < kNPT; ++u) {
+        const int64_t i = base + u * kHeadThreads + tid;
+#pragma unroll
+        for (int k = 0; k < NV; ++k) s[u][k] = i < a.n ? a.S[k * a.npad + i] : T(0);
+    }
 
     if (a.tail) {
-        const long long ps = nstep - 1;
+        const int ps = (int)(nstep - 1);
         for (int d = 0; d < a.ndeliv; ++d) {
             const Deliv<T> &dv = a.deliv[d];
-            if (act && i >= dv.to && i < dv.to + dv.tn) {
-                T *r = dv.ring + (int64_t)(ps % dv.md) * dv.tn + (i - dv.to);
-                const T v = *r;
-                set_var<T, NV>(s, dv.var, rn<T>::add(get_var<T, NV>(s, dv.var), v));
-                if (v != T(0)) *r = T(0);
+            T *row = dv.ring + (int64_t)(ps % dv.md) * dv.tn - dv.to;
+#pragma unroll
+            for (int u = 0; u < kNPT; ++u) {
+                const int64_t i = base + u * kHeadThreads + tid;
+                if (i < a.n && i >= dv.to && i < dv.to + dv.tn) {
+                    const T v = row[i];
+                    set_var<T, NV>(s[u], dv.var, rn<T>::add(get_var<T, NV>(s[u], dv.var), v));
+                    if (v != T(0)) row[i] = T(0);
+                }
             }
         }
         if (a.period > 0) {
-            if (act && ps - (long long)a.last_spike[i] < a.period) set_var<T, NV>(s, a.clamp_var, a.clamp_val);
+#pragma unroll
+            for (int u = 0; u < kNPT; ++u) {
+                const int64_t i = base + u * kHeadThreads + tid;
+                if (i < a.n && (long long)ps - (long long)a.last_spike[i] < a.period)
+                    set_var<T, NV>(s[u], a.clamp_var, a.clamp_val);
+            }
         } else if (a.reset_kind) {
-            const uint32_t w = a.hist[(int64_t)(ps % a.depth) * a.nwords + (i >> 5)];
-            if (act && ((w >> (i & 31)) & 1u)) {
-                if (a.reset_kind == 1) set_var<T, NV>(s, a.reset_var, a.reset_val);
-                else set_var<T, NV>(s, a.reset_var, get_var<T, NV>(s, a.reset_var2));
+            const uint32_t *H = a.hist + (int64_t)(ps % a.depth) * a.nwords;
+#pragma unroll
+            for (int u = 0; u < kNPT; ++u) {
+                const int64_t i = base + u * kHeadThreads + tid;
+                const uint32_t w = H[i >> 5];
+                if (i < a.n && ((w >> lane) & 1u)) {
+                    if (a.reset_kind == 1) set_var<T, NV>(s[u], a.reset_var, a.reset_val);
+                    else set_var<T, NV>(s[u], a.reset_var, get_var<T, NV>(s[u], a.reset_var2));
+                }
             }
         }
         if (a.nrec) {
-            __shared__ T stash[kMaxRec][kHeadThreads];
-            for (int r = 0; r < a.nrec; ++r) stash[r][threadIdx.x] = get_var<T, NV>(s, a.rec[r].var);
-            __syncthreads();
+            __shared__ T stash[kBlockNeurons];
             for (int r = 0; r < a.nrec; ++r) {
                 const RecDev &m = a.rec[r];
-                const long long rel = ps - m.start;
-                if (rel < 0 || rel % m.timestep) continue;
+                const long long rel = (long long)ps - m.start;
+                if (rel < 0 || rel % m.timestep) continue;    // block-uniform
+#pragma unroll
+                for (int u = 0; u < kNPT; ++u) stash[u * kHeadThreads + tid] = get_var<T, NV>(s[u], m.var);
+                __syncthreads();
                 const long long row = rel / m.timestep - *m.row_base;
                 const int e0 = m.blk_lo[blockIdx.x], e1 = m.blk_lo[blockIdx.x + 1];
-                for (int e = e0 + threadIdx.x; e < e1; e += kHeadThreads) {
-                    const int li = m.idx[e] - (int)(blockIdx.x * kHeadThreads);
-                    ((T *)m.buf)[row * m.nidx + m.pos[e]] = stash[r][li];
-                }
+                for (int e = e0 + tid; e < e1; e += kHeadThreads)
+                    ((T *)m.buf)[row * m.nidx + m.pos[e]] = stash[m.idx[e] - (int)base];
+                __syncthreads();
             }
         }
     }
 
     if (a.update) {
-        if (a.linear) {
-            T x[NV];
+        __shared__ uint32_t words[kBlockNeurons / 32];
+        uint32_t nspk = 0;
 #pragma unroll
-            for (int j = 0; j < NV; ++j) {
-                T acc = rn<T>::mul(a.A[j * NV + 0], s[0]);
+        for (int u = 0; u < kNPT; ++u) {
+            const int64_t i = base + u * kHeadThreads + tid;
+            const bool act = i < a.n;
+            if (a.linear) {
+                T x[NV];
 #pragma unroll
-                for (int k = 1; k < NV; ++k) acc = rn<T>::add(acc, rn<T>::mul(a.A[j * NV + k], s[k]));
-                if (a.useC) acc = rn<T>::add(acc, a.C[j]);
-                x[j] = acc;
+                for (int j = 0; j < NV; ++j) {
+                    T acc = rn<T>::mul(a.A[j * NV + 0], s[u][0]);
+#pragma unroll
+                    for (int k = 1; k < NV; ++k) acc = rn<T>::add(acc, rn<T>::mul(a.A[j * NV + k], s[u][k]));
+                    if (a.useC) acc = rn<T>::add(acc, a.C[j]);
+                    x[j] = acc;
+                }
+#pragma unroll
+                for (int j = 0; j < NV; ++j) s[u][j] = x[j];
             }
-#pragma unroll
-            for (int j = 0; j < NV; ++j) s[j] = x[j];
+            bool spk = false;
+            if (act) {
+                switch (a.thr_kind) {
+                case 1: spk = get_var<T, NV>(s[u], a.thr_var) > a.thr_val; break;
+                case 2: spk = get_var<T, NV>(s[u], a.thr_var) > get_var<T, NV>(s[u], a.thr_var2); break;
+                case 3: {
+                    const double rate = (double)get_var<T, NV>(s[u], a.rate_var);
+                    spk = bg_philox_uniform(a.seed, cs, i) < __dmul_rn(rate, a.dt);
+                    break;
+                }
+                case 4: {
+                    // spikes of this clock step: [lo, e) of the (step, index)-sorted list
+                    int64_t lo = 0, hi = a.gen_n;
+                    while (lo < hi) { int64_t m = (lo + hi) >> 1; if (a.gen_steps[m] < cs) lo = m + 1; else hi = m; }
+                    int64_t e = lo, hi2 = a.gen_n;
+                    while (e < hi2) { int64_t m = (e + hi2) >> 1; if (a.gen_steps[m] <= cs) e = m + 1; else hi2 = m; }
+                    int64_t l2 = lo, h2 = e;
+                    while (l2 < h2) { int64_t m = (l2 + h2) >> 1; if (a.gen_idx[m] < i) l2 = m + 1; else h2 = m; }
+                    spk = l2 < e && a.gen_idx[l2] == i;
+                    break;
+                }
+                default: break;
+                }
+                if (spk && a.refr) {
+                    const double t = __dmul_rn((double)cs, a.dt);
+                    if (a.next_allowed[i] <= t) a.next_allowed[i] = __dadd_rn(t, a.refr_time);
+                    else spk = false;
+                }
+                if (spk && a.period > 0) a.last_spike[i] = (int32_t)nstep;
+            }
+            const uint32_t ball = __ballot_sync(0xffffffffu, spk);
+            if (lane == 0) {
+                a.hist[(int64_t)((int)nstep % a.depth) * a.nwords + ((base + u * kHeadThreads) >> 5) + warp] = ball;
+                words[u * (kHeadThreads / 32) + warp] = ball;
+                nspk += __popc(ball);
+            }
         }
-        bool spk = false;
-        if (act) {
-            switch (a.thr_kind) {
-            case 1: spk = get_var<T, NV>(s, a.thr_var) > a.thr_val; break;
-            case 2: spk = get_var<T, NV>(s, a.thr_var) > get_var<T, NV>(s, a.thr_var2); break;
-            case 3: {
-                const double rate = (double)get_var<T, NV>(s, a.rate_var);
-                spk = bg_philox_uniform(a.seed, cs, i) < __dmul_rn(rate, a.dt);
-                break;
-            }
-            case 4: {
-                // spikes of this clock step: [lo, hi) of the (step, index)-sorted list
-                int64_t lo = 0, hi = a.gen_n;
-                while (lo < hi) { int64_t m = (lo + hi) >> 1; if (a.gen_steps[m] < cs) lo = m + 1; else hi = m; }
-                int64_t e = lo, hi2 = a.gen_n;
-                while (e < hi2) { int64_t m = (e + hi2) >> 1; if (a.gen_steps[m] <= cs) e = m + 1; else hi2 = m; }
-                int64_t l2 = lo, h2 = e;
-                while (l2 < h2) { int64_t m = (l2 + h2) >> 1; if (a.gen_idx[m] < i) l2 = m + 1; else h2 = m; }
-                spk = l2 < e && a.gen_idx[l2] == i;
-                break;
-            }
-            default: break;
-            }
-            if (spk && a.refr) {
-                const double t = __dmul_rn((double)cs, a.dt);
-                if (a.next_allowed[i] <= t) a.next_allowed[i] = __dadd_rn(t, a.refr_time);
-                else spk = false;
-            }
-            if (spk && a.period > 0) a.last_spike[i] = (int32_t)nstep;
-        }
-        const uint32_t ball = __ballot_sync(0xffffffffu, spk);
-        if ((threadIdx.x & 31) == 0 && i < a.npad)
-            a.hist[(int64_t)(nstep % a.depth) * a.nwords + (i >> 5)] = ball;
+        block_count(a.spikes, nspk);       // contains __syncthreads: words[] is complete
+        if (a.npush) push_block_spikes<T>(a, words, base, (int)nstep);
     }
-    if (act && (a.update || a.tail)) {
+    if (a.update || a.tail) {
 #pragma unroll
-        for (int k = 0; k < NV; ++k) a.S[k * a.npad + i] = s[k];
+        for (int u = 0; u < kNPT; ++u) {
+            const int64_t i = base + u * kHeadThreads + tid;
+            if (i < a.n) {
+#pragma unroll
+                for (int k = 0; k < NV; ++k) a.S[k * a.npad + i] = s[u][k];
+            }
+        }
     }
     bg_finish_step(a.ctl, a.last);
 }
@@ -184,6 +326,7 @@ template <typename T> struct PropArgs {
     int parts;                      // row split for the atomic path
     // fused presynaptic STDP (stdp.py:370-414): w[i,:] += A_post; clip
     int stdp; double *A_pre; const double *A_post; double Ap; int pre_set; double wmin, wmax;
+    unsigned long long *events;     // running count of synaptic events
     int last;
 };
 
@@ -211,13 +354,14 @@ __global__ void __launch_bounds__(256) k_prop_atomic(const PropArgs<T> a) {
         const int lane = threadIdx.x & 31;
         const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
         const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-        const uint32_t *H = a.hist + (int64_t)((nstep - a.delay) % a.depth) * a.nwords;
+        const uint32_t *H = a.hist + (int64_t)((int)(nstep - a.delay) % a.depth) * a.nwords;
         const int64_t end = a.so + a.sn;
         const int64_t w0 = a.so >> 5, w1 = (end + 31) >> 5;
         const int64_t nch = (w1 - w0 + 31) >> 5;
         const int P = a.parts;
-        const int cur = RING ? (int)(nstep % a.md) : 0;
+        const int cur = RING ? (int)nstep % a.md : 0;
         const WT *W = (const WT *)a.w;
+        unsigned long long ev = 0;
         for (int64_t item = warp; item < nch * P; item += nwarps) {
             const int64_t c = item / P; const int p = (int)(item - c * P);
             const int64_t wi = w0 + c * 32 + lane;
@@ -232,6 +376,7 @@ __global__ void __launch_bounds__(256) k_prop_atomic(const PropArgs<T> a) {
                     const int64_t i = base + b - a.so;
                     const int64_t r0 = a.rowptr[i], r1 = a.rowptr[i + 1], len = r1 - r0;
                     const int64_t q0 = r0 + len * p / P, q1 = r0 + len * (p + 1) / P;
+                    if (p == 0 && lane == 0) ev += (unsigned long long)len;
                     for (int64_t k = q0 + lane; k < q1; k += 32) {
                         const int32_t j = a.cols[k];
                         const T wv = (T)W[k];
@@ -244,6 +389,7 @@ __global__ void __launch_bounds__(256) k_prop_atomic(const PropArgs<T> a) {
                 }
             }
         }
+        block_count(a.events, ev);
     }
     bg_finish_step(a.ctl, a.last);
 }
@@ -264,12 +410,13 @@ __global__ void __launch_bounds__(kOrdThreads) k_prop_ordered(const PropArgs<T> 
     const long long nstep = a.ctl->nstep;
     const int64_t t0 = (int64_t)blockIdx.x * kOrdTB, t1 = min(t0 + (int64_t)kOrdTB, a.tn);
     if (nstep >= a.delay && t0 < a.tn) {
-        const uint32_t *H = a.hist + (int64_t)((nstep - a.delay) % a.depth) * a.nwords;
+        const uint32_t *H = a.hist + (int64_t)((int)(nstep - a.delay) % a.depth) * a.nwords;
         const int64_t end = a.so + a.sn;
         const int64_t w0 = a.so >> 5, w1 = (end + 31) >> 5;
-        const int cur = RING ? (int)(nstep % a.md) : 0;
+        const int cur = RING ? (int)nstep % a.md : 0;
         WT *W = (WT *)a.w;
         const int tid = threadIdx.x;
+        unsigned long long ev = 0;
         // process the source range in chunks of kOrdThreads words
         for (int64_t cw = w0; cw < w1; cw += kOrdThreads) {
             const int64_t wi = cw + tid;
@@ -327,13 +474,16 @@ __global__ void __launch_bounds__(kOrdThreads) k_prop_ordered(const PropArgs<T> 
                         }
                         if (a.stdp) stdp_w<T, WT>(W, k, a.A_post[j], a.wmin, a.wmax);
                     }
-                    if (a.stdp && blockIdx.x == 0 && tid == 0)
-                        a.A_pre[i] = a.pre_set ? a.Ap : __dadd_rn(a.A_pre[i], a.Ap);
+                    if (blockIdx.x == 0 && tid == 0) {
+                        if (a.stdp) a.A_pre[i] = a.pre_set ? a.Ap : __dadd_rn(a.A_pre[i], a.Ap);
+                        ev += (unsigned long long)(a.dense ? a.tn : a.rowptr[i + 1] - a.rowptr[i]);
+                    }
                     __syncthreads();
                 }
             }
             __syncthreads();
         }
+        block_count(a.events, ev);
     }
     bg_finish_step(a.ctl, a.last);
 }
@@ -349,13 +499,14 @@ __global__ void __launch_bounds__(kDenseThreads) k_prop_dense(const PropArgs<T> 
     const long long nstep = a.ctl->nstep;
     const int64_t j = (int64_t)blockIdx.x * kDenseThreads + threadIdx.x;
     if (nstep >= a.delay) {
-        const uint32_t *H = a.hist + (int64_t)((nstep - a.delay) % a.depth) * a.nwords;
+        const uint32_t *H = a.hist + (int64_t)((int)(nstep - a.delay) % a.depth) * a.nwords;
         const int64_t end = a.so + a.sn;
         const int64_t w0 = a.so >> 5, w1 = (end + 31) >> 5;
         WT *W = (WT *)a.w;
         const int tid = threadIdx.x;
         T acc = j < a.tn ? a.sv[j] : T(0);
         const double apost = (a.stdp && j < a.tn) ? a.A_post[j] : 0.0;
+        unsigned long long ev = 0;
         for (int64_t cw = w0; cw < w1; cw += kDenseThreads) {
             const int64_t wi = cw + tid;
             const uint32_t word = wi < w1 ? masked_word(H, wi, a.so, end) : 0u;
@@ -391,10 +542,12 @@ __global__ void __launch_bounds__(kDenseThreads) k_prop_dense(const PropArgs<T> 
                         const int64_t i = sp[s];
                         a.A_pre[i] = a.pre_set ? a.Ap : __dadd_rn(a.A_pre[i], a.Ap);
                     }
+                if (blockIdx.x == 0 && tid == 0) ev += (unsigned long long)n * (unsigned long long)a.tn;
                 __syncthreads();
             }
         }
         if (j < a.tn) a.sv[j] = acc;
+        block_count(a.events, ev);
     }
     bg_finish_step(a.ctl, a.last);
 }
@@ -417,7 +570,7 @@ __global__ void __launch_bounds__(256) k_stdp_pre(const PropArgs<double> a) {
         const int lane = threadIdx.x & 31;
         const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
         const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-        const uint32_t *H = a.hist + (int64_t)((nstep - a.delay) % a.depth) * a.nwords;
+        const uint32_t *H = a.hist + (int64_t)((int)(nstep - a.delay) % a.depth) * a.nwords;
         const int64_t end = a.so + a.sn;
         const int64_t w0 = a.so >> 5, w1 = (end + 31) >> 5;
         WT *W = (WT *)a.w;
@@ -463,7 +616,7 @@ __global__ void __launch_bounds__(256) k_stdp_post(const PostArgs a) {
     __shared__ int ns;
     const long long nstep = a.ctl->nstep;
     if (nstep >= a.delay) {
-        const uint32_t *H = a.hist + (int64_t)((nstep - a.delay) % a.depth) * a.nwords;
+        const uint32_t *H = a.hist + (int64_t)((int)(nstep - a.delay) % a.depth) * a.nwords;
         const int64_t end = a.to + a.tn;
         const int64_t w0 = a.to >> 5, w1 = (end + 31) >> 5;
         WT *W = (WT *)a.w;
@@ -520,7 +673,7 @@ __global__ void __launch_bounds__(kMonThreads) k_spikemon(const MonArgs a) {
     const long long nstep = a.ctl->nstep;
     if (nstep >= a.delay && blockIdx.x == 0) {
         const long long cs = nstep + a.ctl->clock_off;
-        const uint32_t *H = a.hist + (int64_t)((nstep - a.delay) % a.depth) * a.nwords;
+        const uint32_t *H = a.hist + (int64_t)((int)(nstep - a.delay) % a.depth) * a.nwords;
         const int64_t end = a.origin + a.n;
         const int64_t w0 = a.origin >> 5, w1 = (end + 31) >> 5;
         long long base = *a.cnt;

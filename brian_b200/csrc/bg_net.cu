@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "bg_kernels.cuh"
+#include "bg_persist.cuh"
 #include "../../include/brian_b200.h"
 
 namespace {
@@ -50,7 +51,7 @@ struct HConn {
     bool dense = false; int64_t nnz = 0;
     std::vector<int64_t> rowptr; std::vector<int32_t> cols; std::vector<char> w; int w_bits = 64;
     int32_t delay = 0; bool hetero = false; std::vector<uint8_t> d; int md = 0; int mod_var = -1;
-    bool homogeneous = false; int parts = 1; int stdp = -1;
+    bool homogeneous = false; int parts = 1; int stdp = -1; bool fused_push = false;
     int64_t *dRow = nullptr; int32_t *dCols = nullptr; void *dW = nullptr; uint8_t *dD = nullptr; void *dRing = nullptr;
     int64_t *dColptr = nullptr, *dColk = nullptr; int32_t *dColsrc = nullptr;
     int64_t wcount() const { return dense ? sn * tn : nnz; }
@@ -80,6 +81,7 @@ using Launch = std::function<cudaError_t(cudaStream_t, int tail, int last)>;
 
 struct bg_net {
     int device = 0, precision = 64, deterministic = 1; double dt = 1e-4;
+    int allow_persist = 1;
     cudaStream_t stream = nullptr;
     std::vector<HGroup> groups; std::vector<HConn> conns; std::vector<HStdp> stdps;
     std::vector<HSpikeMon> smons; std::vector<HStateMon> stmons; std::vector<Item> items;
@@ -87,8 +89,14 @@ struct bg_net {
     DevCtl *dCtl = nullptr;
     bool prepared = false; long long nstep = 0;
     std::vector<Launch> step_launches;     // per-step kernels in schedule order
+    std::vector<std::string> item_names;   // one per step launch
+    unsigned long long *dCounters = nullptr; // [groups] spikes, then [conns] events
     std::vector<Launch> finalize_launches; // tail-only head kernels
     cudaGraphExec_t gexec = nullptr;
+    // persistent single-launch path (see bg_persist.cuh); empty when the
+    // network does not have its shape
+    std::function<cudaError_t(cudaStream_t, int nsteps)> persist;
+    unsigned int *dArrived = nullptr;
     int64_t launches = 0; double last_ms = 0;
     std::vector<void *> allocs;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -152,6 +160,16 @@ int build_group(bg_net *net, int gid) {
         const HConn &c = net->conns[g.delivs[k]];
         a.deliv[k].ring = (T *)c.dRing; a.deliv[k].tn = c.tn; a.deliv[k].to = c.to; a.deliv[k].md = c.md; a.deliv[k].var = c.var;
     }
+    a.npush = 0;
+    for (size_t ci = 0; ci < net->conns.size(); ++ci) {
+        const HConn &c = net->conns[ci];
+        if (!c.fused_push || c.src != gid) continue;
+        if (a.npush == bg::kMaxPush) return fail(BG_ENOSYS, "too many delayed connections from one group");
+        bg::Push<T> &q = a.push[a.npush++];
+        q.ring = (T *)c.dRing; q.md = c.md; q.so = c.so; q.sn = c.sn; q.tn = c.tn;
+        q.rowptr = c.dRow; q.cols = c.dCols; q.w = c.dW; q.w_bits = c.w_bits; q.d = c.dD;
+        q.events = net->dCounters + net->groups.size() + ci;
+    }
     if ((int)g.recs.size() > bg::kMaxRec) return fail(BG_ENOSYS, "too many StateMonitors on one group");
     a.nrec = (int)g.recs.size();
     for (int k = 0; k < a.nrec; ++k) {
@@ -160,10 +178,12 @@ int build_group(bg_net *net, int gid) {
         r.var = m.var; r.nidx = (int)m.idx.size(); r.idx = m.dIdx; r.pos = m.dPos; r.blk_lo = m.dBlk;
         r.buf = m.dBuf; r.row_base = m.dRowBase; r.timestep = m.timestep; r.start = m.start;
     }
-    const int64_t blocks = g.npad / bg::kHeadThreads;
+    const int64_t blocks = g.npad / bg::kBlockNeurons;
     const int nvar = g.nvar;
     if (nvar > bg::kMaxVars) return fail(BG_ENOSYS, "more than 8 state variables in a linear group");
     const bool has_tail = a.ndeliv || g.reset_kind || g.period > 0 || a.nrec;
+    a.spikes = net->dCounters + gid;
+    net->item_names.push_back("head[g" + std::to_string(gid) + "]");
     net->step_launches.push_back([a, nvar, blocks](cudaStream_t s, int tail, int last) {
         bg::HeadArgs<T> b = a; b.tail = tail; b.update = 1; b.last = last;
         return launch_head<T>(b, nvar, blocks, s);
@@ -216,6 +236,7 @@ int build_conn(bg_net *net, int cid) {
         a.pre_set = (s.inter == BG_STDP_NEAREST || s.inter == BG_STDP_NEAREST_PRE);
         a.wmin = s.wmin; a.wmax = s.wmax;
     }
+    if (c.fused_push) return BG_OK;   // pushed by the source group's head kernel
     int mode; int64_t grid;
     const bool use_atomic = !c.dense && c.mod_var < 0 && (c.homogeneous || !net->deterministic) && !a.stdp;
     if (c.dense) { mode = 4; grid = (c.tn + bg::kDenseThreads - 1) / bg::kDenseThreads; }
@@ -229,6 +250,9 @@ int build_conn(bg_net *net, int cid) {
         grid = std::max<int64_t>(1, (c.tn + bg::kOrdTB - 1) / bg::kOrdTB);
     }
     const int wb = c.w_bits;
+    a.events = net->dCounters + net->groups.size() + cid;
+    static const char *kModeName[] = {"prop_atomic", "prop_ring_atomic", "prop_ordered", "prop_ring_ordered", "prop_dense"};
+    net->item_names.push_back(std::string(kModeName[mode]) + "[c" + std::to_string(cid) + "]");
     net->step_launches.push_back([a, mode, grid, wb](cudaStream_t s, int, int last) {
         bg::PropArgs<T> b = a; b.last = last;
         return wb == 64 ? launch_prop<T, double>(b, mode, grid, s) : launch_prop<T, float>(b, mode, grid, s);
@@ -250,6 +274,7 @@ int build_stdp_pre(bg_net *net, int sid) {
     const int64_t nwords = (c.so + c.sn + 31) / 32 - c.so / 32;
     const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((nwords + 255) / 256, (int64_t)sm_count() * 4));
     const int wb = c.w_bits;
+    net->item_names.push_back("stdp_pre[s" + std::to_string(sid) + "]");
     net->step_launches.push_back([a, grid, wb](cudaStream_t st, int, int last) {
         bg::PropArgs<double> b = a; b.last = last;
         if (wb == 64) bg::k_stdp_pre<double><<<(unsigned)grid, 256, 0, st>>>(b);
@@ -273,6 +298,7 @@ int build_stdp_post(bg_net *net, int sid) {
     a.wmin = s.wmin; a.wmax = s.wmax;
     const int64_t grid = c.dense ? std::max<int64_t>(1, std::min<int64_t>((c.sn + 255) / 256, (int64_t)sm_count() * 2)) : 8;
     const int wb = c.w_bits;
+    net->item_names.push_back("stdp_post[s" + std::to_string(sid) + "]");
     net->step_launches.push_back([a, grid, wb](cudaStream_t st, int, int last) {
         bg::PostArgs b = a; b.last = last;
         if (wb == 64) bg::k_stdp_post<double><<<(unsigned)grid, 256, 0, st>>>(b);
@@ -289,6 +315,7 @@ int build_spikemon(bg_net *net, int k) {
     std::memset(&a, 0, sizeof(a));
     a.ctl = net->dCtl; a.hist = g.dHist; a.depth = g.depth; a.nwords = g.npad / 32; a.delay = m.delay;
     a.origin = m.origin; a.n = m.n; a.cnt = m.dCnt; a.cap = m.cap; a.idx = m.dIdx; a.steps = m.dSteps; a.step_base = m.dBase;
+    net->item_names.push_back("spikemon[m" + std::to_string(k) + "]");
     net->step_launches.push_back([a](cudaStream_t st, int, int last) {
         bg::MonArgs b = a; b.last = last;
         bg::k_spikemon<<<1, bg::kMonThreads, 0, st>>>(b);
@@ -304,6 +331,7 @@ int build_decay(bg_net *net, int sid) {
     a.A_pre = s.dApre; a.npre = c.sn; a.a_pre = s.a_pre; a.c_pre = s.c_pre;
     a.A_post = s.dApost; a.npost = c.tn; a.a_post = s.a_post; a.c_post = s.c_post; a.ctl = net->dCtl; a.last = 0;
     const int64_t grid = std::max<int64_t>(1, (c.sn + c.tn + 255) / 256);
+    net->item_names.push_back("stdp_decay[s" + std::to_string(sid) + "]");
     net->step_launches.push_back([a, grid](cudaStream_t st, int, int last) {
         bg::DecayArgs b = a; b.last = last;
         bg::k_stdp_decay<<<(unsigned)grid, 256, 0, st>>>(b);
@@ -356,6 +384,7 @@ int check_device_error(bg_net *net) {
     BG_CUDA(cudaMemcpyAsync(&h, net->dCtl, sizeof(h), cudaMemcpyDeviceToHost, net->stream));
     BG_CUDA(cudaStreamSynchronize(net->stream));
     if (h.err == BG_DERR_MONITOR_OVERFLOW) return fail(BG_ESTATE, "spike monitor buffer overflow");
+    if (h.err == BG_DERR_TIMEOUT) return fail(BG_ETIMEOUT, "inter-block wait timed out at step " + std::to_string(h.err_info));
     if (h.err) return fail(BG_ESTATE, "device error " + std::to_string(h.err));
     return BG_OK;
 }
@@ -396,6 +425,111 @@ int drain(bg_net *net, long long chunk_base_cs, long long tail_done_upto, long l
         m.rows_done = total;
         BG_CUDA(cudaMemcpy(m.dRowBase, &m.rows_done, 8, cudaMemcpyHostToDevice));
     }
+    return BG_OK;
+}
+
+}  // namespace
+
+namespace {
+
+template <typename T, int NV>
+cudaError_t launch_persist_nv(bg::PersistArgs<T> a, int64_t blocks, cudaStream_t s) {
+    void *args[] = {(void *)&a};
+    return cudaLaunchCooperativeKernel((const void *)bg::k_persist<T, NV>, dim3((unsigned)blocks),
+                                       dim3(bg::kHeadThreads), args, 0, s);
+}
+
+template <typename T, int NV>
+int persist_fits(int64_t blocks) {
+    int per_sm = 0, dev = 0, coop = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    if (!coop) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bg::k_persist<T, NV>, bg::kHeadThreads, 0) != cudaSuccess)
+        return 0;
+    return (int64_t)per_sm * sm_count() >= blocks;
+}
+
+// The persistent path applies to one linear group (at most 4 variables, no
+// refractoriness, no Poisson/generator input) whose every connection is a
+// shared-weight DelayConnection from the group onto itself, with no monitors
+// and no plasticity -- the CUBA benchmark topology.
+template <typename T>
+int build_persist(bg_net *net) {
+    net->persist = nullptr;
+    if (net->groups.size() != 1 || !net->smons.empty() || !net->stmons.empty() || !net->stdps.empty()) return BG_OK;
+    const HGroup &g = net->groups[0];
+    if (!g.linear || g.nvar < 1 || g.nvar > 4 || g.refr || g.period > 0) return BG_OK;
+    if (g.thr_kind != BG_THR_CONST && g.thr_kind != BG_THR_VAR && g.thr_kind != BG_THR_NONE) return BG_OK;
+    if (net->conns.empty() || (int)net->conns.size() > bg::kPersistMaxPush) return BG_OK;
+    int min_d = 255;
+    for (const HConn &c : net->conns) {
+        if (!c.fused_push || c.src != 0 || c.tgt != 0) return BG_OK;
+        for (uint8_t d : c.d) min_d = std::min<int>(min_d, d);
+    }
+    const int64_t blocks = g.npad / bg::kBlockNeurons;
+    int fits = 0;
+    switch (g.nvar) {
+    case 1: fits = persist_fits<T, 1>(blocks); break;
+    case 2: fits = persist_fits<T, 2>(blocks); break;
+    case 3: fits = persist_fits<T, 3>(blocks); break;
+    default: fits = persist_fits<T, 4>(blocks); break;
+    }
+    cudaGetLastError();
+    if (!fits) return BG_OK;
+    if (net->alloc(&net->dArrived, 64) != cudaSuccess) return fail(BG_ENOMEM, "arrival counter");
+    bg::PersistArgs<T> a;
+    std::memset(&a, 0, sizeof(a));
+    a.ctl = net->dCtl; a.S = (T *)g.dS; a.n = g.n; a.npad = g.npad; a.useC = g.useC;
+    for (int j = 0; j < g.nvar; ++j) {
+        for (int k = 0; k < g.nvar; ++k) a.A[j * g.nvar + k] = (T)g.A[j * g.nvar + k];
+        a.C[j] = g.useC ? (T)g.C[j] : T(0);
+    }
+    a.thr_kind = g.thr_kind; a.thr_var = g.thr_var; a.thr_var2 = g.thr_var2; a.thr_val = (T)g.thr_val;
+    a.reset_kind = g.reset_kind; a.reset_var = g.reset_var; a.reset_var2 = g.reset_var2; a.reset_val = (T)g.reset_val;
+    a.hist = g.dHist; a.depth = g.depth; a.nwords = g.npad / 32;
+    a.ndeliv = (int)g.delivs.size();
+    for (int k = 0; k < a.ndeliv; ++k) {
+        const HConn &c = net->conns[g.delivs[k]];
+        a.deliv[k].ring = (T *)c.dRing; a.deliv[k].tn = c.tn; a.deliv[k].to = c.to; a.deliv[k].md = c.md; a.deliv[k].var = c.var;
+    }
+    a.npush = (int)net->conns.size();
+    for (int p = 0; p < a.npush; ++p) {
+        const HConn &c = net->conns[p];
+        bg::Push<T> &q = a.push[p];
+        q.ring = (T *)c.dRing; q.md = c.md; q.so = c.so; q.sn = c.sn; q.tn = c.tn;
+        q.rowptr = c.dRow; q.cols = c.dCols; q.w = c.dW; q.w_bits = c.w_bits; q.d = c.dD;
+        q.events = net->dCounters + net->groups.size() + p;
+    }
+    a.spikes = net->dCounters;
+    a.arrived = net->dArrived;
+    a.lag = min_d >= 1 ? 2 : 1;
+    const int nvar = g.nvar;
+    unsigned int *arr = net->dArrived;
+    net->persist = [a, blocks, nvar, arr](cudaStream_t s, int nsteps) {
+        cudaError_t e = cudaMemsetAsync(arr, 0, 64, s);
+        if (e != cudaSuccess) return e;
+        bg::PersistArgs<T> b = a; b.nsteps = nsteps;
+        switch (nvar) {
+        case 1: return launch_persist_nv<T, 1>(b, blocks, s);
+        case 2: return launch_persist_nv<T, 2>(b, blocks, s);
+        case 3: return launch_persist_nv<T, 3>(b, blocks, s);
+        default: return launch_persist_nv<T, 4>(b, blocks, s);
+        }
+    };
+    return BG_OK;
+}
+
+// Runs nsteps with the persistent kernel (one launch) and advances the step
+// counter on the host and device.
+int run_persist(bg_net *n, int64_t nsteps) {
+    cudaError_t e = n->persist(n->stream, (int)nsteps);
+    if (e != cudaSuccess) return fail(BG_ECUDA, std::string("persistent launch: ") + cudaGetErrorString(e));
+    n->launches += 1;
+    n->nstep += nsteps;
+    long long ns = n->nstep;
+    BG_CUDA(cudaMemcpyAsync(&n->dCtl->nstep, &ns, 8, cudaMemcpyHostToDevice, n->stream));
+    BG_CUDA(cudaStreamSynchronize(n->stream));
     return BG_OK;
 }
 
@@ -449,7 +583,7 @@ int bg_group_add(bg_net *n, int64_t N, int nvar, const double *S0, int32_t *gid)
     if (n->prepared) return fail(BG_ESTATE, "network already prepared");
     if (nvar > bg::kMaxVars) return fail(BG_ENOSYS, "at most 8 state variables per group");
     HGroup g; g.n = N; g.nvar = nvar;
-    g.npad = std::max<int64_t>(bg::kHeadThreads, (N + bg::kHeadThreads - 1) / bg::kHeadThreads * bg::kHeadThreads);
+    g.npad = std::max<int64_t>(bg::kBlockNeurons, (N + bg::kBlockNeurons - 1) / bg::kBlockNeurons * bg::kBlockNeurons);
     g.S0.assign(S0, S0 + (size_t)N * nvar);
     n->groups.push_back(std::move(g));
     *gid = (int32_t)n->groups.size() - 1;
@@ -550,7 +684,11 @@ int bg_conn_add(bg_net *n, int32_t src, int64_t so, int64_t sn, int32_t tgt, int
     if (delays) {
         if (ring_depth < 1 || ring_depth > 255) return fail(BG_EINVAL, "ring depth must be in [1, 255]");
         for (int64_t k = 0; k < nnz; ++k) if (delays[k] >= ring_depth) return fail(BG_EINVAL, "delay >= ring depth");
-        c.hetero = true; c.md = ring_depth; c.d.assign(delays, delays + nnz);
+        // two spare rows beyond the reference's int(max_delay/dt)+1: the rows
+        // written at step t never include the rows delivered at steps t-1 and
+        // t-2, which lets the spike push ride on the source group's update
+        // kernel and lets blocks of the persistent kernel drift by one step
+        c.hetero = true; c.md = ring_depth + 2; c.d.assign(delays, delays + nnz);
     }
     n->conns.push_back(std::move(c));
     *cid = (int32_t)n->conns.size() - 1;
@@ -753,6 +891,7 @@ int bg_net_prepare(bg_net *n) {
             st = upload(n, c.dRow, c.rowptr.data(), (c.sn + 1) * 8); if (st) return st;
             st = upload(n, c.dCols, c.cols.data(), c.nnz * 4); if (st) return st;
         }
+        c.fused_push = c.hetero && !c.dense && c.mod_var < 0 && c.stdp < 0 && (c.homogeneous || !n->deterministic);
         if (c.hetero) {
             if (n->alloc(&c.dD, c.nnz) != cudaSuccess) return fail(BG_ENOMEM, "delays");
             st = upload(n, c.dD, c.d.data(), c.nnz); if (st) return st;
@@ -807,10 +946,10 @@ int bg_net_prepare(bg_net *n) {
         std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return m.idx[a] < m.idx[b]; });
         m.sorted.resize(w); m.pos.resize(w);
         for (int64_t e = 0; e < w; ++e) { m.sorted[e] = m.idx[order[e]]; m.pos[e] = order[e]; }
-        const int64_t nb = g.npad / bg::kHeadThreads;
+        const int64_t nb = g.npad / bg::kBlockNeurons;
         m.blk_lo.assign(nb + 1, 0);
         for (int64_t b = 0, e = 0; b <= nb; ++b) {
-            while (e < w && m.sorted[e] < b * bg::kHeadThreads) ++e;
+            while (e < w && m.sorted[e] < b * bg::kBlockNeurons) ++e;
             m.blk_lo[b] = (int32_t)e;
         }
         m.cap_rows = n->chunk_steps / m.timestep + 2;
@@ -825,6 +964,9 @@ int bg_net_prepare(bg_net *n) {
         BG_CUDA(cudaMemsetAsync(m.dRowBase, 0, 8, n->stream));
         g.recs.push_back((int)k);
     }
+    const size_t ncount = n->groups.size() + n->conns.size();
+    if (n->alloc(&n->dCounters, std::max<size_t>(1, ncount) * 8) != cudaSuccess) return fail(BG_ENOMEM, "counters");
+    BG_CUDA(cudaMemsetAsync(n->dCounters, 0, std::max<size_t>(1, ncount) * 8, n->stream));
     BG_CUDA(cudaStreamSynchronize(n->stream));
     int st = reset_dynamic(n);
     if (st) return st;
@@ -846,6 +988,8 @@ int bg_net_prepare(bg_net *n) {
         if (st) return st;
     }
     if (n->step_launches.empty()) return fail(BG_EINVAL, "empty network");
+    if (n->allow_persist) st = n->precision == 64 ? build_persist<double>(n) : build_persist<float>(n);
+    if (st) return st;
     BG_CUDA(cudaStreamSynchronize(n->stream));
     n->prepared = true;
     return BG_OK;
@@ -881,7 +1025,26 @@ int bg_net_run(bg_net *n, int64_t nsteps, int64_t cs0) {
     if (!n || nsteps < 0) return fail(BG_EINVAL, "bg_net_run");
     if (!n->prepared) { int st = bg_net_prepare(n); if (st) return st; }
     if (nsteps == 0) return BG_OK;
+    if (n->nstep + nsteps >= (1ll << 31) - 1) return fail(BG_EINVAL, "a network runs at most 2^31-1 steps");
     BG_CUDA(cudaSetDevice(n->device));
+    if (n->persist) {
+        long long off0 = cs0 - n->nstep;
+        BG_CUDA(cudaMemcpyAsync(&n->dCtl->clock_off, &off0, 8, cudaMemcpyHostToDevice, n->stream));
+        BG_CUDA(cudaEventRecord(n->ev0, n->stream));
+        const int64_t chunk = 1 << 20;
+        for (int64_t done = 0; done < nsteps;) {
+            const int64_t c = std::min(chunk, nsteps - done);
+            int st = run_persist(n, c);
+            if (st) return st;
+            done += c;
+        }
+        BG_CUDA(cudaEventRecord(n->ev1, n->stream));
+        BG_CUDA(cudaEventSynchronize(n->ev1));
+        float ms = 0;
+        BG_CUDA(cudaEventElapsedTime(&ms, n->ev0, n->ev1));
+        n->last_ms = ms;
+        return check_device_error(n);
+    }
     int st = ensure_graph(n);
     if (st) return st;
     long long off = cs0 - n->nstep;
@@ -954,6 +1117,13 @@ int bg_group_set_state(bg_net *n, int32_t gid, int var, const double *in) {
     return BG_OK;
 }
 
+int bg_net_set_persistent(bg_net *n, int enable) {
+    if (!n) return fail(BG_EINVAL, "net");
+    if (n->prepared) return fail(BG_ESTATE, "set before prepare");
+    n->allow_persist = enable ? 1 : 0;
+    return BG_OK;
+}
+
 int bg_net_reinit(bg_net *n) {
     if (!n) return fail(BG_EINVAL, "net");
     if (!n->prepared) return BG_OK;
@@ -961,6 +1131,78 @@ int bg_net_reinit(bg_net *n) {
     int st = reset_dynamic(n);
     if (st) return st;
     BG_CUDA(cudaStreamSynchronize(n->stream));
+    return BG_OK;
+}
+
+int bg_net_counters(bg_net *n, int64_t *group_spikes, int64_t *conn_events) {
+    if (!n) return fail(BG_EINVAL, "net");
+    if (!n->prepared) return fail(BG_ESTATE, "network not prepared");
+    BG_CUDA(cudaStreamSynchronize(n->stream));
+    std::vector<unsigned long long> h(n->groups.size() + n->conns.size());
+    if (!h.empty()) BG_CUDA(cudaMemcpy(h.data(), n->dCounters, h.size() * 8, cudaMemcpyDeviceToHost));
+    for (size_t g = 0; g < n->groups.size(); ++g) if (group_spikes) group_spikes[g] = (int64_t)h[g];
+    for (size_t c = 0; c < n->conns.size(); ++c) if (conn_events) conn_events[c] = (int64_t)h[n->groups.size() + c];
+    return BG_OK;
+}
+
+int bg_net_profile(bg_net *n, int64_t nsteps, int64_t cs0, double *ms, int64_t cap, int64_t *nitems) {
+    if (!n || nsteps <= 0 || !nitems) return fail(BG_EINVAL, "bg_net_profile");
+    if (!n->prepared) { int st = bg_net_prepare(n); if (st) return st; }
+    if (!n->smons.empty() || !n->stmons.empty())
+        return fail(BG_ENOSYS, "profiling runs networks without monitors");
+    BG_CUDA(cudaSetDevice(n->device));
+    if (n->persist) {
+        *nitems = 1;
+        cudaEvent_t e0, e1;
+        BG_CUDA(cudaEventCreate(&e0)); BG_CUDA(cudaEventCreate(&e1));
+        BG_CUDA(cudaEventRecord(e0, n->stream));
+        int st = run_persist(n, nsteps);
+        if (st) return st;
+        BG_CUDA(cudaEventRecord(e1, n->stream));
+        BG_CUDA(cudaEventSynchronize(e1));
+        float t = 0;
+        cudaEventElapsedTime(&t, e0, e1);
+        cudaEventDestroy(e0); cudaEventDestroy(e1);
+        if (ms && cap > 0) ms[0] = t / (double)nsteps;   // per simulation step
+        return check_device_error(n);
+    }
+    const size_t k = n->step_launches.size();
+    *nitems = (int64_t)k;
+    long long off = cs0 - n->nstep;
+    BG_CUDA(cudaMemcpyAsync(&n->dCtl->clock_off, &off, 8, cudaMemcpyHostToDevice, n->stream));
+    std::vector<cudaEvent_t> ev(k + 1);
+    for (auto &e : ev) BG_CUDA(cudaEventCreate(&e));
+    std::vector<double> acc(k, 0.0);
+    int st = BG_OK;
+    for (int64_t s = 0; s < nsteps && st == BG_OK; ++s) {
+        BG_CUDA(cudaEventRecord(ev[0], n->stream));
+        for (size_t i = 0; i < k; ++i) {
+            cudaError_t e = n->step_launches[i](n->stream, s > 0 ? 1 : 0, i + 1 == k);
+            if (e != cudaSuccess) { st = fail(BG_ECUDA, cudaGetErrorString(e)); break; }
+            BG_CUDA(cudaEventRecord(ev[i + 1], n->stream));
+        }
+        BG_CUDA(cudaEventSynchronize(ev[k]));
+        for (size_t i = 0; i < k; ++i) { float t = 0; cudaEventElapsedTime(&t, ev[i], ev[i + 1]); acc[i] += t; }
+        n->launches += (int64_t)k;
+    }
+    n->nstep += nsteps;
+    for (auto &f : n->finalize_launches) { cudaError_t e = f(n->stream, 1, 0); if (e != cudaSuccess && st == BG_OK) st = fail(BG_ECUDA, cudaGetErrorString(e)); }
+    BG_CUDA(cudaStreamSynchronize(n->stream));
+    for (auto &e : ev) cudaEventDestroy(e);
+    if (st) return st;
+    for (size_t i = 0; i < k && (int64_t)i < cap; ++i) if (ms) ms[i] = acc[i] / (double)nsteps;
+    return check_device_error(n);
+}
+
+int bg_net_item_name(bg_net *n, int64_t idx, char *buf, int64_t len) {
+    if (n && n->persist && buf && len > 0 && idx == 0) {
+        std::strncpy(buf, "persist[g0] (per step)", (size_t)len - 1);
+        buf[len - 1] = 0;
+        return BG_OK;
+    }
+    if (!n || !buf || len <= 0 || idx < 0 || idx >= (int64_t)n->item_names.size()) return fail(BG_EINVAL, "bg_net_item_name");
+    std::strncpy(buf, n->item_names[idx].c_str(), (size_t)len - 1);
+    buf[len - 1] = 0;
     return BG_OK;
 }
 

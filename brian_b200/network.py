@@ -33,13 +33,14 @@ from .stdp import ExponentialSTDP
 __all__ = ["Network", "MagicNetwork", "run", "reinit", "stop", "clear", "network_operation",
            "NetworkOperation", "engine", "set_global_preferences", "get_global_preference"]
 
-_PREFS = {"useweave": False, "precision": 64, "deterministic": True, "device": 0}
+_PREFS = {"useweave": False, "precision": 64, "deterministic": True, "device": 0, "persistent": True}
 _table_override = []
 
 
 def set_global_preferences(**kw):
     """Reference preference registry (globalprefs.py:57-106); engine keys:
-    precision (64|32), deterministic (bool), device (int)."""
+    precision (64|32), deterministic (bool), device (int), persistent (bool:
+    allow the single-launch step loop for networks of its shape)."""
     _PREFS.update(kw)
 
 
@@ -81,7 +82,7 @@ class _Binding(object):
 
     def __init__(self, net, table, dt):
         self.rt = Runtime(table, device=_PREFS["device"], precision=_PREFS["precision"],
-                          deterministic=_PREFS["deterministic"], dt=dt)
+                          deterministic=_PREFS["deterministic"], dt=dt, persistent=_PREFS["persistent"])
         self.gids = {}
         self.cids = {}
         self.sids = {}

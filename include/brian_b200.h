@@ -188,6 +188,31 @@ BG_API int bg_group_set_state(bg_net *net, int32_t gid, int var, const double *i
 /* Clears spike history, rings, refractory state and trace variables
  * (NeuronGroup.reinit / Connection.reinit); states are set by the caller. */
 BG_API int bg_net_reinit(bg_net *net);
+/* Running totals since prepare: spikes emitted per group (index = group id)
+ * and synaptic events (sum over spiking sources of their row length) per
+ * connection (index = connection id).  No counterpart in the reference;
+ * its benchmark derives events as spikes x out-degree. */
+BG_API int bg_net_counters(bg_net *net, int64_t *group_spikes,
+                           int64_t *conn_events);
+/* Runs nsteps steps launching each kernel of the step separately with CUDA
+ * events in between and writes the mean device milliseconds of every
+ * launch of the step (in schedule order) to ms[0..*nitems).  The steps
+ * are real simulation steps.  Networks with monitors are rejected. */
+BG_API int bg_net_profile(bg_net *net, int64_t nsteps, int64_t clock_step0,
+                          double *ms, int64_t cap, int64_t *nitems);
+/* Name of the idx-th launch of a step, e.g. "head[g0]", "prop_ring_atomic[c1]". */
+BG_API int bg_net_item_name(bg_net *net, int64_t idx, char *buf, int64_t len);
+/* Connectivity of random_matrix_fixed_column (construction.py:149-177):
+ * each of n_tgt targets gets k distinct sources drawn uniformly from
+ * [0, n_src); CSR over sources (rowptr n_src+1, cols n_tgt*k) with
+ * ascending targets.  Counter-based draws keyed by (seed, target). */
+BG_API int bg_fixed_indegree_csr(int64_t n_src, int64_t n_tgt, int64_t k,
+                                 uint64_t seed, int64_t *rowptr,
+                                 int32_t *cols);
+/* Allow (1, default) or forbid (0) the persistent single-launch step loop
+ * for networks of its shape; call before bg_net_prepare.  Both paths give
+ * identical results. */
+BG_API int bg_net_set_persistent(bg_net *net, int enable);
 /* steps run, kernel launches issued, device milliseconds of the last run. */
 BG_API int bg_net_stats(bg_net *net, int64_t *steps, int64_t *launches,
                  double *last_run_ms);

@@ -82,6 +82,7 @@ struct Group {
     std::vector<double> next_allowed;
     std::deque<std::vector<int32_t>> hist;   /* hist[0] = current step */
     int32_t depth = 1;
+    int64_t nspikes = 0;
 };
 struct Conn {
     int32_t src, tgt; int64_t so, sn, to, tn; int var;
@@ -93,6 +94,7 @@ struct Conn {
     int mod_var = -1;
     /* column index (built at prepare when STDP needs it) */
     std::vector<int64_t> colptr; std::vector<int64_t> colk; std::vector<int32_t> colsrc;
+    int64_t events = 0;
     double getw(int64_t k) const { return w_bits == 64 ? w64[k] : (double)w32[k]; }
 };
 struct Stdp {
@@ -426,6 +428,7 @@ static void step(or_net *n, int64_t cs) {
             for (int32_t i : kept) g.next_allowed[i] = t + g.refr_time;
             spikes.swap(kept);
         }
+        g.nspikes += (int64_t)spikes.size();
         g.hist.pop_back(); g.hist.push_front(std::move(spikes));
     }
     for (auto &s : n->stdps) {   /* trace groups G_pre / G_post (stdp.py:282-293) */
@@ -441,6 +444,7 @@ static void step(or_net *n, int64_t cs) {
             double *sv = &gt.S[(size_t)c.var * gt.n + c.to];
             const double *mod = c.mod_var >= 0 ? &gs.S[(size_t)c.mod_var * gs.n + c.so] : nullptr;
             for (int32_t i : spk) {
+                c.events += c.dense ? c.tn : c.rowptr[i + 1] - c.rowptr[i];
                 if (c.dense) {
                     for (int64_t j = 0; j < c.tn; ++j) {
                         double w = c.getw((int64_t)i * c.tn + j);
@@ -555,6 +559,12 @@ int or_group_set_state(or_net *n, int32_t gid, int var, const double *in) {
     if (!gid_ok(n, gid) || var < 0 || var >= n->groups[gid].nvar || !in) return fail(OR_EINVAL, "set_state");
     Group &g = n->groups[gid];
     std::copy(in, in + g.n, g.S.begin() + (size_t)var * g.n); return OR_OK;
+}
+int or_net_counters(or_net *n, int64_t *group_spikes, int64_t *conn_events) {
+    if (!n) return fail(OR_EINVAL, "net");
+    for (size_t g = 0; g < n->groups.size(); ++g) if (group_spikes) group_spikes[g] = n->groups[g].nspikes;
+    for (size_t c = 0; c < n->conns.size(); ++c) if (conn_events) conn_events[c] = n->conns[c].events;
+    return OR_OK;
 }
 int or_net_stats(or_net *n, int64_t *steps, int64_t *launches, double *ms) {
     if (!n) return fail(OR_EINVAL, "net");

@@ -60,7 +60,7 @@ def cuba(N=4000, steps=10000, seed=1, p=0.02, record=10, refractory=0.0):
 
 
 def cuba_delay(N=3000, indegree=100, steps=2000, seed=3, wdtype=np.float32, we=0.162e-2, wi=-0.9e-2,
-               hetero_weights=False):
+               hetero_weights=False, monitors=True, dmin=1, runs=1):
     """Config 2 in miniature: fixed in-degree (80% exc / 20% inh), integer
     delays uniform in 1..50 steps, DelayConnections into ge and gi."""
     taum, taue, taui = 20 * ms, 5 * ms, 10 * ms
@@ -78,12 +78,21 @@ def cuba_delay(N=3000, indegree=100, steps=2000, seed=3, wdtype=np.float32, we=0
     conns = []
     for src, n, k, w, var, sd in ((Pe, Ne, ke, we, "ge", seed + 10), (Pi, N - Ne, indegree - ke, wi, "gi", seed + 20)):
         rowptr, cols = fixed_indegree_csr(n, N, k, seed=sd)
-        d = rng.integers(1, 51, size=len(cols)).astype(np.uint8)
+        d = rng.integers(dmin, 51, size=len(cols)).astype(np.uint8)
         C = b.DelayConnection(src, P, var, max_delay=5 * ms, dtype=wdtype)
         wv = (w * (0.5 + rng.random(len(cols)))) if hetero_weights else w
         C.connect_csr(rowptr, cols, wv, delay_steps=d)
         conns.append(C)
     P.v = Vr + rng.random(N) * (Vt - Vr)
+    if not monitors:
+        # no monitors: the engine may take its persistent single-launch path
+        net = b.Network(P, conns[0], conns[1])
+        for _ in range(runs):
+            net.run(steps * 0.1 * ms / runs)
+        out = _result(net, groups=[P])
+        g, c = net._binding.rt.counters(1, 2)
+        out["spikes"], out["events"] = g.copy(), c.copy()
+        return out
     M = b.SpikeMonitor(P)
     S = b.StateMonitor(P, "v", record=[0, 1, N - 1])
     net = b.Network(P, conns[0], conns[1], M, S)

@@ -47,6 +47,19 @@ def test_delay_ring_bit_exact(oracle_table, gpu_table, wdtype):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("dmin,runs", [(1, 1), (1, 3), (0, 2)])
+def test_persistent_path_bit_exact(oracle_table, gpu_table, dmin, runs):
+    """No monitors: single group with shared-weight DelayConnections runs in
+    the persistent cooperative kernel (lag-2 wait; lag-1 when a delay is 0)."""
+    ref, gpu = _both(scenarios.cuba_delay, oracle_table, monitors=False, dmin=dmin, runs=runs, N=6000,
+                     steps=3000)
+    assert ref["spikes"][0] > 1000
+    scenarios.compare(ref, gpu)
+    import brian_b200 as bb
+    assert bb.network._magic_cache is not None
+
+
+@pytest.mark.gpu
 def test_delay_ring_general_weights_ordered(oracle_table, gpu_table):
     ref, gpu = _both(scenarios.cuba_delay, oracle_table, hetero_weights=True, steps=1000)
     scenarios.compare(ref, gpu)
