@@ -326,7 +326,7 @@ def main():
     names = [nm for nm, _ in prof]
     kernels = []
     for name, ms in prof:
-        if name.startswith("head"):
+        if name.startswith("head") or name.startswith("persist"):
             fused = [c for c in (0, 1) if not any(("c%d]" % c) in nm for nm in names)]
             ev = sum(evp[c] for c in fused) / args.profile_steps
             nbytes = n * per_neuron + ev * per_event

@@ -19,9 +19,38 @@ constexpr int kMaxVars = 8;
 constexpr int kMaxDeliv = 4;
 constexpr int kMaxRec = 4;
 
-template <typename T> struct Deliv {   // DelayConnection ring delivered into this group
+// DelayConnection ring delivered into this group.  With one shared weight w
+// the ring holds event COUNTS (uint16, rows of tnp = tn rounded up to even
+// entries) and delivery adds table[k], where table[k] = table[k-1] + w with
+// table[0] = 0: exactly the value the reference's ring entry reaches after k
+// additions of w (delayconnection.py:152-153), in any order.
+template <typename T> struct Deliv {
     T *ring; int64_t tn, to; int md; int var;
+    uint16_t *cring; int64_t tnp; const T *table;
 };
+
+// Count-ring helpers: entry col of a row is the low/high half of a 32-bit word.
+__device__ __forceinline__ void cring_add(uint16_t *row, int32_t col) {
+    atomicAdd(reinterpret_cast<unsigned int *>(row + (col & ~1)), 1u << ((col & 1) << 4));
+}
+
+// Value delivered to target neuron i (group index) from ring row ps % md,
+// which is then cleared.  CG: read through L2 only (the persistent kernel
+// reads rows that other blocks of the same launch incremented).
+template <typename T, bool CG>
+__device__ __forceinline__ T deliver(const Deliv<T> &dv, int ps, int64_t i) {
+    const int64_t r = ps % dv.md;
+    if (dv.cring) {
+        uint16_t *p = dv.cring + r * dv.tnp + (i - dv.to);
+        const uint16_t c = CG ? __ldcg(p) : *p;
+        if (c) { *p = 0; return __ldg(dv.table + c); }
+        return T(0);
+    }
+    T *p = dv.ring + r * dv.tn + (i - dv.to);
+    const T v = CG ? __ldcg(p) : *p;
+    if (v != T(0)) *p = T(0);
+    return v;
+}
 // DelayConnection whose spikes are pushed by the SOURCE group's head kernel
 // right after the threshold (shared-weight / atomic path).  The ring has
 // md >= max delay + 2 rows, so the rows written at step t, (t + d) mod md with
@@ -31,6 +60,7 @@ template <typename T> struct Push {
     T *ring; int md; int64_t so, sn, tn;
     const int64_t *rowptr; const int32_t *cols; const void *w; int w_bits; const uint8_t *d;
     unsigned long long *events;
+    uint16_t *cring; int64_t tnp;      // count ring (shared weight), else null
 };
 constexpr int kMaxPush = 4;
 
@@ -87,6 +117,41 @@ __device__ __forceinline__ T get_var(const T (&s)[NV], int var) {
 // threads; each thread first loads kPushUnroll independent synapses, then
 // issues their atomic adds, so a batch costs two dependent memory latencies
 // (row pointers, then synapses) however many spikes it holds.
+// Scatter the (spike, synapse) pairs of one batch: pair e belongs to spike
+// s with spref[s] <= e < spref[s+1] and is synapse srow[s] + e - spref[s].
+// Each thread loads kPushUnroll independent synapses before issuing their
+// atomics.  Count rings need no weight.
+template <typename T>
+__device__ __forceinline__ void scatter_batch(const Push<T> &q, int cur, const int64_t *srow, const int32_t *spref,
+                                              int nb, int total) {
+    const int tid = threadIdx.x;
+    for (int e0 = 0; e0 < total; e0 += kHeadThreads * kPushUnroll) {
+        int32_t col[kPushUnroll]; T wv[kPushUnroll]; int slot[kPushUnroll];
+#pragma unroll
+        for (int u = 0; u < kPushUnroll; ++u) {
+            const int e = e0 + u * kHeadThreads + tid;
+            col[u] = -1;
+            wv[u] = T(0);
+            slot[u] = 0;
+            if (e < total) {
+                int lo = 0, hi = nb;             // last s with spref[s] <= e
+                while (hi - lo > 1) { const int m = (lo + hi) >> 1; if (spref[m] <= e) lo = m; else hi = m; }
+                const int64_t k = srow[lo] + (e - spref[lo]);
+                col[u] = __ldg(q.cols + k);
+                if (!q.cring) wv[u] = q.w_bits == 32 ? (T)__ldg((const float *)q.w + k) : (T)__ldg((const double *)q.w + k);
+                const int sl2 = cur + (int)__ldg(q.d + k);
+                slot[u] = sl2 >= q.md ? sl2 - q.md : sl2;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kPushUnroll; ++u) {
+            if (col[u] < 0) continue;
+            if (q.cring) cring_add(q.cring + (int64_t)slot[u] * q.tnp, col[u]);
+            else atomicAdd(&q.ring[(int64_t)slot[u] * q.tn + col[u]], wv[u]);
+        }
+    }
+}
+
 template <typename T, typename HA>
 __device__ __forceinline__ void push_block_spikes(const HA &a, const uint32_t *words, int64_t base, int nstep) {
     __shared__ int32_t sl[kBlockNeurons];
@@ -125,26 +190,7 @@ __device__ __forceinline__ void push_block_spikes(const HA &a, const uint32_t *w
             __syncthreads();
             const int total = spref[nb];
             ev += (unsigned long long)total;
-            for (int e0 = 0; e0 < total; e0 += kHeadThreads * kPushUnroll) {
-                int32_t col[kPushUnroll]; T wv[kPushUnroll]; int slot[kPushUnroll];
-#pragma unroll
-                for (int u = 0; u < kPushUnroll; ++u) {
-                    const int e = e0 + u * kHeadThreads + tid;
-                    col[u] = -1;
-                    if (e < total) {
-                        int lo = 0, hi = nb;             // last s with spref[s] <= e
-                        while (hi - lo > 1) { const int m = (lo + hi) >> 1; if (spref[m] <= e) lo = m; else hi = m; }
-                        const int64_t k = srow[lo] + (e - spref[lo]);
-                        col[u] = __ldg(q.cols + k);
-                        wv[u] = q.w_bits == 32 ? (T)__ldg((const float *)q.w + k) : (T)__ldg((const double *)q.w + k);
-                        int sl2 = cur + (int)__ldg(q.d + k);
-                        slot[u] = sl2 >= q.md ? sl2 - q.md : sl2;
-                    }
-                }
-#pragma unroll
-                for (int u = 0; u < kPushUnroll; ++u)
-                    if (col[u] >= 0) atomicAdd(&q.ring[(int64_t)slot[u] * q.tn + col[u]], wv[u]);
-            }
+            scatter_batch<T>(q, cur, srow, spref, nb, total);
             __syncthreads();
         }
         if (tid == 0 && ev && q.events) atomicAdd(q.events, ev);
@@ -181,15 +227,11 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_head(const HeadArgs<T> a) {
         const int ps = (int)(nstep - 1);
         for (int d = 0; d < a.ndeliv; ++d) {
             const Deliv<T> &dv = a.deliv[d];
-            T *row = dv.ring + (int64_t)(ps % dv.md) * dv.tn - dv.to;
 #pragma unroll
             for (int u = 0; u < kNPT; ++u) {
                 const int64_t i = base + u * kHeadThreads + tid;
-                if (i < a.n && i >= dv.to && i < dv.to + dv.tn) {
-                    const T v = row[i];
-                    set_var<T, NV>(s[u], dv.var, rn<T>::add(get_var<T, NV>(s[u], dv.var), v));
-                    if (v != T(0)) row[i] = T(0);
-                }
+                if (i < a.n && i >= dv.to && i < dv.to + dv.tn)
+                    set_var<T, NV>(s[u], dv.var, rn<T>::add(get_var<T, NV>(s[u], dv.var), deliver<T, false>(dv, ps, i)));
             }
         }
         if (a.period > 0) {

@@ -52,6 +52,7 @@ struct HConn {
     std::vector<int64_t> rowptr; std::vector<int32_t> cols; std::vector<char> w; int w_bits = 64;
     int32_t delay = 0; bool hetero = false; std::vector<uint8_t> d; int md = 0; int mod_var = -1;
     bool homogeneous = false; int parts = 1; int stdp = -1; bool fused_push = false;
+    uint16_t *dCRing = nullptr; int64_t tnp = 0; void *dTable = nullptr;   // count ring (shared weight)
     int64_t *dRow = nullptr; int32_t *dCols = nullptr; void *dW = nullptr; uint8_t *dD = nullptr; void *dRing = nullptr;
     int64_t *dColptr = nullptr, *dColk = nullptr; int32_t *dColsrc = nullptr;
     int64_t wcount() const { return dense ? sn * tn : nnz; }
@@ -159,6 +160,7 @@ int build_group(bg_net *net, int gid) {
     for (int k = 0; k < a.ndeliv; ++k) {
         const HConn &c = net->conns[g.delivs[k]];
         a.deliv[k].ring = (T *)c.dRing; a.deliv[k].tn = c.tn; a.deliv[k].to = c.to; a.deliv[k].md = c.md; a.deliv[k].var = c.var;
+        a.deliv[k].cring = c.dCRing; a.deliv[k].tnp = c.tnp; a.deliv[k].table = (const T *)c.dTable;
     }
     a.npush = 0;
     for (size_t ci = 0; ci < net->conns.size(); ++ci) {
@@ -169,6 +171,7 @@ int build_group(bg_net *net, int gid) {
         q.ring = (T *)c.dRing; q.md = c.md; q.so = c.so; q.sn = c.sn; q.tn = c.tn;
         q.rowptr = c.dRow; q.cols = c.dCols; q.w = c.dW; q.w_bits = c.w_bits; q.d = c.dD;
         q.events = net->dCounters + net->groups.size() + ci;
+        q.cring = c.dCRing; q.tnp = c.tnp;
     }
     if ((int)g.recs.size() > bg::kMaxRec) return fail(BG_ENOSYS, "too many StateMonitors on one group");
     a.nrec = (int)g.recs.size();
@@ -369,8 +372,10 @@ int reset_dynamic(bg_net *net) {
             BG_CUDA(cudaStreamSynchronize(net->stream));
         }
     }
-    for (auto &c : net->conns)
+    for (auto &c : net->conns) {
         if (c.dRing) BG_CUDA(cudaMemsetAsync(c.dRing, 0, (size_t)c.md * c.tn * tsize(net), net->stream));
+        if (c.dCRing) BG_CUDA(cudaMemsetAsync(c.dCRing, 0, (size_t)c.md * c.tnp * 2, net->stream));
+    }
     for (auto &s : net->stdps) {
         const HConn &c = net->conns[s.cid];
         BG_CUDA(cudaMemsetAsync(s.dApre, 0, c.sn * 8, net->stream));
@@ -492,6 +497,7 @@ int build_persist(bg_net *net) {
     for (int k = 0; k < a.ndeliv; ++k) {
         const HConn &c = net->conns[g.delivs[k]];
         a.deliv[k].ring = (T *)c.dRing; a.deliv[k].tn = c.tn; a.deliv[k].to = c.to; a.deliv[k].md = c.md; a.deliv[k].var = c.var;
+        a.deliv[k].cring = c.dCRing; a.deliv[k].tnp = c.tnp; a.deliv[k].table = (const T *)c.dTable;
     }
     a.npush = (int)net->conns.size();
     for (int p = 0; p < a.npush; ++p) {
@@ -500,6 +506,7 @@ int build_persist(bg_net *net) {
         q.ring = (T *)c.dRing; q.md = c.md; q.so = c.so; q.sn = c.sn; q.tn = c.tn;
         q.rowptr = c.dRow; q.cols = c.dCols; q.w = c.dW; q.w_bits = c.w_bits; q.d = c.dD;
         q.events = net->dCounters + net->groups.size() + p;
+        q.cring = c.dCRing; q.tnp = c.tnp;
     }
     a.spikes = net->dCounters;
     a.arrived = net->dArrived;
@@ -895,7 +902,34 @@ int bg_net_prepare(bg_net *n) {
         if (c.hetero) {
             if (n->alloc(&c.dD, c.nnz) != cudaSuccess) return fail(BG_ENOMEM, "delays");
             st = upload(n, c.dD, c.d.data(), c.nnz); if (st) return st;
-            if (n->alloc(&c.dRing, (size_t)c.md * c.tn * ts) != cudaSuccess) return fail(BG_ENOMEM, "delay ring");
+            // A shared weight on the atomic path: the ring counts events per
+            // (row, target) and delivery looks up the k-fold sum of the weight.
+            // A row entry collects at most one event per synapse, so counts
+            // stay below the largest in-degree.
+            int64_t kmax = 0;
+            if (c.fused_push && c.homogeneous && c.nnz > 0) {
+                std::vector<int32_t> indeg(c.tn, 0);
+                for (int32_t j : c.cols) kmax = std::max<int64_t>(kmax, ++indeg[j]);
+            }
+            if (kmax > 0 && kmax < 65535) {
+                c.tnp = (c.tn + 1) & ~1ll;
+                if (n->alloc(&c.dCRing, (size_t)c.md * c.tnp * 2) != cudaSuccess) return fail(BG_ENOMEM, "count ring");
+                if (n->alloc(&c.dTable, (size_t)(kmax + 1) * ts) != cudaSuccess) return fail(BG_ENOMEM, "count table");
+                const double w0 = c.w_bits == 64 ? *(const double *)c.w.data() : (double)*(const float *)c.w.data();
+                if (n->precision == 64) {
+                    std::vector<double> tab(kmax + 1, 0.0);
+                    for (int64_t k = 1; k <= kmax; ++k) tab[k] = tab[k - 1] + w0;
+                    st = upload(n, c.dTable, tab.data(), tab.size() * 8); if (st) return st;
+                } else {
+                    std::vector<float> tab(kmax + 1, 0.0f);
+                    const float wf = (float)w0;
+                    for (int64_t k = 1; k <= kmax; ++k) tab[k] = tab[k - 1] + wf;
+                    st = upload(n, c.dTable, tab.data(), tab.size() * 4); if (st) return st;
+                }
+                BG_CUDA(cudaStreamSynchronize(n->stream));
+            } else if (n->alloc(&c.dRing, (size_t)c.md * c.tn * ts) != cudaSuccess) {
+                return fail(BG_ENOMEM, "delay ring");
+            }
             n->groups[c.tgt].delivs.push_back((int)ci);
         }
         if (c.stdp >= 0 && !c.dense) {

@@ -42,6 +42,28 @@ __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int *p) {
     return v;
 }
 
+// Block-uniform variable access without runtime-indexed register arrays:
+// `var` is a kernel parameter, so the switch is a uniform branch.
+template <typename T, int NV>
+__device__ __forceinline__ T uget(const T (&s)[NV], int var) {
+    switch (var) {
+    case 0: return s[0];
+    case 1: if (NV > 1) return s[NV > 1 ? 1 : 0]; break;
+    case 2: if (NV > 2) return s[NV > 2 ? 2 : 0]; break;
+    default: if (NV > 3) return s[NV > 3 ? 3 : 0]; break;
+    }
+    return T(0);
+}
+template <typename T, int NV>
+__device__ __forceinline__ void uset(T (&s)[NV], int var, T v) {
+    switch (var) {
+    case 0: s[0] = v; break;
+    case 1: if (NV > 1) s[NV > 1 ? 1 : 0] = v; break;
+    case 2: if (NV > 2) s[NV > 2 ? 2 : 0] = v; break;
+    default: if (NV > 3) s[NV > 3 ? 3 : 0] = v; break;
+    }
+}
+
 template <typename T, int NV>
 __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T> a) {
     __shared__ int64_t srp[kPersistMaxPush][kBlockNeurons + 1];
@@ -51,26 +73,30 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T
     __shared__ int32_t spref[kPushBatch + 1];
     __shared__ int nsp, abort_flag;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int64_t base = (int64_t)blockIdx.x * kBlockNeurons;
+    const int base = blockIdx.x * kBlockNeurons;               // neuron counts < 2^31
+    const int nvalid = (int)min((int64_t)kBlockNeurons, a.n - (int64_t)base);
     const unsigned int G = gridDim.x;
     const long long t0 = a.ctl->nstep;
-    // row pointers of this block's neurons (clamped: outside the source range
-    // a row is empty)
     for (int p = 0; p < a.npush; ++p) {
         const Push<T> &q = a.push[p];
         for (int j = tid; j <= kBlockNeurons; j += kHeadThreads) {
-            int64_t r = base + j - q.so;
+            int64_t r = (int64_t)base + j - q.so;
             r = r < 0 ? 0 : (r > q.sn ? q.sn : r);
             srp[p][j] = q.rowptr[r];
         }
     }
     if (tid == 0) abort_flag = 0;
+    // deliveries: does this block lie inside the target range?  (uniform)
+    bool dfull[kMaxDeliv];
+#pragma unroll
+    for (int d = 0; d < kMaxDeliv; ++d)
+        dfull[d] = d < a.ndeliv && a.deliv[d].to <= base && (int64_t)base + kBlockNeurons <= a.deliv[d].to + a.deliv[d].tn;
     T s[kNPT][NV];
 #pragma unroll
     for (int u = 0; u < kNPT; ++u) {
-        const int64_t i = base + u * kHeadThreads + tid;
+        const int li = u * kHeadThreads + tid;
 #pragma unroll
-        for (int k = 0; k < NV; ++k) s[u][k] = i < a.n ? a.S[k * a.npad + i] : T(0);
+        for (int k = 0; k < NV; ++k) s[u][k] = li < nvalid ? a.S[k * a.npad + base + li] : T(0);
     }
     unsigned int prev_spk = 0;                  // bit u: neuron u spiked last step
     unsigned long long my_spikes = 0, my_events[kPersistMaxPush] = {0, 0};
@@ -90,7 +116,7 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T
                     unsigned int it = 0;
                     while (ld_acquire_u32(ctr) < target) {
                         if (++it > BG_SPIN_LIMIT) { abort_flag = 1; bg_raise(a.ctl, BG_DERR_TIMEOUT, t); break; }
-                        __nanosleep(64);
+                        __nanosleep(32);
                     }
                 }
                 __syncthreads();
@@ -99,32 +125,50 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T
             const int ps = (int)(t - 1);
             for (int d = 0; d < a.ndeliv; ++d) {
                 const Deliv<T> &dv = a.deliv[d];
-                T *row = dv.ring + (int64_t)(ps % dv.md) * dv.tn - dv.to;
+                const int r = ps % dv.md;
+                if (dv.cring) {
+                    uint16_t *row = dv.cring + (int64_t)r * dv.tnp + (base - dv.to);
+                    uint16_t c[kNPT];
 #pragma unroll
-                for (int u = 0; u < kNPT; ++u) {
-                    const int64_t i = base + u * kHeadThreads + tid;
-                    if (i < a.n && i >= dv.to && i < dv.to + dv.tn) {
-                        const T v = __ldcg(row + i);
-                        set_var<T, NV>(s[u], dv.var, rn<T>::add(get_var<T, NV>(s[u], dv.var), v));
-                        if (v != T(0)) row[i] = T(0);
+                    for (int u = 0; u < kNPT; ++u) {
+                        const int li = u * kHeadThreads + tid;
+                        const int64_t gi = (int64_t)base + li;
+                        c[u] = (li < nvalid && (dfull[d] || (gi >= dv.to && gi < dv.to + dv.tn))) ? __ldcg(row + li) : 0;
+                    }
+#pragma unroll
+                    for (int u = 0; u < kNPT; ++u) {
+                        if (c[u]) row[u * kHeadThreads + tid] = 0;
+                        const T v = c[u] ? __ldg(dv.table + c[u]) : T(0);
+                        uset<T, NV>(s[u], dv.var, rn<T>::add(uget<T, NV>(s[u], dv.var), v));
+                    }
+                } else {
+                    T *row = dv.ring + (int64_t)r * dv.tn + (base - dv.to);
+#pragma unroll
+                    for (int u = 0; u < kNPT; ++u) {
+                        const int li = u * kHeadThreads + tid;
+                        const int64_t gi = (int64_t)base + li;
+                        if (li < nvalid && (dfull[d] || (gi >= dv.to && gi < dv.to + dv.tn))) {
+                            const T v = __ldcg(row + li);
+                            if (v != T(0)) row[li] = T(0);
+                            uset<T, NV>(s[u], dv.var, rn<T>::add(uget<T, NV>(s[u], dv.var), v));
+                        }
                     }
                 }
             }
             if (a.reset_kind) {
 #pragma unroll
                 for (int u = 0; u < kNPT; ++u)
-                    if ((prev_spk >> u) & 1u) {
-                        if (a.reset_kind == 1) set_var<T, NV>(s[u], a.reset_var, a.reset_val);
-                        else set_var<T, NV>(s[u], a.reset_var, get_var<T, NV>(s[u], a.reset_var2));
-                    }
+                    if ((prev_spk >> u) & 1u)
+                        uset<T, NV>(s[u], a.reset_var, a.reset_kind == 1 ? a.reset_val : uget<T, NV>(s[u], a.reset_var2));
             }
         }
         if (st == a.nsteps) break;
         // ---- update, threshold, history
         prev_spk = 0;
+        const int hslot = (int)t % a.depth;
 #pragma unroll
         for (int u = 0; u < kNPT; ++u) {
-            const int64_t i = base + u * kHeadThreads + tid;
+            const int li = u * kHeadThreads + tid;
             T x[NV];
 #pragma unroll
             for (int j = 0; j < NV; ++j) {
@@ -137,20 +181,21 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T
 #pragma unroll
             for (int j = 0; j < NV; ++j) s[u][j] = x[j];
             bool spk = false;
-            if (i < a.n) {
-                if (a.thr_kind == 1) spk = get_var<T, NV>(s[u], a.thr_var) > a.thr_val;
-                else if (a.thr_kind == 2) spk = get_var<T, NV>(s[u], a.thr_var) > get_var<T, NV>(s[u], a.thr_var2);
+            if (li < nvalid) {
+                if (a.thr_kind == 1) spk = uget<T, NV>(s[u], a.thr_var) > a.thr_val;
+                else if (a.thr_kind == 2) spk = uget<T, NV>(s[u], a.thr_var) > uget<T, NV>(s[u], a.thr_var2);
             }
             prev_spk |= (spk ? 1u : 0u) << u;
             const uint32_t ball = __ballot_sync(0xffffffffu, spk);
             if (lane == 0) {
-                a.hist[(int64_t)((int)t % a.depth) * a.nwords + ((base + u * kHeadThreads) >> 5) + warp] = ball;
+                a.hist[(int64_t)hslot * a.nwords + ((base + u * kHeadThreads) >> 5) + warp] = ball;
                 words[u * (kHeadThreads / 32) + warp] = ball;
                 my_spikes += __popc(ball);
             }
         }
         __syncthreads();
-        // ---- push this block's spikes
+        // ---- push this block's spikes: one flattened scatter over every
+        // (connection, spike) pair of the block
         if (a.npush) {
             if (tid < 32) {
                 uint32_t w = words[lane];
@@ -169,35 +214,26 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T
                 const int cur = (int)t % q.md;
                 for (int b0 = 0; b0 < n; b0 += kPushBatch) {
                     const int nb = min(kPushBatch, n - b0);
-                    if (tid < nb) {
-                        const int j = sl[b0 + tid];
-                        srow[tid] = srp[p][j];
-                        spref[tid + 1] = (int32_t)(srp[p][j + 1] - srp[p][j]);
+                    // warp 0: row starts and an inclusive scan of row lengths
+                    if (tid < 32) {
+                        int len0 = 0, len1 = 0;
+                        if (lane < nb) { const int j = sl[b0 + lane]; srow[lane] = srp[p][j]; len0 = (int)(srp[p][j + 1] - srp[p][j]); }
+                        if (lane + 32 < nb) { const int j = sl[b0 + lane + 32]; srow[lane + 32] = srp[p][j]; len1 = (int)(srp[p][j + 1] - srp[p][j]); }
+                        int i0 = len0, i1 = len1;
+#pragma unroll
+                        for (int o = 1; o < 32; o <<= 1) {
+                            const int v0 = __shfl_up_sync(0xffffffffu, i0, o), v1 = __shfl_up_sync(0xffffffffu, i1, o);
+                            if (lane >= o) { i0 += v0; i1 += v1; }
+                        }
+                        const int tot0 = __shfl_sync(0xffffffffu, i0, 31);
+                        spref[lane + 1] = i0;
+                        spref[lane + 33] = tot0 + i1;
+                        if (lane == 0) spref[0] = 0;
                     }
-                    __syncthreads();
-                    if (tid == 0) { spref[0] = 0; for (int k = 1; k <= nb; ++k) spref[k] += spref[k - 1]; my_events[p] += spref[nb]; }
                     __syncthreads();
                     const int total = spref[nb];
-                    for (int e0 = 0; e0 < total; e0 += kHeadThreads * kPushUnroll) {
-                        int32_t col[kPushUnroll]; T wv[kPushUnroll]; int slot[kPushUnroll];
-#pragma unroll
-                        for (int u = 0; u < kPushUnroll; ++u) {
-                            const int e = e0 + u * kHeadThreads + tid;
-                            col[u] = -1;
-                            if (e < total) {
-                                int lo = 0, hi = nb;
-                                while (hi - lo > 1) { const int m = (lo + hi) >> 1; if (spref[m] <= e) lo = m; else hi = m; }
-                                const int64_t k = srow[lo] + (e - spref[lo]);
-                                col[u] = __ldg(q.cols + k);
-                                wv[u] = q.w_bits == 32 ? (T)__ldg((const float *)q.w + k) : (T)__ldg((const double *)q.w + k);
-                                const int sl2 = cur + (int)__ldg(q.d + k);
-                                slot[u] = sl2 >= q.md ? sl2 - q.md : sl2;
-                            }
-                        }
-#pragma unroll
-                        for (int u = 0; u < kPushUnroll; ++u)
-                            if (col[u] >= 0) atomicAdd(&q.ring[(int64_t)slot[u] * q.tn + col[u]], wv[u]);
-                    }
+                    if (tid == 0) my_events[p] += (unsigned long long)total;
+                    scatter_batch<T>(q, cur, srow, spref, nb, total);
                     __syncthreads();
                 }
             }
@@ -208,10 +244,10 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T
     }
 #pragma unroll
     for (int u = 0; u < kNPT; ++u) {
-        const int64_t i = base + u * kHeadThreads + tid;
-        if (i < a.n) {
+        const int li = u * kHeadThreads + tid;
+        if (li < nvalid) {
 #pragma unroll
-            for (int k = 0; k < NV; ++k) a.S[k * a.npad + i] = s[u][k];
+            for (int k = 0; k < NV; ++k) a.S[k * a.npad + base + li] = s[u][k];
         }
     }
     block_count(a.spikes, my_spikes);
