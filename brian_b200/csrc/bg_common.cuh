@@ -13,6 +13,10 @@
 #define BG_ENOSYS (-7)
 #define BG_ECOMPILE (-8)
 
+// Records the calling thread's error message for bg_last_error (library
+// internal; defined in bg_net.cu).
+int bg_internal_fail(int code, const char *msg);
+
 // ---------------------------------------------------------------------------
 // Philox4x32-10 counter-based generator (Salmon, Moraes, Dror, Shaw,
 // "Parallel random numbers: as easy as 1, 2, 3", SC'11).  One 4x32 block per

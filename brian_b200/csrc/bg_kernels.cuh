@@ -596,7 +596,7 @@ __global__ void __launch_bounds__(kDenseThreads) k_prop_dense(const PropArgs<T> 
 
 // STDP trace decay (the G_pre/G_post groups' 1x1 linear updaters).
 struct DecayArgs { double *A_pre; int64_t npre; double a_pre, c_pre; double *A_post; int64_t npost; double a_post, c_post; DevCtl *ctl; int last; };
-__global__ void k_stdp_decay(const DecayArgs a) {
+static __global__ void k_stdp_decay(const DecayArgs a) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < a.npre) a.A_pre[i] = __dadd_rn(__dmul_rn(a.a_pre, a.A_pre[i]), a.c_pre);
     else if (i < a.npre + a.npost) { const int64_t j = i - a.npre; a.A_post[j] = __dadd_rn(__dmul_rn(a.a_post, a.A_post[j]), a.c_post); }
@@ -710,7 +710,7 @@ struct MonArgs {
     int last;
 };
 constexpr int kMonThreads = 1024;
-__global__ void __launch_bounds__(kMonThreads) k_spikemon(const MonArgs a) {
+static __global__ void __launch_bounds__(kMonThreads) k_spikemon(const MonArgs a) {
     __shared__ int wcnt[kMonThreads / 32 + 1];
     const long long nstep = a.ctl->nstep;
     if (nstep >= a.delay && blockIdx.x == 0) {

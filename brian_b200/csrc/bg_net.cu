@@ -542,6 +542,8 @@ int run_persist(bg_net *n, int64_t nsteps) {
 
 }  // namespace
 
+int bg_internal_fail(int code, const char *msg) { return fail(code, msg); }
+
 // ============================================================== C ABI
 extern "C" {
 

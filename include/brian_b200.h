@@ -213,6 +213,38 @@ BG_API int bg_fixed_indegree_csr(int64_t n_src, int64_t n_tgt, int64_t k,
  * for networks of its shape; call before bg_net_prepare.  Both paths give
  * identical results. */
 BG_API int bg_net_set_persistent(bg_net *net, int enable);
+/* ---- allocation-free entry point ------------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory (code inside another framework's caching allocator, a process that
+ * reserved all device memory up front, a call made while a CUDA-graph
+ * recorder forbids allocation): runs one linear group with up to 4
+ * shared-weight DelayConnections onto itself for nsteps steps, like a fresh
+ * bg_net with those objects and bg_net_run(nsteps, 0), with identical
+ * results.  It calls no cudaMalloc/cudaFree; its scratch is a file-scope
+ * device array of bg_noalloc_scratch_bytes() bytes (32 MiB) that every GPU
+ * loading the library holds until the process exits.  Networks needing more
+ * scratch are rejected with BG_EINVAL.
+ *   S      device, [nvar][n] row-major (stride n), updated in place
+ *   A, C   host, the linear propagator (C may be NULL)
+ *   connection c: sources [src_origin[c], +src_n[c]) of the group, target
+ *   variable tgt_var[c]; rowptr[c] (device, src_n+1), cols[c] (device,
+ *   targets in [0,n), ascending per row), delays[c] (device, steps below
+ *   ring_depth[c] = int(max_delay/dt)+1), shared weight weight[c].
+ * All calls share the scratch and each one clears what must start at zero,
+ * so calls that overlap on the GPU (different streams or threads) race.  The
+ * first call on a device looks up the scratch address for that device; make
+ * that first call before any stream capture.  *spikes_out receives the
+ * number of spikes emitted (may be NULL); stream may be NULL. */
+BG_API int bg_delay_group_run_noalloc(
+    int64_t n, int nvar, double *S, const double *A, const double *C,
+    int thr_var, double thr_val, int reset_var, double reset_val, int nconn,
+    const int64_t *src_origin, const int64_t *src_n, const int *tgt_var,
+    const int64_t *const *rowptr, const int32_t *const *cols,
+    const uint8_t *const *delays, const double *weight,
+    const int32_t *ring_depth, int64_t nsteps, void *stream,
+    int64_t *spikes_out);
+/* Size in bytes of the allocation-free entry point's scratch array. */
+BG_API int bg_noalloc_scratch_bytes(int64_t *bytes);
 /* steps run, kernel launches issued, device milliseconds of the last run. */
 BG_API int bg_net_stats(bg_net *net, int64_t *steps, int64_t *launches,
                  double *last_run_ms);
