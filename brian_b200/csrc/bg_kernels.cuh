@@ -27,6 +27,7 @@ constexpr int kMaxRec = 4;
 template <typename T> struct Deliv {
     T *ring; int64_t tn, to; int md; int var;
     uint16_t *cring; int64_t tnp; const T *table;
+    int tablen;    // valid table entries (largest count + 1); 0 when unknown
 };
 
 // Count-ring helpers: entry col of a row is the low/high half of a 32-bit word.
@@ -74,6 +75,7 @@ template <typename T> struct HeadArgs {
     T *S; int64_t n, npad; int nvar;
     int linear, useC;
     T A[kMaxVars * kMaxVars]; T C[kMaxVars];
+    uint64_t anz; uint32_t cnz;    // nonzero masks of A and C
     int thr_kind, thr_var, thr_var2; T thr_val; double dt;
     uint64_t seed; int rate_var;
     const int64_t *gen_steps; const int32_t *gen_idx; int64_t gen_n;
@@ -87,6 +89,33 @@ template <typename T> struct HeadArgs {
     unsigned long long *spikes;    // running spike count of the group
     int tail, update, last;
 };
+
+// Row j of the exact linear update: ((0 + A[j][k0] s_k0) + A[j][k1] s_k1) +
+// ... over the nonzero coefficients (bit j*NV+k of anz), left to right, then
+// + C[j] when nonzero (bit j of cnz).  Exact zeros are skipped: only the sign
+// of an exact-zero result can differ from summing them (SURVEY note N1), and
+// the CPU restatement uses the same rule.  The masks are kernel parameters,
+// so every test is uniform across the grid.
+template <typename T, int NV>
+__device__ __forceinline__ T linear_row(const T *A, const T *C, uint64_t anz, uint32_t cnz, const T (&s)[NV], int j) {
+    T acc = T(0);
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+        if (anz & (1ull << (j * NV + k))) acc = rn<T>::add(acc, rn<T>::mul(A[j * NV + k], s[k]));
+    if (cnz & (1u << j)) acc = rn<T>::add(acc, C[j]);
+    return acc;
+}
+
+// Host side: nonzero masks of the coefficients a kernel argument block holds.
+template <typename Args>
+inline void set_linear_masks(Args &a, int nvar) {
+    a.anz = 0; a.cnz = 0;
+    for (int j = 0; j < nvar; ++j) {
+        for (int k = 0; k < nvar; ++k)
+            if (a.A[j * nvar + k] != 0) a.anz |= 1ull << (j * nvar + k);
+        if (a.useC && a.C[j] != 0) a.cnz |= 1u << j;
+    }
+}
 
 // Block-aggregated counter update (one global atomic per block).
 __device__ __forceinline__ void block_count(unsigned long long *g, unsigned long long v) {
@@ -281,13 +310,7 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_head(const HeadArgs<T> a) {
             if (a.linear) {
                 T x[NV];
 #pragma unroll
-                for (int j = 0; j < NV; ++j) {
-                    T acc = rn<T>::mul(a.A[j * NV + 0], s[u][0]);
-#pragma unroll
-                    for (int k = 1; k < NV; ++k) acc = rn<T>::add(acc, rn<T>::mul(a.A[j * NV + k], s[u][k]));
-                    if (a.useC) acc = rn<T>::add(acc, a.C[j]);
-                    x[j] = acc;
-                }
+                for (int j = 0; j < NV; ++j) x[j] = linear_row<T, NV>(a.A, a.C, a.anz, a.cnz, s[u], j);
 #pragma unroll
                 for (int j = 0; j < NV; ++j) s[u][j] = x[j];
             }

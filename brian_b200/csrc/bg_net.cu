@@ -52,7 +52,7 @@ struct HConn {
     std::vector<int64_t> rowptr; std::vector<int32_t> cols; std::vector<char> w; int w_bits = 64;
     int32_t delay = 0; bool hetero = false; std::vector<uint8_t> d; int md = 0; int mod_var = -1;
     bool homogeneous = false; int parts = 1; int stdp = -1; bool fused_push = false;
-    uint16_t *dCRing = nullptr; int64_t tnp = 0; void *dTable = nullptr;   // count ring (shared weight)
+    uint16_t *dCRing = nullptr; int64_t tnp = 0; void *dTable = nullptr; int tablen = 0;   // count ring (shared weight)
     int64_t *dRow = nullptr; int32_t *dCols = nullptr; void *dW = nullptr; uint8_t *dD = nullptr; void *dRing = nullptr;
     int64_t *dColptr = nullptr, *dColk = nullptr; int32_t *dColsrc = nullptr;
     int64_t wcount() const { return dense ? sn * tn : nnz; }
@@ -148,6 +148,7 @@ int build_group(bg_net *net, int gid) {
         for (int k = 0; k < g.nvar; ++k) a.A[j * g.nvar + k] = (T)g.A[j * g.nvar + k];
         a.C[j] = g.useC ? (T)g.C[j] : T(0);
     }
+    bg::set_linear_masks(a, g.nvar);
     a.thr_kind = g.thr_kind; a.thr_var = g.thr_var; a.thr_var2 = g.thr_var2; a.thr_val = (T)g.thr_val;
     a.dt = net->dt; a.seed = g.seed; a.rate_var = g.rate_var;
     a.gen_steps = g.dGenSteps; a.gen_idx = g.dGenIdx; a.gen_n = (int64_t)g.gen_steps.size();
@@ -160,7 +161,7 @@ int build_group(bg_net *net, int gid) {
     for (int k = 0; k < a.ndeliv; ++k) {
         const HConn &c = net->conns[g.delivs[k]];
         a.deliv[k].ring = (T *)c.dRing; a.deliv[k].tn = c.tn; a.deliv[k].to = c.to; a.deliv[k].md = c.md; a.deliv[k].var = c.var;
-        a.deliv[k].cring = c.dCRing; a.deliv[k].tnp = c.tnp; a.deliv[k].table = (const T *)c.dTable;
+        a.deliv[k].cring = c.dCRing; a.deliv[k].tnp = c.tnp; a.deliv[k].table = (const T *)c.dTable; a.deliv[k].tablen = c.tablen;
     }
     a.npush = 0;
     for (size_t ci = 0; ci < net->conns.size(); ++ci) {
@@ -490,6 +491,7 @@ int build_persist(bg_net *net) {
         for (int k = 0; k < g.nvar; ++k) a.A[j * g.nvar + k] = (T)g.A[j * g.nvar + k];
         a.C[j] = g.useC ? (T)g.C[j] : T(0);
     }
+    bg::set_linear_masks(a, g.nvar);
     a.thr_kind = g.thr_kind; a.thr_var = g.thr_var; a.thr_var2 = g.thr_var2; a.thr_val = (T)g.thr_val;
     a.reset_kind = g.reset_kind; a.reset_var = g.reset_var; a.reset_var2 = g.reset_var2; a.reset_val = (T)g.reset_val;
     a.hist = g.dHist; a.depth = g.depth; a.nwords = g.npad / 32;
@@ -497,7 +499,7 @@ int build_persist(bg_net *net) {
     for (int k = 0; k < a.ndeliv; ++k) {
         const HConn &c = net->conns[g.delivs[k]];
         a.deliv[k].ring = (T *)c.dRing; a.deliv[k].tn = c.tn; a.deliv[k].to = c.to; a.deliv[k].md = c.md; a.deliv[k].var = c.var;
-        a.deliv[k].cring = c.dCRing; a.deliv[k].tnp = c.tnp; a.deliv[k].table = (const T *)c.dTable;
+        a.deliv[k].cring = c.dCRing; a.deliv[k].tnp = c.tnp; a.deliv[k].table = (const T *)c.dTable; a.deliv[k].tablen = c.tablen;
     }
     a.npush = (int)net->conns.size();
     for (int p = 0; p < a.npush; ++p) {
@@ -914,6 +916,7 @@ int bg_net_prepare(bg_net *n) {
                 for (int32_t j : c.cols) kmax = std::max<int64_t>(kmax, ++indeg[j]);
             }
             if (kmax > 0 && kmax < 65535) {
+                c.tablen = (int)kmax + 1;
                 c.tnp = (c.tn + 1) & ~1ll;
                 if (n->alloc(&c.dCRing, (size_t)c.md * c.tnp * 2) != cudaSuccess) return fail(BG_ENOMEM, "count ring");
                 if (n->alloc(&c.dTable, (size_t)(kmax + 1) * ts) != cudaSuccess) return fail(BG_ENOMEM, "count table");

@@ -176,6 +176,7 @@ BG_API int bg_delay_group_run_noalloc(int64_t n, int nvar, double *S, const doub
         for (int k = 0; k < nvar; ++k) a.A[j * nvar + k] = A[j * nvar + k];
         a.C[j] = C ? C[j] : 0.0;
     }
+    bg::set_linear_masks(a, nvar);
     a.thr_kind = BG_THR_CONST; a.thr_var = thr_var; a.thr_val = thr_val;
     a.reset_kind = BG_RESET_CONST; a.reset_var = reset_var; a.reset_val = reset_val;
     a.hist = (uint32_t *)(scr + o_hist); a.depth = 1; a.nwords = nwords;

@@ -20,11 +20,13 @@
 namespace bg {
 
 constexpr int kPersistMaxPush = 2;
+constexpr int kPersistTable = 2048;     // shared-memory entries for count tables
 
 template <typename T> struct PersistArgs {
     DevCtl *ctl;
     T *S; int64_t n, npad;
     T A[kMaxVars * kMaxVars]; T C[kMaxVars]; int useC;
+    uint64_t anz; uint32_t cnz;    // nonzero masks of A and C
     int thr_kind, thr_var, thr_var2; T thr_val;
     int reset_kind, reset_var, reset_var2; T reset_val;
     uint32_t *hist; int depth; int64_t nwords;
@@ -40,6 +42,10 @@ __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int *p) {
     unsigned int v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
+}
+
+__device__ __forceinline__ void red_release_add(unsigned int *p, unsigned int v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
 }
 
 // Block-uniform variable access without runtime-indexed register arrays:
@@ -91,6 +97,31 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T
 #pragma unroll
     for (int d = 0; d < kMaxDeliv; ++d)
         dfull[d] = d < a.ndeliv && a.deliv[d].to <= base && (int64_t)base + kBlockNeurons <= a.deliv[d].to + a.deliv[d].tn;
+    // count tables staged in shared memory when they fit (uniform decision)
+    __shared__ T stab[kPersistTable];
+    int toff[kMaxDeliv];
+    bool staged = true;
+    {
+        int o = 0;
+#pragma unroll
+        for (int d = 0; d < kMaxDeliv; ++d) {
+            toff[d] = o;
+            if (d < a.ndeliv && a.deliv[d].cring) {
+                if (a.deliv[d].tablen <= 0) staged = false;
+                o += a.deliv[d].tablen;
+            }
+        }
+        if (o > kPersistTable) staged = false;
+        if (staged)
+            for (int d = 0; d < a.ndeliv; ++d)
+                if (a.deliv[d].cring)
+                    for (int k = tid; k < a.deliv[d].tablen; k += kHeadThreads) stab[toff[d] + k] = a.deliv[d].table[k];
+    }
+    // pushes whose source range meets this block (uniform)
+    bool pact[kPersistMaxPush];
+#pragma unroll
+    for (int p = 0; p < kPersistMaxPush; ++p)
+        pact[p] = p < a.npush && a.push[p].so < (int64_t)base + kBlockNeurons && a.push[p].so + a.push[p].sn > base;
     T s[kNPT][NV];
 #pragma unroll
     for (int u = 0; u < kNPT; ++u) {
@@ -123,25 +154,41 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T
                 if (abort_flag) break;
             }
             const int ps = (int)(t - 1);
-            for (int d = 0; d < a.ndeliv; ++d) {
-                const Deliv<T> &dv = a.deliv[d];
-                const int r = ps % dv.md;
-                if (dv.cring) {
-                    uint16_t *row = dv.cring + (int64_t)r * dv.tnp + (base - dv.to);
-                    uint16_t c[kNPT];
+            // issue every count-ring load of every delivery first: one L2
+            // latency for all of them
+            uint16_t cnt[kMaxDeliv][kNPT];
+            uint16_t *crow[kMaxDeliv];
+#pragma unroll
+            for (int d = 0; d < kMaxDeliv; ++d) {
+                crow[d] = nullptr;
+#pragma unroll
+                for (int u = 0; u < kNPT; ++u) cnt[d][u] = 0;
+                if (d < a.ndeliv && a.deliv[d].cring) {
+                    const Deliv<T> &dv = a.deliv[d];
+                    crow[d] = dv.cring + (int64_t)(ps % dv.md) * dv.tnp + (base - dv.to);
 #pragma unroll
                     for (int u = 0; u < kNPT; ++u) {
                         const int li = u * kHeadThreads + tid;
                         const int64_t gi = (int64_t)base + li;
-                        c[u] = (li < nvalid && (dfull[d] || (gi >= dv.to && gi < dv.to + dv.tn))) ? __ldcg(row + li) : 0;
+                        if (li < nvalid && (dfull[d] || (gi >= dv.to && gi < dv.to + dv.tn))) cnt[d][u] = __ldcg(crow[d] + li);
                     }
+                }
+            }
+            // then add in connection order (the reference's delivery order)
+#pragma unroll
+            for (int d = 0; d < kMaxDeliv; ++d) {
+                if (d >= a.ndeliv) break;
+                const Deliv<T> &dv = a.deliv[d];
+                if (dv.cring) {
 #pragma unroll
                     for (int u = 0; u < kNPT; ++u) {
-                        if (c[u]) row[u * kHeadThreads + tid] = 0;
-                        const T v = c[u] ? __ldg(dv.table + c[u]) : T(0);
+                        const int c = cnt[d][u];
+                        if (c) crow[d][u * kHeadThreads + tid] = 0;
+                        const T v = c ? (staged ? stab[toff[d] + c] : __ldg(dv.table + c)) : T(0);
                         uset<T, NV>(s[u], dv.var, rn<T>::add(uget<T, NV>(s[u], dv.var), v));
                     }
                 } else {
+                    const int r = ps % dv.md;
                     T *row = dv.ring + (int64_t)r * dv.tn + (base - dv.to);
 #pragma unroll
                     for (int u = 0; u < kNPT; ++u) {
@@ -171,13 +218,7 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T
             const int li = u * kHeadThreads + tid;
             T x[NV];
 #pragma unroll
-            for (int j = 0; j < NV; ++j) {
-                T acc = rn<T>::mul(a.A[j * NV + 0], s[u][0]);
-#pragma unroll
-                for (int k = 1; k < NV; ++k) acc = rn<T>::add(acc, rn<T>::mul(a.A[j * NV + k], s[u][k]));
-                if (a.useC) acc = rn<T>::add(acc, a.C[j]);
-                x[j] = acc;
-            }
+            for (int j = 0; j < NV; ++j) x[j] = linear_row<T, NV>(a.A, a.C, a.anz, a.cnz, s[u], j);
 #pragma unroll
             for (int j = 0; j < NV; ++j) s[u][j] = x[j];
             bool spk = false;
@@ -187,16 +228,18 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T
             }
             prev_spk |= (spk ? 1u : 0u) << u;
             const uint32_t ball = __ballot_sync(0xffffffffu, spk);
+            // (no history words: nothing reads them on this path)
             if (lane == 0) {
-                a.hist[(int64_t)hslot * a.nwords + ((base + u * kHeadThreads) >> 5) + warp] = ball;
                 words[u * (kHeadThreads / 32) + warp] = ball;
                 my_spikes += __popc(ball);
             }
         }
-        __syncthreads();
+        (void)hslot;
+        // the barrier also tells every thread whether the block spiked
+        const int any_spike = __syncthreads_or(prev_spk != 0);
         // ---- push this block's spikes: one flattened scatter over every
         // (connection, spike) pair of the block
-        if (a.npush) {
+        if (a.npush && any_spike) {
             if (tid < 32) {
                 uint32_t w = words[lane];
                 const int c = __popc(w);
@@ -210,6 +253,7 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T
             __syncthreads();
             const int n = nsp;
             for (int p = 0; p < a.npush && n > 0; ++p) {
+                if (!pact[p]) continue;              // block-uniform
                 const Push<T> &q = a.push[p];
                 const int cur = (int)t % q.md;
                 for (int b0 = 0; b0 < n; b0 += kPushBatch) {
@@ -238,9 +282,11 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T
                 }
             }
         }
-        // ---- arrive: this block's pushes of step t are performed
+        // ---- arrive: this block's pushes and ring clears of step t are
+        // ordered before the arrival (release reduction, cumulative over the
+        // block's writes through the barrier)
         __syncthreads();
-        if (tid == 0) { __threadfence(); atomicAdd(a.arrived + (st & 3), 1u); }
+        if (tid == 0) red_release_add(a.arrived + (st & 3), 1u);
     }
 #pragma unroll
     for (int u = 0; u < kNPT; ++u) {

@@ -398,10 +398,17 @@ static void step(or_net *n, int64_t cs) {
             std::vector<double> x(m), s(m);
             for (int64_t i = 0; i < N; ++i) {
                 for (int k = 0; k < m; ++k) s[k] = g.S[(size_t)k * N + i];
+                /* x_j = ((0 + A[j][k0] s_k0) + A[j][k1] s_k1) + ... over the
+                 * nonzero A[j][k] left to right, then + C[j] when nonzero.
+                 * Skipping exact zeros of A and C (SURVEY note N1) and starting
+                 * from +0 change nothing but the sign of an exact-zero result. */
                 for (int j = 0; j < m; ++j) {
-                    double acc = g.A[j * m + 0] * s[0];
-                    for (int k = 1; k < m; ++k) acc = acc + g.A[j * m + k] * s[k];
-                    if (g.useC) acc = acc + g.C[j];
+                    double acc = 0.0;
+                    for (int k = 0; k < m; ++k) {
+                        if (g.A[j * m + k] == 0.0) continue;
+                        acc = acc + g.A[j * m + k] * s[k];
+                    }
+                    if (g.useC && g.C[j] != 0.0) acc = acc + g.C[j];
                     x[j] = acc;
                 }
                 for (int k = 0; k < m; ++k) g.S[(size_t)k * N + i] = x[k];
