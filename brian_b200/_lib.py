@@ -59,6 +59,28 @@ ENGINE_ONLY = {
     "net_item_name": [_vp, _i64, ct.c_char_p, _i64],
     "fixed_indegree_csr": [_i64, _i64, _i64, _u64, _vp, _vp],
     "net_set_persistent": [_vp, ct.c_int],
+    "fit_compile_check": [ct.c_int, ct.c_char_p, ct.c_char_p, ct.c_char_p, ct.c_char_p, _dbl, ct.c_int, ct.c_int,
+                          ct.c_char_p, _i64],
+    "fit_create": [_P(_vp), ct.c_int, ct.c_int, ct.c_char_p, ct.c_char_p, ct.c_char_p, ct.c_char_p, _dbl,
+                   ct.c_int, ct.c_int],
+    "fit_destroy": [_vp],
+    "fit_set_input": [_vp, _vp, _i64],
+    "fit_set_targets": [_vp, _vp, _i64],
+    "fit_set_sims": [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32],
+    "fit_set_record": [_vp, _i32],
+    "fit_reinit": [_vp],
+    "fit_run": [_vp, _i32, _i32],
+    "fit_read": [_vp, _vp, _vp, _vp],
+    "fit_read_spikes": [_vp, _vp, _vp],
+    "fit_set_gamma": [_vp, _i64, _i32, _vp, _vp, _dbl],
+    "fit_set_params": [_vp, _i32, _vp],
+    "fit_evaluate": [_vp, _vp, _vp],
+    "fit_pso_init": [_vp, _i32, _vp, _vp, _vp, _dbl, _dbl, _dbl, _u64],
+    "fit_pso_evaluate_initial": [_vp],
+    "fit_pso_run": [_vp, _i32, _vp, _vp],
+    "fit_pso_best": [_vp, _vp, _vp],
+    "fit_pso_state": [_vp, _vp, _vp, _vp, _vp],
+    "fit_stats": [_vp, _vp, ct.c_int],
 }
 
 
@@ -299,3 +321,144 @@ def fixed_indegree_csr_native(n_src, n_tgt, k, seed):
     t.check(t.fixed_indegree_csr(n_src, n_tgt, k, int(seed) & ((1 << 64) - 1), _ptr(rowptr), _ptr(cols)),
             "fixed_indegree_csr")
     return rowptr, cols
+
+
+class FitHandle(object):
+    """One batched-fitting handle (bg_fit_* in include/brian_b200.h)."""
+
+    def __init__(self, code, dt, delta_steps, exclusive=True, precision=64, device=0, table=None):
+        self.t = table if table is not None else product_table()
+        self.h = ct.c_void_p()
+        self.code = code
+        self.nstate = len(code.state)
+        self.precision = precision
+        self.t.check(self.t.fit_create(ct.byref(self.h), int(device), int(precision), ",".join(code.state).encode(),
+                                       code.update.encode(), code.threshold.encode(), code.reset.encode(),
+                                       float(dt), int(delta_steps), 1 if exclusive else 0), "fit_create")
+        self.ns = 0
+        self.rec_cap = 0
+
+    def close(self):
+        if self.h:
+            self.t.fit_destroy(self.h)
+            self.h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _c(self, st, what):
+        self.t.check(st, what)
+
+    def set_input(self, I):
+        I = np.ascontiguousarray(I, dtype=np.float64)
+        self._c(self.t.fit_set_input(self.h, _ptr(I), len(I)), "fit_set_input")
+
+    def set_targets(self, spiketimes_steps):
+        s = np.ascontiguousarray(spiketimes_steps, dtype=np.int32)
+        self._c(self.t.fit_set_targets(self.h, _ptr(s), len(s)), "fit_set_targets")
+
+    def set_sims(self, S0, I_offset, nsteps, spk_offset, spk_end, delay=None, refractory=None, onset=0):
+        S0 = np.ascontiguousarray(S0, dtype=np.float64)
+        ns = S0.shape[1]
+        a = [np.ascontiguousarray(I_offset, dtype=np.int64), np.ascontiguousarray(nsteps, dtype=np.int32),
+             np.ascontiguousarray(spk_offset, dtype=np.int64), np.ascontiguousarray(spk_end, dtype=np.int64)]
+        d = None if delay is None else np.ascontiguousarray(delay, dtype=np.int32)
+        r = None if refractory is None else np.ascontiguousarray(refractory, dtype=np.int32)
+        for x in a + [d, r]:
+            if x is not None and len(x) != ns:
+                raise ValueError("per-simulation arrays must have %d entries" % ns)
+        self._c(self.t.fit_set_sims(self.h, ns, _ptr(S0), _ptr(a[0]), _ptr(a[1]), _ptr(a[2]), _ptr(a[3]), _ptr(d),
+                                    _ptr(r), int(onset)), "fit_set_sims")
+        self.ns = ns
+
+    def set_record(self, cap):
+        self._c(self.t.fit_set_record(self.h, int(cap)), "fit_set_record")
+        self.rec_cap = int(cap)
+
+    def reinit(self):
+        self._c(self.t.fit_reinit(self.h), "fit_reinit")
+
+    def run(self, Tstart, Tend):
+        self._c(self.t.fit_run(self.h, int(Tstart), int(Tend)), "fit_run")
+
+    def read(self, state=False):
+        c = np.empty(self.ns, dtype=np.int32)
+        n = np.empty(self.ns, dtype=np.int32)
+        S = np.empty((self.nstate, self.ns)) if state else None
+        self._c(self.t.fit_read(self.h, _ptr(c), _ptr(n), _ptr(S)), "fit_read")
+        return (c, n, S) if state else (c, n)
+
+    def read_spikes(self):
+        counts = np.empty(self.ns, dtype=np.int32)
+        steps = np.empty((self.ns, max(1, self.rec_cap)), dtype=np.int32)
+        self._c(self.t.fit_read_spikes(self.h, _ptr(counts), _ptr(steps)), "fit_read_spikes")
+        return counts, steps
+
+    def set_gamma(self, nparticles, slices, target_length, target_rate, delta):
+        tl = np.ascontiguousarray(target_length, dtype=np.int32)
+        tr = np.ascontiguousarray(target_rate, dtype=np.float64)
+        self._c(self.t.fit_set_gamma(self.h, int(nparticles), int(slices), _ptr(tl), _ptr(tr), float(delta)),
+                "fit_set_gamma")
+        self.npart = int(nparticles)
+
+    def set_params(self, dim_var):
+        dv = np.ascontiguousarray(dim_var, dtype=np.int32)
+        self._c(self.t.fit_set_params(self.h, len(dv), _ptr(dv)), "fit_set_params")
+        self.ndim = len(dv)
+
+    def evaluate(self, X):
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        out = np.empty(self.npart)
+        self._c(self.t.fit_evaluate(self.h, _ptr(X), _ptr(out)), "fit_evaluate")
+        return out
+
+    def pso_init(self, group_size, X0, xmin, xmax, omega, c1, c2, seed):
+        X0 = np.ascontiguousarray(X0, dtype=np.float64)
+        lo = np.ascontiguousarray(xmin, dtype=np.float64)
+        hi = np.ascontiguousarray(xmax, dtype=np.float64)
+        self._c(self.t.fit_pso_init(self.h, int(group_size), _ptr(X0), _ptr(lo), _ptr(hi), float(omega), float(c1),
+                                    float(c2), int(seed) & ((1 << 64) - 1)), "fit_pso_init")
+        self.ngroups = self.npart // int(group_size)
+
+    def pso_evaluate_initial(self):
+        self._c(self.t.fit_pso_evaluate_initial(self.h), "fit_pso_evaluate_initial")
+
+    def pso_run(self, iterations, trace=True, timing=True):
+        tr = np.empty((iterations, self.ngroups)) if trace else None
+        ms = np.empty(iterations, dtype=np.float32) if timing else None
+        self._c(self.t.fit_pso_run(self.h, int(iterations), _ptr(tr), _ptr(ms)), "fit_pso_run")
+        return tr, ms
+
+    def pso_best(self):
+        X = np.empty((self.ndim, self.ngroups))
+        f = np.empty(self.ngroups)
+        self._c(self.t.fit_pso_best(self.h, _ptr(X), _ptr(f)), "fit_pso_best")
+        return X, f
+
+    def pso_state(self):
+        X = np.empty((self.ndim, self.npart))
+        V = np.empty_like(X)
+        Xl = np.empty_like(X)
+        fl = np.empty(self.npart)
+        self._c(self.t.fit_pso_state(self.h, _ptr(X), _ptr(V), _ptr(Xl), _ptr(fl)), "fit_pso_state")
+        return X, V, Xl, fl
+
+    def stats(self):
+        out = np.zeros(4)
+        self._c(self.t.fit_stats(self.h, _ptr(out), 4), "fit_stats")
+        return {"last_sim_ms": out[0], "sim_launches": int(out[1]), "neuron_steps": int(out[2]),
+                "max_steps": int(out[3])}
+
+
+def fit_compile_check(code, dt, delta_steps, exclusive=True, precision=64):
+    """Compile a model's fitting kernel with NVRTC without a device; returns
+    the compiler log, raises EngineError on failure."""
+    t = product_table()
+    log = ct.create_string_buffer(1 << 16)
+    t.check(t.fit_compile_check(int(precision), ",".join(code.state).encode(), code.update.encode(),
+                                code.threshold.encode(), code.reset.encode(), float(dt), int(delta_steps),
+                                1 if exclusive else 0, log, 1 << 16), "fit_compile_check")
+    return log.value.decode(errors="replace")

@@ -242,13 +242,20 @@ class NeuronGroup(_GroupBase):
                 self._S[k, :] = v
         self._S_init = self._S.copy()
         self._linear = None
+        # A group the network engine cannot run (numerically integrated or
+        # nonlinear model, general string threshold/reset) can still be built:
+        # GPUModelFitting takes its model.  Lowering it onto a network raises.
+        self._fitting_only = None
+        self._level = level
         if self.eqs is not None:
-            if method not in (None, "linear"):
-                raise NotImplementedError("integration method %r: only exact linear models run on the "
-                                          "network engine; use modelfitting for Euler models" % method)
-            if not self.eqs.is_linear():
-                raise NotImplementedError("nonlinear equations are not supported on the network engine "
-                                          "(only linear models with the exact propagator)")
+            if method not in (None, "linear", "Euler", "RK", "exponential_Euler"):
+                raise NotImplementedError("integration method %r is not supported" % method)
+            if method in ("Euler", "RK", "exponential_Euler"):
+                self._fitting_only = ("integration method %r runs in modelfitting only; the network engine "
+                                      "integrates linear models exactly" % method)
+            elif not self.eqs.is_linear():
+                self._fitting_only = ("nonlinear equations run in modelfitting only; the network engine "
+                                      "integrates linear models with the exact propagator")
         # ---- threshold
         self._threshold = self._select_threshold(threshold, level + 1)
         # ---- reset / refractoriness (neurongroup.py:369-429)
@@ -262,7 +269,7 @@ class NeuronGroup(_GroupBase):
         self._use_refractory_filter = not (float(refractory) < 0.9 * dt)
         if isinstance(self._reset, Refractoriness):
             self._period = int(self._reset.period / dt) + 1
-        elif float(refractory) > 0.9 * dt and type(self._reset) in (Reset, StringReset):
+        elif float(refractory) > 0.9 * dt and type(self._reset) is Reset:
             # a constant reset with a refractory period becomes Refractoriness
             self._reset = Refractoriness(self._reset.resetvalue, float(refractory), self._reset.state)
             self._period = int(float(refractory) / dt) + 1
@@ -292,15 +299,15 @@ class NeuronGroup(_GroupBase):
             return Threshold(float(threshold), state=0)
         if isinstance(threshold, str):
             m = re.match(r"^\s*(\w+)\s*>\s*(.+?)\s*$", threshold)
-            if not m or m.group(1) not in self.var_index:
-                raise NotImplementedError("threshold string %r: only 'x > c' and 'x > y' are supported"
-                                          % threshold)
-            rhs = m.group(2)
+            rhs = m.group(2) if m else ""
+            if not m or m.group(1) not in self.var_index or (
+                    rhs not in self.var_index and _identifiers(rhs) & (set(self._names) | {"t"})):
+                self._fitting_only = self._fitting_only or (
+                    "threshold string %r runs in modelfitting only; the network engine supports 'x > c' "
+                    "and 'x > y'" % threshold)
+                return StringThreshold(threshold, namespace=self._ns(level + 1))
             if rhs in self.var_index:
                 return VariableThreshold(rhs, m.group(1))
-            ids = _identifiers(rhs)
-            if ids & set(self._names):
-                raise NotImplementedError("threshold string %r depends on state variables" % threshold)
             ns = self._ns(level + 1)
             return Threshold(float(eval(rhs, ns)), m.group(1))
         if isinstance(threshold, Threshold):
@@ -314,16 +321,16 @@ class NeuronGroup(_GroupBase):
             return Reset(float(reset), state=0)
         if isinstance(reset, str):
             stmts = [s.strip() for s in re.split(r"[;\n]", reset) if s.strip()]
-            if len(stmts) != 1:
-                raise NotImplementedError("multi-statement string resets run in modelfitting only")
-            m = re.match(r"^(\w+)\s*=\s*(.+)$", stmts[0])
-            if not m or m.group(1) not in self.var_index:
-                raise NotImplementedError("reset string %r: only 'x = c' and 'x = y'" % reset)
-            rhs = m.group(2).strip()
+            m = re.match(r"^(\w+)\s*=\s*(.+)$", stmts[0]) if len(stmts) == 1 else None
+            rhs = m.group(2).strip() if m else ""
+            if not m or m.group(1) not in self.var_index or (
+                    rhs not in self.var_index and _identifiers(rhs) & (set(self._names) | {"t"})):
+                self._fitting_only = self._fitting_only or (
+                    "reset string %r runs in modelfitting only; the network engine supports 'x = c' and "
+                    "'x = y'" % reset)
+                return StringReset(reset, namespace=self._ns(level + 1))
             if rhs in self.var_index:
                 return VariableReset(rhs, m.group(1))
-            if _identifiers(rhs) & set(self._names):
-                raise NotImplementedError("reset string %r depends on state variables" % reset)
             return Reset(float(eval(rhs, self._ns(level + 1))), m.group(1))
         if isinstance(reset, Reset):
             return reset
@@ -358,6 +365,8 @@ class NeuronGroup(_GroupBase):
     # --------------------------------------------------------------- lowering
     def _lower(self, rt, dt):
         """Register this group on a runtime; returns the group id."""
+        if self._fitting_only:
+            raise NotImplementedError(self._fitting_only)
         S0 = self._S_host if self._names else np.zeros((0, self._n))
         gid = rt.group_add(S0)
         if self.eqs is not None and self._names:

@@ -249,6 +249,99 @@ BG_API int bg_noalloc_scratch_bytes(int64_t *bytes);
 BG_API int bg_net_stats(bg_net *net, int64_t *steps, int64_t *launches,
                  double *last_run_ms);
 
+/* ---- batched model fitting ------------------------------------------------
+ * Replaces GPUModelFitting (library/modelfitting/gpu_modelfitting.py:
+ * 202-401) and the fitness loop of ModelFitting (modelfitting.py:26-227).
+ * A handle holds ns independent simulations (particles x targets x slices)
+ * of one generated model; each has its own input row, length, target train,
+ * spike delay and refractory period.  The kernel follows the reference's
+ * runsim template (gpu_modelfitting.py:39-156).
+ *
+ * The model is given as C code over the state registers s_<name>, the input
+ * I_in and the time t: `update_code` (statements of one step),
+ * `threshold_code` (a bool expression) and `reset_code` (statements).
+ * state_names lists the state rows in storage order, comma-separated.
+ * precision 32 or 64 selects the scalar type; delta_steps =
+ * rint(delta/dt); exclusive = 1 for the 'exclusive' coincidence algorithm,
+ * 0 for 'inclusive'.  The kernel is compiled by NVRTC for sm_100a;
+ * BG_ECOMPILE carries the compiler log in bg_last_error. */
+/* Compile only (no device needed); the log is copied to `log`. */
+BG_API int bg_fit_compile_check(int precision, const char *state_names,
+                                const char *update_code, const char *threshold_code,
+                                const char *reset_code, double dt, int delta_steps,
+                                int exclusive, char *log, int64_t log_len);
+/* GPUModelFitting.__init__ (gpu_modelfitting.py:266-331). */
+BG_API int bg_fit_create(bg_fit **out, int device, int precision,
+                         const char *state_names, const char *update_code,
+                         const char *threshold_code, const char *reset_code,
+                         double dt, int delta_steps, int exclusive);
+BG_API int bg_fit_destroy(bg_fit *h);
+/* I (the reference's I_arr): all input traces concatenated; converted to
+ * the scalar type on upload (gpu_modelfitting.py:353). */
+BG_API int bg_fit_set_input(bg_fit *h, const double *I, int64_t n);
+/* All target trains concatenated, in steps (rint(t/dt)), each framed by a
+ * leading sentinel before 0 and a trailing one after its simulation ends
+ * (gpu_modelfitting.py:255-263, 356). */
+BG_API int bg_fit_set_targets(bg_fit *h, const int32_t *spiketimes, int64_t n);
+/* reinit_vars (gpu_modelfitting.py:333-379): S0 is the initial state
+ * [nstate][nsims]; simulation i reads input[I_offset[i] + T] for
+ * T < nsteps[i] and its train spiketimes[spk_offset[i] .. spk_end[i]);
+ * delay/refractory in steps (NULL = 0); spikes before step `onset` are not
+ * counted.  Resets every simulation to S0. */
+BG_API int bg_fit_set_sims(bg_fit *h, int64_t nsims, const double *S0,
+                           const int64_t *I_offset, const int32_t *nsteps,
+                           const int64_t *spk_offset, const int64_t *spk_end,
+                           const int32_t *delay, const int32_t *refractory,
+                           int32_t onset);
+/* Record the first `cap` spike steps of every simulation (0 = off). */
+BG_API int bg_fit_set_record(bg_fit *h, int32_t cap);
+/* State back to S0, counters and train pointers to the start. */
+BG_API int bg_fit_reinit(bg_fit *h);
+/* launch (gpu_modelfitting.py:381-393): steps [Tstart, min(Tend, nsteps[i]))
+ * of every simulation, continuing from the current state. */
+BG_API int bg_fit_run(bg_fit *h, int32_t Tstart, int32_t Tend);
+/* coincidence_count / spike_count (gpu_modelfitting.py:395-401) and,
+ * optionally, the state [nstate][nsims] as doubles.  NULL skips an output. */
+BG_API int bg_fit_read(bg_fit *h, int32_t *coinc, int32_t *nspikes, double *state);
+/* Recorded spikes: counts[nsims] (may exceed cap), steps[nsims][cap]. */
+BG_API int bg_fit_read_spikes(bg_fit *h, int32_t *counts, int32_t *steps);
+/* Gamma factor inputs (ModelFitting.prepare_data, modelfitting.py:117-173):
+ * nparticles x slices = nsims (simulation i is particle i % nparticles),
+ * per particle the target train's length and rate (firing_rate), delta in
+ * seconds. */
+BG_API int bg_fit_set_gamma(bg_fit *h, int64_t nparticles, int32_t slices,
+                            const int32_t *target_length, const double *target_rate,
+                            double delta);
+/* Fitted parameter d writes state row dim_var[d]; -1 = spike delay,
+ * -2 = refractory period (both rint(x/dt) steps). */
+BG_API int bg_fit_set_params(bg_fit *h, int32_t ndim, const int32_t *dim_var);
+/* ModelFitting.evaluate (modelfitting.py:175-227): X is [ndim][nparticles];
+ * resets, simulates every particle over its full length and writes the
+ * gamma factor (FP64, get_gamma_factor, statistics.py:236-240). */
+BG_API int bg_fit_evaluate(bg_fit *h, const double *X, double *gamma_out);
+/* Grouped particle swarm on the device (particle_swarm.py:6-111): groups of
+ * group_size consecutive particles optimise independently (one target
+ * each); X0 [ndim][nparticles] is clipped into [xmin, xmax]. */
+BG_API int bg_fit_pso_init(bg_fit *h, int32_t group_size, const double *X0,
+                           const double *xmin, const double *xmax, double omega,
+                           double c1, double c2, uint64_t seed);
+/* Evaluate the current positions and fold them into the local and group
+ * bests without moving (the initial swarm's scores; the reference's loop
+ * moves before its first evaluation, particle_swarm.py:65-84). */
+BG_API int bg_fit_pso_evaluate_initial(bg_fit *h);
+/* `iterations` swarm iterations (move, evaluate, best updates) queued
+ * without host synchronisation; trace [iterations][ngroups] receives the
+ * group best fitness after each, iter_ms the GPU time of each (NULL = off). */
+BG_API int bg_fit_pso_run(bg_fit *h, int32_t iterations, double *trace, float *iter_ms);
+/* Group bests: X_gbest [ndim][ngroups], fit_gbest [ngroups]. */
+BG_API int bg_fit_pso_best(bg_fit *h, double *X_gbest, double *fit_gbest);
+/* Swarm state: X, V, X_lbest [ndim][nparticles], fit_lbest [nparticles]. */
+BG_API int bg_fit_pso_state(bg_fit *h, double *X, double *V, double *X_lbest,
+                            double *fit_lbest);
+/* out[0..n): last simulation launch (GPU ms), launches, neuron-steps of one
+ * full run, longest simulation (steps). */
+BG_API int bg_fit_stats(bg_fit *h, double *out, int n);
+
 #ifdef __cplusplus
 }
 #endif
