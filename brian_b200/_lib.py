@@ -59,10 +59,8 @@ ENGINE_ONLY = {
     "net_item_name": [_vp, _i64, ct.c_char_p, _i64],
     "fixed_indegree_csr": [_i64, _i64, _i64, _u64, _vp, _vp],
     "net_set_persistent": [_vp, ct.c_int],
-    "fit_compile_check": [ct.c_int, ct.c_char_p, ct.c_char_p, ct.c_char_p, ct.c_char_p, _dbl, ct.c_int, ct.c_int,
-                          ct.c_char_p, _i64],
-    "fit_create": [_P(_vp), ct.c_int, ct.c_int, ct.c_char_p, ct.c_char_p, ct.c_char_p, ct.c_char_p, _dbl,
-                   ct.c_int, ct.c_int],
+    "fit_compile_check": [ct.c_int, _vp, _dbl, ct.c_int, ct.c_int, ct.c_char_p, _i64],
+    "fit_create": [_P(_vp), ct.c_int, ct.c_int, _vp, _dbl, ct.c_int, ct.c_int],
     "fit_destroy": [_vp],
     "fit_set_input": [_vp, _vp, _i64],
     "fit_set_targets": [_vp, _vp, _i64],
@@ -75,6 +73,8 @@ ENGINE_ONLY = {
     "fit_set_gamma": [_vp, _i64, _i32, _vp, _vp, _dbl],
     "fit_set_params": [_vp, _i32, _vp],
     "fit_evaluate": [_vp, _vp, _vp],
+    "fit_set_blocks_per_sm": [_vp, _i32],
+    "fit_autotune": [_vp, _vp, _P(_i32), _vp],
     "fit_pso_init": [_vp, _i32, _vp, _vp, _vp, _dbl, _dbl, _dbl, _u64],
     "fit_pso_evaluate_initial": [_vp],
     "fit_pso_run": [_vp, _i32, _vp, _vp],
@@ -323,6 +323,21 @@ def fixed_indegree_csr_native(n_src, n_tgt, k, seed):
     return rowptr, cols
 
 
+class FitModel(ct.Structure):
+    """bg_fit_model: the generated model code handed to the fitting kernel."""
+    _fields_ = [("state_names", ct.c_char_p), ("update_code", ct.c_char_p), ("update_fast_code", ct.c_char_p),
+                ("threshold_code", ct.c_char_p), ("reset_code", ct.c_char_p), ("aux_decl", ct.c_char_p),
+                ("setup_code", ct.c_char_p)]
+
+    @classmethod
+    def of(cls, code):
+        def b(x):
+            return (x or "").encode()
+        m = cls(b(",".join(code.state)), b(code.update), b(getattr(code, "update_fast", "")), b(code.threshold),
+                b(code.reset), b(getattr(code, "aux_decl", "")), b(getattr(code, "setup", "")))
+        return m
+
+
 class FitHandle(object):
     """One batched-fitting handle (bg_fit_* in include/brian_b200.h)."""
 
@@ -332,8 +347,8 @@ class FitHandle(object):
         self.code = code
         self.nstate = len(code.state)
         self.precision = precision
-        self.t.check(self.t.fit_create(ct.byref(self.h), int(device), int(precision), ",".join(code.state).encode(),
-                                       code.update.encode(), code.threshold.encode(), code.reset.encode(),
+        self._model = FitModel.of(code)
+        self.t.check(self.t.fit_create(ct.byref(self.h), int(device), int(precision), ct.byref(self._model),
                                        float(dt), int(delta_steps), 1 if exclusive else 0), "fit_create")
         self.ns = 0
         self.rec_cap = 0
@@ -415,6 +430,18 @@ class FitHandle(object):
         self._c(self.t.fit_evaluate(self.h, _ptr(X), _ptr(out)), "fit_evaluate")
         return out
 
+    def set_blocks_per_sm(self, b):
+        self._c(self.t.fit_set_blocks_per_sm(self.h, int(b)), "fit_set_blocks_per_sm")
+
+    def autotune(self, X=None):
+        """Fastest launch shape for a full run (results do not depend on it);
+        returns (blocks per SM, ms per candidate)."""
+        X = None if X is None else np.ascontiguousarray(X, dtype=np.float64)
+        b = _i32()
+        ms = np.zeros(6, dtype=np.float32)
+        self._c(self.t.fit_autotune(self.h, _ptr(X), ct.byref(b), _ptr(ms)), "fit_autotune")
+        return b.value, ms
+
     def pso_init(self, group_size, X0, xmin, xmax, omega, c1, c2, seed):
         X0 = np.ascontiguousarray(X0, dtype=np.float64)
         lo = np.ascontiguousarray(xmin, dtype=np.float64)
@@ -458,7 +485,7 @@ def fit_compile_check(code, dt, delta_steps, exclusive=True, precision=64):
     the compiler log, raises EngineError on failure."""
     t = product_table()
     log = ct.create_string_buffer(1 << 16)
-    t.check(t.fit_compile_check(int(precision), ",".join(code.state).encode(), code.update.encode(),
-                                code.threshold.encode(), code.reset.encode(), float(dt), int(delta_steps),
+    model = FitModel.of(code)
+    t.check(t.fit_compile_check(int(precision), ct.byref(model), float(dt), int(delta_steps),
                                 1 if exclusive else 0, log, 1 << 16), "fit_compile_check")
     return log.value.decode(errors="replace")

@@ -42,10 +42,14 @@ class _Emitter(object):
     expressions (state registers, the input, ``t``); other identifiers are
     looked up in ``namespace`` and must be numbers."""
 
-    def __init__(self, scalar, names, namespace):
+    def __init__(self, scalar, names, namespace, fast=None):
         self.scalar = scalar
         self.names = names
         self.namespace = namespace
+        self.fast = fast
+
+    def copy(self):
+        return _Emitter(self.scalar, dict(self.names), self.namespace, self.fast)
 
     def literal(self, value):
         value = float(value)
@@ -100,6 +104,11 @@ class _Emitter(object):
             op = _BINOPS.get(type(node.op))
             if op is None:
                 raise CodegenError("unsupported operator %s" % type(node.op).__name__)
+            if op == "/" and self.fast is not None:
+                k = self.fast.slot(node.right)
+                if k is not None:
+                    return "bg_div_fast(%s, %s, bg_y%d, bg_t%d, suspect)" % (
+                        self.expr(node.left), self.expr(node.right), k, k)
             return "(%s %s %s)" % (self.expr(node.left), op, self.expr(node.right))
         if isinstance(node, ast.Call):
             if not isinstance(node.func, ast.Name) or node.func.id not in _FUNCS1 or len(node.args) != 1 \
@@ -152,6 +161,60 @@ def _cname(name):
     return "s_" + name
 
 
+class _FastDivisions(object):
+    """Divisions whose divisor depends only on parameters the reset never
+    assigns (and on constants) divide by a per-simulation reciprocal fixed at
+    load time.  Each gets members bg_y<k> (the reciprocal, double) and
+    bg_t<k> (the dividend magnitude below which the fast form may round
+    differently, or a guard exponent for double).  The kernel checks those
+    conditions branch-free and redoes a block with IEEE division when any
+    dividend falls outside them, so results equal plain division."""
+
+    def __init__(self, base, invariant):
+        self.base = base            # emitter over the load-time names
+        self.invariant = invariant
+        self.keys = []
+
+    def slot(self, node):
+        for n in ast.walk(node):
+            if isinstance(n, ast.Name):
+                if n.id in self.invariant:
+                    continue
+                if n.id in self.base.names:          # state, input or time
+                    return None
+                if n.id not in self.base.namespace:
+                    return None
+            elif isinstance(n, ast.Call):
+                if not isinstance(n.func, ast.Name) or n.func.id not in _FUNCS1:
+                    return None
+        key = self.base.expr(node)
+        if key not in self.keys:
+            self.keys.append(key)
+        return self.keys.index(key)
+
+    def declarations(self):
+        sc = self.base.scalar
+        return "".join("    double bg_y%d;\n    %s bg_t%d;\n" % (k, sc, k) for k in range(len(self.keys)))
+
+    def setup(self):
+        """Reciprocal and dividend bound of each divisor; a divisor outside
+        the range where the fast forms are exact (zero, subnormal, huge,
+        infinite, NaN) sends the whole simulation down the IEEE path
+        (bg_exact)."""
+        out = []
+        for k, key in enumerate(self.keys):
+            if self.base.scalar == "float":
+                out.append("{ const float b = %s; bg_y%d = 1.0 / (double)b; "
+                           "if (!(fabsf(b) >= 0x1p-126f && fabsf(b) <= 0x1p+126f)) bg_exact = true; "
+                           "bg_t%d = (float)(0x1p-126 * fmax(1.0, fabs((double)b)) * (1.0 + 0x1p-20)); }"
+                           % (key, k, k))
+            else:
+                out.append("{ const double b = %s; bg_y%d = 1.0 / b; "
+                           "if (!(fabs(b) >= 0x1p-100 && fabs(b) <= 0x1p+100)) bg_exact = true; "
+                           "bg_t%d = 0x1p-900; }" % (key, k, k))
+        return "\n".join(out)
+
+
 class ModelCode(object):
     """Generated snippets of one model for one scalar type.
 
@@ -159,9 +222,14 @@ class ModelCode(object):
     their storage order (the prepared equations' differential equations,
     parameters included, without the input variable); ``update``,
     ``threshold`` and ``reset`` are C code over the registers ``s_<name>``,
-    the input ``I_in`` and the time ``t``."""
+    the input ``I_in`` and the time ``t``; the reset statements are selects
+    on the kernel's flag ``reset_on``.  ``update_fast`` is the same step with
+    divisions by invariant divisors in reciprocal form (empty when there are
+    none); ``aux_decl`` and ``setup`` declare and initialise the
+    reciprocals."""
 
-    def __init__(self, state, dynamic, update, threshold, reset, scalar, scheme, uses_t):
+    def __init__(self, state, dynamic, update, threshold, reset, scalar, scheme, uses_t, update_fast="",
+                 aux_decl="", setup=""):
         self.state = list(state)
         self.dynamic = list(dynamic)
         self.update = update
@@ -170,6 +238,9 @@ class ModelCode(object):
         self.scalar = scalar
         self.scheme = scheme
         self.uses_t = uses_t
+        self.update_fast = update_fast
+        self.aux_decl = aux_decl
+        self.setup = setup
 
     def index(self, name):
         return self.state.index(name)
@@ -192,7 +263,7 @@ def _scheme_code(eqs, em, dynamic, state, scheme):
             lines.append("%s %s__buf = %s;" % (sc, v, em.expr(trees[v])))
             lines.append("%s %s__half = (%s * %s__buf);" % (sc, v, half, v))
             lines.append("%s__half = (%s__half + %s);" % (v, v, _cname(v)))
-        sub = _Emitter(sc, dict(em.names), em.namespace)
+        sub = em.copy()
         for v in state:
             sub.names[v] = v + "__half"
         for v in dynamic:
@@ -200,9 +271,9 @@ def _scheme_code(eqs, em, dynamic, state, scheme):
             lines.append("%s = (%s + (%s * %s__buf));" % (_cname(v), _cname(v), dt, v))
     elif scheme == "exponential_Euler":
         for v in dynamic:
-            z = _Emitter(sc, dict(em.names), em.namespace)
+            z = em.copy()
             z.names[v] = em.literal(0.0)
-            o = _Emitter(sc, dict(em.names), em.namespace)
+            o = em.copy()
             o.names[v] = em.literal(1.0)
             lines.append("%s %s__B = %s;" % (sc, v, z.expr(trees[v])))
             lines.append("%s %s__A = %s;" % (sc, v, o.expr(trees[v])))
@@ -244,8 +315,14 @@ def _statements(text, em, state):
             raise CodegenError("unsupported reset statement %r" % line)
         if tgt not in state:
             raise CodegenError("reset assigns %r, which is not a state variable" % tgt)
-        out.append("%s = %s;" % (_cname(tgt), value))
+        out.append(_masked(tgt, value))
     return "\n".join(out)
+
+
+def _masked(tgt, value):
+    """The reset runs every step as selects on `reset_on` (the kernel's
+    spiking-or-refractory flag), so no branch breaks the step's chain."""
+    return "%s = (reset_on ? %s : %s);" % (_cname(tgt), value, _cname(tgt))
 
 
 def generate_model_code(eqs, threshold, reset, dt, input_var="I", scalar="double", scheme="Euler",
@@ -290,17 +367,28 @@ def generate_model_code(eqs, threshold, reset, dt, input_var="I", scalar="double
     if reset is None:
         rst = ""
     elif isinstance(reset, _g.VariableReset):
-        rst = "%s = %s;" % (_cname(var_name(reset.state)), _cname(var_name(reset.resetvaluestate)))
+        rst = _masked(var_name(reset.state), _cname(var_name(reset.resetvaluestate)))
     elif isinstance(reset, _g.StringReset):
         rst = _statements(reset.expr, em, state)
     elif isinstance(reset, _g.Reset):
-        rst = "%s = %s;" % (_cname(var_name(reset.state)), em.literal(reset.resetvalue))
+        rst = _masked(var_name(reset.state), em.literal(reset.resetvalue))
     elif isinstance(reset, str):
         rst = _statements(reset, em, state)
     else:
-        rst = "%s = %s;" % (_cname(vm), em.literal(reset))
+        rst = _masked(vm, em.literal(reset))
 
     upd = _scheme_code(eqs, em, dynamic, state, scheme)
     uses_t = any("t" == n.id for v in dynamic for n in ast.walk(_parse(eqs._string[v]))
                  if isinstance(n, ast.Name))
-    return ModelCode(state, dynamic, upd, thr, rst, scalar, scheme, uses_t)
+    # parameters the reset leaves alone are fixed for a whole run
+    assigned = set()
+    for raw in rst.split("\n"):
+        if raw.strip():
+            assigned.add(raw.split("=", 1)[0].strip()[2:])
+    invariant = {v for v in state if v not in dynamic and v not in assigned}
+    fast = _FastDivisions(_Emitter(scalar, names, ns), invariant)
+    upd_fast = _scheme_code(eqs, _Emitter(scalar, names, ns, fast), dynamic, state, scheme)
+    if not fast.keys:
+        upd_fast = ""
+    return ModelCode(state, dynamic, upd, thr, rst, scalar, scheme, uses_t, upd_fast, fast.declarations(),
+                     fast.setup())

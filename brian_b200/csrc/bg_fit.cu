@@ -60,6 +60,7 @@ struct FitArgsHost {
     const int *order;
     int *rec;
     int *rec_n;
+    int *next_task;
     long long ns;
     int Tstart, Tend, onset, rec_cap;
 };
@@ -86,17 +87,22 @@ bool valid_ident(const std::string &s) {
     return true;
 }
 
-// Full NVRTC source: scalar type, constants, the Model struct, the template.
-int assemble_source(int precision, const char *state_names, const char *update, const char *threshold,
-                    const char *reset, double dt, int delta, int exclusive, std::string *src, int *nstate) {
+const char *nz(const char *p) { return p ? p : ""; }
+
+// Full NVRTC source: scalar type, constants, the division helpers, the Model
+// struct, the template.
+int assemble_source(int precision, const bg_fit_model *model, double dt, int delta, int exclusive, std::string *src,
+                    int *nstate) {
     if (precision != 32 && precision != 64) return fail(BG_EINVAL, "fit: precision must be 32 or 64");
     if (!(dt > 0)) return fail(BG_EINVAL, "fit: dt must be positive");
     if (delta < 0) return fail(BG_EINVAL, "fit: delta must be >= 0");
-    std::vector<std::string> names = split_names(state_names);
+    if (!model) return fail(BG_EINVAL, "fit: null model");
+    std::vector<std::string> names = split_names(model->state_names);
     if (names.empty()) return fail(BG_EINVAL, "fit: no state variables");
     for (auto &n : names)
         if (!valid_ident(n)) return fail(BG_EINVAL, "fit: bad state variable name '" + n + "'");
     const char *sc = precision == 32 ? "float" : "double";
+    const bool has_fast = model->update_fast_code && *model->update_fast_code;
     char dtbuf[64];
     snprintf(dtbuf, sizeof dtbuf, "%a", dt);
     std::ostringstream o;
@@ -104,18 +110,24 @@ int assemble_source(int precision, const char *state_names, const char *update, 
       << "#define BG_DT (" << dtbuf << ")\n"
       << "#define BG_DELTA (" << delta << ")\n"
       << "#define BG_EXCLUSIVE " << (exclusive ? 1 : 0) << "\n"
+      << kFitHelperSource
       << "struct Model {\n";
     for (auto &n : names) o << "    scalar s_" << n << ";\n";
+    o << "    bool bg_exact;\n" << nz(model->aux_decl) << "\n";
     o << "    __device__ __forceinline__ void load(const scalar *S, long long ns, long long i) {\n";
     for (size_t k = 0; k < names.size(); ++k) o << "        s_" << names[k] << " = S[" << k << "LL * ns + i];\n";
+    o << "        bg_exact = false;\n" << nz(model->setup_code) << "\n";
     o << "    }\n    __device__ __forceinline__ void store(scalar *S, long long ns, long long i) const {\n";
     for (size_t k = 0; k < names.size(); ++k) o << "        S[" << k << "LL * ns + i] = s_" << names[k] << ";\n";
     o << "    }\n    __device__ __forceinline__ void update(const scalar I_in, const scalar t) {\n"
-      << (update ? update : "") << "\n    }\n"
+      << nz(model->update_code) << "\n    }\n"
+      << "    __device__ __forceinline__ void update_fast(const scalar I_in, const scalar t, bool &suspect) {\n"
+      << (has_fast ? nz(model->update_fast_code) : "update(I_in, t);") << "\n    }\n"
       << "    __device__ __forceinline__ bool threshold(const scalar I_in, const scalar t) const {\n"
-      << "        return " << (threshold && *threshold ? threshold : "false") << ";\n    }\n"
-      << "    __device__ __forceinline__ void reset(const scalar I_in, const scalar t) {\n"
-      << (reset ? reset : "") << "\n    }\n};\n"
+      << "        return " << (model->threshold_code && *model->threshold_code ? model->threshold_code : "false")
+      << ";\n    }\n"
+      << "    __device__ __forceinline__ void reset(const scalar I_in, const scalar t, const bool reset_on) {\n"
+      << nz(model->reset_code) << "\n    }\n};\n"
       << kFitKernelSource;
     *src = o.str();
     *nstate = (int)names.size();
@@ -177,6 +189,9 @@ struct bg_fit {
     int rec_cap = 0;
     int onset = 0;
     int max_steps = 0;
+    int *next_task = nullptr;
+    int nsm = 148;
+    int blocks_per_sm = 2;      // resident simulation blocks per SM (bg_fit_autotune)
     // gamma
     int64_t npart = 0;
     int slices = 1;
@@ -350,13 +365,18 @@ int sim_launch(bg_fit *h, int Tstart, int Tend) {
     a.order = h->order;
     a.rec = h->rec_cap > 0 ? h->rec : nullptr;
     a.rec_n = h->rec_cap > 0 ? h->rec_n : nullptr;
+    a.next_task = h->next_task;
     a.ns = h->ns;
     a.Tstart = Tstart;
     a.Tend = Tend;
     a.onset = h->onset;
     a.rec_cap = h->rec_cap;
     void *args[] = {&a};
-    const unsigned grid = (unsigned)((h->ns + kSimThreads - 1) / kSimThreads);
+    // persistent warps pulling 32-simulation tasks; no more blocks than tasks
+    const long long ntasks = (h->ns + 31) / 32;
+    const long long want = (long long)h->nsm * h->blocks_per_sm;
+    const unsigned grid = (unsigned)std::max(1LL, std::min(want, (ntasks + kSimThreads / 32 - 1) / (kSimThreads / 32)));
+    FCK(cudaMemsetAsync(h->next_task, 0, sizeof(int), h->stream));
     FCK(cudaLaunchKernel((const void *)h->kern, dim3(grid), dim3(kSimThreads), args, 0, h->stream));
     ++h->sim_launches;
     return BG_OK;
@@ -420,13 +440,11 @@ int upload_scalar(bg_fit *h, void **dst, const double *src, size_t n) {
 // ====================================================================== C ABI
 extern "C" {
 
-BG_API int bg_fit_compile_check(int precision, const char *state_names, const char *update_code,
-                                const char *threshold_code, const char *reset_code, double dt, int delta_steps,
+BG_API int bg_fit_compile_check(int precision, const bg_fit_model *model, double dt, int delta_steps,
                                 int exclusive, char *log, int64_t log_len) {
     std::string src, lg;
     int nstate = 0;
-    int rc = assemble_source(precision, state_names, update_code, threshold_code, reset_code, dt, delta_steps,
-                             exclusive, &src, &nstate);
+    int rc = assemble_source(precision, model, dt, delta_steps, exclusive, &src, &nstate);
     if (rc) return rc;
     std::vector<char> cubin;
     rc = nvrtc_compile(src, &cubin, &lg);
@@ -436,15 +454,13 @@ BG_API int bg_fit_compile_check(int precision, const char *state_names, const ch
     return rc;
 }
 
-BG_API int bg_fit_create(bg_fit **out, int device, int precision, const char *state_names, const char *update_code,
-                         const char *threshold_code, const char *reset_code, double dt, int delta_steps,
-                         int exclusive) {
+BG_API int bg_fit_create(bg_fit **out, int device, int precision, const bg_fit_model *model, double dt,
+                         int delta_steps, int exclusive) {
     if (!out) return fail(BG_EINVAL, "fit: null output pointer");
     *out = nullptr;
     std::string src, lg;
     int nstate = 0;
-    int rc = assemble_source(precision, state_names, update_code, threshold_code, reset_code, dt, delta_steps,
-                             exclusive, &src, &nstate);
+    int rc = assemble_source(precision, model, dt, delta_steps, exclusive, &src, &nstate);
     if (rc) return rc;
     std::vector<char> cubin;
     rc = nvrtc_compile(src, &cubin, &lg);
@@ -460,6 +476,8 @@ BG_API int bg_fit_create(bg_fit **out, int device, int precision, const char *st
     cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaLibraryLoadData(&h->lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
     if (e == cudaSuccess) e = cudaLibraryGetKernel(&h->kern, h->lib, "bg_fit_sim");
+    if (e == cudaSuccess) e = cudaMalloc((void **)&h->next_task, sizeof(int));
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, device);
     if (e == cudaSuccess) e = cudaEventCreate(&h->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&h->ev1);
     if (e != cudaSuccess) {
@@ -481,6 +499,7 @@ BG_API int bg_fit_destroy(bg_fit *h) {
     free_ptr(h->nspikes); free_ptr(h->order); free_ptr(h->flags); free_ptr(h->rec); free_ptr(h->rec_n);
     free_ptr(h->tlen); free_ptr(h->trate); free_ptr(h->fit); free_ptr(h->dimvar); free_ptr(h->X); free_ptr(h->V);
     free_ptr(h->Xl); free_ptr(h->lfit); free_ptr(h->Xg); free_ptr(h->gfit); free_ptr(h->lo); free_ptr(h->hi);
+    free_ptr(h->next_task);
     if (h->lib) cudaLibraryUnload(h->lib);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
@@ -692,6 +711,55 @@ BG_API int bg_fit_evaluate(bg_fit *h, const double *X, double *gamma_out) {
     FCK(cudaEventElapsedTime(&h->last_sim_ms, h->ev0, h->ev1));
     if (gamma_out) FCK(cudaMemcpy(gamma_out, h->fit, (size_t)h->npart * sizeof(double), cudaMemcpyDeviceToHost));
     return BG_OK;
+}
+
+BG_API int bg_fit_set_blocks_per_sm(bg_fit *h, int32_t blocks_per_sm) {
+    if (!h || blocks_per_sm < 1 || blocks_per_sm > 16) return fail(BG_EINVAL, "fit: blocks per SM must be in 1..16");
+    h->blocks_per_sm = blocks_per_sm;
+    return BG_OK;
+}
+
+BG_API int bg_fit_autotune(bg_fit *h, const double *X, int32_t *blocks_per_sm, float *ms_out) {
+    int rc = check_sims(h);
+    if (rc) return rc;
+    if (X && !h->npart) return fail(BG_ESTATE, "fit: bg_fit_set_gamma not called");
+    FCK(cudaSetDevice(h->device));
+    double *dX = nullptr;
+    const size_t nx = X ? (size_t)h->ndim * h->npart : 0;
+    if (nx) {
+        if (cudaMalloc((void **)&dX, nx * sizeof(double)) != cudaSuccess) return fail(BG_ENOMEM, "fit: cudaMalloc failed");
+        cudaMemcpy(dX, X, nx * sizeof(double), cudaMemcpyHostToDevice);
+    }
+    // every candidate launch shape runs the same simulations; results do not
+    // depend on it, only the time does
+    static const int cand[] = {1, 2, 3, 4, 6, 8};
+    float best = INFINITY;
+    int bestb = h->blocks_per_sm;
+    for (int k = 0; k < (int)(sizeof cand / sizeof cand[0]) && !rc; ++k) {
+        h->blocks_per_sm = cand[k];
+        rc = prepare_launch(h, dX);
+        if (!rc) rc = sim_launch(h, 0, h->max_steps);      // warm
+        if (!rc) rc = prepare_launch(h, dX);
+        if (!rc) {
+            cudaEventRecord(h->ev0, h->stream);
+            rc = sim_launch(h, 0, h->max_steps);
+            cudaEventRecord(h->ev1, h->stream);
+        }
+        if (!rc && cudaStreamSynchronize(h->stream) != cudaSuccess) rc = fail(BG_ECUDA, "fit: autotune run failed");
+        float ms = 0;
+        if (!rc) cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+        if (ms_out) ms_out[k] = ms;
+        if (!rc && ms < best) {
+            best = ms;
+            bestb = cand[k];
+        }
+    }
+    h->blocks_per_sm = bestb;
+    if (!rc) rc = prepare_launch(h, dX);
+    cudaStreamSynchronize(h->stream);
+    if (dX) cudaFree(dX);
+    if (blocks_per_sm) *blocks_per_sm = bestb;
+    return rc;
 }
 
 BG_API int bg_fit_pso_init(bg_fit *h, int32_t group_size, const double *X0, const double *xmin, const double *xmax,

@@ -257,23 +257,31 @@ BG_API int bg_net_stats(bg_net *net, int64_t *steps, int64_t *launches,
  * spike delay and refractory period.  The kernel follows the reference's
  * runsim template (gpu_modelfitting.py:39-156).
  *
- * The model is given as C code over the state registers s_<name>, the input
- * I_in and the time t: `update_code` (statements of one step),
- * `threshold_code` (a bool expression) and `reset_code` (statements).
- * state_names lists the state rows in storage order, comma-separated.
- * precision 32 or 64 selects the scalar type; delta_steps =
- * rint(delta/dt); exclusive = 1 for the 'exclusive' coincidence algorithm,
- * 0 for 'inclusive'.  The kernel is compiled by NVRTC for sm_100a;
- * BG_ECOMPILE carries the compiler log in bg_last_error. */
+ * The model is C code over the state registers s_<name>, the input I_in
+ * and the time t (bg_fit_model below).  precision 32 or 64 selects the
+ * scalar type; delta_steps = rint(delta/dt); exclusive = 1 for the
+ * 'exclusive' coincidence algorithm, 0 for 'inclusive'.  The kernel is
+ * compiled by NVRTC for sm_100a; BG_ECOMPILE carries the compiler log in
+ * bg_last_error. */
+typedef struct bg_fit_model {
+    const char *state_names;      /* state rows in storage order, comma-separated */
+    const char *update_code;      /* statements of one step                       */
+    const char *update_fast_code; /* the same step with divisions by run-constant
+                                     divisors written bg_div_fast(a, b, y, thr,
+                                     suspect); NULL/"" = update_code            */
+    const char *threshold_code;   /* bool expression                              */
+    const char *reset_code;       /* statements run every step; the bool reset_on
+                                     is true on a spike and while refractory, so
+                                     write x = reset_on ? v : x                   */
+    const char *aux_decl;         /* extra Model members (reciprocals), or NULL   */
+    const char *setup_code;       /* statements run once after the state is
+                                     loaded (may set bool bg_exact), or NULL      */
+} bg_fit_model;
 /* Compile only (no device needed); the log is copied to `log`. */
-BG_API int bg_fit_compile_check(int precision, const char *state_names,
-                                const char *update_code, const char *threshold_code,
-                                const char *reset_code, double dt, int delta_steps,
-                                int exclusive, char *log, int64_t log_len);
+BG_API int bg_fit_compile_check(int precision, const bg_fit_model *model, double dt,
+                                int delta_steps, int exclusive, char *log, int64_t log_len);
 /* GPUModelFitting.__init__ (gpu_modelfitting.py:266-331). */
-BG_API int bg_fit_create(bg_fit **out, int device, int precision,
-                         const char *state_names, const char *update_code,
-                         const char *threshold_code, const char *reset_code,
+BG_API int bg_fit_create(bg_fit **out, int device, int precision, const bg_fit_model *model,
                          double dt, int delta_steps, int exclusive);
 BG_API int bg_fit_destroy(bg_fit *h);
 /* I (the reference's I_arr): all input traces concatenated; converted to
@@ -319,6 +327,14 @@ BG_API int bg_fit_set_params(bg_fit *h, int32_t ndim, const int32_t *dim_var);
  * resets, simulates every particle over its full length and writes the
  * gamma factor (FP64, get_gamma_factor, statistics.py:236-240). */
 BG_API int bg_fit_evaluate(bg_fit *h, const double *X, double *gamma_out);
+/* Launch shape of the simulation kernel: resident 128-thread blocks per SM
+ * (1..16, default 2).  Results never depend on it. */
+BG_API int bg_fit_set_blocks_per_sm(bg_fit *h, int32_t blocks_per_sm);
+/* Time one full run per candidate launch shape (1, 2, 3, 4, 6, 8 blocks per
+ * SM) with parameters X ([ndim][nparticles], NULL = the initial state), keep
+ * the fastest; ms_out[6] (nullable) receives each candidate's time.  Leaves
+ * the simulations reset with X. */
+BG_API int bg_fit_autotune(bg_fit *h, const double *X, int32_t *blocks_per_sm, float *ms_out);
 /* Grouped particle swarm on the device (particle_swarm.py:6-111): groups of
  * group_size consecutive particles optimise independently (one target
  * each); X0 [ndim][nparticles] is clipped into [xmin, xmax]. */

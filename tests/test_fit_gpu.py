@@ -241,3 +241,42 @@ def test_gpu_modelfitting_class_with_neurongroup():
                     np.full(N, len(spk)), delta=40, exclusive=True)
     assert np.array_equal(mf.coincidence_count, r["coinc"])
     assert np.array_equal(mf.spike_count, r["nspikes"])
+
+
+@pytest.mark.parametrize("precision", [32, 64])
+def test_reciprocal_division_falls_back_exactly(precision):
+    """Divisions by run-constant divisors use reciprocal forms; dividends or
+    quotients outside the range where those are exact (subnormal values,
+    tiny quotients) make the kernel redo the block with IEEE division, zero
+    dividends stay on the fast form, and zero / subnormal / infinite / NaN
+    divisors send the whole simulation to IEEE division.  Every state must
+    equal numpy's IEEE arithmetic bit for bit."""
+    dtype = np.float32 if precision == 32 else np.float64
+    tiny = 1e-36 if precision == 32 else 1e-300
+    eqs = Equations("dV/dt = (a - V)/tau : 1\nI : 1\na : 1\ntau : 1", dummy=0.0)
+    code = generate_model_code(eqs, "V > 1e30", "V = 0", DT, scalar="float" if precision == 32 else "double")
+    assert code.update_fast and "bg_div_fast" in code.update_fast
+    ns = 96
+    rng = np.random.default_rng(8)
+    V0 = np.concatenate([np.full(32, tiny), rng.uniform(-1, 1, 32), np.full(32, 0.25)])
+    a = np.concatenate([np.zeros(32), rng.uniform(-1, 1, 32), np.full(32, 0.25)])   # a == V: zero dividends
+    tau = np.concatenate([np.full(32, 1e-3), rng.uniform(1e-3, 1e-1, 32), np.full(32, 5e-3)])
+    tau[[3, 40, 70]] = 0.0
+    tau[[5, 41]] = 1e-40 if precision == 32 else 1e-320
+    tau[[6, 42]] = np.inf
+    tau[[7, 43]] = np.nan
+    tau[44] = -0.0
+    S0 = np.vstack([V0, a, tau])
+    n = 3000
+    c = dict(S0=S0, I=np.zeros(n), I_offset=np.zeros(ns, int), nsteps=np.full(ns, n),
+             spiketimes=np.array([-10000, n + 10000]), spk_offset=np.zeros(ns, int), spk_end=np.full(ns, 2),
+             delay=np.zeros(ns, int), refractory=np.zeros(ns, int))
+    h = _device(code, c, precision, True)
+    h.run(0, n)
+    S = h.read(state=True)[2]
+    m = of.ModelOracle(eqs, "V > 1e30", "V = 0", DT, dtype)
+    with np.errstate(all="ignore"):
+        r = of.simulate(m, S0, c["I"], c["I_offset"], c["nsteps"], c["spiketimes"], c["spk_offset"], c["spk_end"])
+    assert np.array_equal(S, r["state"], equal_nan=True)
+    # the decaying tiny values did reach the subnormal range
+    assert np.any((np.abs(r["state"][0, :32]) < np.finfo(dtype).tiny) & (r["state"][0, :32] != 0))
