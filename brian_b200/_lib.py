@@ -73,7 +73,17 @@ ENGINE_ONLY = {
     "fit_set_gamma": [_vp, _i64, _i32, _vp, _vp, _dbl],
     "fit_set_params": [_vp, _i32, _vp],
     "fit_evaluate": [_vp, _vp, _vp],
+    "fit_features": [_vp, _vp],
     "fit_set_blocks_per_sm": [_vp, _i32],
+    "mlp_create": [_P(_vp), ct.c_int, ct.c_int],
+    "mlp_destroy": [_vp],
+    "mlp_set_params": [_vp, ct.c_int, _vp, _vp],
+    "mlp_get_params": [_vp, ct.c_int, _vp, _vp],
+    "mlp_forward": [_vp, _vp, _i64, _vp],
+    "mlp_set_data": [_vp, _vp, _vp, _i64],
+    "mlp_train": [_vp, ct.c_int, ct.c_int, ct.c_float, _u64, _vp, _P(ct.c_float)],
+    "mlp_gradients": [_vp, ct.c_int, _P(ct.c_float), _vp, _vp],
+    "gemm_bf16": [_i64, _i64, _i64, _vp, _vp, _vp, _vp],
     "fit_autotune": [_vp, _vp, _P(_i32), _vp],
     "fit_pso_init": [_vp, _i32, _vp, _vp, _vp, _dbl, _dbl, _dbl, _u64],
     "fit_pso_evaluate_initial": [_vp],
@@ -430,6 +440,11 @@ class FitHandle(object):
         self._c(self.t.fit_evaluate(self.h, _ptr(X), _ptr(out)), "fit_evaluate")
         return out
 
+    def features(self):
+        out = np.empty((self.ns, 64), dtype=np.float32)
+        self._c(self.t.fit_features(self.h, _ptr(out)), "fit_features")
+        return out
+
     def set_blocks_per_sm(self, b):
         self._c(self.t.fit_set_blocks_per_sm(self.h, int(b)), "fit_set_blocks_per_sm")
 
@@ -489,3 +504,70 @@ def fit_compile_check(code, dt, delta_steps, exclusive=True, precision=64):
     t.check(t.fit_compile_check(int(precision), ct.byref(model), float(dt), int(delta_steps),
                                 1 if exclusive else 0, log, 1 << 16), "fit_compile_check")
     return log.value.decode(errors="replace")
+
+
+MLP_ROWS = (512, 512, 512, 64)
+MLP_COLS = (64, 512, 512, 512)
+
+
+class MLPHandle(object):
+    """The proposal network (bg_mlp_* in include/brian_b200.h)."""
+
+    def __init__(self, ydim=5, device=0, table=None):
+        self.t = table if table is not None else product_table()
+        self.h = ct.c_void_p()
+        self.ydim = ydim
+        self.t.check(self.t.mlp_create(ct.byref(self.h), int(device), int(ydim)), "mlp_create")
+
+    def close(self):
+        if self.h:
+            self.t.mlp_destroy(self.h)
+            self.h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _c(self, st, what):
+        self.t.check(st, what)
+
+    def set_params(self, layer, W, b):
+        W = np.ascontiguousarray(W, dtype=np.float32)
+        b = np.ascontiguousarray(b, dtype=np.float32)
+        assert W.shape == (MLP_ROWS[layer], MLP_COLS[layer]) and b.shape == (MLP_ROWS[layer],)
+        self._c(self.t.mlp_set_params(self.h, int(layer), _ptr(W), _ptr(b)), "mlp_set_params")
+
+    def get_params(self, layer):
+        W = np.empty((MLP_ROWS[layer], MLP_COLS[layer]), dtype=np.float32)
+        b = np.empty(MLP_ROWS[layer], dtype=np.float32)
+        self._c(self.t.mlp_get_params(self.h, int(layer), _ptr(W), _ptr(b)), "mlp_get_params")
+        return W, b
+
+    def forward(self, X):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        out = np.empty((len(X), 2 * self.ydim), dtype=np.float32)
+        self._c(self.t.mlp_forward(self.h, _ptr(X), len(X), _ptr(out)), "mlp_forward")
+        return out
+
+    def set_data(self, X, Y):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.ascontiguousarray(Y, dtype=np.float32)
+        self._c(self.t.mlp_set_data(self.h, _ptr(X), _ptr(Y), len(X)), "mlp_set_data")
+
+    def train(self, epochs, batch, lr, seed):
+        loss = np.zeros(max(1, epochs), dtype=np.float32)
+        ms = ct.c_float()
+        self._c(self.t.mlp_train(self.h, int(epochs), int(batch), float(lr), int(seed) & ((1 << 64) - 1),
+                                 _ptr(loss), ct.byref(ms)), "mlp_train")
+        return loss[:epochs], ms.value
+
+    def gradients(self, batch):
+        dW = [np.zeros((MLP_ROWS[l], MLP_COLS[l]), dtype=np.float32) for l in range(4)]
+        db = [np.zeros(MLP_ROWS[l], dtype=np.float32) for l in range(4)]
+        pW = (ct.c_void_p * 4)(*[_ptr(x).value for x in dW])
+        pb = (ct.c_void_p * 4)(*[_ptr(x).value for x in db])
+        loss = ct.c_float()
+        self._c(self.t.mlp_gradients(self.h, int(batch), ct.byref(loss), pW, pb), "mlp_gradients")
+        return loss.value, dW, db

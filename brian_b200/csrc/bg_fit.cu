@@ -347,6 +347,102 @@ __global__ void k_pso_best(int64_t M, int ndim, int group_size, const double *X,
     }
 }
 
+// Spike-train and input features of every simulation from its recorded
+// spikes (first `cap`), one warp per simulation, for the learned proposal:
+//   f[0..31]  histogram of log10(ISI / s) over [-3, log10 2) in 32 equal bins
+//             (outside values in the end bins), divided by the ISI count;
+//   f[32]     firing_rate: (n-1) / (t_last - t_first)   (statistics.py:15-21)
+//   f[33]     CV: std(ISI) / mean(ISI), population std   (statistics.py:23-30)
+//   f[34..63] spike-triggered average of the input in nA over 30 ms before
+//             each spike, 30 bins of 1 ms, most recent first, as
+//             spike_triggered_average (statistics.py:125-153) computes it:
+//             spikes with t > 30 ms contribute input[i-1-j] for j < 300,
+//             i = int(t / dt), and the sum is divided by (n - 1).
+// Quantities that need two spikes are 0 with fewer.  Sums run in double in
+// a fixed order.
+template <typename T>
+__global__ void k_features(int64_t ns, const int *rec, const int *rec_n, int cap, const T *I, const long long *I_off,
+                           double dt, float *out) {
+    constexpr int kBins = 32, kSta = 30, kWin = 300, kPerLane = (kWin + 31) / 32;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t i = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
+    __shared__ double sbin[4][kSta];
+    if (i >= ns) return;
+    const int n = min(rec_n[i], cap);
+    const int *s = rec + i * (int64_t)cap;
+    const double lo = -3.0, hi = log10(2.0), width = (hi - lo) / kBins;
+    // ISI histogram: each lane counts its share into registers, bins reduced
+    // across the warp
+    int cnt[kBins];
+#pragma unroll
+    for (int b = 0; b < kBins; ++b) cnt[b] = 0;
+    double sd = 0.0, sd2 = 0.0;
+    for (int k = lane; k + 1 < n; k += 32) {
+        const double d = (double)(s[k + 1] - s[k]) * dt;
+        sd += d;
+        sd2 += d * d;
+        int b = (int)floor((log10(d) - lo) / width);
+        b = b < 0 ? 0 : (b >= kBins ? kBins - 1 : b);
+#pragma unroll
+        for (int q = 0; q < kBins; ++q) cnt[q] += (q == b) ? 1 : 0;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        sd += __shfl_xor_sync(0xffffffffu, sd, off);
+        sd2 += __shfl_xor_sync(0xffffffffu, sd2, off);
+    }
+    float *f = out + i * 64;
+    const int nisi = n > 1 ? n - 1 : 0;
+#pragma unroll
+    for (int q = 0; q < kBins; ++q) {
+        int c = cnt[q];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
+        if (lane == q) f[q] = nisi ? (float)((double)c / nisi) : 0.f;
+    }
+    if (lane == 0) {
+        if (n >= 2) {
+            const double t0 = (double)s[0] * dt, t1 = (double)s[n - 1] * dt;
+            f[32] = (float)((double)(n - 1) / (t1 - t0));
+            const double mean = sd / nisi;
+            const double var = sd2 / nisi - mean * mean;
+            f[33] = (float)(sqrt(var > 0 ? var : 0.0) / mean);
+        } else {
+            f[32] = 0.f;
+            f[33] = 0.f;
+        }
+    }
+    // spike-triggered average: lane handles window samples j = lane + 32u
+    double acc[kPerLane];
+#pragma unroll
+    for (int u = 0; u < kPerLane; ++u) acc[u] = 0.0;
+    const T *in = I + I_off[i];
+    for (int k = 0; k < n; ++k) {
+        const double t = (double)s[k] * dt;
+        if (!(t > 0.03)) continue;   // spikes after the 30 ms window length
+        const long long idx = (long long)(t / dt);
+#pragma unroll
+        for (int u = 0; u < kPerLane; ++u) {
+            const int j = lane + 32 * u;
+            if (j < kWin) acc[u] += (double)in[idx - 1 - j];
+        }
+    }
+    if (lane < kSta) sbin[warp][lane] = 0.0;
+    __syncwarp();
+    // fixed-order bin sums: lanes in turn
+    for (int src = 0; src < 32; ++src) {
+        if (lane == src) {
+#pragma unroll
+            for (int u = 0; u < kPerLane; ++u) {
+                const int j = lane + 32 * u;
+                if (j < kWin) sbin[warp][j / 10] += acc[u];
+            }
+        }
+        __syncwarp();
+    }
+    if (lane < kSta) f[34 + lane] = n >= 2 ? (float)(sbin[warp][lane] / 10.0 / (double)(n - 1) * 1e9) : 0.f;
+}
+
 int sim_launch(bg_fit *h, int Tstart, int Tend) {
     FitArgsHost a;
     a.S = h->S;
@@ -647,6 +743,31 @@ BG_API int bg_fit_read_spikes(bg_fit *h, int32_t *counts, int32_t *steps) {
     if (counts) FCK(cudaMemcpy(counts, h->rec_n, (size_t)h->ns * sizeof(int), cudaMemcpyDeviceToHost));
     if (steps)
         FCK(cudaMemcpy(steps, h->rec, (size_t)h->ns * h->rec_cap * sizeof(int), cudaMemcpyDeviceToHost));
+    return BG_OK;
+}
+
+BG_API int bg_fit_features(bg_fit *h, float *out) {
+    int rc = check_sims(h);
+    if (rc) return rc;
+    if (h->rec_cap <= 0) return fail(BG_ESTATE, "fit: spike recording is off (bg_fit_set_record)");
+    if (!out) return fail(BG_EINVAL, "fit: null output");
+    FCK(cudaSetDevice(h->device));
+    float *d = nullptr;
+    if (cudaMalloc((void **)&d, (size_t)h->ns * 64 * sizeof(float)) != cudaSuccess)
+        return fail(BG_ENOMEM, "fit: cudaMalloc failed");
+    const unsigned grid = (unsigned)((h->ns + 3) / 4);
+    if (h->precision == 32)
+        k_features<float><<<grid, 128, 0, h->stream>>>(h->ns, h->rec, h->rec_n, h->rec_cap, (const float *)h->I,
+                                                       h->I_off, h->dt, d);
+    else
+        k_features<double><<<grid, 128, 0, h->stream>>>(h->ns, h->rec, h->rec_n, h->rec_cap, (const double *)h->I,
+                                                        h->I_off, h->dt, d);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, (size_t)h->ns * 64 * sizeof(float), cudaMemcpyDeviceToHost,
+                                              h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(BG_ECUDA, std::string("fit: features failed: ") + cudaGetErrorString(e));
     return BG_OK;
 }
 

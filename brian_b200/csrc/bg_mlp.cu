@@ -1,0 +1,592 @@
+// bg_mlp.cu -- the learned proposal network for model fitting: a 4-layer MLP
+// (64 -> 512 -> 512 -> 512 -> 10, ReLU) whose output is a diagonal Gaussian
+// over the fitted parameters (5 means, 5 log standard deviations), trained by
+// Gaussian negative log-likelihood with Adam.
+//
+// Every matrix product, forward and backward, runs in one hand-written
+// tcgen05 kernel (bg_umma.cuh) with BF16 operands and FP32 accumulation:
+//
+//   forward   H_l = relu(H_{l-1} W_l^T + b_l)          A = H_{l-1}, B = W_l
+//   backward  G_l = (G_{l+1} W_{l+1}) * [H_l > 0]       A = G_{l+1}, B = W_{l+1}^T
+//             dW_l = G_l^T H_{l-1}                      A = G_l^T,  B = H_{l-1}^T
+//
+// so each layer keeps its activations and gradients in both layouts (the
+// epilogues write the transposed copy), and the weights exist as FP32
+// master copies plus BF16 copies in both layouts, refreshed by the Adam
+// kernel.  The output layer is padded from 10 to 64 rows (zero rows, zero
+// gradients) so every K is a multiple of 64.  Weight gradients split the
+// batch reduction over grid.z and are summed in a fixed order by the Adam
+// kernel (deterministic).
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "bg_common.cuh"
+#include "bg_umma.cuh"
+#include "../../include/brian_b200.h"
+
+namespace {
+
+int fail(int code, const std::string &m) { return bg_internal_fail(code, m.c_str()); }
+
+#define MCK(call)                                                                            \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return fail(BG_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_));       \
+    } while (0)
+
+constexpr int kIn = 64, kHid = 512, kOutPad = 64, kNLayer = 4;
+constexpr int kSplits = 8;
+
+typedef __nv_bfloat16 bf16;
+
+// ------------------------------------------------------------------ kernels
+// Batch rows idx[0..B) of the normalised training set -> X (bf16), X^T, Y.
+__global__ void k_gather(const float *Xall, const float *Yall, const int64_t *idx, int B, int ydim, bf16 *X, bf16 *XT,
+                         float *Y) {
+    const int b = blockIdx.x;
+    const int64_t r = idx[b];
+    for (int j = threadIdx.x; j < kIn; j += blockDim.x) {
+        const bf16 v = __float2bfloat16_rn(Xall[r * kIn + j]);
+        X[(int64_t)b * kIn + j] = v;
+        XT[(int64_t)j * B + b] = v;
+    }
+    for (int j = threadIdx.x; j < ydim; j += blockDim.x) Y[(int64_t)b * ydim + j] = Yall[r * ydim + j];
+}
+
+// Gaussian NLL per sample, mean over the batch:
+//   sum_d 0.5 ((y_d - mu_d) e^{-s_d})^2 + s_d,  s = clamp(log sigma, -7, 7)
+// gradients (already divided by B) into dOUT (bf16, both layouts).
+__global__ void k_nll(const float *OUT, const float *Y, int B, int ydim, bf16 *dO, bf16 *dOT, float *loss_sum) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    float l = 0.f;
+    if (b < B) {
+        const float inv_b = 1.0f / (float)B;
+        for (int j = 0; j < kOutPad; ++j) {
+            float g = 0.f;
+            if (j < ydim) {
+                const float mu = OUT[(int64_t)b * kOutPad + j];
+                const float sr = OUT[(int64_t)b * kOutPad + ydim + j];
+                const float s = fminf(fmaxf(sr, -7.f), 7.f);
+                const float r = (Y[(int64_t)b * ydim + j] - mu) * expf(-s);
+                l += 0.5f * r * r + s;
+                g = -r * expf(-s) * inv_b;                                   // d/d mu
+                const float gs = (sr > -7.f && sr < 7.f) ? (1.f - r * r) * inv_b : 0.f;   // d/d log sigma
+                dO[(int64_t)b * kOutPad + ydim + j] = __float2bfloat16_rn(gs);
+                dOT[(int64_t)(ydim + j) * B + b] = __float2bfloat16_rn(gs);
+            } else if (j >= 2 * ydim) {
+                dO[(int64_t)b * kOutPad + j] = __float2bfloat16_rn(0.f);
+                dOT[(int64_t)j * B + b] = __float2bfloat16_rn(0.f);
+                continue;
+            } else {
+                continue;
+            }
+            dO[(int64_t)b * kOutPad + j] = __float2bfloat16_rn(g);
+            dOT[(int64_t)j * B + b] = __float2bfloat16_rn(g);
+        }
+    }
+    // block sum of the loss
+    __shared__ float red[256];
+    red[threadIdx.x] = l;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) atomicAdd(loss_sum, red[0] / (float)B);
+}
+
+// Row sums of G^T ([N][B]) -> bias gradient, one block per row.
+__global__ void k_rowsum(const bf16 *GT, int B, float *out) {
+    const int n = blockIdx.x;
+    float s = 0.f;
+    for (int b = threadIdx.x; b < B; b += blockDim.x) s += __bfloat162float(GT[(int64_t)n * B + b]);
+    __shared__ float red[256];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+        if ((int)threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[n] = red[0];
+}
+
+// Adam on one parameter tensor [rows][cols] whose gradient is the sum of
+// `splits` partial slices; refreshes the bf16 copy and its transpose.
+__global__ void k_adam(float *W, float *m, float *v, const float *grad, int splits, int64_t split_stride, int rows,
+                       int cols, int rows_train, float lr, float b1, float b2, float eps, float c1, float c2,
+                       bf16 *Wb, bf16 *WbT) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)rows * cols) return;
+    const int r = (int)(i / cols), c = (int)(i % cols);
+    if (r < rows_train) {
+        float g = 0.f;
+        for (int s = 0; s < splits; ++s) g += grad[s * split_stride + i];
+        const float mi = b1 * m[i] + (1.f - b1) * g;
+        const float vi = b2 * v[i] + (1.f - b2) * g * g;
+        m[i] = mi;
+        v[i] = vi;
+        W[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+    const bf16 h = __float2bfloat16_rn(W[i]);
+    if (Wb) Wb[i] = h;
+    if (WbT) WbT[(int64_t)c * rows + r] = h;
+}
+
+__global__ void k_to_bf16(const float *W, int rows, int cols, bf16 *Wb, bf16 *WbT) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)rows * cols) return;
+    const int r = (int)(i / cols), c = (int)(i % cols);
+    const bf16 h = __float2bfloat16_rn(W[i]);
+    Wb[i] = h;
+    if (WbT) WbT[(int64_t)c * rows + r] = h;
+}
+
+template <int NT, int EPI>
+int launch_gemm(const umma::GemmArgs &g, int splits, cudaStream_t st) {
+    static bool attr_set = false;
+    constexpr size_t smem = umma::smem_bytes<NT>();
+    if (!attr_set) {
+        MCK(cudaFuncSetAttribute(umma::k_gemm<NT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = true;
+    }
+    dim3 grid((unsigned)((g.M + umma::kM - 1) / umma::kM), (unsigned)((g.N + NT - 1) / NT), (unsigned)splits);
+    umma::k_gemm<NT, EPI><<<grid, umma::kThreads, smem, st>>>(g);
+    MCK(cudaGetLastError());
+    return BG_OK;
+}
+
+umma::GemmArgs gemm_args(const bf16 *A, int lda, const bf16 *B, int ldb, int M, int N, int K, int *err) {
+    umma::GemmArgs g;
+    memset(&g, 0, sizeof g);
+    g.A = A;
+    g.B = B;
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.lda = lda;
+    g.ldb = ldb;
+    g.k_per_split = K;
+    g.n_valid = N;
+    g.err = err;
+    return g;
+}
+
+template <typename T>
+void dfree(T *&p) {
+    if (p) cudaFree((void *)p);
+    p = nullptr;
+}
+
+template <typename T>
+int dalloc(T **p, size_t n) {
+    dfree(*p);
+    if (n == 0) return BG_OK;
+    if (cudaMalloc((void **)p, n * sizeof(T)) != cudaSuccess) return fail(BG_ENOMEM, "mlp: cudaMalloc failed");
+    cudaMemset(*p, 0, n * sizeof(T));
+    return BG_OK;
+}
+
+}  // namespace
+
+struct bg_mlp {
+    int device = 0;
+    int ydim = 5;
+    cudaStream_t stream = nullptr;
+    int *err = nullptr;
+    // parameters: layer l has W[l] [rows][cols] (fp32 master), b[l]
+    int rows[kNLayer] = {kHid, kHid, kHid, kOutPad};
+    int cols[kNLayer] = {kIn, kHid, kHid, kHid};
+    float *W[kNLayer] = {}, *b[kNLayer] = {}, *mW[kNLayer] = {}, *vW[kNLayer] = {}, *mb[kNLayer] = {},
+          *vb[kNLayer] = {};
+    bf16 *Wb[kNLayer] = {}, *WbT[kNLayer] = {};
+    float *gW = nullptr, *gb = nullptr;   // gradient scratch (largest layer x splits), bias grads
+    int64_t step = 0;
+    // batch buffers
+    int B = 0;
+    bf16 *X = nullptr, *XT = nullptr, *H[3] = {}, *HT[3] = {}, *G[3] = {}, *GT[3] = {}, *dO = nullptr, *dOT = nullptr;
+    float *OUT = nullptr, *Y = nullptr, *loss = nullptr;
+    int64_t *idx = nullptr;
+    // training set
+    int64_t nset = 0;
+    float *Xall = nullptr, *Yall = nullptr;
+};
+
+namespace {
+
+int ensure_batch(bg_mlp *h, int B) {
+    if (B == h->B) return BG_OK;
+    int rc = 0;
+    if ((rc = dalloc(&h->X, (size_t)B * kIn))) return rc;
+    if ((rc = dalloc(&h->XT, (size_t)B * kIn))) return rc;
+    for (int l = 0; l < 3; ++l) {
+        if ((rc = dalloc(&h->H[l], (size_t)B * kHid))) return rc;
+        if ((rc = dalloc(&h->HT[l], (size_t)B * kHid))) return rc;
+        if ((rc = dalloc(&h->G[l], (size_t)B * kHid))) return rc;
+        if ((rc = dalloc(&h->GT[l], (size_t)B * kHid))) return rc;
+    }
+    if ((rc = dalloc(&h->dO, (size_t)B * kOutPad))) return rc;
+    if ((rc = dalloc(&h->dOT, (size_t)B * kOutPad))) return rc;
+    if ((rc = dalloc(&h->OUT, (size_t)B * kOutPad))) return rc;
+    if ((rc = dalloc(&h->Y, (size_t)B * h->ydim))) return rc;
+    if ((rc = dalloc(&h->idx, (size_t)B))) return rc;
+    h->B = B;
+    return BG_OK;
+}
+
+// forward of the batch in h->X -> h->OUT
+int forward(bg_mlp *h, int B) {
+    const bf16 *in = h->X;
+    int K = kIn;
+    for (int l = 0; l < 3; ++l) {
+        umma::GemmArgs g = gemm_args(in, K, h->Wb[l], K, B, kHid, K, h->err);
+        g.bias = h->b[l];
+        g.H = h->H[l];
+        g.ldh = kHid;
+        g.HT = h->HT[l];
+        g.ldht = B;
+        int rc = launch_gemm<128, umma::EPI_RELU_BF16>(g, 1, h->stream);
+        if (rc) return rc;
+        in = h->H[l];
+        K = kHid;
+    }
+    umma::GemmArgs g = gemm_args(in, kHid, h->Wb[3], kHid, B, kOutPad, kHid, h->err);
+    g.bias = h->b[3];
+    g.C = h->OUT;
+    g.ldc = kOutPad;
+    return launch_gemm<64, umma::EPI_BIAS_F32>(g, 1, h->stream);
+}
+
+// backward from the loss gradient in h->dO / h->dOT; weight gradients of
+// layer l into h->gW (split slices) and bias gradients into h->gb, then Adam
+int backward_and_update(bg_mlp *h, int B, float lr, bool update) {
+    int rc = 0;
+    const int splits = B % (kSplits * umma::kKc) == 0 ? kSplits : 1;
+    const int kper = B / splits;
+    const int64_t slice = (int64_t)kHid * kHid;
+    // gradient of the layer input for layers 3, 2, 1 (G[l] = dZ of hidden layer l)
+    const bf16 *gin = h->dO;
+    const bf16 *ginT = h->dOT;
+    int gK = kOutPad;
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    h->step += update ? 1 : 0;
+    const float c1 = 1.f - powf(b1, (float)std::max<int64_t>(h->step, 1));
+    const float c2 = 1.f - powf(b2, (float)std::max<int64_t>(h->step, 1));
+    for (int l = 3; l >= 0; --l) {
+        // dW_l = gin^T . input_l   (input_l = H[l-1] or X)
+        const bf16 *inT = l > 0 ? h->HT[l - 1] : h->XT;
+        const int nin = l > 0 ? kHid : kIn;
+        {
+            umma::GemmArgs g = gemm_args(ginT, B, inT, B, h->rows[l], nin, B, h->err);
+            g.k_per_split = kper;
+            g.C = h->gW;
+            g.ldc = nin;
+            g.split_stride = slice;
+            if (nin == kIn) rc = launch_gemm<64, umma::EPI_F32>(g, splits, h->stream);
+            else rc = launch_gemm<128, umma::EPI_F32>(g, splits, h->stream);
+            if (rc) return rc;
+        }
+        // bias gradient: row sums of gin^T
+        k_rowsum<<<h->rows[l], 256, 0, h->stream>>>(ginT, B, h->gb);
+        MCK(cudaGetLastError());
+        // gradient into the previous hidden layer (needs W_l before its update)
+        if (l > 0) {
+            umma::GemmArgs g = gemm_args(gin, gK, h->WbT[l], h->rows[l], B, kHid, gK, h->err);
+            g.act = h->H[l - 1];
+            g.ldact = kHid;
+            g.H = h->G[l - 1];
+            g.ldh = kHid;
+            g.HT = h->GT[l - 1];
+            g.ldht = B;
+            if ((rc = launch_gemm<128, umma::EPI_DRELU_BF16>(g, 1, h->stream))) return rc;
+        }
+        if (update) {
+            const int rows_train = l == 3 ? 2 * h->ydim : h->rows[l];
+            const int64_t n = (int64_t)h->rows[l] * h->cols[l];
+            k_adam<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(
+                h->W[l], h->mW[l], h->vW[l], h->gW, splits, slice, h->rows[l], h->cols[l], rows_train, lr, b1, b2,
+                eps, c1, c2, h->Wb[l], h->WbT[l]);
+            k_adam<<<(unsigned)((h->rows[l] + 255) / 256), 256, 0, h->stream>>>(
+                h->b[l], h->mb[l], h->vb[l], h->gb, 1, 0, h->rows[l], 1, rows_train, lr, b1, b2, eps, c1, c2,
+                nullptr, nullptr);
+            MCK(cudaGetLastError());
+        }
+        if (l > 0) {
+            gin = h->G[l - 1];
+            ginT = h->GT[l - 1];
+            gK = kHid;
+        }
+    }
+    return BG_OK;
+}
+
+int check_err(bg_mlp *h) {
+    int e = 0;
+    MCK(cudaMemcpy(&e, h->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) return fail(BG_ETIMEOUT, "mlp: a tensor-core wait gave up");
+    return BG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+BG_API int bg_mlp_create(bg_mlp **out, int device, int ydim) {
+    if (!out || ydim <= 0 || 2 * ydim > kOutPad) return fail(BG_EINVAL, "mlp: bad arguments");
+    *out = nullptr;
+    MCK(cudaSetDevice(device));
+    bg_mlp *h = new bg_mlp();
+    h->device = device;
+    h->ydim = ydim;
+    int rc = 0;
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) rc = fail(BG_ECUDA, "mlp: stream");
+    if (!rc) rc = dalloc(&h->err, 1);
+    for (int l = 0; l < kNLayer && !rc; ++l) {
+        const size_t n = (size_t)h->rows[l] * h->cols[l];
+        if (!rc) rc = dalloc(&h->W[l], n);
+        if (!rc) rc = dalloc(&h->mW[l], n);
+        if (!rc) rc = dalloc(&h->vW[l], n);
+        if (!rc) rc = dalloc(&h->b[l], (size_t)h->rows[l]);
+        if (!rc) rc = dalloc(&h->mb[l], (size_t)h->rows[l]);
+        if (!rc) rc = dalloc(&h->vb[l], (size_t)h->rows[l]);
+        if (!rc) rc = dalloc(&h->Wb[l], n);
+        if (!rc) rc = dalloc(&h->WbT[l], n);
+    }
+    if (!rc) rc = dalloc(&h->gW, (size_t)kSplits * kHid * kHid);
+    if (!rc) rc = dalloc(&h->gb, (size_t)kHid);
+    if (!rc) rc = dalloc(&h->loss, 1);
+    if (rc) {
+        bg_mlp_destroy(h);
+        return rc;
+    }
+    *out = h;
+    return BG_OK;
+}
+
+BG_API int bg_mlp_destroy(bg_mlp *h) {
+    if (!h) return BG_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (int l = 0; l < kNLayer; ++l) {
+        dfree(h->W[l]); dfree(h->b[l]); dfree(h->mW[l]); dfree(h->vW[l]); dfree(h->mb[l]); dfree(h->vb[l]);
+        dfree(h->Wb[l]); dfree(h->WbT[l]);
+    }
+    for (int l = 0; l < 3; ++l) { dfree(h->H[l]); dfree(h->HT[l]); dfree(h->G[l]); dfree(h->GT[l]); }
+    dfree(h->X); dfree(h->XT); dfree(h->dO); dfree(h->dOT); dfree(h->OUT); dfree(h->Y); dfree(h->idx);
+    dfree(h->gW); dfree(h->gb); dfree(h->loss); dfree(h->err); dfree(h->Xall); dfree(h->Yall);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return BG_OK;
+}
+
+BG_API int bg_mlp_set_params(bg_mlp *h, int layer, const float *W, const float *b) {
+    if (!h || layer < 0 || layer >= kNLayer || !W || !b) return fail(BG_EINVAL, "mlp: bad parameter set");
+    MCK(cudaSetDevice(h->device));
+    const size_t n = (size_t)h->rows[layer] * h->cols[layer];
+    MCK(cudaMemcpy(h->W[layer], W, n * sizeof(float), cudaMemcpyHostToDevice));
+    MCK(cudaMemcpy(h->b[layer], b, (size_t)h->rows[layer] * sizeof(float), cudaMemcpyHostToDevice));
+    MCK(cudaMemset(h->mW[layer], 0, n * sizeof(float)));
+    MCK(cudaMemset(h->vW[layer], 0, n * sizeof(float)));
+    MCK(cudaMemset(h->mb[layer], 0, (size_t)h->rows[layer] * sizeof(float)));
+    MCK(cudaMemset(h->vb[layer], 0, (size_t)h->rows[layer] * sizeof(float)));
+    k_to_bf16<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->W[layer], h->rows[layer], h->cols[layer],
+                                                                    h->Wb[layer], h->WbT[layer]);
+    MCK(cudaGetLastError());
+    MCK(cudaStreamSynchronize(h->stream));
+    h->step = 0;
+    return BG_OK;
+}
+
+BG_API int bg_mlp_get_params(bg_mlp *h, int layer, float *W, float *b) {
+    if (!h || layer < 0 || layer >= kNLayer) return fail(BG_EINVAL, "mlp: bad layer");
+    MCK(cudaSetDevice(h->device));
+    MCK(cudaStreamSynchronize(h->stream));
+    if (W) MCK(cudaMemcpy(W, h->W[layer], (size_t)h->rows[layer] * h->cols[layer] * sizeof(float),
+                          cudaMemcpyDeviceToHost));
+    if (b) MCK(cudaMemcpy(b, h->b[layer], (size_t)h->rows[layer] * sizeof(float), cudaMemcpyDeviceToHost));
+    return BG_OK;
+}
+
+BG_API int bg_mlp_forward(bg_mlp *h, const float *X, int64_t n, float *out) {
+    if (!h || !X || n <= 0 || !out) return fail(BG_EINVAL, "mlp: bad forward call");
+    MCK(cudaSetDevice(h->device));
+    const int B = (int)((n + 127) / 128 * 128);
+    int rc = ensure_batch(h, B);
+    if (rc) return rc;
+    std::vector<bf16> xb((size_t)B * kIn, __float2bfloat16_rn(0.f)), xt((size_t)B * kIn, __float2bfloat16_rn(0.f));
+    for (int64_t r = 0; r < n; ++r)
+        for (int j = 0; j < kIn; ++j) {
+            const bf16 v = __float2bfloat16_rn(X[r * kIn + j]);
+            xb[(size_t)r * kIn + j] = v;
+            xt[(size_t)j * B + r] = v;
+        }
+    MCK(cudaMemcpyAsync(h->X, xb.data(), xb.size() * sizeof(bf16), cudaMemcpyHostToDevice, h->stream));
+    MCK(cudaMemcpyAsync(h->XT, xt.data(), xt.size() * sizeof(bf16), cudaMemcpyHostToDevice, h->stream));
+    if ((rc = forward(h, B))) return rc;
+    std::vector<float> o((size_t)B * kOutPad);
+    MCK(cudaMemcpyAsync(o.data(), h->OUT, o.size() * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    MCK(cudaStreamSynchronize(h->stream));
+    if ((rc = check_err(h))) return rc;
+    for (int64_t r = 0; r < n; ++r)
+        for (int j = 0; j < 2 * h->ydim; ++j) out[r * 2 * h->ydim + j] = o[(size_t)r * kOutPad + j];
+    return BG_OK;
+}
+
+BG_API int bg_mlp_set_data(bg_mlp *h, const float *X, const float *Y, int64_t n) {
+    if (!h || !X || !Y || n <= 0) return fail(BG_EINVAL, "mlp: bad training set");
+    MCK(cudaSetDevice(h->device));
+    int rc = dalloc(&h->Xall, (size_t)n * kIn);
+    if (!rc) rc = dalloc(&h->Yall, (size_t)n * h->ydim);
+    if (rc) return rc;
+    MCK(cudaMemcpy(h->Xall, X, (size_t)n * kIn * sizeof(float), cudaMemcpyHostToDevice));
+    MCK(cudaMemcpy(h->Yall, Y, (size_t)n * h->ydim * sizeof(float), cudaMemcpyHostToDevice));
+    h->nset = n;
+    return BG_OK;
+}
+
+BG_API int bg_mlp_train(bg_mlp *h, int epochs, int batch, float lr, uint64_t seed, float *epoch_loss,
+                        float *gpu_ms) {
+    if (!h || epochs < 0 || batch < 128 || batch % 128 != 0 || (batch / kSplits) % umma::kKc != 0)
+        return fail(BG_EINVAL, "mlp: batch must be a multiple of 512 (128 rows x 8 batch splits of 64)");
+    if (h->nset < batch) return fail(BG_ESTATE, "mlp: training set smaller than one batch");
+    MCK(cudaSetDevice(h->device));
+    int rc = ensure_batch(h, batch);
+    if (rc) return rc;
+    const int64_t steps = h->nset / batch;
+    std::vector<int64_t> perm(h->nset);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, h->stream);
+    for (int ep = 0; ep < epochs && !rc; ++ep) {
+        // epoch permutation from a Philox stream keyed (seed, epoch)
+        for (int64_t i = 0; i < h->nset; ++i) perm[i] = i;
+        for (int64_t i = h->nset - 1; i > 0; --i) {
+            const int64_t j = (int64_t)(bg_philox_uniform(seed, ep, i) * (double)(i + 1));
+            std::swap(perm[i], perm[std::min(j, i)]);
+        }
+        int64_t *dperm = nullptr;
+        if (cudaMalloc((void **)&dperm, (size_t)steps * batch * sizeof(int64_t)) != cudaSuccess) {
+            rc = fail(BG_ENOMEM, "mlp: cudaMalloc failed");
+            break;
+        }
+        cudaMemcpyAsync(dperm, perm.data(), (size_t)steps * batch * sizeof(int64_t), cudaMemcpyHostToDevice,
+                        h->stream);
+        cudaMemsetAsync(h->loss, 0, sizeof(float), h->stream);
+        for (int64_t s = 0; s < steps && !rc; ++s) {
+            k_gather<<<batch, 64, 0, h->stream>>>(h->Xall, h->Yall, dperm + s * batch, batch, h->ydim, h->X, h->XT,
+                                                h->Y);
+            if ((rc = forward(h, batch))) break;
+            k_nll<<<(batch + 255) / 256, 256, 0, h->stream>>>(h->OUT, h->Y, batch, h->ydim, h->dO, h->dOT, h->loss);
+            rc = backward_and_update(h, batch, lr, true);
+        }
+        float ls = 0;
+        cudaMemcpyAsync(&ls, h->loss, sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+        cudaError_t e = cudaStreamSynchronize(h->stream);
+        cudaFree(dperm);
+        if (!rc && e != cudaSuccess) rc = fail(BG_ECUDA, std::string("mlp: training failed: ") + cudaGetErrorString(e));
+        if (!rc) rc = check_err(h);
+        if (epoch_loss) epoch_loss[ep] = ls / (float)steps;
+    }
+    cudaEventRecord(e1, h->stream);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (gpu_ms) *gpu_ms = ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
+}
+
+// One forward + backward on the first `n` rows of the training set (no
+// update), for gradient checks: loss, dW_l (summed) and db_l of every layer.
+BG_API int bg_mlp_gradients(bg_mlp *h, int batch, float *loss, float *const *dW, float *const *db) {
+    if (!h || batch < 128 || batch % 512 != 0 || h->nset < batch) return fail(BG_EINVAL, "mlp: bad gradient call");
+    MCK(cudaSetDevice(h->device));
+    int rc = ensure_batch(h, batch);
+    if (rc) return rc;
+    std::vector<int64_t> idx(batch);
+    for (int i = 0; i < batch; ++i) idx[i] = i;
+    MCK(cudaMemcpyAsync(h->idx, idx.data(), batch * sizeof(int64_t), cudaMemcpyHostToDevice, h->stream));
+    MCK(cudaMemsetAsync(h->loss, 0, sizeof(float), h->stream));
+    k_gather<<<batch, 64, 0, h->stream>>>(h->Xall, h->Yall, h->idx, batch, h->ydim, h->X, h->XT, h->Y);
+    if ((rc = forward(h, batch))) return rc;
+    k_nll<<<(batch + 255) / 256, 256, 0, h->stream>>>(h->OUT, h->Y, batch, h->ydim, h->dO, h->dOT, h->loss);
+    // run the backward pass layer by layer, reading each layer's gradient
+    // before the next layer reuses the scratch
+    const int splits = kSplits;
+    const int kper = batch / splits;
+    const bf16 *gin = h->dO, *ginT = h->dOT;
+    int gK = kOutPad;
+    for (int l = 3; l >= 0; --l) {
+        const bf16 *inT = l > 0 ? h->HT[l - 1] : h->XT;
+        const int nin = l > 0 ? kHid : kIn;
+        umma::GemmArgs g = gemm_args(ginT, batch, inT, batch, h->rows[l], nin, batch, h->err);
+        g.k_per_split = kper;
+        g.C = h->gW;
+        g.ldc = nin;
+        g.split_stride = (int64_t)kHid * kHid;
+        rc = nin == kIn ? launch_gemm<64, umma::EPI_F32>(g, splits, h->stream)
+                        : launch_gemm<128, umma::EPI_F32>(g, splits, h->stream);
+        if (rc) return rc;
+        k_rowsum<<<h->rows[l], 256, 0, h->stream>>>(ginT, batch, h->gb);
+        std::vector<float> part((size_t)splits * kHid * kHid);
+        MCK(cudaMemcpyAsync(part.data(), h->gW, part.size() * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+        MCK(cudaStreamSynchronize(h->stream));
+        const size_t n = (size_t)h->rows[l] * nin;
+        if (dW && dW[l])
+            for (size_t i = 0; i < n; ++i) {
+                float s = 0;
+                for (int z = 0; z < splits; ++z) s += part[(size_t)z * kHid * kHid + i];
+                dW[l][i] = s;
+            }
+        if (db && db[l]) MCK(cudaMemcpy(db[l], h->gb, (size_t)h->rows[l] * sizeof(float), cudaMemcpyDeviceToHost));
+        if (l > 0) {
+            umma::GemmArgs g2 = gemm_args(gin, gK, h->WbT[l], h->rows[l], batch, kHid, gK, h->err);
+            g2.act = h->H[l - 1];
+            g2.ldact = kHid;
+            g2.H = h->G[l - 1];
+            g2.ldh = kHid;
+            g2.HT = h->GT[l - 1];
+            g2.ldht = batch;
+            if ((rc = launch_gemm<128, umma::EPI_DRELU_BF16>(g2, 1, h->stream))) return rc;
+            gin = h->G[l - 1];
+            ginT = h->GT[l - 1];
+            gK = kHid;
+        }
+    }
+    if (loss) MCK(cudaMemcpy(loss, h->loss, sizeof(float), cudaMemcpyDeviceToHost));
+    MCK(cudaStreamSynchronize(h->stream));
+    return check_err(h);
+}
+
+// Plain GEMM on device buffers: C[M][N] = A[M][K] . B[N][K]^T (bf16 in,
+// fp32 out), K a multiple of 64; the tensor-core kernel of the network.
+BG_API int bg_gemm_bf16(int64_t M, int64_t N, int64_t K, const void *A, const void *B, float *C, void *stream) {
+    if (M <= 0 || N <= 0 || K <= 0 || K % 64 != 0 || !A || !B || !C) return fail(BG_EINVAL, "gemm: bad shape");
+    int *err = nullptr;
+    MCK(cudaMalloc((void **)&err, sizeof(int)));
+    MCK(cudaMemset(err, 0, sizeof(int)));
+    cudaStream_t st = (cudaStream_t)stream;
+    umma::GemmArgs g = gemm_args((const bf16 *)A, (int)K, (const bf16 *)B, (int)K, (int)M, (int)N, (int)K, err);
+    g.C = C;
+    g.ldc = (int)N;
+    int rc = launch_gemm<128, umma::EPI_F32>(g, 1, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    int ev = 0;
+    cudaMemcpy(&ev, err, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(err);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(BG_ECUDA, std::string("gemm: ") + cudaGetErrorString(e));
+    if (ev) return fail(BG_ETIMEOUT, "gemm: a tensor-core wait gave up");
+    return BG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,296 @@
+// bg_umma.cuh -- BF16 GEMM on the 5th-generation tensor cores (tcgen05) for
+// the learned proposal network.
+//
+//   C[M, N] = A[M, K] . B[N, K]^T      A, B bf16, both K-major (rows of K
+//                                      contiguous), accumulation FP32 in TMEM
+//
+// One CTA of 128 threads computes a 128 x NT tile.  The K dimension is
+// streamed in chunks of 64 through a 3-stage ring of shared-memory tiles
+// filled with cp.async (16-byte pieces; rows past M or N are zero-filled).
+// Tiles use the canonical K-major layout without swizzle: 8-row x 16-byte
+// core matrices, core matrices along K 128 bytes apart (leading byte offset)
+// and 8-row groups 1024 bytes apart (stride byte offset).  Thread 0 issues
+// four tcgen05.mma (K = 16 each) per chunk and commits them to the chunk's
+// mbarrier; a stage is refilled only after that mbarrier completes.  The
+// accumulator lives in TMEM (lane = tile row, one column per output column)
+// and is read back by every warp for its 32 rows with tcgen05.ld; the
+// epilogue is fused (bias, ReLU, ReLU gradient, transposed copies).
+//
+// Every wait on an mbarrier is bounded; a wait that gives up records an
+// error code and the CTA leaves after releasing its TMEM.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cstdint>
+
+namespace umma {
+
+constexpr int kM = 128;          // rows per CTA tile (UMMA M)
+constexpr int kKc = 64;          // K elements per stage
+constexpr int kStages = 3;
+constexpr int kThreads = 128;
+constexpr uint32_t kLBO = 128;   // bytes between core matrices along K
+constexpr uint32_t kSBO = 1024;  // bytes between 8-row groups
+constexpr long long kSpinLimit = 1ll << 24;
+
+enum Epi : int {
+    EPI_F32 = 0,        // C fp32 (optionally per split), no bias
+    EPI_BIAS_F32 = 1,   // C fp32 = acc + bias[n]
+    EPI_RELU_BF16 = 2,  // H bf16 = relu(acc + bias[n]), and H^T
+    EPI_DRELU_BF16 = 3  // G bf16 = acc * (act[m][n] > 0), and G^T
+};
+
+struct GemmArgs {
+    const __nv_bfloat16 *A;   // [M][lda]
+    const __nv_bfloat16 *B;   // [N][ldb]
+    int M, N, K, lda, ldb;
+    int k_per_split;          // K range of one grid.z slice (multiple of kKc)
+    float *C;                 // fp32 out [split][M][ldc]
+    int ldc;
+    long long split_stride;   // elements between split slices of C
+    const float *bias;        // [N] or null
+    __nv_bfloat16 *H;         // bf16 out [M][ldh]
+    int ldh;
+    __nv_bfloat16 *HT;        // bf16 transposed out [N][ldht] or null
+    int ldht;
+    const __nv_bfloat16 *act; // [M][ldact] for EPI_DRELU_BF16
+    int ldact;
+    int n_valid;              // columns >= n_valid are written as 0 (bf16 outs) / skipped (fp32)
+    int *err;                 // error flag (device)
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((kLBO >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((kSBO >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;   // sm100 descriptor version; base offset 0, no swizzle
+    return d;
+}
+
+// kind::f16 instruction descriptor: D f32, A bf16, B bf16, both K-major.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ uint32_t tile_off(int r, int q) {
+    return (uint32_t)((r >> 3) * kSBO + q * kLBO + (r & 7) * 16);
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, bool valid) {
+    const int n = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+
+// Bounded wait for the completion of phase `parity`; false when it gave up.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (long long i = 0; i < kSpinLimit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.b32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Shared memory of one CTA: the stage ring, the mbarriers, the TMEM base.
+template <int NT>
+struct Smem {
+    alignas(1024) unsigned char a[kStages][kM * kKc * 2];
+    alignas(1024) unsigned char b[kStages][NT * kKc * 2];
+    alignas(8) unsigned long long bar[kStages];
+    uint32_t tmem_base;
+    int failed;
+};
+
+template <int NT>
+__device__ __forceinline__ void load_stage(Smem<NT> &sm, int st, const GemmArgs &g, int m0, int n0, int k0) {
+    const int tid = threadIdx.x;
+    const uint32_t a_base = smem_u32(sm.a[st]);
+    const uint32_t b_base = smem_u32(sm.b[st]);
+    // A: 128 rows x 8 pieces of 16 bytes
+#pragma unroll
+    for (int p = tid; p < kM * 8; p += kThreads) {
+        const int r = p >> 3, q = p & 7;
+        const int row = m0 + r;
+        const bool ok = row < g.M;
+        const __nv_bfloat16 *src = g.A + (long long)(ok ? row : 0) * g.lda + k0 + q * 8;
+        cp_async16(a_base + tile_off(r, q), src, ok);
+    }
+#pragma unroll
+    for (int p = tid; p < NT * 8; p += kThreads) {
+        const int r = p >> 3, q = p & 7;
+        const int row = n0 + r;
+        const bool ok = row < g.N;
+        const __nv_bfloat16 *src = g.B + (long long)(ok ? row : 0) * g.ldb + k0 + q * 8;
+        cp_async16(b_base + tile_off(r, q), src, ok);
+    }
+}
+
+template <int NT, int EPI>
+__global__ void __launch_bounds__(kThreads, 1) k_gemm(const GemmArgs g) {
+    extern __shared__ unsigned char smem_raw[];
+    Smem<NT> &sm = *reinterpret_cast<Smem<NT> *>(
+        (void *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023));
+    constexpr uint32_t kCols = NT < 32 ? 32 : NT;   // TMEM columns: power of two >= 32
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.x * kM, n0 = blockIdx.y * NT;
+    const int kbeg = blockIdx.z * g.k_per_split;
+    const int kend = min(g.K, kbeg + g.k_per_split);
+    const int nk = (kend - kbeg) / kKc;
+
+    if (tid == 0) {
+        for (int s = 0; s < kStages; ++s) mbar_init(smem_u32(&sm.bar[s]), 1);
+        sm.failed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&sm.tmem_base)),
+                     "r"(kCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = sm.tmem_base;
+    constexpr uint32_t idesc = idesc_bf16(kM, NT);
+
+    // prologue: chunks 0 .. kStages-2
+#pragma unroll
+    for (int s = 0; s < kStages - 1; ++s) {
+        if (s < nk) load_stage(sm, s, g, m0, n0, kbeg + s * kKc);
+        cp_async_commit();
+    }
+    bool ok = true;
+    for (int c = 0; c < nk; ++c) {
+        const int lc = c + kStages - 1;
+        if (lc < nk) {
+            const int st = lc % kStages;
+            if (lc >= kStages) {
+                // the MMAs of chunk lc - kStages read this stage
+                if (!mbar_wait(smem_u32(&sm.bar[st]), (uint32_t)(((lc - kStages) / kStages) & 1))) ok = false;
+            }
+            load_stage(sm, st, g, m0, n0, kbeg + lc * kKc);
+        }
+        cp_async_commit();
+        cp_async_wait<kStages - 1>();
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        if (!ok) atomicExch(&sm.failed, 1);
+        __syncthreads();
+        if (sm.failed) break;
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const int st = c % kStages;
+            const uint32_t a_addr = smem_u32(sm.a[st]), b_addr = smem_u32(sm.b[st]);
+#pragma unroll
+            for (int j = 0; j < kKc / 16; ++j)
+                umma_bf16(tmem, smem_desc(a_addr + j * 2 * kLBO), smem_desc(b_addr + j * 2 * kLBO), idesc,
+                          (c > 0 || j > 0) ? 1u : 0u);
+            umma_commit(smem_u32(&sm.bar[st]));
+        }
+    }
+    // all MMAs done: the last commit covers every earlier one
+    if (!sm.failed && nk > 0) {
+        const int st = (nk - 1) % kStages;
+        if (!mbar_wait(smem_u32(&sm.bar[st]), (uint32_t)(((nk - 1) / kStages) & 1))) atomicExch(&sm.failed, 1);
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (sm.failed) {
+        if (tid == 0 && g.err) atomicExch(g.err, 1);
+    } else {
+        // epilogue: warp w owns tile rows 32w .. 32w+31, TMEM lanes alike
+        const int row = m0 + warp * 32 + lane;
+        const bool row_ok = row < g.M;
+        float *Cz = g.C ? g.C + (long long)blockIdx.z * g.split_stride : nullptr;
+#pragma unroll 1
+        for (int cb = 0; cb < NT; cb += 16) {
+            float v[16];
+            if (nk > 0) {
+                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb, v);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) v[i] = 0.f;
+            }
+            if (!row_ok) continue;
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const int col = n0 + cb + i;
+                if (col >= g.N) continue;
+                float x = v[i];
+                if (EPI == EPI_F32) {
+                    if (col < g.n_valid) Cz[(long long)row * g.ldc + col] = x;
+                } else if (EPI == EPI_BIAS_F32) {
+                    if (col < g.n_valid) Cz[(long long)row * g.ldc + col] = x + g.bias[col];
+                } else {
+                    if (EPI == EPI_RELU_BF16) {
+                        x = x + g.bias[col];
+                        x = x > 0.f ? x : 0.f;
+                    } else {
+                        const float a = __bfloat162float(g.act[(long long)row * g.ldact + col]);
+                        x = a > 0.f ? x : 0.f;
+                    }
+                    if (col >= g.n_valid) x = 0.f;
+                    const __nv_bfloat16 h = __float2bfloat16_rn(x);
+                    g.H[(long long)row * g.ldh + col] = h;
+                    if (g.HT) g.HT[(long long)col * g.ldht + row] = h;
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kCols) : "memory");
+    }
+}
+
+template <int NT>
+constexpr size_t smem_bytes() {
+    return sizeof(Smem<NT>) + 1024;
+}
+
+}  // namespace umma

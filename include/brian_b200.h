@@ -313,6 +313,12 @@ BG_API int bg_fit_run(bg_fit *h, int32_t Tstart, int32_t Tend);
 BG_API int bg_fit_read(bg_fit *h, int32_t *coinc, int32_t *nspikes, double *state);
 /* Recorded spikes: counts[nsims] (may exceed cap), steps[nsims][cap]. */
 BG_API int bg_fit_read_spikes(bg_fit *h, int32_t *counts, int32_t *steps);
+/* Features of every simulation's recorded spikes and its input, out
+ * [nsims][64] (the learned proposal's input): 32-bin log-ISI histogram over
+ * [1 ms, 2 s), firing rate (statistics.py:15-21), CV (statistics.py:23-30)
+ * and a 30-bin spike-triggered average of the input in nA over 30 ms
+ * (statistics.py:125-153).  Needs bg_fit_set_record. */
+BG_API int bg_fit_features(bg_fit *h, float *out);
 /* Gamma factor inputs (ModelFitting.prepare_data, modelfitting.py:117-173):
  * nparticles x slices = nsims (simulation i is particle i % nparticles),
  * per particle the target train's length and rate (firing_rate), delta in
@@ -357,6 +363,41 @@ BG_API int bg_fit_pso_state(bg_fit *h, double *X, double *V, double *X_lbest,
 /* out[0..n): last simulation launch (GPU ms), launches, neuron-steps of one
  * full run, longest simulation (steps). */
 BG_API int bg_fit_stats(bg_fit *h, double *out, int n);
+
+/* ---- learned proposal network ----------------------------------------------
+ * A 4-layer MLP (64 -> 512 -> 512 -> 512 -> 2*ydim, ReLU) whose output is a
+ * diagonal Gaussian (ydim means, ydim log standard deviations) over the
+ * normalised fitted parameters; it proposes starting points for the swarm
+ * (no reference counterpart: the reference starts its optimisers from
+ * uniform draws, modelfitting.py:479-516).  Matrix products run on the
+ * tensor cores (tcgen05, BF16 operands, FP32 accumulation); the loss is the
+ * Gaussian negative log-likelihood, the optimiser Adam. */
+typedef struct bg_mlp bg_mlp;
+BG_API int bg_mlp_create(bg_mlp **out, int device, int ydim);
+BG_API int bg_mlp_destroy(bg_mlp *h);
+/* Layer l (0..3) parameters, fp32 row-major W[rows][cols], b[rows]; rows =
+ * 512, 512, 512, 64 (the output layer padded with zero rows), cols = 64,
+ * 512, 512, 512.  Setting resets the optimiser state of the layer. */
+BG_API int bg_mlp_set_params(bg_mlp *h, int layer, const float *W, const float *b);
+BG_API int bg_mlp_get_params(bg_mlp *h, int layer, float *W, float *b);
+/* out[n][2*ydim] = network(X[n][64]). */
+BG_API int bg_mlp_forward(bg_mlp *h, const float *X, int64_t n, float *out);
+/* Training set: X[n][64] features, Y[n][ydim] targets (already normalised). */
+BG_API int bg_mlp_set_data(bg_mlp *h, const float *X, const float *Y, int64_t n);
+/* `epochs` passes of mini-batch Adam (batch a multiple of 512); the batch
+ * order of each epoch comes from Philox keyed (seed, epoch).  epoch_loss
+ * [epochs] and gpu_ms (nullable) report the mean loss and device time. */
+BG_API int bg_mlp_train(bg_mlp *h, int epochs, int batch, float lr, uint64_t seed,
+                        float *epoch_loss, float *gpu_ms);
+/* Loss and gradients on the first `batch` training rows without an update
+ * (dW[l] [rows][cols], db[l] [rows]; entries may be NULL). */
+BG_API int bg_mlp_gradients(bg_mlp *h, int batch, float *loss, float *const *dW,
+                            float *const *db);
+/* C[M][N] = A[M][K] . B[N][K]^T on device buffers: A, B bf16 row-major, C
+ * fp32, K a multiple of 64; runs on `stream` (a cudaStream_t, NULL =
+ * default) and returns when done. */
+BG_API int bg_gemm_bf16(int64_t M, int64_t N, int64_t K, const void *A, const void *B,
+                        float *C, void *stream);
 
 #ifdef __cplusplus
 }
