@@ -74,6 +74,9 @@ ENGINE_ONLY = {
     "fit_set_params": [_vp, _i32, _vp],
     "fit_evaluate": [_vp, _vp, _vp],
     "fit_features": [_vp, _vp],
+    "fit_train_features": [_vp, _i64, _vp, _vp, _vp, _vp, _P(ct.c_float)],
+    "mlp_last_forward_ms": [_vp, _P(ct.c_float)],
+    "spike_features": [ct.c_int, _i64, _vp, _vp, _vp, _vp, _i64, _dbl, _vp],
     "fit_set_blocks_per_sm": [_vp, _i32],
     "mlp_create": [_P(_vp), ct.c_int, ct.c_int],
     "mlp_destroy": [_vp],
@@ -445,6 +448,21 @@ class FitHandle(object):
         self._c(self.t.fit_features(self.h, _ptr(out)), "fit_features")
         return out
 
+    def train_features(self, trains_steps, I_offset):
+        """Features of given trains (clock steps) whose inputs start at
+        I_offset in this handle's input; returns (features, device ms)."""
+        steps = np.concatenate([np.asarray(x, dtype=np.int32) for x in trains_steps]) if len(trains_steps) else \
+            np.zeros(0, np.int32)
+        if len(steps) == 0:
+            steps = np.zeros(1, np.int32)
+        offs = np.concatenate([[0], np.cumsum([len(x) for x in trains_steps])]).astype(np.int64)
+        ioff = np.ascontiguousarray(I_offset, dtype=np.int64)
+        out = np.empty((len(trains_steps), 64), dtype=np.float32)
+        ms = ct.c_float()
+        self._c(self.t.fit_train_features(self.h, len(trains_steps), _ptr(steps), _ptr(offs), _ptr(ioff), _ptr(out),
+                                          ct.byref(ms)), "fit_train_features")
+        return out, ms.value
+
     def set_blocks_per_sm(self, b):
         self._c(self.t.fit_set_blocks_per_sm(self.h, int(b)), "fit_set_blocks_per_sm")
 
@@ -489,10 +507,10 @@ class FitHandle(object):
         return X, V, Xl, fl
 
     def stats(self):
-        out = np.zeros(4)
-        self._c(self.t.fit_stats(self.h, _ptr(out), 4), "fit_stats")
+        out = np.zeros(5)
+        self._c(self.t.fit_stats(self.h, _ptr(out), 5), "fit_stats")
         return {"last_sim_ms": out[0], "sim_launches": int(out[1]), "neuron_steps": int(out[2]),
-                "max_steps": int(out[3])}
+                "max_steps": int(out[3]), "last_eval_ms": out[4]}
 
 
 def fit_compile_check(code, dt, delta_steps, exclusive=True, precision=64):
@@ -551,6 +569,11 @@ class MLPHandle(object):
         self._c(self.t.mlp_forward(self.h, _ptr(X), len(X), _ptr(out)), "mlp_forward")
         return out
 
+    def last_forward_ms(self):
+        ms = ct.c_float()
+        self._c(self.t.mlp_last_forward_ms(self.h, ct.byref(ms)), "mlp_last_forward_ms")
+        return ms.value
+
     def set_data(self, X, Y):
         X = np.ascontiguousarray(X, dtype=np.float32)
         Y = np.ascontiguousarray(Y, dtype=np.float32)
@@ -571,3 +594,19 @@ class MLPHandle(object):
         loss = ct.c_float()
         self._c(self.t.mlp_gradients(self.h, int(batch), ct.byref(loss), pW, pb), "mlp_gradients")
         return loss.value, dW, db
+
+
+def spike_features(trains_steps, inputs, dt, device=0):
+    """Features of given trains (lists of clock steps) with their inputs."""
+    t = product_table()
+    steps = np.ascontiguousarray(np.concatenate([np.asarray(x, dtype=np.int32) for x in trains_steps])
+                                 if len(trains_steps) else np.zeros(0, np.int32), dtype=np.int32)
+    offs = np.concatenate([[0], np.cumsum([len(x) for x in trains_steps])]).astype(np.int64)
+    I = np.ascontiguousarray(np.concatenate([np.asarray(x, dtype=np.float64) for x in inputs]))
+    ioff = np.concatenate([[0], np.cumsum([len(x) for x in inputs])[:-1]]).astype(np.int64)
+    out = np.empty((len(trains_steps), 64), dtype=np.float32)
+    if len(steps) == 0:
+        steps = np.zeros(1, np.int32)
+    t.check(t.spike_features(int(device), len(trains_steps), _ptr(steps), _ptr(offs), _ptr(I), _ptr(ioff), len(I),
+                             float(dt), _ptr(out)), "spike_features")
+    return out

@@ -19,6 +19,8 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <numeric>
 #include <sstream>
 #include <string>
@@ -134,7 +136,20 @@ int assemble_source(int precision, const bg_fit_model *model, double dt, int del
     return BG_OK;
 }
 
+// Compiled kernels of this process, keyed by their full source.
+std::mutex g_cubin_mutex;
+std::map<std::string, std::vector<char>> g_cubins;
+
 int nvrtc_compile(const std::string &src, std::vector<char> *cubin, std::string *log) {
+    {
+        std::lock_guard<std::mutex> lock(g_cubin_mutex);
+        auto it = g_cubins.find(src);
+        if (it != g_cubins.end()) {
+            *cubin = it->second;
+            log->clear();
+            return BG_OK;
+        }
+    }
     nvrtcProgram prog;
     if (nvrtcCreateProgram(&prog, src.c_str(), "bg_fit_model.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS)
         return fail(BG_ECOMPILE, "nvrtcCreateProgram failed");
@@ -157,6 +172,8 @@ int nvrtc_compile(const std::string &src, std::vector<char> *cubin, std::string 
     cubin->resize(n);
     nvrtcGetCUBIN(prog, cubin->data());
     nvrtcDestroyProgram(&prog);
+    std::lock_guard<std::mutex> lock(g_cubin_mutex);
+    g_cubins[src] = *cubin;
     return BG_OK;
 }
 
@@ -210,6 +227,7 @@ struct bg_fit {
     int64_t iter = 0;
     bool pso_ready = false;
     float last_sim_ms = 0;
+    float last_eval_ms = 0;     // whole evaluation (prepare, simulate, gamma, bests)
     int64_t sim_launches = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
@@ -771,6 +789,122 @@ BG_API int bg_fit_features(bg_fit *h, float *out) {
     return BG_OK;
 }
 
+BG_API int bg_spike_features(int device, int64_t ntrains, const int32_t *steps, const int64_t *offsets,
+                             const double *I, const int64_t *I_offset, int64_t ninput, double dt, float *out) {
+    if (ntrains <= 0 || !steps || !offsets || !I || !I_offset || ninput <= 0 || !out || !(dt > 0))
+        return fail(BG_EINVAL, "features: bad arguments");
+    int cap = 1;
+    for (int64_t i = 0; i < ntrains; ++i) {
+        if (offsets[i + 1] < offsets[i]) return fail(BG_EINVAL, "features: offsets must not decrease");
+        cap = std::max(cap, (int)(offsets[i + 1] - offsets[i]));
+        for (int64_t k = offsets[i]; k < offsets[i + 1]; ++k) {
+            // the window reads 300 samples before every spike after 30 ms
+            const double t = (double)steps[k] * dt;
+            const long long idx = (long long)(t / dt);
+            if (steps[k] < 0 || I_offset[i] < 0 || I_offset[i] + idx > ninput ||
+                (t > 0.03 && I_offset[i] + idx - 300 < 0))
+                return fail(BG_EINVAL, "features: spike " + std::to_string(k) + " lies outside its input");
+        }
+    }
+    std::vector<int> rec((size_t)ntrains * cap, 0), cnt((size_t)ntrains);
+    for (int64_t i = 0; i < ntrains; ++i) {
+        cnt[i] = (int)(offsets[i + 1] - offsets[i]);
+        for (int k = 0; k < cnt[i]; ++k) rec[(size_t)i * cap + k] = steps[offsets[i] + k];
+    }
+    FCK(cudaSetDevice(device));
+    int *drec = nullptr, *dcnt = nullptr;
+    double *dI = nullptr;
+    long long *doff = nullptr;
+    float *dout = nullptr;
+    cudaError_t e = cudaMalloc((void **)&drec, rec.size() * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&dcnt, cnt.size() * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&dI, (size_t)ninput * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&doff, (size_t)ntrains * sizeof(long long));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&dout, (size_t)ntrains * 64 * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemcpy(drec, rec.data(), rec.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dcnt, cnt.data(), cnt.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dI, I, (size_t)ninput * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(doff, I_offset, (size_t)ntrains * sizeof(long long), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_features<double><<<(unsigned)((ntrains + 3) / 4), 128>>>(ntrains, drec, dcnt, cap, dI, doff, dt, dout);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out, dout, (size_t)ntrains * 64 * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaFree(drec);
+    cudaFree(dcnt);
+    cudaFree(dI);
+    cudaFree(doff);
+    cudaFree(dout);
+    if (e != cudaSuccess) return fail(BG_ECUDA, std::string("features: ") + cudaGetErrorString(e));
+    return BG_OK;
+}
+
+BG_API int bg_fit_train_features(bg_fit *h, int64_t ntrains, const int32_t *steps, const int64_t *offsets,
+                                 const int64_t *I_offset, float *out, float *gpu_ms) {
+    if (!h || !h->I) return fail(BG_ESTATE, "fit: bg_fit_set_input not called");
+    if (ntrains <= 0 || !steps || !offsets || !I_offset || !out) return fail(BG_EINVAL, "fit: bad feature arguments");
+    int cap = 1;
+    for (int64_t i = 0; i < ntrains; ++i) {
+        if (offsets[i + 1] < offsets[i]) return fail(BG_EINVAL, "fit: offsets must not decrease");
+        cap = std::max(cap, (int)(offsets[i + 1] - offsets[i]));
+        for (int64_t k = offsets[i]; k < offsets[i + 1]; ++k) {
+            const double t = (double)steps[k] * h->dt;
+            const long long idx = (long long)(t / h->dt);
+            if (steps[k] < 0 || I_offset[i] < 0 || I_offset[i] + idx > h->ninput ||
+                (t > 0.03 && I_offset[i] + idx - 300 < 0))
+                return fail(BG_EINVAL, "fit: spike " + std::to_string(k) + " lies outside its input");
+        }
+    }
+    std::vector<int> rec((size_t)ntrains * cap, 0), cnt((size_t)ntrains);
+    for (int64_t i = 0; i < ntrains; ++i) {
+        cnt[i] = (int)(offsets[i + 1] - offsets[i]);
+        for (int k = 0; k < cnt[i]; ++k) rec[(size_t)i * cap + k] = steps[offsets[i] + k];
+    }
+    FCK(cudaSetDevice(h->device));
+    int *drec = nullptr, *dcnt = nullptr;
+    long long *doff = nullptr;
+    float *dout = nullptr;
+    cudaError_t e = cudaMalloc((void **)&drec, rec.size() * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&dcnt, cnt.size() * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&doff, (size_t)ntrains * sizeof(long long));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&dout, (size_t)ntrains * 64 * sizeof(float));
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    if (e == cudaSuccess) cudaEventRecord(a, h->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(drec, rec.data(), rec.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dcnt, cnt.data(), cnt.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(doff, I_offset, (size_t)ntrains * sizeof(long long), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) {
+        const unsigned grid = (unsigned)((ntrains + 3) / 4);
+        if (h->precision == 32)
+            k_features<float><<<grid, 128, 0, h->stream>>>(ntrains, drec, dcnt, cap, (const float *)h->I, doff, h->dt,
+                                                           dout);
+        else
+            k_features<double><<<grid, 128, 0, h->stream>>>(ntrains, drec, dcnt, cap, (const double *)h->I, doff,
+                                                            h->dt, dout);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, dout, (size_t)ntrains * 64 * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) cudaEventRecord(b, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    float ms = 0;
+    if (e == cudaSuccess) cudaEventElapsedTime(&ms, a, b);
+    if (gpu_ms) *gpu_ms = ms;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(drec);
+    cudaFree(dcnt);
+    cudaFree(doff);
+    cudaFree(dout);
+    if (e != cudaSuccess) return fail(BG_ECUDA, std::string("fit: features failed: ") + cudaGetErrorString(e));
+    return BG_OK;
+}
+
 BG_API int bg_fit_set_gamma(bg_fit *h, int64_t nparticles, int32_t slices, const int32_t *target_length,
                             const double *target_rate, double delta) {
     int rc = check_sims(h);
@@ -818,6 +952,9 @@ BG_API int bg_fit_evaluate(bg_fit *h, const double *X, double *gamma_out) {
             return fail(BG_ECUDA, std::string("fit: copy of X failed: ") + cudaGetErrorString(e));
         }
     }
+    cudaEvent_t e_start = nullptr;
+    cudaEventCreate(&e_start);
+    cudaEventRecord(e_start, h->stream);
     rc = prepare_launch(h, dX);
     if (!rc) {
         cudaEventRecord(h->ev0, h->stream);
@@ -825,8 +962,14 @@ BG_API int bg_fit_evaluate(bg_fit *h, const double *X, double *gamma_out) {
         cudaEventRecord(h->ev1, h->stream);
     }
     if (!rc) rc = gamma_launch(h);
+    cudaEvent_t e_end = nullptr;
+    cudaEventCreate(&e_end);
+    cudaEventRecord(e_end, h->stream);
     cudaError_t e = cudaStreamSynchronize(h->stream);
     if (dX) cudaFree(dX);
+    if (!rc && e == cudaSuccess) cudaEventElapsedTime(&h->last_eval_ms, e_start, e_end);
+    cudaEventDestroy(e_start);
+    cudaEventDestroy(e_end);
     if (rc) return rc;
     if (e != cudaSuccess) return fail(BG_ECUDA, std::string("fit: evaluation failed: ") + cudaGetErrorString(e));
     FCK(cudaEventElapsedTime(&h->last_sim_ms, h->ev0, h->ev1));
@@ -976,13 +1119,16 @@ BG_API int bg_fit_pso_evaluate_initial(bg_fit *h) {
     if (rc) return rc;
     if (!h->pso_ready) return fail(BG_ESTATE, "fit: bg_fit_pso_init not called");
     FCK(cudaSetDevice(h->device));
+    FCK(cudaEventRecord(h->ev0, h->stream));
     if ((rc = prepare_launch(h, h->X))) return rc;
     if ((rc = sim_launch(h, 0, h->max_steps))) return rc;
     if ((rc = gamma_launch(h))) return rc;
     k_pso_best<<<(unsigned)h->ngroups, kAuxThreads, 0, h->stream>>>(h->npart, h->ndim, h->group_size, h->X, h->fit,
                                                                     h->Xl, h->lfit, h->Xg, h->gfit, nullptr, 0);
     FCK(cudaGetLastError());
+    FCK(cudaEventRecord(h->ev1, h->stream));
     FCK(cudaStreamSynchronize(h->stream));
+    FCK(cudaEventElapsedTime(&h->last_eval_ms, h->ev0, h->ev1));
     return BG_OK;
 }
 
@@ -1010,7 +1156,7 @@ BG_API int bg_fit_pso_state(bg_fit *h, double *X, double *V, double *X_lbest, do
 
 // out[0] = GPU ms of the last simulation launch, out[1] = simulation
 // launches so far, out[2] = neuron-steps of one full run, out[3] = longest
-// simulation (steps).
+// simulation (steps), out[4] = GPU ms of the last whole evaluation.
 BG_API int bg_fit_stats(bg_fit *h, double *out, int n) {
     if (!h || !out) return fail(BG_EINVAL, "fit: bad stats call");
     long long steps = 0;
@@ -1020,8 +1166,9 @@ BG_API int bg_fit_stats(bg_fit *h, double *out, int n) {
         FCK(cudaMemcpy(ns.data(), h->nsteps, ns.size() * sizeof(int), cudaMemcpyDeviceToHost));
         for (int v : ns) steps += v;
     }
-    const double v[4] = {h->last_sim_ms, (double)h->sim_launches, (double)steps, (double)h->max_steps};
-    for (int k = 0; k < n && k < 4; ++k) out[k] = v[k];
+    const double v[5] = {h->last_sim_ms, (double)h->sim_launches, (double)steps, (double)h->max_steps,
+                         h->last_eval_ms};
+    for (int k = 0; k < n && k < 5; ++k) out[k] = v[k];
     return BG_OK;
 }
 

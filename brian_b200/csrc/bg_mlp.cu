@@ -217,6 +217,7 @@ struct bg_mlp {
     // training set
     int64_t nset = 0;
     float *Xall = nullptr, *Yall = nullptr;
+    float last_forward_ms = 0;
 };
 
 namespace {
@@ -427,15 +428,29 @@ BG_API int bg_mlp_forward(bg_mlp *h, const float *X, int64_t n, float *out) {
             xb[(size_t)r * kIn + j] = v;
             xt[(size_t)j * B + r] = v;
         }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, h->stream);
     MCK(cudaMemcpyAsync(h->X, xb.data(), xb.size() * sizeof(bf16), cudaMemcpyHostToDevice, h->stream));
     MCK(cudaMemcpyAsync(h->XT, xt.data(), xt.size() * sizeof(bf16), cudaMemcpyHostToDevice, h->stream));
     if ((rc = forward(h, B))) return rc;
     std::vector<float> o((size_t)B * kOutPad);
     MCK(cudaMemcpyAsync(o.data(), h->OUT, o.size() * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    cudaEventRecord(e1, h->stream);
     MCK(cudaStreamSynchronize(h->stream));
+    cudaEventElapsedTime(&h->last_forward_ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
     if ((rc = check_err(h))) return rc;
     for (int64_t r = 0; r < n; ++r)
         for (int j = 0; j < 2 * h->ydim; ++j) out[r * 2 * h->ydim + j] = o[(size_t)r * kOutPad + j];
+    return BG_OK;
+}
+
+BG_API int bg_mlp_last_forward_ms(bg_mlp *h, float *ms) {
+    if (!h || !ms) return fail(BG_EINVAL, "mlp: bad arguments");
+    *ms = h->last_forward_ms;
     return BG_OK;
 }
 

@@ -226,6 +226,7 @@ class FittingProblem(object):
         self.nsteps_group = np.array([int((n * dt) / dt) for n in lens], dtype=np.int32)
         I = np.concatenate([np.asarray(x, dtype=np.float64) for x in inputs])
         ioff = np.concatenate([[0], np.cumsum(lens)[:-1]]).astype(np.int64)
+        self.input_offsets = ioff
         # target trains with sentinels at -1 s and duration + 1 s
         # (modelfitting.py:139-163), lengths and rates (modelfitting.py:144-145)
         trains, tlen, trate = [], [], []

@@ -15,7 +15,7 @@ sampled exactly), from numpy's PCG64 generator.
 """
 import numpy as np
 
-__all__ = ["ADAPTIVE_LIF", "THRESHOLD", "RESET", "PARAMS", "PRIOR", "ou_current", "sample_prior",
+__all__ = ["ADAPTIVE_LIF", "ADAPTIVE_LIF_BASIS", "THRESHOLD", "RESET", "PARAMS", "PRIOR", "ou_current", "sample_prior",
            "adaptive_lif_equations", "make_targets", "FitWorkload"]
 
 ADAPTIVE_LIF = """
@@ -34,6 +34,17 @@ PARAMS = ("R", "tau", "Vt0", "alpha", "tau_t")
 # log-uniform ranges of the hidden parameters (ohm, s, V, V, s)
 PRIOR = {"R": (2.5e7, 5e7), "tau": (5e-3, 2e-2), "Vt0": (1.5e-2, 2.5e-2), "alpha": (2e-3, 1e-2),
          "tau_t": (5e-2, 2e-1)}
+
+
+# The adaptive LIF's spike train is unchanged when R, Vt0 and alpha are all
+# scaled by one factor (V and Vt scale with it and both start at 0); in the
+# coordinates (log R, log tau, log Vt0 - log R, log alpha - log R, log tau_t)
+# only the first carries that freedom.
+ADAPTIVE_LIF_BASIS = [[1, 0, 0, 0, 0],
+                      [0, 1, 0, 0, 0],
+                      [-1, 0, 1, 0, 0],
+                      [-1, 0, 0, 1, 0],
+                      [0, 0, 0, 0, 1]]
 
 
 def adaptive_lif_equations():

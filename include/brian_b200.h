@@ -319,6 +319,18 @@ BG_API int bg_fit_read_spikes(bg_fit *h, int32_t *counts, int32_t *steps);
  * and a 30-bin spike-triggered average of the input in nA over 30 ms
  * (statistics.py:125-153).  Needs bg_fit_set_record. */
 BG_API int bg_fit_features(bg_fit *h, float *out);
+/* The same features for given trains: steps[offsets[i] .. offsets[i+1]) of
+ * train i (clock steps), its input I[I_offset[i] + T] (amperes); out
+ * [ntrains][64].  Every spike's window must lie inside the input. */
+BG_API int bg_spike_features(int device, int64_t ntrains, const int32_t *steps,
+                             const int64_t *offsets, const double *I, const int64_t *I_offset,
+                             int64_t ninput, double dt, float *out);
+/* The same features for given trains whose inputs are already in the
+ * handle: train i's input starts at I_offset[i] of the handle's input array;
+ * gpu_ms (nullable) receives the device time including the copies. */
+BG_API int bg_fit_train_features(bg_fit *h, int64_t ntrains, const int32_t *steps,
+                                 const int64_t *offsets, const int64_t *I_offset, float *out,
+                                 float *gpu_ms);
 /* Gamma factor inputs (ModelFitting.prepare_data, modelfitting.py:117-173):
  * nparticles x slices = nsims (simulation i is particle i % nparticles),
  * per particle the target train's length and rate (firing_rate), delta in
@@ -361,7 +373,7 @@ BG_API int bg_fit_pso_best(bg_fit *h, double *X_gbest, double *fit_gbest);
 BG_API int bg_fit_pso_state(bg_fit *h, double *X, double *V, double *X_lbest,
                             double *fit_lbest);
 /* out[0..n): last simulation launch (GPU ms), launches, neuron-steps of one
- * full run, longest simulation (steps). */
+ * full run, longest simulation (steps), last whole evaluation (GPU ms). */
 BG_API int bg_fit_stats(bg_fit *h, double *out, int n);
 
 /* ---- learned proposal network ----------------------------------------------
@@ -382,6 +394,8 @@ BG_API int bg_mlp_set_params(bg_mlp *h, int layer, const float *W, const float *
 BG_API int bg_mlp_get_params(bg_mlp *h, int layer, float *W, float *b);
 /* out[n][2*ydim] = network(X[n][64]). */
 BG_API int bg_mlp_forward(bg_mlp *h, const float *X, int64_t n, float *out);
+/* Device time (ms) of the last bg_mlp_forward, copies included. */
+BG_API int bg_mlp_last_forward_ms(bg_mlp *h, float *ms);
 /* Training set: X[n][64] features, Y[n][ydim] targets (already normalised). */
 BG_API int bg_mlp_set_data(bg_mlp *h, const float *X, const float *Y, int64_t n);
 /* `epochs` passes of mini-batch Adam (batch a multiple of 512); the batch
