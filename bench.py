@@ -344,17 +344,30 @@ def fitting_bench(args):
     # ---- the race on fresh targets
     w = FitWorkload(ntargets=args.fit_targets, dur_min=1.0, dur_max=20.0, seed=args.seed + 4321)
     w.build_targets()
+    # plain: the config's 1024 particles per target; learned: 64 proposals
+    # per target seed a swarm of 256 that refines them
     res = race(eqs, THRESHOLD, RESET, w.targets, w.inputs, DT, box, net=net, popsize=1024, n_prop=64,
-               max_iter=args.fit_iters, goal=0.9, seed=args.seed)
-    for arm in ("plain", "learned"):
-        r = res[arm]
-        out[arm] = {k: (None if (isinstance(v, float) and not np.isfinite(v)) else
-                        (float(v) if isinstance(v, (float, np.floating)) else v))
-                    for k, v in r.items() if k not in ("hits_ms", "best_gamma")}
-    p90, l90 = res["plain"]["t90_ms"], res["learned"]["t90_ms"]
-    out["speedup_t90"] = (p90 / l90) if np.isfinite(p90) and l90 > 0 else None
-    out["speedup_t50"] = (res["plain"]["t50_ms"] / res["learned"]["t50_ms"]
-                          if np.isfinite(res["plain"]["t50_ms"]) and res["learned"]["t50_ms"] > 0 else None)
+               max_iter=args.fit_iters, goal=0.9, seed=args.seed, widen=1.25, refine_popsize=256)
+    # plain with the learned arm's population, to show the gain is not the
+    # population size (smaller swarms iterate faster but converge worse)
+    res["plain_256"] = race(eqs, THRESHOLD, RESET, w.targets, w.inputs, DT, box, net=None, popsize=256,
+                            max_iter=3 * args.fit_iters, goal=0.9, seed=args.seed, arms=("plain",))["plain"]
+
+    def clean(r):
+        return {k: (None if (isinstance(v, float) and not np.isfinite(v)) else
+                    (float(v) if isinstance(v, (float, np.floating)) else v))
+                for k, v in r.items() if k not in ("hits_ms", "best_gamma")}
+
+    for arm in ("plain", "plain_256", "learned"):
+        out[arm] = clean(res[arm])
+    l90, l50 = res["learned"]["t90_ms"], res["learned"]["t50_ms"]
+
+    def ratio(a, b):
+        return (a / b) if np.isfinite(a) and np.isfinite(b) and b > 0 else None
+
+    out["speedup_t90"] = ratio(res["plain"]["t90_ms"], l90)
+    out["speedup_t50"] = ratio(res["plain"]["t50_ms"], l50)
+    out["speedup_t90_vs_plain_256"] = ratio(res["plain_256"]["t90_ms"], l90)
     return out
 
 

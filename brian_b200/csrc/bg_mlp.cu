@@ -44,6 +44,10 @@ int fail(int code, const std::string &m) { return bg_internal_fail(code, m.c_str
 
 constexpr int kIn = 64, kHid = 512, kOutPad = 64, kNLayer = 4;
 constexpr int kSplits = 8;
+// Output tile width of the network's GEMMs: 64 columns keeps 256 CTAs in
+// flight per 4096-row product (two or three per SM), so one CTA's load
+// latency overlaps another's tensor-core work.
+constexpr int kNT = 64;
 
 typedef __nv_bfloat16 bf16;
 
@@ -63,59 +67,61 @@ __global__ void k_gather(const float *Xall, const float *Yall, const int64_t *id
 
 // Gaussian NLL per sample, mean over the batch:
 //   sum_d 0.5 ((y_d - mu_d) e^{-s_d})^2 + s_d,  s = clamp(log sigma, -7, 7)
-// gradients (already divided by B) into dOUT (bf16, both layouts).
-__global__ void k_nll(const float *OUT, const float *Y, int B, int ydim, bf16 *dO, bf16 *dOT, float *loss_sum) {
+// gradients (already divided by B) into dOUT (bf16, both layouts; the
+// padded columns stay zero from allocation) and per-block column sums of the
+// bf16 gradients into colsum[blockIdx.x][64] (the output bias gradient).
+__global__ void __launch_bounds__(256) k_nll(const float *OUT, const float *Y, int B, int ydim, bf16 *dO, bf16 *dOT,
+                                             float *colsum, float *loss_sum) {
+    constexpr int kMaxY = kOutPad / 2;
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ float red[8][kOutPad];
+    __shared__ float lred[8];
     float l = 0.f;
+    float gcol[kOutPad];
+#pragma unroll
+    for (int j = 0; j < kOutPad; ++j) gcol[j] = 0.f;
     if (b < B) {
         const float inv_b = 1.0f / (float)B;
-        for (int j = 0; j < kOutPad; ++j) {
-            float g = 0.f;
-            if (j < ydim) {
-                const float mu = OUT[(int64_t)b * kOutPad + j];
-                const float sr = OUT[(int64_t)b * kOutPad + ydim + j];
-                const float s = fminf(fmaxf(sr, -7.f), 7.f);
-                const float r = (Y[(int64_t)b * ydim + j] - mu) * expf(-s);
-                l += 0.5f * r * r + s;
-                g = -r * expf(-s) * inv_b;                                   // d/d mu
-                const float gs = (sr > -7.f && sr < 7.f) ? (1.f - r * r) * inv_b : 0.f;   // d/d log sigma
-                dO[(int64_t)b * kOutPad + ydim + j] = __float2bfloat16_rn(gs);
-                dOT[(int64_t)(ydim + j) * B + b] = __float2bfloat16_rn(gs);
-            } else if (j >= 2 * ydim) {
-                dO[(int64_t)b * kOutPad + j] = __float2bfloat16_rn(0.f);
-                dOT[(int64_t)j * B + b] = __float2bfloat16_rn(0.f);
-                continue;
-            } else {
-                continue;
-            }
-            dO[(int64_t)b * kOutPad + j] = __float2bfloat16_rn(g);
-            dOT[(int64_t)j * B + b] = __float2bfloat16_rn(g);
+        for (int j = 0; j < ydim && j < kMaxY; ++j) {
+            const float mu = OUT[(int64_t)b * kOutPad + j];
+            const float sr = OUT[(int64_t)b * kOutPad + ydim + j];
+            const float s = fminf(fmaxf(sr, -7.f), 7.f);
+            const float r = (Y[(int64_t)b * ydim + j] - mu) * expf(-s);
+            l += 0.5f * r * r + s;
+            const bf16 g = __float2bfloat16_rn(-r * expf(-s) * inv_b);                                  // d/d mu
+            const bf16 gs = __float2bfloat16_rn((sr > -7.f && sr < 7.f) ? (1.f - r * r) * inv_b : 0.f);  // d/d log sigma
+            dO[(int64_t)b * kOutPad + j] = g;
+            dO[(int64_t)b * kOutPad + ydim + j] = gs;
+            dOT[(int64_t)j * B + b] = g;
+            dOT[(int64_t)(ydim + j) * B + b] = gs;
+            gcol[j] = __bfloat162float(g);
+            gcol[ydim + j] = __bfloat162float(gs);
         }
     }
-    // block sum of the loss
-    __shared__ float red[256];
-    red[threadIdx.x] = l;
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
-        __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int j = 0; j < kOutPad; ++j) {
+        if (j >= 2 * ydim) break;
+        float v = gcol[j];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if (lane == 0) red[warp][j] = v;
     }
-    if (threadIdx.x == 0) atomicAdd(loss_sum, red[0] / (float)B);
-}
-
-// Row sums of G^T ([N][B]) -> bias gradient, one block per row.
-__global__ void k_rowsum(const bf16 *GT, int B, float *out) {
-    const int n = blockIdx.x;
-    float s = 0.f;
-    for (int b = threadIdx.x; b < B; b += blockDim.x) s += __bfloat162float(GT[(int64_t)n * B + b]);
-    __shared__ float red[256];
-    red[threadIdx.x] = s;
+    float lv = l;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) lv += __shfl_xor_sync(0xffffffffu, lv, off);
+    if (lane == 0) lred[warp] = lv;
     __syncthreads();
-    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
-        if ((int)threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
-        __syncthreads();
+    if ((int)threadIdx.x < 2 * ydim) {
+        float v = 0.f;
+        for (int w = 0; w < 8; ++w) v += red[w][threadIdx.x];
+        colsum[(int64_t)blockIdx.x * kOutPad + threadIdx.x] = v;
     }
-    if (threadIdx.x == 0) out[n] = red[0];
+    if (threadIdx.x == 0) {
+        float v = 0.f;
+        for (int w = 0; w < 8; ++w) v += lred[w];
+        atomicAdd(loss_sum, v / (float)B);
+    }
 }
 
 // Adam on one parameter tensor [rows][cols] whose gradient is the sum of
@@ -207,7 +213,8 @@ struct bg_mlp {
     float *W[kNLayer] = {}, *b[kNLayer] = {}, *mW[kNLayer] = {}, *vW[kNLayer] = {}, *mb[kNLayer] = {},
           *vb[kNLayer] = {};
     bf16 *Wb[kNLayer] = {}, *WbT[kNLayer] = {};
-    float *gW = nullptr, *gb = nullptr;   // gradient scratch (largest layer x splits), bias grads
+    float *gW = nullptr;                  // weight-gradient scratch (largest layer x splits)
+    float *cs[kNLayer] = {};              // bias-gradient partials per layer [row blocks][512]
     int64_t step = 0;
     // batch buffers
     int B = 0;
@@ -238,6 +245,8 @@ int ensure_batch(bg_mlp *h, int B) {
     if ((rc = dalloc(&h->OUT, (size_t)B * kOutPad))) return rc;
     if ((rc = dalloc(&h->Y, (size_t)B * h->ydim))) return rc;
     if ((rc = dalloc(&h->idx, (size_t)B))) return rc;
+    for (int l = 0; l < kNLayer; ++l)
+        if ((rc = dalloc(&h->cs[l], (size_t)((B + 127) / 128) * kHid))) return rc;
     h->B = B;
     return BG_OK;
 }
@@ -253,7 +262,7 @@ int forward(bg_mlp *h, int B) {
         g.ldh = kHid;
         g.HT = h->HT[l];
         g.ldht = B;
-        int rc = launch_gemm<128, umma::EPI_RELU_BF16>(g, 1, h->stream);
+        int rc = launch_gemm<kNT, umma::EPI_RELU_BF16>(g, 1, h->stream);
         if (rc) return rc;
         in = h->H[l];
         K = kHid;
@@ -265,8 +274,23 @@ int forward(bg_mlp *h, int B) {
     return launch_gemm<64, umma::EPI_BIAS_F32>(g, 1, h->stream);
 }
 
+// Bias-gradient partials of layer l: per-block column sums written by the
+// loss kernel (output layer, blocks of 256 rows, 64 columns) or by the
+// ReLU-gradient epilogue that produced G[l] (blocks of 128 rows).
+void bias_partials(const bg_mlp *h, int l, int B, const float **p, int *nblk, int *ld) {
+    *p = h->cs[l];
+    if (l == kNLayer - 1) {
+        *nblk = (B + 255) / 256;
+        *ld = kOutPad;
+    } else {
+        *nblk = (B + umma::kM - 1) / umma::kM;
+        *ld = kHid;
+    }
+}
+
 // backward from the loss gradient in h->dO / h->dOT; weight gradients of
-// layer l into h->gW (split slices) and bias gradients into h->gb, then Adam
+// layer l into h->gW (split slices), bias gradients from the column-sum
+// partials, then Adam
 int backward_and_update(bg_mlp *h, int B, float lr, bool update) {
     int rc = 0;
     const int splits = B % (kSplits * umma::kKc) == 0 ? kSplits : 1;
@@ -291,13 +315,11 @@ int backward_and_update(bg_mlp *h, int B, float lr, bool update) {
             g.ldc = nin;
             g.split_stride = slice;
             if (nin == kIn) rc = launch_gemm<64, umma::EPI_F32>(g, splits, h->stream);
-            else rc = launch_gemm<128, umma::EPI_F32>(g, splits, h->stream);
+            else rc = launch_gemm<kNT, umma::EPI_F32>(g, splits, h->stream);
             if (rc) return rc;
         }
-        // bias gradient: row sums of gin^T
-        k_rowsum<<<h->rows[l], 256, 0, h->stream>>>(ginT, B, h->gb);
-        MCK(cudaGetLastError());
-        // gradient into the previous hidden layer (needs W_l before its update)
+        // gradient into the previous hidden layer (needs W_l before its
+        // update); its epilogue also sums the columns for layer l-1's bias
         if (l > 0) {
             umma::GemmArgs g = gemm_args(gin, gK, h->WbT[l], h->rows[l], B, kHid, gK, h->err);
             g.act = h->H[l - 1];
@@ -306,7 +328,9 @@ int backward_and_update(bg_mlp *h, int B, float lr, bool update) {
             g.ldh = kHid;
             g.HT = h->GT[l - 1];
             g.ldht = B;
-            if ((rc = launch_gemm<128, umma::EPI_DRELU_BF16>(g, 1, h->stream))) return rc;
+            g.colsum = h->cs[l - 1];
+            g.colsum_ld = kHid;
+            if ((rc = launch_gemm<kNT, umma::EPI_DRELU_BF16>(g, 1, h->stream))) return rc;
         }
         if (update) {
             const int rows_train = l == 3 ? 2 * h->ydim : h->rows[l];
@@ -314,8 +338,11 @@ int backward_and_update(bg_mlp *h, int B, float lr, bool update) {
             k_adam<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(
                 h->W[l], h->mW[l], h->vW[l], h->gW, splits, slice, h->rows[l], h->cols[l], rows_train, lr, b1, b2,
                 eps, c1, c2, h->Wb[l], h->WbT[l]);
+            const float *bp;
+            int nblk, ld;
+            bias_partials(h, l, B, &bp, &nblk, &ld);
             k_adam<<<(unsigned)((h->rows[l] + 255) / 256), 256, 0, h->stream>>>(
-                h->b[l], h->mb[l], h->vb[l], h->gb, 1, 0, h->rows[l], 1, rows_train, lr, b1, b2, eps, c1, c2,
+                h->b[l], h->mb[l], h->vb[l], bp, nblk, ld, h->rows[l], 1, rows_train, lr, b1, b2, eps, c1, c2,
                 nullptr, nullptr);
             MCK(cudaGetLastError());
         }
@@ -361,7 +388,6 @@ BG_API int bg_mlp_create(bg_mlp **out, int device, int ydim) {
         if (!rc) rc = dalloc(&h->WbT[l], n);
     }
     if (!rc) rc = dalloc(&h->gW, (size_t)kSplits * kHid * kHid);
-    if (!rc) rc = dalloc(&h->gb, (size_t)kHid);
     if (!rc) rc = dalloc(&h->loss, 1);
     if (rc) {
         bg_mlp_destroy(h);
@@ -381,7 +407,8 @@ BG_API int bg_mlp_destroy(bg_mlp *h) {
     }
     for (int l = 0; l < 3; ++l) { dfree(h->H[l]); dfree(h->HT[l]); dfree(h->G[l]); dfree(h->GT[l]); }
     dfree(h->X); dfree(h->XT); dfree(h->dO); dfree(h->dOT); dfree(h->OUT); dfree(h->Y); dfree(h->idx);
-    dfree(h->gW); dfree(h->gb); dfree(h->loss); dfree(h->err); dfree(h->Xall); dfree(h->Yall);
+    for (int l = 0; l < kNLayer; ++l) dfree(h->cs[l]);
+    dfree(h->gW); dfree(h->loss); dfree(h->err); dfree(h->Xall); dfree(h->Yall);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return BG_OK;
@@ -499,7 +526,8 @@ BG_API int bg_mlp_train(bg_mlp *h, int epochs, int batch, float lr, uint64_t see
             k_gather<<<batch, 64, 0, h->stream>>>(h->Xall, h->Yall, dperm + s * batch, batch, h->ydim, h->X, h->XT,
                                                 h->Y);
             if ((rc = forward(h, batch))) break;
-            k_nll<<<(batch + 255) / 256, 256, 0, h->stream>>>(h->OUT, h->Y, batch, h->ydim, h->dO, h->dOT, h->loss);
+            k_nll<<<(batch + 255) / 256, 256, 0, h->stream>>>(h->OUT, h->Y, batch, h->ydim, h->dO, h->dOT,
+                                                               h->cs[kNLayer - 1], h->loss);
             rc = backward_and_update(h, batch, lr, true);
         }
         float ls = 0;
@@ -533,7 +561,8 @@ BG_API int bg_mlp_gradients(bg_mlp *h, int batch, float *loss, float *const *dW,
     MCK(cudaMemsetAsync(h->loss, 0, sizeof(float), h->stream));
     k_gather<<<batch, 64, 0, h->stream>>>(h->Xall, h->Yall, h->idx, batch, h->ydim, h->X, h->XT, h->Y);
     if ((rc = forward(h, batch))) return rc;
-    k_nll<<<(batch + 255) / 256, 256, 0, h->stream>>>(h->OUT, h->Y, batch, h->ydim, h->dO, h->dOT, h->loss);
+    k_nll<<<(batch + 255) / 256, 256, 0, h->stream>>>(h->OUT, h->Y, batch, h->ydim, h->dO, h->dOT,
+                                                       h->cs[kNLayer - 1], h->loss);
     // run the backward pass layer by layer, reading each layer's gradient
     // before the next layer reuses the scratch
     const int splits = kSplits;
@@ -549,9 +578,8 @@ BG_API int bg_mlp_gradients(bg_mlp *h, int batch, float *loss, float *const *dW,
         g.ldc = nin;
         g.split_stride = (int64_t)kHid * kHid;
         rc = nin == kIn ? launch_gemm<64, umma::EPI_F32>(g, splits, h->stream)
-                        : launch_gemm<128, umma::EPI_F32>(g, splits, h->stream);
+                        : launch_gemm<kNT, umma::EPI_F32>(g, splits, h->stream);
         if (rc) return rc;
-        k_rowsum<<<h->rows[l], 256, 0, h->stream>>>(ginT, batch, h->gb);
         std::vector<float> part((size_t)splits * kHid * kHid);
         MCK(cudaMemcpyAsync(part.data(), h->gW, part.size() * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
         MCK(cudaStreamSynchronize(h->stream));
@@ -562,7 +590,19 @@ BG_API int bg_mlp_gradients(bg_mlp *h, int batch, float *loss, float *const *dW,
                 for (int z = 0; z < splits; ++z) s += part[(size_t)z * kHid * kHid + i];
                 dW[l][i] = s;
             }
-        if (db && db[l]) MCK(cudaMemcpy(db[l], h->gb, (size_t)h->rows[l] * sizeof(float), cudaMemcpyDeviceToHost));
+        if (db && db[l]) {
+            // the bias gradient: fixed-order sum of the column-sum partials
+            const float *bp;
+            int nblk, ld;
+            bias_partials(h, l, batch, &bp, &nblk, &ld);
+            std::vector<float> cp((size_t)nblk * ld);
+            MCK(cudaMemcpy(cp.data(), bp, cp.size() * sizeof(float), cudaMemcpyDeviceToHost));
+            for (int r = 0; r < h->rows[l]; ++r) {
+                float s = 0;
+                for (int z = 0; z < nblk; ++z) s += r < ld ? cp[(size_t)z * ld + r] : 0.f;
+                db[l][r] = s;
+            }
+        }
         if (l > 0) {
             umma::GemmArgs g2 = gemm_args(gin, gK, h->WbT[l], h->rows[l], batch, kHid, gK, h->err);
             g2.act = h->H[l - 1];
@@ -571,7 +611,9 @@ BG_API int bg_mlp_gradients(bg_mlp *h, int batch, float *loss, float *const *dW,
             g2.ldh = kHid;
             g2.HT = h->GT[l - 1];
             g2.ldht = batch;
-            if ((rc = launch_gemm<128, umma::EPI_DRELU_BF16>(g2, 1, h->stream))) return rc;
+            g2.colsum = h->cs[l - 1];
+            g2.colsum_ld = kHid;
+            if ((rc = launch_gemm<kNT, umma::EPI_DRELU_BF16>(g2, 1, h->stream))) return rc;
             gin = h->G[l - 1];
             ginT = h->GT[l - 1];
             gK = kHid;

@@ -14,7 +14,12 @@
 // mbarrier; a stage is refilled only after that mbarrier completes.  The
 // accumulator lives in TMEM (lane = tile row, one column per output column)
 // and is read back by every warp for its 32 rows with tcgen05.ld; the
-// epilogue is fused (bias, ReLU, ReLU gradient, transposed copies).
+// epilogue is fused (bias, ReLU, ReLU gradient, transposed copies, column
+// sums).  Row-major results go through the idle stage buffers: each warp
+// stages its 32 x NT block in shared memory and writes whole rows with
+// 16-byte stores; the ReLU mask of the gradient epilogue is read the same
+// way.  Transposed copies are written from registers (32 consecutive rows
+// of one column per warp store).
 //
 // Every wait on an mbarrier is bounded; a wait that gives up records an
 // error code and the CTA leaves after releasing its TMEM.
@@ -56,6 +61,8 @@ struct GemmArgs {
     const __nv_bfloat16 *act; // [M][ldact] for EPI_DRELU_BF16
     int ldact;
     int n_valid;              // columns >= n_valid are written as 0 (bf16 outs) / skipped (fp32)
+    float *colsum;            // EPI_DRELU_BF16: column sums of the bf16 result over each CTA's
+    int colsum_ld;            //   128 rows, at colsum[blockIdx.x * colsum_ld + col] (or null)
     int *err;                 // error flag (device)
 };
 
@@ -140,6 +147,7 @@ struct Smem {
     alignas(1024) unsigned char a[kStages][kM * kKc * 2];
     alignas(1024) unsigned char b[kStages][NT * kKc * 2];
     alignas(8) unsigned long long bar[kStages];
+    float bias[NT];
     uint32_t tmem_base;
     int failed;
 };
@@ -180,6 +188,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(const GemmArgs g) {
     const int kend = min(g.K, kbeg + g.k_per_split);
     const int nk = (kend - kbeg) / kKc;
 
+    if ((EPI == EPI_RELU_BF16 || EPI == EPI_BIAS_F32) && tid < NT)
+        sm.bias[tid] = (n0 + tid < g.N) ? g.bias[n0 + tid] : 0.f;
     if (tid == 0) {
         for (int s = 0; s < kStages; ++s) mbar_init(smem_u32(&sm.bar[s]), 1);
         sm.failed = 0;
@@ -243,9 +253,52 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(const GemmArgs g) {
         if (tid == 0 && g.err) atomicExch(g.err, 1);
     } else {
         // epilogue: warp w owns tile rows 32w .. 32w+31, TMEM lanes alike
-        const int row = m0 + warp * 32 + lane;
+        constexpr bool kBF = (EPI == EPI_RELU_BF16 || EPI == EPI_DRELU_BF16);
+        constexpr int kEsz = kBF ? 2 : 4;
+        constexpr int kRowE = NT + 16 / kEsz;                   // staged row: NT elements + 16 bytes
+        constexpr int kPieces = NT * kEsz / 16;                 // 16-byte pieces per row
+        static_assert(4 * 32 * kRowE * kEsz + 4 * NT * 4 <= sizeof(((Smem<NT> *)0)->a) +
+                                                             sizeof(((Smem<NT> *)0)->b),
+                      "epilogue staging exceeds the stage buffers");
+        unsigned char *stage = &sm.a[0][0] + (size_t)warp * 32 * kRowE * kEsz;
+        float *red = reinterpret_cast<float *>(&sm.a[0][0] + (size_t)4 * 32 * kRowE * kEsz);
+        const int wrow0 = m0 + warp * 32;
+        const int row = wrow0 + lane;
         const bool row_ok = row < g.M;
-        float *Cz = g.C ? g.C + (long long)blockIdx.z * g.split_stride : nullptr;
+        // row-major destination of this epilogue
+        unsigned char *dst = nullptr;
+        int ldo = 0, col_limit = g.N;
+        if (EPI == EPI_F32 || EPI == EPI_BIAS_F32) {
+            dst = reinterpret_cast<unsigned char *>(g.C + (long long)blockIdx.z * g.split_stride);
+            ldo = g.ldc;
+            col_limit = min(g.N, g.n_valid);
+        } else {
+            dst = reinterpret_cast<unsigned char *>(g.H);
+            ldo = g.ldh;
+        }
+        const bool vec_out = (((size_t)ldo * kEsz) % 16 == 0) && (((uintptr_t)dst & 15) == 0);
+        if (EPI == EPI_DRELU_BF16) {
+            // the mask source, rows of act, into the staging rows
+            const bool vec_in = (((size_t)g.ldact * 2) % 16 == 0) && (((uintptr_t)g.act & 15) == 0);
+            for (int p = lane; p < 32 * kPieces; p += 32) {
+                const int r = p / kPieces, q = p % kPieces;
+                const int grow = wrow0 + r, gcol = n0 + q * 8;
+                uint4 v = make_uint4(0, 0, 0, 0);
+                if (grow < g.M) {
+                    const __nv_bfloat16 *src = g.act + (long long)grow * g.ldact + gcol;
+                    if (vec_in && gcol + 8 <= g.N) {
+                        v = *reinterpret_cast<const uint4 *>(src);
+                    } else {
+                        __nv_bfloat16 t[8];
+#pragma unroll
+                        for (int e = 0; e < 8; ++e) t[e] = gcol + e < g.N ? src[e] : __float2bfloat16_rn(0.f);
+                        v = *reinterpret_cast<uint4 *>(t);
+                    }
+                }
+                *reinterpret_cast<uint4 *>(stage + ((size_t)r * kRowE + q * 8) * 2) = v;
+            }
+            __syncwarp();
+        }
 #pragma unroll 1
         for (int cb = 0; cb < NT; cb += 16) {
             float v[16];
@@ -255,28 +308,75 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(const GemmArgs g) {
 #pragma unroll
                 for (int i = 0; i < 16; ++i) v[i] = 0.f;
             }
-            if (!row_ok) continue;
+            unsigned char *srow = stage + ((size_t)lane * kRowE + cb) * kEsz;
+            if (kBF) {
+                __nv_bfloat16 hv[16];
+                __nv_bfloat16 av[16];
+                if (EPI == EPI_DRELU_BF16) {
+                    *reinterpret_cast<uint4 *>(av) = *reinterpret_cast<const uint4 *>(srow);
+                    *reinterpret_cast<uint4 *>(av + 8) = *reinterpret_cast<const uint4 *>(srow + 16);
+                }
 #pragma unroll
-            for (int i = 0; i < 16; ++i) {
-                const int col = n0 + cb + i;
-                if (col >= g.N) continue;
-                float x = v[i];
-                if (EPI == EPI_F32) {
-                    if (col < g.n_valid) Cz[(long long)row * g.ldc + col] = x;
-                } else if (EPI == EPI_BIAS_F32) {
-                    if (col < g.n_valid) Cz[(long long)row * g.ldc + col] = x + g.bias[col];
-                } else {
+                for (int i = 0; i < 16; ++i) {
+                    const int col = n0 + cb + i;
+                    float x = v[i];
                     if (EPI == EPI_RELU_BF16) {
-                        x = x + g.bias[col];
+                        x = col < g.N ? x + sm.bias[cb + i] : 0.f;
                         x = x > 0.f ? x : 0.f;
                     } else {
-                        const float a = __bfloat162float(g.act[(long long)row * g.ldact + col]);
-                        x = a > 0.f ? x : 0.f;
+                        x = __bfloat162float(av[i]) > 0.f ? x : 0.f;
                     }
-                    if (col >= g.n_valid) x = 0.f;
-                    const __nv_bfloat16 h = __float2bfloat16_rn(x);
-                    g.H[(long long)row * g.ldh + col] = h;
-                    if (g.HT) g.HT[(long long)col * g.ldht + row] = h;
+                    if (col >= g.n_valid || col >= g.N || !row_ok) x = 0.f;
+                    hv[i] = __float2bfloat16_rn(x);
+                    if (g.HT && row_ok && col < g.N) g.HT[(long long)col * g.ldht + row] = hv[i];
+                }
+                *reinterpret_cast<uint4 *>(srow) = *reinterpret_cast<uint4 *>(hv);
+                *reinterpret_cast<uint4 *>(srow + 16) = *reinterpret_cast<uint4 *>(hv + 8);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const int col = n0 + cb + i;
+                    if (EPI == EPI_BIAS_F32 && col < g.N) v[i] += sm.bias[cb + i];
+                }
+#pragma unroll
+                for (int i = 0; i < 16; i += 4)
+                    *reinterpret_cast<float4 *>(srow + i * 4) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+            }
+        }
+        __syncwarp();
+        if (EPI == EPI_DRELU_BF16 && g.colsum) {
+            // column sums of the bf16 results over the CTA's rows, fixed order
+            for (int c = lane; c < NT; c += 32) {
+                float sum = 0.f;
+                for (int r = 0; r < 32; ++r)
+                    sum += __bfloat162float(*reinterpret_cast<const __nv_bfloat16 *>(stage + ((size_t)r * kRowE + c) * 2));
+                red[warp * NT + c] = sum;
+            }
+        }
+        // whole rows out with 16-byte stores
+        for (int p = lane; p < 32 * kPieces; p += 32) {
+            const int r = p / kPieces, q = p % kPieces;
+            const int grow = wrow0 + r;
+            if (grow >= g.M) continue;
+            constexpr int kPer = 16 / kEsz;
+            const int gcol = n0 + q * kPer;
+            const unsigned char *src = stage + ((size_t)r * kRowE + q * kPer) * kEsz;
+            unsigned char *d = dst + ((size_t)grow * ldo + gcol) * kEsz;
+            if (vec_out && gcol + kPer <= col_limit) {
+                *reinterpret_cast<uint4 *>(d) = *reinterpret_cast<const uint4 *>(src);
+            } else {
+                for (int e = 0; e < kPer && gcol + e < col_limit; ++e)
+                    for (int by = 0; by < kEsz; ++by) d[e * kEsz + by] = src[e * kEsz + by];
+            }
+        }
+        if (EPI == EPI_DRELU_BF16 && g.colsum) {
+            __syncthreads();
+            if (warp == 0) {
+                for (int c = lane; c < NT; c += 32) {
+                    const int col = n0 + c;
+                    if (col < g.N)
+                        g.colsum[(long long)blockIdx.x * g.colsum_ld + col] =
+                            ((red[c] + red[NT + c]) + red[2 * NT + c]) + red[3 * NT + c];
                 }
             }
         }

@@ -223,15 +223,16 @@ def _swarm(prob, X0, box_lo, box_hi, pso, seed, goal, max_iter, t_start, chunk=5
 
 def race(model, threshold, reset, targets, inputs, dt, box, net=None, popsize=1024, n_prop=64, max_iter=50,
          goal=0.9, precision="float", seed=0, pso=(0.7298, 1.49618, 1.49618), method="Euler", initial_values=None,
-         widen=1.5, device=0):
+         widen=1.25, device=0, arms=("plain", "learned"), refine_popsize=None):
     """GPU time until each target's fitted gamma reaches `goal`.
 
     Plain: the swarm from uniform draws over `box` (name -> (lo, hi)).
     Learned (when `net` is given): the network proposes n_prop parameter sets
-    per target from the target's features; they are simulated and scored
-    (stage 1); targets still below `goal` get a swarm whose initial
-    positions are those proposals plus draws from the network's Gaussian
-    widened by `widen` (stage 2).  Every time is device time from CUDA
+    per target from the target's features; a swarm of refine_popsize
+    particles per target (default popsize) starts from those proposals plus
+    draws from the network's Gaussian widened by `widen`; its first
+    evaluation re-simulates and scores the proposals, its iterations refine
+    them.  Every time is device time from CUDA
     events, plus the network's own (timed on the host around synchronous
     calls).  Returns a dict per arm with per-target hit times (ms), final
     best gamma and summary times."""
@@ -252,43 +253,47 @@ def race(model, threshold, reset, targets, inputs, dt, box, net=None, popsize=10
         return d
 
     # plain swarm
-    prob = FittingProblem(model, threshold, reset, targets, inputs, dt, popsize, precision=precision, method=method,
-                          param_names=names, initial_values=initial_values, device=device)
-    X0 = lo.reshape(-1, 1) + (hi - lo).reshape(-1, 1) * rng.random((len(names), prob.N))
-    pfirst = {}
+    if "plain" in arms:
+        prob = FittingProblem(model, threshold, reset, targets, inputs, dt, popsize, precision=precision,
+                              method=method, param_names=names, initial_values=initial_values, device=device)
+        X0 = lo.reshape(-1, 1) + (hi - lo).reshape(-1, 1) * rng.random((len(names), prob.N))
+        pfirst = {}
 
-    def pinspect(lfit):
-        f = np.where(np.isnan(lfit), -np.inf, lfit).reshape(G, popsize)
-        pfirst["all"] = float(np.mean(f.max(axis=1) >= goal))
+        def pinspect(lfit):
+            f = np.where(np.isnan(lfit), -np.inf, lfit).reshape(G, popsize)
+            pfirst["all"] = float(np.mean(f.max(axis=1) >= goal))
 
-    hits, best, iters, ms = _swarm(prob, X0, lo, hi, pso, seed + 1, goal, max_iter, 0.0, inspect=pinspect)
-    out["plain"] = summary(hits, best, ms, {"iterations": iters, "first_evaluation_reached": pfirst.get("all")})
-    prob.handle.close()
-    if net is None:
+        hits, best, iters, ms = _swarm(prob, X0, lo, hi, pso, seed + 1, goal, max_iter, 0.0, inspect=pinspect)
+        out["plain"] = summary(hits, best, ms, {"iterations": iters, "first_evaluation_reached": pfirst.get("all")})
+        prob.handle.close()
+    else:
+        rng.random((len(names), G * popsize))      # same draws afterwards either way
+    if net is None or "learned" not in arms:
         return out
 
     # learned: features of the targets (inputs already on the device), the
     # network, then one swarm whose first evaluation re-simulates the n_prop
     # proposals of every target together with popsize - n_prop further draws
     # from the network's Gaussian (widened); the swarm refines from there
-    prob = FittingProblem(model, threshold, reset, targets, inputs, dt, popsize, precision=precision, method=method,
+    rp = int(refine_popsize or popsize)
+    prob = FittingProblem(model, threshold, reset, targets, inputs, dt, rp, precision=precision, method=method,
                           param_names=names, initial_values=initial_values, device=device)
     t0 = time.perf_counter()
     steps = [np.asarray(np.rint(np.asarray(t, dtype=np.float64) / dt), dtype=np.int32) for t in targets]
     F, t_feat = prob.handle.train_features(steps, prob.input_offsets)
     P = net.sample(F, n_prop, rng, widen=1.0)
     t_net = t_feat + net.last_ms
-    extra = net.sample(F, popsize - n_prop, rng, widen=widen)
+    extra = net.sample(F, rp - n_prop, rng, widen=widen)
     wall_net = (time.perf_counter() - t0) * 1e3
-    X0 = np.empty((len(names), G * popsize))
+    X0 = np.empty((len(names), G * rp))
     for j in range(G):
-        X0[:, j * popsize:j * popsize + n_prop] = P[:, j * n_prop:(j + 1) * n_prop]
-        X0[:, j * popsize + n_prop:(j + 1) * popsize] = extra[:, j * (popsize - n_prop):(j + 1) * (popsize - n_prop)]
+        X0[:, j * rp:j * rp + n_prop] = P[:, j * n_prop:(j + 1) * n_prop]
+        X0[:, j * rp + n_prop:(j + 1) * rp] = extra[:, j * (rp - n_prop):(j + 1) * (rp - n_prop)]
     X0 = np.minimum(np.maximum(X0, lo.reshape(-1, 1)), hi.reshape(-1, 1))
     first = {}
 
     def inspect(lfit):
-        f = np.where(np.isnan(lfit), -np.inf, lfit).reshape(G, popsize)
+        f = np.where(np.isnan(lfit), -np.inf, lfit).reshape(G, rp)
         first["proposals"] = float(np.mean(f[:, :n_prop].max(axis=1) >= goal))
         first["all"] = float(np.mean(f.max(axis=1) >= goal))
 
@@ -296,6 +301,7 @@ def race(model, threshold, reset, targets, inputs, dt, box, net=None, popsize=10
     prob.handle.close()
     out["learned"] = summary(hits, best, t_net + ms,
                              {"iterations": iters, "network_ms": t_net, "network_wall_ms": wall_net,
+                              "refine_popsize": rp,
                               "first_evaluation_reached": first.get("all"),
                               "proposals_only_reached": first.get("proposals")})
     return out
