@@ -371,6 +371,45 @@ def fitting_bench(args):
     return out
 
 
+def profile_case(case, seed):
+    """Small cases for ncu captures of single kernels (`--profile-case`).
+
+    fit:  one evaluation of 64 targets x 256 candidates of the adaptive LIF
+          (FP32) on OU inputs of 1-5 s with random target trains; it is the
+          only bg_fit_sim launch of the process.
+    gemm: one training epoch of the proposal network on 65 536 random rows,
+          batch 4096 (launch 12 of k_gemm is the 512 x 512 hidden layer of
+          the second step)."""
+    rng = np.random.default_rng(seed)
+    if case == "fit":
+        from brian_b200.synthetic import (FitWorkload, adaptive_lif_equations, THRESHOLD, RESET, PARAMS,
+                                          sample_prior)
+        from brian_b200.modelfitting import FittingProblem
+        w = FitWorkload(ntargets=64, dur_min=1.0, dur_max=5.0, seed=7)
+        trains = [np.sort(rng.uniform(0, len(x) * DT, rng.integers(5, 200))) for x in w.inputs]
+        prob = FittingProblem(adaptive_lif_equations(), THRESHOLD, RESET, trains, w.inputs, DT, 256,
+                              precision="float", param_names=list(PARAMS))
+        prob.evaluate(sample_prior(prob.N, rng))
+        st = prob.handle.stats()
+        print(json.dumps({"case": "fit", "kernel_ms": st["last_sim_ms"], "neuron_steps": st["neuron_steps"],
+                          "neuron_steps_per_s": st["neuron_steps"] / st["last_sim_ms"] * 1e3}))
+    elif case == "gemm":
+        from brian_b200 import _lib
+        h = _lib.MLPHandle(5)
+        for l in range(4):
+            W = (rng.standard_normal((_lib.MLP_ROWS[l], _lib.MLP_COLS[l])) *
+                 np.sqrt(2.0 / _lib.MLP_COLS[l])).astype(np.float32)
+            if l == 3:
+                W[10:] = 0
+            h.set_params(l, W, np.zeros(_lib.MLP_ROWS[l], dtype=np.float32))
+        n = 65536
+        h.set_data(rng.standard_normal((n, 64)).astype(np.float32), rng.uniform(-1, 1, (n, 5)).astype(np.float32))
+        loss, ms = h.train(1, 4096, 1e-3, seed)
+        print(json.dumps({"case": "gemm", "train_ms": ms, "steps": n // 4096, "loss": float(loss[0])}))
+    else:
+        raise SystemExit("unknown profile case %r" % case)
+
+
 def _numpy_free_builder():
     from brian_b200._lib import fixed_indegree_csr_native
     return fixed_indegree_csr_native
@@ -395,7 +434,12 @@ def main():
     ap.add_argument("--fit-train", type=int, default=1 << 20)
     ap.add_argument("--fit-epochs", type=int, default=40)
     ap.add_argument("--fit-iters", type=int, default=40)
+    ap.add_argument("--profile-case", choices=["fit", "gemm"], default=None,
+                    help="run one small case for a single-kernel ncu capture and exit")
     args = ap.parse_args()
+    if args.profile_case:
+        profile_case(args.profile_case, args.seed)
+        return
     if args.impl == "reference":
         run_reference(args)
         return
