@@ -430,6 +430,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--neurons", type=int, default=N_NEURONS)
     ap.add_argument("--no-fit", action="store_true", help="skip the model-fitting half of the metric")
+    ap.add_argument("--persist-threads", type=int, default=None, choices=[256, 512, 1024],
+                    help="threads per block of the persistent kernel (default: automatic)")
     ap.add_argument("--fit-targets", type=int, default=256)
     ap.add_argument("--fit-train", type=int, default=1 << 20)
     ap.add_argument("--fit-epochs", type=int, default=40)
@@ -445,7 +447,8 @@ def main():
         return
     world, rank, local = dist_setup(args)
     import brian_b200 as b
-    b.set_global_preferences(precision=args.precision, device=local)
+    b.set_global_preferences(precision=args.precision, device=local,
+                             persistent=True if args.persist_threads is None else args.persist_threads)
     inp = make_inputs(args.seed + rank, n=args.neurons)
     net, P, conns, _ = build_network(inp)
     net.prepare()
@@ -467,6 +470,7 @@ def main():
     barrier(world)
     sp1, ev1 = rt.counters(1, 2)
     launches = rt.stats()["launches"] - l0
+    persist_threads = rt.stats().get("persistent_threads", 0)
     events = int(ev1.sum() - ev0.sum())
     spikes = int(sp1.sum() - sp0.sum())
     dev_s = allreduce_max(dev_ms / 1e3, world)
@@ -552,6 +556,7 @@ def main():
                                        "u8 delays 1..50 steps, FP%d state, dt 0.1 ms" % args.precision,
                            "neurons": n, "synapses": int(len(inp["exc"][1]) + len(inp["inh"][1])),
                            "sim_steps_per_step": per, "simulated_s": args.steps * per * DT,
+                           "persistent_threads": persist_threads,
                            "parallelism": "replicas" if world > 1 else "single",
                            "l2": "inputs larger than L2: 1.3 GB of connectivity (int32 targets, u8 delays), of "
                                  "which the spiking sources' rows are read every step; the two uint16 count rings "

@@ -59,6 +59,7 @@ ENGINE_ONLY = {
     "net_item_name": [_vp, _i64, ct.c_char_p, _i64],
     "fixed_indegree_csr": [_i64, _i64, _i64, _u64, _vp, _vp],
     "net_set_persistent": [_vp, ct.c_int],
+    "net_persistent_threads": [_vp, _P(_i32)],
     "fit_compile_check": [ct.c_int, _vp, _dbl, ct.c_int, ct.c_int, ct.c_char_p, _i64],
     "fit_create": [_P(_vp), ct.c_int, ct.c_int, _vp, _dbl, ct.c_int, ct.c_int],
     "fit_destroy": [_vp],
@@ -150,8 +151,8 @@ class Runtime(object):
         self.precision = precision
         self.t.check(self.t.net_create(device, precision, 1 if deterministic else 0, float(dt),
                                        ct.byref(self.h)), "net_create")
-        if not persistent and hasattr(self.t, "net_set_persistent"):
-            self.t.check(self.t.net_set_persistent(self.h, 0), "net_set_persistent")
+        if persistent is not True and hasattr(self.t, "net_set_persistent"):
+            self.t.check(self.t.net_set_persistent(self.h, int(persistent)), "net_set_persistent")
 
     def close(self):
         if self.h:
@@ -322,7 +323,12 @@ class Runtime(object):
     def stats(self):
         s, l, ms = _i64(), _i64(), _dbl()
         self._c(self.t.net_stats(self.h, ct.byref(s), ct.byref(l), ct.byref(ms)), "net_stats")
-        return {"steps": s.value, "launches": l.value, "last_run_ms": ms.value}
+        out = {"steps": s.value, "launches": l.value, "last_run_ms": ms.value}
+        if hasattr(self.t, "net_persistent_threads"):
+            th = _i32()
+            self._c(self.t.net_persistent_threads(self.h, ct.byref(th)), "net_persistent_threads")
+            out["persistent_threads"] = th.value
+        return out
 
 
 def fixed_indegree_csr_native(n_src, n_tgt, k, seed):

@@ -150,15 +150,15 @@ __device__ __forceinline__ T get_var(const T (&s)[NV], int var) {
 // s with spref[s] <= e < spref[s+1] and is synapse srow[s] + e - spref[s].
 // Each thread loads kPushUnroll independent synapses before issuing their
 // atomics.  Count rings need no weight.
-template <typename T>
+template <typename T, int TH = kHeadThreads>
 __device__ __forceinline__ void scatter_batch(const Push<T> &q, int cur, const int64_t *srow, const int32_t *spref,
                                               int nb, int total) {
     const int tid = threadIdx.x;
-    for (int e0 = 0; e0 < total; e0 += kHeadThreads * kPushUnroll) {
+    for (int e0 = 0; e0 < total; e0 += TH * kPushUnroll) {
         int32_t col[kPushUnroll]; T wv[kPushUnroll]; int slot[kPushUnroll];
 #pragma unroll
         for (int u = 0; u < kPushUnroll; ++u) {
-            const int e = e0 + u * kHeadThreads + tid;
+            const int e = e0 + u * TH + tid;
             col[u] = -1;
             wv[u] = T(0);
             slot[u] = 0;

@@ -83,6 +83,8 @@ using Launch = std::function<cudaError_t(cudaStream_t, int tail, int last)>;
 struct bg_net {
     int device = 0, precision = 64, deterministic = 1; double dt = 1e-4;
     int allow_persist = 1;
+    int persist_th = 0;                 // forced threads per block of the persistent kernel (0: automatic)
+    int persist_used = 0;               // threads per block of the built persistent kernel (0: none)
     cudaStream_t stream = nullptr;
     std::vector<HGroup> groups; std::vector<HConn> conns; std::vector<HStdp> stdps;
     std::vector<HSpikeMon> smons; std::vector<HStateMon> stmons; std::vector<Item> items;
@@ -438,22 +440,65 @@ int drain(bg_net *net, long long chunk_base_cs, long long tail_done_upto, long l
 
 namespace {
 
-template <typename T, int NV>
+// Shapes of the persistent kernel: threads per block and neurons per thread.
+// 256 x 4 and 512 x 2 make 1024-neuron blocks, 1024 x 2 makes 2048-neuron
+// blocks.
+constexpr int persist_npt(int th) { return th == 256 ? 4 : 2; }
+
+template <typename T, int NV, int TH>
 cudaError_t launch_persist_nv(bg::PersistArgs<T> a, int64_t blocks, cudaStream_t s) {
     void *args[] = {(void *)&a};
-    return cudaLaunchCooperativeKernel((const void *)bg::k_persist<T, NV>, dim3((unsigned)blocks),
-                                       dim3(bg::kHeadThreads), args, 0, s);
+    return cudaLaunchCooperativeKernel((const void *)bg::k_persist<T, NV, TH, persist_npt(TH)>, dim3((unsigned)blocks),
+                                       dim3(TH), args, 0, s);
 }
 
-template <typename T, int NV>
-int persist_fits(int64_t blocks) {
-    int per_sm = 0, dev = 0, coop = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
-    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-    if (!coop) return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bg::k_persist<T, NV>, bg::kHeadThreads, 0) != cudaSuccess)
-        return 0;
-    return (int64_t)per_sm * sm_count() >= blocks;
+template <typename T, int TH>
+cudaError_t launch_persist_th(bg::PersistArgs<T> a, int nvar, int64_t blocks, cudaStream_t s) {
+    switch (nvar) {
+    case 1: return launch_persist_nv<T, 1, TH>(a, blocks, s);
+    case 2: return launch_persist_nv<T, 2, TH>(a, blocks, s);
+    case 3: return launch_persist_nv<T, 3, TH>(a, blocks, s);
+    default: return launch_persist_nv<T, 4, TH>(a, blocks, s);
+    }
+}
+
+// Co-resident blocks of the persistent kernel of one shape on the device.
+template <typename T, int TH>
+int64_t persist_slots(int nvar) {
+    constexpr int NPT = persist_npt(TH);
+    int per_sm = 0;
+    cudaError_t e;
+    switch (nvar) {
+    case 1: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bg::k_persist<T, 1, TH, NPT>, TH, 0); break;
+    case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bg::k_persist<T, 2, TH, NPT>, TH, 0); break;
+    case 3: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bg::k_persist<T, 3, TH, NPT>, TH, 0); break;
+    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bg::k_persist<T, 4, TH, NPT>, TH, 0); break;
+    }
+    if (e != cudaSuccess) { cudaGetLastError(); return 0; }
+    return (int64_t)per_sm * sm_count();
+}
+
+// Threads per block of the persistent kernel.  Fewer, larger blocks wait on
+// fewer arrivals per step and even out the spike counts per block, and more
+// warps per SM hide the latency of each step's dependent loads: 1024-neuron
+// blocks of 512 threads while one block per SM covers the group, then
+// 2048-neuron blocks of 1024 threads, then 1024-neuron blocks two per SM.
+// 0 when no shape fits co-resident on the device.
+template <typename T>
+int persist_threads(int64_t n, int nvar, int forced) {
+    const int64_t nsm = sm_count();
+    auto blocks = [n](int th) { return (n + (int64_t)th * persist_npt(th) - 1) / ((int64_t)th * persist_npt(th)); };
+    auto fits = [&](int th) {
+        const int64_t b = blocks(th);
+        return th == 256 ? b <= persist_slots<T, 256>(nvar) : th == 512 ? b <= persist_slots<T, 512>(nvar)
+                                                                          : b <= persist_slots<T, 1024>(nvar);
+    };
+    if (forced) return fits(forced) ? forced : 0;
+    if (blocks(512) <= nsm && fits(512)) return 512;
+    if (blocks(1024) <= nsm && fits(1024)) return 1024;
+    if (fits(512)) return 512;
+    if (fits(256)) return 256;
+    return 0;
 }
 
 // The persistent path applies to one linear group (at most 4 variables, no
@@ -473,16 +518,25 @@ int build_persist(bg_net *net) {
         if (!c.fused_push || c.src != 0 || c.tgt != 0) return BG_OK;
         for (uint8_t d : c.d) min_d = std::min<int>(min_d, d);
     }
-    const int64_t blocks = g.npad / bg::kBlockNeurons;
-    int fits = 0;
-    switch (g.nvar) {
-    case 1: fits = persist_fits<T, 1>(blocks); break;
-    case 2: fits = persist_fits<T, 2>(blocks); break;
-    case 3: fits = persist_fits<T, 3>(blocks); break;
-    default: fits = persist_fits<T, 4>(blocks); break;
+    {
+        int dev = 0, coop = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) return BG_OK;
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+        if (!coop) return BG_OK;
     }
+    const int th = persist_threads<T>(g.n, g.nvar, net->persist_th);
     cudaGetLastError();
-    if (!fits) return BG_OK;
+    if (!th) return BG_OK;
+    const int64_t bn = (int64_t)th * persist_npt(th), blocks = (g.n + bn - 1) / bn;
+    net->persist_used = 0;
+    // a block's synapse rows must span fewer than 2^32 entries (32-bit
+    // offsets in shared memory)
+    for (const HConn &c : net->conns)
+        for (int64_t b = 0; b < blocks; ++b) {
+            const int64_t lo = std::min(std::max(b * bn - c.so, (int64_t)0), c.sn);
+            const int64_t hi = std::min(std::max((b + 1) * bn - c.so, (int64_t)0), c.sn);
+            if (c.rowptr[hi] - c.rowptr[lo] >= ((int64_t)1 << 32)) return BG_OK;
+        }
     if (net->alloc(&net->dArrived, 64) != cudaSuccess) return fail(BG_ENOMEM, "arrival counter");
     bg::PersistArgs<T> a;
     std::memset(&a, 0, sizeof(a));
@@ -515,15 +569,15 @@ int build_persist(bg_net *net) {
     a.lag = min_d >= 1 ? 2 : 1;
     const int nvar = g.nvar;
     unsigned int *arr = net->dArrived;
-    net->persist = [a, blocks, nvar, arr](cudaStream_t s, int nsteps) {
+    net->persist_used = th;
+    net->persist = [a, blocks, nvar, arr, th](cudaStream_t s, int nsteps) {
         cudaError_t e = cudaMemsetAsync(arr, 0, 64, s);
         if (e != cudaSuccess) return e;
         bg::PersistArgs<T> b = a; b.nsteps = nsteps;
-        switch (nvar) {
-        case 1: return launch_persist_nv<T, 1>(b, blocks, s);
-        case 2: return launch_persist_nv<T, 2>(b, blocks, s);
-        case 3: return launch_persist_nv<T, 3>(b, blocks, s);
-        default: return launch_persist_nv<T, 4>(b, blocks, s);
+        switch (th) {
+        case 256: return launch_persist_th<T, 256>(b, nvar, blocks, s);
+        case 512: return launch_persist_th<T, 512>(b, nvar, blocks, s);
+        default: return launch_persist_th<T, 1024>(b, nvar, blocks, s);
         }
     };
     return BG_OK;
@@ -1159,7 +1213,17 @@ int bg_group_set_state(bg_net *n, int32_t gid, int var, const double *in) {
 int bg_net_set_persistent(bg_net *n, int enable) {
     if (!n) return fail(BG_EINVAL, "net");
     if (n->prepared) return fail(BG_ESTATE, "set before prepare");
+    if (enable != 0 && enable != 1 && enable != 256 && enable != 512 && enable != 1024)
+        return fail(BG_EINVAL, "persistent: 0, 1, 256, 512 or 1024");
     n->allow_persist = enable ? 1 : 0;
+    n->persist_th = enable > 1 ? enable : 0;
+    return BG_OK;
+}
+
+int bg_net_persistent_threads(bg_net *n, int32_t *threads) {
+    if (!n || !threads) return fail(BG_EINVAL, "net");
+    if (!n->prepared) { int st = bg_net_prepare(n); if (st) return st; }
+    *threads = n->persist ? n->persist_used : 0;
     return BG_OK;
 }
 

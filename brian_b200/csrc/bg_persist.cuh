@@ -2,18 +2,20 @@
 // linear group whose outgoing connections are DelayConnections on the
 // shared-weight (atomic) path: the CUBA topology of Brian's benchmarks.
 //
-// Each block owns kBlockNeurons neurons for the whole launch and keeps their
-// state in registers; the row pointers of those neurons are staged in shared
-// memory once.  A step is: [wait] -> ring delivery + reset of the previous
-// step -> linear update + threshold -> push of this block's spikes into the
-// rings -> arrive.  Ring row r is delivered at step t+1 when r = t mod md and
-// receives pushes from steps t-d (d >= 1), so delivering at step t+1 needs
-// the pushes of steps <= t-1 of every block, i.e. the arrivals of step t-1:
-// blocks may drift one step apart and the wait is nearly always already
-// satisfied.  (With a zero delay the wait is for step t.)  The two spare ring
-// rows keep a block that is one step ahead from pushing into a row that a
-// lagging block is still delivering.  Every wait is bounded; on timeout the
-// block raises BG_DERR_TIMEOUT and leaves the loop.
+// Each block owns TH x NPT neurons for the whole launch and keeps their state
+// in registers; the row pointers of those neurons are staged in shared memory
+// once.  A step is: [wait] -> ring delivery + reset of the previous step ->
+// linear update + threshold -> push of this block's spikes into the rings ->
+// arrive.  Ring row r is delivered at step t+1 when r = t mod md and receives
+// pushes from steps t-d (d >= 1), so delivering at step t+1 needs the pushes
+// of steps <= t-1 of every block, i.e. the arrivals of step t-1: blocks may
+// drift one step apart and the wait is nearly always already satisfied.
+// (With a zero delay the wait is for step t.)  The two spare ring rows keep a
+// block that is one step ahead from pushing into a row that a lagging block
+// is still delivering.  Thread 0 publishes the arrival (a release: one L2
+// round trip) while warp 1 polls for the next step's wait (an acquire: one
+// more), so the two overlap.  Every wait is bounded; on timeout the block
+// raises BG_DERR_TIMEOUT and leaves the loop.
 #pragma once
 #include "bg_kernels.cuh"
 
@@ -70,33 +72,40 @@ __device__ __forceinline__ void uset(T (&s)[NV], int var, T v) {
     }
 }
 
-template <typename T, int NV>
-__global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T> a) {
-    __shared__ int64_t srp[kPersistMaxPush][kBlockNeurons + 1];
-    __shared__ uint32_t words[kBlockNeurons / 32];
-    __shared__ int32_t sl[kBlockNeurons];
+template <typename T, int NV, int TH, int NPT>
+__global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const PersistArgs<T> a) {
+    constexpr int BN = TH * NPT;                                // neurons per block
+    static_assert(TH >= 64 && TH % 32 == 0, "thread 0 arrives while warp 1 polls");
+    // row pointers of the block's neurons, relative to the first one (the
+    // host keeps the persistent path to blocks whose rows span < 2^32)
+    __shared__ uint32_t srp[kPersistMaxPush][BN + 1];
+    __shared__ int64_t srp0[kPersistMaxPush];
+    __shared__ uint32_t words[BN / 32];
+    __shared__ int32_t sl[BN];
     __shared__ int64_t srow[kPushBatch];
     __shared__ int32_t spref[kPushBatch + 1];
     __shared__ int nsp, abort_flag;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int base = blockIdx.x * kBlockNeurons;               // neuron counts < 2^31
-    const int nvalid = (int)min((int64_t)kBlockNeurons, a.n - (int64_t)base);
+    const int base = blockIdx.x * BN;               // neuron counts < 2^31
+    const int nvalid = (int)min((int64_t)BN, a.n - (int64_t)base);
     const unsigned int G = gridDim.x;
     const long long t0 = a.ctl->nstep;
     for (int p = 0; p < a.npush; ++p) {
         const Push<T> &q = a.push[p];
-        for (int j = tid; j <= kBlockNeurons; j += kHeadThreads) {
+        const int64_t r0 = min(max((int64_t)base - q.so, (int64_t)0), q.sn);
+        for (int j = tid; j <= BN; j += TH) {
             int64_t r = (int64_t)base + j - q.so;
             r = r < 0 ? 0 : (r > q.sn ? q.sn : r);
-            srp[p][j] = q.rowptr[r];
+            srp[p][j] = (uint32_t)(q.rowptr[r] - q.rowptr[r0]);
         }
+        if (tid == 0) srp0[p] = q.rowptr[r0];
     }
     if (tid == 0) abort_flag = 0;
     // deliveries: does this block lie inside the target range?  (uniform)
     bool dfull[kMaxDeliv];
 #pragma unroll
     for (int d = 0; d < kMaxDeliv; ++d)
-        dfull[d] = d < a.ndeliv && a.deliv[d].to <= base && (int64_t)base + kBlockNeurons <= a.deliv[d].to + a.deliv[d].tn;
+        dfull[d] = d < a.ndeliv && a.deliv[d].to <= base && (int64_t)base + BN <= a.deliv[d].to + a.deliv[d].tn;
     // count tables staged in shared memory when they fit (uniform decision)
     __shared__ T stab[kPersistTable];
     int toff[kMaxDeliv];
@@ -115,17 +124,17 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T
         if (staged)
             for (int d = 0; d < a.ndeliv; ++d)
                 if (a.deliv[d].cring)
-                    for (int k = tid; k < a.deliv[d].tablen; k += kHeadThreads) stab[toff[d] + k] = a.deliv[d].table[k];
+                    for (int k = tid; k < a.deliv[d].tablen; k += TH) stab[toff[d] + k] = a.deliv[d].table[k];
     }
     // pushes whose source range meets this block (uniform)
     bool pact[kPersistMaxPush];
 #pragma unroll
     for (int p = 0; p < kPersistMaxPush; ++p)
-        pact[p] = p < a.npush && a.push[p].so < (int64_t)base + kBlockNeurons && a.push[p].so + a.push[p].sn > base;
-    T s[kNPT][NV];
+        pact[p] = p < a.npush && a.push[p].so < (int64_t)base + BN && a.push[p].so + a.push[p].sn > base;
+    T s[NPT][NV];
 #pragma unroll
-    for (int u = 0; u < kNPT; ++u) {
-        const int li = u * kHeadThreads + tid;
+    for (int u = 0; u < NPT; ++u) {
+        const int li = u * TH + tid;
 #pragma unroll
         for (int k = 0; k < NV; ++k) s[u][k] = li < nvalid ? a.S[k * a.npad + base + li] : T(0);
     }
@@ -139,7 +148,9 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T
             // local step whose pushes must be complete in every block
             const long long le = (t - 1 - (a.lag == 2 ? 1 : 0)) - t0;
             if (le >= 0) {
-                if (tid == 0) {
+                // warp 1 polls while thread 0 may still be in the release of
+                // the previous step's arrival: the two round trips overlap
+                if (tid == 32) {
                     // arrivals are counted per step (slot le % 4): a running sum
                     // would also count blocks that are already one step ahead
                     const unsigned int *ctr = a.arrived + (le & 3);
@@ -156,19 +167,19 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T
             const int ps = (int)(t - 1);
             // issue every count-ring load of every delivery first: one L2
             // latency for all of them
-            uint16_t cnt[kMaxDeliv][kNPT];
+            uint16_t cnt[kMaxDeliv][NPT];
             uint16_t *crow[kMaxDeliv];
 #pragma unroll
             for (int d = 0; d < kMaxDeliv; ++d) {
                 crow[d] = nullptr;
 #pragma unroll
-                for (int u = 0; u < kNPT; ++u) cnt[d][u] = 0;
+                for (int u = 0; u < NPT; ++u) cnt[d][u] = 0;
                 if (d < a.ndeliv && a.deliv[d].cring) {
                     const Deliv<T> &dv = a.deliv[d];
                     crow[d] = dv.cring + (int64_t)(ps % dv.md) * dv.tnp + (base - dv.to);
 #pragma unroll
-                    for (int u = 0; u < kNPT; ++u) {
-                        const int li = u * kHeadThreads + tid;
+                    for (int u = 0; u < NPT; ++u) {
+                        const int li = u * TH + tid;
                         const int64_t gi = (int64_t)base + li;
                         if (li < nvalid && (dfull[d] || (gi >= dv.to && gi < dv.to + dv.tn))) cnt[d][u] = __ldcg(crow[d] + li);
                     }
@@ -181,9 +192,9 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T
                 const Deliv<T> &dv = a.deliv[d];
                 if (dv.cring) {
 #pragma unroll
-                    for (int u = 0; u < kNPT; ++u) {
+                    for (int u = 0; u < NPT; ++u) {
                         const int c = cnt[d][u];
-                        if (c) crow[d][u * kHeadThreads + tid] = 0;
+                        if (c) crow[d][u * TH + tid] = 0;
                         const T v = c ? (staged ? stab[toff[d] + c] : __ldg(dv.table + c)) : T(0);
                         uset<T, NV>(s[u], dv.var, rn<T>::add(uget<T, NV>(s[u], dv.var), v));
                     }
@@ -191,8 +202,8 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T
                     const int r = ps % dv.md;
                     T *row = dv.ring + (int64_t)r * dv.tn + (base - dv.to);
 #pragma unroll
-                    for (int u = 0; u < kNPT; ++u) {
-                        const int li = u * kHeadThreads + tid;
+                    for (int u = 0; u < NPT; ++u) {
+                        const int li = u * TH + tid;
                         const int64_t gi = (int64_t)base + li;
                         if (li < nvalid && (dfull[d] || (gi >= dv.to && gi < dv.to + dv.tn))) {
                             const T v = __ldcg(row + li);
@@ -204,7 +215,7 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T
             }
             if (a.reset_kind) {
 #pragma unroll
-                for (int u = 0; u < kNPT; ++u)
+                for (int u = 0; u < NPT; ++u)
                     if ((prev_spk >> u) & 1u)
                         uset<T, NV>(s[u], a.reset_var, a.reset_kind == 1 ? a.reset_val : uget<T, NV>(s[u], a.reset_var2));
             }
@@ -214,8 +225,8 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T
         prev_spk = 0;
         const int hslot = (int)t % a.depth;
 #pragma unroll
-        for (int u = 0; u < kNPT; ++u) {
-            const int li = u * kHeadThreads + tid;
+        for (int u = 0; u < NPT; ++u) {
+            const int li = u * TH + tid;
             T x[NV];
 #pragma unroll
             for (int j = 0; j < NV; ++j) x[j] = linear_row<T, NV>(a.A, a.C, a.anz, a.cnz, s[u], j);
@@ -230,7 +241,7 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T
             const uint32_t ball = __ballot_sync(0xffffffffu, spk);
             // (no history words: nothing reads them on this path)
             if (lane == 0) {
-                words[u * (kHeadThreads / 32) + warp] = ball;
+                words[u * (TH / 32) + warp] = ball;
                 my_spikes += __popc(ball);
             }
         }
@@ -241,14 +252,19 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T
         // (connection, spike) pair of the block
         if (a.npush && any_spike) {
             if (tid < 32) {
-                uint32_t w = words[lane];
-                const int c = __popc(w);
-                int incl = c;
+                int acc = 0;
 #pragma unroll
-                for (int o = 1; o < 32; o <<= 1) { const int v = __shfl_up_sync(0xffffffffu, incl, o); if (lane >= o) incl += v; }
-                int off = incl - c;
-                while (w) { const int b = __ffs(w) - 1; w &= w - 1; sl[off++] = lane * 32 + b; }
-                if (lane == 31) nsp = incl;
+                for (int c0 = 0; c0 < BN / 32; c0 += 32) {
+                    uint32_t w = c0 + lane < BN / 32 ? words[c0 + lane] : 0u;
+                    const int c = __popc(w);
+                    int incl = c;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) { const int v = __shfl_up_sync(0xffffffffu, incl, o); if (lane >= o) incl += v; }
+                    int off = acc + incl - c;
+                    while (w) { const int b = __ffs(w) - 1; w &= w - 1; sl[off++] = (c0 + lane) * 32 + b; }
+                    acc += __shfl_sync(0xffffffffu, incl, 31);
+                }
+                if (lane == 0) nsp = acc;
             }
             __syncthreads();
             const int n = nsp;
@@ -261,8 +277,8 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T
                     // warp 0: row starts and an inclusive scan of row lengths
                     if (tid < 32) {
                         int len0 = 0, len1 = 0;
-                        if (lane < nb) { const int j = sl[b0 + lane]; srow[lane] = srp[p][j]; len0 = (int)(srp[p][j + 1] - srp[p][j]); }
-                        if (lane + 32 < nb) { const int j = sl[b0 + lane + 32]; srow[lane + 32] = srp[p][j]; len1 = (int)(srp[p][j + 1] - srp[p][j]); }
+                        if (lane < nb) { const int j = sl[b0 + lane]; srow[lane] = srp0[p] + srp[p][j]; len0 = (int)(srp[p][j + 1] - srp[p][j]); }
+                        if (lane + 32 < nb) { const int j = sl[b0 + lane + 32]; srow[lane + 32] = srp0[p] + srp[p][j]; len1 = (int)(srp[p][j + 1] - srp[p][j]); }
                         int i0 = len0, i1 = len1;
 #pragma unroll
                         for (int o = 1; o < 32; o <<= 1) {
@@ -277,7 +293,7 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T
                     __syncthreads();
                     const int total = spref[nb];
                     if (tid == 0) my_events[p] += (unsigned long long)total;
-                    scatter_batch<T>(q, cur, srow, spref, nb, total);
+                    scatter_batch<T, TH>(q, cur, srow, spref, nb, total);
                     __syncthreads();
                 }
             }
@@ -289,8 +305,8 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_persist(const PersistArgs<T
         if (tid == 0) red_release_add(a.arrived + (st & 3), 1u);
     }
 #pragma unroll
-    for (int u = 0; u < kNPT; ++u) {
-        const int li = u * kHeadThreads + tid;
+    for (int u = 0; u < NPT; ++u) {
+        const int li = u * TH + tid;
         if (li < nvalid) {
 #pragma unroll
             for (int k = 0; k < NV; ++k) a.S[k * a.npad + base + li] = s[u][k];

@@ -60,7 +60,7 @@ def cuba(N=4000, steps=10000, seed=1, p=0.02, record=10, refractory=0.0):
 
 
 def cuba_delay(N=3000, indegree=100, steps=2000, seed=3, wdtype=np.float32, we=0.162e-2, wi=-0.9e-2,
-               hetero_weights=False, monitors=True, dmin=1, runs=1):
+               hetero_weights=False, monitors=True, dmin=1, runs=1, persistent=True):
     """Config 2 in miniature: fixed in-degree (80% exc / 20% inh), integer
     delays uniform in 1..50 steps, DelayConnections into ge and gi."""
     taum, taue, taui = 20 * ms, 5 * ms, 10 * ms
@@ -86,12 +86,20 @@ def cuba_delay(N=3000, indegree=100, steps=2000, seed=3, wdtype=np.float32, we=0
     P.v = Vr + rng.random(N) * (Vt - Vr)
     if not monitors:
         # no monitors: the engine may take its persistent single-launch path
-        net = b.Network(P, conns[0], conns[1])
-        for _ in range(runs):
-            net.run(steps * 0.1 * ms / runs)
+        prev = b.get_global_preference("persistent")
+        b.set_global_preferences(persistent=persistent)
+        try:
+            net = b.Network(P, conns[0], conns[1])
+            for _ in range(runs):
+                net.run(steps * 0.1 * ms / runs)
+        finally:
+            b.set_global_preferences(persistent=prev)
         out = _result(net, groups=[P])
         g, c = net._binding.rt.counters(1, 2)
         out["spikes"], out["events"] = g.copy(), c.copy()
+        st = net.stats()
+        out["launches"] = st["launches"]
+        out["persistent_threads"] = st.get("persistent_threads", 0)
         return out
     M = b.SpikeMonitor(P)
     S = b.StateMonitor(P, "v", record=[0, 1, N - 1])

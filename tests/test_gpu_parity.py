@@ -54,9 +54,28 @@ def test_persistent_path_bit_exact(oracle_table, gpu_table, dmin, runs):
     ref, gpu = _both(scenarios.cuba_delay, oracle_table, monitors=False, dmin=dmin, runs=runs, N=6000,
                      steps=3000)
     assert ref["spikes"][0] > 1000
+    ref.pop("launches"), ref.pop("persistent_threads")
+    launches, th = gpu.pop("launches"), gpu.pop("persistent_threads")
     scenarios.compare(ref, gpu)
+    assert th == 512                        # 6 blocks of 1024 neurons
     import brian_b200 as bb
     assert bb.network._magic_cache is not None
+    assert launches == runs                 # one cooperative launch per run
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("threads", [256, 512, 1024])
+def test_persistent_block_sizes_bit_exact(oracle_table, gpu_table, threads):
+    """Every shape of the persistent kernel (ragged last block at N=7000;
+    for 2048-neuron blocks, spike lists longer than one 32-word warp scan)
+    gives the oracle's results bit for bit."""
+    ref, gpu = _both(scenarios.cuba_delay, oracle_table, monitors=False, N=7000, steps=2000, runs=2,
+                     persistent=threads)
+    assert ref["spikes"][0] > 1000
+    ref.pop("launches"), ref.pop("persistent_threads")
+    launches, th = gpu.pop("launches"), gpu.pop("persistent_threads")
+    scenarios.compare(ref, gpu)
+    assert launches == 2 and th == threads
 
 
 @pytest.mark.gpu
