@@ -72,6 +72,20 @@ __device__ __forceinline__ void uset(T (&s)[NV], int var, T v) {
     }
 }
 
+// Uniform dispatch on a state-variable index hoisted out of the per-neuron
+// loops: f receives the index as a compile-time constant, so the neuron loop
+// inside it indexes registers directly and the branch runs once per thread.
+template <int K> struct VarIdx { static constexpr int value = K; };
+template <int NV, typename F>
+__device__ __forceinline__ void on_var(int var, F &&f) {
+    switch (var) {
+    case 0: f(VarIdx<0>()); break;
+    case 1: if constexpr (NV > 1) f(VarIdx<1>()); break;
+    case 2: if constexpr (NV > 2) f(VarIdx<2>()); break;
+    default: if constexpr (NV > 3) f(VarIdx<3>()); break;
+    }
+}
+
 template <typename T, int NV, int TH, int NPT>
 __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const PersistArgs<T> a) {
     constexpr int BN = TH * NPT;                                // neurons per block
@@ -191,13 +205,18 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
                 if (d >= a.ndeliv) break;
                 const Deliv<T> &dv = a.deliv[d];
                 if (dv.cring) {
+                    T v[NPT];
 #pragma unroll
                     for (int u = 0; u < NPT; ++u) {
                         const int c = cnt[d][u];
                         if (c) crow[d][u * TH + tid] = 0;
-                        const T v = c ? (staged ? stab[toff[d] + c] : __ldg(dv.table + c)) : T(0);
-                        uset<T, NV>(s[u], dv.var, rn<T>::add(uget<T, NV>(s[u], dv.var), v));
+                        v[u] = c ? (staged ? stab[toff[d] + c] : __ldg(dv.table + c)) : T(0);
                     }
+                    on_var<NV>(dv.var, [&](auto K) {
+                        constexpr int k = decltype(K)::value;
+#pragma unroll
+                        for (int u = 0; u < NPT; ++u) s[u][k] = rn<T>::add(s[u][k], v[u]);
+                    });
                 } else {
                     const int r = ps % dv.md;
                     T *row = dv.ring + (int64_t)r * dv.tn + (base - dv.to);
@@ -213,32 +232,68 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
                     }
                 }
             }
-            if (a.reset_kind) {
+            if (a.reset_kind == 1) {
+                on_var<NV>(a.reset_var, [&](auto K) {
+                    constexpr int k = decltype(K)::value;
+#pragma unroll
+                    for (int u = 0; u < NPT; ++u)
+                        if ((prev_spk >> u) & 1u) s[u][k] = a.reset_val;
+                });
+            } else if (a.reset_kind) {
 #pragma unroll
                 for (int u = 0; u < NPT; ++u)
-                    if ((prev_spk >> u) & 1u)
-                        uset<T, NV>(s[u], a.reset_var, a.reset_kind == 1 ? a.reset_val : uget<T, NV>(s[u], a.reset_var2));
+                    if ((prev_spk >> u) & 1u) uset<T, NV>(s[u], a.reset_var, uget<T, NV>(s[u], a.reset_var2));
             }
         }
         if (st == a.nsteps) break;
         // ---- update, threshold, history
         prev_spk = 0;
         const int hslot = (int)t % a.depth;
+        {
+            // x = A s (+ C), each row summed over k in ascending order with the
+            // zero coefficients skipped (the order of linear_row); the mask
+            // tests are uniform and run once per thread, not per neuron
+            T x[NPT][NV];
+#pragma unroll
+            for (int j = 0; j < NV; ++j) {
+#pragma unroll
+                for (int u = 0; u < NPT; ++u) x[u][j] = T(0);
+#pragma unroll
+                for (int k = 0; k < NV; ++k)
+                    if (a.anz & (1ull << (j * NV + k))) {
+                        const T c = a.A[j * NV + k];
+#pragma unroll
+                        for (int u = 0; u < NPT; ++u) x[u][j] = rn<T>::add(x[u][j], rn<T>::mul(c, s[u][k]));
+                    }
+                if (a.cnz & (1u << j)) {
+#pragma unroll
+                    for (int u = 0; u < NPT; ++u) x[u][j] = rn<T>::add(x[u][j], a.C[j]);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < NPT; ++u)
+#pragma unroll
+                for (int j = 0; j < NV; ++j) s[u][j] = x[u][j];
+        }
+        bool spk[NPT];
+#pragma unroll
+        for (int u = 0; u < NPT; ++u) spk[u] = false;
+        if (a.thr_kind == 1) {
+            on_var<NV>(a.thr_var, [&](auto K) {
+                constexpr int k = decltype(K)::value;
+#pragma unroll
+                for (int u = 0; u < NPT; ++u) spk[u] = s[u][k] > a.thr_val;
+            });
+        } else if (a.thr_kind == 2) {
+#pragma unroll
+            for (int u = 0; u < NPT; ++u) spk[u] = uget<T, NV>(s[u], a.thr_var) > uget<T, NV>(s[u], a.thr_var2);
+        }
 #pragma unroll
         for (int u = 0; u < NPT; ++u) {
             const int li = u * TH + tid;
-            T x[NV];
-#pragma unroll
-            for (int j = 0; j < NV; ++j) x[j] = linear_row<T, NV>(a.A, a.C, a.anz, a.cnz, s[u], j);
-#pragma unroll
-            for (int j = 0; j < NV; ++j) s[u][j] = x[j];
-            bool spk = false;
-            if (li < nvalid) {
-                if (a.thr_kind == 1) spk = uget<T, NV>(s[u], a.thr_var) > a.thr_val;
-                else if (a.thr_kind == 2) spk = uget<T, NV>(s[u], a.thr_var) > uget<T, NV>(s[u], a.thr_var2);
-            }
-            prev_spk |= (spk ? 1u : 0u) << u;
-            const uint32_t ball = __ballot_sync(0xffffffffu, spk);
+            spk[u] = spk[u] && li < nvalid;
+            prev_spk |= (spk[u] ? 1u : 0u) << u;
+            const uint32_t ball = __ballot_sync(0xffffffffu, spk[u]);
             // (no history words: nothing reads them on this path)
             if (lane == 0) {
                 words[u * (TH / 32) + warp] = ball;
