@@ -430,7 +430,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--neurons", type=int, default=N_NEURONS)
     ap.add_argument("--no-fit", action="store_true", help="skip the model-fitting half of the metric")
-    ap.add_argument("--persist-threads", type=int, default=None, choices=[256, 512, 1024],
+    ap.add_argument("--persist-threads", type=int, default=None, choices=[256, 512],
                     help="threads per block of the persistent kernel (default: automatic)")
     ap.add_argument("--fit-targets", type=int, default=256)
     ap.add_argument("--fit-train", type=int, default=1 << 20)

@@ -440,9 +440,8 @@ int drain(bg_net *net, long long chunk_base_cs, long long tail_done_upto, long l
 
 namespace {
 
-// Shapes of the persistent kernel: threads per block and neurons per thread.
-// 256 x 4 and 512 x 2 make 1024-neuron blocks, 1024 x 2 makes 2048-neuron
-// blocks.
+// Shapes of the persistent kernel: threads per block x neurons per thread,
+// 512 x 2 or 256 x 4, both 1024-neuron blocks.
 constexpr int persist_npt(int th) { return th == 256 ? 4 : 2; }
 
 template <typename T, int NV, int TH>
@@ -478,24 +477,16 @@ int64_t persist_slots(int nvar) {
     return (int64_t)per_sm * sm_count();
 }
 
-// Threads per block of the persistent kernel.  Fewer, larger blocks wait on
-// fewer arrivals per step and even out the spike counts per block, and more
-// warps per SM hide the latency of each step's dependent loads: 1024-neuron
-// blocks of 512 threads while one block per SM covers the group, then
-// 2048-neuron blocks of 1024 threads, then 1024-neuron blocks two per SM.
-// 0 when no shape fits co-resident on the device.
+// Threads per block of the persistent kernel: 512 x 2 (32 warps per SM at
+// two blocks per SM) hides more of each step's dependent latencies than
+// 256 x 4; both fit the same networks.  0 when no shape fits co-resident.
 template <typename T>
 int persist_threads(int64_t n, int nvar, int forced) {
-    const int64_t nsm = sm_count();
     auto blocks = [n](int th) { return (n + (int64_t)th * persist_npt(th) - 1) / ((int64_t)th * persist_npt(th)); };
     auto fits = [&](int th) {
-        const int64_t b = blocks(th);
-        return th == 256 ? b <= persist_slots<T, 256>(nvar) : th == 512 ? b <= persist_slots<T, 512>(nvar)
-                                                                          : b <= persist_slots<T, 1024>(nvar);
+        return th == 256 ? blocks(256) <= persist_slots<T, 256>(nvar) : blocks(512) <= persist_slots<T, 512>(nvar);
     };
     if (forced) return fits(forced) ? forced : 0;
-    if (blocks(512) <= nsm && fits(512)) return 512;
-    if (blocks(1024) <= nsm && fits(1024)) return 1024;
     if (fits(512)) return 512;
     if (fits(256)) return 256;
     return 0;
@@ -513,6 +504,7 @@ int build_persist(bg_net *net) {
     if (!g.linear || g.nvar < 1 || g.nvar > 4 || g.refr || g.period > 0) return BG_OK;
     if (g.thr_kind != BG_THR_CONST && g.thr_kind != BG_THR_VAR && g.thr_kind != BG_THR_NONE) return BG_OK;
     if (net->conns.empty() || (int)net->conns.size() > bg::kPersistMaxPush) return BG_OK;
+    if ((int)g.delivs.size() > bg::kPersistMaxDeliv) return BG_OK;
     int min_d = 255;
     for (const HConn &c : net->conns) {
         if (!c.fused_push || c.src != 0 || c.tgt != 0) return BG_OK;
@@ -574,11 +566,7 @@ int build_persist(bg_net *net) {
         cudaError_t e = cudaMemsetAsync(arr, 0, 64, s);
         if (e != cudaSuccess) return e;
         bg::PersistArgs<T> b = a; b.nsteps = nsteps;
-        switch (th) {
-        case 256: return launch_persist_th<T, 256>(b, nvar, blocks, s);
-        case 512: return launch_persist_th<T, 512>(b, nvar, blocks, s);
-        default: return launch_persist_th<T, 1024>(b, nvar, blocks, s);
-        }
+        return th == 256 ? launch_persist_th<T, 256>(b, nvar, blocks, s) : launch_persist_th<T, 512>(b, nvar, blocks, s);
     };
     return BG_OK;
 }
@@ -1213,8 +1201,8 @@ int bg_group_set_state(bg_net *n, int32_t gid, int var, const double *in) {
 int bg_net_set_persistent(bg_net *n, int enable) {
     if (!n) return fail(BG_EINVAL, "net");
     if (n->prepared) return fail(BG_ESTATE, "set before prepare");
-    if (enable != 0 && enable != 1 && enable != 256 && enable != 512 && enable != 1024)
-        return fail(BG_EINVAL, "persistent: 0, 1, 256, 512 or 1024");
+    if (enable != 0 && enable != 1 && enable != 256 && enable != 512)
+        return fail(BG_EINVAL, "persistent: 0, 1, 256 or 512");
     n->allow_persist = enable ? 1 : 0;
     n->persist_th = enable > 1 ? enable : 0;
     return BG_OK;

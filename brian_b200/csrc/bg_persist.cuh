@@ -22,6 +22,7 @@
 namespace bg {
 
 constexpr int kPersistMaxPush = 2;
+constexpr int kPersistMaxDeliv = 2;     // every connection targets the group itself
 constexpr int kPersistTable = 2048;     // shared-memory entries for count tables
 
 template <typename T> struct PersistArgs {
@@ -115,19 +116,35 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
         if (tid == 0) srp0[p] = q.rowptr[r0];
     }
     if (tid == 0) abort_flag = 0;
-    // deliveries: does this block lie inside the target range?  (uniform)
-    bool dfull[kMaxDeliv];
+    // deliveries: which of this thread's neurons each one targets (bit u),
+    // the thread's column in ring row 0, and the row delivered next (ring
+    // rows advance by one per step: no division in the loop)
+    uint32_t dm[kPersistMaxDeliv];
+    int drow[kPersistMaxDeliv];
+    int64_t dcol[kPersistMaxDeliv];
 #pragma unroll
-    for (int d = 0; d < kMaxDeliv; ++d)
-        dfull[d] = d < a.ndeliv && a.deliv[d].to <= base && (int64_t)base + BN <= a.deliv[d].to + a.deliv[d].tn;
+    for (int d = 0; d < kPersistMaxDeliv; ++d) {
+        dm[d] = 0; drow[d] = 0; dcol[d] = 0;
+        if (d < a.ndeliv) {
+            const Deliv<T> &dv = a.deliv[d];
+#pragma unroll
+            for (int u = 0; u < NPT; ++u) {
+                const int li = u * TH + tid;
+                const int64_t gi = (int64_t)base + li;
+                if (li < nvalid && gi >= dv.to && gi < dv.to + dv.tn) dm[d] |= 1u << u;
+            }
+            drow[d] = (int)(t0 % dv.md);         // row of the first delivery (step t0)
+            dcol[d] = (int64_t)base - dv.to + tid;
+        }
+    }
     // count tables staged in shared memory when they fit (uniform decision)
     __shared__ T stab[kPersistTable];
-    int toff[kMaxDeliv];
+    int toff[kPersistMaxDeliv];
     bool staged = true;
     {
         int o = 0;
 #pragma unroll
-        for (int d = 0; d < kMaxDeliv; ++d) {
+        for (int d = 0; d < kPersistMaxDeliv; ++d) {
             toff[d] = o;
             if (d < a.ndeliv && a.deliv[d].cring) {
                 if (a.deliv[d].tablen <= 0) staged = false;
@@ -152,6 +169,9 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
 #pragma unroll
         for (int k = 0; k < NV; ++k) s[u][k] = li < nvalid ? a.S[k * a.npad + base + li] : T(0);
     }
+    int pcur[kPersistMaxPush];                  // ring row of the current step, per push
+#pragma unroll
+    for (int p = 0; p < kPersistMaxPush; ++p) pcur[p] = p < a.npush ? (int)(t0 % a.push[p].md) : 0;
     unsigned int prev_spk = 0;                  // bit u: neuron u spiked last step
     unsigned long long my_spikes = 0, my_events[kPersistMaxPush] = {0, 0};
     __syncthreads();
@@ -178,30 +198,26 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
                 __syncthreads();
                 if (abort_flag) break;
             }
-            const int ps = (int)(t - 1);
             // issue every count-ring load of every delivery first: one L2
             // latency for all of them
-            uint16_t cnt[kMaxDeliv][NPT];
-            uint16_t *crow[kMaxDeliv];
+            uint16_t cnt[kPersistMaxDeliv][NPT];
+            uint16_t *crow[kPersistMaxDeliv];
 #pragma unroll
-            for (int d = 0; d < kMaxDeliv; ++d) {
+            for (int d = 0; d < kPersistMaxDeliv; ++d) {
                 crow[d] = nullptr;
 #pragma unroll
                 for (int u = 0; u < NPT; ++u) cnt[d][u] = 0;
                 if (d < a.ndeliv && a.deliv[d].cring) {
                     const Deliv<T> &dv = a.deliv[d];
-                    crow[d] = dv.cring + (int64_t)(ps % dv.md) * dv.tnp + (base - dv.to);
+                    crow[d] = dv.cring + (int64_t)drow[d] * dv.tnp + dcol[d];
 #pragma unroll
-                    for (int u = 0; u < NPT; ++u) {
-                        const int li = u * TH + tid;
-                        const int64_t gi = (int64_t)base + li;
-                        if (li < nvalid && (dfull[d] || (gi >= dv.to && gi < dv.to + dv.tn))) cnt[d][u] = __ldcg(crow[d] + li);
-                    }
+                    for (int u = 0; u < NPT; ++u)
+                        if ((dm[d] >> u) & 1u) cnt[d][u] = __ldcg(crow[d] + u * TH);
                 }
             }
             // then add in connection order (the reference's delivery order)
 #pragma unroll
-            for (int d = 0; d < kMaxDeliv; ++d) {
+            for (int d = 0; d < kPersistMaxDeliv; ++d) {
                 if (d >= a.ndeliv) break;
                 const Deliv<T> &dv = a.deliv[d];
                 if (dv.cring) {
@@ -209,7 +225,7 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
 #pragma unroll
                     for (int u = 0; u < NPT; ++u) {
                         const int c = cnt[d][u];
-                        if (c) crow[d][u * TH + tid] = 0;
+                        if (c) crow[d][u * TH] = 0;
                         v[u] = c ? (staged ? stab[toff[d] + c] : __ldg(dv.table + c)) : T(0);
                     }
                     on_var<NV>(dv.var, [&](auto K) {
@@ -218,19 +234,17 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
                         for (int u = 0; u < NPT; ++u) s[u][k] = rn<T>::add(s[u][k], v[u]);
                     });
                 } else {
-                    const int r = ps % dv.md;
-                    T *row = dv.ring + (int64_t)r * dv.tn + (base - dv.to);
+                    T *row = dv.ring + (int64_t)drow[d] * dv.tn + dcol[d];
 #pragma unroll
                     for (int u = 0; u < NPT; ++u) {
-                        const int li = u * TH + tid;
-                        const int64_t gi = (int64_t)base + li;
-                        if (li < nvalid && (dfull[d] || (gi >= dv.to && gi < dv.to + dv.tn))) {
-                            const T v = __ldcg(row + li);
-                            if (v != T(0)) row[li] = T(0);
+                        if ((dm[d] >> u) & 1u) {
+                            const T v = __ldcg(row + u * TH);
+                            if (v != T(0)) row[u * TH] = T(0);
                             uset<T, NV>(s[u], dv.var, rn<T>::add(uget<T, NV>(s[u], dv.var), v));
                         }
                     }
                 }
+                drow[d] = drow[d] + 1 == dv.md ? 0 : drow[d] + 1;
             }
             if (a.reset_kind == 1) {
                 on_var<NV>(a.reset_var, [&](auto K) {
@@ -248,7 +262,6 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
         if (st == a.nsteps) break;
         // ---- update, threshold, history
         prev_spk = 0;
-        const int hslot = (int)t % a.depth;
         {
             // x = A s (+ C), each row summed over k in ascending order with the
             // zero coefficients skipped (the order of linear_row); the mask
@@ -300,7 +313,6 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
                 my_spikes += __popc(ball);
             }
         }
-        (void)hslot;
         // the barrier also tells every thread whether the block spiked
         const int any_spike = __syncthreads_or(prev_spk != 0);
         // ---- push this block's spikes: one flattened scatter over every
@@ -323,10 +335,13 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
             }
             __syncthreads();
             const int n = nsp;
-            for (int p = 0; p < a.npush && n > 0; ++p) {
+            // unrolled over the push slots: pcur, pact and my_events stay in registers
+#pragma unroll
+            for (int p = 0; p < kPersistMaxPush; ++p) {
+                if (p >= a.npush || n == 0) break;
                 if (!pact[p]) continue;              // block-uniform
                 const Push<T> &q = a.push[p];
-                const int cur = (int)t % q.md;
+                const int cur = pcur[p];
                 for (int b0 = 0; b0 < n; b0 += kPushBatch) {
                     const int nb = min(kPushBatch, n - b0);
                     // warp 0: row starts and an inclusive scan of row lengths
@@ -353,6 +368,9 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
                 }
             }
         }
+#pragma unroll
+        for (int p = 0; p < kPersistMaxPush; ++p)
+            if (p < a.npush) pcur[p] = pcur[p] + 1 == a.push[p].md ? 0 : pcur[p] + 1;
         // ---- arrive: this block's pushes and ring clears of step t are
         // ordered before the arrival (release reduction, cumulative over the
         // block's writes through the barrier)

@@ -40,8 +40,8 @@ _table_override = []
 def set_global_preferences(**kw):
     """Reference preference registry (globalprefs.py:57-106); engine keys:
     precision (64|32), deterministic (bool), device (int), persistent (bool:
-    allow the single-launch step loop for networks of its shape; or 256, 512
-    or 1024: allow it with that many threads per block)."""
+    allow the single-launch step loop for networks of its shape; or 256 or
+    512: allow it with that many threads per block)."""
     _PREFS.update(kw)
 
 

@@ -210,11 +210,10 @@ BG_API int bg_fixed_indegree_csr(int64_t n_src, int64_t n_tgt, int64_t k,
                                  uint64_t seed, int64_t *rowptr,
                                  int32_t *cols);
 /* Allow (1, default) or forbid (0) the persistent single-launch step loop
- * for networks of its shape; call before bg_net_prepare.  256, 512 or 1024
- * allow it with that many threads per block (256 x 4 and 512 x 2 neurons
- * make 1024-neuron blocks, 1024 x 2 makes 2048-neuron blocks) instead of the
- * automatic choice, when the blocks fit co-resident.  All paths and block
- * shapes give identical results. */
+ * for networks of its shape; call before bg_net_prepare.  256 or 512 allow
+ * it with that many threads per block (256 x 4 or 512 x 2 neurons per
+ * block) instead of the automatic choice, when the blocks fit co-resident.
+ * All paths and block shapes give identical results. */
 BG_API int bg_net_set_persistent(bg_net *net, int enable);
 /* Threads per block of the persistent kernel the prepared network runs
  * with, or 0 when it runs the general per-step launches. */
