@@ -62,6 +62,7 @@ template <typename T> struct Push {
     const int64_t *rowptr; const int32_t *cols; const void *w; int w_bits; const uint8_t *d;
     unsigned long long *events;
     uint16_t *cring; int64_t tnp;      // count ring (shared weight), else null
+    const uint32_t *packed;            // persistent path: target | delay << 24 per synapse, else null
 };
 constexpr int kMaxPush = 4;
 
@@ -138,6 +139,34 @@ __device__ __forceinline__ T get_var(const T (&s)[NV], int var) {
 #pragma unroll
     for (int k = 0; k < NV; ++k) if (k == var) r = s[k];
     return r;
+}
+
+// scatter_batch for count rings whose synapses are packed as one word each
+// (target in the low 24 bits, delay in the high 8): one load per synapse.
+template <int TH>
+__device__ __forceinline__ void scatter_batch_packed(const uint32_t *packed, uint16_t *cring, int64_t tnp, int md,
+                                                     int cur, const int64_t *srow, const int32_t *spref, int nb,
+                                                     int total) {
+    const int tid = threadIdx.x;
+    for (int e0 = 0; e0 < total; e0 += TH * kPushUnroll) {
+        uint32_t pk[kPushUnroll];
+#pragma unroll
+        for (int u = 0; u < kPushUnroll; ++u) {
+            const int e = e0 + u * TH + tid;
+            pk[u] = 0xffffffffu;
+            if (e < total) {
+                int lo = 0, hi = nb;             // last s with spref[s] <= e
+                while (hi - lo > 1) { const int m = (lo + hi) >> 1; if (spref[m] <= e) lo = m; else hi = m; }
+                pk[u] = __ldg(packed + srow[lo] + (e - spref[lo]));
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kPushUnroll; ++u) {
+            if (pk[u] == 0xffffffffu) continue;
+            const int sl2 = cur + (int)(pk[u] >> 24);
+            cring_add(cring + (int64_t)(sl2 >= md ? sl2 - md : sl2) * tnp, (int32_t)(pk[u] & 0xffffffu));
+        }
+    }
 }
 
 // Push the spikes of one block (ascending, from the history words in shared

@@ -54,6 +54,7 @@ struct HConn {
     bool homogeneous = false; int parts = 1; int stdp = -1; bool fused_push = false;
     uint16_t *dCRing = nullptr; int64_t tnp = 0; void *dTable = nullptr; int tablen = 0;   // count ring (shared weight)
     int64_t *dRow = nullptr; int32_t *dCols = nullptr; void *dW = nullptr; uint8_t *dD = nullptr; void *dRing = nullptr;
+    uint32_t *dPacked = nullptr;       // persistent path: target | delay << 24 (count rings, targets < 2^24)
     int64_t *dColptr = nullptr, *dColk = nullptr; int32_t *dColsrc = nullptr;
     int64_t wcount() const { return dense ? sn * tn : nnz; }
 };
@@ -549,12 +550,24 @@ int build_persist(bg_net *net) {
     }
     a.npush = (int)net->conns.size();
     for (int p = 0; p < a.npush; ++p) {
-        const HConn &c = net->conns[p];
+        HConn &c = net->conns[p];
         bg::Push<T> &q = a.push[p];
         q.ring = (T *)c.dRing; q.md = c.md; q.so = c.so; q.sn = c.sn; q.tn = c.tn;
         q.rowptr = c.dRow; q.cols = c.dCols; q.w = c.dW; q.w_bits = c.w_bits; q.d = c.dD;
         q.events = net->dCounters + net->groups.size() + p;
         q.cring = c.dCRing; q.tnp = c.tnp;
+        // one word per synapse for the scatter: a single load (and a single
+        // stream of cache lines and pages) per synapse instead of two
+        if (c.dCRing && c.tn <= (1 << 24) && !c.cols.empty() && c.d.size() == c.cols.size()) {
+            if (!c.dPacked) {
+                std::vector<uint32_t> pk(c.cols.size());
+                for (size_t k = 0; k < pk.size(); ++k) pk[k] = (uint32_t)c.cols[k] | ((uint32_t)c.d[k] << 24);
+                if (net->alloc(&c.dPacked, pk.size() * 4) != cudaSuccess) return fail(BG_ENOMEM, "packed synapses");
+                int st = upload(net, c.dPacked, pk.data(), pk.size() * 4);
+                if (st) return st;
+            }
+            q.packed = c.dPacked;
+        }
     }
     a.spikes = net->dCounters;
     a.arrived = net->dArrived;

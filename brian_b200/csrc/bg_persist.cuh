@@ -363,7 +363,8 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
                     __syncthreads();
                     const int total = spref[nb];
                     if (tid == 0) my_events[p] += (unsigned long long)total;
-                    scatter_batch<T, TH>(q, cur, srow, spref, nb, total);
+                    if (q.packed) scatter_batch_packed<TH>(q.packed, q.cring, q.tnp, q.md, cur, srow, spref, nb, total);
+                    else scatter_batch<T, TH>(q, cur, srow, spref, nb, total);
                     __syncthreads();
                 }
             }
