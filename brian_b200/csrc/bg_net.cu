@@ -446,33 +446,35 @@ namespace {
 constexpr int persist_npt(int th) { return th == 256 ? 4 : 2; }
 
 template <typename T, int NV, int TH>
-cudaError_t launch_persist_nv(bg::PersistArgs<T> a, int64_t blocks, cudaStream_t s) {
+cudaError_t launch_persist_nv(bg::PersistArgs<T> a, bool diag, int64_t blocks, cudaStream_t s) {
     void *args[] = {(void *)&a};
-    return cudaLaunchCooperativeKernel((const void *)bg::k_persist<T, NV, TH, persist_npt(TH)>, dim3((unsigned)blocks),
-                                       dim3(TH), args, 0, s);
+    const void *k = diag ? (const void *)bg::k_persist<T, NV, TH, persist_npt(TH), true>
+                         : (const void *)bg::k_persist<T, NV, TH, persist_npt(TH), false>;
+    return cudaLaunchCooperativeKernel(k, dim3((unsigned)blocks), dim3(TH), args, 0, s);
 }
 
 template <typename T, int TH>
-cudaError_t launch_persist_th(bg::PersistArgs<T> a, int nvar, int64_t blocks, cudaStream_t s) {
+cudaError_t launch_persist_th(bg::PersistArgs<T> a, int nvar, bool diag, int64_t blocks, cudaStream_t s) {
     switch (nvar) {
-    case 1: return launch_persist_nv<T, 1, TH>(a, blocks, s);
-    case 2: return launch_persist_nv<T, 2, TH>(a, blocks, s);
-    case 3: return launch_persist_nv<T, 3, TH>(a, blocks, s);
-    default: return launch_persist_nv<T, 4, TH>(a, blocks, s);
+    case 1: return launch_persist_nv<T, 1, TH>(a, diag, blocks, s);
+    case 2: return launch_persist_nv<T, 2, TH>(a, diag, blocks, s);
+    case 3: return launch_persist_nv<T, 3, TH>(a, diag, blocks, s);
+    default: return launch_persist_nv<T, 4, TH>(a, diag, blocks, s);
     }
 }
 
-// Co-resident blocks of the persistent kernel of one shape on the device.
+// Co-resident blocks of the persistent kernel of one shape on the device
+// (the DIAG instance has the same limits or fewer registers).
 template <typename T, int TH>
 int64_t persist_slots(int nvar) {
     constexpr int NPT = persist_npt(TH);
     int per_sm = 0;
     cudaError_t e;
     switch (nvar) {
-    case 1: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bg::k_persist<T, 1, TH, NPT>, TH, 0); break;
-    case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bg::k_persist<T, 2, TH, NPT>, TH, 0); break;
-    case 3: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bg::k_persist<T, 3, TH, NPT>, TH, 0); break;
-    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bg::k_persist<T, 4, TH, NPT>, TH, 0); break;
+    case 1: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bg::k_persist<T, 1, TH, NPT, false>, TH, 0); break;
+    case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bg::k_persist<T, 2, TH, NPT, false>, TH, 0); break;
+    case 3: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bg::k_persist<T, 3, TH, NPT, false>, TH, 0); break;
+    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bg::k_persist<T, 4, TH, NPT, false>, TH, 0); break;
     }
     if (e != cudaSuccess) { cudaGetLastError(); return 0; }
     return (int64_t)per_sm * sm_count();
@@ -574,12 +576,19 @@ int build_persist(bg_net *net) {
     a.lag = min_d >= 1 ? 2 : 1;
     const int nvar = g.nvar;
     unsigned int *arr = net->dArrived;
+    // first row full, other rows diagonal, C at most in its first entry
+    // (read from the masks of the coefficients as the kernel's type holds them)
+    bool diag = (a.cnz & ~1u) == 0;
+    for (int j = 0; j < g.nvar; ++j)
+        for (int k = 0; k < g.nvar; ++k)
+            if ((((a.anz >> (j * g.nvar + k)) & 1ull) != 0) != (j == 0 || j == k)) diag = false;
     net->persist_used = th;
-    net->persist = [a, blocks, nvar, arr, th](cudaStream_t s, int nsteps) {
+    net->persist = [a, blocks, nvar, arr, th, diag](cudaStream_t s, int nsteps) {
         cudaError_t e = cudaMemsetAsync(arr, 0, 64, s);
         if (e != cudaSuccess) return e;
         bg::PersistArgs<T> b = a; b.nsteps = nsteps;
-        return th == 256 ? launch_persist_th<T, 256>(b, nvar, blocks, s) : launch_persist_th<T, 512>(b, nvar, blocks, s);
+        return th == 256 ? launch_persist_th<T, 256>(b, nvar, diag, blocks, s)
+                         : launch_persist_th<T, 512>(b, nvar, diag, blocks, s);
     };
     return BG_OK;
 }

@@ -87,7 +87,10 @@ __device__ __forceinline__ void on_var(int var, F &&f) {
     }
 }
 
-template <typename T, int NV, int TH, int NPT>
+// DIAG: the host found A's nonzeros to be exactly its first row and its
+// diagonal, and C's to be at most its first entry (a potential driven by
+// decaying synaptic variables, as in CUBA), so the update needs no mask tests.
+template <typename T, int NV, int TH, int NPT, bool DIAG>
 __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const PersistArgs<T> a) {
     constexpr int BN = TH * NPT;                                // neurons per block
     static_assert(TH >= 64 && TH % 32 == 0, "thread 0 arrives while warp 1 polls");
@@ -267,20 +270,37 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
             // zero coefficients skipped (the order of linear_row); the mask
             // tests are uniform and run once per thread, not per neuron
             T x[NPT][NV];
+            if constexpr (DIAG) {
+                // the same sums as below with the zero terms already left out
 #pragma unroll
-            for (int j = 0; j < NV; ++j) {
+                for (int u = 0; u < NPT; ++u) {
+                    T acc = T(0);
 #pragma unroll
-                for (int u = 0; u < NPT; ++u) x[u][j] = T(0);
+                    for (int k = 0; k < NV; ++k) acc = rn<T>::add(acc, rn<T>::mul(a.A[k], s[u][k]));
+                    x[u][0] = acc;
 #pragma unroll
-                for (int k = 0; k < NV; ++k)
-                    if (a.anz & (1ull << (j * NV + k))) {
-                        const T c = a.A[j * NV + k];
+                    for (int j = 1; j < NV; ++j) x[u][j] = rn<T>::add(T(0), rn<T>::mul(a.A[j * NV + j], s[u][j]));
+                }
+                if (a.cnz & 1u) {
 #pragma unroll
-                        for (int u = 0; u < NPT; ++u) x[u][j] = rn<T>::add(x[u][j], rn<T>::mul(c, s[u][k]));
+                    for (int u = 0; u < NPT; ++u) x[u][0] = rn<T>::add(x[u][0], a.C[0]);
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < NV; ++j) {
+#pragma unroll
+                    for (int u = 0; u < NPT; ++u) x[u][j] = T(0);
+#pragma unroll
+                    for (int k = 0; k < NV; ++k)
+                        if (a.anz & (1ull << (j * NV + k))) {
+                            const T c = a.A[j * NV + k];
+#pragma unroll
+                            for (int u = 0; u < NPT; ++u) x[u][j] = rn<T>::add(x[u][j], rn<T>::mul(c, s[u][k]));
+                        }
+                    if (a.cnz & (1u << j)) {
+#pragma unroll
+                        for (int u = 0; u < NPT; ++u) x[u][j] = rn<T>::add(x[u][j], a.C[j]);
                     }
-                if (a.cnz & (1u << j)) {
-#pragma unroll
-                    for (int u = 0; u < NPT; ++u) x[u][j] = rn<T>::add(x[u][j], a.C[j]);
                 }
             }
 #pragma unroll

@@ -60,16 +60,18 @@ def cuba(N=4000, steps=10000, seed=1, p=0.02, record=10, refractory=0.0):
 
 
 def cuba_delay(N=3000, indegree=100, steps=2000, seed=3, wdtype=np.float32, we=0.162e-2, wi=-0.9e-2,
-               hetero_weights=False, monitors=True, dmin=1, runs=1, persistent=True):
+               hetero_weights=False, monitors=True, dmin=1, runs=1, persistent=True, coupled=False):
     """Config 2 in miniature: fixed in-degree (80% exc / 20% inh), integer
     delays uniform in 1..50 steps, DelayConnections into ge and gi."""
     taum, taue, taui = 20 * ms, 5 * ms, 10 * ms
     Vt, Vr, El = -50 * mV, -60 * mV, -49 * mV
+    # coupled: gi is also driven by ge, so the update matrix is not "first
+    # row full, the rest diagonal"
     eqs = b.Equations("""
     dv/dt  = (ge+gi-(v-El))/taum : volt
     dge/dt = -ge/taue : volt
-    dgi/dt = -gi/taui : volt
-    """, taum=taum, taue=taue, taui=taui, El=El)
+    dgi/dt = %s/taui : volt
+    """ % ("(0.25*ge-gi)" if coupled else "-gi"), taum=taum, taue=taue, taui=taui, El=El)
     P = b.NeuronGroup(N, model=eqs, threshold=Vt, reset=Vr)
     Ne = int(0.8 * N)
     Pe, Pi = P.subgroup(Ne), P.subgroup(N - Ne)

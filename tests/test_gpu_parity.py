@@ -64,6 +64,18 @@ def test_persistent_path_bit_exact(oracle_table, gpu_table, dmin, runs):
 
 
 @pytest.mark.gpu
+def test_persistent_general_matrix_bit_exact(oracle_table, gpu_table):
+    """A linear update outside the specialised pattern (gi driven by ge)
+    takes the persistent kernel's general update."""
+    ref, gpu = _both(scenarios.cuba_delay, oracle_table, monitors=False, N=6000, steps=2000, coupled=True)
+    assert ref["spikes"][0] > 1000
+    ref.pop("launches"), ref.pop("persistent_threads")
+    launches, th = gpu.pop("launches"), gpu.pop("persistent_threads")
+    scenarios.compare(ref, gpu)
+    assert launches == 1 and th == 512
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("threads", [256, 512])
 def test_persistent_block_sizes_bit_exact(oracle_table, gpu_table, threads):
     """Both shapes of the persistent kernel (ragged last block at N=7000)
