@@ -102,6 +102,8 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
     __shared__ int32_t sl[BN];
     __shared__ int64_t srow[kPushBatch];
     __shared__ int32_t spref[kPushBatch + 1];
+    __shared__ int64_t srow1[kPersistMaxPush][kPushBatch];      // first batch, per connection
+    __shared__ int32_t spref1[kPersistMaxPush][kPushBatch + 1];
     __shared__ int nsp, abort_flag;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int base = blockIdx.x * BN;               // neuron counts < 2^31
@@ -338,6 +340,24 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
         // ---- push this block's spikes: one flattened scatter over every
         // (connection, spike) pair of the block
         if (a.npush && any_spike) {
+            // warp 0: the spike list, then for every connection the row starts
+            // and an inclusive scan of the row lengths of a batch of spikes
+            // (the first batch here, before the barrier; later ones below)
+            auto batch_rows = [&](int p, int b0, int nb, int64_t *rows, int32_t *pref) {
+                int len0 = 0, len1 = 0;
+                if (lane < nb) { const int j = sl[b0 + lane]; rows[lane] = srp0[p] + srp[p][j]; len0 = (int)(srp[p][j + 1] - srp[p][j]); }
+                if (lane + 32 < nb) { const int j = sl[b0 + lane + 32]; rows[lane + 32] = srp0[p] + srp[p][j]; len1 = (int)(srp[p][j + 1] - srp[p][j]); }
+                int i0 = len0, i1 = len1;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int v0 = __shfl_up_sync(0xffffffffu, i0, o), v1 = __shfl_up_sync(0xffffffffu, i1, o);
+                    if (lane >= o) { i0 += v0; i1 += v1; }
+                }
+                const int tot0 = __shfl_sync(0xffffffffu, i0, 31);
+                pref[lane + 1] = i0;
+                pref[lane + 33] = tot0 + i1;
+                if (lane == 0) pref[0] = 0;
+            };
             if (tid < 32) {
                 int acc = 0;
 #pragma unroll
@@ -351,6 +371,11 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
                     while (w) { const int b = __ffs(w) - 1; w &= w - 1; sl[off++] = (c0 + lane) * 32 + b; }
                     acc += __shfl_sync(0xffffffffu, incl, 31);
                 }
+                __syncwarp();
+                const int nb = min(kPushBatch, acc);
+#pragma unroll
+                for (int p = 0; p < kPersistMaxPush; ++p)
+                    if (p < a.npush && pact[p]) batch_rows(p, 0, nb, srow1[p], spref1[p]);
                 if (lane == 0) nsp = acc;
             }
             __syncthreads();
@@ -358,34 +383,25 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
             // unrolled over the push slots: pcur, pact and my_events stay in registers
 #pragma unroll
             for (int p = 0; p < kPersistMaxPush; ++p) {
-                if (p >= a.npush || n == 0) break;
+                if (p >= a.npush) break;
                 if (!pact[p]) continue;              // block-uniform
                 const Push<T> &q = a.push[p];
                 const int cur = pcur[p];
                 for (int b0 = 0; b0 < n; b0 += kPushBatch) {
                     const int nb = min(kPushBatch, n - b0);
-                    // warp 0: row starts and an inclusive scan of row lengths
-                    if (tid < 32) {
-                        int len0 = 0, len1 = 0;
-                        if (lane < nb) { const int j = sl[b0 + lane]; srow[lane] = srp0[p] + srp[p][j]; len0 = (int)(srp[p][j + 1] - srp[p][j]); }
-                        if (lane + 32 < nb) { const int j = sl[b0 + lane + 32]; srow[lane + 32] = srp0[p] + srp[p][j]; len1 = (int)(srp[p][j + 1] - srp[p][j]); }
-                        int i0 = len0, i1 = len1;
-#pragma unroll
-                        for (int o = 1; o < 32; o <<= 1) {
-                            const int v0 = __shfl_up_sync(0xffffffffu, i0, o), v1 = __shfl_up_sync(0xffffffffu, i1, o);
-                            if (lane >= o) { i0 += v0; i1 += v1; }
-                        }
-                        const int tot0 = __shfl_sync(0xffffffffu, i0, 31);
-                        spref[lane + 1] = i0;
-                        spref[lane + 33] = tot0 + i1;
-                        if (lane == 0) spref[0] = 0;
+                    const int64_t *rows = srow1[p];
+                    const int32_t *pref = spref1[p];
+                    if (b0 > 0) {
+                        __syncthreads();             // the previous batch is scattered
+                        if (tid < 32) batch_rows(p, b0, nb, srow, spref);
+                        __syncthreads();
+                        rows = srow;
+                        pref = spref;
                     }
-                    __syncthreads();
-                    const int total = spref[nb];
+                    const int total = pref[nb];
                     if (tid == 0) my_events[p] += (unsigned long long)total;
-                    if (q.packed) scatter_batch_packed<TH>(q.packed, q.cring, q.tnp, q.md, cur, srow, spref, nb, total);
-                    else scatter_batch<T, TH>(q, cur, srow, spref, nb, total);
-                    __syncthreads();
+                    if (q.packed) scatter_batch_packed<TH>(q.packed, q.cring, q.tnp, q.md, cur, rows, pref, nb, total);
+                    else scatter_batch<T, TH>(q, cur, rows, pref, nb, total);
                 }
             }
         }

@@ -60,7 +60,8 @@ def cuba(N=4000, steps=10000, seed=1, p=0.02, record=10, refractory=0.0):
 
 
 def cuba_delay(N=3000, indegree=100, steps=2000, seed=3, wdtype=np.float32, we=0.162e-2, wi=-0.9e-2,
-               hetero_weights=False, monitors=True, dmin=1, runs=1, persistent=True, coupled=False):
+               hetero_weights=False, monitors=True, dmin=1, runs=1, persistent=True, coupled=False,
+               burst=False):
     """Config 2 in miniature: fixed in-degree (80% exc / 20% inh), integer
     delays uniform in 1..50 steps, DelayConnections into ge and gi."""
     taum, taue, taui = 20 * ms, 5 * ms, 10 * ms
@@ -86,6 +87,10 @@ def cuba_delay(N=3000, indegree=100, steps=2000, seed=3, wdtype=np.float32, we=0
         C.connect_csr(rowptr, cols, wv, delay_steps=d)
         conns.append(C)
     P.v = Vr + rng.random(N) * (Vt - Vr)
+    if burst:
+        # every neuron a hair below threshold: the whole group fires within
+        # the first steps, far more spikes per block and step than one batch
+        P.v = Vt - 1e-7 * rng.random(N)
     if not monitors:
         # no monitors: the engine may take its persistent single-launch path
         prev = b.get_global_preference("persistent")

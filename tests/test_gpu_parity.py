@@ -64,6 +64,18 @@ def test_persistent_path_bit_exact(oracle_table, gpu_table, dmin, runs):
 
 
 @pytest.mark.gpu
+def test_persistent_burst_bit_exact(oracle_table, gpu_table):
+    """Synchronous firing: blocks push hundreds of spikes in one step, in
+    several batches of the persistent kernel's push."""
+    ref, gpu = _both(scenarios.cuba_delay, oracle_table, monitors=False, N=6000, steps=1500, burst=True)
+    assert ref["spikes"][0] > 10000       # all 6000 fire at step 0, then a second wave
+    ref.pop("launches"), ref.pop("persistent_threads")
+    launches, th = gpu.pop("launches"), gpu.pop("persistent_threads")
+    scenarios.compare(ref, gpu)
+    assert launches == 1 and th == 512
+
+
+@pytest.mark.gpu
 def test_persistent_general_matrix_bit_exact(oracle_table, gpu_table):
     """A linear update outside the specialised pattern (gi driven by ge)
     takes the persistent kernel's general update."""
