@@ -7,10 +7,13 @@
 // replays it from a CUDA graph of kGraphSteps steps, draining monitor
 // buffers to host memory between chunks.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "bg_kernels.cuh"
@@ -46,11 +49,60 @@ struct HGroup {
     int64_t *dGenSteps = nullptr; int32_t *dGenIdx = nullptr;
     std::vector<int> delivs, recs;
 };
+// A std::vector that leaves new elements uninitialised: the large host
+// copies of the connectivity are filled by parallel copies, which also
+// spreads the first touch of their pages over threads.
+template <typename T> struct NoInitAlloc : std::allocator<T> {
+    template <typename U> struct rebind { using other = NoInitAlloc<U>; };
+    NoInitAlloc() = default;
+    template <typename U> NoInitAlloc(const NoInitAlloc<U> &) {}
+    template <typename U> void construct(U *p) noexcept { ::new ((void *)p) U; }
+    template <typename U, typename... A> void construct(U *p, A &&...a) { ::new ((void *)p) U(std::forward<A>(a)...); }
+};
+template <typename T> using hvec = std::vector<T, NoInitAlloc<T>>;
+
+// f(lo, hi, t) over [0, n) split into contiguous parts, one per host thread
+// (at most 32, at least 4M items each); t is the part's index.
+template <typename F> void parallel_for(int64_t n, F f) {
+    const int64_t grain = (int64_t)1 << 22;
+    int nt = (int)std::min<int64_t>(std::min<unsigned>(32u, std::max(1u, std::thread::hardware_concurrency())),
+                                    (n + grain - 1) / grain);
+    if (nt <= 1) { f((int64_t)0, n, 0); return; }
+    std::vector<std::thread> th;
+    th.reserve(nt);
+    for (int t = 0; t < nt; ++t) th.emplace_back([&f, n, nt, t] { f(n * t / nt, n * (t + 1) / nt, t); });
+    for (auto &x : th) x.join();
+}
+static int parallel_parts(int64_t n) {
+    const int64_t grain = (int64_t)1 << 22;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(std::min<unsigned>(32u, std::max(1u, std::thread::hardware_concurrency())),
+                                                       (n + grain - 1) / grain));
+}
+
+// device helpers of the network set-up (grid-stride loops)
+__global__ void k_fill_u32(uint32_t *p, int64_t n, uint32_t v) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) p[i] = v;
+}
+__global__ void k_fill_u64(unsigned long long *p, int64_t n, unsigned long long v) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) p[i] = v;
+}
+// in-degree of every target (columns validated to lie in [0, tn))
+__global__ void k_indegree(const int32_t *cols, int64_t n, int32_t *deg) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        atomicAdd(deg + cols[i], 1);
+}
+// persistent push words: target | delay << 24
+__global__ void k_pack_synapses(const int32_t *cols, const uint8_t *d, int64_t n, uint32_t *out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (uint32_t)cols[i] | ((uint32_t)d[i] << 24);
+}
+
 struct HConn {
     int32_t src = 0, tgt = 0; int64_t so = 0, sn = 0, to = 0, tn = 0; int var = 0;
     bool dense = false; int64_t nnz = 0;
-    std::vector<int64_t> rowptr; std::vector<int32_t> cols; std::vector<char> w; int w_bits = 64;
-    int32_t delay = 0; bool hetero = false; std::vector<uint8_t> d; int md = 0; int mod_var = -1;
+    std::vector<int64_t> rowptr; hvec<int32_t> cols; hvec<char> w; int w_bits = 64;
+    bool wshared = false;      // w holds the one weight every synapse shares (the device array is filled)
+    int32_t delay = 0; bool hetero = false; hvec<uint8_t> d; int md = 0; int mod_var = -1;
     bool homogeneous = false; int parts = 1; int stdp = -1; bool fused_push = false;
     uint16_t *dCRing = nullptr; int64_t tnp = 0; void *dTable = nullptr; int tablen = 0;   // count ring (shared weight)
     int64_t *dRow = nullptr; int32_t *dCols = nullptr; void *dW = nullptr; uint8_t *dD = nullptr; void *dRing = nullptr;
@@ -86,6 +138,8 @@ struct bg_net {
     int allow_persist = 1;
     int persist_th = 0;                 // forced threads per block of the persistent kernel (0: automatic)
     int persist_used = 0;               // threads per block of the built persistent kernel (0: none)
+    uint32_t *dMonWords = nullptr;      // persistent path with spike monitors: spike words per step of a chunk
+    long long *dMonOff = nullptr;       //   and per-step record offsets
     cudaStream_t stream = nullptr;
     std::vector<HGroup> groups; std::vector<HConn> conns; std::vector<HStdp> stdps;
     std::vector<HSpikeMon> smons; std::vector<HStateMon> stmons; std::vector<Item> items;
@@ -400,20 +454,28 @@ int check_device_error(bg_net *net) {
 
 // Copy monitor records of the finished chunk to host memory.
 // `tail_done_upto`: last step whose 'end' slot has run.
+// Move one spike monitor's device records (steps relative to
+// chunk_base_cs) to host memory and empty its buffer.
+int drain_spikemon(bg_net *net, HSpikeMon &m, long long chunk_base_cs) {
+    long long cnt = 0;
+    BG_CUDA(cudaMemcpy(&cnt, m.dCnt, 8, cudaMemcpyDeviceToHost));
+    if (cnt > m.cap) return fail(BG_ESTATE, "spike monitor buffer overflow");
+    if (cnt > 0) {
+        std::vector<int32_t> idx(cnt), st(cnt);
+        BG_CUDA(cudaMemcpy(idx.data(), m.dIdx, cnt * 4, cudaMemcpyDeviceToHost));
+        BG_CUDA(cudaMemcpy(st.data(), m.dSteps, cnt * 4, cudaMemcpyDeviceToHost));
+        for (long long k = 0; k < cnt; ++k) { m.idx.push_back(idx[k]); m.steps.push_back(chunk_base_cs + st[k]); }
+        long long z = 0;
+        BG_CUDA(cudaMemcpy(m.dCnt, &z, 8, cudaMemcpyHostToDevice));
+    }
+    return BG_OK;
+}
+
 int drain(bg_net *net, long long chunk_base_cs, long long tail_done_upto, long long off) {
     BG_CUDA(cudaStreamSynchronize(net->stream));
     for (auto &m : net->smons) {
-        long long cnt = 0;
-        BG_CUDA(cudaMemcpy(&cnt, m.dCnt, 8, cudaMemcpyDeviceToHost));
-        if (cnt > m.cap) return fail(BG_ESTATE, "spike monitor buffer overflow");
-        if (cnt > 0) {
-            std::vector<int32_t> idx(cnt), st(cnt);
-            BG_CUDA(cudaMemcpy(idx.data(), m.dIdx, cnt * 4, cudaMemcpyDeviceToHost));
-            BG_CUDA(cudaMemcpy(st.data(), m.dSteps, cnt * 4, cudaMemcpyDeviceToHost));
-            for (long long k = 0; k < cnt; ++k) { m.idx.push_back(idx[k]); m.steps.push_back(chunk_base_cs + st[k]); }
-            long long z = 0;
-            BG_CUDA(cudaMemcpy(m.dCnt, &z, 8, cudaMemcpyHostToDevice));
-        }
+        int st = drain_spikemon(net, m, chunk_base_cs);
+        if (st) return st;
     }
     for (auto &m : net->stmons) {
         // records exist for ps in [start, tail_done_upto] with (ps-start) % timestep == 0
@@ -499,10 +561,18 @@ int persist_threads(int64_t n, int nvar, int forced) {
 // refractoriness, no Poisson/generator input) whose every connection is a
 // shared-weight DelayConnection from the group onto itself, with no monitors
 // and no plasticity -- the CUBA benchmark topology.
+// Steps per persistent launch when spike monitors record: the spike words of
+// a launch are converted to records after it (32 KB per step at 262144
+// neurons), in step ranges that fit each monitor's record buffer.
+constexpr int64_t kPersistMonSteps = bg::kMonWordsThreads;
+
 template <typename T>
 int build_persist(bg_net *net) {
     net->persist = nullptr;
-    if (net->groups.size() != 1 || !net->smons.empty() || !net->stmons.empty() || !net->stdps.empty()) return BG_OK;
+    if (net->groups.size() != 1 || !net->stmons.empty() || !net->stdps.empty()) return BG_OK;
+    for (const HSpikeMon &m : net->smons)
+        if (m.gid != 0 || m.delay != 0) return BG_OK;
+
     const HGroup &g = net->groups[0];
     if (!g.linear || g.nvar < 1 || g.nvar > 4 || g.refr || g.period > 0) return BG_OK;
     if (g.thr_kind != BG_THR_CONST && g.thr_kind != BG_THR_VAR && g.thr_kind != BG_THR_NONE) return BG_OK;
@@ -560,13 +630,12 @@ int build_persist(bg_net *net) {
         q.cring = c.dCRing; q.tnp = c.tnp;
         // one word per synapse for the scatter: a single load (and a single
         // stream of cache lines and pages) per synapse instead of two
-        if (c.dCRing && c.tn <= (1 << 24) && !c.cols.empty() && c.d.size() == c.cols.size()) {
+        if (c.dCRing && c.tn <= (1 << 24) && c.nnz > 0 && c.dCols && c.dD) {
             if (!c.dPacked) {
-                std::vector<uint32_t> pk(c.cols.size());
-                for (size_t k = 0; k < pk.size(); ++k) pk[k] = (uint32_t)c.cols[k] | ((uint32_t)c.d[k] << 24);
-                if (net->alloc(&c.dPacked, pk.size() * 4) != cudaSuccess) return fail(BG_ENOMEM, "packed synapses");
-                int st = upload(net, c.dPacked, pk.data(), pk.size() * 4);
-                if (st) return st;
+                if (net->alloc(&c.dPacked, c.nnz * 4) != cudaSuccess) return fail(BG_ENOMEM, "packed synapses");
+                const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((c.nnz + 255) / 256, (int64_t)sm_count() * 8));
+                k_pack_synapses<<<grid, 256, 0, net->stream>>>(c.dCols, c.dD, c.nnz, c.dPacked);
+                BG_CUDA(cudaGetLastError());
             }
             q.packed = c.dPacked;
         }
@@ -574,6 +643,17 @@ int build_persist(bg_net *net) {
     a.spikes = net->dCounters;
     a.arrived = net->dArrived;
     a.lag = min_d >= 1 ? 2 : 1;
+    if (!net->smons.empty()) {
+        // spike monitors: the kernel writes each step's spike words; the
+        // monitor kernels turn a launch's words into records (one launch per
+        // chunk of at most chunk_steps steps)
+        a.mon_stride = g.npad / 32;
+        if (!net->dMonWords &&
+            (net->alloc(&net->dMonWords, (size_t)kPersistMonSteps * a.mon_stride * 4) != cudaSuccess ||
+             net->alloc(&net->dMonOff, (size_t)kPersistMonSteps * 8) != cudaSuccess))
+            return fail(BG_ENOMEM, "spike words");
+        a.mon_words = net->dMonWords;
+    }
     const int nvar = g.nvar;
     unsigned int *arr = net->dArrived;
     // first row full, other rows diagonal, C at most in its first entry
@@ -743,27 +823,72 @@ int bg_conn_add(bg_net *n, int32_t src, int64_t so, int64_t sn, int32_t tgt, int
     if (w_bits != 32 && w_bits != 64) return fail(BG_EINVAL, "w_bits must be 32 or 64");
     if (!rowptr || nnz < 0 || (nnz > 0 && (!cols || !w)) || !cid) return fail(BG_EINVAL, "CSR arrays");
     if (rowptr[0] != 0 || rowptr[sn] != nnz) return fail(BG_EINVAL, "rowptr must start at 0 and end at nnz");
-    for (int64_t i = 0; i < sn; ++i) {
+    for (int64_t i = 0; i < sn; ++i)
         if (rowptr[i + 1] < rowptr[i]) return fail(BG_EINVAL, "rowptr not monotone");
-        for (int64_t k = rowptr[i]; k < rowptr[i + 1]; ++k) {
-            if (cols[k] < 0 || cols[k] >= tn) return fail(BG_EINVAL, "column index out of range");
-            if (k > rowptr[i] && cols[k] <= cols[k - 1]) return fail(BG_EINVAL, "columns not strictly ascending in a row");
-        }
+    {
+        // rows in parallel; the first bad row (lowest index) decides the message
+        const int parts = parallel_parts(sn);
+        std::vector<int64_t> bad_row(parts, sn);
+        std::vector<int> bad_kind(parts, 0);
+        parallel_for(sn, [&](int64_t lo, int64_t hi, int t) {
+            for (int64_t i = lo; i < hi; ++i)
+                for (int64_t k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+                    const int kind = (cols[k] < 0 || cols[k] >= tn) ? 1 : (k > rowptr[i] && cols[k] <= cols[k - 1]) ? 2 : 0;
+                    if (kind) { bad_row[t] = i; bad_kind[t] = kind; return; }
+                }
+        });
+        int64_t r = sn; int kind = 0;
+        for (int t = 0; t < parts; ++t) if (bad_row[t] < r) { r = bad_row[t]; kind = bad_kind[t]; }
+        if (kind == 1) return fail(BG_EINVAL, "column index out of range");
+        if (kind == 2) return fail(BG_EINVAL, "columns not strictly ascending in a row");
     }
-    c.nnz = nnz; c.rowptr.assign(rowptr, rowptr + sn + 1); c.cols.assign(cols, cols + nnz);
+    c.nnz = nnz; c.rowptr.assign(rowptr, rowptr + sn + 1);
+    c.cols.resize(nnz);
+    parallel_for(nnz, [&](int64_t lo, int64_t hi, int) { std::memcpy(c.cols.data() + lo, cols + lo, (hi - lo) * 4); });
     c.w_bits = w_bits;
-    c.w.assign((const char *)w, (const char *)w + nnz * (w_bits / 8));
-    c.homogeneous = true;
-    for (int64_t k = 1; k < nnz && c.homogeneous; ++k)
-        c.homogeneous = std::memcmp(&c.w[0], &c.w[k * (w_bits / 8)], w_bits / 8) == 0;
+    // one shared weight (bit pattern) is kept once and filled on the device
+    {
+        const int parts = parallel_parts(nnz);
+        std::vector<char> same(parts, 1);
+        parallel_for(nnz, [&](int64_t lo, int64_t hi, int t) {
+            if (w_bits == 32) {
+                const uint32_t *p = (const uint32_t *)w; const uint32_t v = p[0]; bool ok = true;
+                for (int64_t k = lo; k < hi; ++k) ok &= p[k] == v;
+                same[t] = ok;
+            } else {
+                const uint64_t *p = (const uint64_t *)w; const uint64_t v = p[0]; bool ok = true;
+                for (int64_t k = lo; k < hi; ++k) ok &= p[k] == v;
+                same[t] = ok;
+            }
+        });
+        c.homogeneous = true;
+        for (char x : same) c.homogeneous = c.homogeneous && x;
+    }
+    const int64_t wb = w_bits / 8;
+    if (c.homogeneous && nnz > 0) {
+        c.wshared = true;
+        c.w.assign((const char *)w, (const char *)w + wb);
+    } else {
+        c.w.resize(nnz * wb);
+        parallel_for(nnz, [&](int64_t lo, int64_t hi, int) { std::memcpy(c.w.data() + lo * wb, (const char *)w + lo * wb, (hi - lo) * wb); });
+    }
     if (delays) {
         if (ring_depth < 1 || ring_depth > 255) return fail(BG_EINVAL, "ring depth must be in [1, 255]");
-        for (int64_t k = 0; k < nnz; ++k) if (delays[k] >= ring_depth) return fail(BG_EINVAL, "delay >= ring depth");
+        const int parts = parallel_parts(nnz);
+        std::vector<int> dmax(parts, 0);
+        parallel_for(nnz, [&](int64_t lo, int64_t hi, int t) {
+            uint8_t m = 0;
+            for (int64_t k = lo; k < hi; ++k) m = std::max(m, delays[k]);
+            dmax[t] = m;
+        });
+        for (int m : dmax) if (m >= ring_depth) return fail(BG_EINVAL, "delay >= ring depth");
         // two spare rows beyond the reference's int(max_delay/dt)+1: the rows
         // written at step t never include the rows delivered at steps t-1 and
         // t-2, which lets the spike push ride on the source group's update
         // kernel and lets blocks of the persistent kernel drift by one step
-        c.hetero = true; c.md = ring_depth + 2; c.d.assign(delays, delays + nnz);
+        c.hetero = true; c.md = ring_depth + 2;
+        c.d.resize(nnz);
+        parallel_for(nnz, [&](int64_t lo, int64_t hi, int) { std::memcpy(c.d.data() + lo, delays + lo, hi - lo); });
     }
     n->conns.push_back(std::move(c));
     *cid = (int32_t)n->conns.size() - 1;
@@ -785,10 +910,24 @@ int bg_conn_add_dense(bg_net *n, int32_t src, int64_t so, int64_t sn, int32_t tg
     return BG_OK;
 }
 
+// A shared weight kept once on the host becomes a full host array (for
+// reading weights back or changing them).
+static void expand_shared_weight(HConn &c) {
+    if (!c.wshared) return;
+    const int64_t wb = c.w_bits / 8, cnt = c.wcount();
+    hvec<char> full(cnt * wb);
+    parallel_for(cnt, [&](int64_t lo, int64_t hi, int) {
+        for (int64_t k = lo; k < hi; ++k) std::memcpy(full.data() + k * wb, c.w.data(), wb);
+    });
+    c.w.swap(full);
+    c.wshared = false;
+}
+
 int bg_conn_get_weights(bg_net *n, int32_t cid, double *out) {
     if (!n || cid < 0 || cid >= (int32_t)n->conns.size() || !out) return fail(BG_EINVAL, "bg_conn_get_weights");
     HConn &c = n->conns[cid];
     const int64_t cnt = c.wcount();
+    expand_shared_weight(c);
     if (n->prepared) {
         BG_CUDA(cudaStreamSynchronize(n->stream));
         BG_CUDA(cudaMemcpy(c.w.data(), c.dW, c.w.size(), cudaMemcpyDeviceToHost));
@@ -802,6 +941,24 @@ int bg_conn_set_weights(bg_net *n, int32_t cid, const double *in) {
     if (!n || cid < 0 || cid >= (int32_t)n->conns.size() || !in) return fail(BG_EINVAL, "bg_conn_set_weights");
     HConn &c = n->conns[cid];
     const int64_t cnt = c.wcount();
+    if (n->prepared && c.dCRing && cnt > 0) {
+        // the count ring delivers k-fold sums of one weight: a new shared
+        // value rebuilds the sum table, unequal weights cannot be taken
+        const double w0 = c.w_bits == 64 ? in[0] : (double)(float)in[0];
+        for (int64_t k = 1; k < cnt; ++k)
+            if ((c.w_bits == 64 ? in[k] : (double)(float)in[k]) != w0 || std::signbit(in[k]) != std::signbit(in[0]))
+                return fail(BG_ENOSYS, "weights of a shared-weight delayed connection must stay equal after prepare");
+        if (n->precision == 64) {
+            std::vector<double> tab(c.tablen, 0.0);
+            for (int k = 1; k < c.tablen; ++k) tab[k] = tab[k - 1] + w0;
+            int st = upload(n, c.dTable, tab.data(), tab.size() * 8); if (st) return st;
+        } else {
+            std::vector<float> tab(c.tablen, 0.0f);
+            for (int k = 1; k < c.tablen; ++k) tab[k] = tab[k - 1] + (float)w0;
+            int st = upload(n, c.dTable, tab.data(), tab.size() * 4); if (st) return st;
+        }
+    }
+    expand_shared_weight(c);
     for (int64_t k = 0; k < cnt; ++k) {
         if (c.w_bits == 64) ((double *)c.w.data())[k] = in[k];
         else ((float *)c.w.data())[k] = (float)in[k];
@@ -958,8 +1115,17 @@ int bg_net_prepare(bg_net *n) {
     }
     for (size_t ci = 0; ci < n->conns.size(); ++ci) {
         HConn &c = n->conns[ci];
-        if (n->alloc(&c.dW, c.w.size()) != cudaSuccess) return fail(BG_ENOMEM, "weights");
-        int st = upload(n, c.dW, c.w.data(), c.w.size()); if (st) return st;
+        const int64_t wbytes = c.wcount() * (c.w_bits / 8);
+        if (n->alloc(&c.dW, wbytes) != cudaSuccess) return fail(BG_ENOMEM, "weights");
+        int st = BG_OK;
+        if (c.wshared) {
+            const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((c.wcount() + 255) / 256, (int64_t)sm_count() * 8));
+            if (c.w_bits == 32) k_fill_u32<<<grid, 256, 0, n->stream>>>((uint32_t *)c.dW, c.wcount(), *(const uint32_t *)c.w.data());
+            else k_fill_u64<<<grid, 256, 0, n->stream>>>((unsigned long long *)c.dW, c.wcount(), *(const unsigned long long *)c.w.data());
+            BG_CUDA(cudaGetLastError());
+        } else {
+            st = upload(n, c.dW, c.w.data(), wbytes); if (st) return st;
+        }
         if (!c.dense) {
             if (n->alloc(&c.dRow, (c.sn + 1) * 8) != cudaSuccess || n->alloc(&c.dCols, c.nnz * 4) != cudaSuccess)
                 return fail(BG_ENOMEM, "CSR");
@@ -976,8 +1142,18 @@ int bg_net_prepare(bg_net *n) {
             // stay below the largest in-degree.
             int64_t kmax = 0;
             if (c.fused_push && c.homogeneous && c.nnz > 0) {
-                std::vector<int32_t> indeg(c.tn, 0);
-                for (int32_t j : c.cols) kmax = std::max<int64_t>(kmax, ++indeg[j]);
+                // largest in-degree, counted on the device from the uploaded columns
+                int32_t *dDeg = nullptr;
+                BG_CUDA(cudaMalloc(&dDeg, c.tn * 4));
+                std::vector<int32_t> indeg(c.tn);
+                cudaError_t e = cudaMemsetAsync(dDeg, 0, c.tn * 4, n->stream);
+                const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((c.nnz + 255) / 256, (int64_t)sm_count() * 8));
+                if (e == cudaSuccess) { k_indegree<<<grid, 256, 0, n->stream>>>(c.dCols, c.nnz, dDeg); e = cudaGetLastError(); }
+                if (e == cudaSuccess) e = cudaMemcpyAsync(indeg.data(), dDeg, c.tn * 4, cudaMemcpyDeviceToHost, n->stream);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(n->stream);
+                cudaFree(dDeg);
+                if (e != cudaSuccess) return fail(BG_ECUDA, std::string("in-degree: ") + cudaGetErrorString(e));
+                for (int32_t k : indeg) kmax = std::max<int64_t>(kmax, k);
             }
             if (kmax > 0 && kmax < 65535) {
                 c.tablen = (int)kmax + 1;
@@ -1134,11 +1310,47 @@ int bg_net_run(bg_net *n, int64_t nsteps, int64_t cs0) {
         long long off0 = cs0 - n->nstep;
         BG_CUDA(cudaMemcpyAsync(&n->dCtl->clock_off, &off0, 8, cudaMemcpyHostToDevice, n->stream));
         BG_CUDA(cudaEventRecord(n->ev0, n->stream));
-        const int64_t chunk = 1 << 20;
+        const bool mons = !n->smons.empty();
+        const int64_t chunk = mons ? kPersistMonSteps : (int64_t)1 << 20;
+        std::vector<long long> cnt;
         for (int64_t done = 0; done < nsteps;) {
             const int64_t c = std::min(chunk, nsteps - done);
             int st = run_persist(n, c);
             if (st) return st;
+            if (mons) {
+                const HGroup &g = n->groups[0];
+                for (auto &m : n->smons) {
+                    bg::MonWordsArgs w;
+                    w.ctl = n->dCtl; w.words = n->dMonWords; w.stride = g.npad / 32; w.nsteps = (int)c; w.s0 = 0;
+                    w.origin = m.origin; w.n = m.n; w.cnt = m.dCnt; w.cap = m.cap; w.idx = m.dIdx; w.steps = m.dSteps;
+                    w.off = n->dMonOff;
+                    bg::k_monw_count<<<(unsigned)c, bg::kMonWordsThreads, 0, n->stream>>>(w);
+                    BG_CUDA(cudaGetLastError());
+                    n->launches += 1;
+                    cnt.resize(c);
+                    BG_CUDA(cudaMemcpyAsync(cnt.data(), n->dMonOff, c * 8, cudaMemcpyDeviceToHost, n->stream));
+                    BG_CUDA(cudaStreamSynchronize(n->stream));
+                    // step ranges whose records fit the (empty) buffer; a step
+                    // alone always fits (at most m.n records, cap >= m.n)
+                    for (int64_t s0 = 0; s0 < c;) {
+                        int64_t s1 = s0, tot = 0;
+                        while (s1 < c && tot + cnt[s1] <= m.cap) tot += cnt[s1++];
+                        bg::MonWordsArgs r = w;
+                        r.words = n->dMonWords + s0 * w.stride; r.off = n->dMonOff + s0;
+                        r.nsteps = (int)(s1 - s0); r.s0 = (int)s0;
+                        bg::k_monw_scan<<<1, bg::kMonWordsThreads, 0, n->stream>>>(r);
+                        bg::k_monw_write<<<(unsigned)(s1 - s0), bg::kMonWordsThreads, 0, n->stream>>>(r);
+                        BG_CUDA(cudaGetLastError());
+                        n->launches += 2;
+                        BG_CUDA(cudaStreamSynchronize(n->stream));
+                        st = check_device_error(n);
+                        if (st) return st;
+                        st = drain_spikemon(n, m, cs0 + done);
+                        if (st) return st;
+                        s0 = s1;
+                    }
+                }
+            }
             done += c;
         }
         BG_CUDA(cudaEventRecord(n->ev1, n->stream));

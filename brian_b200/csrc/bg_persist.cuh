@@ -39,6 +39,8 @@ template <typename T> struct PersistArgs {
     unsigned int *arrived;      // [4] arrivals per step mod 4 (zeroed before the launch)
     int nsteps;
     int lag;                    // 1 when some delay is zero, else 2
+    uint32_t *mon_words;        // spike monitors: spike words of each step of the launch, else null
+    int64_t mon_stride;         // words per step in mon_words
 };
 
 __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int *p) {
@@ -333,6 +335,7 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
             if (lane == 0) {
                 words[u * (TH / 32) + warp] = ball;
                 my_spikes += __popc(ball);
+                if (a.mon_words) a.mon_words[(int64_t)st * a.mon_stride + (base >> 5) + u * (TH / 32) + warp] = ball;
             }
         }
         // the barrier also tells every thread whether the block spiked
@@ -426,6 +429,90 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
     if (tid == 0)
         for (int p = 0; p < a.npush; ++p)
             if (my_events[p] && a.push[p].events) atomicAdd(a.push[p].events, my_events[p]);
+}
+
+// ---- spike monitors of the persistent path ---------------------------------
+// After a launch of nsteps steps, the words it wrote become the monitor's
+// (step, index) records in the order of k_spikemon (steps ascending, indices
+// ascending within a step): per-step counts, one scan over the steps, then
+// one block per step writes its records at its offset.
+struct MonWordsArgs {
+    DevCtl *ctl;
+    const uint32_t *words; int64_t stride; int nsteps;
+    int s0;                               // launch-relative step of words[0] (records carry s0 + s)
+    int64_t origin, n;                    // monitored range of the group
+    long long *cnt; int64_t cap; int32_t *idx; int32_t *steps;
+    long long *off;                       // [nsteps] per-step record offsets (scratch)
+};
+constexpr int kMonWordsThreads = 1024;
+
+__global__ void __launch_bounds__(kMonWordsThreads) k_monw_count(const MonWordsArgs a) {
+    __shared__ int wsum[kMonWordsThreads / 32];
+    const int s = blockIdx.x, tid = threadIdx.x;
+    const uint32_t *H = a.words + (int64_t)s * a.stride;
+    const int64_t end = a.origin + a.n, w0 = a.origin >> 5, w1 = (end + 31) >> 5;
+    int c = 0;
+    for (int64_t wi = w0 + tid; wi < w1; wi += kMonWordsThreads) c += __popc(masked_word(H, wi, a.origin, end));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((tid & 31) == 0) wsum[tid >> 5] = c;
+    __syncthreads();
+    if (tid < 32) {
+        int v = wsum[tid];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (tid == 0) a.off[s] = v;
+    }
+}
+
+// one block: exclusive scan of the per-step counts from the buffer's fill
+// level; advances the fill level (nsteps <= kMonWordsThreads)
+__global__ void __launch_bounds__(kMonWordsThreads) k_monw_scan(const MonWordsArgs a) {
+    __shared__ long long wsum[kMonWordsThreads / 32 + 1];
+    const int tid = threadIdx.x, lane = tid & 31;
+    const long long v = tid < a.nsteps ? a.off[tid] : 0;
+    long long incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) { const long long x = __shfl_up_sync(0xffffffffu, incl, o); if (lane >= o) incl += x; }
+    if (lane == 31) wsum[tid >> 5] = incl;
+    __syncthreads();
+    if (tid == 0) {
+        long long r = *a.cnt;
+        for (int q = 0; q < kMonWordsThreads / 32; ++q) { const long long x = wsum[q]; wsum[q] = r; r += x; }
+        wsum[kMonWordsThreads / 32] = r;
+    }
+    __syncthreads();
+    if (tid < a.nsteps) a.off[tid] = wsum[tid >> 5] + incl - v;
+    if (tid == 0) *a.cnt = wsum[kMonWordsThreads / 32];
+}
+
+__global__ void __launch_bounds__(kMonWordsThreads) k_monw_write(const MonWordsArgs a) {
+    __shared__ int wcnt[kMonWordsThreads / 32 + 1];
+    const int s = blockIdx.x, tid = threadIdx.x;
+    const uint32_t *H = a.words + (int64_t)s * a.stride;
+    const int64_t end = a.origin + a.n, w0 = a.origin >> 5, w1 = (end + 31) >> 5;
+    long long base = a.off[s];
+    for (int64_t cw = w0; cw < w1; cw += kMonWordsThreads) {
+        const int64_t wi = cw + tid;
+        uint32_t word = wi < w1 ? masked_word(H, wi, a.origin, end) : 0u;
+        const int pc = __popc(word);
+        int incl = pc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) { const int v = __shfl_up_sync(0xffffffffu, incl, o); if ((tid & 31) >= o) incl += v; }
+        if ((tid & 31) == 31) wcnt[tid >> 5] = incl;
+        __syncthreads();
+        if (tid == 0) { int r = 0; for (int q = 0; q < kMonWordsThreads / 32; ++q) { const int v = wcnt[q]; wcnt[q] = r; r += v; } wcnt[kMonWordsThreads / 32] = r; }
+        __syncthreads();
+        long long o = base + wcnt[tid >> 5] + incl - pc;
+        while (word) {
+            const int b = __ffs(word) - 1; word &= word - 1;
+            if (o < a.cap) { a.idx[o] = (int32_t)(((wi << 5) + b) - a.origin); a.steps[o] = a.s0 + s; }
+            else bg_raise(a.ctl, BG_DERR_MONITOR_OVERFLOW, o);
+            ++o;
+        }
+        base += wcnt[kMonWordsThreads / 32];
+        __syncthreads();
+    }
 }
 
 }  // namespace bg

@@ -91,17 +91,21 @@ def cuba_delay(N=3000, indegree=100, steps=2000, seed=3, wdtype=np.float32, we=0
         # every neuron a hair below threshold: the whole group fires within
         # the first steps, far more spikes per block and step than one batch
         P.v = Vt - 1e-7 * rng.random(N)
-    if not monitors:
-        # no monitors: the engine may take its persistent single-launch path
+    if not monitors or monitors == "spikes":
+        # no monitors (or spike monitors only): the engine may take its
+        # persistent single-launch path
         prev = b.get_global_preference("persistent")
         b.set_global_preferences(persistent=persistent)
+        # monitors="spikes": spike monitors only (the whole group and the
+        # inhibitory subgroup), which the persistent kernel records itself
+        mons = [b.SpikeMonitor(P), b.SpikeMonitor(Pi)] if monitors == "spikes" else []
         try:
-            net = b.Network(P, conns[0], conns[1])
+            net = b.Network(P, conns[0], conns[1], *mons)
             for _ in range(runs):
                 net.run(steps * 0.1 * ms / runs)
         finally:
             b.set_global_preferences(persistent=prev)
-        out = _result(net, groups=[P])
+        out = _result(net, groups=[P], spikemons=mons)
         g, c = net._binding.rt.counters(1, 2)
         out["spikes"], out["events"] = g.copy(), c.copy()
         st = net.stats()

@@ -64,6 +64,24 @@ def test_persistent_path_bit_exact(oracle_table, gpu_table, dmin, runs):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("burst", [False, True])
+def test_persistent_spike_monitors_bit_exact(oracle_table, gpu_table, burst):
+    """Spike monitors (the whole group, and the inhibitory subgroup whose
+    range starts and ends inside a 32-neuron word at N=6010) on
+    the persistent path: the kernel's per-step spike words become the same
+    (step, index) records as the reference's SpikeMonitor, across launches
+    of at most 1024 steps and across runs."""
+    ref, gpu = _both(scenarios.cuba_delay, oracle_table, monitors="spikes", N=6010, steps=3000, runs=2,
+                     burst=burst)
+    assert len(ref["spk0.idx"]) > 1000 and len(ref["spk1.idx"]) > 100
+    ref.pop("launches"), ref.pop("persistent_threads")
+    launches, th = gpu.pop("launches"), gpu.pop("persistent_threads")
+    scenarios.compare(ref, gpu)
+    # per run: two launches of <= 1024 steps, each followed by 3 monitor kernels per monitor
+    assert th == 512 and launches == 2 * 2 * (1 + 3 * 2)
+
+
+@pytest.mark.gpu
 def test_persistent_burst_bit_exact(oracle_table, gpu_table):
     """Synchronous firing: blocks push hundreds of spikes in one step, in
     several batches of the persistent kernel's push."""
