@@ -59,6 +59,8 @@ ENGINE_ONLY = {
     "net_item_name": [_vp, _i64, ct.c_char_p, _i64],
     "fixed_indegree_csr": [_i64, _i64, _i64, _u64, _vp, _vp],
     "net_set_persistent": [_vp, ct.c_int],
+    "conn_add_shared": [_vp, _i32, _i64, _i64, _i32, _i64, _i64, ct.c_int, _i64, _vp, _vp, _dbl, ct.c_int, _i32,
+                        _vp, _i32, ct.c_int, _P(_i32)],
     "net_persistent_threads": [_vp, _P(_i32)],
     "fit_compile_check": [ct.c_int, _vp, _dbl, ct.c_int, ct.c_int, ct.c_char_p, _i64],
     "fit_create": [_P(_vp), ct.c_int, ct.c_int, _vp, _dbl, ct.c_int, ct.c_int],
@@ -214,6 +216,24 @@ class Runtime(object):
         self._c(self.t.conn_add(self.h, src, so, sn, tgt, to, tn, var, len(cols), _ptr(rowptr), _ptr(cols),
                                 _ptr(w), wbits, int(delay_steps), _ptr(d), int(ring_depth), int(mod_var),
                                 ct.byref(cid)), "conn_add")
+        return cid.value
+
+    def conn_add_shared(self, src, so, sn, tgt, to, tn, var, rowptr, cols, weight, dtype, delay_steps=0,
+                        delays=None, ring_depth=0, mod_var=-1):
+        """conn_add for synapses that all carry `weight` (stored as `dtype`):
+        no weight array crosses the boundary.  Tables without the entry
+        point get the full array."""
+        if not hasattr(self.t, "conn_add_shared"):
+            return self.conn_add(src, so, sn, tgt, to, tn, var, rowptr, cols,
+                                 np.full(len(cols), weight, dtype=dtype), delay_steps, delays, ring_depth, mod_var)
+        rowptr = np.ascontiguousarray(rowptr, dtype=np.int64)
+        cols = np.ascontiguousarray(cols, dtype=np.int32)
+        wbits = 32 if np.dtype(dtype) == np.float32 else 64
+        d = None if delays is None else np.ascontiguousarray(delays, dtype=np.uint8)
+        cid = _i32()
+        self._c(self.t.conn_add_shared(self.h, src, so, sn, tgt, to, tn, var, len(cols), _ptr(rowptr), _ptr(cols),
+                                       float(weight), wbits, int(delay_steps), _ptr(d), int(ring_depth),
+                                       int(mod_var), ct.byref(cid)), "conn_add_shared")
         return cid.value
 
     def conn_add_dense(self, src, so, sn, tgt, to, tn, var, W, delay_steps=0, mod_var=-1):

@@ -192,6 +192,7 @@ class Connection(object):
         self._denseW = np.zeros((len(source), len(target))) if structure == "dense" else None
         self.iscompressed = False
         self._rowptr = self._cols = self._w = self._dense = None
+        self._wshared = None       # the one weight of every synapse (then _w stays None until needed)
         self._binding = None
         if not isinstance(self, DelayConnection):
             self.delay = int(float(delay) / source.clock.dt)   # homogeneous delay in bins
@@ -327,8 +328,13 @@ class Connection(object):
         if len(rowptr) != len(self.source) + 1 or rowptr[-1] != len(cols):
             raise ValueError("rowptr does not match the source size / number of synapses")
         w = np.asarray(weights)
-        w = np.broadcast_to(w, cols.shape).astype(self.dtype) if w.ndim == 0 else w.astype(self.dtype, copy=False)
-        self._rowptr, self._cols, self._w = rowptr, cols, np.ascontiguousarray(w)
+        if w.ndim == 0:
+            # a scalar weight stays one value (no per-synapse array)
+            self._rowptr, self._cols, self._w = rowptr, cols, None
+            self._wshared = w.astype(self.dtype)[()]
+        else:
+            self._rowptr, self._cols, self._w = rowptr, cols, np.ascontiguousarray(w.astype(self.dtype, copy=False))
+            self._wshared = None
         self._build = None
         self.iscompressed = True
         if isinstance(self, DelayConnection):
@@ -400,14 +406,19 @@ class Connection(object):
         pass
 
     def _nnz(self):
-        return len(self._w)
+        return len(self._cols) if self._w is None else len(self._w)
 
     def _weights(self):
         if self._binding is not None:
             self._w = self._binding.read_weights(self).astype(self.dtype)
+            self._wshared = None
+        elif self._w is None and self._wshared is not None:
+            self._w = np.full(len(self._cols), self._wshared, dtype=self.dtype)
+            self._wshared = None
         return self._w
 
     def _set_weights(self, w):
+        self._wshared = None
         self._w = np.asarray(w).astype(self.dtype)
         if self._binding is not None:
             self._binding.write_weights(self, self._w)
@@ -421,8 +432,12 @@ class Connection(object):
     def _lower(self, rt, gids):
         self.compress()
         src, tgt = self.source._owner, self.target._owner
-        w = self._weights()
         mod = -1 if self._nstate_mod is None else self._nstate_mod
+        if self._dense is None and self._wshared is not None:
+            return rt.conn_add_shared(gids[src], self.source._origin, len(self.source), gids[tgt],
+                                      self.target._origin, len(self.target), self.nstate, self._rowptr, self._cols,
+                                      self._wshared, self.dtype, delay_steps=self.delay, mod_var=mod)
+        w = self._weights()
         if self._dense is not None:
             return rt.conn_add_dense(gids[src], self.source._origin, len(self.source), gids[tgt],
                                      self.target._origin, len(self.target), self.nstate,
@@ -533,6 +548,11 @@ class DelayConnection(Connection):
         self.compress()
         src, tgt = self.source._owner, self.target._owner
         mod = -1 if self._nstate_mod is None else self._nstate_mod
+        if self._wshared is not None:
+            return rt.conn_add_shared(gids[src], self.source._origin, len(self.source), gids[tgt],
+                                      self.target._origin, len(self.target), self.nstate, self._rowptr, self._cols,
+                                      self._wshared, self.dtype, delay_steps=0, delays=self._delay_steps(),
+                                      ring_depth=self._md, mod_var=mod)
         return rt.conn_add(gids[src], self.source._origin, len(self.source), gids[tgt], self.target._origin,
                            len(self.target), self.nstate, self._rowptr, self._cols, self._weights(),
                            delay_steps=0, delays=self._delay_steps(), ring_depth=self._md, mod_var=mod)

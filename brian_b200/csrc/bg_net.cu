@@ -814,9 +814,11 @@ static int conn_common(bg_net *n, int32_t src, int64_t so, int64_t sn, int32_t t
     return BG_OK;
 }
 
-int bg_conn_add(bg_net *n, int32_t src, int64_t so, int64_t sn, int32_t tgt, int64_t to, int64_t tn, int var,
-                int64_t nnz, const int64_t *rowptr, const int32_t *cols, const void *w, int w_bits, int32_t delay,
-                const uint8_t *delays, int32_t ring_depth, int mod_var, int32_t *cid) {
+// shared_w: w points to the one weight of every synapse
+static int conn_add_impl(bg_net *n, int32_t src, int64_t so, int64_t sn, int32_t tgt, int64_t to, int64_t tn, int var,
+                         int64_t nnz, const int64_t *rowptr, const int32_t *cols, const void *w, bool shared_w,
+                         int w_bits, int32_t delay, const uint8_t *delays, int32_t ring_depth, int mod_var,
+                         int32_t *cid) {
     HConn c;
     int st = conn_common(n, src, so, sn, tgt, to, tn, var, delay, mod_var, c);
     if (st) return st;
@@ -847,7 +849,9 @@ int bg_conn_add(bg_net *n, int32_t src, int64_t so, int64_t sn, int32_t tgt, int
     parallel_for(nnz, [&](int64_t lo, int64_t hi, int) { std::memcpy(c.cols.data() + lo, cols + lo, (hi - lo) * 4); });
     c.w_bits = w_bits;
     // one shared weight (bit pattern) is kept once and filled on the device
-    {
+    if (shared_w) {
+        c.homogeneous = true;
+    } else {
         const int parts = parallel_parts(nnz);
         std::vector<char> same(parts, 1);
         parallel_for(nnz, [&](int64_t lo, int64_t hi, int t) {
@@ -894,6 +898,22 @@ int bg_conn_add(bg_net *n, int32_t src, int64_t so, int64_t sn, int32_t tgt, int
     *cid = (int32_t)n->conns.size() - 1;
     n->items.push_back({IT_CONN, *cid});
     return BG_OK;
+}
+
+int bg_conn_add(bg_net *n, int32_t src, int64_t so, int64_t sn, int32_t tgt, int64_t to, int64_t tn, int var,
+                int64_t nnz, const int64_t *rowptr, const int32_t *cols, const void *w, int w_bits, int32_t delay,
+                const uint8_t *delays, int32_t ring_depth, int mod_var, int32_t *cid) {
+    return conn_add_impl(n, src, so, sn, tgt, to, tn, var, nnz, rowptr, cols, w, false, w_bits, delay, delays,
+                         ring_depth, mod_var, cid);
+}
+
+int bg_conn_add_shared(bg_net *n, int32_t src, int64_t so, int64_t sn, int32_t tgt, int64_t to, int64_t tn, int var,
+                       int64_t nnz, const int64_t *rowptr, const int32_t *cols, double weight, int w_bits,
+                       int32_t delay, const uint8_t *delays, int32_t ring_depth, int mod_var, int32_t *cid) {
+    const float wf = (float)weight;
+    const void *w = w_bits == 32 ? (const void *)&wf : (const void *)&weight;
+    return conn_add_impl(n, src, so, sn, tgt, to, tn, var, nnz, rowptr, cols, w, true, w_bits, delay, delays,
+                         ring_depth, mod_var, cid);
 }
 
 int bg_conn_add_dense(bg_net *n, int32_t src, int64_t so, int64_t sn, int32_t tgt, int64_t to, int64_t tn, int var,

@@ -135,6 +135,15 @@ BG_API int bg_conn_add(bg_net *net, int32_t src_gid, int64_t src_origin,
                 const int64_t *rowptr, const int32_t *cols, const void *w,
                 int w_bits, int32_t delay_steps, const uint8_t *delays,
                 int32_t ring_depth, int mod_var, int32_t *cid);
+/* bg_conn_add for a connection whose synapses all carry one weight (the
+ * scalar `weight` argument of Connection.connect*, connection.py:354-475,
+ * stored as w_bits 32 or 64): no per-synapse weight array is passed. */
+BG_API int bg_conn_add_shared(bg_net *net, int32_t src_gid, int64_t src_origin,
+                int64_t src_n, int32_t tgt_gid, int64_t tgt_origin,
+                int64_t tgt_n, int tgt_var, int64_t nnz,
+                const int64_t *rowptr, const int32_t *cols, double weight,
+                int w_bits, int32_t delay_steps, const uint8_t *delays,
+                int32_t ring_depth, int mod_var, int32_t *cid);
 /* DenseConnectionMatrix (connectionmatrix.py:141-193): W[src_n][tgt_n]. */
 BG_API int bg_conn_add_dense(bg_net *net, int32_t src_gid, int64_t src_origin,
                       int64_t src_n, int32_t tgt_gid, int64_t tgt_origin,
