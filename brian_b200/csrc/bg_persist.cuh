@@ -335,11 +335,12 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
             if (lane == 0) {
                 words[u * (TH / 32) + warp] = ball;
                 my_spikes += __popc(ball);
-                if (a.mon_words) a.mon_words[(int64_t)st * a.mon_stride + (base >> 5) + u * (TH / 32) + warp] = ball;
             }
         }
         // the barrier also tells every thread whether the block spiked
         const int any_spike = __syncthreads_or(prev_spk != 0);
+        // spike monitors: the block's words of this step, one coalesced row
+        if (a.mon_words && tid < BN / 32) a.mon_words[(int64_t)st * a.mon_stride + (base >> 5) + tid] = words[tid];
         // ---- push this block's spikes: one flattened scatter over every
         // (connection, spike) pair of the block
         if (a.npush && any_spike) {
