@@ -200,12 +200,21 @@ def print_table(results, precision=4, colwidth=16):
 class FittingProblem(object):
     """Device state of one fit: every candidate of every target group, with
     its input row, target train and gamma normalisation
-    (ModelFitting.initialize/prepare_data, modelfitting.py:27-173, for
-    slices = 1)."""
+    (ModelFitting.initialize/prepare_data, modelfitting.py:27-173).
+
+    Time slicing (modelfitting.py:49-58, 126-163, 221-223): each input is cut
+    to a multiple of `slices` steps; slice k of a candidate simulates its
+    k-th piece preceded by `overlap` of the previous piece (zeros before the
+    first), against the target spikes of that piece shifted into the
+    slice's clock, and coincidences and spike counts are summed over the
+    slices before gamma.  Simulations are slice-major (i = k * N + n, the
+    reference's I_offset layout), every simulation runs the slice plus the
+    overlap, and each gets its own candidate's parameters."""
 
     def __init__(self, model, threshold, reset, data, inputs, dt, popsize, delta=4e-3, refractory=0.0,
                  initial_values=None, precision="double", method="Euler", param_names=(), onset=0.0,
-                 coincidence_count_algorithm="exclusive", input_var="I", device=0, record=0):
+                 coincidence_count_algorithm="exclusive", input_var="I", device=0, record=0, slices=1,
+                 overlap=0.0):
         if isinstance(model, str):
             model = Equations(model, level=2)
         self.eqs = model
@@ -222,27 +231,64 @@ class FittingProblem(object):
         self.N = N = groups * popsize
         # inputs: one row per target group; each group's duration is its
         # input's (modelfitting.py:398, 44-49)
-        lens = [len(x) for x in inputs]
-        self.nsteps_group = np.array([int((n * dt) / dt) for n in lens], dtype=np.int32)
-        I = np.concatenate([np.asarray(x, dtype=np.float64) for x in inputs])
-        ioff = np.concatenate([[0], np.cumsum(lens)[:-1]]).astype(np.int64)
+        self.slices = slices = int(slices)
+        if slices < 1:
+            raise ValueError("slices must be at least 1")
+        if slices == 1:
+            overlap = 0.0                        # no overlap without slicing (modelfitting.py:427-429)
+        ov = int(float(overlap) / dt)
+        self.overlap_steps = ov
+        # per group: input cut to a multiple of `slices`, zeros of the overlap
+        # in front, steps per slice (modelfitting.py:50-58)
+        pieces, sliced, lens = [], [], []
+        for x in inputs:
+            x = np.asarray(x, dtype=np.float64)
+            L = slices * (len(x) // slices)
+            pieces.append(np.hstack((np.zeros(ov), x[:L])))
+            sliced.append(L // slices)
+            lens.append(L)
+        # steps simulated: int(duration / dt) without slicing (the float round
+        # trip of GPUModelFitting.launch, gpu_modelfitting.py:388), else the
+        # slice plus the overlap (total_steps, modelfitting.py:54)
+        self.nsteps_group = np.array([int((L * dt) / dt) if slices == 1 else s + ov for L, s in zip(lens, sliced)],
+                                     dtype=np.int32)
+        I = np.concatenate(pieces)
+        ioff = np.concatenate([[0], np.cumsum([len(p) for p in pieces])[:-1]]).astype(np.int64)
         self.input_offsets = ioff
-        # target trains with sentinels at -1 s and duration + 1 s
-        # (modelfitting.py:139-163), lengths and rates (modelfitting.py:144-145)
-        trains, tlen, trate = [], [], []
+        # target trains with sentinels at -1 s and the slice's duration + 1 s
+        # (modelfitting.py:139-163), lengths and rates of the whole train
+        # (modelfitting.py:144-145); trains[k][j] is slice k of target j
+        trains = [[None] * groups for _ in range(slices)]
+        tlen, trate = [], []
         for j in range(groups):
             s = np.sort(np.asarray(data[j], dtype=np.float64))
             tlen.append(len(s))
             trate.append(firing_rate(s))
-            trains.append(np.hstack(([-1.0], s, [lens[j] * dt + 1.0])))
+            duration = lens[j] * dt
+            sliced_duration = float(overlap) + duration / slices
+            for k in range(slices):
+                inside = (s >= k * sliced[j] * dt) & (s < (k + 1) * sliced[j] * dt)
+                local = s[inside] - k * sliced[j] * dt + ov * dt
+                trains[k][j] = np.hstack(([-1.0], local, [sliced_duration + 1.0]))
         self.target_length = np.repeat(np.array(tlen, dtype=np.int32), popsize)
         self.target_rate = np.repeat(np.array(trate, dtype=np.float64), popsize)
-        toff = np.concatenate([[0], np.cumsum([len(t) for t in trains])[:-1]]).astype(np.int64)
-        tend = toff + np.array([len(t) for t in trains], dtype=np.int64)
-        spk = np.asarray(np.rint(np.concatenate(trains) / dt), dtype=np.int32)
+        flat = [trains[k][j] for k in range(slices) for j in range(groups)]
+        toff_kj = np.concatenate([[0], np.cumsum([len(t) for t in flat])[:-1]]).astype(np.int64).reshape(slices, groups)
+        tend_kj = toff_kj + np.array([len(t) for t in flat], dtype=np.int64).reshape(slices, groups)
+        spk = np.asarray(np.rint(np.concatenate(flat) / dt), dtype=np.int32)
         gidx = np.repeat(np.arange(groups), popsize)
+        kidx = np.repeat(np.arange(slices), N)
+        gall = np.tile(gidx, slices)
+        sim_ioff = ioff[gall] + kidx * np.array(sliced, dtype=np.int64)[gall]
+        sim_toff, sim_tend = toff_kj[kidx, gall], tend_kj[kidx, gall]
+        NS = N * slices
+        # the simulations as the device holds them (input offsets and steps,
+        # target trains in steps and their [offset, end) per simulation)
+        self.sim_input = I
+        self.sim_input_offsets, self.sim_nsteps = sim_ioff, self.nsteps_group[gall]
+        self.sim_trains, self.sim_train_offsets, self.sim_train_ends = spk, sim_toff, sim_tend
         # initial state: zeros (NeuronGroup.reinit), then initial_values
-        S0 = np.zeros((len(self.code.state), N))
+        S0 = np.zeros((len(self.code.state), NS))
         initial_values = initial_values or {}
         for k, v in initial_values.items():
             if k in param_names:
@@ -250,7 +296,7 @@ class FittingProblem(object):
             if k not in self.code.state:
                 raise ValueError("initial value for unknown variable %r" % k)
             S0[self.code.index(k)] = v
-        refr = np.full(N, int(np.rint(float(refractory) / dt)), dtype=np.int32)
+        refr = np.full(NS, int(np.rint(float(refractory) / dt)), dtype=np.int32)
         self.handle = h = _lib.FitHandle(self.code, dt, int(np.rint(self.delta / dt)),
                                          exclusive=coincidence_count_algorithm == "exclusive",
                                          precision=self.precision, device=device)
@@ -258,9 +304,9 @@ class FittingProblem(object):
         h.set_targets(spk)
         if record:
             h.set_record(record)
-        h.set_sims(S0, ioff[gidx], self.nsteps_group[gidx], toff[gidx], tend[gidx], None, refr,
+        h.set_sims(S0, sim_ioff, self.nsteps_group[gall], sim_toff, sim_tend, None, refr,
                    int(np.rint(float(onset) / dt)))
-        h.set_gamma(N, 1, self.target_length, self.target_rate, self.delta)
+        h.set_gamma(N, slices, self.target_length, self.target_rate, self.delta)
         dim_var = []
         for p in param_names:
             if p == "delays":
@@ -279,7 +325,7 @@ class FittingProblem(object):
         return self.handle.evaluate(X)
 
     def neuron_steps(self):
-        return int(np.sum(self.nsteps_group.astype(np.int64)) * self.popsize)
+        return int(np.sum(self.nsteps_group.astype(np.int64)) * self.popsize * self.slices)
 
 
 def _split_data(data):
@@ -334,8 +380,6 @@ def modelfitting(model=None, reset=None, threshold=None, refractory=0.0, data=No
     if algorithm is not PSO:
         raise NotImplementedError("only the particle swarm optimiser (algorithm=PSO) is built; CMA-ES and GA "
                                   "come from the external playdoh package")
-    if slices != 1:
-        raise NotImplementedError("time slicing is not built: uneven durations run whole in one launch")
     if isinstance(model, str):
         model = Equations(model, level=1)
     trains = _split_data(data)
@@ -356,7 +400,7 @@ def modelfitting(model=None, reset=None, threshold=None, refractory=0.0, data=No
     names, lo, hi, imin, imax = _bounds(params)
     prob = FittingProblem(model, threshold, reset, trains, inputs, dt, popsize, delta=delta, refractory=refractory,
                           initial_values=initial_values, precision=precision, method=method, param_names=names,
-                          input_var=input_var, device=device)
+                          input_var=input_var, device=device, slices=slices, overlap=overlap)
     M = prob.N
     rng = np.random.default_rng(seed)
     if initial_positions is None:

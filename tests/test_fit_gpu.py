@@ -183,9 +183,11 @@ def test_device_swarm_matches_oracle():
     assert ms.shape == (4,) and np.all(ms > 0)
 
 
-def test_modelfitting_recovers_targets():
+@pytest.mark.parametrize("slices,overlap", [(1, 0.0), (4, 0.05)])
+def test_modelfitting_recovers_targets(slices, overlap):
     """End to end through modelfitting(): 4 targets with their own OU inputs
-    and lengths; the swarm finds parameter sets with high gamma."""
+    and lengths; the swarm finds parameter sets with high gamma (also with
+    each input cut into 4 time slices simulated side by side)."""
     from brian_b200.synthetic import FitWorkload
     w = FitWorkload(ntargets=4, dur_min=2.0, dur_max=3.0, seed=5)
     w.build_targets()
@@ -193,7 +195,8 @@ def test_modelfitting_recovers_targets():
           "tau_t": [5e-2, 2e-1]}
     pr = {k: [v[0], v[0], v[1], v[1]] for k, v in pr.items()}
     res = modelfitting(model=_eqs(), reset=RESET, threshold=THRESHOLD, data=w.data(), input=w.inputs, dt=DT,
-                       popsize=512, maxiter=25, delta=4e-3, precision="float", seed=3, **pr)
+                       popsize=512, maxiter=25, delta=4e-3, precision="float", seed=3, slices=slices,
+                       overlap=overlap, **pr)
     assert len(res.best_fit) == 4
     assert np.min(res.best_fit) > 0.5
     assert res.info["trace"].shape == (25, 4)
@@ -280,3 +283,53 @@ def test_reciprocal_division_falls_back_exactly(precision):
     assert np.array_equal(S, r["state"], equal_nan=True)
     # the decaying tiny values did reach the subnormal range
     assert np.any((np.abs(r["state"][0, :32]) < np.finfo(dtype).tiny) & (r["state"][0, :32] != 0))
+
+
+@pytest.mark.parametrize("slices,overlap", [(1, 0.0), (3, 5e-3), (4, 0.0)])
+def test_time_slicing_matches_oracle(slices, overlap):
+    """Time slicing (modelfitting.py:49-58, 126-163, 221-223): every slice
+    of every candidate is simulated by the oracle from the input piece and
+    the shifted target spikes the slicing rules give, counts are summed over
+    the slices and gamma must equal the device's bit for bit."""
+    from brian_b200.modelfitting import FittingProblem
+    rng = np.random.default_rng(21)
+    lens = [9001, 7003]                      # not multiples of the slice count
+    inputs = [ou_current(n, DT, rng) for n in lens]
+    data = [np.sort(rng.uniform(0, n * DT, 40)) for n in lens]
+    pop = 16
+    prob = FittingProblem(_eqs(), THRESHOLD, RESET, data, inputs, DT, pop, precision="double",
+                          param_names=list(PARAMS), slices=slices, overlap=overlap)
+    N = 2 * pop
+    ov = int(overlap / DT) if slices > 1 else 0
+    # the slicing rules restated: input pieces, offsets, steps and trains
+    for j, (x, s) in enumerate(zip(inputs, data)):
+        L = slices * (len(x) // slices)
+        sl = L // slices
+        piece = np.hstack((np.zeros(ov), x[:L]))
+        base = prob.input_offsets[j]
+        assert np.array_equal(prob.sim_input[base:base + len(piece)], piece)
+        for k in range(slices):
+            for p in range(pop):
+                i = k * N + j * pop + p
+                assert prob.sim_input_offsets[i] == base + k * sl
+                assert prob.sim_nsteps[i] == (int((L * DT) / DT) if slices == 1 else sl + ov)
+                inside = s[(s >= k * sl * DT) & (s < (k + 1) * sl * DT)]
+                tr = np.hstack(([-1.0], inside - k * sl * DT + ov * DT, [overlap * (slices > 1) + L * DT / slices + 1.0]))
+                got = prob.sim_trains[prob.sim_train_offsets[i]:prob.sim_train_ends[i]]
+                assert np.array_equal(got, np.rint(tr / DT).astype(np.int32))
+    X = sample_prior(N, rng)
+    g = prob.evaluate(X)
+    state = prob.code.state
+    S0 = np.zeros((len(state), N * slices))
+    for d, k in enumerate(PARAMS):
+        S0[state.index(k)] = np.tile(X[d], slices)
+    m = of.ModelOracle(_eqs(), THRESHOLD, RESET, DT, np.float64)
+    r = of.simulate(m, S0, prob.sim_input, prob.sim_input_offsets, prob.sim_nsteps, prob.sim_trains,
+                    prob.sim_train_offsets, prob.sim_train_ends, np.zeros(N * slices, dtype=int),
+                    np.zeros(N * slices, dtype=int), delta=40, exclusive=True)
+    nc = r["coinc"].reshape(slices, N).sum(axis=0)
+    nm = r["nspikes"].reshape(slices, N).sum(axis=0)
+    ref = of.gamma(nc, nm, prob.target_length, prob.target_rate, 4e-3)
+    assert np.isfinite(ref).all() and nm.sum() > 100
+    assert np.array_equal(g, ref)
+    prob.handle.close()
