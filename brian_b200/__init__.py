@@ -13,7 +13,7 @@ from .clock import Clock, defaultclock, reinit_default_clock, guess_clock, defin
 from .equations import Equations
 from .groups import (NeuronGroup, PoissonGroup, SpikeGeneratorGroup, Threshold, VariableThreshold,
                      PoissonThreshold, NoThreshold, StringThreshold, Reset, VariableReset, StringReset, NoReset,
-                     Refractoriness, LazyStateUpdater)
+                     Refractoriness, LazyStateUpdater, EmpiricalThreshold)
 from .connections import Connection, DelayConnection, IdentityConnection
 from .stdp import ExponentialSTDP, STDP
 from .monitors import (SpikeMonitor, StateMonitor, SpikeCounter, PopulationSpikeCounter, PopulationRateMonitor,

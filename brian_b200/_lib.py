@@ -29,6 +29,8 @@ SIGNATURES = {
     "group_set_generator": [_vp, _i32, _i64, _vp, _vp],
     "group_set_reset": [_vp, _i32, ct.c_int, ct.c_int, _dbl, ct.c_int],
     "group_set_refractory": [_vp, _i32, _dbl, _i32, ct.c_int, _dbl],
+    "group_set_empirical": [_vp, _i32, _i32],
+    "group_set_model": [_vp, _i32, _vp],
     "conn_add": [_vp, _i32, _i64, _i64, _i32, _i64, _i64, ct.c_int, _i64, _vp, _vp, _vp, ct.c_int,
                  _i32, _vp, _i32, ct.c_int, _P(_i32)],
     "conn_add_dense": [_vp, _i32, _i64, _i64, _i32, _i64, _i64, ct.c_int, _vp, ct.c_int, _i32, ct.c_int,
@@ -202,6 +204,19 @@ class Runtime(object):
     def group_set_refractory(self, gid, refractory_time, period, var, value):
         self._c(self.t.group_set_refractory(self.h, gid, float(refractory_time), int(period), var,
                                             float(value)), "group_set_refractory")
+
+    def group_set_empirical(self, gid, steps):
+        self._c(self.t.group_set_empirical(self.h, gid, int(steps)), "group_set_empirical")
+
+    def group_set_model(self, gid, code, update=True, threshold=True, reset=True):
+        """Generated C of the group's model (codegen.ModelCode); the parts
+        left out keep the built-in linear update / threshold / reset."""
+        def b(x, keep):
+            return (x or "").encode() if keep else b""
+        m = FitModel(b(",".join(code.state), True), b(code.update, update), b"", b(code.threshold, threshold),
+                     b(code.reset, reset), b"", b"")
+        self._model_refs = getattr(self, "_model_refs", []) + [m]
+        self._c(self.t.group_set_model(self.h, gid, ct.byref(m)), "group_set_model")
 
     def conn_add(self, src, so, sn, tgt, to, tn, var, rowptr, cols, w, delay_steps=0, delays=None,
                  ring_depth=0, mod_var=-1):

@@ -23,6 +23,42 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
          "-fmad=false"]
 
 
+# Headers the network engine compiles again at run time (NVRTC) around a
+# generated model: embedded into bg_rtc_src.cu, which this script writes.
+RTC_HEADERS = ["bg_common.cuh", "bg_kernels.cuh"]
+RTC_OUT = os.path.join(CSRC, "bg_rtc_src.cu")
+
+
+def write_rtc_sources():
+    text = ""
+    for h in RTC_HEADERS:
+        with open(os.path.join(CSRC, h)) as f:
+            for line in f:
+                if line.strip().startswith('#include "'):
+                    continue
+                text += line
+        text += "\n"
+    if ")BGRTC\"" in text:
+        raise RuntimeError("embedded source contains the raw-string delimiter")
+    chunks, cur = [], ""
+    for line in text.splitlines(True):
+        if len(cur) + len(line) > 12000:
+            chunks.append(cur)
+            cur = ""
+        cur += line
+    chunks.append(cur)
+    out = ("// Generated by brian_b200/build.py from %s: the network engine's kernel\n"
+           "// sources, compiled again at run time around a generated model.\n"
+           "#include \"bg_rtc.h\"\n\nconst char *const kNetRtcSource[] = {\n" % ", ".join(RTC_HEADERS))
+    for c in chunks:
+        out += 'R"BGRTC(' + c + ')BGRTC",\n'
+    out += "nullptr};\n"
+    old = open(RTC_OUT).read() if os.path.exists(RTC_OUT) else None
+    if old != out:
+        with open(RTC_OUT, "w") as f:
+            f.write(out)
+
+
 def sources():
     return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
 
@@ -39,6 +75,7 @@ def needs_build():
 def build(force=False, verbose=False):
     if not force and not needs_build():
         return LIB
+    write_rtc_sources()
     objs = []
     for src in sources():
         obj = os.path.join(CSRC, os.path.basename(src)[:-3] + ".o")

@@ -1,7 +1,20 @@
 // bg_common.cuh -- shared device/host helpers for the brian_b200 engine.
 #pragma once
+#ifdef __CUDACC_RTC__
+// compiled at run time by NVRTC (generated network models): no host headers
+typedef signed char int8_t;
+typedef unsigned char uint8_t;
+typedef short int16_t;
+typedef unsigned short uint16_t;
+typedef int int32_t;
+typedef unsigned int uint32_t;
+typedef long long int64_t;
+typedef unsigned long long uint64_t;
+typedef unsigned long long uintptr_t;
+#else
 #include <cstdint>
 #include <cuda_runtime.h>
+#endif
 
 #define BG_OK 0
 #define BG_EINVAL (-1)
@@ -13,9 +26,11 @@
 #define BG_ENOSYS (-7)
 #define BG_ECOMPILE (-8)
 
+#ifndef __CUDACC_RTC__
 // Records the calling thread's error message for bg_last_error (library
 // internal; defined in bg_net.cu).
 int bg_internal_fail(int code, const char *msg);
+#endif
 
 // ---------------------------------------------------------------------------
 // Philox4x32-10 counter-based generator (Salmon, Moraes, Dror, Shaw,

@@ -185,6 +185,11 @@ void free_ptr(T *&p) {
 
 }  // namespace
 
+// Shared with the network engine (generated group kernels).
+int bg_nvrtc_compile(const std::string &src, std::vector<char> *cubin, std::string *log) {
+    return nvrtc_compile(src, cubin, log);
+}
+
 struct bg_fit {
     int device = 0;
     int precision = 64;

@@ -82,6 +82,7 @@ template <typename T> struct HeadArgs {
     const int64_t *gen_steps; const int32_t *gen_idx; int64_t gen_n;
     int reset_kind, reset_var, reset_var2; T reset_val;
     int refr; double refr_time; int period; int clamp_var; T clamp_val;
+    int emp_steps;                 // EmpiricalThreshold: no spike within this many steps of the last one (0: off)
     double *next_allowed; int32_t *last_spike;
     uint32_t *hist; int depth; int64_t nwords;
     int ndeliv; Deliv<T> deliv[kMaxDeliv];
@@ -107,6 +108,7 @@ __device__ __forceinline__ T linear_row(const T *A, const T *C, uint64_t anz, ui
     return acc;
 }
 
+#ifndef __CUDACC_RTC__
 // Host side: nonzero masks of the coefficients a kernel argument block holds.
 template <typename Args>
 inline void set_linear_masks(Args &a, int nvar) {
@@ -117,6 +119,7 @@ inline void set_linear_masks(Args &a, int nvar) {
         if (a.useC && a.C[j] != 0) a.cnz |= 1u << j;
     }
 }
+#endif
 
 // Block-aggregated counter update (one global atomic per block).
 __device__ __forceinline__ void block_count(unsigned long long *g, unsigned long long v) {
@@ -267,8 +270,20 @@ __device__ __forceinline__ void push_block_spikes(const HA &a, const uint32_t *w
 //   update: this step's 'groups' slot -- state update, threshold, refractory
 //           filter, history push -- then the pushes of this block's spikes
 //           into the rings of outgoing delayed connections.
-template <typename T, int NV>
-__global__ void __launch_bounds__(kHeadThreads, 2) k_head(const HeadArgs<T> a) {
+//
+// The model hooks come from M: BuiltinModel runs the exact linear update and
+// the threshold/reset kinds of HeadArgs; a generated model (compiled at run
+// time by NVRTC for a nonlinear model or a general string threshold/reset)
+// supplies any of update(s, t), threshold(s, t) and reset(s, t) itself.
+struct BuiltinModel {
+    static constexpr bool custom_update = false, custom_threshold = false, custom_reset = false;
+    template <typename T, int NV> static __device__ void update(T (&)[NV], double) {}
+    template <typename T, int NV> static __device__ bool threshold(const T (&)[NV], double) { return false; }
+    template <typename T, int NV> static __device__ void reset(T (&)[NV], double) {}
+};
+
+template <typename T, int NV, class M>
+__device__ __forceinline__ void head_body(const HeadArgs<T> &a) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int64_t base = (int64_t)blockIdx.x * kBlockNeurons;
     const long long nstep = a.ctl->nstep;
@@ -299,14 +314,16 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_head(const HeadArgs<T> a) {
                 if (i < a.n && (long long)ps - (long long)a.last_spike[i] < a.period)
                     set_var<T, NV>(s[u], a.clamp_var, a.clamp_val);
             }
-        } else if (a.reset_kind) {
+        } else if (M::custom_reset || a.reset_kind) {
             const uint32_t *H = a.hist + (int64_t)(ps % a.depth) * a.nwords;
+            const double tp = __dmul_rn((double)(cs - 1), a.dt);    // time of the step being finished
 #pragma unroll
             for (int u = 0; u < kNPT; ++u) {
                 const int64_t i = base + u * kHeadThreads + tid;
                 const uint32_t w = H[i >> 5];
                 if (i < a.n && ((w >> lane) & 1u)) {
-                    if (a.reset_kind == 1) set_var<T, NV>(s[u], a.reset_var, a.reset_val);
+                    if constexpr (M::custom_reset) M::template reset<T, NV>(s[u], tp);
+                    else if (a.reset_kind == 1) set_var<T, NV>(s[u], a.reset_var, a.reset_val);
                     else set_var<T, NV>(s[u], a.reset_var, get_var<T, NV>(s[u], a.reset_var2));
                 }
             }
@@ -336,7 +353,9 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_head(const HeadArgs<T> a) {
         for (int u = 0; u < kNPT; ++u) {
             const int64_t i = base + u * kHeadThreads + tid;
             const bool act = i < a.n;
-            if (a.linear) {
+            if constexpr (M::custom_update) {
+                M::template update<T, NV>(s[u], __dmul_rn((double)cs, a.dt));
+            } else if (a.linear) {
                 T x[NV];
 #pragma unroll
                 for (int j = 0; j < NV; ++j) x[j] = linear_row<T, NV>(a.A, a.C, a.anz, a.cnz, s[u], j);
@@ -344,7 +363,9 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_head(const HeadArgs<T> a) {
                 for (int j = 0; j < NV; ++j) s[u][j] = x[j];
             }
             bool spk = false;
-            if (act) {
+            if (act && M::custom_threshold) {
+                spk = M::template threshold<T, NV>(s[u], __dmul_rn((double)cs, a.dt));
+            } else if (act) {
                 switch (a.thr_kind) {
                 case 1: spk = get_var<T, NV>(s[u], a.thr_var) > a.thr_val; break;
                 case 2: spk = get_var<T, NV>(s[u], a.thr_var) > get_var<T, NV>(s[u], a.thr_var2); break;
@@ -366,12 +387,17 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_head(const HeadArgs<T> a) {
                 }
                 default: break;
                 }
+            }
+            if (act) {
+                // EmpiricalThreshold (threshold.py:449-457): no spike while the
+                // neuron is among the spikes of the last emp_steps steps
+                if (spk && a.emp_steps > 0 && (long long)nstep - (long long)a.last_spike[i] <= a.emp_steps) spk = false;
                 if (spk && a.refr) {
                     const double t = __dmul_rn((double)cs, a.dt);
                     if (a.next_allowed[i] <= t) a.next_allowed[i] = __dadd_rn(t, a.refr_time);
                     else spk = false;
                 }
-                if (spk && a.period > 0) a.last_spike[i] = (int32_t)nstep;
+                if (spk && (a.period > 0 || a.emp_steps > 0)) a.last_spike[i] = (int32_t)nstep;
             }
             const uint32_t ball = __ballot_sync(0xffffffffu, spk);
             if (lane == 0) {
@@ -394,6 +420,11 @@ __global__ void __launch_bounds__(kHeadThreads, 2) k_head(const HeadArgs<T> a) {
         }
     }
     bg_finish_step(a.ctl, a.last);
+}
+
+template <typename T, int NV>
+__global__ void __launch_bounds__(kHeadThreads, 2) k_head(const HeadArgs<T> a) {
+    head_body<T, NV, BuiltinModel>(a);
 }
 
 // ---------------------------------------------------------------------------

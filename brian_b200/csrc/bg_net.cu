@@ -7,6 +7,7 @@
 // replays it from a CUDA graph of kGraphSteps steps, draining monitor
 // buffers to host memory between chunks.
 #include <algorithm>
+#include <cctype>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -18,6 +19,7 @@
 
 #include "bg_kernels.cuh"
 #include "bg_persist.cuh"
+#include "bg_rtc.h"
 #include "../../include/brian_b200.h"
 
 namespace {
@@ -48,6 +50,13 @@ struct HGroup {
     void *dS = nullptr; uint32_t *dHist = nullptr; double *dNext = nullptr; int32_t *dLast = nullptr;
     int64_t *dGenSteps = nullptr; int32_t *dGenIdx = nullptr;
     std::vector<int> delivs, recs;
+    int emp_steps = 0;                  // EmpiricalThreshold window (steps), 0: off
+    // generated model (update / threshold / reset as C over s_<name>),
+    // compiled with the head kernel by NVRTC at prepare
+    std::vector<std::string> gen_names;
+    std::string gen_update, gen_threshold, gen_reset;
+    cudaLibrary_t gen_lib = nullptr; cudaKernel_t gen_kernel = nullptr;
+    bool generated() const { return !gen_update.empty() || !gen_threshold.empty() || !gen_reset.empty(); }
 };
 // A std::vector that leaves new elements uninitialised: the large host
 // copies of the connectivity are filled by parallel copies, which also
@@ -194,6 +203,61 @@ cudaError_t launch_head(const bg::HeadArgs<T> &a, int nvar, int64_t blocks, cuda
     }
 }
 
+// The head kernel of a group with a generated model: the engine's kernel
+// sources with a model policy over the group's registers (head_body).
+template <typename T>
+int compile_generated_head(HGroup &g) {
+    if (g.gen_kernel) return BG_OK;
+    const char *sc = sizeof(T) == 8 ? "double" : "float";
+    std::string src = "#define BG_GENERATED_MODEL 1\n";
+    for (const char *const *p = kNetRtcSource; *p; ++p) src += *p;
+    auto load = [&](bool cnst) {
+        std::string o;
+        for (size_t k = 0; k < g.gen_names.size(); ++k)
+            o += std::string("        ") + (cnst ? "const " : "") + "scalar s_" + g.gen_names[k] + " = S[" +
+                 std::to_string(k) + "];\n";
+        return o;
+    };
+    auto store = [&]() {
+        std::string o;
+        for (size_t k = 0; k < g.gen_names.size(); ++k)
+            o += "        S[" + std::to_string(k) + "] = s_" + g.gen_names[k] + ";\n";
+        return o;
+    };
+    src += "namespace bg {\nstruct GenModel {\n";
+    src += std::string("    static constexpr bool custom_update = ") + (g.gen_update.empty() ? "false" : "true") +
+           ", custom_threshold = " + (g.gen_threshold.empty() ? "false" : "true") +
+           ", custom_reset = " + (g.gen_reset.empty() ? "false" : "true") + ";\n";
+    src += "    template <typename T, int NV> static __device__ __forceinline__ void update(T (&S)[NV], double t_) {\n"
+           "        typedef T scalar; const scalar t = (scalar)t_; const scalar I_in = (scalar)0; (void)t; (void)I_in;\n" +
+           load(false) + g.gen_update + "\n" + store() + "    }\n";
+    src += "    template <typename T, int NV> static __device__ __forceinline__ bool threshold(const T (&S)[NV], double t_) {\n"
+           "        typedef T scalar; const scalar t = (scalar)t_; const scalar I_in = (scalar)0; (void)t; (void)I_in;\n" +
+           load(true) + "        return (bool)(" + (g.gen_threshold.empty() ? std::string("false") : g.gen_threshold) +
+           ");\n    }\n";
+    src += "    template <typename T, int NV> static __device__ __forceinline__ void reset(T (&S)[NV], double t_) {\n"
+           "        typedef T scalar; const scalar t = (scalar)t_; const scalar I_in = (scalar)0; const bool reset_on = true;\n"
+           "        (void)t; (void)I_in; (void)reset_on;\n" +
+           load(false) + g.gen_reset + "\n" + store() + "    }\n";
+    src += "};\n}  // namespace bg\n";
+    src += std::string("extern \"C\" __global__ void __launch_bounds__(bg::kHeadThreads, 2) bg_gen_head(const bg::HeadArgs<") +
+           sc + "> a) {\n    bg::head_body<" + sc + ", " + std::to_string(std::max(1, g.nvar)) + ", bg::GenModel>(a);\n}\n";
+    std::vector<char> cubin;
+    std::string log;
+    int rc = bg_nvrtc_compile(src, &cubin, &log);
+    if (rc) return rc;
+    cudaError_t e = cudaLibraryLoadData(&g.gen_lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
+    if (e == cudaSuccess) e = cudaLibraryGetKernel(&g.gen_kernel, g.gen_lib, "bg_gen_head");
+    if (e != cudaSuccess) return fail(BG_ECUDA, std::string("generated group kernel: ") + cudaGetErrorString(e));
+    return BG_OK;
+}
+
+template <typename T>
+cudaError_t launch_generated_head(cudaKernel_t k, const bg::HeadArgs<T> &a, int64_t blocks, cudaStream_t s) {
+    void *args[] = {(void *)&a};
+    return cudaLaunchKernel((const void *)k, dim3((unsigned)blocks), dim3(bg::kHeadThreads), args, 0, s);
+}
+
 template <typename T>
 int build_group(bg_net *net, int gid) {
     HGroup &g = net->groups[gid];
@@ -211,7 +275,7 @@ int build_group(bg_net *net, int gid) {
     a.gen_steps = g.dGenSteps; a.gen_idx = g.dGenIdx; a.gen_n = (int64_t)g.gen_steps.size();
     a.reset_kind = g.reset_kind; a.reset_var = g.reset_var; a.reset_var2 = g.reset_var2; a.reset_val = (T)g.reset_val;
     a.refr = g.refr; a.refr_time = g.refr_time; a.period = g.period; a.clamp_var = g.clamp_var; a.clamp_val = (T)g.clamp_val;
-    a.next_allowed = g.dNext; a.last_spike = g.dLast;
+    a.next_allowed = g.dNext; a.last_spike = g.dLast; a.emp_steps = g.emp_steps;
     a.hist = g.dHist; a.depth = g.depth; a.nwords = g.npad / 32;
     if ((int)g.delivs.size() > bg::kMaxDeliv) return fail(BG_ENOSYS, "too many DelayConnections into one group");
     a.ndeliv = (int)g.delivs.size();
@@ -241,9 +305,26 @@ int build_group(bg_net *net, int gid) {
     }
     const int64_t blocks = g.npad / bg::kBlockNeurons;
     const int nvar = g.nvar;
+    a.spikes = net->dCounters + gid;
+    if (g.generated()) {
+        int st = compile_generated_head<T>(g);
+        if (st) return st;
+        const bool has_tail = a.ndeliv || g.reset_kind || !g.gen_reset.empty() || g.period > 0 || a.nrec;
+        const cudaKernel_t k = g.gen_kernel;
+        net->item_names.push_back("genhead[g" + std::to_string(gid) + "]");
+        net->step_launches.push_back([a, k, blocks](cudaStream_t s, int tail, int last) {
+            bg::HeadArgs<T> b = a; b.tail = tail; b.update = 1; b.last = last;
+            return launch_generated_head<T>(k, b, blocks, s);
+        });
+        if (has_tail)
+            net->finalize_launches.push_back([a, k, blocks](cudaStream_t s, int, int) {
+                bg::HeadArgs<T> b = a; b.tail = 1; b.update = 0; b.last = 0;
+                return launch_generated_head<T>(k, b, blocks, s);
+            });
+        return BG_OK;
+    }
     if (nvar > bg::kMaxVars) return fail(BG_ENOSYS, "more than 8 state variables in a linear group");
     const bool has_tail = a.ndeliv || g.reset_kind || g.period > 0 || a.nrec;
-    a.spikes = net->dCounters + gid;
     net->item_names.push_back("head[g" + std::to_string(gid) + "]");
     net->step_launches.push_back([a, nvar, blocks](cudaStream_t s, int tail, int last) {
         bg::HeadArgs<T> b = a; b.tail = tail; b.update = 1; b.last = last;
@@ -575,6 +656,7 @@ int build_persist(bg_net *net) {
 
     const HGroup &g = net->groups[0];
     if (!g.linear || g.nvar < 1 || g.nvar > 4 || g.refr || g.period > 0) return BG_OK;
+    if (g.generated() || g.emp_steps > 0) return BG_OK;
     if (g.thr_kind != BG_THR_CONST && g.thr_kind != BG_THR_VAR && g.thr_kind != BG_THR_NONE) return BG_OK;
     if (net->conns.empty() || (int)net->conns.size() > bg::kPersistMaxPush) return BG_OK;
     if ((int)g.delivs.size() > bg::kPersistMaxDeliv) return BG_OK;
@@ -725,6 +807,8 @@ int bg_net_destroy(bg_net *n) {
     cudaSetDevice(n->device);
     if (n->stream) cudaStreamSynchronize(n->stream);
     if (n->gexec) cudaGraphExecDestroy(n->gexec);
+    for (auto &g : n->groups)
+        if (g.gen_lib) cudaLibraryUnload(g.gen_lib);
     for (void *p : n->allocs) cudaFree(p);
     if (n->ev0) cudaEventDestroy(n->ev0);
     if (n->ev1) cudaEventDestroy(n->ev1);
@@ -798,6 +882,41 @@ int bg_group_set_refractory(bg_net *n, int32_t gid, double rt, int32_t period, i
     if (period > 0 && (var < 0 || var >= g.nvar)) return fail(BG_EINVAL, "clamp variable out of range");
     // rt <= 0: no spike filter (refractory < 0.9*dt), clamp only
     g.refr = rt > 0; g.refr_time = rt; g.period = period; g.clamp_var = var; g.clamp_val = value;
+    return BG_OK;
+}
+
+int bg_group_set_empirical(bg_net *n, int32_t gid, int32_t steps) {
+    if (!gid_ok(n, gid) || steps < 0) return fail(BG_EINVAL, "bg_group_set_empirical");
+    if (n->prepared) return fail(BG_ESTATE, "network already prepared");
+    n->groups[gid].emp_steps = steps;
+    return BG_OK;
+}
+
+int bg_group_set_model(bg_net *n, int32_t gid, const bg_fit_model *m) {
+    if (!gid_ok(n, gid) || !m || !m->state_names) return fail(BG_EINVAL, "bg_group_set_model");
+    if (n->prepared) return fail(BG_ESTATE, "network already prepared");
+    HGroup &g = n->groups[gid];
+    std::vector<std::string> names;
+    std::string cur;
+    for (const char *p = m->state_names;; ++p) {
+        if (*p == ',' || *p == 0) {
+            if (cur.empty()) return fail(BG_EINVAL, "empty state variable name");
+            names.push_back(cur);
+            cur.clear();
+            if (*p == 0) break;
+        } else if (std::isalnum((unsigned char)*p) || *p == '_') {
+            cur += *p;
+        } else if (*p != ' ') {
+            return fail(BG_EINVAL, "bad state variable name");
+        }
+    }
+    if ((int)names.size() != g.nvar) return fail(BG_EINVAL, "model names do not match the group's variables");
+    if (g.nvar > 16) return fail(BG_ENOSYS, "more than 16 state variables in a generated model");
+    g.gen_names = names;
+    g.gen_update = m->update_code ? m->update_code : "";
+    g.gen_threshold = m->threshold_code ? m->threshold_code : "";
+    g.gen_reset = m->reset_code ? m->reset_code : "";
+    if (!g.gen_update.empty()) g.linear = false;
     return BG_OK;
 }
 
@@ -1125,7 +1244,8 @@ int bg_net_prepare(bg_net *n) {
         for (int v = 0; v < g.nvar; ++v) { int st = upload_state(n, g, v, g.S0.data() + (size_t)v * g.n); if (st) return st; }
         if (n->alloc(&g.dHist, (size_t)g.depth * (g.npad / 32) * 4) != cudaSuccess) return fail(BG_ENOMEM, "spike history");
         if (g.refr && n->alloc(&g.dNext, g.npad * 8) != cudaSuccess) return fail(BG_ENOMEM, "refractory");
-        if (g.period > 0 && n->alloc(&g.dLast, g.npad * 4) != cudaSuccess) return fail(BG_ENOMEM, "refractory");
+        if ((g.period > 0 || g.emp_steps > 0) && n->alloc(&g.dLast, g.npad * 4) != cudaSuccess)
+            return fail(BG_ENOMEM, "refractory");
         if (!g.gen_steps.empty()) {
             if (n->alloc(&g.dGenSteps, g.gen_steps.size() * 8) != cudaSuccess || n->alloc(&g.dGenIdx, g.gen_idx.size() * 4) != cudaSuccess)
                 return fail(BG_ENOMEM, "generator");

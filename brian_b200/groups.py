@@ -17,7 +17,7 @@ from .equations import Equations, linear_propagator, _identifiers
 
 __all__ = ["NeuronGroup", "PoissonGroup", "SpikeGeneratorGroup", "Threshold", "VariableThreshold",
            "PoissonThreshold", "NoThreshold", "StringThreshold", "Reset", "VariableReset", "StringReset",
-           "NoReset", "Refractoriness", "LazyStateUpdater"]
+           "NoReset", "Refractoriness", "LazyStateUpdater", "EmpiricalThreshold"]
 
 _counter = itertools.count()
 
@@ -53,9 +53,30 @@ class NoThreshold(Threshold):
         pass
 
 
+class EmpiricalThreshold(Threshold):
+    """S[state] > threshold for neurons that did not spike in the last
+    `refractory` (threshold.py:409-457), for models such as Hodgkin-Huxley
+    that return to rest by their own dynamics (use with no reset)."""
+
+    def __init__(self, threshold=1e-3, refractory=1e-3, state=0, clock=None):
+        self.threshold = float(threshold)
+        self.state = state
+        dt = guess_clock(clock).dt
+        self.refractory = int(float(refractory) / dt)
+        # a whole number of steps is taken one step shorter (threshold.py:444-447)
+        if self.refractory > 0 and _approx_equal(self.refractory * dt, float(refractory)):
+            self.refractory -= 1
+
+
+def _approx_equal(x, y):
+    """is_approx_equal (utils/approximatecomparisons.py:96-98): within
+    10000 machine epsilons relative to x."""
+    return x == y or abs(x - y) < abs(x) * (np.finfo(np.float64).eps * 10000)
+
+
 class StringThreshold(Threshold):
-    """Threshold given as a string; the forms ``x > <constant>`` and
-    ``x > y`` (state variables x, y) are supported."""
+    """Threshold given as a string: any condition on the state variables
+    (and t), compiled into the group's kernel."""
 
     def __init__(self, expr, level=0, namespace=None):
         self.expr = expr
@@ -203,11 +224,15 @@ class _GroupBase(object):
 class NeuronGroup(_GroupBase):
     """Group of neurons sharing one model (neurongroup.py:258-456).
 
-    Supported models on the device path: linear equations (exact propagator)
-    and groups without dynamics.  Thresholds: scalar, Threshold,
-    VariableThreshold, 'x > c' / 'x > y' strings, PoissonThreshold.  Resets:
-    scalar, Reset, VariableReset, 'x = c' / 'x = y' strings; refractory
-    period > 0.9*dt selects Refractoriness as in the reference."""
+    The state updater follows magic_state_updater (stateupdater.py:70-172):
+    linear equations get the exact propagator; nonlinear ones (or an explicit
+    `method`) are integrated by Euler, second-order Runge-Kutta (order=2 or
+    method='RK') or exponential Euler (implicit=True or
+    method='exponential_Euler'), generated as C and compiled into the group's
+    kernel.  Thresholds: scalar, Threshold, VariableThreshold,
+    EmpiricalThreshold, PoissonThreshold, or any condition string; resets:
+    scalar, Reset, VariableReset, or statement strings; refractory period >
+    0.9*dt selects Refractoriness as in the reference."""
 
     def __init__(self, N, model=None, threshold=None, reset=None, init=None, refractory=0.0, level=0,
                  clock=None, order=1, implicit=False, unit_checking=True, max_delay=0.0, compile=False,
@@ -247,15 +272,17 @@ class NeuronGroup(_GroupBase):
         # GPUModelFitting takes its model.  Lowering it onto a network raises.
         self._fitting_only = None
         self._level = level
+        # integration scheme of a generated update (None: exact linear)
+        self._scheme = None
         if self.eqs is not None:
             if method not in (None, "linear", "Euler", "RK", "exponential_Euler"):
                 raise NotImplementedError("integration method %r is not supported" % method)
             if method in ("Euler", "RK", "exponential_Euler"):
-                self._fitting_only = ("integration method %r runs in modelfitting only; the network engine "
-                                      "integrates linear models exactly" % method)
+                self._scheme = method
             elif not self.eqs.is_linear():
-                self._fitting_only = ("nonlinear equations run in modelfitting only; the network engine "
-                                      "integrates linear models with the exact propagator")
+                if method == "linear":
+                    raise TypeError("method='linear' given for nonlinear equations")
+                self._scheme = "exponential_Euler" if implicit else ("RK" if order == 2 else "Euler")
         # ---- threshold
         self._threshold = self._select_threshold(threshold, level + 1)
         # ---- reset / refractoriness (neurongroup.py:369-429)
@@ -302,9 +329,7 @@ class NeuronGroup(_GroupBase):
             rhs = m.group(2) if m else ""
             if not m or m.group(1) not in self.var_index or (
                     rhs not in self.var_index and _identifiers(rhs) & (set(self._names) | {"t"})):
-                self._fitting_only = self._fitting_only or (
-                    "threshold string %r runs in modelfitting only; the network engine supports 'x > c' "
-                    "and 'x > y'" % threshold)
+                # a general condition: compiled into the group's kernel
                 return StringThreshold(threshold, namespace=self._ns(level + 1))
             if rhs in self.var_index:
                 return VariableThreshold(rhs, m.group(1))
@@ -325,9 +350,7 @@ class NeuronGroup(_GroupBase):
             rhs = m.group(2).strip() if m else ""
             if not m or m.group(1) not in self.var_index or (
                     rhs not in self.var_index and _identifiers(rhs) & (set(self._names) | {"t"})):
-                self._fitting_only = self._fitting_only or (
-                    "reset string %r runs in modelfitting only; the network engine supports 'x = c' and "
-                    "'x = y'" % reset)
+                # general statements: compiled into the group's kernel
                 return StringReset(reset, namespace=self._ns(level + 1))
             if rhs in self.var_index:
                 return VariableReset(rhs, m.group(1))
@@ -369,10 +392,32 @@ class NeuronGroup(_GroupBase):
             raise NotImplementedError(self._fitting_only)
         S0 = self._S_host if self._names else np.zeros((0, self._n))
         gid = rt.group_add(S0)
-        if self.eqs is not None and self._names:
+        if self.eqs is not None and self._names and self._scheme is None:
             A, C = linear_propagator(self.eqs, dt)
             rt.group_set_linear(gid, A, C)
         th = self._threshold
+        gen_thr = isinstance(th, StringThreshold)
+        gen_reset = isinstance(self._reset, StringReset)
+        if self._scheme is not None or gen_thr or gen_reset:
+            from .codegen import generate_model_code
+            if self.eqs is None:
+                raise NotImplementedError("string thresholds and resets need a model with equations")
+            ns = {}
+            for obj in (th, self._reset):
+                ns.update(getattr(obj, "namespace", None) or {})
+            code = generate_model_code(self.eqs, th.expr if gen_thr else 0.0,
+                                       self._reset.expr if gen_reset else None, dt, input_var=None,
+                                       scalar="float" if rt.precision == 32 else "double",
+                                       scheme=self._scheme or "Euler", namespace=ns)
+            if list(code.state) != list(self._names):
+                raise NotImplementedError("generated model variables %s differ from the group's %s"
+                                          % (code.state, self._names))
+            rt.group_set_model(gid, code, update=self._scheme is not None, threshold=gen_thr, reset=gen_reset)
+        if isinstance(th, EmpiricalThreshold):
+            rt.group_set_threshold(gid, 1, self._var(th.state), th.threshold, 0)
+            if th.refractory > 0:
+                rt.group_set_empirical(gid, th.refractory)
+            th = None
         if isinstance(th, PoissonThreshold):
             seed = th.seed if th.seed is not None else int(np.random.randint(0, 2 ** 31 - 1))
             th.seed = seed
@@ -381,7 +426,7 @@ class NeuronGroup(_GroupBase):
             rt.group_set_generator(gid, th.steps, th.idx)
         elif isinstance(th, VariableThreshold):
             rt.group_set_threshold(gid, 2, self._var(th.state), 0.0, self._var(th.threshold_state))
-        elif isinstance(th, NoThreshold):
+        elif th is None or isinstance(th, (NoThreshold, StringThreshold)):
             pass
         elif isinstance(th, Threshold):
             rt.group_set_threshold(gid, 1, self._var(th.state), th.threshold, 0)
@@ -396,7 +441,7 @@ class NeuronGroup(_GroupBase):
             pass
         elif isinstance(rs, VariableReset):
             rt.group_set_reset(gid, 2, self._var(rs.state), 0.0, self._var(rs.resetvaluestate))
-        elif isinstance(rs, NoReset):
+        elif isinstance(rs, (NoReset, StringReset)):
             pass
         elif isinstance(rs, Reset):
             rt.group_set_reset(gid, 1, self._var(rs.state), rs.resetvalue, 0)

@@ -116,6 +116,10 @@ BG_API int bg_group_set_reset(bg_net *net, int32_t gid, int kind, int var,
  * the spike filter off, as for T < 0.9*dt);
  * period = int(T/dt)+1 bins during which S[var] is clamped to value
  * (period 0: no clamp, only the spike filter). */
+/* EmpiricalThreshold (threshold.py:409-457): a neuron that spiked in the
+ * last `steps` steps does not spike (steps = the threshold's refractory in
+ * steps); 0 turns it off. */
+BG_API int bg_group_set_empirical(bg_net *net, int32_t gid, int32_t steps);
 BG_API int bg_group_set_refractory(bg_net *net, int32_t gid, double refractory_time,
                             int32_t period, int var, double value);
 
@@ -291,6 +295,16 @@ typedef struct bg_fit_model {
     const char *setup_code;       /* statements run once after the state is
                                      loaded (may set bool bg_exact), or NULL      */
 } bg_fit_model;
+
+/* A group's model as generated C (the snippets of bg_fit_model over the
+ * registers s_<name>, names in the group's variable order): any of the
+ * update of one step, the threshold condition and the reset statements
+ * (selects on `reset_on`) replaces the built-in linear update, threshold
+ * kind and reset kind of that group.  The group's head kernel is compiled
+ * with them by NVRTC at bg_net_prepare.  Replaces the state updater,
+ * StringThreshold and StringReset of a nonlinear NeuronGroup
+ * (stateupdater.py:70-172, threshold.py:203-242, reset.py:155-217). */
+BG_API int bg_group_set_model(bg_net *net, int32_t gid, const bg_fit_model *model);
 /* Compile only (no device needed); the log is copied to `log`. */
 BG_API int bg_fit_compile_check(int precision, const bg_fit_model *model, double dt,
                                 int delta_steps, int exclusive, char *log, int64_t log_len);

@@ -29,6 +29,12 @@
  *   STDP pre/post updaters ........ stdp.py:31-54, 370-414, 452-539
  *   SpikeMonitor .................. monitor.py:156-166
  *   StateMonitor .................. monitor.py:824-842
+ *   EmpiricalThreshold ............ threshold.py:449-457 (LS[0:refractory])
+ *   nonlinear model / StringThreshold / StringReset: the generated C snippets
+ *   of the model (the engine compiles the same text with NVRTC) are compiled
+ *   here with gcc -O2 -ffp-contract=off and applied neuron by neuron in the
+ *   slots above; the numpy evaluation of the equations (oracle/fitting.py)
+ *   checks the snippets themselves.
  */
 #include <cstdint>
 #include <cstring>
@@ -37,6 +43,9 @@
 #include <vector>
 #include <deque>
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <dlfcn.h>
 
 #define OR_OK 0
 #define OR_EINVAL (-1)
@@ -44,6 +53,8 @@
 #define OR_ENOSYS (-7)
 
 static thread_local std::string g_err;
+#include <unistd.h>
+static long getpid_or() { return (long)getpid(); }
 static int fail(int code, const std::string &m) { g_err = m; return code; }
 
 /* ---------------- Philox4x32-10 (Salmon et al., SC'11) ------------------ */
@@ -83,6 +94,11 @@ struct Group {
     std::deque<std::vector<int32_t>> hist;   /* hist[0] = current step */
     int32_t depth = 1;
     int64_t nspikes = 0;
+    int32_t emp_steps = 0; std::vector<int64_t> last_spike;
+    /* generated model: one neuron at a time over S[var * n + i] */
+    void (*gen_update)(double *, int64_t, int64_t, double) = nullptr;
+    int (*gen_threshold)(const double *, int64_t, int64_t, double) = nullptr;
+    void (*gen_reset)(double *, int64_t, int64_t, double) = nullptr;
 };
 struct Conn {
     int32_t src, tgt; int64_t so, sn, to, tn; int var;
@@ -179,6 +195,71 @@ int or_group_set_reset(or_net *n, int32_t gid, int kind, int var, double value, 
     if (kind == 2 && (var2 < 0 || var2 >= g.nvar)) return fail(OR_EINVAL, "reset var2");
     g.reset_kind = kind; g.reset_var = var; g.reset_val = value; g.reset_var2 = var2; return OR_OK;
 }
+int or_group_set_empirical(or_net *n, int32_t gid, int32_t steps) {
+    if (!gid_ok(n, gid) || steps < 0) return fail(OR_EINVAL, "set_empirical");
+    n->groups[gid].emp_steps = steps;
+    return OR_OK;
+}
+
+/* Same layout as bg_fit_model: state names (comma separated), update,
+ * update with reciprocals (unused here), threshold, reset, aux decl, setup. */
+struct or_model {
+    const char *state_names, *update_code, *update_fast_code, *threshold_code, *reset_code, *aux_decl, *setup_code;
+};
+
+int or_group_set_model(or_net *n, int32_t gid, const or_model *m) {
+    if (!gid_ok(n, gid) || !m || !m->state_names) return fail(OR_EINVAL, "set_model");
+    Group &g = n->groups[gid];
+    std::vector<std::string> names;
+    std::string cur;
+    for (const char *p = m->state_names;; ++p) {
+        if (*p == ',' || *p == 0) { names.push_back(cur); cur.clear(); if (!*p) break; }
+        else if (*p != ' ') cur += *p;
+    }
+    if ((int)names.size() != g.nvar) return fail(OR_EINVAL, "model names do not match the group");
+    auto s = [](const char *x) { return std::string(x ? x : ""); };
+    const std::string upd = s(m->update_code), thr = s(m->threshold_code), rst = s(m->reset_code);
+    std::string c = "#include <math.h>\ntypedef double scalar;\n"
+                    "static inline double __longlong_as_double(long long x) { union { long long i; double d; } u; u.i = x; return u.d; }\n";
+    auto load = [&]() {
+        std::string o;
+        for (size_t k = 0; k < names.size(); ++k)
+            o += "    scalar s_" + names[k] + " = S[" + std::to_string(k) + "LL * N + i];\n";
+        return o;
+    };
+    auto store = [&]() {
+        std::string o;
+        for (size_t k = 0; k < names.size(); ++k) o += "    S[" + std::to_string(k) + "LL * N + i] = s_" + names[k] + ";\n";
+        return o;
+    };
+    const std::string pre = "    const scalar t = (scalar)t_; const scalar I_in = 0; (void)t; (void)I_in;\n";
+    c += "void gm_update(double *S, long long N, long long i, double t_) {\n" + pre + load() + upd + "\n" + store() + "}\n";
+    c += "int gm_threshold(const double *S, long long N, long long i, double t_) {\n" + pre + load() + "    return (" +
+         (thr.empty() ? std::string("0") : thr) + ") ? 1 : 0;\n}\n";
+    c += "void gm_reset(double *S, long long N, long long i, double t_) {\n" + pre +
+         "    const int reset_on = 1; (void)reset_on;\n" + load() + rst + "\n" + store() + "}\n";
+    /* compile next to this library (_ref/gen under the oracle's directory) */
+    Dl_info info;
+    if (!dladdr((void *)&or_group_set_model, &info) || !info.dli_fname) return fail(OR_ESTATE, "dladdr");
+    std::string dir = info.dli_fname;
+    dir = dir.substr(0, dir.find_last_of('/')) + "/_ref/gen";
+    static int counter = 0;
+    const std::string stem = dir + "/model_" + std::to_string((long long)getpid_or()) + "_" + std::to_string(counter++);
+    if (std::system(("mkdir -p '" + dir + "'").c_str()) != 0) return fail(OR_ESTATE, "mkdir " + dir);
+    FILE *f = std::fopen((stem + ".c").c_str(), "w");
+    if (!f) return fail(OR_ESTATE, "cannot write " + stem + ".c");
+    std::fputs(c.c_str(), f);
+    std::fclose(f);
+    const std::string cmd = "gcc -O2 -ffp-contract=off -fno-fast-math -shared -fPIC -w -o '" + stem + ".so' '" + stem + ".c' -lm";
+    if (std::system(cmd.c_str()) != 0) return fail(OR_ESTATE, "gcc failed on the generated model: " + stem + ".c");
+    void *h = dlopen((stem + ".so").c_str(), RTLD_NOW | RTLD_LOCAL);
+    if (!h) return fail(OR_ESTATE, std::string("dlopen: ") + dlerror());
+    if (!upd.empty()) { g.gen_update = (void (*)(double *, int64_t, int64_t, double))dlsym(h, "gm_update"); g.linear = false; }
+    if (!thr.empty()) g.gen_threshold = (int (*)(const double *, int64_t, int64_t, double))dlsym(h, "gm_threshold");
+    if (!rst.empty()) g.gen_reset = (void (*)(double *, int64_t, int64_t, double))dlsym(h, "gm_reset");
+    return OR_OK;
+}
+
 int or_group_set_refractory(or_net *n, int32_t gid, double rt, int32_t period, int var, double value) {
     if (!gid_ok(n, gid) || period < 0) return fail(OR_EINVAL, "set_refractory");
     Group &g = n->groups[gid];
@@ -365,13 +446,18 @@ int or_net_prepare(or_net *n) {
     for (auto &g : n->groups) {
         g.hist.assign(g.depth, std::vector<int32_t>());
         if (g.refr) g.next_allowed.assign(g.n, -1.0);
+        if (g.emp_steps > 0) g.last_spike.assign(g.n, -(1ll << 40));
     }
     n->prepared = true; return OR_OK;
 }
 
 int or_net_reinit(or_net *n) {
     if (!n) return fail(OR_EINVAL, "net");
-    for (auto &g : n->groups) { for (auto &h : g.hist) h.clear(); if (g.refr) std::fill(g.next_allowed.begin(), g.next_allowed.end(), -1.0); }
+    for (auto &g : n->groups) {
+        for (auto &h : g.hist) h.clear();
+        if (g.refr) std::fill(g.next_allowed.begin(), g.next_allowed.end(), -1.0);
+        std::fill(g.last_spike.begin(), g.last_spike.end(), -(1ll << 40));
+    }
     for (auto &c : n->conns) std::fill(c.ring.begin(), c.ring.end(), 0.0);
     for (auto &s : n->stdps) { std::fill(s.A_pre.begin(), s.A_pre.end(), 0.0); std::fill(s.A_post.begin(), s.A_post.end(), 0.0); }
     return OR_OK;
@@ -394,7 +480,9 @@ static void step(or_net *n, int64_t cs) {
     /* ---- groups slot ---- */
     for (auto &g : n->groups) {
         const int64_t N = g.n; const int m = g.nvar;
-        if (g.linear) {
+        if (g.gen_update) {
+            for (int64_t i = 0; i < N; ++i) g.gen_update(g.S.data(), N, i, t);
+        } else if (g.linear) {
             std::vector<double> x(m), s(m);
             for (int64_t i = 0; i < N; ++i) {
                 for (int k = 0; k < m; ++k) s[k] = g.S[(size_t)k * N + i];
@@ -415,6 +503,9 @@ static void step(or_net *n, int64_t cs) {
             }
         }
         std::vector<int32_t> spikes;
+        if (g.gen_threshold) {
+            for (int64_t i = 0; i < N; ++i) if (g.gen_threshold(g.S.data(), N, i, t)) spikes.push_back((int32_t)i);
+        } else
         switch (g.thr_kind) {
         case 1: { const double *v = &g.S[(size_t)g.thr_var * N];
                   for (int64_t i = 0; i < N; ++i) if (v[i] > g.thr_val) spikes.push_back((int32_t)i); break; }
@@ -428,6 +519,13 @@ static void step(or_net *n, int64_t cs) {
                       if (spikes.empty() || spikes.back() != i) spikes.push_back(i);
                   } break; }
         default: break;
+        }
+        if (g.emp_steps > 0) {   /* not among the spikes of the last emp_steps steps */
+            if (g.last_spike.empty()) g.last_spike.assign(N, -(1ll << 40));
+            std::vector<int32_t> kept;
+            for (int32_t i : spikes) if (n->nstep - g.last_spike[i] > g.emp_steps) kept.push_back(i);
+            for (int32_t i : kept) g.last_spike[i] = n->nstep;
+            spikes.swap(kept);
         }
         if (g.refr) {
             std::vector<int32_t> kept;
@@ -532,6 +630,8 @@ static void step(or_net *n, int64_t cs) {
             double *v = &g.S[(size_t)g.clamp_var * N];
             for (int32_t b = 0; b < g.period && b < g.depth; ++b)
                 for (int32_t i : g.hist[b]) v[i] = g.clamp_val;
+        } else if (g.gen_reset) {
+            for (int32_t i : g.hist[0]) g.gen_reset(g.S.data(), N, i, t);
         } else if (g.reset_kind == 1) {
             double *v = &g.S[(size_t)g.reset_var * N];
             for (int32_t i : g.hist[0]) v[i] = g.reset_val;

@@ -119,6 +119,49 @@ def cuba_delay(N=3000, indegree=100, steps=2000, seed=3, wdtype=np.float32, we=0
     return _result(net, groups=[P], spikemons=[M], statemons=[S])
 
 
+def coba(N=2000, steps=2000, seed=7, method=None, implicit=False, order=1, string_threshold=True,
+         string_reset=True, delays=True, empirical=False, linear=False):
+    """A conductance-based (nonlinear) network: v driven by ge*(Ee-v) and
+    gi*(Ei-v), integrated by the generated scheme of `method`/`implicit`/
+    `order`; a condition string threshold and a two-statement string reset,
+    or EmpiricalThreshold with no reset; sparse excitatory and (delayed)
+    inhibitory connections; spike and state monitors."""
+    taum, taue, taui = 20 * ms, 5 * ms, 10 * ms
+    Ee, Ei, El, Vt, Vr = 0 * mV, -80 * mV, -49 * mV, -50 * mV, -60 * mV
+    # linear: current-based instead (exact update, generated threshold/reset)
+    eqs = b.Equations("""
+    dv/dt  = (%s + (El-v))/taum : volt
+    dge/dt = -ge/taue : 1
+    dgi/dt = -gi/taui : 1
+    """ % ("0.01*ge*volt - 0.04*gi*volt" if linear else "ge*(Ee-v) + gi*(Ei-v)"),
+                       taum=taum, taue=taue, taui=taui, Ee=Ee, Ei=Ei, El=El, volt=1.0)
+    if empirical:
+        thr, rst = b.EmpiricalThreshold(threshold=Vt, refractory=3 * ms), None
+    else:
+        thr = "v > Vt + 2*mV*ge" if string_threshold else Vt
+        rst = "v = Vr\nge = ge*0.5" if string_reset else Vr
+    P = b.NeuronGroup(N, model=eqs, threshold=thr, reset=rst, method=method, implicit=implicit, order=order)
+    Ne = int(0.8 * N)
+    Pe, Pi = P.subgroup(Ne), P.subgroup(N - Ne)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    rowe, cole = fixed_indegree_csr(Ne, N, 40, seed=seed + 1)
+    rowi, coli = fixed_indegree_csr(N - Ne, N, 10, seed=seed + 2)
+    Ce = b.Connection(Pe, P, "ge")
+    Ce.connect_csr(rowe, cole, 0.05 * (0.5 + rng.random(len(cole))))
+    if delays:
+        Ci = b.DelayConnection(Pi, P, "gi", max_delay=2 * ms)
+        Ci.connect_csr(rowi, coli, 0.2, delay_steps=rng.integers(1, 21, len(coli)).astype(np.uint8))
+    else:
+        Ci = b.Connection(Pi, P, "gi")
+        Ci.connect_csr(rowi, coli, 0.2)
+    P.v = Vr + rng.random(N) * (Vt - Vr + 2 * mV)
+    M = b.SpikeMonitor(P)
+    S = b.StateMonitor(P, "v", record=[0, 1, N - 1])
+    net = b.Network(P, Ce, Ci, M, S)
+    net.run(steps * 0.1 * ms)
+    return _result(net, groups=[P], spikemons=[M], statemons=[S])
+
+
 def stdp(Nin=400, Nout=32, steps=3000, seed=5, dense=True, rate_lo=5.0, rate_hi=25.0, wdtype=np.float32):
     """Config 3 in miniature: Poisson inputs -> LIF outputs, all-to-all,
     ExponentialSTDP (examples/plasticity/STDP1.py)."""

@@ -148,3 +148,29 @@ def test_run_split_equals_single_run(gpu_table):
     b.clear(); b.reinit_default_clock(); np.random.seed(1)
     two = scenarios.cuba(N=2000, steps=617, _split=True) if False else None
     assert one["spk0.idx"].size > 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kw", [dict(), dict(method="RK"), dict(string_threshold=False, string_reset=False),
+                                dict(delays=False), dict(empirical=True), dict(linear=True)],
+                         ids=["euler-strings", "rk2", "euler-builtin-thr-reset", "no-delays", "empirical",
+                              "linear-strings"])
+def test_generated_model_bit_exact(oracle_table, gpu_table, kw):
+    """Nonlinear (conductance-based) groups and string thresholds/resets:
+    the group kernel compiled by NVRTC around the generated model gives the
+    oracle's spikes and states bit for bit (polynomial model, FP64)."""
+    ref, gpu = _both(scenarios.coba, oracle_table, **kw)
+    assert len(ref["spk0.idx"]) > 1000
+    scenarios.compare(ref, gpu)
+
+
+@pytest.mark.gpu
+def test_generated_exponential_euler_close(oracle_table, gpu_table):
+    """Exponential Euler calls exp (CUDA's against the C library's): the
+    first 300 steps agree in spikes and to 1e-12 in states."""
+    ref, gpu = _both(scenarios.coba, oracle_table, implicit=True, steps=300)
+    assert len(ref["spk0.idx"]) > 100
+    for k in ("spk0.idx", "spk0.steps"):
+        assert np.array_equal(ref[k], gpu[k])
+    for k in ("g0.v", "g0.ge", "g0.gi"):
+        assert np.allclose(ref[k], gpu[k], rtol=1e-12, atol=1e-15)
