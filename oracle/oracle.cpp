@@ -253,6 +253,8 @@ int or_group_set_model(or_net *n, int32_t gid, const or_model *m) {
     const std::string cmd = "gcc -O2 -ffp-contract=off -fno-fast-math -shared -fPIC -w -o '" + stem + ".so' '" + stem + ".c' -lm";
     if (std::system(cmd.c_str()) != 0) return fail(OR_ESTATE, "gcc failed on the generated model: " + stem + ".c");
     void *h = dlopen((stem + ".so").c_str(), RTLD_NOW | RTLD_LOCAL);
+    std::remove((stem + ".c").c_str());     /* the loaded image stays mapped */
+    std::remove((stem + ".so").c_str());
     if (!h) return fail(OR_ESTATE, std::string("dlopen: ") + dlerror());
     if (!upd.empty()) { g.gen_update = (void (*)(double *, int64_t, int64_t, double))dlsym(h, "gm_update"); g.linear = false; }
     if (!thr.empty()) g.gen_threshold = (int (*)(const double *, int64_t, int64_t, double))dlsym(h, "gm_threshold");

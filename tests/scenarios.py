@@ -162,6 +162,56 @@ def coba(N=2000, steps=2000, seed=7, method=None, implicit=False, order=1, strin
     return _result(net, groups=[P], spikemons=[M], statemons=[S])
 
 
+def cobahh(steps=10000):
+    """The reference's COBAHH regression (dev/tests/correctness/
+    test_optimizations.py:58-128): 4000 Hodgkin-Huxley neurons, exponential
+    Euler (implicit=True), EmpiricalThreshold(-20 mV, 3 ms), the fixed 0/1
+    excitatory/inhibitory matrices of tests/golden/cobahh.npz, deterministic
+    initial state; returns the spike monitor's (steps, indices)."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "cobahh.npz"))
+    nS, msiemens, ufarad, umetre, cm, siemens = 1e-9, 1e-3, 1e-6, 1e-6, 1e-2, 1.0
+    area = 20000 * umetre ** 2
+    Cm = (1 * ufarad * cm ** -2) * area
+    gl = (5e-5 * siemens * cm ** -2) * area
+    El, EK, ENa = -60 * mV, -90 * mV, 50 * mV
+    g_na = (100 * msiemens * cm ** -2) * area
+    g_kd = (30 * msiemens * cm ** -2) * area
+    VT = -63 * mV
+    taue, taui = 5 * ms, 10 * ms
+    Ee, Ei = 0 * mV, -80 * mV
+    eqs = b.Equations("""
+    dv/dt = (gl*(El-v)+ge*(Ee-v)+gi*(Ei-v)-g_na*(m*m*m)*h*(v-ENa)-g_kd*(n*n*n*n)*(v-EK))/Cm : volt
+    dm/dt = alpham*(1-m)-betam*m : 1
+    dn/dt = alphan*(1-n)-betan*n : 1
+    dh/dt = alphah*(1-h)-betah*h : 1
+    dge/dt = -ge*(1./taue) : siemens
+    dgi/dt = -gi*(1./taui) : siemens
+    alpham = 0.32*(mV**-1)*(13*mV-v+VT)/(exp((13*mV-v+VT)/(4*mV))-1.)/ms : Hz
+    betam = 0.28*(mV**-1)*(v-VT-40*mV)/(exp((v-VT-40*mV)/(5*mV))-1)/ms : Hz
+    alphah = 0.128*exp((17*mV-v+VT)/(18*mV))/ms : Hz
+    betah = 4./(1+exp((40*mV-v+VT)/(5*mV)))/ms : Hz
+    alphan = 0.032*(mV**-1)*(15*mV-v+VT)/(exp((15*mV-v+VT)/(5*mV))-1.)/ms : Hz
+    betan = .5*exp((10*mV-v+VT)/(40*mV))/ms : Hz
+    """, gl=gl, El=El, Ee=Ee, Ei=Ei, g_na=g_na, ENa=ENa, g_kd=g_kd, EK=EK, Cm=Cm, VT=VT, taue=taue, taui=taui)
+    P = b.NeuronGroup(4000, model=eqs, threshold=b.EmpiricalThreshold(threshold=-20 * mV, refractory=3 * ms),
+                      implicit=True, freeze=True)
+    Pe, Pi = P.subgroup(3200), P.subgroup(800)
+    Ce = b.Connection(Pe, P, "ge")
+    Ce.connect_csr(g["ce_rowptr"], g["ce_cols"].astype(np.int32), 6 * nS)
+    Ci = b.Connection(Pi, P, "gi")
+    Ci.connect_csr(g["ci_rowptr"], g["ci_cols"].astype(np.int32), 67 * nS)
+    x = np.arange(4000, dtype=float) / 4000
+    P.v = El + ((x - 0.5) * 20 - 5) * mV
+    P.ge = ((x - 0.5) * 6 + 4) * 10. * nS
+    P.gi = ((x - 0.5) * 48 + 20) * 10. * nS
+    M = b.SpikeMonitor(P)
+    net = b.Network(P, Ce, Ci, M)
+    net.run(steps * 0.1 * ms)
+    s, i = M._record()
+    return {"steps": s.copy(), "idx": i.copy(), "golden_steps": g["spk_step"], "golden_idx": g["spk_i"]}
+
+
 def stdp(Nin=400, Nout=32, steps=3000, seed=5, dense=True, rate_lo=5.0, rate_hi=25.0, wdtype=np.float32):
     """Config 3 in miniature: Poisson inputs -> LIF outputs, all-to-all,
     ExponentialSTDP (examples/plasticity/STDP1.py)."""
