@@ -155,18 +155,65 @@ __global__ void k_to_bf16(const float *W, int rows, int cols, bf16 *Wb, bf16 *Wb
     if (WbT) WbT[(int64_t)c * rows + r] = h;
 }
 
-template <int NT, int EPI>
-int launch_gemm(const umma::GemmArgs &g, int splits, cudaStream_t st) {
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no
+// link against the driver library); null when unavailable.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+        cudaGetLastError();
+    }
+    return fn;
+}
+
+// 2-D map of a row-major bf16 matrix [rows][ld] over its first `cols`
+// columns, boxes of 8 columns x box_rows rows, zero fill past the edges.
+bool tile_map(CUtensorMap *m, const bf16 *base, int rows, int cols, int ld, int box_rows) {
+    EncodeTiledFn f = encode_tiled();
+    if (!f || ((uintptr_t)base & 15) || ((size_t)ld * 2) % 16 || cols % 8) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+    const cuuint32_t box[2] = {8, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return f(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void *)base, dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int NT, int EPI, bool TMA>
+int launch_gemm_as(const umma::GemmArgs &g, int splits, cudaStream_t st, const CUtensorMap &ta,
+                   const CUtensorMap &tb) {
     static bool attr_set = false;
     constexpr size_t smem = umma::smem_bytes<NT>();
     if (!attr_set) {
-        MCK(cudaFuncSetAttribute(umma::k_gemm<NT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        MCK(cudaFuncSetAttribute(umma::k_gemm<NT, EPI, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr_set = true;
     }
     dim3 grid((unsigned)((g.M + umma::kM - 1) / umma::kM), (unsigned)((g.N + NT - 1) / NT), (unsigned)splits);
-    umma::k_gemm<NT, EPI><<<grid, umma::kThreads, smem, st>>>(g);
+    umma::k_gemm<NT, EPI, TMA><<<grid, umma::kThreads, smem, st>>>(g, ta, tb);
     MCK(cudaGetLastError());
     return BG_OK;
+}
+
+// TMA-fed stages when both operands allow a tensor map (16-byte aligned
+// rows, K a multiple of 8), else cp.async.
+template <int NT, int EPI>
+int launch_gemm(const umma::GemmArgs &g, int splits, cudaStream_t st) {
+    CUtensorMap ta, tb;
+    memset(&ta, 0, sizeof ta);
+    memset(&tb, 0, sizeof tb);
+    if (tile_map(&ta, g.A, g.M, g.K, g.lda, umma::kM) && tile_map(&tb, g.B, g.N, g.K, g.ldb, NT))
+        return launch_gemm_as<NT, EPI, true>(g, splits, st, ta, tb);
+    return launch_gemm_as<NT, EPI, false>(g, splits, st, ta, tb);
 }
 
 umma::GemmArgs gemm_args(const bf16 *A, int lda, const bf16 *B, int ldb, int M, int N, int K, int *err) {

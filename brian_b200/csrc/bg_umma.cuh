@@ -21,10 +21,23 @@
 // way.  Transposed copies are written from registers (32 consecutive rows
 // of one column per warp store).
 //
+// With TMA (template flag, when the operands' rows are 16-byte aligned) the
+// stages are filled by cp.async.bulk.tensor from 2-D tensor maps (K inner,
+// rows outer) in boxes of 8 K-elements x all tile rows: each box lands as
+// one 16-byte K-slab of every row, so core matrices are 128 bytes apart
+// along M (stride byte offset) and one slab (rows x 16 bytes) apart along K
+// (leading byte offset).  Thread 0 alone runs the pipeline: it arms a
+// stage's full mbarrier with the expected bytes, issues the 16 boxes, and,
+// kStages-1 chunks later, waits for the stage, issues its MMAs and commits
+// them to the stage's empty mbarrier, which the next fill of the stage waits
+// for -- no block-wide barrier inside the K loop.  No multicast.
+//
 // Every wait on an mbarrier is bounded; a wait that gives up records an
-// error code and the CTA leaves after releasing its TMEM.
+// error code and the CTA leaves after its copies in flight have landed and
+// its TMEM is released.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cstdint>
 
@@ -70,13 +83,25 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo = kLBO, uint32_t sbo = kSBO) {
     uint64_t d = 0;
     d |= (uint64_t)((addr >> 4) & 0x3FFFu);
-    d |= (uint64_t)((kLBO >> 4) & 0x3FFFu) << 16;
-    d |= (uint64_t)((kSBO >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
     d |= (uint64_t)1 << 46;   // sm100 descriptor version; base offset 0, no swizzle
     return d;
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// One 2-D box of a tensor map into shared memory, completing on `bar`.
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
 }
 
 // kind::f16 instruction descriptor: D f32, A bf16, B bf16, both K-major.
@@ -146,7 +171,9 @@ template <int NT>
 struct Smem {
     alignas(1024) unsigned char a[kStages][kM * kKc * 2];
     alignas(1024) unsigned char b[kStages][NT * kKc * 2];
-    alignas(8) unsigned long long bar[kStages];
+    alignas(8) unsigned long long bar[kStages];   // stage consumed (MMAs committed)
+    alignas(8) unsigned long long full[kStages];  // stage filled (TMA path)
+    alignas(8) unsigned long long done;           // every MMA finished (TMA path)
     float bias[NT];
     uint32_t tmem_base;
     int failed;
@@ -176,8 +203,9 @@ __device__ __forceinline__ void load_stage(Smem<NT> &sm, int st, const GemmArgs 
     }
 }
 
-template <int NT, int EPI>
-__global__ void __launch_bounds__(kThreads, 1) k_gemm(const GemmArgs g) {
+template <int NT, int EPI, bool TMA>
+__global__ void __launch_bounds__(kThreads, 1) k_gemm(const GemmArgs g, const __grid_constant__ CUtensorMap ta,
+                                                      const __grid_constant__ CUtensorMap tb) {
     extern __shared__ unsigned char smem_raw[];
     Smem<NT> &sm = *reinterpret_cast<Smem<NT> *>(
         (void *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023));
@@ -191,7 +219,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(const GemmArgs g) {
     if ((EPI == EPI_RELU_BF16 || EPI == EPI_BIAS_F32) && tid < NT)
         sm.bias[tid] = (n0 + tid < g.N) ? g.bias[n0 + tid] : 0.f;
     if (tid == 0) {
-        for (int s = 0; s < kStages; ++s) mbar_init(smem_u32(&sm.bar[s]), 1);
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(smem_u32(&sm.bar[s]), 1);
+            mbar_init(smem_u32(&sm.full[s]), 1);
+        }
+        mbar_init(smem_u32(&sm.done), 1);
         sm.failed = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
@@ -207,47 +239,97 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(const GemmArgs g) {
     const uint32_t tmem = sm.tmem_base;
     constexpr uint32_t idesc = idesc_bf16(kM, NT);
 
-    // prologue: chunks 0 .. kStages-2
-#pragma unroll
-    for (int s = 0; s < kStages - 1; ++s) {
-        if (s < nk) load_stage(sm, s, g, m0, n0, kbeg + s * kKc);
-        cp_async_commit();
-    }
-    bool ok = true;
-    for (int c = 0; c < nk; ++c) {
-        const int lc = c + kStages - 1;
-        if (lc < nk) {
-            const int st = lc % kStages;
-            if (lc >= kStages) {
-                // the MMAs of chunk lc - kStages read this stage
-                if (!mbar_wait(smem_u32(&sm.bar[st]), (uint32_t)(((lc - kStages) / kStages) & 1))) ok = false;
-            }
-            load_stage(sm, st, g, m0, n0, kbeg + lc * kKc);
-        }
-        cp_async_commit();
-        cp_async_wait<kStages - 1>();
-        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-        if (!ok) atomicExch(&sm.failed, 1);
-        __syncthreads();
-        if (sm.failed) break;
+    if constexpr (TMA) {
         if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-            const int st = c % kStages;
-            const uint32_t a_addr = smem_u32(sm.a[st]), b_addr = smem_u32(sm.b[st]);
+            constexpr uint32_t kLboA = kM * 16, kLboB = NT * 16;     // one 16-byte K-slab of all rows
+            constexpr uint32_t kBytes = (kM + NT) * kKc * 2;
+            bool ok = true;
+            int issued = 0, consumed = 0;
+            for (int c = 0; c < nk + kStages - 1 && ok; ++c) {
+                if (c < nk) {
+                    const int st = c % kStages;
+                    // the MMAs of chunk c - kStages read this stage
+                    if (c >= kStages && !mbar_wait(smem_u32(&sm.bar[st]), (uint32_t)(((c / kStages) - 1) & 1))) {
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t fb = smem_u32(&sm.full[st]);
+                    mbar_expect_tx(fb, kBytes);
+                    const uint32_t a_addr = smem_u32(sm.a[st]), b_addr = smem_u32(sm.b[st]);
+                    const int kx = kbeg + c * kKc;
 #pragma unroll
-            for (int j = 0; j < kKc / 16; ++j)
-                umma_bf16(tmem, smem_desc(a_addr + j * 2 * kLBO), smem_desc(b_addr + j * 2 * kLBO), idesc,
-                          (c > 0 || j > 0) ? 1u : 0u);
-            umma_commit(smem_u32(&sm.bar[st]));
+                    for (int q = 0; q < kKc / 8; ++q) {
+                        tma_load_2d(a_addr + q * kLboA, &ta, kx + q * 8, m0, fb);
+                        tma_load_2d(b_addr + q * kLboB, &tb, kx + q * 8, n0, fb);
+                    }
+                    issued = c + 1;
+                }
+                const int cc = c - (kStages - 1);
+                if (cc >= 0) {
+                    const int st = cc % kStages;
+                    if (!mbar_wait(smem_u32(&sm.full[st]), (uint32_t)((cc / kStages) & 1))) { ok = false; break; }
+                    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                    const uint32_t a_addr = smem_u32(sm.a[st]), b_addr = smem_u32(sm.b[st]);
+#pragma unroll
+                    for (int j = 0; j < kKc / 16; ++j)
+                        umma_bf16(tmem, smem_desc(a_addr + j * 2 * kLboA, kLboA, 128),
+                                  smem_desc(b_addr + j * 2 * kLboB, kLboB, 128), idesc, (cc > 0 || j > 0) ? 1u : 0u);
+                    umma_commit(smem_u32(&sm.bar[st]));
+                    consumed = cc + 1;
+                }
+            }
+            if (!ok) {
+                // let the boxes in flight land before the CTA leaves
+                for (int c = consumed; c < issued; ++c) mbar_wait(smem_u32(&sm.full[c % kStages]), (uint32_t)((c / kStages) & 1));
+                sm.failed = 1;
+            }
+            umma_commit(smem_u32(&sm.done));     // arrives once every MMA issued above has finished
         }
+        if (!mbar_wait(smem_u32(&sm.done), 0u)) atomicExch(&sm.failed, 1);
+        __syncthreads();
+    } else {
+        // prologue: chunks 0 .. kStages-2
+#pragma unroll
+        for (int s = 0; s < kStages - 1; ++s) {
+            if (s < nk) load_stage(sm, s, g, m0, n0, kbeg + s * kKc);
+            cp_async_commit();
+        }
+        bool ok = true;
+        for (int c = 0; c < nk; ++c) {
+            const int lc = c + kStages - 1;
+            if (lc < nk) {
+                const int st = lc % kStages;
+                if (lc >= kStages) {
+                    // the MMAs of chunk lc - kStages read this stage
+                    if (!mbar_wait(smem_u32(&sm.bar[st]), (uint32_t)(((lc - kStages) / kStages) & 1))) ok = false;
+                }
+                load_stage(sm, st, g, m0, n0, kbeg + lc * kKc);
+            }
+            cp_async_commit();
+            cp_async_wait<kStages - 1>();
+            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+            if (!ok) atomicExch(&sm.failed, 1);
+            __syncthreads();
+            if (sm.failed) break;
+            if (tid == 0) {
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                const int st = c % kStages;
+                const uint32_t a_addr = smem_u32(sm.a[st]), b_addr = smem_u32(sm.b[st]);
+#pragma unroll
+                for (int j = 0; j < kKc / 16; ++j)
+                    umma_bf16(tmem, smem_desc(a_addr + j * 2 * kLBO), smem_desc(b_addr + j * 2 * kLBO), idesc,
+                              (c > 0 || j > 0) ? 1u : 0u);
+                umma_commit(smem_u32(&sm.bar[st]));
+            }
+        }
+        // all MMAs done: the last commit covers every earlier one
+        if (!sm.failed && nk > 0) {
+            const int st = (nk - 1) % kStages;
+            if (!mbar_wait(smem_u32(&sm.bar[st]), (uint32_t)(((nk - 1) / kStages) & 1))) atomicExch(&sm.failed, 1);
+        }
+        cp_async_wait<0>();
+        __syncthreads();
     }
-    // all MMAs done: the last commit covers every earlier one
-    if (!sm.failed && nk > 0) {
-        const int st = (nk - 1) % kStages;
-        if (!mbar_wait(smem_u32(&sm.bar[st]), (uint32_t)(((nk - 1) / kStages) & 1))) atomicExch(&sm.failed, 1);
-    }
-    cp_async_wait<0>();
-    __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     if (sm.failed) {
         if (tid == 0 && g.err) atomicExch(g.err, 1);
