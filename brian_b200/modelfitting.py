@@ -50,11 +50,13 @@ class PSO(object):
 
 
 class GA(object):
-    pass
+    """Genetic algorithm of the external playdoh package: not built."""
 
 
 class CMAES(object):
-    pass
+    """Covariance matrix adaptation evolution strategy (brian_b200/cmaes.py);
+    optparams ``sigma0`` (initial step in the [-1, 1]-scaled space)."""
+    defaults = {"sigma0": 0.5}
 
 
 _PRECISION = {"double": 64, "float": 32, 64: 64, 32: 32}
@@ -357,7 +359,7 @@ def _bounds(params):
 def modelfitting(model=None, reset=None, threshold=None, refractory=0.0, data=None, input_var="I", input=None,
                  dt=None, popsize=1000, maxiter=10, delta=4e-3, slices=1, overlap=0.0, initial_values=None,
                  stepsize=0.1, unit_type=None, total_units=None, cpu=None, gpu=None, precision="double",
-                 machines=(), allocation=None, returninfo=False, scaling=None, algorithm=PSO, optparams=None,
+                 machines=(), allocation=None, returninfo=False, scaling=None, algorithm=CMAES, optparams=None,
                  method="Euler", seed=None, evaluate_initial=True, initial_positions=None, device=0, **params):
     """Fit a spiking neuron model to target spike trains (modelfitting.py:232-518).
 
@@ -365,8 +367,10 @@ def modelfitting(model=None, reset=None, threshold=None, refractory=0.0, data=No
     input trace shared by all targets, or a list with one trace per target
     (own durations).  ``params``: ``name=[min, max]`` or ``name=[bound_min,
     min, max, bound_max]``; ``delays`` and a list-valued ``refractory`` fit
-    the spike delay and refractory period.  ``popsize`` particles per target
-    and ``maxiter`` swarm iterations, all on the GPU.
+    the spike delay and refractory period.  ``popsize`` candidates per target
+    and ``maxiter`` iterations of ``algorithm``: CMAES (the default, as in the
+    reference; one search per target, generations evaluated on the GPU) or
+    PSO (the whole swarm on the GPU).
 
     ``initial_positions`` ([ndim][groups*popsize], optional) replaces the
     uniform initial draw, e.g. with proposals of a learned model;
@@ -377,9 +381,9 @@ def modelfitting(model=None, reset=None, threshold=None, refractory=0.0, data=No
         raise ValueError("model, data and input are required")
     if dt is None:
         raise Exception("dt (sampling frequency of the input) must be set")
-    if algorithm is not PSO:
-        raise NotImplementedError("only the particle swarm optimiser (algorithm=PSO) is built; CMA-ES and GA "
-                                  "come from the external playdoh package")
+    if algorithm not in (PSO, CMAES):
+        raise NotImplementedError("the genetic algorithm (GA) of the external playdoh package is not built; "
+                                  "use algorithm=CMAES (the default) or PSO")
     if isinstance(model, str):
         model = Equations(model, level=1)
     trains = _split_data(data)
@@ -403,6 +407,9 @@ def modelfitting(model=None, reset=None, threshold=None, refractory=0.0, data=No
                           input_var=input_var, device=device, slices=slices, overlap=overlap)
     M = prob.N
     rng = np.random.default_rng(seed)
+    if algorithm is CMAES:
+        return _fit_cmaes(prob, names, lo, hi, imin, imax, groups, popsize, maxiter, rng, optparams,
+                          initial_positions)
     if initial_positions is None:
         X0 = imin.reshape(-1, 1) + (imax - imin).reshape(-1, 1) * rng.random((len(names), M))
     else:
@@ -422,6 +429,50 @@ def modelfitting(model=None, reset=None, threshold=None, refractory=0.0, data=No
     if groups == 1:
         return OptimizationResult(best_pos[0], float(fg[0]), info)
     return OptimizationResult(best_pos, list(map(float, fg)), info)
+
+
+def _fit_cmaes(prob, names, lo, hi, imin, imax, groups, popsize, maxiter, rng, optparams, initial_positions):
+    """CMA-ES per target group with mapminmax scaling (modelfitting.py:442-443):
+    every generation's candidates of all groups in one device evaluation."""
+    from .cmaes import CMAState
+    opt = dict(CMAES.defaults)
+    opt.update(optparams or {})
+    n = len(names)
+    span = (imax - imin)
+    span = np.where(span > 0, span, 1.0)
+
+    def to_params(xs):                       # scaled [-1, 1] -> parameter space
+        return imin + (xs + 1.0) * 0.5 * span
+
+    if initial_positions is None:
+        mean = np.zeros((groups, n))
+    else:
+        X0 = np.asarray(initial_positions, dtype=np.float64).reshape(n, groups, popsize)
+        mean = ((X0.mean(axis=2).T - imin) / (0.5 * span)) - 1.0
+    st = CMAState(groups, n, popsize, mean, opt["sigma0"], rng)
+    best_x = np.zeros((groups, n))
+    best_f = np.full(groups, -np.inf)
+    trace = np.zeros((int(maxiter), groups))
+    ms = np.zeros(int(maxiter))
+    for it in range(int(maxiter)):
+        xs, y = st.ask()
+        P = np.clip(to_params(xs), lo, hi)                  # [G][lam][n]
+        X = np.ascontiguousarray(P.transpose(2, 0, 1).reshape(n, groups * popsize))
+        f = prob.evaluate(X).reshape(groups, popsize)
+        ms[it] = prob.handle.stats()["last_eval_ms"]
+        fv = np.where(np.isnan(f), -np.inf, f)
+        k = np.argmax(fv, axis=1)
+        better = fv[np.arange(groups), k] > best_f
+        best_f = np.where(better, fv[np.arange(groups), k], best_f)
+        best_x[better] = P[np.arange(groups), k][better]
+        trace[it] = best_f
+        st.tell(y, f)
+    best_pos = [{k_: float(best_x[j, d]) for d, k_ in enumerate(names)} for j in range(groups)]
+    info = {"trace": trace, "iteration_ms": ms, "neuron_steps_per_iteration": prob.neuron_steps(),
+            "groups": groups, "popsize": popsize, "algorithm": "CMAES"}
+    if groups == 1:
+        return OptimizationResult(best_pos[0], float(best_f[0]), info)
+    return OptimizationResult(best_pos, list(map(float, best_f)), info)
 
 
 def get_spikes(model=None, reset=None, threshold=None, input=None, input_var="I", dt=None, initial_values=None,

@@ -183,11 +183,13 @@ def test_device_swarm_matches_oracle():
     assert ms.shape == (4,) and np.all(ms > 0)
 
 
-@pytest.mark.parametrize("slices,overlap", [(1, 0.0), (4, 0.05)])
-def test_modelfitting_recovers_targets(slices, overlap):
+@pytest.mark.parametrize("slices,overlap,algorithm", [(1, 0.0, None), (4, 0.05, None), (1, 0.0, "PSO")])
+def test_modelfitting_recovers_targets(slices, overlap, algorithm):
     """End to end through modelfitting(): 4 targets with their own OU inputs
-    and lengths; the swarm finds parameter sets with high gamma (also with
-    each input cut into 4 time slices simulated side by side)."""
+    and lengths; CMA-ES (the default, as in the reference) and the particle
+    swarm find parameter sets with high gamma (also with each input cut into
+    4 time slices simulated side by side)."""
+    from brian_b200.modelfitting import PSO, CMAES
     from brian_b200.synthetic import FitWorkload
     w = FitWorkload(ntargets=4, dur_min=2.0, dur_max=3.0, seed=5)
     w.build_targets()
@@ -196,7 +198,8 @@ def test_modelfitting_recovers_targets(slices, overlap):
     pr = {k: [v[0], v[0], v[1], v[1]] for k, v in pr.items()}
     res = modelfitting(model=_eqs(), reset=RESET, threshold=THRESHOLD, data=w.data(), input=w.inputs, dt=DT,
                        popsize=512, maxiter=25, delta=4e-3, precision="float", seed=3, slices=slices,
-                       overlap=overlap, **pr)
+                       overlap=overlap, algorithm=PSO if algorithm == "PSO" else CMAES, **pr)
+    assert res.info.get("algorithm", "PSO") == (algorithm or "CMAES")
     assert len(res.best_fit) == 4
     assert np.min(res.best_fit) > 0.5
     assert res.info["trace"].shape == (25, 4)
