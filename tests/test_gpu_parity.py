@@ -174,3 +174,42 @@ def test_generated_exponential_euler_close(oracle_table, gpu_table):
         assert np.array_equal(ref[k], gpu[k])
     for k in ("g0.v", "g0.ge", "g0.gi"):
         assert np.allclose(ref[k], gpu[k], rtol=1e-12, atol=1e-15)
+
+
+def _fp32_and_oracle(fn, oracle_table, **kw):
+    """fn on the FP64 oracle and on the GPU engine at precision 32."""
+    b.clear(); b.reinit_default_clock(); np.random.seed(1234)
+    with engine(oracle_table):
+        ref = fn(**kw)
+    prev = b.get_global_preference("precision")
+    b.set_global_preferences(precision=32)
+    try:
+        b.clear(); b.reinit_default_clock(); np.random.seed(1234)
+        gpu = fn(**kw)
+    finally:
+        b.set_global_preferences(precision=prev)
+    return ref, gpu
+
+
+def _spike_total(r):
+    return int(r["spikes"][0]) if "spikes" in r else len(r["spk0.idx"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["cuba", "persistent", "generated"])
+def test_fp32_network_close_to_fp64_oracle(oracle_table, gpu_table, case):
+    """The FP32 engine (state and ring values in float) against the FP64
+    oracle: states after 20 steps agree to float precision, and over 2000
+    steps the spike counts stay within 3 %."""
+    fn, kw = {"cuba": (scenarios.cuba, dict(N=4000)),
+              "persistent": (scenarios.cuba_delay, dict(monitors=False, N=6000)),
+              "generated": (scenarios.coba, dict())}[case]
+    ref, gpu = _fp32_and_oracle(fn, oracle_table, steps=20, **kw)
+    for k in ref:
+        if k.startswith("g0."):
+            scale = max(1e-3, float(np.max(np.abs(ref[k]))))
+            assert np.max(np.abs(np.asarray(gpu[k], dtype=np.float64) - ref[k])) <= 1e-4 * scale, k
+    ref, gpu = _fp32_and_oracle(fn, oracle_table, steps=2000, **kw)
+    n_ref, n_gpu = _spike_total(ref), _spike_total(gpu)
+    assert n_ref > 500
+    assert abs(n_gpu - n_ref) <= 0.03 * n_ref, (n_gpu, n_ref)
