@@ -71,9 +71,8 @@ template <typename T> struct NoInitAlloc : std::allocator<T> {
 template <typename T> using hvec = std::vector<T, NoInitAlloc<T>>;
 
 // f(lo, hi, t) over [0, n) split into contiguous parts, one per host thread
-// (at most 32, at least 4M items each); t is the part's index.
-template <typename F> void parallel_for(int64_t n, F f) {
-    const int64_t grain = (int64_t)1 << 22;
+// (at most 32, at least `grain` items each); t is the part's index.
+template <typename F> void parallel_for(int64_t n, F f, int64_t grain = (int64_t)1 << 22) {
     int nt = (int)std::min<int64_t>(std::min<unsigned>(32u, std::max(1u, std::thread::hardware_concurrency())),
                                     (n + grain - 1) / grain);
     if (nt <= 1) { f((int64_t)0, n, 0); return; }
@@ -82,8 +81,7 @@ template <typename F> void parallel_for(int64_t n, F f) {
     for (int t = 0; t < nt; ++t) th.emplace_back([&f, n, nt, t] { f(n * t / nt, n * (t + 1) / nt, t); });
     for (auto &x : th) x.join();
 }
-static int parallel_parts(int64_t n) {
-    const int64_t grain = (int64_t)1 << 22;
+static int parallel_parts(int64_t n, int64_t grain = (int64_t)1 << 22) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(std::min<unsigned>(32u, std::max(1u, std::thread::hardware_concurrency())),
                                                        (n + grain - 1) / grain));
 }
@@ -147,6 +145,9 @@ struct bg_net {
     int allow_persist = 1;
     int persist_th = 0;                 // forced threads per block of the persistent kernel (0: automatic)
     int persist_used = 0;               // threads per block of the built persistent kernel (0: none)
+    void *stage[2] = {nullptr, nullptr};                 // pinned staging of large uploads (prepare only)
+    cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+    bool stage_used[2] = {false, false};
     uint32_t *dMonWords = nullptr;      // persistent path with spike monitors: spike words per step of a chunk
     long long *dMonOff = nullptr;       //   and per-step record offsets
     cudaStream_t stream = nullptr;
@@ -482,9 +483,50 @@ int build_decay(bg_net *net, int sid) {
     return BG_OK;
 }
 
+// Host-to-device copy.  Large arrays (the connectivity) go through two
+// pinned staging buffers: all host threads copy one chunk in while the DMA
+// of the previous chunk runs (a pageable copy is staged by the driver one
+// thread at a time).  The buffers live until the end of bg_net_prepare.
+constexpr size_t kStageBytes = (size_t)64 << 20;
+
 int upload(bg_net *net, void *dst, const void *src, size_t bytes) {
-    BG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, net->stream));
+    if (bytes < 2 * kStageBytes || net->prepared) {
+        BG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, net->stream));
+        return BG_OK;
+    }
+    if (!net->stage[0]) {
+        for (int b = 0; b < 2; ++b) {
+            if (cudaHostAlloc(&net->stage[b], kStageBytes, cudaHostAllocDefault) != cudaSuccess ||
+                cudaEventCreateWithFlags(&net->stage_ev[b], cudaEventDisableTiming) != cudaSuccess) {
+                cudaGetLastError();
+                BG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, net->stream));
+                return BG_OK;
+            }
+        }
+        net->stage_used[0] = net->stage_used[1] = false;
+    }
+    size_t k = 0;
+    for (size_t off = 0; off < bytes; off += kStageBytes, ++k) {
+        const int b = (int)(k & 1);
+        const size_t len = std::min(kStageBytes, bytes - off);
+        if (net->stage_used[b]) BG_CUDA(cudaEventSynchronize(net->stage_ev[b]));
+        char *stg = (char *)net->stage[b];
+        const char *s = (const char *)src + off;
+        parallel_for((int64_t)len, [&](int64_t lo, int64_t hi, int) { std::memcpy(stg + lo, s + lo, hi - lo); },
+                     (int64_t)4 << 20);
+        BG_CUDA(cudaMemcpyAsync((char *)dst + off, stg, len, cudaMemcpyHostToDevice, net->stream));
+        BG_CUDA(cudaEventRecord(net->stage_ev[b], net->stream));
+        net->stage_used[b] = true;
+    }
     return BG_OK;
+}
+
+void release_staging(bg_net *net) {
+    for (int b = 0; b < 2; ++b) {
+        if (net->stage_ev[b]) { cudaEventSynchronize(net->stage_ev[b]); cudaEventDestroy(net->stage_ev[b]); }
+        if (net->stage[b]) cudaFreeHost(net->stage[b]);
+        net->stage[b] = nullptr; net->stage_ev[b] = nullptr; net->stage_used[b] = false;
+    }
 }
 
 int upload_state(bg_net *net, HGroup &g, int var, const double *in) {
@@ -806,6 +848,7 @@ int bg_net_destroy(bg_net *n) {
     if (!n) return BG_OK;
     cudaSetDevice(n->device);
     if (n->stream) cudaStreamSynchronize(n->stream);
+    release_staging(n);
     if (n->gexec) cudaGraphExecDestroy(n->gexec);
     for (auto &g : n->groups)
         if (g.gen_lib) cudaLibraryUnload(g.gen_lib);
@@ -947,8 +990,10 @@ static int conn_add_impl(bg_net *n, int32_t src, int64_t so, int64_t sn, int32_t
     for (int64_t i = 0; i < sn; ++i)
         if (rowptr[i + 1] < rowptr[i]) return fail(BG_EINVAL, "rowptr not monotone");
     {
-        // rows in parallel; the first bad row (lowest index) decides the message
-        const int parts = parallel_parts(sn);
+        // rows in parallel (about 4M synapses per part); the first bad row
+        // (lowest index) decides the message
+        const int64_t row_grain = std::max<int64_t>(1, ((int64_t)1 << 22) / std::max<int64_t>(1, nnz / std::max<int64_t>(1, sn)));
+        const int parts = parallel_parts(sn, row_grain);
         std::vector<int64_t> bad_row(parts, sn);
         std::vector<int> bad_kind(parts, 0);
         parallel_for(sn, [&](int64_t lo, int64_t hi, int t) {
@@ -957,7 +1002,7 @@ static int conn_add_impl(bg_net *n, int32_t src, int64_t so, int64_t sn, int32_t
                     const int kind = (cols[k] < 0 || cols[k] >= tn) ? 1 : (k > rowptr[i] && cols[k] <= cols[k - 1]) ? 2 : 0;
                     if (kind) { bad_row[t] = i; bad_kind[t] = kind; return; }
                 }
-        });
+        }, row_grain);
         int64_t r = sn; int kind = 0;
         for (int t = 0; t < parts; ++t) if (bad_row[t] < r) { r = bad_row[t]; kind = bad_kind[t]; }
         if (kind == 1) return fail(BG_EINVAL, "column index out of range");
@@ -1217,7 +1262,15 @@ int bg_monitor_clear(bg_net *n, int32_t mid) {
     return BG_OK;
 }
 
+static int prepare_impl(bg_net *n);
+
 int bg_net_prepare(bg_net *n) {
+    const int st = prepare_impl(n);
+    if (n) release_staging(n);
+    return st;
+}
+
+static int prepare_impl(bg_net *n) {
     if (!n) return fail(BG_EINVAL, "net");
     if (n->prepared) return BG_OK;
     BG_CUDA(cudaSetDevice(n->device));
