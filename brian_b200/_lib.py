@@ -38,6 +38,7 @@ SIGNATURES = {
     "conn_get_weights": [_vp, _i32, _vp],
     "conn_set_weights": [_vp, _i32, _vp],
     "stdp_add": [_vp, _i32, _vp, _dbl, _dbl, _dbl, _dbl, ct.c_int, _i32, _i32, _P(_i32)],
+    "stdp_add_delayed": [_vp, _i32, _vp, _dbl, _dbl, _dbl, _dbl, ct.c_int, _i32, _i32, _vp, _vp, _P(_i32)],
     "stdp_get_traces": [_vp, _i32, _vp, _vp],
     "spikemon_add": [_vp, _i32, _i64, _i64, _i32, _P(_i32)],
     "statemon_add": [_vp, _i32, ct.c_int, _i64, _vp, _i32, _P(_i32)],
@@ -275,6 +276,16 @@ class Runtime(object):
         sid = _i32()
         self._c(self.t.stdp_add(self.h, cid, _ptr(decay), float(Ap), float(Am), float(wmin), float(wmax),
                                 int(interactions), int(pre_delay), int(post_delay), ct.byref(sid)), "stdp_add")
+        return sid.value
+
+    def stdp_add_delayed(self, cid, decay, Ap, Am, wmin, wmax, interactions, pre_delay, hist_len, lag_pre, lag_post):
+        decay = np.ascontiguousarray(decay, dtype=np.float64)
+        lag_pre = np.ascontiguousarray(lag_pre, dtype=np.uint8)
+        lag_post = np.ascontiguousarray(lag_post, dtype=np.uint8)
+        sid = _i32()
+        self._c(self.t.stdp_add_delayed(self.h, cid, _ptr(decay), float(Ap), float(Am), float(wmin), float(wmax),
+                                        int(interactions), int(pre_delay), int(hist_len), _ptr(lag_pre),
+                                        _ptr(lag_post), ct.byref(sid)), "stdp_add_delayed")
         return sid.value
 
     def stdp_get_traces(self, sid, npre, npost):

@@ -489,6 +489,13 @@ class DelayConnection(Connection):
         if self.iscompressed:
             self._apply_delay_ops()
 
+    def connect(self, source=None, target=None, W=None, delay=None):
+        """Connection.connect, then the delays of the inserted block
+        (delayconnection.py:315-318)."""
+        Connection.connect(self, source=source, target=target, W=W)
+        if delay is not None:
+            self.set_delays(source, target, delay)
+
     def _after_connect(self, P, Q, rows, cols, kwds):
         d = kwds.get("delay")
         if d is not None:
@@ -535,6 +542,14 @@ class DelayConnection(Connection):
         if len(steps) and (steps.min() < 0 or steps.max() >= self._md):
             raise ValueError("synaptic delay beyond max_delay")
         return steps.astype(np.uint8)
+
+    def _delay_seconds(self):
+        """Per-synapse delays in seconds, CSR order (delays given in bins
+        count as bins * dt)."""
+        self.compress()
+        if getattr(self, "_dvals", None) is None:
+            return np.asarray(self._dsteps, dtype=np.float64) * float(self.target.clock.dt)
+        return np.asarray(self._dvals, dtype=np.float64)
 
     @property
     def delay(self):

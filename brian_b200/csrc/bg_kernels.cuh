@@ -678,11 +678,96 @@ __global__ void __launch_bounds__(kDenseThreads) k_prop_dense(const PropArgs<T> 
 }
 
 // STDP trace decay (the G_pre/G_post groups' 1x1 linear updaters).
-struct DecayArgs { double *A_pre; int64_t npre; double a_pre, c_pre; double *A_post; int64_t npost; double a_post, c_post; DevCtl *ctl; int last; };
+// On a DelayConnection the traces are also kept for `hlen` steps, as the
+// RecentStateMonitors recording them at the end of each step do
+// (monitor.py:1036-1049): the record of step s-1 is the trace before the
+// decay of step s, so this kernel writes it into slot (s-1) mod hlen first.
+struct DecayArgs {
+    double *A_pre; int64_t npre; double a_pre, c_pre; double *A_post; int64_t npost; double a_post, c_post;
+    double *H_pre, *H_post; int hlen;     // trace histories [hlen][n], or null
+    DevCtl *ctl; int last;
+};
 static __global__ void k_stdp_decay(const DecayArgs a) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < a.npre) a.A_pre[i] = __dadd_rn(__dmul_rn(a.a_pre, a.A_pre[i]), a.c_pre);
-    else if (i < a.npre + a.npost) { const int64_t j = i - a.npre; a.A_post[j] = __dadd_rn(__dmul_rn(a.a_post, a.A_post[j]), a.c_post); }
+    const long long nstep = a.ctl->nstep;
+    const bool rec = a.H_pre != nullptr && nstep > 0;
+    const int64_t slot = rec ? (int64_t)((nstep - 1) % a.hlen) : 0;
+    if (i < a.npre) {
+        const double x = a.A_pre[i];
+        if (rec) a.H_pre[slot * a.npre + i] = x;
+        a.A_pre[i] = __dadd_rn(__dmul_rn(a.a_pre, x), a.c_pre);
+    } else if (i < a.npre + a.npost) {
+        const int64_t j = i - a.npre;
+        const double x = a.A_post[j];
+        if (rec) a.H_post[slot * a.npost + j] = x;
+        a.A_post[j] = __dadd_rn(__dmul_rn(a.a_post, x), a.c_post);
+    }
+    bg_finish_step(a.ctl, a.last);
+}
+
+// Slot of the trace record `lag` records before the last one at step nstep
+// (monitor.py:1092: (current_time_index - 1 - lag) mod M, one record per
+// step; lag < hlen).
+__device__ __forceinline__ int64_t hist_slot(long long nstep, int lag, int hlen) {
+    return (int64_t)((nstep + hlen - 1 - lag) % hlen);
+}
+
+// Presynaptic rule on a DelayConnection (stdp.py:296-352): the immediate
+// part, A_pre[i] (+)= Ap for this step's spikes, and the delayed part for
+// the spikes of `delay` (the connection's max_delay) steps ago:
+// w[i,k] += A_post[cols[k]] as recorded lag[k] records back; clip.
+struct DelayedPreArgs {
+    DevCtl *ctl;
+    const uint32_t *hist; int depth; int64_t nwords; int delay;
+    int64_t so, sn, tn;
+    const int64_t *rowptr; const int32_t *cols; void *w;
+    double *A_pre; double Ap; int pre_set;
+    const double *H_post; int hlen; const uint8_t *lag;
+    double wmin, wmax;
+    int last;
+};
+template <typename WT>
+__global__ void __launch_bounds__(256) k_dstdp_pre(const DelayedPreArgs a) {
+    const long long nstep = a.ctl->nstep;
+    const int lane = threadIdx.x & 31;
+    const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+    const int64_t end = a.so + a.sn;
+    const int64_t w0 = a.so >> 5, w1 = (end + 31) >> 5;
+    {   // immediate: one thread per history word of this step
+        const uint32_t *H = a.hist + (int64_t)((int)(nstep % a.depth)) * a.nwords;
+        for (int64_t wi = w0 + gtid; wi < w1; wi += nthreads) {
+            uint32_t wd = masked_word(H, wi, a.so, end);
+            while (wd) {
+                const int b = __ffs(wd) - 1; wd &= wd - 1;
+                const int64_t i = (wi << 5) + b - a.so;
+                a.A_pre[i] = a.pre_set ? a.Ap : __dadd_rn(a.A_pre[i], a.Ap);
+            }
+        }
+    }
+    if (nstep >= a.delay) {   // delayed: one warp per spike, lanes over the row
+        const int64_t warp = gtid >> 5, nwarps = nthreads >> 5;
+        const uint32_t *H = a.hist + (int64_t)((int)((nstep - a.delay) % a.depth)) * a.nwords;
+        WT *W = (WT *)a.w;
+        for (int64_t wi0 = w0 + warp * 32; wi0 < w1; wi0 += nwarps * 32) {
+            const int64_t wi = wi0 + lane;
+            const uint32_t word = wi < w1 ? masked_word(H, wi, a.so, end) : 0u;
+            uint32_t nz = __ballot_sync(0xffffffffu, word != 0u);
+            while (nz) {
+                const int l = __ffs(nz) - 1; nz &= nz - 1;
+                uint32_t wd = __shfl_sync(0xffffffffu, word, l);
+                const int64_t base = (wi0 + l) << 5;
+                while (wd) {
+                    const int b = __ffs(wd) - 1; wd &= wd - 1;
+                    const int64_t i = base + b - a.so;
+                    for (int64_t k = a.rowptr[i] + lane; k < a.rowptr[i + 1]; k += 32) {
+                        const int64_t s = hist_slot(nstep, a.lag[k], a.hlen);
+                        stdp_w<double, WT>(W, k, a.H_post[s * a.tn + a.cols[k]], a.wmin, a.wmax);
+                    }
+                }
+            }
+        }
+    }
     bg_finish_step(a.ctl, a.last);
 }
 
@@ -733,6 +818,9 @@ struct PostArgs {
     void *w; int dense;
     const int64_t *colptr; const int64_t *colk; const int32_t *colsrc;
     double *A_post; const double *A_pre; double Am; int post_set; double wmin, wmax;
+    // DelayConnection (stdp.py:296-368): w[:,j] += A_pre as recorded lag[p]
+    // records back, lag in column order; null on a plain Connection
+    const double *H_pre; int hlen; const uint8_t *lagc;
     int last;
 };
 template <typename WT>
@@ -767,8 +855,11 @@ __global__ void __launch_bounds__(256) k_stdp_post(const PostArgs a) {
                         stdp_w<double, WT>(W, i * a.tn + j, a.A_pre[i], a.wmin, a.wmax);
                 } else {
                     for (int64_t p = a.colptr[j] + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < a.colptr[j + 1];
-                         p += (int64_t)gridDim.x * blockDim.x)
-                        stdp_w<double, WT>(W, a.colk[p], a.A_pre[a.colsrc[p]], a.wmin, a.wmax);
+                         p += (int64_t)gridDim.x * blockDim.x) {
+                        const double add = a.H_pre ? a.H_pre[hist_slot(nstep, a.lagc[p], a.hlen) * a.sn + a.colsrc[p]]
+                                                   : a.A_pre[a.colsrc[p]];
+                        stdp_w<double, WT>(W, a.colk[p], add, a.wmin, a.wmax);
+                    }
                 }
             }
             if (blockIdx.x == 0)

@@ -120,6 +120,9 @@ struct HConn {
 struct HStdp {
     int cid; double a_pre, c_pre, a_post, c_post, Ap, Am, wmin, wmax; int inter; int pre_delay, post_delay;
     double *dApre = nullptr, *dApost = nullptr; bool fused = false;
+    // DelayConnection: trace histories of hlen steps and per-synapse lags
+    bool delayed = false; int hlen = 0; std::vector<uint8_t> lag_pre, lag_post;
+    double *dHpre = nullptr, *dHpost = nullptr; uint8_t *dLagPre = nullptr, *dLagPostC = nullptr;
 };
 struct HSpikeMon {
     int gid; int64_t origin, n; int delay;
@@ -381,7 +384,8 @@ int build_conn(bg_net *net, int cid) {
     }
     if (c.fused_push) return BG_OK;   // pushed by the source group's head kernel
     int mode; int64_t grid;
-    const bool use_atomic = !c.dense && c.mod_var < 0 && (c.homogeneous || !net->deterministic) && !a.stdp;
+    // equal weights sum to the same value in any order; STDP makes them differ
+    const bool use_atomic = !c.dense && c.mod_var < 0 && ((c.homogeneous && c.stdp < 0) || !net->deterministic) && !a.stdp;
     if (c.dense) { mode = 4; grid = (c.tn + bg::kDenseThreads - 1) / bg::kDenseThreads; }
     else if (use_atomic) {
         mode = c.hetero ? 1 : 0;
@@ -403,9 +407,33 @@ int build_conn(bg_net *net, int cid) {
     return BG_OK;
 }
 
+int build_stdp_pre_delayed(bg_net *net, int sid) {
+    HStdp &s = net->stdps[sid];
+    HConn &c = net->conns[s.cid];
+    const HGroup &gs = net->groups[c.src];
+    bg::DelayedPreArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.ctl = net->dCtl; a.hist = gs.dHist; a.depth = gs.depth; a.nwords = gs.npad / 32; a.delay = s.pre_delay;
+    a.so = c.so; a.sn = c.sn; a.tn = c.tn; a.rowptr = c.dRow; a.cols = c.dCols; a.w = c.dW;
+    a.A_pre = s.dApre; a.Ap = s.Ap; a.pre_set = (s.inter == BG_STDP_NEAREST || s.inter == BG_STDP_NEAREST_PRE);
+    a.H_post = s.dHpost; a.hlen = s.hlen; a.lag = s.dLagPre; a.wmin = s.wmin; a.wmax = s.wmax;
+    const int64_t nwords = (c.so + c.sn + 31) / 32 - c.so / 32;
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((nwords + 255) / 256, (int64_t)sm_count() * 4));
+    const int wb = c.w_bits;
+    net->item_names.push_back("stdp_pre_delayed[s" + std::to_string(sid) + "]");
+    net->step_launches.push_back([a, grid, wb](cudaStream_t st, int, int last) {
+        bg::DelayedPreArgs b = a; b.last = last;
+        if (wb == 64) bg::k_dstdp_pre<double><<<(unsigned)grid, 256, 0, st>>>(b);
+        else bg::k_dstdp_pre<float><<<(unsigned)grid, 256, 0, st>>>(b);
+        return cudaGetLastError();
+    });
+    return BG_OK;
+}
+
 int build_stdp_pre(bg_net *net, int sid) {
     HStdp &s = net->stdps[sid];
     if (s.fused) return BG_OK;
+    if (s.delayed) return build_stdp_pre_delayed(net, sid);
     HConn &c = net->conns[s.cid];
     const HGroup &gs = net->groups[c.src];
     bg::PropArgs<double> a;
@@ -439,6 +467,7 @@ int build_stdp_post(bg_net *net, int sid) {
     a.A_post = s.dApost; a.A_pre = s.dApre; a.Am = s.Am;
     a.post_set = (s.inter != BG_STDP_ALL);   // 'nearest_pre' writes A_post=+Am (stdp.py:500-502)
     a.wmin = s.wmin; a.wmax = s.wmax;
+    if (s.delayed) { a.H_pre = s.dHpre; a.hlen = s.hlen; a.lagc = s.dLagPostC; }
     const int64_t grid = c.dense ? std::max<int64_t>(1, std::min<int64_t>((c.sn + 255) / 256, (int64_t)sm_count() * 2)) : 8;
     const int wb = c.w_bits;
     net->item_names.push_back("stdp_post[s" + std::to_string(sid) + "]");
@@ -471,6 +500,8 @@ int build_decay(bg_net *net, int sid) {
     HStdp &s = net->stdps[sid];
     const HConn &c = net->conns[s.cid];
     bg::DecayArgs a;
+    std::memset(&a, 0, sizeof(a));
+    if (s.delayed) { a.H_pre = s.dHpre; a.H_post = s.dHpost; a.hlen = s.hlen; }
     a.A_pre = s.dApre; a.npre = c.sn; a.a_pre = s.a_pre; a.c_pre = s.c_pre;
     a.A_post = s.dApost; a.npost = c.tn; a.a_post = s.a_post; a.c_post = s.c_post; a.ctl = net->dCtl; a.last = 0;
     const int64_t grid = std::max<int64_t>(1, (c.sn + c.tn + 255) / 256);
@@ -561,6 +592,10 @@ int reset_dynamic(bg_net *net) {
         const HConn &c = net->conns[s.cid];
         BG_CUDA(cudaMemsetAsync(s.dApre, 0, c.sn * 8, net->stream));
         BG_CUDA(cudaMemsetAsync(s.dApost, 0, c.tn * 8, net->stream));
+        if (s.delayed) {
+            BG_CUDA(cudaMemsetAsync(s.dHpre, 0, (size_t)s.hlen * c.sn * 8, net->stream));
+            BG_CUDA(cudaMemsetAsync(s.dHpost, 0, (size_t)s.hlen * c.tn * 8, net->stream));
+        }
     }
     return BG_OK;
 }
@@ -1172,6 +1207,30 @@ int bg_stdp_add(bg_net *n, int32_t cid, const double *decay, double Ap, double A
     return BG_OK;
 }
 
+int bg_stdp_add_delayed(bg_net *n, int32_t cid, const double *decay, double Ap, double Am, double wmin, double wmax,
+                        int inter, int32_t pre_delay, int32_t hist_len, const uint8_t *lag_pre, const uint8_t *lag_post,
+                        int32_t *sid) {
+    if (!n || cid < 0 || cid >= (int32_t)n->conns.size() || !decay || !sid) return fail(BG_EINVAL, "bg_stdp_add_delayed");
+    if (n->prepared) return fail(BG_ESTATE, "network already prepared");
+    HConn &c = n->conns[cid];
+    if (!c.hetero || c.dense) return fail(BG_EINVAL, "delayed STDP needs a sparse DelayConnection");
+    if (c.stdp >= 0) return fail(BG_ENOSYS, "one STDP rule per connection");
+    if (pre_delay < 0 || inter < 0 || inter > 3 || hist_len < 1 || hist_len > 256) return fail(BG_EINVAL, "STDP parameters");
+    if (c.nnz > 0 && (!lag_pre || !lag_post)) return fail(BG_EINVAL, "STDP lags");
+    for (int64_t k = 0; k < c.nnz; ++k)
+        if (lag_pre[k] >= hist_len || lag_post[k] >= hist_len) return fail(BG_EINVAL, "STDP lag beyond the trace history");
+    HStdp s; s.cid = cid; s.a_pre = decay[0]; s.c_pre = decay[1]; s.a_post = decay[2]; s.c_post = decay[3];
+    s.Ap = Ap; s.Am = Am; s.wmin = wmin; s.wmax = wmax; s.inter = inter; s.pre_delay = pre_delay; s.post_delay = 0;
+    s.delayed = true; s.hlen = hist_len;
+    s.lag_pre.assign(lag_pre, lag_pre + c.nnz); s.lag_post.assign(lag_post, lag_post + c.nnz);
+    n->stdps.push_back(std::move(s));
+    *sid = (int32_t)n->stdps.size() - 1;
+    c.stdp = *sid;
+    n->items.push_back({IT_STDP_PRE, *sid});
+    n->items.push_back({IT_STDP_POST, *sid});
+    return BG_OK;
+}
+
 int bg_stdp_get_traces(bg_net *n, int32_t sid, double *a_pre, double *a_post) {
     if (!n || sid < 0 || sid >= (int32_t)n->stdps.size()) return fail(BG_EINVAL, "bg_stdp_get_traces");
     if (!n->prepared) return fail(BG_ESTATE, "network not prepared");
@@ -1383,6 +1442,15 @@ static int prepare_impl(bg_net *n) {
             st = upload(n, c.dColptr, colptr.data(), (c.tn + 1) * 8); if (st) return st;
             st = upload(n, c.dColk, colk.data(), c.nnz * 8); if (st) return st;
             st = upload(n, c.dColsrc, colsrc.data(), c.nnz * 4); if (st) return st;
+            HStdp &s = n->stdps[c.stdp];
+            if (s.delayed && c.nnz > 0) {
+                std::vector<uint8_t> lagc(c.nnz);
+                for (int64_t p = 0; p < c.nnz; ++p) lagc[p] = s.lag_post[colk[p]];
+                if (n->alloc(&s.dLagPre, c.nnz) != cudaSuccess || n->alloc(&s.dLagPostC, c.nnz) != cudaSuccess)
+                    return fail(BG_ENOMEM, "STDP lags");
+                st = upload(n, s.dLagPre, s.lag_pre.data(), c.nnz); if (st) return st;
+                st = upload(n, s.dLagPostC, lagc.data(), c.nnz); if (st) return st;
+            }
             BG_CUDA(cudaStreamSynchronize(n->stream));
         }
     }
@@ -1390,9 +1458,12 @@ static int prepare_impl(bg_net *n) {
         const HConn &c = n->conns[s.cid];
         if (n->alloc(&s.dApre, std::max<int64_t>(1, c.sn) * 8) != cudaSuccess || n->alloc(&s.dApost, std::max<int64_t>(1, c.tn) * 8) != cudaSuccess)
             return fail(BG_ENOMEM, "STDP traces");
+        if (s.delayed && (n->alloc(&s.dHpre, (size_t)s.hlen * std::max<int64_t>(1, c.sn) * 8) != cudaSuccess ||
+                          n->alloc(&s.dHpost, (size_t)s.hlen * std::max<int64_t>(1, c.tn) * 8) != cudaSuccess))
+            return fail(BG_ENOMEM, "STDP trace histories");
         // the presynaptic update rides on the propagation kernel when it reads
         // the same spikes and the items are adjacent (connection, then updater)
-        s.fused = (s.pre_delay == c.delay);
+        s.fused = !s.delayed && (s.pre_delay == c.delay);
         if (s.fused) {
             for (size_t k = 0; k + 1 < n->items.size(); ++k)
                 if (n->items[k + 1].kind == IT_STDP_PRE && n->items[k + 1].id == (int)(&s - &n->stdps[0])) {

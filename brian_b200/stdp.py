@@ -9,6 +9,15 @@ into two NeuronGroups with 1x1 linear updaters (stdp.py:282-293) and runs
 the pre/post code as SpikeMonitors in the connections slot (stdp.py:31-54,
 370-414); the engine keeps the traces on the device and fuses the
 presynaptic update into the connection's propagation kernel.
+
+On a DelayConnection (stdp.py:296-368) the presynaptic code splits into an
+immediate part (``A_pre += Ap`` at the spike) and a delayed part run for the
+spikes of max_delay ago, whose ``w += A_post`` reads A_post as it was when
+the spike reached each target; the postsynaptic ``w += A_pre`` reads A_pre
+as it was when each source's spike left.  The reference gets those past
+values from two RecentStateMonitors (monitor.py:991-1099); the engine keeps
+the same ring of recorded traces on the device and looks each synapse up by
+a lag computed here with the reference's float arithmetic.
 """
 import numpy as np
 
@@ -41,6 +50,10 @@ class ExponentialSTDP(object):
         self.wmin, self.wmax = _code_bound(float(wmin)), _code_bound(wmax)
         self.interactions = _INTER[interactions]
         self.clock = clock if clock is not None else C.source.clock
+        from .connections import DelayConnection
+        self.delayed = isinstance(C, DelayConnection)
+        if self.delayed and (delay_pre is not None or delay_post is not None):
+            raise ValueError("Must use delay_pre=delay_post=None for the moment.")
         dt = self.clock.dt
         eqs = Equations("dA_pre/dt=-A_pre/taup : 1\ndA_post/dt=-A_post/taum : 1", taup=self.taup,
                         taum=self.taum)
@@ -69,7 +82,38 @@ class ExponentialSTDP(object):
         self._A_post = np.zeros(len(C.target))
         self.contained_objects = []
 
+    def _delayed_schedule(self):
+        """(pre_delay bins, history length, lag_pre, lag_post) of the delayed
+        updaters, per synapse in the connection's CSR order.
+
+        max_delay = C._max_delay * dt (stdp.py:297); the delayed presynaptic
+        updater is a SpikeMonitor delayed by int(max_delay / dt) bins
+        (monitor.py:142); the trace monitors keep int((C._max_delay+1)*dt / dt)
+        + 1 records (monitor.py:1024-1026) and look a synapse of delay d up
+        int((1/dt) * times) records before the last one (monitor.py:1092),
+        times = max_delay - d before a presynaptic update and d before a
+        postsynaptic one (stdp.py:335-336).  The expression 'max_delay-d' gets
+        max_delay substituted as text by str(float(max_delay)), which keeps 12
+        significant digits (stdp.py:78)."""
+        C = self.C
+        dt_t, dt_s, dt = float(C.target.clock.dt), float(C.source.clock.dt), float(self.clock.dt)
+        max_delay = C._md * dt_t
+        pre_delay = int(max_delay / dt_s)
+        hist_len = int(((C._md + 1) * dt_t) / (1 * dt)) + 1
+        if hist_len > 256:
+            raise NotImplementedError("STDP on a DelayConnection with max_delay beyond 254 steps")
+        maxd = float("%.12g" % max_delay)
+        inv = 1.0 / dt
+        d = C._delay_seconds()
+        lag_pre = np.array(inv * (maxd - d), dtype=np.int64) % hist_len
+        lag_post = np.array(inv * d, dtype=np.int64) % hist_len
+        return pre_delay, hist_len, lag_pre.astype(np.uint8), lag_post.astype(np.uint8)
+
     def _lower(self, rt, cid):
+        if self.delayed:
+            pre_delay, hist_len, lag_pre, lag_post = self._delayed_schedule()
+            return rt.stdp_add_delayed(cid, self.decay, self.Ap, self.Am, self.wmin, self.wmax, self.interactions,
+                                       pre_delay, hist_len, lag_pre, lag_post)
         return rt.stdp_add(cid, self.decay, self.Ap, self.Am, self.wmin, self.wmax, self.interactions,
                            self.pre_delay, self.post_delay)
 

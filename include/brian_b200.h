@@ -167,6 +167,25 @@ BG_API int bg_conn_set_weights(bg_net *net, int32_t cid, const double *in);
 BG_API int bg_stdp_add(bg_net *net, int32_t cid, const double *decay, double Ap,
                 double Am, double wmin, double wmax, int interactions,
                 int32_t pre_delay, int32_t post_delay, int32_t *sid);
+/* ExponentialSTDP on a sparse DelayConnection (stdp.py:296-368, replacing
+ * the STDPUpdater / DelayedSTDPUpdater pair and the two RecentStateMonitors
+ * of monitor.py:991-1099).  Three items run in the connections slot, after
+ * the connection: a spike of source i now does A_pre[i] (+)= Ap; a spike of
+ * source i `pre_delay` bins ago (the connection's max_delay) does
+ * w[k] += A_post[cols[k]] as recorded lag_pre[k] steps back, clip, for each
+ * synapse k of row i; a spike of target j now does A_post[j] (+)= Am, then
+ * w[k] += A_pre[src(k)] as recorded lag_post[k] steps back, clip, for each
+ * synapse k of column j.  The traces are recorded once per step, at the end
+ * of the step, into `hist_len` slots; lag L at step t reads the record of
+ * step t-1-L, zero before the first record.  lag_pre / lag_post are per
+ * synapse in CSR order, each in [0, hist_len): the reference's
+ * int((1/dt) * (max_delay - d)) and int((1/dt) * d) modulo hist_len, d the
+ * synapse's delay in seconds.  hist_len <= 256. */
+BG_API int bg_stdp_add_delayed(bg_net *net, int32_t cid, const double *decay,
+                double Ap, double Am, double wmin, double wmax,
+                int interactions, int32_t pre_delay, int32_t hist_len,
+                const uint8_t *lag_pre, const uint8_t *lag_post,
+                int32_t *sid);
 BG_API int bg_stdp_get_traces(bg_net *net, int32_t sid, double *a_pre,
                        double *a_post);
 

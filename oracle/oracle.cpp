@@ -117,6 +117,12 @@ struct Stdp {
     int32_t cid; double a_pre, c_pre, a_post, c_post, Ap, Am, wmin, wmax;
     int inter; int32_t pre_delay, post_delay;
     std::vector<double> A_pre, A_post;
+    /* DelayConnection (stdp.py:296-368): RecentStateMonitors of both traces
+     * (monitor.py:991-1099): M slots [M][n], written at the end of each step
+     * at current_time_index, which then advances modulo M */
+    bool delayed = false; int32_t M = 0; int64_t cur = 0;
+    std::vector<uint8_t> lag_pre, lag_post;
+    std::vector<double> H_pre, H_post;
 };
 struct SpikeMon { int32_t gid; int64_t origin, n; int32_t delay; std::vector<int64_t> steps; std::vector<int32_t> idx; };
 struct StateMon { int32_t gid; int var; std::vector<int32_t> idx; int32_t timestep; int64_t start;
@@ -353,6 +359,38 @@ int or_stdp_add(or_net *n, int32_t cid, const double *decay, double Ap, double A
     n->items.push_back({IT_STDP_PRE, *sid}); n->items.push_back({IT_STDP_POST, *sid});
     return OR_OK;
 }
+/* ExponentialSTDP on a DelayConnection: the presynaptic code splits into an
+ * immediate updater (delay 0) and a delayed one (delay = pre_delay, the
+ * connection's max_delay), the postsynaptic code runs at delay 0; the w
+ * lines read past trace values (stdp.py:296-352, DelayedSTDPUpdater
+ * stdp.py:57-89). */
+int or_stdp_add_delayed(or_net *n, int32_t cid, const double *decay, double Ap, double Am, double wmin, double wmax,
+                        int inter, int32_t pre_delay, int32_t hist_len, const uint8_t *lag_pre, const uint8_t *lag_post,
+                        int32_t *sid) {
+    if (!n || cid < 0 || cid >= (int32_t)n->conns.size() || !decay) return fail(OR_EINVAL, "stdp_add_delayed");
+    if (n->prepared) return fail(OR_ESTATE, "network already prepared");
+    Conn &c = n->conns[cid];
+    if (!c.hetero || c.dense) return fail(OR_EINVAL, "delayed STDP needs a sparse DelayConnection");
+    if (pre_delay < 0 || hist_len < 1 || hist_len > 256) return fail(OR_EINVAL, "stdp parameters");
+    const size_t nnz = c.cols.size();
+    for (size_t k = 0; k < nnz; ++k)
+        if (lag_pre[k] >= hist_len || lag_post[k] >= hist_len) return fail(OR_EINVAL, "stdp lags");
+    Stdp s; s.cid = cid; s.a_pre = decay[0]; s.c_pre = decay[1]; s.a_post = decay[2]; s.c_post = decay[3];
+    s.Ap = Ap; s.Am = Am; s.wmin = wmin; s.wmax = wmax; s.inter = inter;
+    s.pre_delay = pre_delay; s.post_delay = 0;
+    s.A_pre.assign(c.sn, 0.0); s.A_post.assign(c.tn, 0.0);
+    s.delayed = true; s.M = hist_len; s.cur = 0;
+    s.lag_pre.assign(lag_pre, lag_pre + nnz); s.lag_post.assign(lag_post, lag_post + nnz);
+    s.H_pre.assign((size_t)hist_len * c.sn, 0.0); s.H_post.assign((size_t)hist_len * c.tn, 0.0);
+    n->stdps.push_back(std::move(s)); *sid = (int32_t)n->stdps.size() - 1;
+    n->items.push_back({IT_STDP_PRE, *sid}); n->items.push_back({IT_STDP_POST, *sid});
+    return OR_OK;
+}
+/* get_past_values_sequence (monitor.py:1088-1096): the slot of the value
+ * recorded `lag` records before the last one */
+static inline size_t past_slot(const Stdp &s, int lag) {
+    int64_t q = (s.cur - 1 - lag) % s.M; if (q < 0) q += s.M; return (size_t)q;
+}
 int or_stdp_get_traces(or_net *n, int32_t sid, double *a_pre, double *a_post) {
     if (!n || sid < 0 || sid >= (int32_t)n->stdps.size()) return fail(OR_EINVAL, "stdp id");
     const Stdp &s = n->stdps[sid];
@@ -461,7 +499,10 @@ int or_net_reinit(or_net *n) {
         std::fill(g.last_spike.begin(), g.last_spike.end(), -(1ll << 40));
     }
     for (auto &c : n->conns) std::fill(c.ring.begin(), c.ring.end(), 0.0);
-    for (auto &s : n->stdps) { std::fill(s.A_pre.begin(), s.A_pre.end(), 0.0); std::fill(s.A_post.begin(), s.A_post.end(), 0.0); }
+    for (auto &s : n->stdps) {
+        std::fill(s.A_pre.begin(), s.A_pre.end(), 0.0); std::fill(s.A_post.begin(), s.A_post.end(), 0.0);
+        std::fill(s.H_pre.begin(), s.H_pre.end(), 0.0); std::fill(s.H_post.begin(), s.H_post.end(), 0.0); s.cur = 0;
+    }
     return OR_OK;
 }
 
@@ -576,6 +617,34 @@ static void step(or_net *n, int64_t cs) {
             SpikeMon &m = n->smons[it.id];
             get_spikes(n->groups[m.gid], m.delay, m.origin, m.n, spk);
             for (int32_t i : spk) { m.steps.push_back(cs); m.idx.push_back(i); }
+        } else if (it.kind == IT_STDP_PRE && n->stdps[it.id].delayed) {
+            Stdp &s = n->stdps[it.id]; Conn &c = n->conns[s.cid];
+            /* immediate updater: spikes of this step */
+            get_spikes(n->groups[c.src], 0, c.so, c.sn, spk);
+            for (int32_t i : spk) {
+                if (s.inter == 0 || s.inter == 3) s.A_pre[i] = s.A_pre[i] + s.Ap; else s.A_pre[i] = s.Ap;
+            }
+            /* delayed updater: spikes of max_delay ago, w[i,:] += A_post past values */
+            get_spikes(n->groups[c.src], s.pre_delay, c.so, c.sn, spk);
+            for (int32_t i : spk)
+                for (int64_t k = c.rowptr[i]; k < c.rowptr[i + 1]; ++k) {
+                    const double add = s.H_post[past_slot(s, s.lag_pre[k]) * c.tn + c.cols[k]];
+                    if (c.w_bits == 64) c.w64[k] = clipd(c.w64[k] + add, s.wmin, s.wmax);
+                    else c.w32[k] = clipf((float)((double)c.w32[k] + add), (float)s.wmin, (float)s.wmax);
+                }
+        } else if (it.kind == IT_STDP_POST && n->stdps[it.id].delayed) {
+            Stdp &s = n->stdps[it.id]; Conn &c = n->conns[s.cid];
+            get_spikes(n->groups[c.tgt], 0, c.to, c.tn, spk);
+            for (int32_t j : spk) {
+                if (s.inter == 0) s.A_post[j] = s.A_post[j] + s.Am; else s.A_post[j] = s.Am;
+            }
+            for (int32_t j : spk)
+                for (int64_t p = c.colptr[j]; p < c.colptr[j + 1]; ++p) {
+                    const int64_t k = c.colk[p]; const int32_t i = c.colsrc[p];
+                    const double add = s.H_pre[past_slot(s, s.lag_post[k]) * c.sn + i];
+                    if (c.w_bits == 64) c.w64[k] = clipd(c.w64[k] + add, s.wmin, s.wmax);
+                    else c.w32[k] = clipf((float)((double)c.w32[k] + add), (float)s.wmin, (float)s.wmax);
+                }
         } else if (it.kind == IT_STDP_PRE) {
             Stdp &s = n->stdps[it.id]; Conn &c = n->conns[s.cid];
             get_spikes(n->groups[c.src], s.pre_delay, c.so, c.sn, spk);
@@ -649,6 +718,13 @@ static void step(or_net *n, int64_t cs) {
         const double *v = &g.S[(size_t)m.var * g.n];
         for (int32_t i : m.idx) m.vals.push_back(v[i]);
         m.steps.push_back(cs);
+    }
+    /* ---- end: the STDP trace RecentStateMonitors (monitor.py:1036-1049) ---- */
+    for (auto &s : n->stdps) {
+        if (!s.delayed) continue;
+        std::copy(s.A_pre.begin(), s.A_pre.end(), s.H_pre.begin() + (size_t)s.cur * s.A_pre.size());
+        std::copy(s.A_post.begin(), s.A_post.end(), s.H_post.begin() + (size_t)s.cur * s.A_post.size());
+        s.cur = (s.cur + 1) % s.M;
     }
     n->nstep++;
 }

@@ -241,6 +241,43 @@ def stdp(Nin=400, Nout=32, steps=3000, seed=5, dense=True, rate_lo=5.0, rate_hi=
     return _result(net, groups=[out], spikemons=[M, Mi], conns=[C], stdps=[S])
 
 
+def stdp_delay(Nin=400, Nout=40, steps=3000, seed=9, p=0.5, wdtype=np.float64, interactions="all", runs=1,
+               rate_lo=5.0, rate_hi=25.0):
+    """ExponentialSTDP on a DelayConnection: Poisson inputs -> LIF outputs
+    through float delays (seconds) uniform below max_delay = 5 ms, so that
+    the per-synapse lags int((1/dt)*(max_delay-d)) and int((1/dt)*d) are
+    not complements of each other.  Also returns the connectivity and the
+    initial weights (CSR order) for replays of the rule."""
+    taum, taue = 10 * ms, 5 * ms
+    Ee, vt, vr, El = 0 * mV, -54 * mV, -60 * mV, -74 * mV
+    gmax = 0.01
+    eqs = b.Equations("""
+    dv/dt=(ge*(Ee-vr)+El-v)/taum : volt
+    dge/dt=-ge/taue : 1
+    """, taum=taum, taue=taue, Ee=Ee, vr=vr, El=El)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    inp = b.PoissonGroup(Nin, rates=rng.uniform(rate_lo, rate_hi, Nin) * 20, seed=seed)
+    out = b.NeuronGroup(Nout, model=eqs, threshold=vt, reset=vr)
+    out.v = vr
+    mask = rng.random((Nin, Nout)) < p
+    W0 = rng.uniform(0, gmax, (Nin, Nout)) * mask
+    D = rng.uniform(0.0, 4.99e-3, (Nin, Nout))
+    C = b.DelayConnection(inp, out, "ge", max_delay=5 * ms, dtype=wdtype)
+    C.connect(inp, out, W0, delay=D)
+    S = b.ExponentialSTDP(C, 20 * ms, 20 * ms, 0.01, -0.0105, wmax=gmax, interactions=interactions)
+    C.compress()
+    extra = {"rowptr": np.array(C._rowptr), "cols": np.array(C._cols), "d": C._delay_seconds().copy(),
+             "w_init": C._weights().astype(np.float64).copy(), "decay": np.array(S.decay)}
+    M = b.SpikeMonitor(out)
+    Mi = b.SpikeMonitor(inp)
+    net = b.Network(inp, out, C, S, M, Mi)
+    for _ in range(runs):
+        net.run(steps * 0.1 * ms / runs)
+    res = _result(net, groups=[out], spikemons=[M, Mi], conns=[C], stdps=[S])
+    res.update(extra)
+    return res
+
+
 def kitchen_sink(steps=400, seed=7):
     """Refractoriness, variable threshold/reset, homogeneous delays,
     modulation, dense structure, generators and subgroup monitors."""

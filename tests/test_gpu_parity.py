@@ -134,6 +134,25 @@ def test_stdp_bit_exact(oracle_table, gpu_table, dense):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("wdtype,interactions,runs", [(np.float64, "all", 1), (np.float32, "all", 1),
+                                                      (np.float64, "nearest", 2), (np.float64, "nearest_pre", 1)])
+def test_stdp_delay_bit_exact(oracle_table, gpu_table, wdtype, interactions, runs):
+    """ExponentialSTDP on a DelayConnection: weights, traces and spikes."""
+    ref, gpu = _both(scenarios.stdp_delay, oracle_table, wdtype=wdtype, interactions=interactions, runs=runs)
+    assert len(ref["spk0.idx"]) > 20
+    assert not np.array_equal(ref["w0"], ref["w_init"])
+    scenarios.compare(ref, gpu)
+
+
+@pytest.mark.gpu
+def test_stdp_delay_large_bit_exact(oracle_table, gpu_table):
+    """More sources than one block's words, several spikes per step."""
+    ref, gpu = _both(scenarios.stdp_delay, oracle_table, Nin=5000, Nout=300, p=0.1, steps=1500)
+    assert len(ref["spk0.idx"]) > 100
+    scenarios.compare(ref, gpu)
+
+
+@pytest.mark.gpu
 def test_kitchen_sink_bit_exact(oracle_table, gpu_table):
     ref, gpu = _both(scenarios.kitchen_sink, oracle_table)
     scenarios.compare(ref, gpu)
