@@ -16,6 +16,7 @@ from .groups import (NeuronGroup, PoissonGroup, SpikeGeneratorGroup, Threshold, 
                      Refractoriness, LazyStateUpdater, EmpiricalThreshold)
 from .connections import Connection, DelayConnection, IdentityConnection
 from .stdp import ExponentialSTDP, STDP
+from .synapses import Synapses
 from .monitors import (SpikeMonitor, StateMonitor, SpikeCounter, PopulationSpikeCounter, PopulationRateMonitor,
                        CoincidenceCounter, MultiStateMonitor)
 from .network import (Network, MagicNetwork, run, reinit, stop, clear, network_operation, NetworkOperation,

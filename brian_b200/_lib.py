@@ -38,6 +38,9 @@ SIGNATURES = {
     "conn_get_weights": [_vp, _i32, _vp],
     "conn_set_weights": [_vp, _i32, _vp],
     "stdp_add": [_vp, _i32, _vp, _dbl, _dbl, _dbl, _dbl, ct.c_int, _i32, _i32, _P(_i32)],
+    "synapses_add": [_vp, _i32, _i64, _i64, _i32, _i64, _i64, _i64, _vp, _vp, _vp, ct.c_int, _vp, _vp, _vp,
+                     _P(_i32)],
+    "synapses_set_terms": [_vp, _i32, _vp],
     "stdp_add_delayed": [_vp, _i32, _vp, _dbl, _dbl, _dbl, _dbl, ct.c_int, _i32, _i32, _vp, _vp, _P(_i32)],
     "stdp_get_traces": [_vp, _i32, _vp, _vp],
     "spikemon_add": [_vp, _i32, _i64, _i64, _i32, _P(_i32)],
@@ -287,6 +290,24 @@ class Runtime(object):
                                         int(interactions), int(pre_delay), int(hist_len), _ptr(lag_pre),
                                         _ptr(lag_post), ct.byref(sid)), "stdp_add_delayed")
         return sid.value
+
+    def synapses_add(self, src_gid, src_origin, src_n, tgt_gid, tgt_origin, tgt_n, pre, post, delay, op_var, op_sub,
+                     terms):
+        pre = np.ascontiguousarray(pre, dtype=np.int32)
+        post = np.ascontiguousarray(post, dtype=np.int32)
+        delay = np.ascontiguousarray(delay, dtype=np.int32)
+        op_var = np.ascontiguousarray(op_var, dtype=np.int32)
+        op_sub = np.ascontiguousarray(op_sub, dtype=np.int32)
+        terms = np.ascontiguousarray(terms, dtype=np.float64)
+        sid = _i32()
+        self._c(self.t.synapses_add(self.h, src_gid, src_origin, src_n, tgt_gid, tgt_origin, tgt_n, len(pre),
+                                    _ptr(pre), _ptr(post), _ptr(delay), len(op_var), _ptr(op_var), _ptr(op_sub),
+                                    _ptr(terms), ct.byref(sid)), "synapses_add")
+        return sid.value
+
+    def synapses_set_terms(self, sid, terms):
+        terms = np.ascontiguousarray(terms, dtype=np.float64)
+        self._c(self.t.synapses_set_terms(self.h, sid, _ptr(terms)), "synapses_set_terms")
 
     def stdp_get_traces(self, sid, npre, npost):
         a = np.empty(npre)

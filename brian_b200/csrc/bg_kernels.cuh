@@ -873,6 +873,75 @@ __global__ void __launch_bounds__(256) k_stdp_post(const PostArgs a) {
     bg_finish_step(a.ctl, a.last);
 }
 
+// Synapses delivery (synapses.py:808-827, SpikeQueue of spikequeue.py:
+// 69-330).  An event of a spike at step s through a synapse of delay d is
+// applied at step s + 1 + d, after the target group's update; the events
+// reaching one target are applied in queue order.  Each target's incoming
+// synapses are stored in that order (delay descending, then source, then
+// synapse index) as words source | (d + 1) << 24; one warp per target tests
+// 32 of them at a time against the source's spike history and applies the
+// hits in order, statement by statement: x = x + term or x = x - term.
+constexpr int kSynMaxOps = 4;
+struct SynArgs {
+    DevCtl *ctl;
+    const uint32_t *hist; int depth; int64_t nwords;
+    int64_t so, to, tn;
+    const int64_t *colptr; const uint32_t *word;
+    const double *term; int64_t nsyn;                      // [nops][nsyn], column order
+    int nops, nslots;
+    int slot_of[kSynMaxOps], sub[kSynMaxOps], slot_var[kSynMaxOps];
+    double *S; int64_t npad;
+    int last;
+};
+static __global__ void __launch_bounds__(256) k_syn_deliver(const SynArgs a) {
+    const long long nstep = a.ctl->nstep;
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t j = warp; j < a.tn; j += nwarps) {
+        const int64_t p0 = a.colptr[j], p1 = a.colptr[j + 1];
+        if (p0 == p1) continue;
+        double x[kSynMaxOps];
+#pragma unroll
+        for (int s = 0; s < kSynMaxOps; ++s)
+            x[s] = s < a.nslots ? a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] : 0.0;
+        bool any = false;
+        for (int64_t base = p0; base < p1; base += 32) {
+            const int64_t p = base + lane;
+            bool hit = false;
+            if (p < p1) {
+                const uint32_t w = a.word[p];
+                const long long lag = (long long)(w >> 24);
+                if (nstep >= lag) {
+                    const int64_t src = a.so + (int64_t)(w & 0xFFFFFFu);
+                    const uint32_t *H = a.hist + (int64_t)((nstep - lag) % a.depth) * a.nwords;
+                    hit = ((H[src >> 5] >> (src & 31)) & 1u) != 0u;
+                }
+            }
+            uint32_t m = __ballot_sync(0xffffffffu, hit);
+            any = any || m != 0u;
+            while (m) {
+                const int l = __ffs(m) - 1; m &= m - 1;
+                const int64_t q = base + l;
+#pragma unroll
+                for (int k = 0; k < kSynMaxOps; ++k) {
+                    if (k >= a.nops) break;
+                    const double t = a.term[(int64_t)k * a.nsyn + q];
+#pragma unroll
+                    for (int s = 0; s < kSynMaxOps; ++s)
+                        if (s == a.slot_of[k]) x[s] = a.sub[k] ? __dsub_rn(x[s], t) : __dadd_rn(x[s], t);
+                }
+            }
+        }
+        if (any && lane == 0) {
+#pragma unroll
+            for (int s = 0; s < kSynMaxOps; ++s)
+                if (s < a.nslots) a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] = x[s];
+        }
+    }
+    bg_finish_step(a.ctl, a.last);
+}
+
 // SpikeMonitor (monitor.py:156-166): one block appends the step's spikes in
 // ascending order.
 struct MonArgs {

@@ -124,6 +124,15 @@ struct HStdp {
     bool delayed = false; int hlen = 0; std::vector<uint8_t> lag_pre, lag_post;
     double *dHpre = nullptr, *dHpost = nullptr; uint8_t *dLagPre = nullptr, *dLagPostC = nullptr;
 };
+// Synapses: incoming synapses of each target in queue order (delay
+// descending, source, synapse index), as words source | (delay+1) << 24
+// with the statements' terms permuted alike.
+struct HSyn {
+    int32_t src = 0, tgt = 0; int64_t so = 0, sn = 0, to = 0, tn = 0, nsyn = 0; int nops = 0, dmax = 0;
+    std::vector<int32_t> op_var, op_sub;
+    std::vector<int64_t> colptr, perm; std::vector<uint32_t> word; std::vector<double> terms;   // terms: [nops][nsyn], synapse order
+    int64_t *dColptr = nullptr; uint32_t *dWord = nullptr; double *dTerm = nullptr;
+};
 struct HSpikeMon {
     int gid; int64_t origin, n; int delay;
     long long *dCnt = nullptr, *dBase = nullptr; int32_t *dIdx = nullptr, *dSteps = nullptr; int64_t cap = 0;
@@ -154,7 +163,7 @@ struct bg_net {
     uint32_t *dMonWords = nullptr;      // persistent path with spike monitors: spike words per step of a chunk
     long long *dMonOff = nullptr;       //   and per-step record offsets
     cudaStream_t stream = nullptr;
-    std::vector<HGroup> groups; std::vector<HConn> conns; std::vector<HStdp> stdps;
+    std::vector<HGroup> groups; std::vector<HConn> conns; std::vector<HStdp> stdps; std::vector<HSyn> syns;
     std::vector<HSpikeMon> smons; std::vector<HStateMon> stmons; std::vector<Item> items;
     std::vector<int> mon_kind, mon_idx;
     DevCtl *dCtl = nullptr;
@@ -480,6 +489,32 @@ int build_stdp_post(bg_net *net, int sid) {
     return BG_OK;
 }
 
+int build_syn(bg_net *net, int yi) {
+    HSyn &y = net->syns[yi];
+    const HGroup &gs = net->groups[y.src];
+    HGroup &gt = net->groups[y.tgt];
+    bg::SynArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.ctl = net->dCtl; a.hist = gs.dHist; a.depth = gs.depth; a.nwords = gs.npad / 32;
+    a.so = y.so; a.to = y.to; a.tn = y.tn; a.colptr = y.dColptr; a.word = y.dWord; a.term = y.dTerm; a.nsyn = y.nsyn;
+    a.nops = y.nops;
+    for (int k = 0; k < y.nops; ++k) {
+        int sl = -1;
+        for (int q = 0; q < a.nslots; ++q) if (a.slot_var[q] == y.op_var[k]) sl = q;
+        if (sl < 0) { sl = a.nslots++; a.slot_var[sl] = y.op_var[k]; }
+        a.slot_of[k] = sl; a.sub[k] = y.op_sub[k];
+    }
+    a.S = (double *)gt.dS; a.npad = gt.npad;
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((y.tn + 7) / 8, (int64_t)sm_count() * 8));
+    net->item_names.push_back("syn_deliver[y" + std::to_string(yi) + "]");
+    net->step_launches.push_back([a, grid](cudaStream_t st, int, int last) {
+        bg::SynArgs b = a; b.last = last;
+        bg::k_syn_deliver<<<(unsigned)grid, 256, 0, st>>>(b);
+        return cudaGetLastError();
+    });
+    return BG_OK;
+}
+
 int build_spikemon(bg_net *net, int k) {
     HSpikeMon &m = net->smons[k];
     const HGroup &g = net->groups[m.gid];
@@ -727,7 +762,7 @@ constexpr int64_t kPersistMonSteps = bg::kMonWordsThreads;
 template <typename T>
 int build_persist(bg_net *net) {
     net->persist = nullptr;
-    if (net->groups.size() != 1 || !net->stmons.empty() || !net->stdps.empty()) return BG_OK;
+    if (net->groups.size() != 1 || !net->stmons.empty() || !net->stdps.empty() || !net->syns.empty()) return BG_OK;
     for (const HSpikeMon &m : net->smons)
         if (m.gid != 0 || m.delay != 0) return BG_OK;
 
@@ -1207,6 +1242,68 @@ int bg_stdp_add(bg_net *n, int32_t cid, const double *decay, double Ap, double A
     return BG_OK;
 }
 
+int bg_synapses_add(bg_net *n, int32_t src_gid, int64_t src_origin, int64_t src_n, int32_t tgt_gid, int64_t tgt_origin,
+                    int64_t tgt_n, int64_t nsyn, const int32_t *pre, const int32_t *post, const int32_t *delay, int nops,
+                    const int32_t *op_var, const int32_t *op_sub, const double *terms, int32_t *sid) {
+    if (!gid_ok(n, src_gid) || !gid_ok(n, tgt_gid) || nsyn < 0 || nops < 0 || nops > bg::kSynMaxOps || !sid ||
+        (nsyn > 0 && (!pre || !post || !delay)) || (nops > 0 && (!op_var || !op_sub || (nsyn > 0 && !terms))))
+        return fail(BG_EINVAL, "bg_synapses_add");
+    if (n->prepared) return fail(BG_ESTATE, "network already prepared");
+    if (n->precision != 64) return fail(BG_ENOSYS, "Synapses run on the FP64 network path");
+    const HGroup &gs = n->groups[src_gid], &gt = n->groups[tgt_gid];
+    if (src_origin < 0 || src_n < 0 || src_origin + src_n > gs.n || tgt_origin < 0 || tgt_n < 0 || tgt_origin + tgt_n > gt.n)
+        return fail(BG_EINVAL, "synapse ranges");
+    if (src_n > (1 << 24)) return fail(BG_ENOSYS, "Synapses from more than 2^24 sources");
+    for (int k = 0; k < nops; ++k) if (op_var[k] < 0 || op_var[k] >= gt.nvar) return fail(BG_EINVAL, "synaptic statement");
+    HSyn y; y.src = src_gid; y.tgt = tgt_gid; y.so = src_origin; y.sn = src_n; y.to = tgt_origin; y.tn = tgt_n;
+    y.nsyn = nsyn; y.nops = nops; y.op_var.assign(op_var, op_var + nops); y.op_sub.assign(op_sub, op_sub + nops);
+    for (int64_t k = 0; k < nsyn; ++k) {
+        if (pre[k] < 0 || pre[k] >= src_n || post[k] < 0 || post[k] >= tgt_n) return fail(BG_EINVAL, "synapse index");
+        if (delay[k] < 0 || delay[k] > 253) return fail(BG_ENOSYS, "synaptic delay beyond 253 bins");
+        y.dmax = std::max(y.dmax, (int)delay[k]);
+    }
+    // queue order per target: later insertion (shorter delay) last, then
+    // ascending source, then ascending synapse index
+    y.perm.resize(nsyn);
+    for (int64_t k = 0; k < nsyn; ++k) y.perm[k] = k;
+    std::stable_sort(y.perm.begin(), y.perm.end(), [&](int64_t a, int64_t b) {
+        if (post[a] != post[b]) return post[a] < post[b];
+        if (delay[a] != delay[b]) return delay[a] > delay[b];
+        return pre[a] < pre[b];
+    });
+    y.colptr.assign(tgt_n + 1, 0);
+    for (int64_t k = 0; k < nsyn; ++k) y.colptr[post[k] + 1]++;
+    for (int64_t j = 0; j < tgt_n; ++j) y.colptr[j + 1] += y.colptr[j];
+    y.word.resize(nsyn);
+    for (int64_t p = 0; p < nsyn; ++p) {
+        const int64_t k = y.perm[p];
+        y.word[p] = (uint32_t)pre[k] | ((uint32_t)(delay[k] + 1) << 24);
+    }
+    if (nops > 0 && nsyn > 0) y.terms.assign(terms, terms + (size_t)nops * nsyn);
+    n->syns.push_back(std::move(y));
+    *sid = (int32_t)n->syns.size() - 1;
+    return BG_OK;
+}
+
+// Upload the statements' terms in column order (from `terms` in synapse
+// order, or from the stored copy when null).
+static int bg_synapses_set_terms_impl(bg_net *n, int yi, const double *terms) {
+    HSyn &y = n->syns[yi];
+    if (terms && !y.terms.empty()) std::copy(terms, terms + (size_t)y.nops * y.nsyn, y.terms.begin());
+    if (!y.dTerm || y.nops == 0 || y.nsyn == 0) return BG_OK;
+    std::vector<double> col((size_t)y.nops * y.nsyn);
+    for (int k = 0; k < y.nops; ++k)
+        for (int64_t p = 0; p < y.nsyn; ++p) col[(size_t)k * y.nsyn + p] = y.terms[(size_t)k * y.nsyn + y.perm[p]];
+    BG_CUDA(cudaStreamSynchronize(n->stream));
+    BG_CUDA(cudaMemcpy(y.dTerm, col.data(), col.size() * 8, cudaMemcpyHostToDevice));
+    return BG_OK;
+}
+
+int bg_synapses_set_terms(bg_net *n, int32_t sid, const double *terms) {
+    if (!n || sid < 0 || sid >= (int32_t)n->syns.size() || !terms) return fail(BG_EINVAL, "bg_synapses_set_terms");
+    return bg_synapses_set_terms_impl(n, sid, terms);
+}
+
 int bg_stdp_add_delayed(bg_net *n, int32_t cid, const double *decay, double Ap, double Am, double wmin, double wmax,
                         int inter, int32_t pre_delay, int32_t hist_len, const uint8_t *lag_pre, const uint8_t *lag_post,
                         int32_t *sid) {
@@ -1343,6 +1440,7 @@ static int prepare_impl(bg_net *n) {
         n->groups[c.tgt].depth = std::max(n->groups[c.tgt].depth, s.post_delay + 1);
     }
     for (auto &m : n->smons) { HGroup &g = n->groups[m.gid]; g.depth = std::max(g.depth, m.delay + 1); }
+    for (auto &y : n->syns) { HGroup &g = n->groups[y.src]; g.depth = std::max(g.depth, y.dmax + 2); }
     // chunk length bounded by monitor buffer sizes
     int64_t chunk = kChunkSteps;
     for (auto &m : n->smons) chunk = std::min<int64_t>(chunk, std::max<int64_t>(kGraphSteps, (int64_t)(1 << 25) / std::max<int64_t>(1, m.n)));
@@ -1507,6 +1605,16 @@ static int prepare_impl(bg_net *n) {
         BG_CUDA(cudaMemsetAsync(m.dRowBase, 0, 8, n->stream));
         g.recs.push_back((int)k);
     }
+    for (auto &y : n->syns) {
+        if (n->alloc(&y.dColptr, (y.tn + 1) * 8) != cudaSuccess || n->alloc(&y.dWord, std::max<int64_t>(1, y.nsyn) * 4) != cudaSuccess ||
+            n->alloc(&y.dTerm, std::max<int64_t>(1, (int64_t)y.nops * y.nsyn) * 8) != cudaSuccess)
+            return fail(BG_ENOMEM, "synapses");
+        int st = upload(n, y.dColptr, y.colptr.data(), (y.tn + 1) * 8); if (st) return st;
+        if (y.nsyn) { st = upload(n, y.dWord, y.word.data(), y.nsyn * 4); if (st) return st; }
+    }
+    for (size_t yi = 0; yi < n->syns.size(); ++yi) {
+        int st = bg_synapses_set_terms_impl(n, (int)yi, nullptr); if (st) return st;
+    }
     const size_t ncount = n->groups.size() + n->conns.size();
     if (n->alloc(&n->dCounters, std::max<size_t>(1, ncount) * 8) != cudaSuccess) return fail(BG_ENOMEM, "counters");
     BG_CUDA(cudaMemsetAsync(n->dCounters, 0, std::max<size_t>(1, ncount) * 8, n->stream));
@@ -1517,6 +1625,9 @@ static int prepare_impl(bg_net *n) {
     for (size_t gi = 0; gi < n->groups.size(); ++gi) {
         st = n->precision == 64 ? build_group<double>(n, (int)gi) : build_group<float>(n, (int)gi);
         if (st) return st;
+        // Synapses update in the groups slot, after their target group
+        for (size_t yi = 0; yi < n->syns.size(); ++yi)
+            if (n->syns[yi].tgt == (int)gi) { st = build_syn(n, (int)yi); if (st) return st; }
     }
     for (size_t si = 0; si < n->stdps.size(); ++si) { st = build_decay(n, (int)si); if (st) return st; }
     for (const Item &it : n->items) {

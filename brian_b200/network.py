@@ -29,6 +29,7 @@ from .connections import Connection, DelayConnection
 from .groups import NeuronGroup, Subgroup, _GroupBase
 from .monitors import SpikeMonitor, StateMonitor, MultiStateMonitor
 from .stdp import ExponentialSTDP
+from .synapses import Synapses
 
 __all__ = ["Network", "MagicNetwork", "run", "reinit", "stop", "clear", "network_operation",
            "NetworkOperation", "engine", "set_global_preferences", "get_global_preference"]
@@ -88,6 +89,7 @@ class _Binding(object):
         self.cids = {}
         self.sids = {}
         self.mids = {}
+        self.yids = {}
         self.objects = []
 
     def read_state(self, grp, var):
@@ -101,6 +103,9 @@ class _Binding(object):
 
     def write_weights(self, c, w):
         self.rt.conn_set_weights(self.cids[c], w)
+
+    def write_synapse_terms(self, y, terms):
+        self.rt.synapses_set_terms(self.yids[y], terms)
 
     def read_traces(self, s):
         return self.rt.stdp_get_traces(self.sids[s], len(s.C.source), len(s.C.target))
@@ -128,6 +133,8 @@ class _Binding(object):
             elif isinstance(o, ExponentialSTDP):
                 o._traces()
                 o._binding = None
+            elif isinstance(o, Synapses):
+                o._binding = None
             elif isinstance(o, (SpikeMonitor, StateMonitor)):
                 o._archive()
                 o._binding = None
@@ -140,6 +147,7 @@ class Network(object):
         self.connections = []
         self.operations = []
         self.stdps = []
+        self.synapses = []
         self.monitors = []
         self._order = []
         self.clock = None
@@ -167,6 +175,8 @@ class Network(object):
                 self.monitors.append(o)
             elif isinstance(o, ExponentialSTDP):
                 self.stdps.append(o)
+            elif isinstance(o, Synapses):
+                self.synapses.append(o)
             elif isinstance(o, MultiStateMonitor):
                 self.add(*o.contained_objects)
                 continue
@@ -196,6 +206,8 @@ class Network(object):
                 cands = [o.P._owner]
             elif isinstance(o, ExponentialSTDP):
                 cands = [o.C.source._owner, o.C.target._owner]
+            elif isinstance(o, Synapses):
+                cands = [o.source._owner, o.target._owner]
             for g in cands:
                 if not any(g is x for x in owners):
                     owners.append(g)
@@ -221,6 +233,13 @@ class Network(object):
         for s in self.stdps:
             if not any(s.C is c for c in self.connections):
                 raise ValueError("STDP on a connection that is not in the network")
+        for y in self.synapses:
+            # Synapses update in the groups slot at their place in the group
+            # order; the engine applies them right after their target group
+            tgt = y.target._owner
+            pos = [k for k, o in enumerate(self._order) if o is tgt]
+            if pos and pos[0] > next(k for k, o in enumerate(self._order) if o is y):
+                raise NotImplementedError("a Synapses object must follow its target group in the network")
         b = _Binding(self, _current_table(), self.clock.dt)
         rt = b.rt
         for g in groups:
@@ -241,6 +260,9 @@ class Network(object):
                 b.objects.append(o)
             elif isinstance(o, StateMonitor):
                 b.mids[o] = o._lower(rt, b.gids)
+                b.objects.append(o)
+            elif isinstance(o, Synapses):
+                b.yids[o] = o._lower(rt, b.gids)
                 b.objects.append(o)
         rt.prepare()
         for o in b.objects:
@@ -280,7 +302,7 @@ class Network(object):
 
 # ------------------------------------------------------------------ magic
 _magic_cache = {}
-_CLASSES = (NeuronGroup, Connection, SpikeMonitor, StateMonitor, ExponentialSTDP, MultiStateMonitor)
+_CLASSES = (NeuronGroup, Connection, SpikeMonitor, StateMonitor, ExponentialSTDP, MultiStateMonitor, Synapses)
 
 
 def _find_instances(level):

@@ -1,0 +1,406 @@
+"""Synapses (synapses/synapses.py:43-1058 of Brian 1.4.4) with static
+synaptic variables and presynaptic code that adds to postsynaptic variables.
+
+What runs on the engine:
+
+* ``model``: declarations of static synaptic variables (``w : 1``,
+  ``w : volt``); synaptic differential equations and event-driven code
+  raise NotImplementedError.
+* ``pre``: one code string whose lines are ``x += e`` or ``x -= e`` with
+  ``x`` a variable of the target group (optionally ``x_post``) and ``e`` a
+  synaptic variable, a constant, a product of both or its negation.
+  ``post`` code and lists of ``pre`` codes raise NotImplementedError.
+* Synapse creation as the reference's ``S[i, j] = True | int | float |
+  'condition'`` (synapses.py:583-723), ``connect_random`` and
+  ``connect_one_to_one``; synapse indices are allocated in the same order
+  (row by row).
+* Presynaptic delays: ``S.delay[...] = seconds`` is stored in bins as
+  ``int(value / dt)`` (synapticvariable.py:161).
+
+Event timing follows the SpikeQueue (spikequeue.py:69-330): the queue is
+filled in the connections slot with the spikes of step s and read in the
+groups slot, after ``next()`` has advanced it, so an event of delay d
+bins is applied at step s + 1 + d, where the Synapses object sits in the
+group order.  The engine supports the order in which the Synapses object
+follows its target group (the usual order of creation).  Events reaching
+one target in one step are applied in queue order: insertion step, then
+source index, then synapse index.  The reference applies repeated targets
+in rounds over numpy's default (unstable) argsort (synapses.py:502-516),
+which orders ties by numpy's sort implementation; queue order is the order
+a stable sort gives.
+"""
+import ast
+import re
+import sys
+
+import numpy as np
+
+from .groups import NeuronGroup, Subgroup
+
+__all__ = ["Synapses"]
+
+
+def _flat(code):
+    if "\n" in code:
+        return [ln.strip() for ln in code.split("\n") if ln.strip()]
+    return [ln.strip() for ln in code.split(";") if ln.strip()]
+
+
+def _caller_namespace(level):
+    """Globals and locals of the first frame outside this module, `level`
+    frames further out (the namespace the reference's code strings see)."""
+    frame = sys._getframe(1)
+    while frame is not None and frame.f_globals is globals():
+        frame = frame.f_back
+    for _ in range(level):
+        frame = frame.f_back
+    ns = dict(frame.f_globals)
+    ns.update(frame.f_locals)
+    return ns
+
+
+def _group_range(x, G):
+    """Indices (relative to the group G) of an int, slice, array or subgroup
+    (synapses.py:1100-1111 neuron_indexes)."""
+    if isinstance(x, (NeuronGroup, Subgroup)):
+        owner = x._owner
+        if owner is not G._owner:
+            raise ValueError("subgroup of another group")
+        lo = x._origin - G._origin
+        if lo < 0 or lo + len(x) > len(G):
+            raise ValueError("subgroup outside the group")
+        return np.arange(lo, lo + len(x), dtype=np.int64)
+    if isinstance(x, slice):
+        return np.arange(len(G), dtype=np.int64)[x]
+    if np.isscalar(x):
+        return np.array([int(x)], dtype=np.int64)
+    return np.asarray(x, dtype=np.int64).ravel()
+
+
+class _SynapticVariable(object):
+    """``S.w[...]`` (synapticvariable.py): synapse indices, (i, j) pairs of
+    neuron indices, or a string of i, j (and rand()) as the index of a
+    write."""
+
+    def __init__(self, S, name):
+        self._S, self._name = S, name
+
+    def _get(self):
+        return self._S._vars[self._name]
+
+    def __array__(self, dtype=None, copy=None):
+        a = self._get()
+        return a.astype(dtype) if dtype is not None else a.copy()
+
+    def __len__(self):
+        return len(self._S)
+
+    def __getitem__(self, key):
+        return self._get()[self._S._synapse_index(key)]
+
+    def __setitem__(self, key, value):
+        S = self._S
+        idx = S._synapse_index(key)
+        if isinstance(value, str):
+            value = S._eval_string(value, idx)
+        S._vars[self._name][idx] = np.asarray(value, dtype=np.float64)
+        S._changed()
+
+
+class _SynapticDelay(_SynapticVariable):
+    """Presynaptic delays, stored in bins as int(value / dt)
+    (synapticvariable.py:143-161); read back in seconds."""
+
+    def _get(self):
+        return self._S._delay * self._S.clock.dt
+
+    def __setitem__(self, key, value):
+        S = self._S
+        idx = S._synapse_index(key)
+        if isinstance(value, str):
+            value = S._eval_string(value, idx)
+        steps = np.array(np.asarray(value, dtype=np.float64) / S.clock.dt, dtype=np.int16)
+        S._delay[idx] = steps
+        S._changed(delays=True)
+
+
+class Synapses(object):
+    def __init__(self, source, target=None, model=None, pre=None, post=None, max_delay=0.0, level=0, clock=None,
+                 code_namespace=None, **kwds):
+        target = target or source
+        if source.clock is not target.clock:
+            raise ValueError("Source and target groups must have the same clock")
+        if post is not None:
+            raise NotImplementedError("postsynaptic code of Synapses is not run by the engine")
+        if isinstance(pre, (list, tuple)):
+            if len(pre) != 1:
+                raise NotImplementedError("several presynaptic codes are not run by the engine")
+            pre = pre[0]
+        if kwds.get("method") is not None or kwds.get("implicit") or kwds.get("order", 1) != 1:
+            raise NotImplementedError("synaptic differential equations are not run by the engine")
+        object.__setattr__(self, "_vars", {})
+        self.source, self.target = source, target
+        self.clock = clock or source.clock
+        self.max_delay = float(max_delay)
+        ns = _caller_namespace(level)
+        if code_namespace:
+            ns.update(code_namespace)
+        self._names = self._parse_model(model or "")
+        for n in self._names:
+            self._vars[n] = np.zeros(0)
+        self.presynaptic = np.zeros(0, dtype=np.int64)
+        self.postsynaptic = np.zeros(0, dtype=np.int64)
+        self._delay = np.zeros(0, dtype=np.int16)
+        self._ops = self._parse_pre(pre or "", ns)
+        self._binding = None
+        self._iscompressed = False
+
+    # ---------------------------------------------------------------- model
+    def _parse_model(self, model):
+        names = []
+        for line in _flat(model):
+            line = line.split("#")[0].strip()
+            if not line:
+                continue
+            m = re.match(r"^(\w+)\s*:\s*[\w\s\*/\.]+$", line)
+            if not m or "=" in line:
+                raise NotImplementedError("only static synaptic variables ('w : unit') are run by the engine: %r"
+                                          % line)
+            names.append(m.group(1))
+        for n in names:
+            if n in ("delay", "delay_pre", "delay_post", "lastupdate"):
+                raise NotImplementedError("synaptic variable %r" % n)
+        return names
+
+    def _parse_pre(self, pre, ns):
+        """Lines 'x += e' / 'x -= e' -> (target var index, subtract, synaptic
+        variable name or None, constant factor)."""
+        ops = []
+        tvars = self.target._owner.var_index
+        for line in _flat(pre):
+            if re.search(r"\b\w+_pre\s*[-+*/]?=", line):
+                raise ValueError('The synaptic code "%s" changes the value of a pre-synaptic variable.' % line)
+            m = re.match(r"^(\w+)\s*(\+=|-=)\s*(.+)$", line)
+            if not m:
+                raise NotImplementedError("presynaptic code other than 'x += e' / 'x -= e': %r" % line)
+            lhs, op, rhs = m.groups()
+            name = lhs[:-5] if lhs.endswith("_post") and lhs[:-5] in tvars else lhs
+            if name in self._names or name not in tvars or not isinstance(name, str):
+                raise NotImplementedError("presynaptic code must modify a postsynaptic variable: %r" % line)
+            var, c = self._term(ast.parse(rhs.strip(), mode="eval").body, ns, line)
+            ops.append((int(tvars[name]), op == "-=", var, c))
+        if len(ops) > 4:
+            raise NotImplementedError("more than four presynaptic statements")
+        return ops
+
+    def _term(self, node, ns, line):
+        """(synaptic variable or None, constant) of e = c, w, c*w, w*c, -e."""
+        if isinstance(node, ast.UnaryOp) and isinstance(node.op, ast.USub):
+            var, c = self._term(node.operand, ns, line)
+            return var, -c
+        if isinstance(node, ast.Constant) and isinstance(node.value, (int, float)):
+            return None, float(node.value)
+        if isinstance(node, ast.Name):
+            if node.id in self._names:
+                return node.id, 1.0
+            if node.id in ns and np.isscalar(ns[node.id]):
+                return None, float(ns[node.id])
+        if isinstance(node, ast.BinOp) and isinstance(node.op, ast.Mult):
+            a = self._term(node.left, ns, line)
+            b = self._term(node.right, ns, line)
+            if (a[0] is None) != (b[0] is None):
+                var = a[0] if a[0] is not None else b[0]
+                c = b[1] if a[0] is not None else a[1]
+                if (a[0] is not None and a[1] != 1.0) or (b[0] is not None and b[1] != 1.0):
+                    raise NotImplementedError("presynaptic expression: %r" % line)
+                return var, c
+        raise NotImplementedError("presynaptic expression other than c, w, c*w: %r" % line)
+
+    # ------------------------------------------------------------ creation
+    def __len__(self):
+        return len(self.presynaptic)
+
+    def _check_open(self):
+        if self._iscompressed:
+            raise AttributeError("Synapses cannot be added after they have been run")
+
+    def __setitem__(self, key, value):
+        """Create synapses (synapses.py:583-723).  Synapses are added, never
+        replaced: S[1,2]=True twice makes two."""
+        self._check_open()
+        if not isinstance(key, tuple):
+            raise AttributeError("Synapses behave as 2-D objects")
+        pre, post = key
+        pre_idx = _group_range(pre, self.source)
+        post_idx = _group_range(post, self.target)
+        if len(pre_idx) and pre_idx[-1] >= len(self.source):
+            raise ValueError("Presynaptic index %d greater than number of presynaptic neurons (%d)"
+                             % (pre_idx[-1], len(self.source)))
+        if len(post_idx) and post_idx[-1] >= len(self.target):
+            raise ValueError("Postsynaptic index %d greater than number of postsynaptic neurons (%d)"
+                             % (post_idx[-1], len(self.target)))
+        if isinstance(value, float):
+            self.connect_random(pre, post, value)
+            return
+        if isinstance(value, (bool, int, np.integer)) and not isinstance(value, str):
+            if value is False:
+                raise ValueError("Synapses cannot be deleted")
+            k = 1 if value is True else int(value)
+            # row-major over (pre, post), the whole block repeated k times
+            P, Q = np.meshgrid(pre_idx, post_idx, indexing="ij")
+            pres = np.tile(P.ravel(), k)
+            posts = np.tile(Q.ravel(), k)
+            self._create(pres, posts)
+            return
+        if isinstance(value, str):
+            # the condition is evaluated row by row with i a scalar and j the
+            # post indices; subgroup indices are relative to the subgroup
+            pre_shift = pre_idx[0] if isinstance(pre, (NeuronGroup, Subgroup)) and len(pre_idx) else 0
+            post_shift = post_idx[0] if isinstance(post, (NeuronGroup, Subgroup)) and len(post_idx) else 0
+            code = re.sub(r"\brand\(\)", "rand(n)", value)
+            code = re.sub(r"\brandn\(\)", "randn(n)", code)
+            ns = _caller_namespace(0)
+            ns.update({"j": post_idx - post_shift, "n": len(post_idx), "rand": np.random.rand,
+                       "randn": np.random.randn})
+            pres, posts = [], []
+            for i in pre_idx:
+                ns["i"] = int(i) - pre_shift
+                res = np.asarray(eval(code, ns))
+                if res.dtype.kind == "f":
+                    res = np.random.rand(len(post_idx)) < res
+                res = np.broadcast_to(res, (len(post_idx),))
+                sel = np.nonzero(res)[0]
+                pres.append(np.full(len(sel), i, dtype=np.int64))
+                posts.append(post_idx[sel])
+            self._create(np.concatenate(pres) if pres else np.zeros(0, np.int64),
+                         np.concatenate(posts) if posts else np.zeros(0, np.int64))
+            return
+        raise NotImplementedError("synapse creation from %r" % type(value))
+
+    def connect_random(self, pre=None, post=None, sparseness=None):
+        """Each presynaptic neuron gets Binomial(m, p) targets drawn without
+        replacement (synapses.py:845-885)."""
+        self._check_open()
+        pre_idx = _group_range(self.source if pre is None else pre, self.source)
+        post_idx = _group_range(self.target if post is None else post, self.target)
+        m = len(post_idx)
+        pres, posts = [], []
+        for i in pre_idx:
+            k = int(np.random.binomial(m, sparseness))
+            sel = np.random.choice(m, k, replace=False)
+            pres.append(np.full(k, i, dtype=np.int64))
+            posts.append(post_idx[sel])
+        self._create(np.concatenate(pres) if pres else np.zeros(0, np.int64),
+                     np.concatenate(posts) if posts else np.zeros(0, np.int64))
+
+    def connect_one_to_one(self, pre=None, post=None):
+        self._check_open()
+        pre_idx = _group_range(self.source if pre is None else pre, self.source)
+        post_idx = _group_range(self.target if post is None else post, self.target)
+        if len(pre_idx) != len(post_idx):
+            raise TypeError("Source and target groups do not have the same size")
+        self._create(pre_idx, post_idx)
+
+    def _create(self, pres, posts):
+        """create_synapses (synapses.py:725-763): new synapses take the next
+        indices in the given order."""
+        n = len(pres)
+        self.presynaptic = np.concatenate([self.presynaptic, np.asarray(pres, dtype=np.int64)])
+        self.postsynaptic = np.concatenate([self.postsynaptic, np.asarray(posts, dtype=np.int64)])
+        self._delay = np.concatenate([self._delay, np.zeros(n, dtype=np.int16)])
+        for name in self._names:
+            self._vars[name] = np.concatenate([self._vars[name], np.zeros(n)])
+        self._changed(delays=True)
+
+    # ------------------------------------------------------------- indexing
+    def synapse_index(self, key):
+        return self._synapse_index(key)
+
+    def _synapse_index(self, key):
+        """Synapse indices of a slice / int / array, or of (i, j) neuron
+        indices (synapses.py:946-1001)."""
+        if isinstance(key, tuple):
+            i, j = key
+            pi = _group_range(i, self.source)
+            qj = _group_range(j, self.target)
+            sel = np.isin(self.presynaptic, pi) & np.isin(self.postsynaptic, qj)
+            return np.nonzero(sel)[0]
+        if isinstance(key, slice):
+            return np.arange(len(self))[key]
+        return np.asarray(key, dtype=np.int64)
+
+    def _eval_string(self, code, idx):
+        ns = _caller_namespace(0)
+        n = len(idx)
+        code = re.sub(r"\brand\(\)", "rand(n)", code)
+        code = re.sub(r"\brandn\(\)", "randn(n)", code)
+        ns.update({"i": self.presynaptic[idx], "j": self.postsynaptic[idx], "n": n,
+                   "rand": np.random.rand, "randn": np.random.randn})
+        for name in self._names:
+            ns[name] = self._vars[name][idx]
+        return np.broadcast_to(np.asarray(eval(code, ns), dtype=np.float64), (n,))
+
+    def __getattr__(self, name):
+        if name.startswith("_"):
+            raise AttributeError(name)
+        if name in ("delay", "delay_pre"):
+            return _SynapticDelay(self, name)
+        if name in self.__dict__.get("_vars", {}):
+            return _SynapticVariable(self, name)
+        raise AttributeError(name)
+
+    def __setattr__(self, name, value):
+        if name in ("delay", "delay_pre"):
+            _SynapticDelay(self, name)[:] = value
+        elif name in self.__dict__.get("_vars", {}):
+            _SynapticVariable(self, name)[:] = value
+        else:
+            object.__setattr__(self, name, value)
+
+    # ------------------------------------------------------------- lowering
+    def _changed(self, delays=False):
+        b = self.__dict__.get("_binding")
+        if b is None:
+            return
+        if delays:
+            raise NotImplementedError("changing synapses or delays after the first run is not supported")
+        b.write_synapse_terms(self, self._terms())
+
+    def _terms(self):
+        """Per statement and synapse, the value added or subtracted:
+        c*w evaluated as numpy does it (one rounding), w itself for c = 1."""
+        out = np.empty((len(self._ops), len(self)))
+        for k, (_, _, name, c) in enumerate(self._ops):
+            if name is None:
+                out[k] = c
+            else:
+                v = self._vars[name]
+                out[k] = v if c == 1.0 else c * v
+        return out
+
+    def _queue_check(self):
+        """SpikeQueue.compress (spikequeue.py:172-208): with max_delay > 0
+        the queue has int(floor(max_delay/dt)) + 1 rows and longer delays
+        are refused."""
+        if len(self) == 0:
+            return
+        dmax = int(self._delay.max())
+        if int(self._delay.min()) < 0:
+            raise ValueError("negative synaptic delay")
+        if self.max_delay > 0 and dmax + 1 > int(np.floor(self.max_delay / self.clock.dt)) + 1:
+            raise ValueError("Synaptic delays exceed maximum delay")
+        if dmax > 253:
+            raise NotImplementedError("synaptic delays of more than 253 bins are not supported")
+
+    def _lower(self, rt, gids):
+        self._queue_check()
+        src, tgt = self.source._owner, self.target._owner
+        ops = self._ops
+        sid = rt.synapses_add(gids[src], self.source._origin, len(self.source), gids[tgt], self.target._origin,
+                              len(self.target), self.presynaptic, self.postsynaptic, self._delay,
+                              [o[0] for o in ops], [1 if o[1] else 0 for o in ops], self._terms())
+        self._iscompressed = True
+        return sid
+
+    def __repr__(self):
+        return "Synapses(%r -> %r, %d synapses)" % (self.source, self.target, len(self))

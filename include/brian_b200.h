@@ -167,6 +167,26 @@ BG_API int bg_conn_set_weights(bg_net *net, int32_t cid, const double *in);
 BG_API int bg_stdp_add(bg_net *net, int32_t cid, const double *decay, double Ap,
                 double Am, double wmin, double wmax, int interactions,
                 int32_t pre_delay, int32_t post_delay, int32_t *sid);
+/* Synapses (synapses/synapses.py:43-1058) with static synaptic variables and
+ * presynaptic code of `nops` (<= 4) statements x (+|-)= term, replacing
+ * Synapses.__init__/create_synapses and the SpikeQueue
+ * (synapses/spikequeue.py:69-330).  Synapse k joins source pre[k] (relative
+ * to src_origin) to target post[k] (relative to tgt_origin) with a delay of
+ * delay[k] bins (<= 253).  Statement q sets target variable op_var[q] to
+ * x - terms[q][k] when op_sub[q], else x + terms[q][k], terms [nops][nsyn]
+ * in synapse order.  A spike of step s is applied at step s + 1 + delay,
+ * in the groups slot right after the target group's update; the events
+ * reaching one target in one step are applied in queue order (insertion
+ * step, then source index, then synapse index).  FP64 networks only. */
+BG_API int bg_synapses_add(bg_net *net, int32_t src_gid, int64_t src_origin,
+                int64_t src_n, int32_t tgt_gid, int64_t tgt_origin, int64_t tgt_n,
+                int64_t nsyn, const int32_t *pre, const int32_t *post,
+                const int32_t *delay, int nops, const int32_t *op_var,
+                const int32_t *op_sub, const double *terms, int32_t *sid);
+/* New statement terms ([nops][nsyn], synapse order), e.g. after S.w[:] = ...
+ * (synapticvariable.py __setitem__) between runs. */
+BG_API int bg_synapses_set_terms(bg_net *net, int32_t sid, const double *terms);
+
 /* ExponentialSTDP on a sparse DelayConnection (stdp.py:296-368, replacing
  * the STDPUpdater / DelayedSTDPUpdater pair and the two RecentStateMonitors
  * of monitor.py:991-1099).  Three items run in the connections slot, after

@@ -124,16 +124,29 @@ struct Stdp {
     std::vector<uint8_t> lag_pre, lag_post;
     std::vector<double> H_pre, H_post;
 };
+/* Synapses (synapses/synapses.py:43-1058) with static synaptic variables
+ * and presynaptic statements x (+|-)= term on the target; SpikeQueue
+ * (synapses/spikequeue.py:69-330): L rows of synapse indices, filled in the
+ * connections slot at row (cur + delay) % L after cur has advanced, read and
+ * cleared at row cur in the groups slot. */
+struct Syn {
+    int32_t src, tgt; int64_t so, sn, to, tn; int64_t nsyn;
+    std::vector<int32_t> pre, post, delay;
+    int nops; std::vector<int32_t> op_var, op_sub; std::vector<double> terms;   /* [nops][nsyn] */
+    std::vector<std::vector<int32_t>> syn_of_pre;                               /* ascending */
+    int32_t L = 1; int64_t cur = 0; std::vector<std::vector<int32_t>> X;
+};
 struct SpikeMon { int32_t gid; int64_t origin, n; int32_t delay; std::vector<int64_t> steps; std::vector<int32_t> idx; };
 struct StateMon { int32_t gid; int var; std::vector<int32_t> idx; int32_t timestep; int64_t start;
                   std::vector<double> vals; std::vector<int64_t> steps; };
-enum { IT_CONN = 0, IT_SPIKEMON = 1, IT_STDP_PRE = 2, IT_STDP_POST = 3 };
+enum { IT_CONN = 0, IT_SPIKEMON = 1, IT_STDP_PRE = 2, IT_STDP_POST = 3, IT_SYN = 4 };
 struct Item { int kind; int32_t id; };
 
 struct or_net {
     double dt; int precision;
     std::vector<Group> groups; std::vector<Conn> conns; std::vector<Stdp> stdps;
     std::vector<SpikeMon> smons; std::vector<StateMon> stmons; std::vector<Item> items;
+    std::vector<Syn> syns;
     std::vector<int32_t> mon_kind;   /* monitor id -> 0 spike, 1 state (index into vector in mon_idx) */
     std::vector<int32_t> mon_idx;
     bool prepared = false; int64_t nstep = 0;
@@ -386,6 +399,57 @@ int or_stdp_add_delayed(or_net *n, int32_t cid, const double *decay, double Ap, 
     n->items.push_back({IT_STDP_PRE, *sid}); n->items.push_back({IT_STDP_POST, *sid});
     return OR_OK;
 }
+int or_synapses_add(or_net *n, int32_t src_gid, int64_t src_origin, int64_t src_n, int32_t tgt_gid, int64_t tgt_origin,
+                    int64_t tgt_n, int64_t nsyn, const int32_t *pre, const int32_t *post, const int32_t *delay, int nops,
+                    const int32_t *op_var, const int32_t *op_sub, const double *terms, int32_t *sid) {
+    if (!gid_ok(n, src_gid) || !gid_ok(n, tgt_gid) || nsyn < 0 || nops < 0 || nops > 4 || !sid)
+        return fail(OR_EINVAL, "synapses_add");
+    if (n->prepared) return fail(OR_ESTATE, "network already prepared");
+    const Group &gs = n->groups[src_gid], &gt = n->groups[tgt_gid];
+    if (src_origin < 0 || src_n < 0 || src_origin + src_n > gs.n || tgt_origin < 0 || tgt_n < 0 || tgt_origin + tgt_n > gt.n)
+        return fail(OR_EINVAL, "synapses ranges");
+    Syn y; y.src = src_gid; y.tgt = tgt_gid; y.so = src_origin; y.sn = src_n; y.to = tgt_origin; y.tn = tgt_n;
+    y.nsyn = nsyn; y.nops = nops;
+    y.pre.assign(pre, pre + nsyn); y.post.assign(post, post + nsyn); y.delay.assign(delay, delay + nsyn);
+    y.op_var.assign(op_var, op_var + nops); y.op_sub.assign(op_sub, op_sub + nops);
+    y.terms.assign(terms, terms + (size_t)nops * nsyn);
+    int32_t dmax = 0;
+    for (int64_t k = 0; k < nsyn; ++k) {
+        if (pre[k] < 0 || pre[k] >= src_n || post[k] < 0 || post[k] >= tgt_n || delay[k] < 0) return fail(OR_EINVAL, "synapse");
+        dmax = std::max(dmax, delay[k]);
+    }
+    for (int k = 0; k < nops; ++k) if (op_var[k] < 0 || op_var[k] >= gt.nvar) return fail(OR_EINVAL, "synaptic statement");
+    y.syn_of_pre.assign(src_n, std::vector<int32_t>());
+    for (int64_t k = 0; k < nsyn; ++k) y.syn_of_pre[pre[k]].push_back((int32_t)k);
+    y.L = dmax + 1; y.cur = 0; y.X.assign(y.L, std::vector<int32_t>());
+    n->syns.push_back(std::move(y)); *sid = (int32_t)n->syns.size() - 1;
+    n->items.push_back({IT_SYN, *sid});
+    return OR_OK;
+}
+int or_synapses_set_terms(or_net *n, int32_t sid, const double *terms) {
+    if (!n || sid < 0 || sid >= (int32_t)n->syns.size() || !terms) return fail(OR_EINVAL, "synapses_set_terms");
+    Syn &y = n->syns[sid];
+    std::copy(terms, terms + (size_t)y.nops * y.nsyn, y.terms.begin());
+    return OR_OK;
+}
+/* Synapses.update (synapses.py:808-827): the events of this step, in queue
+ * order, applied statement by statement; then next(). */
+static void synapses_deliver(or_net *n, int32_t gid) {
+    for (auto &y : n->syns) {
+        if (y.tgt != gid) continue;
+        Group &g = n->groups[gid];
+        for (int32_t e : y.X[y.cur]) {
+            const int64_t j = y.to + y.post[e];
+            for (int k = 0; k < y.nops; ++k) {
+                double &x = g.S[(size_t)y.op_var[k] * g.n + j];
+                const double term = y.terms[(size_t)k * y.nsyn + e];
+                x = y.op_sub[k] ? x - term : x + term;
+            }
+        }
+        y.X[y.cur].clear();
+        y.cur = (y.cur + 1) % y.L;
+    }
+}
 /* get_past_values_sequence (monitor.py:1088-1096): the slot of the value
  * recorded `lag` records before the last one */
 static inline size_t past_slot(const Stdp &s, int lag) {
@@ -499,6 +563,7 @@ int or_net_reinit(or_net *n) {
         std::fill(g.last_spike.begin(), g.last_spike.end(), -(1ll << 40));
     }
     for (auto &c : n->conns) std::fill(c.ring.begin(), c.ring.end(), 0.0);
+    for (auto &y : n->syns) { for (auto &r : y.X) r.clear(); y.cur = 0; }
     for (auto &s : n->stdps) {
         std::fill(s.A_pre.begin(), s.A_pre.end(), 0.0); std::fill(s.A_post.begin(), s.A_post.end(), 0.0);
         std::fill(s.H_pre.begin(), s.H_pre.end(), 0.0); std::fill(s.H_post.begin(), s.H_post.end(), 0.0); s.cur = 0;
@@ -521,7 +586,8 @@ static void step(or_net *n, int64_t cs) {
     const double t = (double)cs * dt;
     std::vector<int32_t> spk;
     /* ---- groups slot ---- */
-    for (auto &g : n->groups) {
+    for (size_t gi = 0; gi < n->groups.size(); ++gi) {
+        Group &g = n->groups[gi];
         const int64_t N = g.n; const int m = g.nvar;
         if (g.gen_update) {
             for (int64_t i = 0; i < N; ++i) g.gen_update(g.S.data(), N, i, t);
@@ -578,6 +644,8 @@ static void step(or_net *n, int64_t cs) {
         }
         g.nspikes += (int64_t)spikes.size();
         g.hist.pop_back(); g.hist.push_front(std::move(spikes));
+        /* Synapses placed after their target group in the group order */
+        synapses_deliver(n, (int32_t)gi);
     }
     for (auto &s : n->stdps) {   /* trace groups G_pre / G_post (stdp.py:282-293) */
         for (auto &a : s.A_pre) a = s.a_pre * a + s.c_pre;
@@ -613,6 +681,11 @@ static void step(or_net *n, int64_t cs) {
                     }
                 }
             }
+        } else if (it.kind == IT_SYN) {
+            Syn &y = n->syns[it.id];
+            get_spikes(n->groups[y.src], 0, y.so, y.sn, spk);
+            for (int32_t i : spk)
+                for (int32_t e : y.syn_of_pre[i]) y.X[(size_t)((y.cur + y.delay[e]) % y.L)].push_back(e);
         } else if (it.kind == IT_SPIKEMON) {
             SpikeMon &m = n->smons[it.id];
             get_spikes(n->groups[m.gid], m.delay, m.origin, m.n, spk);

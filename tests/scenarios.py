@@ -278,6 +278,41 @@ def stdp_delay(Nin=400, Nout=40, steps=3000, seed=9, p=0.5, wdtype=np.float64, i
     return res
 
 
+def synapses_cuba(N=2000, steps=2000, seed=11, p=0.02, runs=1, two_statements=True, multi=True):
+    """CUBA through Synapses: excitatory and inhibitory subgroups onto the
+    whole group with per-synapse weights and float delays (0-4 ms); the
+    excitatory code has two statements; some pairs get two synapses."""
+    taum, taue, taui = 20 * ms, 5 * ms, 10 * ms
+    Vt, Vr, El = -50 * mV, -60 * mV, -49 * mV
+    eqs = b.Equations("""
+    dv/dt  = (ge+gi-(v-El))/taum : volt
+    dge/dt = -ge/taue : volt
+    dgi/dt = -gi/taui : volt
+    """, taum=taum, taue=taue, taui=taui, El=El)
+    P = b.NeuronGroup(N, model=eqs, threshold=Vt, reset=Vr)
+    Ne = int(0.8 * N)
+    Pe, Pi = P.subgroup(Ne), P.subgroup(N - Ne)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    pre_e = "ge += w\nv += 0.05*w" if two_statements else "ge += w"
+    Se = b.Synapses(Pe, P, model="w : volt", pre=pre_e, max_delay=5 * ms)
+    Si = b.Synapses(Pi, P, model="w : volt", pre="gi -= w")
+    Se.connect_random(sparseness=p)
+    Si.connect_random(sparseness=p)
+    if multi:
+        Se[0:20, 0:20] = 2          # pairs with two synapses
+    Se.w = 1.62 * mV * (0.5 + rng.random(len(Se)))
+    Si.w = 9 * mV * (0.5 + rng.random(len(Si)))
+    Se.delay = rng.random(len(Se)) * 4 * ms
+    Si.delay = rng.random(len(Si)) * 4 * ms
+    P.v = Vr + rng.random(N) * (Vt - Vr)
+    M = b.SpikeMonitor(P)
+    S = b.StateMonitor(P, "v", record=[0, 1, N - 1])
+    net = b.Network(P, Se, Si, M, S)
+    for _ in range(runs):
+        net.run(steps * 0.1 * ms / runs)
+    return _result(net, groups=[P], spikemons=[M], statemons=[S])
+
+
 def kitchen_sink(steps=400, seed=7):
     """Refractoriness, variable threshold/reset, homogeneous delays,
     modulation, dense structure, generators and subgroup monitors."""

@@ -1,0 +1,71 @@
+"""Synapses on the GPU: the known answers and bit-exact parity with the
+oracle (spikes, states, state monitors)."""
+import numpy as np
+import pytest
+
+import brian_b200 as b
+from brian_b200.network import engine
+
+import scenarios
+import test_synapses_oracle as kat
+
+
+def _both(fn, oracle_table, **kw):
+    out = []
+    for tab in (oracle_table, None):
+        b.clear()
+        b.reinit_default_clock()
+        np.random.seed(1234)
+        if tab is None:
+            out.append(fn(**kw))
+        else:
+            with engine(tab):
+                out.append(fn(**kw))
+    return out
+
+
+@pytest.mark.gpu
+def test_known_answers_gpu(gpu_table):
+    kat._fresh()
+    steps, v = kat._kat(gpu_table)
+    v0, v1 = kat.expected_known_answer()
+    np.testing.assert_array_equal(v[:, 0], v0)
+    np.testing.assert_array_equal(v[:, 1], v1)
+    kat._fresh()
+    np.testing.assert_array_equal(kat.kat_insertion_order(gpu_table), kat.expected_insertion_order())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kw", [dict(), dict(runs=2), dict(two_statements=False, multi=False),
+                                dict(N=6000, p=0.01, steps=1500)])
+def test_synapses_bit_exact(oracle_table, gpu_table, kw):
+    ref, gpu = _both(scenarios.synapses_cuba, oracle_table, **kw)
+    assert len(ref["spk0.idx"]) > 100
+    scenarios.compare(ref, gpu)
+
+
+def _weights_between_runs():
+    out = scenarios.synapses_cuba(N=800, steps=400, runs=1)
+    return out
+
+
+@pytest.mark.gpu
+def test_synapse_weights_changed_between_runs(oracle_table, gpu_table):
+    def fn():
+        from brian_b200 import ms, mV
+        G = b.NeuronGroup(300, model="dv/dt = -v/(10*ms) : volt", threshold=-50 * mV, reset=-60 * mV)
+        src = b.PoissonGroup(200, rates=40.0, seed=3)
+        S = b.Synapses(src, G, model="w : volt", pre="v += w")
+        S.connect_random(sparseness=0.2)
+        S.w = 0.5 * mV
+        S.delay = "rand() * 2*ms"
+        M = b.SpikeMonitor(G)
+        St = b.StateMonitor(G, "v", record=[0, 5])
+        net = b.Network(src, G, S, M, St)
+        net.run(20 * ms)
+        S.w = "w * (1 + (i % 3))"
+        net.run(20 * ms)
+        return scenarios._result(net, groups=[G], spikemons=[M], statemons=[St])
+    ref, gpu = _both(fn, oracle_table)
+    assert len(ref["spk0.idx"]) > 10
+    scenarios.compare(ref, gpu)
