@@ -301,6 +301,21 @@ class Synapses(object):
             raise TypeError("Source and target groups do not have the same size")
         self._create(pre_idx, post_idx)
 
+    def create_synapses(self, presynaptic, postsynaptic, synapses_pre=None, synapses_post=None):
+        """New synapses from arrays of pre- and postsynaptic indices, taking
+        the next synapse indices in array order (synapses.py:725-763)."""
+        self._check_open()
+        if synapses_pre is not None or synapses_post is not None:
+            raise NotImplementedError("explicit synapse index maps")
+        pres = np.asarray(presynaptic, dtype=np.int64)
+        posts = np.asarray(postsynaptic, dtype=np.int64)
+        if pres.shape != posts.shape:
+            raise ValueError("presynaptic and postsynaptic arrays differ in length")
+        if len(pres) and (pres.min() < 0 or pres.max() >= len(self.source) or posts.min() < 0
+                          or posts.max() >= len(self.target)):
+            raise ValueError("neuron index out of range")
+        self._create(pres, posts)
+
     def _create(self, pres, posts):
         """create_synapses (synapses.py:725-763): new synapses take the next
         indices in the given order."""
