@@ -416,59 +416,71 @@ def synapses_case(seed, n=32768, indegree=160, sim_steps=2000, profile_steps=300
     """CUBA through Synapses: n LIF neurons, fixed in-degree (80 % exc, 20 %
     inh) built with create_synapses, per-synapse weights, float delays
     uniform in 0-4 ms, FP64.  Reports synaptic events per second of device
-    time over `sim_steps` steps and the delivery kernel's algorithmic bytes
-    per launch (every incoming synapse word tested, the terms of the hits,
-    the targets' state) against its mean duration."""
+    time over `sim_steps` steps (events counted from a SpikeMonitor and the
+    out-degrees) and, on a copy of the network without the monitor, the
+    delivery kernel's algorithmic bytes per launch (every incoming synapse
+    word tested, the targets' state, the terms of the hits) against its
+    mean duration."""
     import brian_b200 as b
     from brian_b200 import ms, mV
     from brian_b200._lib import fixed_indegree_csr_native
-    rng = np.random.default_rng(seed)
-    b.clear()
-    b.reinit_default_clock()
-    eqs = b.Equations("""
-    dv/dt  = (ge+gi-(v-El))/taum : volt
-    dge/dt = -ge/taue : volt
-    dgi/dt = -gi/taui : volt
-    """, taum=20 * ms, taue=5 * ms, taui=10 * ms, El=-49 * mV)
-    P = b.NeuronGroup(n, model=eqs, threshold=-50 * mV, reset=-60 * mV)
-    ne = int(0.8 * n)
-    Pe, Pi = P.subgroup(ne), P.subgroup(n - ne)
-    syns, outdeg = [], np.zeros(n, dtype=np.int64)
-    for src, cnt, k, w, var, off in ((Pe, ne, int(0.8 * indegree), 1.62 * 80 / indegree * mV, "ge", 0),
-                                     (Pi, n - ne, indegree - int(0.8 * indegree), 9 * 80 / indegree * mV, "gi", ne)):
-        S = b.Synapses(src, P, model="w : volt", pre="%s %s= w" % (var, "+" if var == "ge" else "-"))
-        rowptr, cols = fixed_indegree_csr_native(cnt, n, k, seed + off)
-        rows = np.repeat(np.arange(cnt), np.diff(rowptr))
-        S.create_synapses(rows, cols)
-        S.w = w * (0.5 + rng.random(len(S)))
-        S.delay = rng.random(len(S)) * 4 * ms
-        outdeg[off:off + cnt] = np.diff(rowptr)
-        syns.append(S)
-    P.v = -60 * mV + rng.random(n) * 10 * mV
-    M = b.SpikeMonitor(P)
-    net = b.Network(P, syns[0], syns[1], M)
-    net.prepare()
+
+    def build(monitor):
+        rng = np.random.default_rng(seed)
+        b.clear()
+        b.reinit_default_clock()
+        eqs = b.Equations("""
+        dv/dt  = (ge+gi-(v-El))/taum : volt
+        dge/dt = -ge/taue : volt
+        dgi/dt = -gi/taui : volt
+        """, taum=20 * ms, taue=5 * ms, taui=10 * ms, El=-49 * mV)
+        P = b.NeuronGroup(n, model=eqs, threshold=-50 * mV, reset=-60 * mV)
+        ne = int(0.8 * n)
+        Pe, Pi = P.subgroup(ne), P.subgroup(n - ne)
+        syns, outdeg = [], np.zeros(n, dtype=np.int64)
+        for src, cnt, k, w, var, off in ((Pe, ne, int(0.8 * indegree), 1.62 * 80 / indegree * mV, "ge", 0),
+                                         (Pi, n - ne, indegree - int(0.8 * indegree), 9 * 80 / indegree * mV, "gi",
+                                          ne)):
+            S = b.Synapses(src, P, model="w : volt", pre="%s %s= w" % (var, "+" if var == "ge" else "-"))
+            rowptr, cols = fixed_indegree_csr_native(cnt, n, k, seed + off)
+            S.create_synapses(np.repeat(np.arange(cnt), np.diff(rowptr)), cols)
+            S.w = w * (0.5 + rng.random(len(S)))
+            S.delay = rng.random(len(S)) * 4 * ms
+            outdeg[off:off + cnt] = np.diff(rowptr)
+            syns.append(S)
+        P.v = -60 * mV + rng.random(n) * 10 * mV
+        objs = [P] + syns
+        M = None
+        if monitor:
+            M = b.SpikeMonitor(P)
+            objs.append(M)
+        net = b.Network(*objs)
+        net.prepare()
+        return net, syns, outdeg, M
+
+    net, syns, outdeg, _ = build(False)
     rt = net._binding.rt
     net.run(100 * DT)
     prof = rt.profile(profile_steps, net.clock.step)
+    net, syns, outdeg, M = build(True)
+    rt = net._binding.rt
+    net.run(100 * DT)
     ev0 = len(M._record()[1])
     t0 = time.perf_counter()
     net.run(sim_steps * DT)
     wall = time.perf_counter() - t0
     st = rt.stats()
-    steps, idx = M._record()
-    idx = np.asarray(idx)[ev0:]
+    idx = np.asarray(M._record()[1])[ev0:]
     events = int(outdeg[idx].sum())
     nnz = sum(len(S) for S in syns)
-    deliver = [(k, v) for k, v in prof if k.startswith("syn_deliver")]
-    dms = sum(v for _, v in deliver)
+    dms = sum(v for k, v in prof if k.startswith("syn_deliver"))
     hits_per_step = events / sim_steps
     alg = nnz * 4 + (n + 1) * 8 * 2 + n * 8 * 2 + hits_per_step * 8
     peak, peak_src = peaks()
     return {"case": "synapses", "neurons": n, "synapses": nnz, "sim_steps": sim_steps,
             "spikes": int(len(idx)), "events": events, "device_ms": st["last_run_ms"], "wall_s": wall,
             "events_per_s": events / (st["last_run_ms"] * 1e-3), "us_per_step": st["last_run_ms"] * 1e3 / sim_steps,
-            "launches": [(k, round(v * 1e3, 3)) for k, v in prof],
+            "launches_us": [(k, round(v * 1e3, 3)) for k, v in prof],
             "deliver_us_per_step": dms * 1e3, "deliver_alg_bytes": alg,
             "deliver_gbs": alg / (dms * 1e-3) / 1e9 if dms > 0 else None,
             "hbm_peak_gbs": peak, "peak_source": peak_src}
