@@ -477,7 +477,25 @@ def synapses_case(seed, n=32768, indegree=160, sim_steps=2000, profile_steps=300
     hits_per_step = events / sim_steps
     alg = nnz * 4 + (n + 1) * 8 * 2 + n * 8 * 2 + hits_per_step * 8
     peak, peak_src = peaks()
-    return {"case": "synapses", "neurons": n, "synapses": nnz, "sim_steps": sim_steps,
+    # the oracle (single-threaded C restatement, SpikeQueue in host memory)
+    # on the same network, a bounded sample of steps from the same state
+    import oracle
+    from brian_b200.network import engine
+    cpu_steps = 2000
+    with engine(oracle.table()):
+        cnet, _, _, cM = build(True)
+        cnet.run(100 * DT)
+        c0 = len(cM._record()[1])
+        t1 = time.perf_counter()
+        cnet.run(cpu_steps * DT)
+        cwall = time.perf_counter() - t1
+        cidx = np.asarray(cM._record()[1])[c0:]
+        cev = int(outdeg[cidx].sum())
+    cnet._invalidate()
+    cpu = {"value": cev / cwall, "unit": "events/s", "cores": 1, "kind": "port",
+           "sample": "same network, %d steps after 100 warm-up steps, %d events in %.1f s wall"
+                     % (cpu_steps, cev, cwall)}
+    return {"case": "synapses", "neurons": n, "synapses": nnz, "sim_steps": sim_steps, "cpu_baseline": cpu,
             "spikes": int(len(idx)), "events": events, "device_ms": st["last_run_ms"], "wall_s": wall,
             "events_per_s": events / (st["last_run_ms"] * 1e-3), "us_per_step": st["last_run_ms"] * 1e3 / sim_steps,
             "launches_us": [(k, round(v * 1e3, 3)) for k, v in prof],
