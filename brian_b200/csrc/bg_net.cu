@@ -1264,13 +1264,21 @@ int bg_synapses_add(bg_net *n, int32_t src_gid, int64_t src_origin, int64_t src_
     }
     // queue order per target: later insertion (shorter delay) last, then
     // ascending source, then ascending synapse index
-    y.perm.resize(nsyn);
-    for (int64_t k = 0; k < nsyn; ++k) y.perm[k] = k;
-    std::stable_sort(y.perm.begin(), y.perm.end(), [&](int64_t a, int64_t b) {
-        if (post[a] != post[b]) return post[a] < post[b];
-        if (delay[a] != delay[b]) return delay[a] > delay[b];
-        return pre[a] < pre[b];
-    });
+    // three stable counting passes (least significant key first): source,
+    // delay descending, target
+    std::vector<int64_t> cur(nsyn), nxt(nsyn);
+    for (int64_t k = 0; k < nsyn; ++k) cur[k] = k;
+    auto pass = [&](int64_t range, auto key) {
+        std::vector<int64_t> cnt(range + 1, 0);
+        for (int64_t k = 0; k < nsyn; ++k) cnt[key(cur[k]) + 1]++;
+        for (int64_t r = 0; r < range; ++r) cnt[r + 1] += cnt[r];
+        for (int64_t k = 0; k < nsyn; ++k) nxt[cnt[key(cur[k])]++] = cur[k];
+        cur.swap(nxt);
+    };
+    pass(src_n, [&](int64_t k) { return (int64_t)pre[k]; });
+    pass(254, [&](int64_t k) { return (int64_t)(253 - delay[k]); });
+    pass(tgt_n, [&](int64_t k) { return (int64_t)post[k]; });
+    y.perm.swap(cur);
     y.colptr.assign(tgt_n + 1, 0);
     for (int64_t k = 0; k < nsyn; ++k) y.colptr[post[k] + 1]++;
     for (int64_t j = 0; j < tgt_n; ++j) y.colptr[j + 1] += y.colptr[j];
