@@ -878,10 +878,19 @@ __global__ void __launch_bounds__(256) k_stdp_post(const PostArgs a) {
 // applied at step s + 1 + d, after the target group's update; the events
 // reaching one target are applied in queue order.  Each target's incoming
 // synapses are stored in that order (delay descending, then source, then
-// synapse index) as words source | (d + 1) << 24; one warp per target tests
-// 32 of them at a time against the source's spike history and applies the
-// hits in order, statement by statement: x = x + term or x = x - term.
+// synapse index) as words source | (d + 1) << 24.  A block takes a tile of
+// kSynTile consecutive targets: phase A tests the tile's words (all
+// threads, kSynUnroll independent loads in flight each) against the
+// sources' spike history and leaves one hit bit per synapse in shared
+// memory; phase B gives each target a thread that applies its hits in
+// order, statement by statement: x = x + term or x = x - term.  Tiles whose
+// synapses exceed kSynChunk words are processed in chunks, each target
+// keeping its values in registers across chunks.
 constexpr int kSynMaxOps = 4;
+constexpr int kSynThreads = 256;
+constexpr int kSynTile = 32;
+constexpr int kSynChunk = 8192;
+constexpr int kSynUnroll = 8;
 struct SynArgs {
     DevCtl *ctl;
     const uint32_t *hist; int depth; int64_t nwords;
@@ -893,47 +902,79 @@ struct SynArgs {
     double *S; int64_t npad;
     int last;
 };
-static __global__ void __launch_bounds__(256) k_syn_deliver(const SynArgs a) {
+static __global__ void __launch_bounds__(kSynThreads) k_syn_deliver(const SynArgs a) {
+    __shared__ uint32_t mask[kSynChunk / 32];
     const long long nstep = a.ctl->nstep;
-    const int lane = threadIdx.x & 31;
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t j = warp; j < a.tn; j += nwarps) {
-        const int64_t p0 = a.colptr[j], p1 = a.colptr[j + 1];
-        if (p0 == p1) continue;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    constexpr int kWarps = kSynThreads / 32;
+    const int64_t ntiles = (a.tn + kSynTile - 1) / kSynTile;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int64_t j0 = tile * kSynTile, j1 = min(a.tn, j0 + kSynTile);
+        const int64_t P0 = a.colptr[j0], P1 = a.colptr[j1];
+        const int64_t j = j0 + tid;
+        const bool own = tid < kSynTile && j < j1;
+        const int64_t q0 = own ? a.colptr[j] : 0, q1 = own ? a.colptr[j + 1] : 0;
         double x[kSynMaxOps];
 #pragma unroll
         for (int s = 0; s < kSynMaxOps; ++s)
-            x[s] = s < a.nslots ? a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] : 0.0;
+            x[s] = (own && q0 < q1 && s < a.nslots) ? a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] : 0.0;
         bool any = false;
-        for (int64_t base = p0; base < p1; base += 32) {
-            const int64_t p = base + lane;
-            bool hit = false;
-            if (p < p1) {
-                const uint32_t w = a.word[p];
-                const long long lag = (long long)(w >> 24);
-                if (nstep >= lag) {
-                    const int64_t src = a.so + (int64_t)(w & 0xFFFFFFu);
-                    const uint32_t *H = a.hist + (int64_t)((nstep - lag) % a.depth) * a.nwords;
-                    hit = ((H[src >> 5] >> (src & 31)) & 1u) != 0u;
+        for (int64_t c0 = P0; c0 < P1; c0 += kSynChunk) {
+            const int64_t c1 = min(P1, c0 + (int64_t)kSynChunk);
+            const int nw = (int)((c1 - c0 + 31) >> 5);
+            // phase A: word w of the chunk's mask is tested by warp w % kWarps
+            for (int w0 = wid; w0 < nw; w0 += kWarps * kSynUnroll) {
+                uint32_t wd[kSynUnroll];
+#pragma unroll
+                for (int u = 0; u < kSynUnroll; ++u) {
+                    const int64_t p = c0 + (int64_t)(w0 + u * kWarps) * 32 + lane;
+                    wd[u] = (w0 + u * kWarps < nw && p < c1) ? a.word[p] : 0u;
+                }
+                uint32_t hb[kSynUnroll];
+#pragma unroll
+                for (int u = 0; u < kSynUnroll; ++u) {
+                    const long long lag = (long long)(wd[u] >> 24);
+                    hb[u] = 0u;
+                    if (lag > 0 && nstep >= lag) {
+                        const int64_t src = a.so + (int64_t)(wd[u] & 0xFFFFFFu);
+                        hb[u] = (a.hist[(int64_t)((nstep - lag) % a.depth) * a.nwords + (src >> 5)] >> (src & 31)) & 1u;
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kSynUnroll; ++u) {
+                    const uint32_t m = __ballot_sync(0xffffffffu, hb[u] != 0u);
+                    if (lane == 0 && w0 + u * kWarps < nw) mask[w0 + u * kWarps] = m;
                 }
             }
-            uint32_t m = __ballot_sync(0xffffffffu, hit);
-            any = any || m != 0u;
-            while (m) {
-                const int l = __ffs(m) - 1; m &= m - 1;
-                const int64_t q = base + l;
+            __syncthreads();
+            // phase B: each target's hits within the chunk, in order
+            if (own) {
+                const int64_t lo = max(q0, c0), hi = min(q1, c1);
+                for (int64_t p = lo; p < hi;) {
+                    const int w = (int)((p - c0) >> 5), b = (int)((p - c0) & 31);
+                    const int64_t wend = min(hi, c0 + (int64_t)(w + 1) * 32);
+                    uint32_t m = mask[w] >> b;
+                    const int nb = (int)(wend - p);
+                    if (nb < 32) m &= (1u << nb) - 1u;
+                    while (m) {
+                        const int l = __ffs(m) - 1; m &= m - 1;
+                        const int64_t q = p + l;
+                        any = true;
 #pragma unroll
-                for (int k = 0; k < kSynMaxOps; ++k) {
-                    if (k >= a.nops) break;
-                    const double t = a.term[(int64_t)k * a.nsyn + q];
+                        for (int k = 0; k < kSynMaxOps; ++k) {
+                            if (k >= a.nops) break;
+                            const double t = a.term[(int64_t)k * a.nsyn + q];
 #pragma unroll
-                    for (int s = 0; s < kSynMaxOps; ++s)
-                        if (s == a.slot_of[k]) x[s] = a.sub[k] ? __dsub_rn(x[s], t) : __dadd_rn(x[s], t);
+                            for (int s = 0; s < kSynMaxOps; ++s)
+                                if (s == a.slot_of[k]) x[s] = a.sub[k] ? __dsub_rn(x[s], t) : __dadd_rn(x[s], t);
+                        }
+                    }
+                    p = wend;
                 }
             }
+            __syncthreads();
         }
-        if (any && lane == 0) {
+        if (own && any) {
 #pragma unroll
             for (int s = 0; s < kSynMaxOps; ++s)
                 if (s < a.nslots) a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] = x[s];

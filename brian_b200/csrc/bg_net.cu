@@ -505,11 +505,12 @@ int build_syn(bg_net *net, int yi) {
         a.slot_of[k] = sl; a.sub[k] = y.op_sub[k];
     }
     a.S = (double *)gt.dS; a.npad = gt.npad;
-    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((y.tn + 7) / 8, (int64_t)sm_count() * 8));
+    const int64_t ntiles = (y.tn + bg::kSynTile - 1) / bg::kSynTile;
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)sm_count() * 8));
     net->item_names.push_back("syn_deliver[y" + std::to_string(yi) + "]");
     net->step_launches.push_back([a, grid](cudaStream_t st, int, int last) {
         bg::SynArgs b = a; b.last = last;
-        bg::k_syn_deliver<<<(unsigned)grid, 256, 0, st>>>(b);
+        bg::k_syn_deliver<<<(unsigned)grid, bg::kSynThreads, 0, st>>>(b);
         return cudaGetLastError();
     });
     return BG_OK;
