@@ -705,11 +705,15 @@ static __global__ void k_stdp_decay(const DecayArgs a) {
     bg_finish_step(a.ctl, a.last);
 }
 
-// Slot of the trace record `lag` records before the last one at step nstep
+// Slot of the trace record `lag` records before the last one
 // (monitor.py:1092: (current_time_index - 1 - lag) mod M, one record per
-// step; lag < hlen).
-__device__ __forceinline__ int64_t hist_slot(long long nstep, int lag, int hlen) {
-    return (int64_t)((nstep + hlen - 1 - lag) % hlen);
+// step; lag < hlen); last = (nstep - 1) mod hlen, taken once per thread.
+__device__ __forceinline__ int64_t hist_slot(int last, int lag, int hlen) {
+    const int s = last - lag;
+    return (int64_t)(s < 0 ? s + hlen : s);
+}
+__device__ __forceinline__ int hist_last(long long nstep, int hlen) {
+    return (int)((nstep + hlen - 1) % hlen);
 }
 
 // Presynaptic rule on a DelayConnection (stdp.py:296-352): the immediate
@@ -747,6 +751,7 @@ __global__ void __launch_bounds__(256) k_dstdp_pre(const DelayedPreArgs a) {
     }
     if (nstep >= a.delay) {   // delayed: one warp per spike, lanes over the row
         const int64_t warp = gtid >> 5, nwarps = nthreads >> 5;
+        const int hlast = hist_last(nstep, a.hlen);
         const uint32_t *H = a.hist + (int64_t)((int)((nstep - a.delay) % a.depth)) * a.nwords;
         WT *W = (WT *)a.w;
         for (int64_t wi0 = w0 + warp * 32; wi0 < w1; wi0 += nwarps * 32) {
@@ -761,7 +766,7 @@ __global__ void __launch_bounds__(256) k_dstdp_pre(const DelayedPreArgs a) {
                     const int b = __ffs(wd) - 1; wd &= wd - 1;
                     const int64_t i = base + b - a.so;
                     for (int64_t k = a.rowptr[i] + lane; k < a.rowptr[i + 1]; k += 32) {
-                        const int64_t s = hist_slot(nstep, a.lag[k], a.hlen);
+                        const int64_t s = hist_slot(hlast, a.lag[k], a.hlen);
                         stdp_w<double, WT>(W, k, a.H_post[s * a.tn + a.cols[k]], a.wmin, a.wmax);
                     }
                 }
@@ -828,6 +833,7 @@ __global__ void __launch_bounds__(256) k_stdp_post(const PostArgs a) {
     __shared__ int32_t sp[1024];
     __shared__ int ns;
     const long long nstep = a.ctl->nstep;
+    const int hlast = a.H_pre ? hist_last(nstep, a.hlen) : 0;
     if (nstep >= a.delay) {
         const uint32_t *H = a.hist + (int64_t)((int)(nstep - a.delay) % a.depth) * a.nwords;
         const int64_t end = a.to + a.tn;
@@ -856,7 +862,7 @@ __global__ void __launch_bounds__(256) k_stdp_post(const PostArgs a) {
                 } else {
                     for (int64_t p = a.colptr[j] + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < a.colptr[j + 1];
                          p += (int64_t)gridDim.x * blockDim.x) {
-                        const double add = a.H_pre ? a.H_pre[hist_slot(nstep, a.lagc[p], a.hlen) * a.sn + a.colsrc[p]]
+                        const double add = a.H_pre ? a.H_pre[hist_slot(hlast, a.lagc[p], a.hlen) * a.sn + a.colsrc[p]]
                                                    : a.A_pre[a.colsrc[p]];
                         stdp_w<double, WT>(W, a.colk[p], add, a.wmin, a.wmax);
                     }
@@ -908,6 +914,9 @@ static __global__ void __launch_bounds__(kSynThreads) k_syn_deliver(const SynArg
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     constexpr int kWarps = kSynThreads / 32;
     const int64_t ntiles = (a.tn + kSynTile - 1) / kSynTile;
+    // history row of step nstep - lag: (nstep mod depth) - lag, wrapped once
+    // (lag <= depth - 1); no 64-bit modulo per synapse
+    const int row0 = (int)(nstep % a.depth);
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int64_t j0 = tile * kSynTile, j1 = min(a.tn, j0 + kSynTile);
         const int64_t P0 = a.colptr[j0], P1 = a.colptr[j1];
@@ -933,11 +942,13 @@ static __global__ void __launch_bounds__(kSynThreads) k_syn_deliver(const SynArg
                 uint32_t hb[kSynUnroll];
 #pragma unroll
                 for (int u = 0; u < kSynUnroll; ++u) {
-                    const long long lag = (long long)(wd[u] >> 24);
+                    const int lag = (int)(wd[u] >> 24);
                     hb[u] = 0u;
                     if (lag > 0 && nstep >= lag) {
                         const int64_t src = a.so + (int64_t)(wd[u] & 0xFFFFFFu);
-                        hb[u] = (a.hist[(int64_t)((nstep - lag) % a.depth) * a.nwords + (src >> 5)] >> (src & 31)) & 1u;
+                        int row = row0 - lag;
+                        row += row < 0 ? a.depth : 0;
+                        hb[u] = (a.hist[(int64_t)row * a.nwords + (src >> 5)] >> (src & 31)) & 1u;
                     }
                 }
 #pragma unroll
