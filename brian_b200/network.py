@@ -28,7 +28,7 @@ from .clock import guess_clock
 from .connections import Connection, DelayConnection
 from .groups import NeuronGroup, Subgroup, _GroupBase
 from .monitors import SpikeMonitor, StateMonitor, MultiStateMonitor
-from .stdp import ExponentialSTDP
+from .stdp import ExponentialSTDP, STDP
 from .synapses import Synapses
 
 __all__ = ["Network", "MagicNetwork", "run", "reinit", "stop", "clear", "network_operation",
@@ -130,7 +130,7 @@ class _Binding(object):
                 w = o._weights()
                 o._binding = None
                 o._w = w
-            elif isinstance(o, ExponentialSTDP):
+            elif isinstance(o, STDP):
                 o._traces()
                 o._binding = None
             elif isinstance(o, Synapses):
@@ -173,7 +173,7 @@ class Network(object):
                 self.connections.append(o)
             elif isinstance(o, StateMonitor):
                 self.monitors.append(o)
-            elif isinstance(o, ExponentialSTDP):
+            elif isinstance(o, STDP):
                 self.stdps.append(o)
             elif isinstance(o, Synapses):
                 self.synapses.append(o)
@@ -204,7 +204,7 @@ class Network(object):
                 cands = [o.source._owner]
             elif isinstance(o, StateMonitor):
                 cands = [o.P._owner]
-            elif isinstance(o, ExponentialSTDP):
+            elif isinstance(o, STDP):
                 cands = [o.C.source._owner, o.C.target._owner]
             elif isinstance(o, Synapses):
                 cands = [o.source._owner, o.target._owner]
@@ -302,7 +302,7 @@ class Network(object):
 
 # ------------------------------------------------------------------ magic
 _magic_cache = {}
-_CLASSES = (NeuronGroup, Connection, SpikeMonitor, StateMonitor, ExponentialSTDP, MultiStateMonitor, Synapses)
+_CLASSES = (NeuronGroup, Connection, SpikeMonitor, StateMonitor, STDP, MultiStateMonitor, Synapses)
 
 
 def _find_instances(level):

@@ -21,7 +21,9 @@ a lag computed here with the reference's float arithmetic.
 """
 import numpy as np
 
-from .equations import Equations, linear_propagator
+import re
+
+from .equations import Equations, linear_propagator, _caller_namespace, _identifiers
 
 __all__ = ["ExponentialSTDP", "STDP"]
 
@@ -34,35 +36,103 @@ def _code_bound(x):
     return float("%e" % x)
 
 
-class ExponentialSTDP(object):
-    def __init__(self, C, taup, taum, Ap, Am, interactions="all", wmin=0, wmax=None, update="additive",
-                 delay_pre=None, delay_post=None, clock=None):
-        if wmax is None:
-            raise AttributeError("You must specify the maximum synaptic weight")
-        if interactions not in _INTER:
-            raise AttributeError("Unknown interaction type " + interactions)
-        if update != "additive":
-            raise NotImplementedError("only additive ExponentialSTDP runs on the engine")
-        wmax = float(wmax)
+def _lines(code):
+    """Statements of a code string: lines, or ';'-separated on one line
+    (stdp.py:205-214)."""
+    if "\n" in code:
+        parts = code.split("\n")
+    else:
+        parts = code.split(";")
+    return [p.split("#", 1)[0].strip() for p in parts if p.split("#", 1)[0].strip()]
+
+
+def _modified(lines):
+    """Variables assigned by the statements (modified_variables)."""
+    out = set()
+    for ln in lines:
+        m = re.match(r"^(\w+)\s*[-+*/]?=(?!=)", ln)
+        if m:
+            out.add(m.group(1))
+    return out
+
+
+class STDP(object):
+    """Spike-timing-dependent plasticity from equations and code strings
+    (stdp.py:92-449).
+
+    The reference separates the equations into a presynaptic and a
+    postsynaptic group and runs the code strings in SpikeMonitors.  The
+    engine runs the family ExponentialSTDP generates: one linear trace
+    equation per side, a presynaptic code of ``x_pre += c`` (or ``= c``) and
+    ``w += x_post``, a postsynaptic code of ``x_post += c`` (or ``= c``) and
+    ``w += x_pre``; weights clipped to [wmin, wmax] after each update.  Other
+    code raises NotImplementedError.  Constants in the code are looked up
+    in the caller's namespace (``level`` frames up), as the reference does."""
+
+    def __init__(self, C, eqs, pre, post, wmin=0, wmax=np.inf, level=0, clock=None, delay_pre=None,
+                 delay_post=None):
+        ns = _caller_namespace(level + 1)
+        eqs_obj = eqs if isinstance(eqs, Equations) else Equations(eqs, level=level + 1)
+        ns_eq = dict(eqs_obj._namespace)
+        pre_lines, post_lines = _lines(pre), _lines(post)
+        names = list(eqs_obj._diffeq_names)
+        vars_pre = [v for v in names if v in _modified(pre_lines)]
+        vars_post = [v for v in names if v in _modified(post_lines)]
+        if len(names) != 2 or len(vars_pre) != 1 or len(vars_post) != 1 or vars_pre == vars_post:
+            raise NotImplementedError("the engine runs STDP with one presynaptic and one postsynaptic trace")
+        xp, xq = vars_pre[0], vars_post[0]
+        Ap, pre_set = self._trace_rule(pre_lines, xp, xq, ns)
+        Am, post_set = self._trace_rule(post_lines, xq, xp, ns)
+        inter = {(False, False): 0, (True, True): 1, (False, True): 3}.get((pre_set, post_set))
+        if inter is None:
+            raise NotImplementedError("presynaptic '=' with postsynaptic '+=' rule")
+        clock = clock if clock is not None else C.source.clock
+        decay = []
+        for v in (xp, xq):
+            # each trace is a separate 1x1 linear group (stdp.py:282-293)
+            one = Equations("d%s/dt=%s : %s" % (v, eqs_obj._string[v], eqs_obj._units[v] or "1"), **ns_eq) \
+                if ns_eq else Equations("d%s/dt=%s : %s" % (v, eqs_obj._string[v], eqs_obj._units[v] or "1"),
+                                        level=level + 1)
+            if set(_identifiers(eqs_obj._string[v])) & (set(names) - {v}):
+                raise NotImplementedError("coupled trace equations")
+            a, c = linear_propagator(one, clock.dt)
+            decay += [a[0, 0], c[0]]
+        self.eqs = eqs_obj
+        self._setup(C, np.array(decay, dtype=np.float64), Ap, Am, wmin, wmax, inter, clock, delay_pre, delay_post)
+
+    @staticmethod
+    def _trace_rule(lines, own, other, ns):
+        """(constant, '=' instead of '+=') of 'own (+)= c' next to 'w += other'."""
+        if len(lines) != 2:
+            raise NotImplementedError("STDP code other than a trace update and 'w += trace': %r" % (lines,))
+        rule, wline = None, None
+        for ln in lines:
+            m = re.match(r"^(\w+)\s*(\+=|=)\s*(.+)$", ln)
+            if not m:
+                raise NotImplementedError("STDP statement: %r" % ln)
+            lhs, op, rhs = m.groups()
+            if lhs == "w" and op == "+=" and rhs.strip() == other:
+                wline = ln
+            elif lhs == own and not (_identifiers(rhs) & {own, other, "w"}):
+                rule = (float(eval(rhs, {"__builtins__": {}}, ns)), op == "=")
+            else:
+                raise NotImplementedError("STDP statement: %r" % ln)
+        if rule is None or wline is None:
+            raise NotImplementedError("STDP code other than a trace update and 'w += trace': %r" % (lines,))
+        return rule
+
+    def _setup(self, C, decay, Ap, Am, wmin, wmax, inter, clock, delay_pre, delay_post):
         self.C = C
-        self.taup, self.taum = float(taup), float(taum)
-        self.Ap, self.Am = float(Ap) * wmax, float(Am) * wmax
-        self.wmin, self.wmax = _code_bound(float(wmin)), _code_bound(wmax)
-        self.interactions = _INTER[interactions]
-        self.clock = clock if clock is not None else C.source.clock
+        self.Ap, self.Am = float(Ap), float(Am)
+        self.wmin, self.wmax = _code_bound(float(wmin)), _code_bound(float(wmax))
+        self.interactions = inter
+        self.clock = clock
         from .connections import DelayConnection
         self.delayed = isinstance(C, DelayConnection)
         if self.delayed and (delay_pre is not None or delay_post is not None):
             raise ValueError("Must use delay_pre=delay_post=None for the moment.")
         dt = self.clock.dt
-        eqs = Equations("dA_pre/dt=-A_pre/taup : 1\ndA_post/dt=-A_post/taum : 1", taup=self.taup,
-                        taum=self.taum)
-        # each trace is a separate 1x1 linear group in the reference
-        a_pre, c_pre = linear_propagator(Equations("dA_pre/dt=-A_pre/taup : 1", taup=self.taup), dt)
-        a_post, c_post = linear_propagator(Equations("dA_post/dt=-A_post/taum : 1", taup=self.taup,
-                                                     taum=self.taum), dt)
-        self.decay = np.array([a_pre[0, 0], c_pre[0], a_post[0, 0], c_post[0]], dtype=np.float64)
-        self.eqs = eqs
+        self.decay = decay
         conn_delay = getattr(C, "delay", 0) if isinstance(getattr(C, "delay", 0), int) else 0
         if delay_pre is None and delay_post is None:
             self.pre_delay, self.post_delay = conn_delay, 0
@@ -131,7 +201,36 @@ class ExponentialSTDP(object):
         return self._traces()[1]
 
 
-def STDP(C, eqs, pre, post, wmin=0, wmax=np.inf, level=0, clock=None, delay_pre=None, delay_post=None):
-    """General STDP rules are generated code in the reference (stdp.py:92-449);
-    the engine runs the exponential additive family through ExponentialSTDP."""
-    raise NotImplementedError("use ExponentialSTDP: general STDP code strings are not compiled by the engine")
+class ExponentialSTDP(STDP):
+    """Exponential STDP (stdp.py:452-539): the trace equations and code
+    strings of the reference's ExponentialSTDP, run through STDP.  Additive
+    updates only (multiplicative and mixed raise NotImplementedError)."""
+
+    def __init__(self, C, taup, taum, Ap, Am, interactions="all", wmin=0, wmax=None, update="additive",
+                 delay_pre=None, delay_post=None, clock=None):
+        if wmax is None:
+            raise AttributeError("You must specify the maximum synaptic weight")
+        wmax = float(wmax)
+        eqs = Equations("dA_pre/dt=-A_pre/taup : 1\ndA_post/dt=-A_post/taum : 1", taup=float(taup),
+                        taum=float(taum), wmax=wmax)
+        if interactions == "all":
+            pre, post = "A_pre+=Ap", "A_post+=Am"
+        elif interactions == "nearest":
+            pre, post = "A_pre=Ap", "A_post=Am"
+        elif interactions == "nearest_pre":
+            pre, post = "A_pre=Ap", "A_post=+Am"
+        elif interactions == "nearest_post":
+            pre, post = "A_pre+=Ap", "A_post=Am"
+        else:
+            raise AttributeError("Unknown interaction type " + interactions)
+        if update != "additive":
+            raise NotImplementedError("only additive ExponentialSTDP runs on the engine")
+        Ap = float(Ap) * wmax
+        Am = float(Am) * wmax
+        pre += "\nw+=A_post"
+        post += "\nw+=A_pre"
+        self.taup, self.taum = float(taup), float(taum)
+        STDP.__init__(self, C, eqs=eqs, pre=pre, post=post, wmin=wmin, wmax=wmax, delay_pre=delay_pre,
+                      delay_post=delay_post, clock=clock)
+        # the reference's interaction names (nearest_pre runs as nearest)
+        self.interactions = _INTER[interactions]

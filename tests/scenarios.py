@@ -212,7 +212,23 @@ def cobahh(steps=10000):
     return {"steps": s.copy(), "idx": i.copy(), "golden_steps": g["spk_step"], "golden_idx": g["spk_i"]}
 
 
-def stdp(Nin=400, Nout=32, steps=3000, seed=5, dense=True, rate_lo=5.0, rate_hi=25.0, wdtype=np.float32):
+def _stdp_rule(C, gmax, general, interactions="all"):
+    """ExponentialSTDP, or the same rule written as STDP code strings."""
+    if not general:
+        return b.ExponentialSTDP(C, 20 * ms, 20 * ms, 0.01, -0.0105, wmax=gmax, interactions=interactions)
+    taup = taum = 20 * ms
+    dA_pre, dA_post = 0.01 * gmax, -0.0105 * gmax
+    eqs = b.Equations("""
+    dA_pre/dt = -A_pre/taup : 1
+    dA_post/dt = -A_post/taum : 1""", taup=taup, taum=taum)
+    op_pre = "+=" if interactions in ("all", "nearest_post") else "="
+    op_post = "+=" if interactions == "all" else "="
+    return b.STDP(C, eqs, pre="A_pre %s dA_pre; w += A_post" % op_pre,
+                  post="A_post %s dA_post\nw += A_pre" % op_post, wmax=gmax)
+
+
+def stdp(Nin=400, Nout=32, steps=3000, seed=5, dense=True, rate_lo=5.0, rate_hi=25.0, wdtype=np.float32,
+         general=False):
     """Config 3 in miniature: Poisson inputs -> LIF outputs, all-to-all,
     ExponentialSTDP (examples/plasticity/STDP1.py)."""
     taum, taue = 10 * ms, 5 * ms
@@ -233,7 +249,7 @@ def stdp(Nin=400, Nout=32, steps=3000, seed=5, dense=True, rate_lo=5.0, rate_hi=
     else:
         mask = rng.random((Nin, Nout)) < 0.5
         C.connect(W=W0 * mask)
-    S = b.ExponentialSTDP(C, 20 * ms, 20 * ms, 0.01, -0.0105, wmax=gmax)
+    S = _stdp_rule(C, gmax, general)
     M = b.SpikeMonitor(out)
     Mi = b.SpikeMonitor(inp)
     net = b.Network(inp, out, C, S, M, Mi)
@@ -242,7 +258,7 @@ def stdp(Nin=400, Nout=32, steps=3000, seed=5, dense=True, rate_lo=5.0, rate_hi=
 
 
 def stdp_delay(Nin=400, Nout=40, steps=3000, seed=9, p=0.5, wdtype=np.float64, interactions="all", runs=1,
-               rate_lo=5.0, rate_hi=25.0):
+               rate_lo=5.0, rate_hi=25.0, general=False):
     """ExponentialSTDP on a DelayConnection: Poisson inputs -> LIF outputs
     through float delays (seconds) uniform below max_delay = 5 ms, so that
     the per-synapse lags int((1/dt)*(max_delay-d)) and int((1/dt)*d) are
@@ -264,7 +280,7 @@ def stdp_delay(Nin=400, Nout=40, steps=3000, seed=9, p=0.5, wdtype=np.float64, i
     D = rng.uniform(0.0, 4.99e-3, (Nin, Nout))
     C = b.DelayConnection(inp, out, "ge", max_delay=5 * ms, dtype=wdtype)
     C.connect(inp, out, W0, delay=D)
-    S = b.ExponentialSTDP(C, 20 * ms, 20 * ms, 0.01, -0.0105, wmax=gmax, interactions=interactions)
+    S = _stdp_rule(C, gmax, general, interactions)
     C.compress()
     extra = {"rowptr": np.array(C._rowptr), "cols": np.array(C._cols), "d": C._delay_seconds().copy(),
              "w_init": C._weights().astype(np.float64).copy(), "decay": np.array(S.decay)}
