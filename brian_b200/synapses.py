@@ -327,6 +327,24 @@ class Synapses(object):
             self._vars[name] = np.concatenate([self._vars[name], np.zeros(n)])
         self._changed(delays=True)
 
+    def save_connectivity(self, fn):
+        """Save the synapses' neuron indices and delays (bins) with
+        numpy.savez under the reference's keys (synapses.py:1003-1038):
+        presynaptic, postsynaptic, _delay_pre (one row per pre code),
+        _delay_post."""
+        np.savez(fn, presynaptic=self.presynaptic, postsynaptic=self.postsynaptic,
+                 _delay_pre=self._delay.reshape(1, -1), _delay_post=np.zeros(len(self), dtype=np.int16))
+        return 1
+
+    def load_connectivity(self, fn):
+        """Create the saved synapses (appended after any existing ones) with
+        their delays (synapses.py:1040-1054)."""
+        data = np.load(fn)
+        n0 = len(self)
+        self.create_synapses(data["presynaptic"], data["postsynaptic"])
+        d = np.asarray(data["_delay_pre"])
+        self._delay[n0:] = (d[0] if d.ndim == 2 else d).astype(np.int16)
+
     # ------------------------------------------------------------- indexing
     def synapse_index(self, key):
         return self._synapse_index(key)

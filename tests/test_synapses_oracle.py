@@ -156,3 +156,19 @@ def test_two_runs_continue(oracle_table):
         two = scenarios.synapses_cuba(N=600, steps=600, runs=2)
     assert len(one["spk0.idx"]) > 50
     scenarios.compare(one, two)
+
+
+def test_save_load_connectivity(tmp_path):
+    _fresh()
+    G = b.NeuronGroup(30, model="v : 1")
+    S = b.Synapses(G, G, model="w : 1", pre="v += w")
+    S.connect_random(sparseness=0.3)
+    S.delay = "rand() * 1*ms"
+    fn = str(tmp_path / "conn.npz")
+    S.save_connectivity(fn)
+    T = b.Synapses(G, G, model="w : 1", pre="v += w")
+    T.load_connectivity(fn)
+    np.testing.assert_array_equal(T.presynaptic, S.presynaptic)
+    np.testing.assert_array_equal(T.postsynaptic, S.postsynaptic)
+    np.testing.assert_array_equal(T._delay, S._delay)
+    assert set(np.load(fn).files) == {"presynaptic", "postsynaptic", "_delay_pre", "_delay_post"}
