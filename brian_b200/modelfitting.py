@@ -376,8 +376,9 @@ def modelfitting(model=None, reset=None, threshold=None, refractory=0.0, data=No
     min, max, bound_max]``; ``delays`` and a list-valued ``refractory`` fit
     the spike delay and refractory period.  ``popsize`` candidates per target
     and ``maxiter`` iterations of ``algorithm``: CMAES (the default, as in the
-    reference; one search per target, generations evaluated on the GPU) or
-    PSO (the whole swarm on the GPU).
+    reference; one search per target, generations evaluated on the GPU), GA
+    (one population per target, likewise) or PSO (the whole swarm on the
+    GPU).
 
     ``initial_positions`` ([ndim][groups*popsize], optional) replaces the
     uniform initial draw, e.g. with proposals of a learned model;
