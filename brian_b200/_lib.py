@@ -41,6 +41,7 @@ SIGNATURES = {
     "synapses_add": [_vp, _i32, _i64, _i64, _i32, _i64, _i64, _i64, _vp, _vp, _vp, ct.c_int, _vp, _vp, _vp,
                      _P(_i32)],
     "synapses_set_terms": [_vp, _i32, _vp],
+    "stdp_set_update": [_vp, _i32, ct.c_int, ct.c_int, _dbl],
     "stdp_add_delayed": [_vp, _i32, _vp, _dbl, _dbl, _dbl, _dbl, ct.c_int, _i32, _i32, _vp, _vp, _P(_i32)],
     "stdp_get_traces": [_vp, _i32, _vp, _vp],
     "spikemon_add": [_vp, _i32, _i64, _i64, _i32, _P(_i32)],
@@ -308,6 +309,10 @@ class Runtime(object):
     def synapses_set_terms(self, sid, terms):
         terms = np.ascontiguousarray(terms, dtype=np.float64)
         self._c(self.t.synapses_set_terms(self.h, sid, _ptr(terms)), "synapses_set_terms")
+
+    def stdp_set_update(self, sid, pre_mode, post_mode, wmax_exact):
+        self._c(self.t.stdp_set_update(self.h, sid, int(pre_mode), int(post_mode), float(wmax_exact)),
+                "stdp_set_update")
 
     def stdp_get_traces(self, sid, npre, npost):
         a = np.empty(npre)

@@ -451,19 +451,29 @@ template <typename T> struct PropArgs {
     int parts;                      // row split for the atomic path
     // fused presynaptic STDP (stdp.py:370-414): w[i,:] += A_post; clip
     int stdp; double *A_pre; const double *A_post; double Ap; int pre_set; double wmin, wmax;
+    int wmode; double wx;           // update form of the presynaptic w line (stdp_w)
     unsigned long long *events;     // running count of synaptic events
     int last;
 };
 
+// w (+)= the rule's change, then clip (stdp.py:395-408).  mode 0: w + a;
+// mode 1: w * (1 + a); mode 2: w + (wx - w) * a, wx the exact maximum
+// weight of the code string (stdp.py:510-533); modes 1 and 2 on FP64
+// weights only.
 template <typename T, typename WT>
-__device__ __forceinline__ void stdp_w(WT *w, int64_t k, double add, double wmin, double wmax) {
+__device__ __forceinline__ void stdp_w(WT *w, int64_t k, double add, double wmin, double wmax, int mode = 0,
+                                       double wx = 0.0) {
     if (sizeof(WT) == 4) {
         float x = __double2float_rn(__dadd_rn((double)w[k], add));
         const float lo = __double2float_rn(wmin), hi = __double2float_rn(wmax);
         x = x < lo ? lo : (x > hi ? hi : x);
         w[k] = (WT)x;
     } else {
-        double x = __dadd_rn((double)w[k], add);
+        const double w0 = (double)w[k];
+        double x;
+        if (mode == 1) x = __dmul_rn(w0, __dadd_rn(1.0, add));
+        else if (mode == 2) x = __dadd_rn(w0, __dmul_rn(__dsub_rn(wx, w0), add));
+        else x = __dadd_rn(w0, add);
         x = x < wmin ? wmin : (x > wmax ? wmax : x);
         w[k] = (WT)x;
     }
@@ -507,7 +517,7 @@ __global__ void __launch_bounds__(256) k_prop_atomic(const PropArgs<T> a) {
                         const T wv = (T)W[k];
                         if (RING) atomicAdd(&a.ring[(int64_t)((cur + a.d[k]) % a.md) * a.tn + j], wv);
                         else atomicAdd(&a.sv[j], wv);
-                        if (a.stdp) stdp_w<T, WT>((WT *)a.w, k, a.A_post[j], a.wmin, a.wmax);
+                        if (a.stdp) stdp_w<T, WT>((WT *)a.w, k, a.A_post[j], a.wmin, a.wmax, a.wmode, a.wx);
                     }
                     if (a.stdp && p == 0 && lane == 0)
                         a.A_pre[i] = a.pre_set ? a.Ap : __dadd_rn(a.A_pre[i], a.Ap);
@@ -597,7 +607,7 @@ __global__ void __launch_bounds__(kOrdThreads) k_prop_ordered(const PropArgs<T> 
                         } else {
                             a.sv[j] = rn<T>::add(a.sv[j], wv);
                         }
-                        if (a.stdp) stdp_w<T, WT>(W, k, a.A_post[j], a.wmin, a.wmax);
+                        if (a.stdp) stdp_w<T, WT>(W, k, a.A_post[j], a.wmin, a.wmax, a.wmode, a.wx);
                     }
                     if (blockIdx.x == 0 && tid == 0) {
                         if (a.stdp) a.A_pre[i] = a.pre_set ? a.Ap : __dadd_rn(a.A_pre[i], a.Ap);
@@ -659,7 +669,7 @@ __global__ void __launch_bounds__(kDenseThreads) k_prop_dense(const PropArgs<T> 
                         T wv = (T)W[k];
                         if (a.mod) wv = rn<T>::mul(wv, a.mod[i]);
                         acc = rn<T>::add(acc, wv);
-                        if (a.stdp) stdp_w<T, WT>(W, k, apost, a.wmin, a.wmax);
+                        if (a.stdp) stdp_w<T, WT>(W, k, apost, a.wmin, a.wmax, a.wmode, a.wx);
                     }
                 }
                 if (a.stdp && blockIdx.x == 0)
@@ -728,6 +738,7 @@ struct DelayedPreArgs {
     double *A_pre; double Ap; int pre_set;
     const double *H_post; int hlen; const uint8_t *lag;
     double wmin, wmax;
+    int wmode; double wx;
     int last;
 };
 template <typename WT>
@@ -767,7 +778,7 @@ __global__ void __launch_bounds__(256) k_dstdp_pre(const DelayedPreArgs a) {
                     const int64_t i = base + b - a.so;
                     for (int64_t k = a.rowptr[i] + lane; k < a.rowptr[i + 1]; k += 32) {
                         const int64_t s = hist_slot(hlast, a.lag[k], a.hlen);
-                        stdp_w<double, WT>(W, k, a.H_post[s * a.tn + a.cols[k]], a.wmin, a.wmax);
+                        stdp_w<double, WT>(W, k, a.H_post[s * a.tn + a.cols[k]], a.wmin, a.wmax, a.wmode, a.wx);
                     }
                 }
             }
@@ -804,7 +815,7 @@ __global__ void __launch_bounds__(256) k_stdp_pre(const PropArgs<double> a) {
                     const int64_t r1 = a.dense ? r0 + a.tn : a.rowptr[i + 1];
                     for (int64_t k = r0 + lane; k < r1; k += 32) {
                         const int64_t j = a.dense ? k - r0 : a.cols[k];
-                        stdp_w<double, WT>(W, k, a.A_post[j], a.wmin, a.wmax);
+                        stdp_w<double, WT>(W, k, a.A_post[j], a.wmin, a.wmax, a.wmode, a.wx);
                     }
                     if (lane == 0) a.A_pre[i] = a.pre_set ? a.Ap : __dadd_rn(a.A_pre[i], a.Ap);
                 }
@@ -826,6 +837,7 @@ struct PostArgs {
     // DelayConnection (stdp.py:296-368): w[:,j] += A_pre as recorded lag[p]
     // records back, lag in column order; null on a plain Connection
     const double *H_pre; int hlen; const uint8_t *lagc;
+    int wmode; double wx;           // update form of the postsynaptic w line (stdp_w)
     int last;
 };
 template <typename WT>
@@ -858,13 +870,13 @@ __global__ void __launch_bounds__(256) k_stdp_post(const PostArgs a) {
                 const int64_t j = sp[s];
                 if (a.dense) {
                     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.sn; i += (int64_t)gridDim.x * blockDim.x)
-                        stdp_w<double, WT>(W, i * a.tn + j, a.A_pre[i], a.wmin, a.wmax);
+                        stdp_w<double, WT>(W, i * a.tn + j, a.A_pre[i], a.wmin, a.wmax, a.wmode, a.wx);
                 } else {
                     for (int64_t p = a.colptr[j] + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < a.colptr[j + 1];
                          p += (int64_t)gridDim.x * blockDim.x) {
                         const double add = a.H_pre ? a.H_pre[hist_slot(hlast, a.lagc[p], a.hlen) * a.sn + a.colsrc[p]]
                                                    : a.A_pre[a.colsrc[p]];
-                        stdp_w<double, WT>(W, a.colk[p], add, a.wmin, a.wmax);
+                        stdp_w<double, WT>(W, a.colk[p], add, a.wmin, a.wmax, a.wmode, a.wx);
                     }
                 }
             }

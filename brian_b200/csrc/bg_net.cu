@@ -120,6 +120,7 @@ struct HConn {
 struct HStdp {
     int cid; double a_pre, c_pre, a_post, c_post, Ap, Am, wmin, wmax; int inter; int pre_delay, post_delay;
     double *dApre = nullptr, *dApost = nullptr; bool fused = false;
+    int pre_mode = 0, post_mode = 0; double wx = 0.0;   // update forms of the w lines (stdp_w)
     // DelayConnection: trace histories of hlen steps and per-synapse lags
     bool delayed = false; int hlen = 0; std::vector<uint8_t> lag_pre, lag_post;
     double *dHpre = nullptr, *dHpost = nullptr; uint8_t *dLagPre = nullptr, *dLagPostC = nullptr;
@@ -389,7 +390,7 @@ int build_conn(bg_net *net, int cid) {
         HStdp &s = net->stdps[c.stdp];
         a.stdp = 1; a.A_pre = s.dApre; a.A_post = s.dApost; a.Ap = s.Ap;
         a.pre_set = (s.inter == BG_STDP_NEAREST || s.inter == BG_STDP_NEAREST_PRE);
-        a.wmin = s.wmin; a.wmax = s.wmax;
+        a.wmin = s.wmin; a.wmax = s.wmax; a.wmode = s.pre_mode; a.wx = s.wx;
     }
     if (c.fused_push) return BG_OK;   // pushed by the source group's head kernel
     int mode; int64_t grid;
@@ -426,6 +427,7 @@ int build_stdp_pre_delayed(bg_net *net, int sid) {
     a.so = c.so; a.sn = c.sn; a.tn = c.tn; a.rowptr = c.dRow; a.cols = c.dCols; a.w = c.dW;
     a.A_pre = s.dApre; a.Ap = s.Ap; a.pre_set = (s.inter == BG_STDP_NEAREST || s.inter == BG_STDP_NEAREST_PRE);
     a.H_post = s.dHpost; a.hlen = s.hlen; a.lag = s.dLagPre; a.wmin = s.wmin; a.wmax = s.wmax;
+    a.wmode = s.pre_mode; a.wx = s.wx;
     const int64_t nwords = (c.so + c.sn + 31) / 32 - c.so / 32;
     const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((nwords + 255) / 256, (int64_t)sm_count() * 4));
     const int wb = c.w_bits;
@@ -451,6 +453,7 @@ int build_stdp_pre(bg_net *net, int sid) {
     a.so = c.so; a.sn = c.sn; a.to = c.to; a.tn = c.tn; a.rowptr = c.dRow; a.cols = c.dCols; a.w = c.dW; a.dense = c.dense;
     a.stdp = 1; a.A_pre = s.dApre; a.A_post = s.dApost; a.Ap = s.Ap;
     a.pre_set = (s.inter == BG_STDP_NEAREST || s.inter == BG_STDP_NEAREST_PRE); a.wmin = s.wmin; a.wmax = s.wmax;
+    a.wmode = s.pre_mode; a.wx = s.wx;
     const int64_t nwords = (c.so + c.sn + 31) / 32 - c.so / 32;
     const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((nwords + 255) / 256, (int64_t)sm_count() * 4));
     const int wb = c.w_bits;
@@ -475,7 +478,7 @@ int build_stdp_post(bg_net *net, int sid) {
     a.colptr = c.dColptr; a.colk = c.dColk; a.colsrc = c.dColsrc;
     a.A_post = s.dApost; a.A_pre = s.dApre; a.Am = s.Am;
     a.post_set = (s.inter != BG_STDP_ALL);   // 'nearest_pre' writes A_post=+Am (stdp.py:500-502)
-    a.wmin = s.wmin; a.wmax = s.wmax;
+    a.wmin = s.wmin; a.wmax = s.wmax; a.wmode = s.post_mode; a.wx = s.wx;
     if (s.delayed) { a.H_pre = s.dHpre; a.hlen = s.hlen; a.lagc = s.dLagPostC; }
     const int64_t grid = c.dense ? std::max<int64_t>(1, std::min<int64_t>((c.sn + 255) / 256, (int64_t)sm_count() * 2)) : 8;
     const int wb = c.w_bits;
@@ -1334,6 +1337,18 @@ int bg_stdp_add_delayed(bg_net *n, int32_t cid, const double *decay, double Ap, 
     c.stdp = *sid;
     n->items.push_back({IT_STDP_PRE, *sid});
     n->items.push_back({IT_STDP_POST, *sid});
+    return BG_OK;
+}
+
+int bg_stdp_set_update(bg_net *n, int32_t sid, int pre_mode, int post_mode, double wmax_exact) {
+    if (!n || sid < 0 || sid >= (int32_t)n->stdps.size() || pre_mode < 0 || pre_mode > 2 || post_mode < 0 ||
+        post_mode > 2)
+        return fail(BG_EINVAL, "bg_stdp_set_update");
+    if (n->prepared) return fail(BG_ESTATE, "network already prepared");
+    HStdp &s = n->stdps[sid];
+    if ((pre_mode || post_mode) && n->conns[s.cid].w_bits != 64)
+        return fail(BG_ENOSYS, "multiplicative STDP updates need FP64 weights");
+    s.pre_mode = pre_mode; s.post_mode = post_mode; s.wx = wmax_exact;
     return BG_OK;
 }
 

@@ -81,8 +81,10 @@ class STDP(object):
         if len(names) != 2 or len(vars_pre) != 1 or len(vars_post) != 1 or vars_pre == vars_post:
             raise NotImplementedError("the engine runs STDP with one presynaptic and one postsynaptic trace")
         xp, xq = vars_pre[0], vars_post[0]
-        Ap, pre_set = self._trace_rule(pre_lines, xp, xq, ns)
-        Am, post_set = self._trace_rule(post_lines, xq, xp, ns)
+        Ap, pre_set, pre_mode, wx_pre = self._trace_rule(pre_lines, xp, xq, ns)
+        Am, post_set, post_mode, wx_post = self._trace_rule(post_lines, xq, xp, ns)
+        if wx_pre is not None and wx_post is not None and wx_pre != wx_post:
+            raise NotImplementedError("two different maxima in the soft-bound updates")
         inter = {(False, False): 0, (True, True): 1, (False, True): 3}.get((pre_set, post_set))
         if inter is None:
             raise NotImplementedError("presynaptic '=' with postsynaptic '+=' rule")
@@ -99,27 +101,43 @@ class STDP(object):
             decay += [a[0, 0], c[0]]
         self.eqs = eqs_obj
         self._setup(C, np.array(decay, dtype=np.float64), Ap, Am, wmin, wmax, inter, clock, delay_pre, delay_post)
+        self.pre_mode, self.post_mode = pre_mode, post_mode
+        self.wx = wx_pre if wx_pre is not None else (wx_post if wx_post is not None else 0.0)
 
     @staticmethod
-    def _trace_rule(lines, own, other, ns):
-        """(constant, '=' instead of '+=') of 'own (+)= c' next to 'w += other'."""
+    def _w_line(line, other, ns):
+        """(mode, exact maximum or None) of a w line: 'w += other' (0),
+        'w *= (1+other)' (1), 'w += (wmax-w)*other' (2) (stdp.py:510-533)."""
+        t = line.replace(" ", "")
+        if t == "w+=%s" % other:
+            return 0, None
+        if t in ("w*=(1+%s)" % other, "w*=1+%s" % other):
+            return 1, None
+        m = re.match(r"^w\+=\((.+)-w\)\*%s$" % re.escape(other), t)
+        if m and not (_identifiers(m.group(1)) & {"w", other}):
+            return 2, float(eval(m.group(1), {"__builtins__": {}}, ns))
+        return None
+
+    @classmethod
+    def _trace_rule(cls, lines, own, other, ns):
+        """(constant, '=' instead of '+=', w-line mode, exact maximum) of
+        'own (+)= c' next to a w line."""
         if len(lines) != 2:
-            raise NotImplementedError("STDP code other than a trace update and 'w += trace': %r" % (lines,))
-        rule, wline = None, None
+            raise NotImplementedError("STDP code other than a trace update and a w update: %r" % (lines,))
+        rule, wl = None, None
         for ln in lines:
+            w = cls._w_line(ln, other, ns) if ln.lstrip().startswith("w") else None
+            if w is not None:
+                wl = w
+                continue
             m = re.match(r"^(\w+)\s*(\+=|=)\s*(.+)$", ln)
-            if not m:
-                raise NotImplementedError("STDP statement: %r" % ln)
-            lhs, op, rhs = m.groups()
-            if lhs == "w" and op == "+=" and rhs.strip() == other:
-                wline = ln
-            elif lhs == own and not (_identifiers(rhs) & {own, other, "w"}):
-                rule = (float(eval(rhs, {"__builtins__": {}}, ns)), op == "=")
+            if m and m.group(1) == own and not (_identifiers(m.group(3)) & {own, other, "w"}):
+                rule = (float(eval(m.group(3), {"__builtins__": {}}, ns)), m.group(2) == "=")
             else:
                 raise NotImplementedError("STDP statement: %r" % ln)
-        if rule is None or wline is None:
-            raise NotImplementedError("STDP code other than a trace update and 'w += trace': %r" % (lines,))
-        return rule
+        if rule is None or wl is None:
+            raise NotImplementedError("STDP code other than a trace update and a w update: %r" % (lines,))
+        return rule[0], rule[1], wl[0], wl[1]
 
     def _setup(self, C, decay, Ap, Am, wmin, wmax, inter, clock, delay_pre, delay_post):
         self.C = C
@@ -146,6 +164,8 @@ class STDP(object):
             self.pre_delay, self.post_delay = int(float(delay_pre) / dt), int(float(delay_post) / dt)
         if self.pre_delay < 0 or self.post_delay < 0:
             raise AttributeError("STDP delay larger than the connection delay")
+        self.pre_mode = self.post_mode = 0
+        self.wx = 0.0
         self._binding = None
         self._sid = None
         self._A_pre = np.zeros(len(C.source))
@@ -182,10 +202,14 @@ class STDP(object):
     def _lower(self, rt, cid):
         if self.delayed:
             pre_delay, hist_len, lag_pre, lag_post = self._delayed_schedule()
-            return rt.stdp_add_delayed(cid, self.decay, self.Ap, self.Am, self.wmin, self.wmax, self.interactions,
-                                       pre_delay, hist_len, lag_pre, lag_post)
-        return rt.stdp_add(cid, self.decay, self.Ap, self.Am, self.wmin, self.wmax, self.interactions,
-                           self.pre_delay, self.post_delay)
+            sid = rt.stdp_add_delayed(cid, self.decay, self.Ap, self.Am, self.wmin, self.wmax, self.interactions,
+                                      pre_delay, hist_len, lag_pre, lag_post)
+        else:
+            sid = rt.stdp_add(cid, self.decay, self.Ap, self.Am, self.wmin, self.wmax, self.interactions,
+                              self.pre_delay, self.post_delay)
+        if self.pre_mode or self.post_mode:
+            rt.stdp_set_update(sid, self.pre_mode, self.post_mode, self.wx)
+        return sid
 
     def _traces(self):
         if self._binding is not None:
@@ -223,12 +247,30 @@ class ExponentialSTDP(STDP):
             pre, post = "A_pre+=Ap", "A_post=Am"
         else:
             raise AttributeError("Unknown interaction type " + interactions)
-        if update != "additive":
-            raise NotImplementedError("only additive ExponentialSTDP runs on the engine")
-        Ap = float(Ap) * wmax
-        Am = float(Am) * wmax
-        pre += "\nw+=A_post"
-        post += "\nw+=A_pre"
+        Ap, Am = float(Ap), float(Am)
+        if update == "additive":
+            Ap *= wmax
+            Am *= wmax
+            pre += "\nw+=A_post"
+            post += "\nw+=A_pre"
+        elif update == "multiplicative":
+            pre += "\nw*=(1+A_post)" if Am < 0 else "\nw+=(wmax-w)*A_post"
+            post += "\nw*=(1+A_pre)" if Ap < 0 else "\nw+=(wmax-w)*A_pre"
+        elif update == "mixed":
+            if Am < 0 and Ap > 0:
+                Ap *= wmax
+                pre += "\nw*=(1+A_post)"
+                post += "\nw+=A_pre"
+            elif Am > 0 and Ap < 0:
+                Am *= wmax
+                post += "\nw*=(1+A_pre)"
+                pre += "\nw+=A_post"
+            elif Am > 0:
+                raise AttributeError("There is no depression in STDP rule")
+            else:
+                raise AttributeError("There is no potentiation in STDP rule")
+        else:
+            raise AttributeError("Unknown update type " + update)
         self.taup, self.taum = float(taup), float(taum)
         STDP.__init__(self, C, eqs=eqs, pre=pre, post=post, wmin=wmin, wmax=wmax, delay_pre=delay_pre,
                       delay_post=delay_post, clock=clock)

@@ -206,6 +206,13 @@ BG_API int bg_stdp_add_delayed(bg_net *net, int32_t cid, const double *decay,
                 int interactions, int32_t pre_delay, int32_t hist_len,
                 const uint8_t *lag_pre, const uint8_t *lag_post,
                 int32_t *sid);
+/* Update forms of the rule's w lines (ExponentialSTDP update='multiplicative'
+ * or 'mixed', stdp.py:510-533): mode 0 w += a (the default), mode 1
+ * w *= (1 + a), mode 2 w += (wmax_exact - w) * a, then the clip; pre_mode
+ * for the presynaptic line (a = A_post), post_mode for the postsynaptic one
+ * (a = A_pre).  Modes 1 and 2 need FP64 weights. */
+BG_API int bg_stdp_set_update(bg_net *net, int32_t sid, int pre_mode, int post_mode,
+                double wmax_exact);
 BG_API int bg_stdp_get_traces(bg_net *net, int32_t sid, double *a_pre,
                        double *a_post);
 

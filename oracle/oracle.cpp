@@ -27,6 +27,10 @@
  *   delayed propagation ........... delayconnection.py:132-206 (ring row
  *                                   (cur + d) % md), delivery :112-121
  *   STDP pre/post updaters ........ stdp.py:31-54, 370-414, 452-539
+ *   STDP on a DelayConnection ..... stdp.py:57-89, 296-368; RecentStateMonitor
+ *                                   monitor.py:991-1099
+ *   Synapses / SpikeQueue ......... synapses/synapses.py:808-827;
+ *                                   synapses/spikequeue.py:209-216, 270-363
  *   SpikeMonitor .................. monitor.py:156-166
  *   StateMonitor .................. monitor.py:824-842
  *   EmpiricalThreshold ............ threshold.py:449-457 (LS[0:refractory])
@@ -117,6 +121,9 @@ struct Stdp {
     int32_t cid; double a_pre, c_pre, a_post, c_post, Ap, Am, wmin, wmax;
     int inter; int32_t pre_delay, post_delay;
     std::vector<double> A_pre, A_post;
+    /* update forms of the w lines: 0 w += a, 1 w *= (1 + a), 2 w += (wx - w)*a
+     * (ExponentialSTDP update='multiplicative'/'mixed', stdp.py:510-533) */
+    int pre_mode = 0, post_mode = 0; double wx = 0.0;
     /* DelayConnection (stdp.py:296-368): RecentStateMonitors of both traces
      * (monitor.py:991-1099): M slots [M][n], written at the end of each step
      * at current_time_index, which then advances modulo M */
@@ -450,6 +457,21 @@ static void synapses_deliver(or_net *n, int32_t gid) {
         y.cur = (y.cur + 1) % y.L;
     }
 }
+int or_stdp_set_update(or_net *n, int32_t sid, int pre_mode, int post_mode, double wmax_exact) {
+    if (!n || sid < 0 || sid >= (int32_t)n->stdps.size() || pre_mode < 0 || pre_mode > 2 || post_mode < 0 ||
+        post_mode > 2)
+        return fail(OR_EINVAL, "stdp_set_update");
+    Stdp &s = n->stdps[sid];
+    if ((pre_mode || post_mode) && n->conns[s.cid].w_bits != 64) return fail(OR_ENOSYS, "multiplicative STDP on FP32 weights");
+    s.pre_mode = pre_mode; s.post_mode = post_mode; s.wx = wmax_exact;
+    return OR_OK;
+}
+/* the w line of an STDP code string, as numpy evaluates it */
+static inline double wupd(double w, double a, int mode, double wx) {
+    if (mode == 1) return w * (1.0 + a);
+    if (mode == 2) return w + (wx - w) * a;
+    return w + a;
+}
 /* get_past_values_sequence (monitor.py:1088-1096): the slot of the value
  * recorded `lag` records before the last one */
 static inline size_t past_slot(const Stdp &s, int lag) {
@@ -702,7 +724,7 @@ static void step(or_net *n, int64_t cs) {
             for (int32_t i : spk)
                 for (int64_t k = c.rowptr[i]; k < c.rowptr[i + 1]; ++k) {
                     const double add = s.H_post[past_slot(s, s.lag_pre[k]) * c.tn + c.cols[k]];
-                    if (c.w_bits == 64) c.w64[k] = clipd(c.w64[k] + add, s.wmin, s.wmax);
+                    if (c.w_bits == 64) c.w64[k] = clipd(wupd(c.w64[k], add, s.pre_mode, s.wx), s.wmin, s.wmax);
                     else c.w32[k] = clipf((float)((double)c.w32[k] + add), (float)s.wmin, (float)s.wmax);
                 }
         } else if (it.kind == IT_STDP_POST && n->stdps[it.id].delayed) {
@@ -715,7 +737,7 @@ static void step(or_net *n, int64_t cs) {
                 for (int64_t p = c.colptr[j]; p < c.colptr[j + 1]; ++p) {
                     const int64_t k = c.colk[p]; const int32_t i = c.colsrc[p];
                     const double add = s.H_pre[past_slot(s, s.lag_post[k]) * c.sn + i];
-                    if (c.w_bits == 64) c.w64[k] = clipd(c.w64[k] + add, s.wmin, s.wmax);
+                    if (c.w_bits == 64) c.w64[k] = clipd(wupd(c.w64[k], add, s.post_mode, s.wx), s.wmin, s.wmax);
                     else c.w32[k] = clipf((float)((double)c.w32[k] + add), (float)s.wmin, (float)s.wmax);
                 }
         } else if (it.kind == IT_STDP_PRE) {
@@ -726,13 +748,13 @@ static void step(or_net *n, int64_t cs) {
                 if (c.dense) {
                     for (int64_t j = 0; j < c.tn; ++j) {
                         size_t k = (size_t)i * c.tn + j;
-                        if (c.w_bits == 64) c.w64[k] = clipd(c.w64[k] + s.A_post[j], s.wmin, s.wmax);
+                        if (c.w_bits == 64) c.w64[k] = clipd(wupd(c.w64[k], s.A_post[j], s.pre_mode, s.wx), s.wmin, s.wmax);
                         else c.w32[k] = clipf((float)((double)c.w32[k] + s.A_post[j]), (float)s.wmin, (float)s.wmax);
                     }
                 } else {
                     for (int64_t k = c.rowptr[i]; k < c.rowptr[i + 1]; ++k) {
                         int32_t j = c.cols[k];
-                        if (c.w_bits == 64) c.w64[k] = clipd(c.w64[k] + s.A_post[j], s.wmin, s.wmax);
+                        if (c.w_bits == 64) c.w64[k] = clipd(wupd(c.w64[k], s.A_post[j], s.pre_mode, s.wx), s.wmin, s.wmax);
                         else c.w32[k] = clipf((float)((double)c.w32[k] + s.A_post[j]), (float)s.wmin, (float)s.wmax);
                     }
                 }
@@ -745,13 +767,13 @@ static void step(or_net *n, int64_t cs) {
                 if (c.dense) {
                     for (int64_t i = 0; i < c.sn; ++i) {
                         size_t k = (size_t)i * c.tn + j;
-                        if (c.w_bits == 64) c.w64[k] = clipd(c.w64[k] + s.A_pre[i], s.wmin, s.wmax);
+                        if (c.w_bits == 64) c.w64[k] = clipd(wupd(c.w64[k], s.A_pre[i], s.post_mode, s.wx), s.wmin, s.wmax);
                         else c.w32[k] = clipf((float)((double)c.w32[k] + s.A_pre[i]), (float)s.wmin, (float)s.wmax);
                     }
                 } else {
                     for (int64_t p = c.colptr[j]; p < c.colptr[j + 1]; ++p) {
                         int64_t k = c.colk[p]; int32_t i = c.colsrc[p];
-                        if (c.w_bits == 64) c.w64[k] = clipd(c.w64[k] + s.A_pre[i], s.wmin, s.wmax);
+                        if (c.w_bits == 64) c.w64[k] = clipd(wupd(c.w64[k], s.A_pre[i], s.post_mode, s.wx), s.wmin, s.wmax);
                         else c.w32[k] = clipf((float)((double)c.w32[k] + s.A_pre[i]), (float)s.wmin, (float)s.wmax);
                     }
                 }

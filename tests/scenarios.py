@@ -212,10 +212,11 @@ def cobahh(steps=10000):
     return {"steps": s.copy(), "idx": i.copy(), "golden_steps": g["spk_step"], "golden_idx": g["spk_i"]}
 
 
-def _stdp_rule(C, gmax, general, interactions="all"):
+def _stdp_rule(C, gmax, general, interactions="all", update="additive"):
     """ExponentialSTDP, or the same rule written as STDP code strings."""
     if not general:
-        return b.ExponentialSTDP(C, 20 * ms, 20 * ms, 0.01, -0.0105, wmax=gmax, interactions=interactions)
+        return b.ExponentialSTDP(C, 20 * ms, 20 * ms, 0.01, -0.0105, wmax=gmax, interactions=interactions,
+                                 update=update)
     taup = taum = 20 * ms
     dA_pre, dA_post = 0.01 * gmax, -0.0105 * gmax
     eqs = b.Equations("""
@@ -228,7 +229,7 @@ def _stdp_rule(C, gmax, general, interactions="all"):
 
 
 def stdp(Nin=400, Nout=32, steps=3000, seed=5, dense=True, rate_lo=5.0, rate_hi=25.0, wdtype=np.float32,
-         general=False):
+         general=False, update="additive"):
     """Config 3 in miniature: Poisson inputs -> LIF outputs, all-to-all,
     ExponentialSTDP (examples/plasticity/STDP1.py)."""
     taum, taue = 10 * ms, 5 * ms
@@ -249,16 +250,20 @@ def stdp(Nin=400, Nout=32, steps=3000, seed=5, dense=True, rate_lo=5.0, rate_hi=
     else:
         mask = rng.random((Nin, Nout)) < 0.5
         C.connect(W=W0 * mask)
-    S = _stdp_rule(C, gmax, general)
+    S = _stdp_rule(C, gmax, general, update=update)
+    C.compress()
+    w_init = C._weights().astype(np.float64).copy()
     M = b.SpikeMonitor(out)
     Mi = b.SpikeMonitor(inp)
     net = b.Network(inp, out, C, S, M, Mi)
     net.run(steps * 0.1 * ms)
-    return _result(net, groups=[out], spikemons=[M, Mi], conns=[C], stdps=[S])
+    res = _result(net, groups=[out], spikemons=[M, Mi], conns=[C], stdps=[S])
+    res["w_init"], res["decay"] = w_init, np.array(S.decay)
+    return res
 
 
 def stdp_delay(Nin=400, Nout=40, steps=3000, seed=9, p=0.5, wdtype=np.float64, interactions="all", runs=1,
-               rate_lo=5.0, rate_hi=25.0, general=False):
+               rate_lo=5.0, rate_hi=25.0, general=False, update="additive"):
     """ExponentialSTDP on a DelayConnection: Poisson inputs -> LIF outputs
     through float delays (seconds) uniform below max_delay = 5 ms, so that
     the per-synapse lags int((1/dt)*(max_delay-d)) and int((1/dt)*d) are
@@ -280,7 +285,7 @@ def stdp_delay(Nin=400, Nout=40, steps=3000, seed=9, p=0.5, wdtype=np.float64, i
     D = rng.uniform(0.0, 4.99e-3, (Nin, Nout))
     C = b.DelayConnection(inp, out, "ge", max_delay=5 * ms, dtype=wdtype)
     C.connect(inp, out, W0, delay=D)
-    S = _stdp_rule(C, gmax, general, interactions)
+    S = _stdp_rule(C, gmax, general, interactions, update)
     C.compress()
     extra = {"rowptr": np.array(C._rowptr), "cols": np.array(C._cols), "d": C._delay_seconds().copy(),
              "w_init": C._weights().astype(np.float64).copy(), "decay": np.array(S.decay)}

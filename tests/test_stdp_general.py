@@ -51,7 +51,7 @@ def test_engine_parameters():
     assert isinstance(E, b.STDP)
 
 
-@pytest.mark.parametrize("pre,post", [("A_pre+=0.01; w*=(1+A_post)", "A_post+=-0.01; w+=A_pre"),
+@pytest.mark.parametrize("pre,post", [("A_pre+=0.01; w*=(2+A_post)", "A_post+=-0.01; w+=A_pre"),
                                       ("A_pre+=0.01; w+=A_post; w+=0.1", "A_post+=-0.01; w+=A_pre"),
                                       ("A_pre=0.01; w+=A_post", "A_post+=-0.01; w+=A_pre"),
                                       ("A_pre+=A_pre; w+=A_post", "A_post+=-0.01; w+=A_pre")])
