@@ -227,8 +227,8 @@ class STDP(object):
 
 class ExponentialSTDP(STDP):
     """Exponential STDP (stdp.py:452-539): the trace equations and code
-    strings of the reference's ExponentialSTDP, run through STDP.  Additive
-    updates only (multiplicative and mixed raise NotImplementedError)."""
+    strings of the reference's ExponentialSTDP, run through STDP; additive,
+    multiplicative and mixed updates (the last two on FP64 weights)."""
 
     def __init__(self, C, taup, taum, Ap, Am, interactions="all", wmin=0, wmax=None, update="additive",
                  delay_pre=None, delay_post=None, clock=None):

@@ -145,6 +145,23 @@ def test_stdp_delay_bit_exact(oracle_table, gpu_table, wdtype, interactions, run
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("dense,update", [(True, "multiplicative"), (False, "multiplicative"), (True, "mixed"),
+                                          (False, "mixed")])
+def test_stdp_update_forms_bit_exact(oracle_table, gpu_table, dense, update):
+    """ExponentialSTDP update='multiplicative' / 'mixed' (FP64 weights)."""
+    ref, gpu = _both(scenarios.stdp, oracle_table, dense=dense, wdtype=np.float64, update=update)
+    assert len(ref["spk0.idx"]) > 0
+    scenarios.compare(ref, gpu)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("update", ["multiplicative", "mixed"])
+def test_stdp_delay_update_forms_bit_exact(oracle_table, gpu_table, update):
+    ref, gpu = _both(scenarios.stdp_delay, oracle_table, update=update)
+    scenarios.compare(ref, gpu)
+
+
+@pytest.mark.gpu
 def test_stdp_delay_large_bit_exact(oracle_table, gpu_table):
     """More sources than one block's words, several spikes per step."""
     ref, gpu = _both(scenarios.stdp_delay, oracle_table, Nin=5000, Nout=300, p=0.1, steps=1500)
