@@ -64,9 +64,11 @@ class STDP(object):
     postsynaptic group and runs the code strings in SpikeMonitors.  The
     engine runs the family ExponentialSTDP generates: one linear trace
     equation per side, a presynaptic code of ``x_pre += c`` (or ``= c``) and
-    ``w += x_post``, a postsynaptic code of ``x_post += c`` (or ``= c``) and
-    ``w += x_pre``; weights clipped to [wmin, wmax] after each update.  Other
-    code raises NotImplementedError.  Constants in the code are looked up
+    a w line in ``x_post``, a postsynaptic code of ``x_post += c`` (or
+    ``= c``) and a w line in ``x_pre``, each w line one of ``w += x``,
+    ``w *= (1+x)``, ``w += (wmax-w)*x`` (the last two on FP64 weights);
+    weights clipped to [wmin, wmax] after each update.  Other code raises
+    NotImplementedError.  Constants in the code are looked up
     in the caller's namespace (``level`` frames up), as the reference does."""
 
     def __init__(self, C, eqs, pre, post, wmin=0, wmax=np.inf, level=0, clock=None, delay_pre=None,
