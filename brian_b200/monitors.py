@@ -13,7 +13,7 @@ import numpy as np
 from .clock import guess_clock
 
 __all__ = ["SpikeMonitor", "StateMonitor", "SpikeCounter", "PopulationSpikeCounter",
-           "PopulationRateMonitor", "CoincidenceCounter", "MultiStateMonitor"]
+           "PopulationRateMonitor", "CoincidenceCounter", "MultiStateMonitor", "RecentStateMonitor"]
 
 
 class SpikeMonitor(object):
@@ -308,3 +308,96 @@ class CoincidenceCounter(SpikeMonitor):
     @property
     def target_length(self):
         return self._count()[2]
+
+
+class RecentStateMonitor(StateMonitor):
+    """StateMonitor of the most recent ``duration`` (monitor.py:991-1141).
+
+    Records like StateMonitor (``record`` defaults to True); the reference's
+    ring of ``num_duration = int(duration / (timestep*dt)) + 1`` slots, where
+    record r sits in slot r mod num_duration, is a view over the records.
+    ``values``/``times`` are sorted by time (values [time][neuron], as in the
+    reference); ``unsorted_values``/``unsorted_times`` are the ring itself;
+    ``get_past_values`` reads the slot ``(current_time_index - 1 -
+    int((1/dt) * times)) mod num_duration`` (monitor.py:1078-1096)."""
+
+    def __init__(self, P, varname, duration=5e-3, clock=None, record=True, timestep=1, when="end"):
+        StateMonitor.__init__(self, P, varname, clock=clock, record=record, timestep=timestep, when=when)
+        self.duration = float(duration)
+        self.num_duration = int(self.duration / (self.timestep * self.clock.dt)) + 1
+        self._invtargetdt = 1.0 / self.clock.dt
+
+    def _ring(self):
+        s, v = self._record()
+        M, R = self.num_duration, len(s)
+        vals = np.zeros((M, v.shape[1]))
+        times = np.zeros(M)
+        k = np.arange(max(0, R - M), R)
+        vals[k % M] = v[k]
+        times[k % M] = s[k] * self.clock.dt
+        return vals, times, R % M, R >= M
+
+    @property
+    def current_time_index(self):
+        return self._ring()[2]
+
+    @property
+    def has_looped(self):
+        return self._ring()[3]
+
+    def sorted_times_indices(self):
+        _, times, cur, looped = self._ring()
+        if not looped:
+            return np.arange(cur)
+        return np.argsort(times)
+
+    @property
+    def unsorted_values(self):
+        return self._ring()[0]
+
+    unsorted_values_ = unsorted_values
+
+    def getvalues(self):
+        return self._ring()[0]
+
+    getvalues_ = getvalues
+
+    @property
+    def unsorted_times(self):
+        return self._ring()[1]
+
+    unsorted_times_ = unsorted_times
+
+    def get_sorted_times(self):
+        return self._ring()[1][self.sorted_times_indices()]
+
+    def get_sorted_values(self):
+        return self._ring()[0][self.sorted_times_indices(), :]
+
+    times = property(get_sorted_times)
+    times_ = times
+    values = property(get_sorted_values)
+    values_ = values
+
+    def __getitem__(self, i):
+        if self.record is False:
+            raise IndexError("Neuron %d was not recorded." % i)
+        pos = np.nonzero(self._indices == i)[0]
+        if len(pos) == 0:
+            raise IndexError("Neuron %d was not recorded." % i)
+        return self.get_sorted_values()[:, pos[0]]
+
+    def get_past_values(self, times):
+        vals, _, cur, _ = self._ring()
+        idx = (cur - 1 - np.array(self._invtargetdt * np.asarray(times), dtype=int)) % self.num_duration
+        return vals[idx, np.arange(vals.shape[1])]
+
+    def get_past_values_sequence(self, times_seq):
+        if len(times_seq) == 0:
+            return []
+        vals, _, cur, _ = self._ring()
+        out = []
+        for times in times_seq:
+            idx = (cur - 1 - np.array(self._invtargetdt * np.asarray(times), dtype=int)) % self.num_duration
+            out.append(vals[idx, np.arange(vals.shape[1])])
+        return out
