@@ -278,20 +278,27 @@ class Synapses(object):
         raise NotImplementedError("synapse creation from %r" % type(value))
 
     def connect_random(self, pre=None, post=None, sparseness=None):
-        """Each presynaptic neuron gets Binomial(m, p) targets drawn without
-        replacement (synapses.py:845-885)."""
+        """Each presynaptic neuron gets Binomial(m, p) distinct targets drawn
+        uniformly (synapses.py:845-885)."""
         self._check_open()
         pre_idx = _group_range(self.source if pre is None else pre, self.source)
         post_idx = _group_range(self.target if post is None else post, self.target)
         m = len(post_idx)
-        pres, posts = [], []
-        for i in pre_idx:
-            k = int(np.random.binomial(m, sparseness))
-            sel = np.random.choice(m, k, replace=False)
-            pres.append(np.full(k, i, dtype=np.int64))
-            posts.append(post_idx[sel])
-        self._create(np.concatenate(pres) if pres else np.zeros(0, np.int64),
-                     np.concatenate(posts) if posts else np.zeros(0, np.int64))
+        ks = np.random.binomial(m, sparseness, size=len(pre_idx)).astype(np.int64)
+        rows = np.repeat(np.arange(len(pre_idx)), ks)
+        # k distinct targets per row: draw with replacement for all rows at
+        # once, then redraw the repeats within a row until none is left
+        sel = np.random.randint(0, max(m, 1), size=len(rows)).astype(np.int64) if m else np.zeros(0, np.int64)
+        while len(sel):
+            key = rows * max(m, 1) + sel
+            order = np.argsort(key, kind="stable")
+            dup = np.zeros(len(sel), dtype=bool)
+            dup[order[1:]] = key[order[1:]] == key[order[:-1]]
+            nd = int(dup.sum())
+            if nd == 0:
+                break
+            sel[dup] = np.random.randint(0, m, size=nd)
+        self._create(pre_idx[rows], post_idx[sel])
 
     def connect_one_to_one(self, pre=None, post=None):
         self._check_open()
