@@ -35,7 +35,8 @@ from .codegen import generate_model_code, SCHEMES
 from .equations import Equations
 from .statistics import firing_rate, gamma_factor
 
-__all__ = ["GPUModelFitting", "modelfitting", "get_spikes", "predict", "print_table", "PSO", "GA", "CMAES",
+__all__ = ["GPUModelFitting", "modelfitting", "distributed_modelfitting", "get_spikes", "predict", "print_table",
+           "PSO", "GA", "CMAES",
            "OptimizationResult", "euler_scheme", "rk2_scheme", "exp_euler_scheme", "MAXCPU", "MAXGPU"]
 
 # integration scheme names (experimental/codegen/integration_schemes.py)
@@ -524,6 +525,47 @@ def _fit_ga(prob, names, lo, hi, imin, imax, groups, popsize, maxiter, rng, optp
     if groups == 1:
         return OptimizationResult(best_pos[0], float(best_f[0]), info)
     return OptimizationResult(best_pos, list(map(float, best_f)), info)
+
+
+def distributed_modelfitting(data=None, input=None, process_group=None, **kwargs):
+    """modelfitting with the targets split over the ranks of a
+    torch.distributed job, one GPU per rank (the reference spreads a fit
+    over GPUs and machines through playdoh, modelfitting.py:446-518).
+
+    Targets are independent groups of the search, so nothing is exchanged
+    during the fit: rank r fits targets [r*G/W, (r+1)*G/W) on device
+    LOCAL_RANK (unless ``device`` is given) with the same arguments, and
+    the results are gathered (``all_gather_object``) into one
+    OptimizationResult in target order on every rank; ``info["ranks"]``
+    holds each rank's own info.  ``data`` is (target index, spike time)
+    pairs; ``input`` one shared trace or one trace per target."""
+    import os
+    import torch.distributed as dist
+    world = dist.get_world_size(process_group)
+    rank = dist.get_rank(process_group)
+    trains = _split_data(data)
+    G = len(trains)
+    lo, hi = rank * G // world, (rank + 1) * G // world
+    per_target = isinstance(input, (list, tuple)) and len(input) and np.ndim(input[0]) == 1
+    pos, fit, info = [], [], None
+    if hi > lo:
+        pairs = np.array([(k, t) for k, j in enumerate(range(lo, hi)) for t in trains[j]], dtype=np.float64)
+        inp = list(input[lo:hi]) if per_target else input
+        kw = dict(kwargs)
+        kw.setdefault("device", int(os.environ.get("LOCAL_RANK", "0")))
+        res = modelfitting(data=pairs, input=inp, **kw)
+        pos = res.best_pos if isinstance(res.best_pos, list) else [res.best_pos]
+        fit = res.best_fit if isinstance(res.best_fit, list) else [res.best_fit]
+        info = res.info
+    parts = [None] * world
+    dist.all_gather_object(parts, (lo, pos, fit, info), group=process_group)
+    parts.sort(key=lambda x: x[0])
+    all_pos = [p for part in parts for p in part[1]]
+    all_fit = [f for part in parts for f in part[2]]
+    ginfo = {"ranks": [part[3] for part in parts], "world_size": world, "groups": G}
+    if G == 1:
+        return OptimizationResult(all_pos[0], all_fit[0], ginfo)
+    return OptimizationResult(all_pos, all_fit, ginfo)
 
 
 def get_spikes(model=None, reset=None, threshold=None, input=None, input_var="I", dt=None, initial_values=None,
