@@ -172,3 +172,36 @@ def test_save_load_connectivity(tmp_path):
     np.testing.assert_array_equal(T.postsynaptic, S.postsynaptic)
     np.testing.assert_array_equal(T._delay, S._delay)
     assert set(np.load(fn).files) == {"presynaptic", "postsynaptic", "_delay_pre", "_delay_post"}
+
+
+def test_edge_cases(oracle_table):
+    _fresh()
+    src = b.SpikeGeneratorGroup(2, [(0, 1 * DT), (1, 2 * DT)])
+    P = b.NeuronGroup(6, model="v : 1")
+    empty = b.Synapses(src, P, model="w : 1", pre="v += w")            # no synapses at all
+    sub = b.Synapses(src, P[2:5], model="w : 1", pre="v -= 2*w")       # a subgroup as target
+    sub[0, 1] = True                                                   # -> neuron 3 of P
+    sub[1, 2] = True                                                   # -> neuron 4 of P
+    sub.w = [0.25, 0.5]
+    M = b.StateMonitor(P, "v", record=True)
+    net = b.Network(src, P, empty, sub, M)
+    with engine(oracle_table):
+        net.run(6 * DT)
+        _, vals = M._record()
+    vals = np.asarray(vals).reshape(6, 6)
+    want = np.zeros((6, 6))
+    want[2:, 3] = -0.5          # spike of step 1, delay 0 -> applied at step 2
+    want[3:, 4] = -1.0          # spike of step 2 -> step 3
+    np.testing.assert_array_equal(vals, want)
+
+
+def test_synapses_before_target_refused(oracle_table):
+    _fresh()
+    G = b.NeuronGroup(3, model="v : 1")
+    H = b.NeuronGroup(3, model="v : 1")
+    S = b.Synapses(G, H, model="w : 1", pre="v += w")
+    S[:, :] = True
+    net = b.Network(G, S, H)
+    with pytest.raises(NotImplementedError):
+        with engine(oracle_table):
+            net.run(2 * DT)
