@@ -95,8 +95,8 @@ template <typename T> struct HeadArgs {
 // Row j of the exact linear update: ((0 + A[j][k0] s_k0) + A[j][k1] s_k1) +
 // ... over the nonzero coefficients (bit j*NV+k of anz), left to right, then
 // + C[j] when nonzero (bit j of cnz).  Exact zeros are skipped: only the sign
-// of an exact-zero result can differ from summing them (SURVEY note N1), and
-// the CPU restatement uses the same rule.  The masks are kernel parameters,
+// of an exact-zero result can differ from summing them (x + 0*y equals x
+// for every finite x except -0), and the CPU restatement uses the same rule.  The masks are kernel parameters,
 // so every test is uniform across the grid.
 template <typename T, int NV>
 __device__ __forceinline__ T linear_row(const T *A, const T *C, uint64_t anz, uint32_t cnz, const T (&s)[NV], int j) {

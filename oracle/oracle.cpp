@@ -619,8 +619,9 @@ static void step(or_net *n, int64_t cs) {
                 for (int k = 0; k < m; ++k) s[k] = g.S[(size_t)k * N + i];
                 /* x_j = ((0 + A[j][k0] s_k0) + A[j][k1] s_k1) + ... over the
                  * nonzero A[j][k] left to right, then + C[j] when nonzero.
-                 * Skipping exact zeros of A and C (SURVEY note N1) and starting
-                 * from +0 change nothing but the sign of an exact-zero result. */
+                 * Skipping exact zeros of A and C (the reference's dot product
+                 * adds them) and starting from +0 change nothing but the sign
+                 * of an exact-zero result. */
                 for (int j = 0; j < m; ++j) {
                     double acc = 0.0;
                     for (int k = 0; k < m; ++k) {
