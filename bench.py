@@ -524,6 +524,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--neurons", type=int, default=N_NEURONS)
     ap.add_argument("--no-fit", action="store_true", help="skip the model-fitting half of the metric")
+    ap.add_argument("--no-synapses", action="store_true", help="skip the Synapses measurement")
     ap.add_argument("--persist-threads", type=int, default=None, choices=[256, 512],
                     help="threads per block of the persistent kernel (default: automatic)")
     ap.add_argument("--fit-targets", type=int, default=256)
@@ -641,6 +642,15 @@ def main():
     if rank == 0 and world == 1 and not args.no_fit:
         fitting = fitting_bench(args)
 
+    # Synapses (static, queue-ordered delivery): the --profile-case synapses
+    # workload, reported beside the headline (after its timed region)
+    synapses = None
+    if rank == 0 and world == 1 and not args.no_synapses:
+        try:
+            synapses = synapses_case(args.seed)
+        except Exception as e:  # the headline line is printed either way
+            synapses = {"error": "%s: %s" % (type(e).__name__, e)}
+
     if rank == 0:
         line = {"metric": "synaptic events/s (CUBA-262k)", "value": value, "unit": "events/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps,
@@ -657,7 +667,7 @@ def main():
                                  "(2 x 28 MB) stay L2-resident"},
                 "mean_rate_hz": rate_hz, "events_timed": total_events, "wall_s": wall,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-                "clocks": clk.summary(), "fitting": fitting}
+                "clocks": clk.summary(), "fitting": fitting, "synapses": synapses}
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist
