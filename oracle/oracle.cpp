@@ -461,6 +461,7 @@ int or_stdp_set_update(or_net *n, int32_t sid, int pre_mode, int post_mode, doub
     if (!n || sid < 0 || sid >= (int32_t)n->stdps.size() || pre_mode < 0 || pre_mode > 2 || post_mode < 0 ||
         post_mode > 2)
         return fail(OR_EINVAL, "stdp_set_update");
+    if (n->prepared) return fail(OR_ESTATE, "network already prepared");
     Stdp &s = n->stdps[sid];
     if ((pre_mode || post_mode) && n->conns[s.cid].w_bits != 64) return fail(OR_ENOSYS, "multiplicative STDP on FP32 weights");
     s.pre_mode = pre_mode; s.post_mode = post_mode; s.wx = wmax_exact;
