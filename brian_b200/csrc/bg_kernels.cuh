@@ -893,10 +893,11 @@ __global__ void __launch_bounds__(256) k_stdp_post(const PostArgs a) {
 
 // Synapses delivery (synapses.py:808-827, SpikeQueue of spikequeue.py:
 // 69-330).  An event of a spike at step s through a synapse of delay d is
-// applied at step s + 1 + d, after the target group's update; the events
-// reaching one target are applied in queue order.  Each target's incoming
-// synapses are stored in that order (delay descending, then source, then
-// synapse index) as words source | (d + 1) << 24.  A block takes a tile of
+// applied at step s + d in the 'synapses' slot (after the connections,
+// before the resets, network.py:365-380); the events reaching one target
+// are applied in queue order.  Each target's incoming synapses are stored
+// in that order (delay descending, then source, then synapse index) as
+// words source | (d + 1) << 24 (a zero word is padding).  A block takes a tile of
 // kSynTile consecutive targets: phase A tests the tile's words (all
 // threads, kSynUnroll independent loads in flight each) against the
 // sources' spike history and leaves one hit bit per synapse in shared
@@ -954,9 +955,9 @@ static __global__ void __launch_bounds__(kSynThreads) k_syn_deliver(const SynArg
                 uint32_t hb[kSynUnroll];
 #pragma unroll
                 for (int u = 0; u < kSynUnroll; ++u) {
-                    const int lag = (int)(wd[u] >> 24);
+                    const int lag = (int)(wd[u] >> 24) - 1;
                     hb[u] = 0u;
-                    if (lag > 0 && nstep >= lag) {
+                    if (lag >= 0 && nstep >= lag) {
                         const int64_t src = a.so + (int64_t)(wd[u] & 0xFFFFFFu);
                         int row = row0 - lag;
                         row += row < 0 ? a.depth : 0;

@@ -1465,6 +1465,15 @@ static int prepare_impl(bg_net *n) {
     }
     for (auto &m : n->smons) { HGroup &g = n->groups[m.gid]; g.depth = std::max(g.depth, m.delay + 1); }
     for (auto &y : n->syns) { HGroup &g = n->groups[y.src]; g.depth = std::max(g.depth, y.dmax + 2); }
+    // the reference adds a DelayConnection's due row (after_connections)
+    // before the Synapses slot; here the row is added in the next step's
+    // head kernel, after the Synapses kernel: refuse targets fed by both
+    for (const auto &y : n->syns)
+        for (const auto &c : n->conns)
+            if (c.hetero && c.tgt == y.tgt && c.to < y.to + y.tn && y.to < c.to + c.tn)
+                for (int v : y.op_var)
+                    if (v == c.var)
+                        return fail(BG_ENOSYS, "a variable fed by both a DelayConnection and Synapses");
     // chunk length bounded by monitor buffer sizes
     int64_t chunk = kChunkSteps;
     for (auto &m : n->smons) chunk = std::min<int64_t>(chunk, std::max<int64_t>(kGraphSteps, (int64_t)(1 << 25) / std::max<int64_t>(1, m.n)));
@@ -1649,9 +1658,6 @@ static int prepare_impl(bg_net *n) {
     for (size_t gi = 0; gi < n->groups.size(); ++gi) {
         st = n->precision == 64 ? build_group<double>(n, (int)gi) : build_group<float>(n, (int)gi);
         if (st) return st;
-        // Synapses update in the groups slot, after their target group
-        for (size_t yi = 0; yi < n->syns.size(); ++yi)
-            if (n->syns[yi].tgt == (int)gi) { st = build_syn(n, (int)yi); if (st) return st; }
     }
     for (size_t si = 0; si < n->stdps.size(); ++si) { st = build_decay(n, (int)si); if (st) return st; }
     for (const Item &it : n->items) {
@@ -1665,6 +1671,10 @@ static int prepare_impl(bg_net *n) {
         }
         if (st) return st;
     }
+    // the 'synapses' slot: after the connections, before the resets
+    // (DelayConnection rows and resets of this step run in the next step's
+    // head kernel, so a target variable fed by both is refused at prepare)
+    for (size_t yi = 0; yi < n->syns.size(); ++yi) { st = build_syn(n, (int)yi); if (st) return st; }
     if (n->step_launches.empty()) return fail(BG_EINVAL, "empty network");
     if (n->allow_persist) st = n->precision == 64 ? build_persist<double>(n) : build_persist<float>(n);
     if (st) return st;

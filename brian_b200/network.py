@@ -233,13 +233,6 @@ class Network(object):
         for s in self.stdps:
             if not any(s.C is c for c in self.connections):
                 raise ValueError("STDP on a connection that is not in the network")
-        for y in self.synapses:
-            # Synapses update in the groups slot at their place in the group
-            # order; the engine applies them right after their target group
-            tgt = y.target._owner
-            pos = [k for k, o in enumerate(self._order) if o is tgt]
-            if pos and pos[0] > next(k for k, o in enumerate(self._order) if o is y):
-                raise NotImplementedError("a Synapses object must follow its target group in the network")
         b = _Binding(self, _current_table(), self.clock.dt)
         rt = b.rt
         for g in groups:

@@ -17,14 +17,16 @@ What runs on the engine:
 * Presynaptic delays: ``S.delay[...] = seconds`` is stored in bins as
   ``int(value / dt)`` (synapticvariable.py:161).
 
-Event timing follows the SpikeQueue (spikequeue.py:69-330): the queue is
-filled in the connections slot with the spikes of step s and read in the
-groups slot, after ``next()`` has advanced it, so an event of delay d
-bins is applied at step s + 1 + d, where the Synapses object sits in the
-group order.  The engine supports the order in which the Synapses object
-follows its target group (the usual order of creation).  Events reaching
-one target in one step are applied in queue order: insertion step, then
-source index, then synapse index.  The reference applies repeated targets
+Event timing follows the SpikeQueue (spikequeue.py:69-330) and the
+schedule (network.py:365-380, 472-483): the queue is filled in the
+connections slot with the spikes of step s, at the row due d steps later,
+and read in the 'synapses' slot (after the connections, before the resets)
+before ``next()`` advances it, so an event of delay d bins is applied at
+step s + d.  Events reaching one target in one step are applied in queue
+order: insertion step, then source index, then synapse index.  A target
+variable that a DelayConnection also feeds on the same neurons is refused
+by the engine (it adds the connection's due row after the Synapses, the
+reference before).  The reference applies repeated targets
 in rounds over numpy's default (unstable) argsort (synapses.py:502-516),
 which orders ties by numpy's sort implementation; queue order is the order
 a stable sort gives.

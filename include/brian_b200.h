@@ -174,10 +174,12 @@ BG_API int bg_stdp_add(bg_net *net, int32_t cid, const double *decay, double Ap,
  * to src_origin) to target post[k] (relative to tgt_origin) with a delay of
  * delay[k] bins (<= 253).  Statement q sets target variable op_var[q] to
  * x - terms[q][k] when op_sub[q], else x + terms[q][k], terms [nops][nsyn]
- * in synapse order.  A spike of step s is applied at step s + 1 + delay,
- * in the groups slot right after the target group's update; the events
- * reaching one target in one step are applied in queue order (insertion
- * step, then source index, then synapse index).  FP64 networks only. */
+ * in synapse order.  A spike of step s is applied at step s + delay, in
+ * the 'synapses' slot after the connections and before the resets
+ * (network.py:365-380); the events reaching one target in one step are
+ * applied in queue order (insertion step, then source index, then synapse
+ * index).  FP64 networks only; a target variable also fed by a
+ * DelayConnection on the same neurons is refused at prepare (BG_ENOSYS). */
 BG_API int bg_synapses_add(bg_net *net, int32_t src_gid, int64_t src_origin,
                 int64_t src_n, int32_t tgt_gid, int64_t tgt_origin, int64_t tgt_n,
                 int64_t nsyn, const int32_t *pre, const int32_t *post,

@@ -134,8 +134,9 @@ struct Stdp {
 /* Synapses (synapses/synapses.py:43-1058) with static synaptic variables
  * and presynaptic statements x (+|-)= term on the target; SpikeQueue
  * (synapses/spikequeue.py:69-330): L rows of synapse indices, filled in the
- * connections slot at row (cur + delay) % L after cur has advanced, read and
- * cleared at row cur in the groups slot. */
+ * connections slot at row (cur + delay) % L, read and cleared at row cur in
+ * the 'synapses' slot of the same step (after 'after_connections', before
+ * the resets, network.py:365-380, 472-483), which then advances cur. */
 struct Syn {
     int32_t src, tgt; int64_t so, sn, to, tn; int64_t nsyn;
     std::vector<int32_t> pre, post, delay;
@@ -439,12 +440,11 @@ int or_synapses_set_terms(or_net *n, int32_t sid, const double *terms) {
     std::copy(terms, terms + (size_t)y.nops * y.nsyn, y.terms.begin());
     return OR_OK;
 }
-/* Synapses.update (synapses.py:808-827): the events of this step, in queue
- * order, applied statement by statement; then next(). */
-static void synapses_deliver(or_net *n, int32_t gid) {
+/* Synapses.update (synapses.py:808-827) in the 'synapses' slot: the events
+ * of this step, in queue order, applied statement by statement; then next(). */
+static void synapses_deliver(or_net *n) {
     for (auto &y : n->syns) {
-        if (y.tgt != gid) continue;
-        Group &g = n->groups[gid];
+        Group &g = n->groups[y.tgt];
         for (int32_t e : y.X[y.cur]) {
             const int64_t j = y.to + y.post[e];
             for (int k = 0; k < y.nops; ++k) {
@@ -668,8 +668,6 @@ static void step(or_net *n, int64_t cs) {
         }
         g.nspikes += (int64_t)spikes.size();
         g.hist.pop_back(); g.hist.push_front(std::move(spikes));
-        /* Synapses placed after their target group in the group order */
-        synapses_deliver(n, (int32_t)gi);
     }
     for (auto &s : n->stdps) {   /* trace groups G_pre / G_post (stdp.py:282-293) */
         for (auto &a : s.A_pre) a = s.a_pre * a + s.c_pre;
@@ -791,6 +789,8 @@ static void step(or_net *n, int64_t cs) {
         for (int64_t j = 0; j < c.tn; ++j) { sv[j] = sv[j] + row[j]; row[j] = 0.0; }
         c.cur = (c.cur + 1) % c.md;
     }
+    /* ---- synapses ---- */
+    synapses_deliver(n);
     /* ---- resets ---- */
     for (auto &g : n->groups) {
         const int64_t N = g.n;

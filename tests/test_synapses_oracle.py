@@ -1,10 +1,13 @@
 """Synapses on the oracle and the host side of the class.
 
-The known-answer case is worked out by hand from the reference's SpikeQueue
-(spikequeue.py:209-216 next/peek, 270-302 insert, 340-363 propagate) and
-Synapses.update (synapses.py:808-827): a spike of step s through a synapse
-of delay d bins is applied in the groups slot of step s + 1 + d, and the
-events reaching one target are applied one after the other in queue order.
+The known-answer cases are worked out by hand from the reference's
+SpikeQueue (spikequeue.py:209-216 next/peek, 270-302 insert, 340-363
+propagate), Synapses.update (synapses.py:808-827) and the schedule
+(network.py:365-380: connections, after_connections, synapses, resets): a
+spike of step s through a synapse of delay d bins is inserted in the
+connections slot at the queue row due d steps later and applied in the
+synapses slot of step s + d; the events reaching one target are applied one
+after the other in queue order.
 """
 import numpy as np
 import pytest
@@ -49,15 +52,15 @@ def test_known_answer(oracle_table):
     _fresh()
     steps, v = _kat(oracle_table)
     v0 = np.full(12, 1.0)
-    # spikes of step 2 through synapses 0 and 1 (delay 3) arrive at step 6,
+    # spikes of step 2 through synapses 0 and 1 (delay 3) arrive at step 5,
     # in queue order: source 0 first: (1 + 2^-53) + 2^-52
     x = (1.0 + 2.0 ** -53) + 2.0 ** -52
-    v0[6:] = x
-    # the second spike of source 0 (step 5) arrives at step 9
-    v0[9:] = x + 2.0 ** -53
+    v0[5:] = x
+    # the second spike of source 0 (step 5) arrives at step 8
+    v0[8:] = x + 2.0 ** -53
     v1 = np.zeros(12)
-    v1[5:] = 0.25            # step 4, delay 0 -> step 5
-    v1[6:] = 0.25 + 0.5      # step 4, delay 1 -> step 6
+    v1[4:] = 0.25            # step 4, delay 0 -> step 4
+    v1[5:] = 0.25 + 0.5      # step 4, delay 1 -> step 5
     np.testing.assert_array_equal(steps, np.arange(12))
     np.testing.assert_array_equal(v[:, 0], v0)
     np.testing.assert_array_equal(v[:, 1], v1)
@@ -67,7 +70,7 @@ def test_known_answer(oracle_table):
 
 def kat_insertion_order(tab, steps=10):
     """Source 1 spikes at step 2 through a delay of 3, source 0 at step 4
-    through a delay of 1: both events reach target 0 at step 6, the one
+    through a delay of 1: both events reach target 0 at step 5, the one
     inserted first (source 1) applied first."""
     src = b.SpikeGeneratorGroup(2, [(1, 2 * DT), (0, 4 * DT)])
     P = b.NeuronGroup(1, model="v : 1")
@@ -88,18 +91,18 @@ def kat_insertion_order(tab, steps=10):
 
 def expected_insertion_order(steps=10):
     v = np.full(steps, 1.0)
-    v[6:] = (1.0 + 2.0 ** -53) + 2.0 ** -52
+    v[5:] = (1.0 + 2.0 ** -53) + 2.0 ** -52
     return v
 
 
 def expected_known_answer():
     v0 = np.full(12, 1.0)
     x = (1.0 + 2.0 ** -53) + 2.0 ** -52
-    v0[6:] = x
-    v0[9:] = x + 2.0 ** -53
+    v0[5:] = x
+    v0[8:] = x + 2.0 ** -53
     v1 = np.zeros(12)
-    v1[5:] = 0.25
-    v1[6:] = 0.25 + 0.5
+    v1[4:] = 0.25
+    v1[5:] = 0.25 + 0.5
     return v0, v1
 
 
@@ -190,18 +193,27 @@ def test_edge_cases(oracle_table):
         _, vals = M._record()
     vals = np.asarray(vals).reshape(6, 6)
     want = np.zeros((6, 6))
-    want[2:, 3] = -0.5          # spike of step 1, delay 0 -> applied at step 2
-    want[3:, 4] = -1.0          # spike of step 2 -> step 3
+    want[1:, 3] = -0.5          # spike of step 1, delay 0 -> applied at step 1
+    want[2:, 4] = -1.0          # spike of step 2 -> step 2
     np.testing.assert_array_equal(vals, want)
 
 
-def test_synapses_before_target_refused(oracle_table):
-    _fresh()
-    G = b.NeuronGroup(3, model="v : 1")
-    H = b.NeuronGroup(3, model="v : 1")
-    S = b.Synapses(G, H, model="w : 1", pre="v += w")
-    S[:, :] = True
-    net = b.Network(G, S, H)
-    with pytest.raises(NotImplementedError):
+def test_order_in_network_does_not_matter(oracle_table):
+    """Synapses run in their own slot after the connections, wherever they
+    sit among the groups (network.py:472-483)."""
+    out = []
+    for order in ("GSH", "GHS"):
+        _fresh()
+        G = b.SpikeGeneratorGroup(3, [(0, 1 * DT), (2, 3 * DT)])
+        H = b.NeuronGroup(3, model="dv/dt = -v/(2*ms) : 1")
+        S = b.Synapses(G, H, model="w : 1", pre="v += w")
+        S[:, :] = True
+        S.w = "0.1 + i + 10*j"
+        M = b.StateMonitor(H, "v", record=True)
+        objs = {"G": G, "S": S, "H": H}
+        net = b.Network(*[objs[c] for c in order], M)
         with engine(oracle_table):
-            net.run(2 * DT)
+            net.run(6 * DT)
+            out.append(np.asarray(M._record()[1]).copy())
+    np.testing.assert_array_equal(out[0], out[1])
+    assert np.any(out[0] != 0)
