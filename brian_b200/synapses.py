@@ -283,6 +283,8 @@ class Synapses(object):
         """Each presynaptic neuron gets Binomial(m, p) distinct targets drawn
         uniformly (synapses.py:845-885)."""
         self._check_open()
+        if sparseness is None or not 0.0 <= float(sparseness) <= 1.0:
+            raise ValueError("connection probability must lie in [0, 1], not %r" % (sparseness,))
         pre_idx = _group_range(self.source if pre is None else pre, self.source)
         post_idx = _group_range(self.target if post is None else post, self.target)
         m = len(post_idx)
@@ -304,10 +306,19 @@ class Synapses(object):
 
     def connect_one_to_one(self, pre=None, post=None):
         self._check_open()
+
+        def size(x, G):
+            if x is None:
+                return len(G)
+            if isinstance(x, (NeuronGroup, Subgroup)):
+                return len(x)
+            return len(_group_range(x, G))
+
+        # the sizes are compared first, as in synapses.py:829-843
+        if size(pre, self.source) != size(post, self.target):
+            raise TypeError("Source and target groups do not have the same size")
         pre_idx = _group_range(self.source if pre is None else pre, self.source)
         post_idx = _group_range(self.target if post is None else post, self.target)
-        if len(pre_idx) != len(post_idx):
-            raise TypeError("Source and target groups do not have the same size")
         self._create(pre_idx, post_idx)
 
     def create_synapses(self, presynaptic, postsynaptic, synapses_pre=None, synapses_post=None):
@@ -362,11 +373,28 @@ class Synapses(object):
         """Synapse indices of a slice / int / array, or of (i, j) neuron
         indices (synapses.py:946-1001)."""
         if isinstance(key, tuple):
-            i, j = key
+            # (i, j): every synapse between the neurons; (i, j, k): the k-th
+            # synapse of each pair, in creation order
+            i, j = key[0], key[1]
             pi = _group_range(i, self.source)
             qj = _group_range(j, self.target)
-            sel = np.isin(self.presynaptic, pi) & np.isin(self.postsynaptic, qj)
-            return np.nonzero(sel)[0]
+            sel = np.nonzero(np.isin(self.presynaptic, pi) & np.isin(self.postsynaptic, qj))[0]
+            if len(key) == 3:
+                pair = self.presynaptic[sel] * max(1, len(self.target)) + self.postsynaptic[sel]
+                rank = np.zeros(len(sel), dtype=np.int64)
+                seen = {}
+                for n_, p_ in enumerate(pair.tolist()):
+                    rank[n_] = seen.get(p_, 0)
+                    seen[p_] = rank[n_] + 1
+                k = key[2]
+                if isinstance(k, slice):
+                    want = np.arange(int(rank.max()) + 1 if len(rank) else 0)[k]
+                elif np.isscalar(k):
+                    want = [int(k)]
+                else:
+                    want = np.asarray(k, dtype=np.int64).ravel()
+                sel = sel[np.isin(rank, want)]
+            return sel
         if isinstance(key, slice):
             return np.arange(len(self))[key]
         return np.asarray(key, dtype=np.int64)
