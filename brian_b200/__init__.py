@@ -17,7 +17,8 @@ from .groups import (NeuronGroup, PoissonGroup, SpikeGeneratorGroup, Threshold, 
 from .connections import Connection, DelayConnection, IdentityConnection
 from .stdp import ExponentialSTDP, STDP
 from .synapses import Synapses
-from .monitors import (SpikeMonitor, StateMonitor, RecentStateMonitor, SpikeCounter, PopulationSpikeCounter,
+from .monitors import (SpikeMonitor, StateMonitor, RecentStateMonitor, ISIHistogramMonitor, SpikeCounter,
+                       PopulationSpikeCounter,
                        PopulationRateMonitor,
                        CoincidenceCounter, MultiStateMonitor)
 from .network import (Network, MagicNetwork, run, reinit, stop, clear, network_operation, NetworkOperation,

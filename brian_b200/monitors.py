@@ -13,7 +13,8 @@ import numpy as np
 from .clock import guess_clock
 
 __all__ = ["SpikeMonitor", "StateMonitor", "SpikeCounter", "PopulationSpikeCounter",
-           "PopulationRateMonitor", "CoincidenceCounter", "MultiStateMonitor", "RecentStateMonitor"]
+           "PopulationRateMonitor", "CoincidenceCounter", "MultiStateMonitor", "RecentStateMonitor",
+           "ISIHistogramMonitor"]
 
 
 class SpikeMonitor(object):
@@ -400,4 +401,40 @@ class RecentStateMonitor(StateMonitor):
         for times in times_seq:
             idx = (cur - 1 - np.array(self._invtargetdt * np.asarray(times), dtype=int)) % self.num_duration
             out.append(vals[idx, np.arange(vals.shape[1])])
+        return out
+
+
+class ISIHistogramMonitor(SpikeMonitor):
+    """Interspike-interval histogram of a group (monitor.py:430-504),
+    computed from the recorded spikes.
+
+    ``bins`` are the lower bounds of the bins, the last one open-ended.  As
+    in the reference, each neuron's previous spike time starts at 1000 s,
+    so a neuron's first spike gives a negative interval; intervals inside
+    [bins[0], bins[-1]] are counted with numpy's histogram over the bin
+    edges, every other interval (the first spikes among them) in the last
+    bin.  The reference passes ``delay`` on as SpikeMonitor's ``record``
+    argument, so it never delays the spikes; it is ignored here too."""
+
+    def __init__(self, source, bins, delay=0):
+        SpikeMonitor.__init__(self, source, record=True, delay=0)
+        self.bins = np.array(bins, dtype=np.float64)
+
+    @property
+    def count(self):
+        steps, idx = self._record()
+        t = np.asarray(steps, dtype=np.float64) * self.source.clock.dt
+        idx = np.asarray(idx, dtype=np.int64)
+        last = np.full(len(self.source), 1000.0)
+        isi = np.empty(len(idx))
+        for k in range(len(idx)):           # chronological order, as the updates run
+            isi[k] = t[k] - last[idx[k]]
+            last[idx[k]] = t[k]
+        out = np.zeros(len(self.bins))
+        if len(self.bins) > 1:
+            h, _ = np.histogram(isi, self.bins)
+            out[:-1] += h
+            out[-1] += len(isi) - h.sum()
+        else:
+            out[-1] += len(isi)
         return out

@@ -41,3 +41,19 @@ def test_before_and_after_wrap(oracle_table):
     lags = np.array([0.0, 1.5 * DT, 4 * DT]) * (1.0 / DT)
     for k in range(3):
         assert past[k] == full[-1 - int(lags[k]), k]
+
+
+def test_isi_histogram(oracle_table):
+    """ISIHistogramMonitor (monitor.py:430-504): intervals 5 ms -> bin 0,
+    15 and 12 ms -> bin 1, 26 ms and the two first spikes (negative
+    intervals from the 1000 s start) -> the last bin."""
+    b.clear()
+    b.reinit_default_clock()
+    G = b.SpikeGeneratorGroup(2, [(0, 1 * ms), (1, 2 * ms), (0, 6 * ms), (1, 14 * ms), (0, 21 * ms),
+                                  (1, 40 * ms)])
+    H = b.ISIHistogramMonitor(G, [0 * ms, 10 * ms, 20 * ms])
+    net = b.Network(G, H)
+    with engine(oracle_table):
+        net.run(45 * ms)
+        np.testing.assert_array_equal(H.count, [1, 2, 3])
+    np.testing.assert_array_equal(H.bins, [0, 0.01, 0.02])
