@@ -44,11 +44,6 @@ def test_synapses_bit_exact(oracle_table, gpu_table, kw):
     scenarios.compare(ref, gpu)
 
 
-def _weights_between_runs():
-    out = scenarios.synapses_cuba(N=800, steps=400, runs=1)
-    return out
-
-
 @pytest.mark.gpu
 def test_synapse_weights_changed_between_runs(oracle_table, gpu_table):
     def fn():
