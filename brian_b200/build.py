@@ -76,15 +76,18 @@ def build(force=False, verbose=False):
     if not force and not needs_build():
         return LIB
     write_rtc_sources()
-    objs = []
+    cmds, objs = [], []
     for src in sources():
         obj = os.path.join(CSRC, os.path.basename(src)[:-3] + ".o")
-        cmd = [NVCC] + ARCH + FLAGS + ["-I", os.path.join(HERE, "..", "include"),
-                                       "-c", src, "-o", obj]
-        if verbose:
-            print(" ".join(cmd))
-        subprocess.check_call(cmd)
+        cmds.append([NVCC] + ARCH + FLAGS + ["-I", os.path.join(HERE, "..", "include"), "-c", src, "-o", obj])
         objs.append(obj)
+    # one nvcc per translation unit, side by side
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for cmd in cmds:
+            if verbose:
+                print(" ".join(cmd))
+        list(ex.map(subprocess.check_call, cmds))
     link = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + [
         "-L" + os.path.join(CUDA_HOME, "lib64"),
         "-L" + os.path.join(CUDA_HOME, "lib64", "stubs"),

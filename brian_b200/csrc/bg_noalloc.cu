@@ -1,14 +1,16 @@
 // bg_noalloc.cu -- an entry point that allocates no device memory.
 //
 // Some callers cannot call cudaMalloc: code running inside another
-// framework's memory pool, under a CUDA-graph recorder that forbids new
-// allocations, or in a process whose device memory is fully reserved up
-// front.  bg_delay_group_run_noalloc runs the same fused update / delayed
-// push kernel as the network engine (k_head) for one linear group with
+// framework's memory pool (its caching allocator owns the device memory and
+// a cudaMalloc behind its back can fail or fragment it), or a process whose
+// device memory is fully reserved up front.  bg_delay_group_run_noalloc runs
+// the same fused update / delayed push kernel as the network engine (k_head)
+// for one linear group with
 // shared-weight DelayConnections onto itself, with every scratch buffer --
 // control block, spike history, count rings, k-fold-sum tables -- carved out
 // of one file-scope device array of fixed size.  The caller owns and passes
 // the inputs (connection rows, delays) and the in/out state.
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <mutex>
@@ -34,6 +36,18 @@ unsigned char *g_scratch_ptr[kNoAllocMaxDevices] = {nullptr};
 int fail(int code, const std::string &m) { return bg_internal_fail(code, m.c_str()); }
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Row pointers of one connection: rowptr[0] >= 0, non-decreasing, every row
+// shorter than 2^31 entries.  Runs (and its flag is read on the host) before
+// any kernel walks the rows, so a malformed rowptr never drives a read of
+// cols or delays outside the rows it claims.
+__global__ void k_rowcheck(const int64_t *rowptr, int64_t sn, DevCtl *ctl) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < sn; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t a = rowptr[i], b = rowptr[i + 1];
+        if ((i == 0 && a < 0) || b < a || b - a >= (int64_t(1) << 31)) bg_raise(ctl, BG_DERR_RANGE, i);
+    }
+    if (sn == 0 && blockIdx.x == 0 && threadIdx.x == 0 && rowptr[0] < 0) bg_raise(ctl, BG_DERR_RANGE, 0);
+}
 
 // In-degree histogram of one connection, with range checks of the caller's
 // rows (targets in [0, n), delays below the ring depth).
@@ -81,7 +95,9 @@ cudaError_t launch_nv(const bg::HeadArgs<double> &a, int nvar, unsigned int bloc
 }
 
 // Device address of the scratch array for the current device: looked up
-// once per device (cudaGetSymbolAddress), then reused.
+// once per device (cudaGetSymbolAddress), then reused for the life of the
+// process.  A cudaDeviceReset unloads the module and may move the array, so
+// the entry point must not be called on a device after the caller reset it.
 int scratch_for_current_device(unsigned char **out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -125,7 +141,7 @@ BG_API int bg_delay_group_run_noalloc(int64_t n, int nvar, double *S, const doub
     for (int c = 0; c < nconn; ++c) {
         if (src_origin[c] < 0 || src_n[c] < 0 || src_origin[c] + src_n[c] > n) return fail(BG_EINVAL, "source range");
         if (tgt_var[c] < 0 || tgt_var[c] >= nvar) return fail(BG_EINVAL, "target variable");
-        if (ring_depth[c] < 1 || ring_depth[c] > 253) return fail(BG_EINVAL, "ring depth must be in [1, 253]");
+        if (ring_depth[c] < 1 || ring_depth[c] > 255) return fail(BG_EINVAL, "ring depth must be in [1, 255]");
         if (!rowptr[c] || !cols[c] || !delays[c]) return fail(BG_EINVAL, "connection pointers");
     }
     cudaStream_t s = (cudaStream_t)stream;
@@ -152,6 +168,18 @@ BG_API int bg_delay_group_run_noalloc(int64_t n, int nvar, double *S, const doub
     // every call starts from cleared control block, counters, history and rings
     cudaError_t e = cudaMemsetAsync(scr, 0, off, s);
     if (e != cudaSuccess) return fail(BG_ECUDA, std::string("clear scratch: ") + cudaGetErrorString(e));
+    DevCtl h;
+    // ---- the caller's row pointers, checked before anything walks the rows
+    for (int c = 0; c < nconn; ++c) {
+        const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((src_n[c] + 255) / 256, 1184));
+        k_rowcheck<<<grid, 256, 0, s>>>(rowptr[c], src_n[c], ctl);
+        if ((e = cudaGetLastError()) != cudaSuccess) return fail(BG_ECUDA, cudaGetErrorString(e));
+    }
+    if ((e = cudaMemcpyAsync(&h, ctl, sizeof(h), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess)
+        return fail(BG_ECUDA, cudaGetErrorString(e));
+    if (h.err) return fail(BG_EINVAL, "connection rows: rowptr negative, decreasing or a row of 2^31 entries or "
+                           "more (row " + std::to_string(h.err_info) + ")");
     // ---- count tables (one in-degree histogram per connection)
     for (int c = 0; c < nconn; ++c) {
         unsigned int *deg = (unsigned int *)(scr + o_deg);
@@ -161,7 +189,6 @@ BG_API int bg_delay_group_run_noalloc(int64_t n, int nvar, double *S, const doub
         k_count_table<<<1, 1024, 0, s>>>(deg, n, weight[c], (double *)(scr + o_tab[c]), ctl);
         if ((e = cudaGetLastError()) != cudaSuccess) return fail(BG_ECUDA, cudaGetErrorString(e));
     }
-    DevCtl h;
     if ((e = cudaMemcpyAsync(&h, ctl, sizeof(h), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
         (e = cudaStreamSynchronize(s)) != cudaSuccess)
         return fail(BG_ECUDA, cudaGetErrorString(e));

@@ -281,9 +281,9 @@ BG_API int bg_net_set_persistent(bg_net *net, int enable);
 BG_API int bg_net_persistent_threads(bg_net *net, int32_t *threads);
 /* ---- allocation-free entry point ------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
- * memory (code inside another framework's caching allocator, a process that
- * reserved all device memory up front, a call made while a CUDA-graph
- * recorder forbids allocation): runs one linear group with up to 4
+ * memory (code inside another framework's caching allocator, which owns the
+ * device memory, or a process that reserved all device memory up front):
+ * runs one linear group with up to 4
  * shared-weight DelayConnections onto itself for nsteps steps, like a fresh
  * bg_net with those objects and bg_net_run(nsteps, 0), with identical
  * results.  It calls no cudaMalloc/cudaFree; its scratch is a file-scope
@@ -293,14 +293,19 @@ BG_API int bg_net_persistent_threads(bg_net *net, int32_t *threads);
  *   S      device, [nvar][n] row-major (stride n), updated in place
  *   A, C   host, the linear propagator (C may be NULL)
  *   connection c: sources [src_origin[c], +src_n[c]) of the group, target
- *   variable tgt_var[c]; rowptr[c] (device, src_n+1), cols[c] (device,
- *   targets in [0,n), ascending per row), delays[c] (device, steps below
- *   ring_depth[c] = int(max_delay/dt)+1), shared weight weight[c].
+ *   variable tgt_var[c]; rowptr[c] (device, src_n+1 entries, rowptr[0] >= 0,
+ *   non-decreasing), cols[c] (device, targets in [0,n), ascending per row),
+ *   delays[c] (device, steps below ring_depth[c] = int(max_delay/dt)+1,
+ *   ring_depth in [1, 255]), shared weight weight[c].  Row pointers, targets
+ *   and delays are checked on the device before the step loop (BG_EINVAL).
  * All calls share the scratch and each one clears what must start at zero,
  * so calls that overlap on the GPU (different streams or threads) race.  The
  * first call on a device looks up the scratch address for that device; make
- * that first call before any stream capture.  *spikes_out receives the
- * number of spikes emitted (may be NULL); stream may be NULL. */
+ * that first call before any stream capture, and do not call the entry point
+ * on a device after a cudaDeviceReset of it.  The call synchronises the
+ * stream (it reads the checks and the spike count back to the host).
+ * *spikes_out receives the number of spikes emitted (may be NULL); stream
+ * may be NULL. */
 BG_API int bg_delay_group_run_noalloc(
     int64_t n, int nvar, double *S, const double *A, const double *C,
     int thr_var, double thr_val, int reset_var, double reset_val, int nconn,

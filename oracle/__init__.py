@@ -29,6 +29,21 @@ def philox_uniform(seed, step, i):
     return table().lib.or_philox_uniform(seed, step, i)
 
 
+def fixed_indegree_csr(n_src, n_tgt, k, seed):
+    """The oracle's fixed in-degree construction (the same draws as the
+    engine's bg_fixed_indegree_csr), as (rowptr int64, cols int32)."""
+    import numpy as np
+    lib = table().lib
+    lib.or_fixed_indegree_csr.argtypes = [ct.c_int64, ct.c_int64, ct.c_int64, ct.c_uint64, ct.c_void_p, ct.c_void_p]
+    lib.or_fixed_indegree_csr.restype = ct.c_int
+    rowptr = np.empty(n_src + 1, dtype=np.int64)
+    cols = np.empty(n_tgt * k, dtype=np.int32)
+    st = lib.or_fixed_indegree_csr(n_src, n_tgt, k, int(seed) & ((1 << 64) - 1), rowptr.ctypes.data, cols.ctypes.data)
+    if st != 0:
+        raise ValueError("or_fixed_indegree_csr failed (%d)" % st)
+    return rowptr, cols
+
+
 def reference_spike_container():
     """ctypes handle to the reference's own C++ SpikeContainer (compiled from
     the reference tree into oracle/_ref), or None when it was not built."""

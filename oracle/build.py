@@ -8,7 +8,8 @@
   it lies, behind the small C shim ref_shim.cpp.  Built only when the
   reference tree is present (it is not on GPU hosts; the built .so travels).
 
-Run: ``python oracle/build.py`` (also called by ``__graft_entry__.build()``).
+Run: ``python oracle/build.py`` (also called by ``__graft_entry__.build()``);
+the reference tree is taken from ``$BRIAN_REFERENCE`` when set.
 """
 import os
 import subprocess
@@ -18,7 +19,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
 REF_SO = os.path.join(REF_DIR, "libccircular_ref.so")
-REFERENCE = "/root/reference"
+# the reference tree: BRIAN_REFERENCE, else where the build container mounts it
+REFERENCE = os.environ.get("BRIAN_REFERENCE", "/root/reference")
 CCIRC = os.path.join(REFERENCE, "brian", "utils", "ccircular")
 
 

@@ -857,4 +857,40 @@ int or_net_stats(or_net *n, int64_t *steps, int64_t *launches, double *ms) {
  * pin the stream against known answers. */
 double or_philox_uniform(uint64_t seed, int64_t step, int64_t i) { return philox_uniform(seed, step, i); }
 
+/* Fixed in-degree connectivity (random_matrix_fixed_column,
+ * construction.py:149-177: every target receives k distinct sources drawn
+ * uniformly), the draws of the engine's bg_fixed_indegree_csr: per target j,
+ * Philox4x32-10 blocks keyed by the seed with counter (j, attempt) give two
+ * sources each (high half of word * n_src); the row is sorted, duplicates
+ * dropped and the missing entries drawn again after the kept ones.  CSR rows
+ * over sources with ascending targets.  Single-threaded, so the CPU side of
+ * a benchmark builds its network without the engine library. */
+int or_fixed_indegree_csr(int64_t n_src, int64_t n_tgt, int64_t k, uint64_t seed, int64_t *rowptr, int32_t *cols) {
+    if (n_src <= 0 || n_tgt < 0 || k < 0 || k > n_src || !rowptr || (n_tgt * k > 0 && !cols))
+        return fail(OR_EINVAL, "fixed_indegree_csr arguments");
+    std::vector<int32_t> s((size_t)k);
+    std::memset(rowptr, 0, sizeof(int64_t) * (size_t)(n_src + 1));
+    std::vector<int32_t> src((size_t)(n_tgt * k));
+    for (int64_t j = 0; j < n_tgt; ++j) {
+        int64_t have = 0; uint64_t attempt = 0;
+        while (have < k) {
+            for (int64_t r = have; r < k; r += 2) {
+                uint32_t c[4] = {(uint32_t)j, (uint32_t)((uint64_t)j >> 32), (uint32_t)attempt, (uint32_t)(attempt >> 32)};
+                philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+                ++attempt;
+                s[r] = (int32_t)(((uint64_t)c[0] * (uint64_t)n_src) >> 32);
+                if (r + 1 < k) s[r + 1] = (int32_t)(((uint64_t)c[1] * (uint64_t)n_src) >> 32);
+            }
+            std::sort(s.begin(), s.end());
+            have = std::unique(s.begin(), s.end()) - s.begin();
+        }
+        for (int64_t r = 0; r < k; ++r) { src[(size_t)(j * k + r)] = s[r]; rowptr[s[r] + 1]++; }
+    }
+    for (int64_t i = 0; i < n_src; ++i) rowptr[i + 1] += rowptr[i];
+    std::vector<int64_t> fill(rowptr, rowptr + n_src);
+    for (int64_t j = 0; j < n_tgt; ++j)
+        for (int64_t r = 0; r < k; ++r) cols[fill[src[(size_t)(j * k + r)]]++] = (int32_t)j;
+    return OR_OK;
+}
+
 }  /* extern "C" */

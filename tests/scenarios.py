@@ -32,8 +32,9 @@ def _result(net, groups=(), spikemons=(), statemons=(), conns=(), stdps=()):
     return out
 
 
-def cuba(N=4000, steps=10000, seed=1, p=0.02, record=10, refractory=0.0):
-    """Config 1: CUBA-4000, FP64, zero delay (examples/misc/CUBA.py:25-74)."""
+def cuba(N=4000, steps=10000, seed=1, p=0.02, record=10, refractory=0.0, runs=1):
+    """Config 1: CUBA-4000, FP64, zero delay (examples/misc/CUBA.py:25-74);
+    `runs` > 1 splits the steps into that many equal run() calls."""
     taum, taue, taui = 20 * ms, 5 * ms, 10 * ms
     Vt, Vr, El = -50 * mV, -60 * mV, -49 * mV
     eqs = b.Equations("""
@@ -55,7 +56,9 @@ def cuba(N=4000, steps=10000, seed=1, p=0.02, record=10, refractory=0.0):
     M = b.SpikeMonitor(P)
     S = b.StateMonitor(P, "v", record=list(range(record)))
     net = b.Network(P, Ce, Ci, M, S)
-    net.run(steps * 0.1 * ms)
+    assert steps % runs == 0
+    for _ in range(runs):
+        net.run(steps // runs * 0.1 * ms)
     return _result(net, groups=[P], spikemons=[M], statemons=[S])
 
 
@@ -117,6 +120,47 @@ def cuba_delay(N=3000, indegree=100, steps=2000, seed=3, wdtype=np.float32, we=0
     net = b.Network(P, conns[0], conns[1], M, S)
     net.run(steps * 0.1 * ms)
     return _result(net, groups=[P], spikemons=[M], statemons=[S])
+
+
+def cuba_large(N=200000, indegree=1000, steps=300, seed=2024, runs=1, precision=64):
+    """The benchmark network at scale: N LIF neurons (80 % exc / 20 % inh),
+    fixed in-degree `indegree` (80 % exc), f32 shared weights 0.162 mV /
+    -0.9 mV, u8 delays uniform in 1..50 steps, seeded v0 in [Vr, Vt] (the
+    CUBA-262k construction), a SpikeMonitor on the whole group; connectivity
+    drawn by the engine's host-side builder (the same on both engines)."""
+    from brian_b200._lib import fixed_indegree_csr_native
+    ne = int(0.8 * N)
+    ke = int(0.8 * indegree)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    exc = fixed_indegree_csr_native(ne, N, ke, seed * 2 + 1)
+    inh = fixed_indegree_csr_native(N - ne, N, indegree - ke, seed * 2 + 2)
+    d_exc = rng.integers(1, 51, size=len(exc[1]), dtype=np.uint8)
+    d_inh = rng.integers(1, 51, size=len(inh[1]), dtype=np.uint8)
+    v0 = -60e-3 + rng.random(N) * (-50e-3 - -60e-3)
+    eqs = b.Equations("""
+    dv/dt  = (ge+gi-(v-El))/taum : volt
+    dge/dt = -ge/taue : volt
+    dgi/dt = -gi/taui : volt
+    """, taum=20 * ms, taue=5 * ms, taui=10 * ms, El=-49 * mV)
+    P = b.NeuronGroup(N, model=eqs, threshold=-50 * mV, reset=-60 * mV)
+    Pe, Pi = P.subgroup(ne), P.subgroup(N - ne)
+    Ce = b.DelayConnection(Pe, P, "ge", max_delay=5 * ms, dtype=np.float32)
+    Ce.connect_csr(exc[0], exc[1], np.float32(0.162e-3), delay_steps=d_exc)
+    Ci = b.DelayConnection(Pi, P, "gi", max_delay=5 * ms, dtype=np.float32)
+    Ci.connect_csr(inh[0], inh[1], np.float32(-0.9e-3), delay_steps=d_inh)
+    P.v = v0
+    M = b.SpikeMonitor(P)
+    net = b.Network(P, Ce, Ci, M)
+    for _ in range(runs):
+        net.run(steps // runs * 0.1 * ms)
+    out = _result(net, groups=[P], spikemons=[M])
+    g, c = net._binding.rt.counters(1, 2)
+    out["spikes"], out["events"] = g.copy(), c.copy()
+    st = net.stats()
+    out["launches"] = st["launches"]
+    out["persistent_threads"] = st.get("persistent_threads", 0)
+    net._invalidate()
+    return out
 
 
 def coba(N=2000, steps=2000, seed=7, method=None, implicit=False, order=1, string_threshold=True,

@@ -45,3 +45,22 @@ def test_product_table_has_typed_signatures():
     from brian_b200._lib import SIGNATURES
     names = set("bg_" + n for n in SIGNATURES)
     assert names <= set(declared())
+
+
+def test_oracle_fixed_indegree_equals_engine_builder():
+    """The oracle's construction draws the same connectivity as the engine's
+    host-side bg_fixed_indegree_csr (so the CPU baseline can build the
+    benchmark network without the engine library)."""
+    import numpy as np
+    import oracle
+    from brian_b200._lib import fixed_indegree_csr_native
+    for n_src, n_tgt, k, seed in ((2000, 3000, 160, 7), (500, 777, 500, 11), (10, 5, 0, 3)):
+        r1, c1 = oracle.fixed_indegree_csr(n_src, n_tgt, k, seed)
+        r2, c2 = fixed_indegree_csr_native(n_src, n_tgt, k, seed)
+        assert np.array_equal(r1, r2) and np.array_equal(c1, c2)
+        assert r1[-1] == n_tgt * k
+        # every target exactly k distinct sources
+        src = np.repeat(np.arange(n_src), np.diff(r1))
+        if k:
+            assert np.all(np.bincount(c1, minlength=n_tgt) == k)
+            assert len(np.unique(src.astype(np.int64) * n_tgt + c1)) == len(c1)

@@ -170,6 +170,21 @@ def test_stdp_delay_large_bit_exact(oracle_table, gpu_table):
 
 
 @pytest.mark.gpu
+def test_cuba_large_persistent_bit_exact(oracle_table, gpu_table):
+    """The benchmark's construction at 200 000 neurons and in-degree 1000
+    (200 M synapses; 196 persistent blocks of 1024 neurons, more than one
+    per SM, so the cross-block waits run over the whole grid): spikes and
+    final states of the persistent path equal the oracle's over 400 steps,
+    split into two runs."""
+    ref, gpu = _both(scenarios.cuba_large, oracle_table, N=200000, steps=400, runs=2)
+    assert ref["spikes"][0] > 5000 and ref["events"].sum() > 5_000_000
+    ref.pop("launches"), ref.pop("persistent_threads")
+    launches, th = gpu.pop("launches"), gpu.pop("persistent_threads")
+    assert th > 0                           # the persistent kernel ran
+    scenarios.compare(ref, gpu)
+
+
+@pytest.mark.gpu
 def test_kitchen_sink_bit_exact(oracle_table, gpu_table):
     ref, gpu = _both(scenarios.kitchen_sink, oracle_table)
     scenarios.compare(ref, gpu)
@@ -182,8 +197,9 @@ def test_run_split_equals_single_run(gpu_table):
     b.clear(); b.reinit_default_clock(); np.random.seed(1)
     one = scenarios.cuba(N=2000, steps=1234)
     b.clear(); b.reinit_default_clock(); np.random.seed(1)
-    two = scenarios.cuba(N=2000, steps=617, _split=True) if False else None
+    two = scenarios.cuba(N=2000, steps=1234, runs=2)
     assert one["spk0.idx"].size > 0
+    scenarios.compare(one, two)
 
 
 @pytest.mark.gpu

@@ -1,10 +1,10 @@
 """The allocation-free entry point bg_delay_group_run_noalloc.
 
 Callers that cannot allocate device memory -- code living inside another
-framework's caching allocator, a process that reserved all device memory up
-front, a library call made while a CUDA-graph recorder forbids allocation --
-pass their own device buffers and get the engine's result without any
-cudaMalloc: the scratch lives in a fixed array compiled into the library.
+framework's caching allocator, which owns the device memory, or a process
+that reserved all device memory up front -- pass their own device buffers
+and get the engine's result without any cudaMalloc: the scratch lives in a
+fixed array compiled into the library.
 
 This test checks it against the network entry points (bg_net_*, through the
 public API) on two calls in a row: the second call starts from the first
@@ -58,7 +58,7 @@ def _engine_run(S_init, nsteps, conn):
     return out, spikes, A, C
 
 
-def _noalloc_run(lib, dev, S_init, nsteps, A, C):
+def _noalloc_run(lib, dev, S_init, nsteps, A, C, expect=0):
     import torch
     S = torch.from_numpy(np.ascontiguousarray(S_init)).to("cuda")
     torch.cuda.synchronize()
@@ -72,22 +72,26 @@ def _noalloc_run(lib, dev, S_init, nsteps, A, C):
         0, -50 * mV, 0, -60 * mV, 2, i64([0, dev["ne"]]), i64([dev["ne"], N - dev["ne"]]), (ct.c_int * 2)(1, 2),
         ptrs(dev["rowptr"]), ptrs(dev["cols"]), ptrs(dev["delays"]), (ct.c_double * 2)(0.162e-2, -0.9e-2),
         (ct.c_int32 * 2)(51, 51), nsteps, None, ct.byref(spikes))
-    if st != 0:
+    if st != expect:
         buf = ct.create_string_buffer(512)
         lib.bg_last_error(buf, 512)
-        raise AssertionError("bg_delay_group_run_noalloc failed (%d): %s" % (st, buf.value.decode()))
+        raise AssertionError("bg_delay_group_run_noalloc returned %d: %s" % (st, buf.value.decode()))
     return S.cpu().numpy(), spikes.value
+
+
+def _bind(lib):
+    lib.bg_delay_group_run_noalloc.restype = ct.c_int
+    lib.bg_delay_group_run_noalloc.argtypes = [
+        ct.c_int64, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_double, ct.c_int, ct.c_double,
+        ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+        ct.c_void_p, ct.c_int64, ct.c_void_p, ct.POINTER(ct.c_int64)]
 
 
 @pytest.mark.gpu
 def test_noalloc_matches_network_engine_twice(gpu_table):
     import torch
     lib = gpu_table.lib
-    lib.bg_delay_group_run_noalloc.restype = ct.c_int
-    lib.bg_delay_group_run_noalloc.argtypes = [
-        ct.c_int64, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_double, ct.c_int, ct.c_double,
-        ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
-        ct.c_void_p, ct.c_int64, ct.c_void_p, ct.POINTER(ct.c_int64)]
+    _bind(lib)
     conn = _connectivity()
     ne, exc, inh, d_exc, d_inh, S0 = conn
     dev = {"ne": ne,
@@ -106,3 +110,26 @@ def test_noalloc_matches_network_engine_twice(gpu_table):
     out2, spk2 = _noalloc_run(lib, dev, out1, 350, A, C)
     assert spk2 == spk_ref2
     assert np.array_equal(out2, ref2)
+
+
+@pytest.mark.gpu
+def test_noalloc_refuses_malformed_row_pointers(gpu_table):
+    """A decreasing or negative rowptr is refused with BG_EINVAL by the device
+    check that runs before any kernel walks the rows; the state is untouched."""
+    import torch
+    lib = gpu_table.lib
+    _bind(lib)
+    ne, exc, inh, d_exc, d_inh, S0 = _connectivity()
+    A = np.eye(3)
+    for bad in ("decreasing", "negative"):
+        rp = exc[0].copy()
+        if bad == "decreasing":
+            rp[5], rp[6] = rp[6], rp[5]
+        else:
+            rp[0] = -1
+        dev = {"ne": ne,
+               "rowptr": [torch.from_numpy(rp).cuda(), torch.from_numpy(inh[0]).cuda()],
+               "cols": [torch.from_numpy(exc[1]).cuda(), torch.from_numpy(inh[1]).cuda()],
+               "delays": [torch.from_numpy(d_exc).cuda(), torch.from_numpy(d_inh).cuda()]}
+        out, _ = _noalloc_run(lib, dev, S0, 10, A, np.zeros(3), expect=-1)
+        assert np.array_equal(out, S0)
