@@ -46,44 +46,93 @@ def peaks():
 
 def make_inputs(seed, n=N_NEURONS, indegree=INDEGREE, builder=None):
     """Host arrays of the network: CSR of both connections, delays, v0."""
-    ne = int(0.8 * n)
-    ni = n - ne
-    ke = int(0.8 * indegree)
-    ki = indegree - ke
-    if builder is None:
-        from brian_b200._lib import fixed_indegree_csr_native as builder
-    rng = np.random.Generator(np.random.PCG64(seed))
-    exc = builder(ne, n, ke, seed * 2 + 1)
-    inh = builder(ni, n, ki, seed * 2 + 2)
-    d_exc = rng.integers(1, 51, size=len(exc[1]), dtype=np.uint8)
-    d_inh = rng.integers(1, 51, size=len(inh[1]), dtype=np.uint8)
-    v0 = -60e-3 + rng.random(n) * (-50e-3 - -60e-3)
-    return dict(n=n, ne=ne, exc=exc, inh=inh, d_exc=d_exc, d_inh=d_inh, v0=v0)
+    from brian_b200.workloads import cuba_scaled_inputs
+    return cuba_scaled_inputs(seed, n=n, indegree=indegree, builder=builder)
 
 
-def build_network(inp, with_monitor=False):
-    import brian_b200 as b
-    from brian_b200 import ms, mV
-    eqs = b.Equations("""
-    dv/dt  = (ge+gi-(v-El))/taum : volt
-    dge/dt = -ge/taue : volt
-    dgi/dt = -gi/taui : volt
-    """, taum=20 * ms, taue=5 * ms, taui=10 * ms, El=-49 * mV)
-    P = b.NeuronGroup(inp["n"], model=eqs, threshold=-50 * mV, reset=-60 * mV)
-    Pe = P.subgroup(inp["ne"])
-    Pi = P.subgroup(inp["n"] - inp["ne"])
-    Ce = b.DelayConnection(Pe, P, "ge", max_delay=5 * ms, dtype=np.float32)
-    Ce.connect_csr(inp["exc"][0], inp["exc"][1], np.float32(0.162e-3), delay_steps=inp["d_exc"])
-    Ci = b.DelayConnection(Pi, P, "gi", max_delay=5 * ms, dtype=np.float32)
-    Ci.connect_csr(inp["inh"][0], inp["inh"][1], np.float32(-0.9e-3), delay_steps=inp["d_inh"])
-    P.v = inp["v0"]
-    objs = [P, Ce, Ci]
-    M = None
-    if with_monitor:
-        M = b.SpikeMonitor(P)
-        objs.append(M)
-    net = b.Network(*objs)
-    return net, P, (Ce, Ci), M
+def build_network(inp, with_monitor=False, record=None):
+    from brian_b200.workloads import cuba_scaled
+    net, P, conns, M, _ = cuba_scaled(inp, spike_monitor=with_monitor, record=record)
+    return net, P, conns, M
+
+
+def host_cpu():
+    """Host cores and CPU model of this machine (nproc, lscpu's model name)."""
+    model = None
+    try:
+        out = subprocess.run(["lscpu"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True, timeout=10).stdout
+        for line in out.splitlines():
+            if line.lower().startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except Exception:
+        pass
+    return {"nproc": os.cpu_count(), "model": model}
+
+
+def spike_trains(steps, idx, n, dt=DT):
+    """Per-neuron spike times (s) of a SpikeMonitor record."""
+    steps = np.asarray(steps)
+    idx = np.asarray(idx)
+    order = np.argsort(idx, kind="stable")
+    cuts = np.searchsorted(idx[order], np.arange(n + 1))
+    t = steps[order] * dt
+    return [t[cuts[i]:cuts[i + 1]] for i in range(n)]
+
+
+def precision_report(rec64, rec32, n, duration, v64=None, v32=None, delta=4e-3):
+    """Agreement of an FP32-state run with the FP64 run of the same network:
+    gamma factor (delta 4 ms, tools/statistics.py:261-314) of each neuron's
+    FP32 train against its FP64 train, over neurons with at least two FP64
+    spikes and 2 delta r < 1 (gamma is undefined at higher rates); firing
+    rates and their relative error; the fraction of FP64 spikes (step,
+    index) the FP32 run repeats exactly; the RMS difference of the recorded
+    v traces."""
+    from brian_b200.statistics import gamma_factor
+    t64 = spike_trains(rec64[0], rec64[1], n)
+    t32 = spike_trains(rec32[0], rec32[1], n)
+    g, skipped = [], 0
+    for a, b_ in zip(t32, t64):
+        if len(b_) < 2:
+            continue
+        r = (len(b_) - 1) / (b_[-1] - b_[0]) if b_[-1] > b_[0] else np.inf
+        if not 2 * delta * r < 1:
+            skipped += 1
+            continue
+        g.append(float(gamma_factor(a, b_, delta, dt=DT)))
+    # the windows [0, T) over which the FP32 run still tracks the FP64 one
+    windows = {}
+    for T in (0.01, 0.02, 0.05, 0.1, 0.2, 0.5, 1.0, 2.0, 5.0, 10.0):
+        if T > duration + 1e-12:
+            break
+        gw = []
+        for a, b_ in zip(t32, t64):
+            b_ = b_[b_ < T]
+            if len(b_) < 2 or b_[-1] <= b_[0]:
+                continue
+            r = (len(b_) - 1) / (b_[-1] - b_[0])
+            if 2 * delta * r < 1:
+                gw.append(float(gamma_factor(a[a < T], b_, delta, dt=DT)))
+        windows["%g" % (T * 1e3)] = float(np.mean(gw)) if gw else None
+    key64 = np.asarray(rec64[0], dtype=np.int64) * n + np.asarray(rec64[1], dtype=np.int64)
+    key32 = np.asarray(rec32[0], dtype=np.int64) * n + np.asarray(rec32[1], dtype=np.int64)
+    match = len(np.intersect1d(key64, key32)) / max(1, len(key64))
+    r64 = len(key64) / (n * duration)
+    r32 = len(key32) / (n * duration)
+    out = {"neurons": n, "duration_s": duration, "delta_ms": delta * 1e3,
+           "gamma_mean": float(np.mean(g)) if g else None, "gamma_median": float(np.median(g)) if g else None,
+           "gamma_min": float(np.min(g)) if g else None,
+           "gamma_frac_ge_0.95": float(np.mean(np.asarray(g) >= 0.95)) if g else None,
+           "gamma_neurons": len(g), "gamma_skipped_rate": skipped,
+           "rate_fp64_hz": r64, "rate_fp32_hz": r32, "rate_rel_err": abs(r32 - r64) / r64 if r64 > 0 else None,
+           "spikes_fp64": int(len(key64)), "spikes_fp32": int(len(key32)), "spike_match_frac": float(match),
+           "gamma_mean_by_window_ms": windows}
+    diff = np.setxor1d(key64, key32)
+    out["first_differing_step"] = int(diff.min() // n) if len(diff) else None
+    if v64 is not None and v32 is not None:
+        d = np.asarray(v32, dtype=np.float64) - np.asarray(v64, dtype=np.float64)
+        out["v_rms_err_mV"] = float(np.sqrt(np.mean(d * d)) * 1e3)
+    return out
 
 
 def out_degree_events(inp, steps, idx):
@@ -107,10 +156,13 @@ class ClockSampler(object):
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 3.0:   # nvidia-smi started
+                time.sleep(0.02)
         except Exception:
             self.proc = None
         return self
@@ -199,14 +251,16 @@ def traffic_from_profiles(kernel_name):
 
 
 def cpu_baseline(inp, nsteps):
-    """The oracle (single-threaded C restatement) on the same network."""
+    """The oracle (single-threaded C restatement) on the same network from
+    the same initial state.  Returns the baseline and the oracle's spike
+    record and final state, which the parity check compares with the GPU."""
     import oracle
     import brian_b200 as b
     from brian_b200.network import engine
     b.clear()
     b.reinit_default_clock()
     with engine(oracle.table()):
-        net, P, conns, _ = build_network(inp)
+        net, P, conns, M = build_network(inp, with_monitor=True)
         net.prepare()
         rt = net._binding.rt
         _, ev0 = rt.counters(1, 2)
@@ -215,18 +269,47 @@ def cpu_baseline(inp, nsteps):
         wall = time.perf_counter() - t0
         _, ev1 = rt.counters(1, 2)
         events = int(ev1.sum() - ev0.sum())
+        rec = tuple(x.copy() for x in M._record())
+        state = {v: np.array(getattr(P, v)) for v in ("v", "ge", "gi")}
     net._invalidate()
-    return {"value": events / wall, "unit": "events/s", "cores": 1, "kind": "port",
-            "sample": "CUBA-262k, first %d simulation steps (%.2f s simulated) from the same initial state, "
-                      "%d events in %.1f s wall" % (nsteps, nsteps * DT, events, wall)}
+    cpu = {"value": events / wall, "unit": "events/s", "cores": 1, "kind": "port", "host": host_cpu(),
+           "sample": "CUBA-262k, first %d simulation steps (%.2f s simulated) from the same initial state, "
+                     "%d events in %.1f s wall, single-threaded C++ oracle" % (nsteps, nsteps * DT, events, wall)}
+    return cpu, rec, state
+
+
+def gpu_parity(inp, nsteps, rec_ref, state_ref):
+    """The GPU engine on the benchmark network from the same initial state for
+    the oracle's steps, spike record and final state compared exactly."""
+    import brian_b200 as b
+    b.clear()
+    b.reinit_default_clock()
+    net, P, conns, M = build_network(inp, with_monitor=True)
+    net.run(nsteps * DT)
+    th = net.stats().get("persistent_threads", 0)
+    rec = M._record()
+    spikes_equal = all(np.array_equal(x, y) for x, y in zip(rec, rec_ref))
+
+    def same(a, b_):
+        a, b_ = np.asarray(a), np.asarray(b_)
+        return bool(np.array_equal(a, b_) or np.all((a == b_) | ((a == 0) & (b_ == 0))))
+    states_equal = all(same(getattr(P, v), state_ref[v]) for v in ("v", "ge", "gi"))
+    net._invalidate()
+    return {"steps": nsteps, "neurons": inp["n"], "spikes": int(len(rec_ref[1])), "spikes_equal": bool(spikes_equal),
+            "states_equal": bool(states_equal), "persistent_threads": int(th),
+            "against": "the oracle (single-threaded C++ restatement), same network and initial state"}
 
 
 def run_reference(args):
+    """The CPU implementation of the path (the oracle restatement; the
+    reference is Python 2 with scipy.weave and cannot run here) on the same
+    network, config, metric and step size as the GPU arm; its inputs are
+    built by the oracle, without the engine library."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    inp = make_inputs(args.seed, n=args.neurons, builder=_numpy_free_builder())
     import oracle
+    inp = make_inputs(args.seed, n=args.neurons, builder=oracle.fixed_indegree_csr)
     import brian_b200 as b
     from brian_b200.network import engine
     with engine(oracle.table()):
@@ -248,13 +331,22 @@ def run_reference(args):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "CUBA-262k", "neurons": inp["n"], "indegree": INDEGREE,
-                       "sim_steps_per_step": per, "dt": DT},
-            "cpu_baseline": {"value": value, "unit": "events/s", "cores": 1, "kind": "port",
-                             "sample": "each step = %d simulation steps of CUBA-262k on the CPU restatement "
-                                       "(the reference is Python 2 and cannot run here)" % per},
+            "config": bench_config(args, inp["n"], int(len(inp["exc"][1]) + len(inp["inh"][1])), per, 1),
+            "cpu_baseline": {"value": value, "unit": "events/s", "cores": 1, "kind": "port", "host": host_cpu(),
+                             "sample": "each step = %d simulation steps of CUBA-262k on the single-threaded C++ "
+                                       "oracle restatement (the reference is Python 2 with scipy.weave and cannot "
+                                       "run here)" % per},
             "e2e": {"value": value, "unit": "events/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+def bench_config(args, n, nsyn, per, world):
+    return {"workload": "CUBA-262k: 262144 LIF, in-degree 1000 (800 exc/200 inh), f32 weights, u8 delays 1..50 "
+                        "steps, FP%d state, dt 0.1 ms" % args.precision,
+            "neurons": n, "synapses": nsyn, "sim_steps_per_step": per, "simulated_s": args.steps * per * DT,
+            "parallelism": "replicas" if world > 1 else "single",
+            "l2": "inputs larger than L2: 1.3 GB of connectivity (int32 targets, u8 delays), of which the spiking "
+                  "sources' rows are read every step; the two uint16 count rings (2 x 28 MB) stay L2-resident"}
 
 
 def fitting_bench(args):
@@ -379,7 +471,9 @@ def profile_case(case, seed):
           only bg_fit_sim launch of the process.
     gemm: one training epoch of the proposal network on 65 536 random rows,
           batch 4096 (launch 12 of k_gemm is the 512 x 512 hidden layer of
-          the second step)."""
+          the second step).
+    synapses: CUBA through Synapses (see synapses_case).
+    stdp: the STDP scale-up network, 300 steps."""
     rng = np.random.default_rng(seed)
     if case == "fit":
         from brian_b200.synthetic import (FitWorkload, adaptive_lif_equations, THRESHOLD, RESET, PARAMS,
@@ -408,6 +502,15 @@ def profile_case(case, seed):
         print(json.dumps({"case": "gemm", "train_ms": ms, "steps": n // 4096, "loss": float(loss[0])}))
     elif case == "synapses":
         print(json.dumps(synapses_case(seed)))
+    elif case == "stdp":
+        # the STDP scale-up network (164 MB of weights) for 300 steps: the
+        # outputs fire on about half the steps from step ~100 on, so launches
+        # 250+ of k_stdp_post_rows sweep the matrix in the steady regime
+        from brian_b200 import workloads
+        d = workloads.stdp_scaleup(seed=seed)
+        d["net"].run(300 * DT)
+        sp, _ = d["net"]._binding.rt.counters(2, 1)
+        print(json.dumps({"case": "stdp", "steps": 300, "input_spikes": int(sp[0]), "output_spikes": int(sp[1])}))
     else:
         raise SystemExit("unknown profile case %r" % case)
 
@@ -504,9 +607,215 @@ def synapses_case(seed, n=32768, indegree=160, sim_steps=2000, profile_steps=300
             "hbm_peak_gbs": peak, "peak_source": peak_src}
 
 
-def _numpy_free_builder():
-    from brian_b200._lib import fixed_indegree_csr_native
-    return fixed_indegree_csr_native
+def cuba4000_bench(args):
+    """The plain CUBA network (4000 LIF, p = 0.02, zero delay, FP64, 1 s,
+    SpikeMonitor and the v trace of 10 neurons) on the GPU: device time per
+    step and synaptic events/s, the oracle on the same network for the CPU
+    side, and the FP32-state run against the FP64 run."""
+    import brian_b200 as b
+    from brian_b200 import workloads
+    from brian_b200.network import engine
+    steps = 10000
+    out = {"workload": "CUBA-4000: 4000 LIF (3200 exc / 800 inh), Bernoulli p=0.02, we=1.62 mV, wi=-9 mV, zero "
+                       "delay, dt 0.1 ms, 1 s, SpikeMonitor + v of 10 neurons"}
+    recs = {}
+    for prec in (64, 32):
+        b.set_global_preferences(precision=prec)
+        b.clear()
+        b.reinit_default_clock()
+        net, P, M, S = workloads.cuba4000(seed=args.seed)
+        net.prepare()
+        rt = net._binding.rt
+        net.run(steps * DT)
+        st = rt.stats()
+        ev = int(rt.counters(1, 2)[1].sum())
+        recs[prec] = (tuple(x.copy() for x in M._record()), S._record()[1].copy())
+        if prec == 64:
+            out.update({"device_ms": st["last_run_ms"], "us_per_step": st["last_run_ms"] * 1e3 / steps,
+                        "events": ev, "events_per_s": ev / (st["last_run_ms"] * 1e-3),
+                        "spikes": int(len(recs[64][0][1])), "launches": int(st["launches"])})
+        else:
+            out["fp32_us_per_step"] = st["last_run_ms"] * 1e3 / steps
+        net._invalidate()
+    b.set_global_preferences(precision=args.precision)
+    out["precision"] = precision_report(recs[64][0], recs[32][0], 4000, steps * DT, recs[64][1], recs[32][1])
+    if not args.no_cpu:
+        import oracle
+        b.clear()
+        b.reinit_default_clock()
+        with engine(oracle.table()):
+            net, P, M, S = workloads.cuba4000(seed=args.seed)
+            net.prepare()
+            rt = net._binding.rt
+            t0 = time.perf_counter()
+            net.run(steps * DT)
+            wall = time.perf_counter() - t0
+            ev = int(rt.counters(1, 2)[1].sum())
+            same = all(np.array_equal(x, y) for x, y in zip(M._record(), recs[64][0]))
+        net._invalidate()
+        out["cpu_baseline"] = {"value": ev / wall, "unit": "events/s", "cores": 1, "kind": "port",
+                               "sample": "the whole run (1 s simulated) on the single-threaded C++ oracle"}
+        out["spikes_equal_oracle"] = bool(same)
+    return out
+
+
+def cuba262k_precision(args, inp, nsteps=2000):
+    """CUBA-262k with FP32 state against FP64 (same network and initial
+    state, spike monitor and v of 10 neurons, `nsteps` steps), and the FP32
+    path's events/s on the benchmark shape (no monitors, persistent kernel)."""
+    import brian_b200 as b
+    recs = {}
+    for prec in (64, 32):
+        b.set_global_preferences(precision=prec)
+        b.clear()
+        b.reinit_default_clock()
+        from brian_b200.workloads import cuba_scaled
+        net, P, conns, M, S = cuba_scaled(inp, spike_monitor=True, record=range(10))
+        net.run(nsteps * DT)
+        recs[prec] = (tuple(x.copy() for x in M._record()), S._record()[1].copy())
+        net._invalidate()
+    out = {"compare": precision_report(recs[64][0], recs[32][0], inp["n"], nsteps * DT, recs[64][1], recs[32][1])}
+    # FP32 throughput on the bench shape
+    b.set_global_preferences(precision=32)
+    b.clear()
+    b.reinit_default_clock()
+    net, P, conns, _ = build_network(inp)
+    net.prepare()
+    rt = net._binding.rt
+    net.run(2000 * DT)
+    _, ev0 = rt.counters(1, 2)
+    dev_ms = 0.0
+    for _ in range(5):
+        net.run(SIM_STEPS_PER_BENCH_STEP * DT)
+        dev_ms += rt.stats()["last_run_ms"]
+    _, ev1 = rt.counters(1, 2)
+    ev = int(ev1.sum() - ev0.sum())
+    out["fp32_events_per_s"] = ev / (dev_ms * 1e-3)
+    out["fp32_us_per_step"] = dev_ms * 1e3 / (5 * SIM_STEPS_PER_BENCH_STEP)
+    out["fp32_persistent_threads"] = int(net.stats().get("persistent_threads", 0))
+    net._invalidate()
+    b.set_global_preferences(precision=args.precision)
+    return out
+
+
+def stdp_bench(args):
+    """The STDP scale-up (10 000 Poisson inputs at 5-25 Hz onto 4096 LIF
+    outputs, all to all, dense f32 W of 41 M plastic synapses,
+    ExponentialSTDP, 10 s): device time per step, synaptic events (input
+    spikes x 4096) and postsynaptic weight updates (output spikes x 10 000)
+    per second, the row-sweep kernel against the HBM peak, the final weight
+    histogram; the oracle on a shortened run of the same network (weights,
+    traces and spikes compared exactly); the FP32-state run against FP64."""
+    import brian_b200 as b
+    from brian_b200 import workloads
+    from brian_b200.network import engine
+    nin, nout, steps = 10000, 4096, args.stdp_steps
+    out = {"workload": "STDP scale-up: 10000 Poisson inputs (rates U[5,25] Hz) -> 4096 LIF outputs all-to-all, "
+                       "dense f32 W (41M plastic synapses), ExponentialSTDP taupre=taupost=20 ms, gmax=0.01, "
+                       "dApre=0.01 gmax, dApost=-1.05 dApre, dt 0.1 ms",
+           "sim_steps": steps}
+    recs = {}
+    peak, peak_src = peaks()
+    for prec in (64, 32):
+        b.set_global_preferences(precision=prec)
+        b.clear()
+        b.reinit_default_clock()
+        d = workloads.stdp_scaleup(seed=args.seed, spike_record=256, record=range(10))
+        net = d["net"]
+        net.prepare()
+        rt = net._binding.rt
+        t0 = time.perf_counter()
+        dev_ms = 0.0
+        chunk = 10000
+        for k in range(0, steps, chunk):
+            net.run(min(chunk, steps - k) * DT)
+            dev_ms += rt.stats()["last_run_ms"]
+        wall = time.perf_counter() - t0
+        sp, ev = rt.counters(2, 1)
+        recs[prec] = (tuple(x.copy() for x in d["M"]._record()), d["S"]._record()[1].copy())
+        W = d["C"]._weights()
+        hist = np.histogram(W, bins=20, range=(0, d["gmax"]))[0]
+        if prec == 64:
+            pre, post = int(sp[0]), int(sp[1])
+            out.update({"device_ms": dev_ms, "wall_s": wall, "us_per_step": dev_ms * 1e3 / steps,
+                        "input_spikes": pre, "output_spikes": post,
+                        "output_rate_hz": post / (nout * steps * DT),
+                        "synaptic_events_per_s": pre * nout / (dev_ms * 1e-3),
+                        "weight_updates_per_s": (pre * nout + post * nin) / (dev_ms * 1e-3),
+                        "w_hist_edges": [0.0, d["gmax"]], "w_hist": hist.tolist(),
+                        "w_mean": float(W.mean())})
+            # kernel durations (CUDA events between launches) over 200 steps
+            # of a monitor-free copy in the steady firing regime
+            net._invalidate()
+            b.clear()
+            b.reinit_default_clock()
+            dp = workloads.stdp_scaleup(seed=args.seed)
+            dp["net"].run(500 * DT)
+            rtp = dp["net"]._binding.rt
+            sp1, _ = rtp.counters(2, 1)
+            prof = rtp.profile(200, dp["net"].clock.step)
+            sp2, _ = rtp.counters(2, 1)
+            dp["net"]._invalidate()
+            post_per_step = (int(sp2[1]) - int(sp1[1])) / 200.0
+            pre_per_step = (int(sp2[0]) - int(sp1[0])) / 200.0
+            kern = dict(prof)
+            name = [k for k in kern if k.startswith("stdp_post_rows")][0]
+            # algorithmic bytes of the postsynaptic sweep: each weight of a
+            # spiking column read and written (8 B); the sweep itself moves
+            # every 16-byte group holding such a weight
+            alg = post_per_step * nin * 8
+            out["kernels_us"] = {k: round(v * 1e3, 3) for k, v in prof}
+            out["post_sweep"] = {"kernel": name, "us": kern[name] * 1e3, "output_spikes_per_step": post_per_step,
+                                 "alg_bytes": alg, "achieved_gbs": alg / (kern[name] * 1e-3) / 1e9,
+                                 "matrix_bytes_per_step": nin * nout * 4 * 2,
+                                 "matrix_gbs": nin * nout * 8 / (kern[name] * 1e-3) / 1e9,
+                                 "peak": peak, "peak_source": peak_src,
+                                 "frac": alg / (kern[name] * 1e-3) / 1e9 / peak}
+            step_bytes = post_per_step * nin * 8 + pre_per_step * nout * (8 + 8) + (nin + nout) * 16 + nout * 32
+            out["step_alg_bytes"] = step_bytes
+            out["step_frac"] = step_bytes / (dev_ms * 1e-3 / steps) / 1e9 / peak
+        else:
+            out["fp32_us_per_step"] = dev_ms * 1e3 / steps
+            out["fp32_w_hist"] = hist.tolist()
+            net._invalidate()
+    b.set_global_preferences(precision=args.precision)
+    out["precision"] = precision_report(recs[64][0], recs[32][0], 256, steps * DT, recs[64][1], recs[32][1])
+    # the oracle on a shortened run, compared exactly
+    if not args.no_cpu:
+        import oracle
+        ps = args.stdp_parity_steps
+        res = {}
+        for tab in (oracle.table(), None):
+            b.clear()
+            b.reinit_default_clock()
+            ctx = engine(tab) if tab is not None else None
+            if ctx:
+                ctx.__enter__()
+            try:
+                d = workloads.stdp_scaleup(seed=args.seed, spike_record=nout)
+                d["net"].prepare()
+                t0 = time.perf_counter()
+                d["net"].run(ps * DT)
+                wall = time.perf_counter() - t0
+                a_pre, a_post = d["stdp"]._traces()
+                res[tab is None] = {"W": d["C"]._weights().copy(), "A": (a_pre.copy(), a_post.copy()),
+                                    "spk": tuple(x.copy() for x in d["M"]._record()), "wall": wall,
+                                    "events": int(d["net"]._binding.rt.counters(2, 1)[0][0]) * nout}
+                d["net"]._invalidate()
+            finally:
+                if ctx:
+                    ctx.__exit__(None, None, None)
+        o, g = res[False], res[True]
+        out["parity"] = {"steps": ps, "w_equal": bool(np.array_equal(o["W"], g["W"])),
+                         "traces_equal": bool(all(np.array_equal(x, y) for x, y in zip(o["A"], g["A"]))),
+                         "spikes_equal": bool(all(np.array_equal(x, y) for x, y in zip(o["spk"], g["spk"]))),
+                         "w_hist_equal": bool(np.array_equal(np.histogram(o["W"], 20, (0, 0.01))[0],
+                                                             np.histogram(g["W"], 20, (0, 0.01))[0])),
+                         "output_spikes": int(len(o["spk"][1]))}
+        out["cpu_baseline"] = {"value": o["events"] / o["wall"], "unit": "synaptic events/s", "cores": 1,
+                               "kind": "port", "sample": "first %d steps of the same network on the single-threaded "
+                               "C++ oracle (%.1f s wall)" % (ps, o["wall"])}
+    return out
 
 
 def main():
@@ -519,19 +828,24 @@ def main():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--profile-steps", type=int, default=300)
     ap.add_argument("--cpu-steps", type=int, default=1000)
-    ap.add_argument("--ref-sim-steps", type=int, default=50)
+    ap.add_argument("--ref-sim-steps", type=int, default=SIM_STEPS_PER_BENCH_STEP)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--neurons", type=int, default=N_NEURONS)
     ap.add_argument("--no-fit", action="store_true", help="skip the model-fitting half of the metric")
     ap.add_argument("--no-synapses", action="store_true", help="skip the Synapses measurement")
+    ap.add_argument("--no-stdp", action="store_true", help="skip the STDP scale-up measurement")
+    ap.add_argument("--no-cuba4000", action="store_true", help="skip the CUBA-4000 measurement")
+    ap.add_argument("--no-precision", action="store_true", help="skip the FP32-vs-FP64 report of CUBA-262k")
+    ap.add_argument("--stdp-steps", type=int, default=100000, help="simulation steps of the STDP scale-up run")
+    ap.add_argument("--stdp-parity-steps", type=int, default=240)
     ap.add_argument("--persist-threads", type=int, default=None, choices=[256, 512],
                     help="threads per block of the persistent kernel (default: automatic)")
     ap.add_argument("--fit-targets", type=int, default=256)
     ap.add_argument("--fit-train", type=int, default=1 << 20)
     ap.add_argument("--fit-epochs", type=int, default=40)
     ap.add_argument("--fit-iters", type=int, default=40)
-    ap.add_argument("--profile-case", choices=["fit", "gemm", "synapses"], default=None,
+    ap.add_argument("--profile-case", choices=["fit", "gemm", "synapses", "stdp"], default=None,
                     help="run one small case for a single-kernel ncu capture and exit")
     args = ap.parse_args()
     if args.profile_case:
@@ -549,20 +863,22 @@ def main():
     net.prepare()
     rt = net._binding.rt
     per = SIM_STEPS_PER_BENCH_STEP
-    for _ in range(args.warmup):
-        net.run(per * DT)
-    _, ev0 = rt.counters(1, 2)
-    sp0, _ = rt.counters(1, 2)
-    l0 = rt.stats()["launches"]
-    dev_ms = 0.0
-    barrier(world)
+    # clocks are sampled every 50 ms from the warm-up steps on (the timed
+    # region alone is shorter than nvidia-smi's sampling at small --steps)
     with ClockSampler(local) as clk:
+        for _ in range(args.warmup):
+            net.run(per * DT)
+        _, ev0 = rt.counters(1, 2)
+        sp0, _ = rt.counters(1, 2)
+        l0 = rt.stats()["launches"]
+        dev_ms = 0.0
+        barrier(world)
         t0 = time.perf_counter()
         for _ in range(args.steps):
             net.run(per * DT)
             dev_ms += rt.stats()["last_run_ms"]
         wall = time.perf_counter() - t0
-    barrier(world)
+        barrier(world)
     sp1, ev1 = rt.counters(1, 2)
     launches = rt.stats()["launches"] - l0
     persist_threads = rt.stats().get("persistent_threads", 0)
@@ -633,41 +949,48 @@ def main():
                "wall_s": wall_e2e, "includes": "network upload (CSR, weights, delays, state), run, spike read-back"}
         net2._invalidate()
 
-    cpu = None
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(inp, args.cpu_steps)
+        cpu, rec_ref, state_ref = cpu_baseline(inp, args.cpu_steps)
+        # the GPU engine from the same state, compared with the oracle's
+        # spikes and final state
+        parity = gpu_parity(inp, args.cpu_steps, rec_ref, state_ref)
 
-    # the fitting half runs on one GPU (a single-rank job)
-    fitting = None
-    if rank == 0 and world == 1 and not args.no_fit:
-        fitting = fitting_bench(args)
-
-    # Synapses (static, queue-ordered delivery): the --profile-case synapses
-    # workload, reported beside the headline (after its timed region)
-    synapses = None
-    if rank == 0 and world == 1 and not args.no_synapses:
+    def guarded(fn, *a):
+        # the headline line is printed even if a side measurement fails
         try:
-            synapses = synapses_case(args.seed)
-        except Exception as e:  # the headline line is printed either way
-            synapses = {"error": "%s: %s" % (type(e).__name__, e)}
+            return fn(*a)
+        except Exception as e:
+            return {"error": "%s: %s" % (type(e).__name__, e)}
+
+    side = {}
+    if rank == 0 and world == 1:
+        if not args.no_cuba4000:
+            side["cuba4000"] = guarded(cuba4000_bench, args)
+        if not args.no_precision:
+            side["precision_cuba262k"] = guarded(cuba262k_precision, args, inp)
+        if not args.no_stdp:
+            side["stdp"] = guarded(stdp_bench, args)
+        # the fitting half runs on one GPU (a single-rank job)
+        if not args.no_fit:
+            side["fitting"] = fitting_bench(args)
+        # Synapses (static, queue-ordered delivery): the --profile-case
+        # synapses workload, reported beside the headline
+        if not args.no_synapses:
+            side["synapses"] = guarded(synapses_case, args.seed)
 
     if rank == 0:
+        config = bench_config(args, n, int(len(inp["exc"][1]) + len(inp["inh"][1])), per, world)
+        config["persistent_threads"] = persist_threads
         line = {"metric": "synaptic events/s (CUBA-262k)", "value": value, "unit": "events/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64" if args.precision == 64 else "f32", "data": "synthetic",
-                "config": {"workload": "CUBA-262k: 262144 LIF, in-degree 1000 (800 exc/200 inh), f32 weights, "
-                                       "u8 delays 1..50 steps, FP%d state, dt 0.1 ms" % args.precision,
-                           "neurons": n, "synapses": int(len(inp["exc"][1]) + len(inp["inh"][1])),
-                           "sim_steps_per_step": per, "simulated_s": args.steps * per * DT,
-                           "persistent_threads": persist_threads,
-                           "parallelism": "replicas" if world > 1 else "single",
-                           "l2": "inputs larger than L2: 1.3 GB of connectivity (int32 targets, u8 delays), of "
-                                 "which the spiking sources' rows are read every step; the two uint16 count rings "
-                                 "(2 x 28 MB) stay L2-resident"},
+                "config": config,
                 "mean_rate_hz": rate_hz, "events_timed": total_events, "wall_s": wall,
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-                "clocks": clk.summary(), "fitting": fitting, "synapses": synapses}
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "parity": parity,
+                "gpu_launches": int(launches), "clocks": clk.summary()}
+        line.update(side)
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist

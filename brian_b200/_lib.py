@@ -183,6 +183,7 @@ class Runtime(object):
         nvar, n = S0.shape
         gid = _i32()
         self._c(self.t.group_add(self.h, n, nvar, _ptr(S0), ct.byref(gid)), "group_add")
+        self._ng = max(getattr(self, "_ng", 0), gid.value + 1)
         return gid.value
 
     def group_set_linear(self, gid, A, C):
@@ -236,6 +237,7 @@ class Runtime(object):
         self._c(self.t.conn_add(self.h, src, so, sn, tgt, to, tn, var, len(cols), _ptr(rowptr), _ptr(cols),
                                 _ptr(w), wbits, int(delay_steps), _ptr(d), int(ring_depth), int(mod_var),
                                 ct.byref(cid)), "conn_add")
+        self._nc = max(getattr(self, "_nc", 0), cid.value + 1)
         return cid.value
 
     def conn_add_shared(self, src, so, sn, tgt, to, tn, var, rowptr, cols, weight, dtype, delay_steps=0,
@@ -254,6 +256,7 @@ class Runtime(object):
         self._c(self.t.conn_add_shared(self.h, src, so, sn, tgt, to, tn, var, len(cols), _ptr(rowptr), _ptr(cols),
                                        float(weight), wbits, int(delay_steps), _ptr(d), int(ring_depth),
                                        int(mod_var), ct.byref(cid)), "conn_add_shared")
+        self._nc = max(getattr(self, "_nc", 0), cid.value + 1)
         return cid.value
 
     def conn_add_dense(self, src, so, sn, tgt, to, tn, var, W, delay_steps=0, mod_var=-1):
@@ -264,6 +267,7 @@ class Runtime(object):
         cid = _i32()
         self._c(self.t.conn_add_dense(self.h, src, so, sn, tgt, to, tn, var, _ptr(W), wbits, int(delay_steps),
                                       int(mod_var), ct.byref(cid)), "conn_add_dense")
+        self._nc = max(getattr(self, "_nc", 0), cid.value + 1)
         return cid.value
 
     def conn_get_weights(self, cid, count):
@@ -374,8 +378,9 @@ class Runtime(object):
         self._c(self.t.net_reinit(self.h), "net_reinit")
 
     def counters(self, ngroups, nconns):
-        g = np.zeros(max(1, ngroups), dtype=np.int64)
-        c = np.zeros(max(1, nconns), dtype=np.int64)
+        # the engine writes one entry per group and per connection it holds
+        g = np.zeros(max(1, ngroups, getattr(self, "_ng", 0)), dtype=np.int64)
+        c = np.zeros(max(1, nconns, getattr(self, "_nc", 0)), dtype=np.int64)
         self._c(self.t.net_counters(self.h, _ptr(g), _ptr(c)), "net_counters")
         return g[:ngroups], c[:nconns]
 

@@ -460,23 +460,27 @@ template <typename T> struct PropArgs {
 // mode 1: w * (1 + a); mode 2: w + (wx - w) * a, wx the exact maximum
 // weight of the code string (stdp.py:510-533); modes 1 and 2 on FP64
 // weights only.
-template <typename T, typename WT>
-__device__ __forceinline__ void stdp_w(WT *w, int64_t k, double add, double wmin, double wmax, int mode = 0,
-                                       double wx = 0.0) {
+template <typename WT>
+__device__ __forceinline__ WT stdp_w_val(WT w, double add, double wmin, double wmax, int mode = 0, double wx = 0.0) {
     if (sizeof(WT) == 4) {
-        float x = __double2float_rn(__dadd_rn((double)w[k], add));
+        float x = __double2float_rn(__dadd_rn((double)w, add));
         const float lo = __double2float_rn(wmin), hi = __double2float_rn(wmax);
         x = x < lo ? lo : (x > hi ? hi : x);
-        w[k] = (WT)x;
+        return (WT)x;
     } else {
-        const double w0 = (double)w[k];
+        const double w0 = (double)w;
         double x;
         if (mode == 1) x = __dmul_rn(w0, __dadd_rn(1.0, add));
         else if (mode == 2) x = __dadd_rn(w0, __dmul_rn(__dsub_rn(wx, w0), add));
         else x = __dadd_rn(w0, add);
         x = x < wmin ? wmin : (x > wmax ? wmax : x);
-        w[k] = (WT)x;
+        return (WT)x;
     }
+}
+template <typename T, typename WT>
+__device__ __forceinline__ void stdp_w(WT *w, int64_t k, double add, double wmin, double wmax, int mode = 0,
+                                       double wx = 0.0) {
+    w[k] = stdp_w_val<WT>(w[k], add, wmin, wmax, mode, wx);
 }
 
 // Shared-weight path (every addend of one accumulator is the same number, so
@@ -663,13 +667,31 @@ __global__ void __launch_bounds__(kDenseThreads) k_prop_dense(const PropArgs<T> 
                 __syncthreads();
                 const int n = min(kDenseList, total - bstart);
                 if (j < a.tn) {
-                    for (int s = 0; s < n; ++s) {
+                    // eight rows' weights loaded before any is used (the rows
+                    // are distinct, so the stores below never feed a load)
+                    constexpr int kB = 8;
+                    int s = 0;
+                    for (; s + kB <= n; s += kB) {
+                        WT wl[kB];
+#pragma unroll
+                        for (int u = 0; u < kB; ++u) wl[u] = W[(int64_t)sp[s + u] * a.tn + j];
+#pragma unroll
+                        for (int u = 0; u < kB; ++u) {
+                            const int64_t i = sp[s + u];
+                            T wv = (T)wl[u];
+                            if (a.mod) wv = rn<T>::mul(wv, a.mod[i]);
+                            acc = rn<T>::add(acc, wv);
+                            if (a.stdp) W[i * a.tn + j] = stdp_w_val<WT>(wl[u], apost, a.wmin, a.wmax, a.wmode, a.wx);
+                        }
+                    }
+                    for (; s < n; ++s) {
                         const int64_t i = sp[s];
                         const int64_t k = i * a.tn + j;
-                        T wv = (T)W[k];
+                        const WT w0 = W[k];
+                        T wv = (T)w0;
                         if (a.mod) wv = rn<T>::mul(wv, a.mod[i]);
                         acc = rn<T>::add(acc, wv);
-                        if (a.stdp) stdp_w<T, WT>(W, k, apost, a.wmin, a.wmax, a.wmode, a.wx);
+                        if (a.stdp) W[k] = stdp_w_val<WT>(w0, apost, a.wmin, a.wmax, a.wmode, a.wx);
                     }
                 }
                 if (a.stdp && blockIdx.x == 0)
@@ -885,6 +907,114 @@ __global__ void __launch_bounds__(256) k_stdp_post(const PostArgs a) {
                     const int64_t j = sp[s];
                     a.A_post[j] = a.post_set ? a.Am : __dadd_rn(a.A_post[j], a.Am);
                 }
+            __syncthreads();
+        }
+    }
+    bg_finish_step(a.ctl, a.last);
+}
+
+// Postsynaptic STDP on a dense connection as a sweep over the rows:
+// w[i,j] (+)= A_pre[i], clipped, for every target j that spiked this step
+// (stdp.py:395-408; the column updates of different spikes touch disjoint
+// elements, so one pass over the matrix applies all of them).  Each block
+// takes bands of kPostRows rows; the spike bits of the step sit in shared
+// memory and a group of 4 columns (one 16-byte vector of f32 weights) is
+// loaded and stored only when one of its targets spiked.  Odd steps walk the
+// bands from the end of the matrix, so the part of the previous step's sweep
+// still in L2 is read first.  Block 0 also applies A_post[j] (+)= Am.
+constexpr int kPostThreads = 256;
+constexpr int kPostRows = 8;
+constexpr int kPostVec = 4;                 // 16-byte groups per thread and row in flight
+constexpr int kPostMaskWords = 2048;        // targets per pass: 65 536
+// the lanes of one 16-byte group of f32 weights whose targets spiked
+__device__ __forceinline__ void post_vec(float4 &v, uint32_t nib, double add, const PostArgs &a) {
+    if (nib & 1u) v.x = stdp_w_val<float>(v.x, add, a.wmin, a.wmax, a.wmode, a.wx);
+    if (nib & 2u) v.y = stdp_w_val<float>(v.y, add, a.wmin, a.wmax, a.wmode, a.wx);
+    if (nib & 4u) v.z = stdp_w_val<float>(v.z, add, a.wmin, a.wmax, a.wmode, a.wx);
+    if (nib & 8u) v.w = stdp_w_val<float>(v.w, add, a.wmin, a.wmax, a.wmode, a.wx);
+}
+template <typename WT>
+__global__ void __launch_bounds__(kPostThreads) k_stdp_post_rows(const PostArgs a) {
+    __shared__ uint32_t mask[kPostMaskWords];
+    __shared__ int any;
+    const long long nstep = a.ctl->nstep;
+    if (nstep >= a.delay) {
+        const uint32_t *H = a.hist + (int64_t)((int)(nstep - a.delay) % a.depth) * a.nwords;
+        const int sh = (int)(a.to & 31);
+        const int64_t wbase = a.to >> 5;
+        const int64_t hend = a.nwords;
+        WT *W = (WT *)a.w;
+        const int64_t nb = (a.sn + kPostRows - 1) / kPostRows;
+        for (int64_t c0 = 0; c0 < a.tn; c0 += (int64_t)kPostMaskWords * 32) {
+            const int64_t cn = min((int64_t)kPostMaskWords * 32, a.tn - c0);
+            const int nw = (int)((cn + 31) >> 5);
+            if (threadIdx.x == 0) any = 0;
+            __syncthreads();
+            int mine = 0;
+            for (int q = threadIdx.x; q < nw; q += kPostThreads) {
+                // bits of targets to + c0 + 32q .. +31, shifted out of the history words
+                const int64_t hw = wbase + ((c0 >> 5) + q);
+                uint32_t lo = H[hw], hi = (sh && hw + 1 < hend) ? H[hw + 1] : 0u;
+                uint32_t m = sh ? ((lo >> sh) | (hi << (32 - sh))) : lo;
+                const int64_t left = cn - ((int64_t)q << 5);
+                if (left < 32) m &= (1u << left) - 1u;
+                mask[q] = m;
+                mine |= (m != 0u);
+            }
+            if (mine) any = 1;
+            __syncthreads();
+            if (any) {
+                if (blockIdx.x == 0)
+                    for (int q = threadIdx.x; q < nw; q += kPostThreads) {
+                        uint32_t m = mask[q];
+                        while (m) {
+                            const int b = __ffs(m) - 1; m &= m - 1;
+                            const int64_t j = c0 + ((int64_t)q << 5) + b;
+                            a.A_post[j] = a.post_set ? a.Am : __dadd_rn(a.A_post[j], a.Am);
+                        }
+                    }
+                const bool vec = sizeof(WT) == 4 && (a.tn & 3) == 0 && (c0 & 3) == 0 &&
+                                 (((uintptr_t)W) & 15) == 0;
+                for (int64_t bb = blockIdx.x; bb < nb; bb += gridDim.x) {
+                    const int64_t band = (nstep & 1) ? nb - 1 - bb : bb;
+                    const int64_t r0 = band * kPostRows, r1 = min(a.sn, r0 + kPostRows);
+                    if (vec) {
+                        // two rows at a time, every 16-byte group of both
+                        // loaded before any is updated and stored
+                        for (int64_t i = r0; i < r1; i += 2) {
+                            const bool two = i + 1 < r1;
+                            const double add0 = a.A_pre[i], add1 = two ? a.A_pre[i + 1] : 0.0;
+                            float4 *row0 = reinterpret_cast<float4 *>(W + i * a.tn + c0);
+                            float4 *row1 = reinterpret_cast<float4 *>(W + (two ? i + 1 : i) * a.tn + c0);
+                            for (int64_t cc = 0; cc < cn; cc += 4 * kPostThreads * kPostVec) {
+                                float4 v0[kPostVec], v1[kPostVec];
+                                uint32_t nib[kPostVec];
+#pragma unroll
+                                for (int u = 0; u < kPostVec; ++u) {
+                                    const int64_t g = (cc >> 2) + threadIdx.x + u * kPostThreads;
+                                    nib[u] = 4 * g < cn ? (mask[g >> 3] >> ((g & 7) * 4)) & 15u : 0u;
+                                    if (nib[u]) { v0[u] = row0[g]; if (two) v1[u] = row1[g]; }
+                                }
+#pragma unroll
+                                for (int u = 0; u < kPostVec; ++u) {
+                                    if (!nib[u]) continue;
+                                    const int64_t g = (cc >> 2) + threadIdx.x + u * kPostThreads;
+                                    post_vec(v0[u], nib[u], add0, a);
+                                    row0[g] = v0[u];
+                                    if (two) { post_vec(v1[u], nib[u], add1, a); row1[g] = v1[u]; }
+                                }
+                            }
+                        }
+                    } else {
+                        for (int64_t i = r0; i < r1; ++i) {
+                            const double add = a.A_pre[i];
+                            WT *row = W + i * a.tn + c0;
+                            for (int64_t c = threadIdx.x; c < cn; c += kPostThreads)
+                                if ((mask[c >> 5] >> (c & 31)) & 1u) stdp_w<double, WT>(row, c, add, a.wmin, a.wmax, a.wmode, a.wx);
+                        }
+                    }
+                }
+            }
             __syncthreads();
         }
     }

@@ -480,8 +480,21 @@ int build_stdp_post(bg_net *net, int sid) {
     a.post_set = (s.inter != BG_STDP_ALL);   // 'nearest_pre' writes A_post=+Am (stdp.py:500-502)
     a.wmin = s.wmin; a.wmax = s.wmax; a.wmode = s.post_mode; a.wx = s.wx;
     if (s.delayed) { a.H_pre = s.dHpre; a.hlen = s.hlen; a.lagc = s.dLagPostC; }
-    const int64_t grid = c.dense ? std::max<int64_t>(1, std::min<int64_t>((c.sn + 255) / 256, (int64_t)sm_count() * 2)) : 8;
     const int wb = c.w_bits;
+    if (c.dense) {
+        // one pass over the rows applies every column update of the step
+        const int64_t bands = (c.sn + bg::kPostRows - 1) / bg::kPostRows;
+        const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(bands, (int64_t)sm_count() * 8));
+        net->item_names.push_back("stdp_post_rows[s" + std::to_string(sid) + "]");
+        net->step_launches.push_back([a, grid, wb](cudaStream_t st, int, int last) {
+            bg::PostArgs b = a; b.last = last;
+            if (wb == 64) bg::k_stdp_post_rows<double><<<(unsigned)grid, bg::kPostThreads, 0, st>>>(b);
+            else bg::k_stdp_post_rows<float><<<(unsigned)grid, bg::kPostThreads, 0, st>>>(b);
+            return cudaGetLastError();
+        });
+        return BG_OK;
+    }
+    const int64_t grid = 8;
     net->item_names.push_back("stdp_post[s" + std::to_string(sid) + "]");
     net->step_launches.push_back([a, grid, wb](cudaStream_t st, int, int last) {
         bg::PostArgs b = a; b.last = last;

@@ -762,15 +762,26 @@ static void step(or_net *n, int64_t cs) {
         } else if (it.kind == IT_STDP_POST) {
             Stdp &s = n->stdps[it.id]; Conn &c = n->conns[s.cid];
             get_spikes(n->groups[c.tgt], s.post_delay, c.to, c.tn, spk);
+            if (c.dense) {
+                /* w[:, j] += A_pre for every spiking j: the columns are
+                 * disjoint, so the matrix is walked row by row (one update
+                 * of each element, as column by column) */
+                for (int32_t j : spk) {
+                    if (s.inter == 0) s.A_post[j] = s.A_post[j] + s.Am; else s.A_post[j] = s.Am;
+                }
+                for (int64_t i = 0; i < c.sn && !spk.empty(); ++i) {
+                    const double add = s.A_pre[i];
+                    for (int32_t j : spk) {
+                        size_t k = (size_t)i * c.tn + j;
+                        if (c.w_bits == 64) c.w64[k] = clipd(wupd(c.w64[k], add, s.post_mode, s.wx), s.wmin, s.wmax);
+                        else c.w32[k] = clipf((float)((double)c.w32[k] + add), (float)s.wmin, (float)s.wmax);
+                    }
+                }
+                continue;
+            }
             for (int32_t j : spk) {
                 if (s.inter == 0) s.A_post[j] = s.A_post[j] + s.Am; else s.A_post[j] = s.Am;   /* 'nearest_pre' is A_post=+Am */
-                if (c.dense) {
-                    for (int64_t i = 0; i < c.sn; ++i) {
-                        size_t k = (size_t)i * c.tn + j;
-                        if (c.w_bits == 64) c.w64[k] = clipd(wupd(c.w64[k], s.A_pre[i], s.post_mode, s.wx), s.wmin, s.wmax);
-                        else c.w32[k] = clipf((float)((double)c.w32[k] + s.A_pre[i]), (float)s.wmin, (float)s.wmax);
-                    }
-                } else {
+                {
                     for (int64_t p = c.colptr[j]; p < c.colptr[j + 1]; ++p) {
                         int64_t k = c.colk[p]; int32_t i = c.colsrc[p];
                         if (c.w_bits == 64) c.w64[k] = clipd(wupd(c.w64[k], s.A_pre[i], s.post_mode, s.wx), s.wmin, s.wmax);
