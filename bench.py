@@ -70,71 +70,6 @@ def host_cpu():
     return {"nproc": os.cpu_count(), "model": model}
 
 
-def spike_trains(steps, idx, n, dt=DT):
-    """Per-neuron spike times (s) of a SpikeMonitor record."""
-    steps = np.asarray(steps)
-    idx = np.asarray(idx)
-    order = np.argsort(idx, kind="stable")
-    cuts = np.searchsorted(idx[order], np.arange(n + 1))
-    t = steps[order] * dt
-    return [t[cuts[i]:cuts[i + 1]] for i in range(n)]
-
-
-def precision_report(rec64, rec32, n, duration, v64=None, v32=None, delta=4e-3):
-    """Agreement of an FP32-state run with the FP64 run of the same network:
-    gamma factor (delta 4 ms, tools/statistics.py:261-314) of each neuron's
-    FP32 train against its FP64 train, over neurons with at least two FP64
-    spikes and 2 delta r < 1 (gamma is undefined at higher rates); firing
-    rates and their relative error; the fraction of FP64 spikes (step,
-    index) the FP32 run repeats exactly; the RMS difference of the recorded
-    v traces."""
-    from brian_b200.statistics import gamma_factor
-    t64 = spike_trains(rec64[0], rec64[1], n)
-    t32 = spike_trains(rec32[0], rec32[1], n)
-    g, skipped = [], 0
-    for a, b_ in zip(t32, t64):
-        if len(b_) < 2:
-            continue
-        r = (len(b_) - 1) / (b_[-1] - b_[0]) if b_[-1] > b_[0] else np.inf
-        if not 2 * delta * r < 1:
-            skipped += 1
-            continue
-        g.append(float(gamma_factor(a, b_, delta, dt=DT)))
-    # the windows [0, T) over which the FP32 run still tracks the FP64 one
-    windows = {}
-    for T in (0.01, 0.02, 0.05, 0.1, 0.2, 0.5, 1.0, 2.0, 5.0, 10.0):
-        if T > duration + 1e-12:
-            break
-        gw = []
-        for a, b_ in zip(t32, t64):
-            b_ = b_[b_ < T]
-            if len(b_) < 2 or b_[-1] <= b_[0]:
-                continue
-            r = (len(b_) - 1) / (b_[-1] - b_[0])
-            if 2 * delta * r < 1:
-                gw.append(float(gamma_factor(a[a < T], b_, delta, dt=DT)))
-        windows["%g" % (T * 1e3)] = float(np.mean(gw)) if gw else None
-    key64 = np.asarray(rec64[0], dtype=np.int64) * n + np.asarray(rec64[1], dtype=np.int64)
-    key32 = np.asarray(rec32[0], dtype=np.int64) * n + np.asarray(rec32[1], dtype=np.int64)
-    match = len(np.intersect1d(key64, key32)) / max(1, len(key64))
-    r64 = len(key64) / (n * duration)
-    r32 = len(key32) / (n * duration)
-    out = {"neurons": n, "duration_s": duration, "delta_ms": delta * 1e3,
-           "gamma_mean": float(np.mean(g)) if g else None, "gamma_median": float(np.median(g)) if g else None,
-           "gamma_min": float(np.min(g)) if g else None,
-           "gamma_frac_ge_0.95": float(np.mean(np.asarray(g) >= 0.95)) if g else None,
-           "gamma_neurons": len(g), "gamma_skipped_rate": skipped,
-           "rate_fp64_hz": r64, "rate_fp32_hz": r32, "rate_rel_err": abs(r32 - r64) / r64 if r64 > 0 else None,
-           "spikes_fp64": int(len(key64)), "spikes_fp32": int(len(key32)), "spike_match_frac": float(match),
-           "gamma_mean_by_window_ms": windows}
-    diff = np.setxor1d(key64, key32)
-    out["first_differing_step"] = int(diff.min() // n) if len(diff) else None
-    if v64 is not None and v32 is not None:
-        d = np.asarray(v32, dtype=np.float64) - np.asarray(v64, dtype=np.float64)
-        out["v_rms_err_mV"] = float(np.sqrt(np.mean(d * d)) * 1e3)
-    return out
-
-
 def out_degree_events(inp, steps, idx):
     """Events of recorded spikes: out-degree of each spiking source."""
     deg = np.concatenate([np.diff(inp["exc"][0]), np.diff(inp["inh"][0])])
@@ -607,6 +542,9 @@ def synapses_case(seed, n=32768, indegree=160, sim_steps=2000, profile_steps=300
             "hbm_peak_gbs": peak, "peak_source": peak_src}
 
 
+from brian_b200.statistics import precision_agreement as precision_report  # noqa: E402
+
+
 def cuba4000_bench(args):
     """The plain CUBA network (4000 LIF, p = 0.02, zero delay, FP64, 1 s,
     SpikeMonitor and the v trace of 10 neurons) on the GPU: device time per
@@ -957,11 +895,14 @@ def main():
         parity = gpu_parity(inp, args.cpu_steps, rec_ref, state_ref)
 
     def guarded(fn, *a):
-        # the headline line is printed even if a side measurement fails
+        # the headline line is printed even if a side measurement fails; the
+        # precision preference is put back whatever the measurement did
         try:
             return fn(*a)
         except Exception as e:
             return {"error": "%s: %s" % (type(e).__name__, e)}
+        finally:
+            b.set_global_preferences(precision=args.precision)
 
     side = {}
     if rank == 0 and world == 1:

@@ -355,6 +355,7 @@ int build_group(bg_net *net, int gid) {
 template <typename T, typename WT>
 cudaError_t launch_prop(const bg::PropArgs<T> &a, int mode, int64_t grid, cudaStream_t s) {
     switch (mode) {
+    case 5: bg::k_prop_dense<T, WT, 64><<<(unsigned)grid, 64, 0, s>>>(a); break;
     case 0: bg::k_prop_atomic<T, WT, false><<<(unsigned)grid, 256, 0, s>>>(a); break;
     case 1: bg::k_prop_atomic<T, WT, true><<<(unsigned)grid, 256, 0, s>>>(a); break;
     case 2: bg::k_prop_ordered<T, WT, false><<<(unsigned)grid, bg::kOrdThreads, 0, s>>>(a); break;
@@ -396,7 +397,13 @@ int build_conn(bg_net *net, int cid) {
     int mode; int64_t grid;
     // equal weights sum to the same value in any order; STDP makes them differ
     const bool use_atomic = !c.dense && c.mod_var < 0 && ((c.homogeneous && c.stdp < 0) || !net->deterministic) && !a.stdp;
-    if (c.dense) { mode = 4; grid = (c.tn + bg::kDenseThreads - 1) / bg::kDenseThreads; }
+    if (c.dense) {
+        // one thread per target column; blocks of 64 when blocks of 256
+        // would leave most SMs idle
+        mode = (c.tn + bg::kDenseThreads - 1) / bg::kDenseThreads < sm_count() ? 5 : 4;
+        const int th = mode == 5 ? 64 : bg::kDenseThreads;
+        grid = (c.tn + th - 1) / th;
+    }
     else if (use_atomic) {
         mode = c.hetero ? 1 : 0;
         const int64_t nch = ((c.so + c.sn + 31) / 32 - c.so / 32 + 31) / 32;
@@ -408,7 +415,8 @@ int build_conn(bg_net *net, int cid) {
     }
     const int wb = c.w_bits;
     a.events = net->dCounters + net->groups.size() + cid;
-    static const char *kModeName[] = {"prop_atomic", "prop_ring_atomic", "prop_ordered", "prop_ring_ordered", "prop_dense"};
+    static const char *kModeName[] = {"prop_atomic", "prop_ring_atomic", "prop_ordered", "prop_ring_ordered", "prop_dense",
+                                      "prop_dense"};
     net->item_names.push_back(std::string(kModeName[mode]) + "[c" + std::to_string(cid) + "]");
     net->step_launches.push_back([a, mode, grid, wb](cudaStream_t s, int, int last) {
         bg::PropArgs<T> b = a; b.last = last;
@@ -1677,9 +1685,9 @@ static int prepare_impl(bg_net *n) {
         switch (it.kind) {
         case IT_CONN: st = n->precision == 64 ? build_conn<double>(n, it.id) : build_conn<float>(n, it.id); break;
         case IT_SPIKEMON: st = build_spikemon(n, it.id); break;
-        case IT_STDP_PRE:
-            if (n->precision != 64) return fail(BG_ENOSYS, "STDP runs on the FP64 network path");
-            st = build_stdp_pre(n, it.id); break;
+        // STDP keeps FP64 traces and weight arithmetic on both paths (the
+        // FP32 path moves the neuron state and the propagation to FP32)
+        case IT_STDP_PRE: st = build_stdp_pre(n, it.id); break;
         case IT_STDP_POST: st = build_stdp_post(n, it.id); break;
         }
         if (st) return st;

@@ -248,17 +248,18 @@ def _spike_total(r):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["cuba", "persistent", "generated"])
+@pytest.mark.parametrize("case", ["cuba", "persistent", "generated", "stdp"])
 def test_fp32_network_close_to_fp64_oracle(oracle_table, gpu_table, case):
     """The FP32 engine (state and ring values in float) against the FP64
     oracle: states after 20 steps agree to float precision, and over 2000
     steps the spike counts stay within 3 %."""
     fn, kw = {"cuba": (scenarios.cuba, dict(N=4000)),
               "persistent": (scenarios.cuba_delay, dict(monitors=False, N=6000)),
-              "generated": (scenarios.coba, dict())}[case]
+              "generated": (scenarios.coba, dict()),
+              "stdp": (scenarios.stdp, dict(Nin=400, Nout=64))}[case]
     ref, gpu = _fp32_and_oracle(fn, oracle_table, steps=20, **kw)
     for k in ref:
-        if k.startswith("g0."):
+        if k.startswith("g0.") or k == "w0":
             scale = max(1e-3, float(np.max(np.abs(ref[k]))))
             assert np.max(np.abs(np.asarray(gpu[k], dtype=np.float64) - ref[k])) <= 1e-4 * scale, k
     ref, gpu = _fp32_and_oracle(fn, oracle_table, steps=2000, **kw)
