@@ -58,6 +58,11 @@ SIGNATURES = {
     "net_reinit": [_vp],
     "net_stats": [_vp, _P(_i64), _P(_i64), _P(_dbl)],
     "net_counters": [_vp, _vp, _vp],
+    "net_state_bytes": [_vp, _P(_i64)],
+    "net_save_state": [_vp, ct.c_char_p, _i64, _P(_i64)],
+    "net_load_state": [_vp, ct.c_char_p, _i64],
+    "net_save": [_vp, ct.c_char_p],
+    "net_load": [_vp, ct.c_char_p],
 }
 
 # entry points of the CUDA engine only
@@ -69,6 +74,12 @@ ENGINE_ONLY = {
     "conn_add_shared": [_vp, _i32, _i64, _i64, _i32, _i64, _i64, ct.c_int, _i64, _vp, _vp, _dbl, ct.c_int, _i32,
                         _vp, _i32, ct.c_int, _P(_i32)],
     "net_persistent_threads": [_vp, _P(_i32)],
+    "net_set_spin_limit": [_vp, _i64],
+    "import_device_ptr": [_vp, _vp, _i64, ct.c_int, _P(_i32)],
+    "group_use_buffer": [_vp, _i32, _i32],
+    "group_padded_size": [_vp, _i32, _P(_i64)],
+    "net_debug_hold_arrival": [_vp, _i32],
+    "net_set_check_finite": [_vp, ct.c_int],
     "fit_compile_check": [ct.c_int, _vp, _dbl, ct.c_int, ct.c_int, ct.c_char_p, _i64],
     "fit_create": [_P(_vp), ct.c_int, ct.c_int, _vp, _dbl, ct.c_int, ct.c_int],
     "fit_destroy": [_vp],
@@ -108,7 +119,33 @@ ENGINE_ONLY = {
 
 
 class EngineError(RuntimeError):
-    pass
+    """An engine call failed; `code` is its BG_* status (BG_EINVAL -1,
+    BG_ENOMEM -2, BG_ECUDA -3, BG_ETIMEOUT -4, BG_ENUMERIC -5, BG_ESTATE -6,
+    BG_ENOSYS -7, BG_ECOMPILE -8)."""
+
+    def __init__(self, msg, code=None):
+        RuntimeError.__init__(self, msg)
+        self.code = code
+
+
+class EngineBound(object):
+    """Objects that a Network lowers onto an engine handle.  They pickle
+    without the handle: `_host_state(d)` puts the values the engine holds
+    (states, plastic weights, traces, monitor records) into the pickled dict
+    `d`, leaving the live object as it is."""
+
+    def _host_state(self, d):
+        pass
+
+    def __getstate__(self):
+        d = dict(self.__dict__)
+        if d.get("_binding") is not None:
+            self._host_state(d)
+        d["_binding"] = None
+        return d
+
+    def __setstate__(self, d):
+        self.__dict__.update(d)
 
 
 class FunctionTable(object):
@@ -130,7 +167,7 @@ class FunctionTable(object):
         if status != 0:
             buf = ct.create_string_buffer(1024)
             self.last_error(buf, 1024)
-            raise EngineError("%s failed (%d): %s" % (what, status, buf.value.decode(errors="replace")))
+            raise EngineError("%s failed (%d): %s" % (what, status, buf.value.decode(errors="replace")), status)
 
 
 _product = None
@@ -154,7 +191,8 @@ def _ptr(a):
 class Runtime(object):
     """One network handle on a function table."""
 
-    def __init__(self, table=None, device=0, precision=64, deterministic=True, dt=1e-4, persistent=True):
+    def __init__(self, table=None, device=0, precision=64, deterministic=True, dt=1e-4, persistent=True,
+                 spin_limit=None, check_finite=False):
         self.t = table if table is not None else product_table()
         self.h = ct.c_void_p()
         self.precision = precision
@@ -162,6 +200,43 @@ class Runtime(object):
                                        ct.byref(self.h)), "net_create")
         if persistent is not True and hasattr(self.t, "net_set_persistent"):
             self.t.check(self.t.net_set_persistent(self.h, int(persistent)), "net_set_persistent")
+        if spin_limit is not None and hasattr(self.t, "net_set_spin_limit"):
+            self.t.check(self.t.net_set_spin_limit(self.h, int(spin_limit)), "net_set_spin_limit")
+        if check_finite and hasattr(self.t, "net_set_check_finite"):
+            self.t.check(self.t.net_set_check_finite(self.h, 1), "net_set_check_finite")
+
+    def import_device_ptr(self, ptr, nbytes, precision):
+        bid = _i32()
+        self._c(self.t.import_device_ptr(self.h, ct.c_void_p(int(ptr)), int(nbytes), 0 if precision == 64 else 1,
+                                         ct.byref(bid)), "import_device_ptr")
+        return bid.value
+
+    def group_use_buffer(self, gid, bid):
+        self._c(self.t.group_use_buffer(self.h, gid, bid), "group_use_buffer")
+
+    def group_padded_size(self, gid):
+        n = _i64()
+        self._c(self.t.group_padded_size(self.h, gid, ct.byref(n)), "group_padded_size")
+        return n.value
+
+    def save_state(self):
+        """The network's dynamic state as bytes (bg_net_save_state)."""
+        n = _i64()
+        self._c(self.t.net_state_bytes(self.h, ct.byref(n)), "net_state_bytes")
+        buf = ct.create_string_buffer(max(1, n.value))
+        w = _i64()
+        self._c(self.t.net_save_state(self.h, buf, n.value, ct.byref(w)), "net_save_state")
+        return buf.raw[:w.value]
+
+    def load_state(self, data):
+        """Load bytes from save_state into this (identically built) network."""
+        data = bytes(data)
+        self._c(self.t.net_load_state(self.h, data, len(data)), "net_load_state")
+
+    def debug_hold_arrival(self, block):
+        """Test hook of the bounded waits: persistent block `block` never
+        publishes its step arrivals (set before prepare)."""
+        self.t.check(self.t.net_debug_hold_arrival(self.h, int(block)), "net_debug_hold_arrival")
 
     def close(self):
         if self.h:

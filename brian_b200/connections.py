@@ -15,6 +15,7 @@ import math
 
 import numpy as np
 
+from ._lib import EngineBound
 from .groups import NeuronGroup, Subgroup
 
 __all__ = ["Connection", "DelayConnection", "IdentityConnection", "random_matrix_csr",
@@ -160,7 +161,7 @@ class ConnectionMatrixView(object):
         return self._c.__getitem__(key)
 
 
-class Connection(object):
+class Connection(EngineBound):
     """Propagates source spikes to a target state variable (connection.py:15).
 
     ``Connection(source, target, state=0, delay=0*ms, modulation=None,
@@ -407,6 +408,11 @@ class Connection(object):
 
     def _nnz(self):
         return len(self._cols) if self._w is None else len(self._w)
+
+    def _host_state(self, d):
+        # a shared weight stays one value; other weights may be plastic
+        if self._wshared is None:
+            d["_w"] = self._binding.read_weights(self).astype(self.dtype)
 
     def _weights(self):
         if self._binding is not None:

@@ -101,6 +101,7 @@ struct DevCtl {
 #define BG_DERR_MONITOR_OVERFLOW 1
 #define BG_DERR_RANGE 2
 #define BG_DERR_TIMEOUT 3      // a bounded inter-block wait gave up
+#define BG_DERR_NONFINITE 4    // a state variable is NaN or infinite (finite-state check)
 
 // Spin limit of inter-block waits: about a second of polling.
 #define BG_SPIN_LIMIT (1u << 22)

@@ -48,6 +48,7 @@ struct HGroup {
     bool refr = false; double refr_time = 0; int period = 0; int clamp_var = 0; double clamp_val = 0;
     int depth = 1;
     void *dS = nullptr; uint32_t *dHist = nullptr; double *dNext = nullptr; int32_t *dLast = nullptr;
+    int borrowed = -1;                  // index into bg_net::imports when the state lives in a caller's buffer
     int64_t *dGenSteps = nullptr; int32_t *dGenIdx = nullptr;
     std::vector<int> delivs, recs;
     int emp_steps = 0;                  // EmpiricalThreshold window (steps), 0: off
@@ -179,7 +180,13 @@ struct bg_net {
     std::function<cudaError_t(cudaStream_t, int nsteps)> persist;
     unsigned int *dArrived = nullptr;
     int64_t launches = 0; double last_ms = 0;
+    unsigned int spin_limit = BG_SPIN_LIMIT;   // polls of a bounded inter-block wait
+    int hold_block = -1;                // test hook: a persistent block that never arrives
+    int check_finite = 0;               // check the states for NaN/inf after every run
+    bool failed = false;                // a device error stopped the network
     std::vector<void *> allocs;
+    struct Import { void *ptr; int64_t bytes; int dtype; };
+    std::vector<Import> imports;        // borrowed device buffers (the caller owns and frees them)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int64_t chunk_steps = kChunkSteps;
 
@@ -664,10 +671,38 @@ int check_device_error(bg_net *net) {
     DevCtl h;
     BG_CUDA(cudaMemcpyAsync(&h, net->dCtl, sizeof(h), cudaMemcpyDeviceToHost, net->stream));
     BG_CUDA(cudaStreamSynchronize(net->stream));
+    if (h.err) net->failed = true;       // the network's device state is no longer consistent
     if (h.err == BG_DERR_MONITOR_OVERFLOW) return fail(BG_ESTATE, "spike monitor buffer overflow");
     if (h.err == BG_DERR_TIMEOUT) return fail(BG_ETIMEOUT, "inter-block wait timed out at step " + std::to_string(h.err_info));
+    if (h.err == BG_DERR_NONFINITE)
+        return fail(BG_ENUMERIC, "non-finite state: group " + std::to_string(h.err_info >> 48) + ", variable " +
+                    std::to_string((h.err_info >> 40) & 0xff) + ", neuron " + std::to_string(h.err_info & 0xffffffffffll));
+    if (h.err == BG_DERR_RANGE) return fail(BG_EINVAL, "device range check failed (entry " + std::to_string(h.err_info) + ")");
     if (h.err) return fail(BG_ESTATE, "device error " + std::to_string(h.err));
     return BG_OK;
+}
+
+// NaN/inf in the first n entries of each of the nvar rows (stride npad) of a
+// group's state: raises BG_DERR_NONFINITE with (group, variable, neuron).
+template <typename T>
+__global__ void k_check_finite(const T *S, int64_t n, int64_t npad, int nvar, int gid, DevCtl *ctl) {
+    const int64_t total = n * nvar;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t var = q / n, i = q - var * n;
+        const T x = S[var * npad + i];
+        if (!isfinite(x)) bg_raise(ctl, BG_DERR_NONFINITE, ((long long)gid << 48) | ((long long)var << 40) | i);
+    }
+}
+
+int check_finite_states(bg_net *n) {
+    for (size_t gi = 0; gi < n->groups.size(); ++gi) {
+        const HGroup &g = n->groups[gi];
+        const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((g.n * g.nvar + 255) / 256, 1184));
+        if (n->precision == 64) k_check_finite<double><<<grid, 256, 0, n->stream>>>((const double *)g.dS, g.n, g.npad, g.nvar, (int)gi, n->dCtl);
+        else k_check_finite<float><<<grid, 256, 0, n->stream>>>((const float *)g.dS, g.n, g.npad, g.nvar, (int)gi, n->dCtl);
+        BG_CUDA(cudaGetLastError());
+    }
+    return check_device_error(n);
 }
 
 // Copy monitor records of the finished chunk to host memory.
@@ -862,6 +897,8 @@ int build_persist(bg_net *net) {
     a.spikes = net->dCounters;
     a.arrived = net->dArrived;
     a.lag = min_d >= 1 ? 2 : 1;
+    a.spin_limit = net->spin_limit;
+    a.hold_block = net->hold_block;
     if (!net->smons.empty()) {
         // spike monitors: the kernel writes each step's spike words; the
         // monitor kernels turn a launch's words into records (one launch per
@@ -1503,8 +1540,16 @@ static int prepare_impl(bg_net *n) {
     n->chunk_steps = chunk;
     // ---- device allocations
     for (auto &g : n->groups) {
-        if (n->alloc(&g.dS, (size_t)std::max(1, g.nvar) * g.npad * ts) != cudaSuccess) return fail(BG_ENOMEM, "group state");
-        BG_CUDA(cudaMemsetAsync(g.dS, 0, (size_t)std::max(1, g.nvar) * g.npad * ts, n->stream));
+        const size_t sbytes = (size_t)std::max(1, g.nvar) * g.npad * ts;
+        if (g.borrowed >= 0) {
+            const bg_net::Import &im = n->imports[g.borrowed];
+            if ((size_t)im.bytes < sbytes)
+                return fail(BG_EINVAL, "borrowed buffer smaller than the group state (" + std::to_string(sbytes) + " bytes)");
+            if (im.dtype != (n->precision == 64 ? BG_DTYPE_F64 : BG_DTYPE_F32))
+                return fail(BG_EINVAL, "borrowed buffer type differs from the network precision");
+            g.dS = im.ptr;
+        } else if (n->alloc(&g.dS, sbytes) != cudaSuccess) return fail(BG_ENOMEM, "group state");
+        BG_CUDA(cudaMemsetAsync(g.dS, 0, sbytes, n->stream));
         for (int v = 0; v < g.nvar; ++v) { int st = upload_state(n, g, v, g.S0.data() + (size_t)v * g.n); if (st) return st; }
         if (n->alloc(&g.dHist, (size_t)g.depth * (g.npad / 32) * 4) != cudaSuccess) return fail(BG_ENOMEM, "spike history");
         if (g.refr && n->alloc(&g.dNext, g.npad * 8) != cudaSuccess) return fail(BG_ENOMEM, "refractory");
@@ -1730,8 +1775,17 @@ static int ensure_graph(bg_net *n) {
     return BG_OK;
 }
 
+static int net_run_steps(bg_net *n, int64_t nsteps, int64_t cs0);
+
 int bg_net_run(bg_net *n, int64_t nsteps, int64_t cs0) {
     if (!n || nsteps < 0) return fail(BG_EINVAL, "bg_net_run");
+    if (n->failed) return fail(BG_ESTATE, "the network stopped after a device error; rebuild it");
+    int st = net_run_steps(n, nsteps, cs0);
+    if (st == BG_OK && n->check_finite && n->prepared) st = check_finite_states(n);
+    return st;
+}
+
+static int net_run_steps(bg_net *n, int64_t nsteps, int64_t cs0) {
     if (!n->prepared) { int st = bg_net_prepare(n); if (st) return st; }
     if (nsteps == 0) return BG_OK;
     if (n->nstep + nsteps >= (1ll << 31) - 1) return fail(BG_EINVAL, "a network runs at most 2^31-1 steps");
@@ -1869,6 +1923,238 @@ int bg_net_set_persistent(bg_net *n, int enable) {
         return fail(BG_EINVAL, "persistent: 0, 1, 256 or 512");
     n->allow_persist = enable ? 1 : 0;
     n->persist_th = enable > 1 ? enable : 0;
+    return BG_OK;
+}
+
+}  // extern "C"
+
+// ---- checkpoint / resume ----------------------------------------------------
+// The dynamic state of a prepared network as one byte string: the step
+// counter, every group's state rows, spike history, refractory and
+// empirical-threshold bookkeeping, the delay rings (value and count rings),
+// plastic weights and STDP traces (with their trace records), the spike and
+// event counters and the monitors' records.  Ring cursors and the Poisson
+// draws are functions of the step counter.  Static data (connectivity, fixed
+// weights, model code) is not included: the state is loaded into a network
+// built the same way, and every section's size is checked.
+namespace {
+constexpr uint64_t kStateMagic = 0x3153544e47425242ull;   // "BRBGNTS1"
+
+struct StateWriter {
+    bg_net *n; std::vector<char> out; int err = 0;
+    void raw(const void *p, size_t b) { const char *c = (const char *)p; out.insert(out.end(), c, c + b); }
+    template <typename V> void val(const V &v) { raw(&v, sizeof(v)); }
+    void dev(const void *d, size_t b) {
+        val((uint64_t)b);
+        if (!b || err) return;
+        const size_t o = out.size();
+        out.resize(o + b);
+        if (cudaMemcpy(out.data() + o, d, b, cudaMemcpyDeviceToHost) != cudaSuccess) err = 1;
+    }
+    template <typename V> void vec(const std::vector<V> &v) { val((uint64_t)v.size()); raw(v.data(), v.size() * sizeof(V)); }
+};
+struct StateReader {
+    const char *p; size_t left; std::string err;
+    bool raw(void *d, size_t b) { if (b > left) { err = "truncated state"; return false; } std::memcpy(d, p, b); p += b; left -= b; return true; }
+    template <typename V> bool val(V &v) { return raw(&v, sizeof(v)); }
+    bool expect(uint64_t want, const char *what) {
+        uint64_t got = 0;
+        if (!val(got)) return false;
+        if (got != want) { err = std::string("state does not match this network (") + what + ")"; return false; }
+        return true;
+    }
+    bool dev(void *d, size_t b, const char *what) {
+        if (!expect(b, what)) return false;
+        if (!b) return true;
+        if (b > left) { err = "truncated state"; return false; }
+        if (cudaMemcpy(d, p, b, cudaMemcpyHostToDevice) != cudaSuccess) { err = "copy to the device failed"; return false; }
+        p += b; left -= b;
+        return true;
+    }
+    template <typename V> bool vec(std::vector<V> &v) {
+        uint64_t k = 0;
+        if (!val(k) || k * sizeof(V) > left) { err = "truncated state"; return false; }
+        v.resize(k);
+        return raw(v.data(), k * sizeof(V));
+    }
+};
+
+// visits every dynamic buffer in one fixed order for the writer and the reader
+template <typename F> void visit_state(bg_net *n, F &&f) {
+    const size_t ts = tsize(n);
+    f.devbuf(n->dCounters, (n->groups.size() + n->conns.size()) * 8, "counters");
+    for (auto &g : n->groups) {
+        f.devbuf(g.dS, (size_t)g.nvar * g.npad * ts, "group state");
+        f.devbuf(g.dHist, (size_t)g.depth * (g.npad / 32) * 4, "spike history");
+        f.devbuf(g.dNext, g.dNext ? (size_t)g.npad * 8 : 0, "refractory");
+        f.devbuf(g.dLast, g.dLast ? (size_t)g.npad * 4 : 0, "empirical threshold");
+    }
+    for (auto &c : n->conns) {
+        f.devbuf(c.dRing, c.dRing ? (size_t)c.md * c.tn * ts : 0, "delay ring");
+        f.devbuf(c.dCRing, c.dCRing ? (size_t)c.md * c.tnp * 2 : 0, "count ring");
+        f.devbuf(c.stdp >= 0 ? c.dW : nullptr, c.stdp >= 0 ? (size_t)c.wcount() * (c.w_bits / 8) : 0, "plastic weights");
+    }
+    for (auto &st : n->stdps) {
+        const HConn &c = n->conns[st.cid];
+        f.devbuf(st.dApre, (size_t)c.sn * 8, "presynaptic trace");
+        f.devbuf(st.dApost, (size_t)c.tn * 8, "postsynaptic trace");
+        f.devbuf(st.delayed ? st.dHpre : nullptr, st.delayed ? (size_t)st.hlen * c.sn * 8 : 0, "trace records");
+        f.devbuf(st.delayed ? st.dHpost : nullptr, st.delayed ? (size_t)st.hlen * c.tn * 8 : 0, "trace records");
+    }
+    for (auto &m : n->smons) { f.hostvec(m.steps); f.hostvec(m.idx); }
+    for (auto &m : n->stmons) { f.hostvec(m.vals); f.hostvec(m.steps); f.hostval(m.rows_done); }
+}
+
+struct SizeVisitor {
+    int64_t *t;
+    void devbuf(const void *, size_t b, const char *) { *t += 8 + (int64_t)b; }
+    template <typename V> void hostvec(const std::vector<V> &v) { *t += 8 + (int64_t)(v.size() * sizeof(V)); }
+    template <typename V> void hostval(const V &) { *t += sizeof(V); }
+};
+struct SaveVisitor {
+    StateWriter *w;
+    void devbuf(const void *d, size_t b, const char *) { w->dev(d, b); }
+    template <typename V> void hostvec(const std::vector<V> &v) { w->vec(v); }
+    template <typename V> void hostval(const V &v) { w->val(v); }
+};
+struct LoadVisitor {
+    StateReader *r; bool *ok;
+    void devbuf(void *d, size_t b, const char *what) { if (*ok) *ok = r->dev(d, b, what); }
+    template <typename V> void hostvec(std::vector<V> &v) { if (*ok) *ok = r->vec(v); }
+    template <typename V> void hostval(V &v) { if (*ok) *ok = r->val(v); }
+};
+uint64_t state_shape(const bg_net *n) {
+    return (uint64_t)(n->groups.size() | (n->conns.size() << 16) | (n->stdps.size() << 32) |
+                      ((n->smons.size() + n->stmons.size()) << 48));
+}
+}  // namespace
+
+extern "C" {
+
+int bg_net_state_bytes(bg_net *n, int64_t *bytes) {
+    if (!n || !bytes) return fail(BG_EINVAL, "bg_net_state_bytes");
+    if (!n->prepared) { int st = bg_net_prepare(n); if (st) return st; }
+    int64_t total = 8 * 4;
+    SizeVisitor f{&total};
+    visit_state(n, f);
+    *bytes = total;
+    return BG_OK;
+}
+
+int bg_net_save_state(bg_net *n, void *buf, int64_t cap, int64_t *written) {
+    if (!n || (!buf && cap > 0) || cap < 0) return fail(BG_EINVAL, "bg_net_save_state");
+    if (n->failed) return fail(BG_ESTATE, "the network stopped after a device error");
+    if (!n->prepared) { int st = bg_net_prepare(n); if (st) return st; }
+    BG_CUDA(cudaSetDevice(n->device));
+    BG_CUDA(cudaStreamSynchronize(n->stream));
+    StateWriter w{n};
+    w.val(kStateMagic); w.val((uint64_t)n->precision); w.val((int64_t)n->nstep); w.val(state_shape(n));
+    SaveVisitor f{&w};
+    visit_state(n, f);
+    if (w.err) return fail(BG_ECUDA, "reading the device state failed");
+    if ((int64_t)w.out.size() > cap) return fail(BG_EINVAL, "buffer too small for the state (" + std::to_string(w.out.size()) + " bytes)");
+    std::memcpy(buf, w.out.data(), w.out.size());
+    if (written) *written = (int64_t)w.out.size();
+    return BG_OK;
+}
+
+int bg_net_load_state(bg_net *n, const void *buf, int64_t bytes) {
+    if (!n || !buf || bytes < 0) return fail(BG_EINVAL, "bg_net_load_state");
+    if (!n->prepared) { int st = bg_net_prepare(n); if (st) return st; }
+    BG_CUDA(cudaSetDevice(n->device));
+    BG_CUDA(cudaStreamSynchronize(n->stream));
+    StateReader r{(const char *)buf, (size_t)bytes};
+    uint64_t magic = 0, prec = 0, shape = 0; int64_t nstep = 0;
+    if (!r.val(magic) || magic != kStateMagic) return fail(BG_EINVAL, "not a saved network state");
+    if (!r.val(prec) || prec != (uint64_t)n->precision) return fail(BG_EINVAL, "state saved at another precision");
+    if (!r.val(nstep) || nstep < 0) return fail(BG_EINVAL, "bad step counter");
+    if (!r.val(shape) || shape != state_shape(n)) return fail(BG_EINVAL, "state does not match this network (objects)");
+    bool ok = true;
+    LoadVisitor f{&r, &ok};
+    visit_state(n, f);
+    if (!ok) { n->failed = true; return fail(BG_EINVAL, r.err + "; the network must be rebuilt"); }
+    if (r.left) { n->failed = true; return fail(BG_EINVAL, "state has trailing bytes; the network must be rebuilt"); }
+    n->nstep = nstep;
+    long long ns = nstep;
+    BG_CUDA(cudaMemcpy(&n->dCtl->nstep, &ns, 8, cudaMemcpyHostToDevice));
+    for (auto &m : n->stmons) BG_CUDA(cudaMemcpy(m.dRowBase, &m.rows_done, 8, cudaMemcpyHostToDevice));
+    n->failed = false;
+    return BG_OK;
+}
+
+int bg_net_save(bg_net *n, const char *path) {
+    if (!n || !path) return fail(BG_EINVAL, "bg_net_save");
+    int64_t bytes = 0;
+    int st = bg_net_state_bytes(n, &bytes); if (st) return st;
+    std::vector<char> buf((size_t)bytes);
+    int64_t written = 0;
+    st = bg_net_save_state(n, buf.data(), bytes, &written); if (st) return st;
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return fail(BG_EINVAL, std::string("cannot open ") + path);
+    const bool good = std::fwrite(buf.data(), 1, (size_t)written, f) == (size_t)written;
+    if (std::fclose(f) != 0 || !good) return fail(BG_EINVAL, std::string("writing ") + path + " failed");
+    return BG_OK;
+}
+
+int bg_net_load(bg_net *n, const char *path) {
+    if (!n || !path) return fail(BG_EINVAL, "bg_net_load");
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(BG_EINVAL, std::string("cannot open ") + path);
+    std::vector<char> buf;
+    char tmp[1 << 16];
+    size_t k;
+    while ((k = std::fread(tmp, 1, sizeof(tmp), f)) > 0) buf.insert(buf.end(), tmp, tmp + k);
+    std::fclose(f);
+    return bg_net_load_state(n, buf.data(), (int64_t)buf.size());
+}
+
+int bg_import_device_ptr(bg_net *n, void *ptr, int64_t bytes, int dtype, int32_t *buf_id) {
+    if (!n || !ptr || bytes <= 0 || !buf_id) return fail(BG_EINVAL, "bg_import_device_ptr");
+    if (dtype != BG_DTYPE_F64 && dtype != BG_DTYPE_F32) return fail(BG_EINVAL, "dtype must be BG_DTYPE_F64 or BG_DTYPE_F32");
+    if (((uintptr_t)ptr & 255) != 0) return fail(BG_EINVAL, "borrowed buffer must be 256-byte aligned");
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess || (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)) {
+        cudaGetLastError();
+        return fail(BG_EINVAL, "borrowed pointer is not device memory");
+    }
+    if (at.device != n->device) return fail(BG_EINVAL, "borrowed buffer lives on another device");
+    n->imports.push_back({ptr, bytes, dtype});
+    *buf_id = (int32_t)n->imports.size() - 1;
+    return BG_OK;
+}
+
+int bg_group_use_buffer(bg_net *n, int32_t gid, int32_t buf_id) {
+    if (!gid_ok(n, gid) || buf_id < 0 || buf_id >= (int32_t)n->imports.size()) return fail(BG_EINVAL, "bg_group_use_buffer");
+    if (n->prepared) return fail(BG_ESTATE, "network already prepared");
+    for (const HGroup &g : n->groups)
+        if (g.borrowed == buf_id) return fail(BG_EINVAL, "buffer already holds another group's state");
+    n->groups[gid].borrowed = buf_id;
+    return BG_OK;
+}
+
+int bg_group_padded_size(bg_net *n, int32_t gid, int64_t *npad) {
+    if (!gid_ok(n, gid) || !npad) return fail(BG_EINVAL, "bg_group_padded_size");
+    *npad = n->groups[gid].npad;
+    return BG_OK;
+}
+
+int bg_net_set_spin_limit(bg_net *n, int64_t polls) {
+    if (!n || polls < 1 || polls > 0xffffffffll) return fail(BG_EINVAL, "spin limit: 1 .. 2^32-1 polls");
+    if (n->prepared) return fail(BG_ESTATE, "set before prepare");
+    n->spin_limit = (unsigned int)polls;
+    return BG_OK;
+}
+
+int bg_net_debug_hold_arrival(bg_net *n, int32_t block) {
+    if (!n || block < -1) return fail(BG_EINVAL, "block index");
+    if (n->prepared) return fail(BG_ESTATE, "set before prepare");
+    n->hold_block = block;
+    return BG_OK;
+}
+
+int bg_net_set_check_finite(bg_net *n, int enable) {
+    if (!n || (enable != 0 && enable != 1)) return fail(BG_EINVAL, "check_finite: 0 or 1");
+    n->check_finite = enable;
     return BG_OK;
 }
 

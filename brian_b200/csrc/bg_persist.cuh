@@ -41,6 +41,8 @@ template <typename T> struct PersistArgs {
     int lag;                    // 1 when some delay is zero, else 2
     uint32_t *mon_words;        // spike monitors: spike words of each step of the launch, else null
     int64_t mon_stride;         // words per step in mon_words
+    unsigned int spin_limit;    // polls of a wait before it gives up (BG_DERR_TIMEOUT)
+    int hold_block;             // test hook: this block never publishes its arrivals (-1: none)
 };
 
 __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int *p) {
@@ -198,7 +200,7 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
                     const unsigned int target = (unsigned int)((le >> 2) + 1) * G;
                     unsigned int it = 0;
                     while (ld_acquire_u32(ctr) < target) {
-                        if (++it > BG_SPIN_LIMIT) { abort_flag = 1; bg_raise(a.ctl, BG_DERR_TIMEOUT, t); break; }
+                        if (++it > a.spin_limit) { abort_flag = 1; bg_raise(a.ctl, BG_DERR_TIMEOUT, t); break; }
                         __nanosleep(32);
                     }
                 }
@@ -416,7 +418,7 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
         // ordered before the arrival (release reduction, cumulative over the
         // block's writes through the barrier)
         __syncthreads();
-        if (tid == 0) red_release_add(a.arrived + (st & 3), 1u);
+        if (tid == 0 && (int)blockIdx.x != a.hold_block) red_release_add(a.arrived + (st & 3), 1u);
     }
 #pragma unroll
     for (int u = 0; u < NPT; ++u) {

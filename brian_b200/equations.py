@@ -42,6 +42,14 @@ def _identifiers(expr):
     return {n.id for n in ast.walk(tree) if isinstance(n, ast.Name)}
 
 
+def _picklable_namespace(ns):
+    """The entries of a captured namespace that model code can use and that
+    pickle: numbers, arrays and strings (a caller's modules and functions
+    are left out)."""
+    keep = (int, float, complex, bool, str, np.number, np.ndarray)
+    return {k: v for k, v in ns.items() if isinstance(v, keep) and not k.startswith("__")}
+
+
 def _caller_namespace(level):
     frame = inspect.currentframe()
     for _ in range(level + 1):
@@ -59,6 +67,9 @@ class Equations(object):
     ``Equations(expr, level=0, **kwds)``: names in ``expr`` that are not
     variables are looked up in ``kwds`` if given, else in the caller's
     namespace (``level`` frames up), as in the reference."""
+
+    def __getstate__(self):
+        return dict(self.__dict__, _namespace=_picklable_namespace(self._namespace))
 
     def __init__(self, expr="", level=0, **kwds):
         self._diffeq_names = []

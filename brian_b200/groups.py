@@ -13,7 +13,8 @@ import re
 import numpy as np
 
 from .clock import guess_clock
-from .equations import Equations, linear_propagator, _identifiers
+from ._lib import EngineBound
+from .equations import Equations, linear_propagator, _identifiers, _picklable_namespace
 
 __all__ = ["NeuronGroup", "PoissonGroup", "SpikeGeneratorGroup", "Threshold", "VariableThreshold",
            "PoissonThreshold", "NoThreshold", "StringThreshold", "Reset", "VariableReset", "StringReset",
@@ -82,6 +83,9 @@ class StringThreshold(Threshold):
         self.expr = expr
         self.namespace = namespace or {}
 
+    def __getstate__(self):
+        return dict(self.__dict__, namespace=_picklable_namespace(self.namespace))
+
 
 class LazyStateUpdater(object):
     """State variables that do not evolve (stateupdater.py LazyStateUpdater)."""
@@ -115,6 +119,9 @@ class StringReset(Reset):
         self.expr = expr
         self.namespace = namespace or {}
 
+    def __getstate__(self):
+        return dict(self.__dict__, namespace=_picklable_namespace(self.namespace))
+
 
 class NoReset(Reset):
     def __init__(self):
@@ -145,7 +152,7 @@ class StateArray(np.ndarray):
         self._sink = None
 
 
-class _GroupBase(object):
+class _GroupBase(EngineBound):
     def __len__(self):
         return self._n
 
@@ -371,6 +378,30 @@ class NeuronGroup(_GroupBase):
         else:
             self._S[var, :] = values
 
+    def _host_state(self, d):
+        d["_S"] = self._S_host
+
+    def padded_size(self):
+        """Rows of the engine's state layout: a multiple of 1024 >= len(self)."""
+        return max(1024, (self._n + 1023) // 1024 * 1024)
+
+    def use_device_buffer(self, tensor):
+        """Keep this group's state in `tensor`, a contiguous CUDA tensor of
+        shape (number of state variables, padded_size()) and the network's
+        precision, on the network's device.  No copy: after each run the
+        tensor holds the state (column i = neuron i; columns past len(self)
+        are scratch), and values written into it between runs are what the
+        next run starts from.  Set before the network's first run; the
+        caller keeps ownership of the memory (bg_import_device_ptr)."""
+        if self.__dict__.get("_binding") is not None:
+            raise RuntimeError("set the device buffer before the network's first run")
+        self._device_state = tensor
+
+    def __getstate__(self):
+        d = _GroupBase.__getstate__(self)
+        d.pop("_device_state", None)      # device memory of this process does not pickle
+        return d
+
     @property
     def _S_host(self):
         if self._binding is not None:
@@ -392,6 +423,17 @@ class NeuronGroup(_GroupBase):
             raise NotImplementedError(self._fitting_only)
         S0 = self._S_host if self._names else np.zeros((0, self._n))
         gid = rt.group_add(S0)
+        dev = self.__dict__.get("_device_state")
+        if dev is not None:
+            npad = rt.group_padded_size(gid)
+            want = (len(self._names), npad)
+            if tuple(dev.shape) != want:
+                raise ValueError("device state buffer must have shape %s" % (want,))
+            import torch
+            if dev.dtype != (torch.float64 if rt.precision == 64 else torch.float32) or not dev.is_contiguous():
+                raise ValueError("device state buffer must be a contiguous float%d tensor" % rt.precision)
+            bid = rt.import_device_ptr(dev.data_ptr(), dev.numel() * dev.element_size(), rt.precision)
+            rt.group_use_buffer(gid, bid)
         if self.eqs is not None and self._names and self._scheme is None:
             A, C = linear_propagator(self.eqs, dt)
             rt.group_set_linear(gid, A, C)

@@ -10,6 +10,7 @@ the recorded spikes with the reference's online algorithm.
 """
 import numpy as np
 
+from ._lib import EngineBound
 from .clock import guess_clock
 
 __all__ = ["SpikeMonitor", "StateMonitor", "SpikeCounter", "PopulationSpikeCounter",
@@ -17,7 +18,7 @@ __all__ = ["SpikeMonitor", "StateMonitor", "SpikeCounter", "PopulationSpikeCount
            "ISIHistogramMonitor"]
 
 
-class SpikeMonitor(object):
+class SpikeMonitor(EngineBound):
     def __init__(self, source, record=True, delay=0, function=None):
         if function is not None:
             raise NotImplementedError("per-step Python callbacks are not supported on the engine")
@@ -41,6 +42,9 @@ class SpikeMonitor(object):
 
     def _archive(self):
         self._archived = self._record()
+
+    def _host_state(self, d):
+        d["_archived"] = self._record()
 
     def reinit(self):
         self._archived = (np.zeros(0, dtype=np.int64), np.zeros(0, dtype=np.int32))
@@ -133,7 +137,7 @@ class PopulationRateMonitor(SpikeMonitor):
         return np.convolve(rate, k, mode="same")
 
 
-class StateMonitor(object):
+class StateMonitor(EngineBound):
     """Records S[varname] at `record` (True, index, list) every `timestep`
     steps at the end of each step (monitor.py:683-989).  ``record=False``
     keeps the running mean and variance of every neuron."""
@@ -170,6 +174,9 @@ class StateMonitor(object):
 
     def _archive(self):
         self._archived = self._record()
+
+    def _host_state(self, d):
+        d["_archived"] = self._record()
 
     def reinit(self):
         self._archived = (np.zeros(0, dtype=np.int64), np.zeros((0, len(self._indices))))

@@ -34,7 +34,8 @@ from .synapses import Synapses
 __all__ = ["Network", "MagicNetwork", "run", "reinit", "stop", "clear", "network_operation",
            "NetworkOperation", "engine", "set_global_preferences", "get_global_preference"]
 
-_PREFS = {"useweave": False, "precision": 64, "deterministic": True, "device": 0, "persistent": True}
+_PREFS = {"useweave": False, "precision": 64, "deterministic": True, "device": 0, "persistent": True,
+          "spin_limit": None, "check_finite": False}
 _table_override = []
 
 
@@ -42,7 +43,10 @@ def set_global_preferences(**kw):
     """Reference preference registry (globalprefs.py:57-106); engine keys:
     precision (64|32), deterministic (bool), device (int), persistent (bool:
     allow the single-launch step loop for networks of its shape; or 256 or
-    512: allow it with that many threads per block)."""
+    512: allow it with that many threads per block), spin_limit (polls of a
+    bounded inter-block wait before the run fails with BG_ETIMEOUT; None:
+    the engine's default), check_finite (bool: every run ends with a scan of
+    the state variables and a NaN or infinity fails it with BG_ENUMERIC)."""
     _PREFS.update(kw)
 
 
@@ -84,7 +88,8 @@ class _Binding(object):
 
     def __init__(self, net, table, dt):
         self.rt = Runtime(table, device=_PREFS["device"], precision=_PREFS["precision"],
-                          deterministic=_PREFS["deterministic"], dt=dt, persistent=_PREFS["persistent"])
+                          deterministic=_PREFS["deterministic"], dt=dt, persistent=_PREFS["persistent"],
+                          spin_limit=_PREFS["spin_limit"], check_finite=_PREFS["check_finite"])
         self.gids = {}
         self.cids = {}
         self.sids = {}
@@ -213,7 +218,10 @@ class Network(object):
                     owners.append(g)
         return owners
 
-    def prepare(self):
+    def prepare(self, configure=None):
+        """Lower the network onto one engine handle (done by the first run).
+        `configure(runtime)`, when given, runs on the new handle before the
+        engine builds its step (engine settings such as test hooks)."""
         if self._binding is not None:
             return
         groups = self._all_groups()
@@ -257,10 +265,37 @@ class Network(object):
             elif isinstance(o, Synapses):
                 b.yids[o] = o._lower(rt, b.gids)
                 b.objects.append(o)
+        if configure is not None:
+            configure(rt)
         rt.prepare()
+        pending = self.__dict__.pop("_pending_state", None)
+        if pending is not None:
+            # a pickled network: its dynamic state (rings, histories, traces,
+            # counters) goes back into the rebuilt engine; the monitors keep
+            # their records on the Python side, so the engine's copies go
+            rt.load_state(pending)
+            for o, mid in b.mids.items():
+                rt.monitor_clear(mid)
         for o in b.objects:
             o._binding = b
         self._binding = b
+
+    def __getstate__(self):
+        """Pickling (Network.__reduce__, network.py:652): the objects pickle
+        with their host-side values, and the engine's dynamic state --
+        delay rings, spike histories, refractory bookkeeping, STDP traces,
+        counters -- travels as bytes and is loaded into the engine that the
+        first run after unpickling builds (the same objects give the same
+        engine layout), so run(T1); pickle; unpickle; run(T2) equals
+        run(T1 + T2)."""
+        d = dict(self.__dict__)
+        d["_binding"] = None
+        if self._binding is not None:
+            d["_pending_state"] = self._binding.rt.save_state()
+        return d
+
+    def __setstate__(self, d):
+        self.__dict__.update(d)
 
     def run(self, duration, threads=1, report=None, report_period=10.0):
         self.stopped = False

@@ -23,6 +23,7 @@ import numpy as np
 
 import re
 
+from ._lib import EngineBound
 from .equations import Equations, linear_propagator, _caller_namespace, _identifiers
 
 __all__ = ["ExponentialSTDP", "STDP"]
@@ -56,7 +57,7 @@ def _modified(lines):
     return out
 
 
-class STDP(object):
+class STDP(EngineBound):
     """Spike-timing-dependent plasticity from equations and code strings
     (stdp.py:92-449).
 
@@ -212,6 +213,9 @@ class STDP(object):
         if self.pre_mode or self.post_mode:
             rt.stdp_set_update(sid, self.pre_mode, self.post_mode, self.wx)
         return sid
+
+    def _host_state(self, d):
+        d["_A_pre"], d["_A_post"] = self._binding.read_traces(self)
 
     def _traces(self):
         if self._binding is not None:

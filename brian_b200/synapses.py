@@ -37,6 +37,7 @@ import sys
 
 import numpy as np
 
+from ._lib import EngineBound
 from .groups import NeuronGroup, Subgroup
 
 __all__ = ["Synapses"]
@@ -126,7 +127,7 @@ class _SynapticDelay(_SynapticVariable):
         S._changed(delays=True)
 
 
-class Synapses(object):
+class Synapses(EngineBound):
     def __init__(self, source, target=None, model=None, pre=None, post=None, max_delay=0.0, level=0, clock=None,
                  code_namespace=None, **kwds):
         target = target or source

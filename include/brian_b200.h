@@ -279,6 +279,57 @@ BG_API int bg_net_set_persistent(bg_net *net, int enable);
 /* Threads per block of the persistent kernel the prepared network runs
  * with, or 0 when it runs the general per-step launches. */
 BG_API int bg_net_persistent_threads(bg_net *net, int32_t *threads);
+/* ---- borrowed device buffers --------------------------------------------
+ * Device memory the caller owns (a torch tensor, another library's buffer)
+ * registered with the network; the library never frees it.  bytes >= what
+ * its use needs, 256-byte aligned, on the network's device.  No counterpart
+ * in the reference (its state arrays are numpy arrays the updaters mutate in
+ * place, stateupdater.py:175-221; here a group's state can likewise be an
+ * array the caller holds). */
+#define BG_DTYPE_F64 0
+#define BG_DTYPE_F32 1
+BG_API int bg_import_device_ptr(bg_net *net, void *ptr, int64_t bytes,
+                                int dtype, int32_t *buf_id);
+/* The group's state lives in the borrowed buffer: [nvar][npad] rows of the
+ * network's precision (npad from bg_group_padded_size, a multiple of 1024;
+ * entries past the group's size are scratch).  bg_net_prepare writes the
+ * initial state into it; between runs (after the call returns) the caller
+ * may read and write it directly, as bg_group_get_state/set_state do.  Set
+ * before bg_net_prepare. */
+BG_API int bg_group_use_buffer(bg_net *net, int32_t gid, int32_t buf_id);
+BG_API int bg_group_padded_size(bg_net *net, int32_t gid, int64_t *npad);
+/* ---- checkpoint / resume (Network.__reduce__, network.py:652;
+ * SpikeContainer.__reduce__, utils/circular.py:249-269;
+ * LinearStateUpdater.__getstate__, stateupdater.py:469-481) ----------------
+ * The dynamic state of a prepared network -- step counter, group states,
+ * spike histories, refractory bookkeeping, delay and count rings, plastic
+ * weights, STDP traces and trace records, counters and monitor records --
+ * as one byte string.  It is loaded into a network built the same way
+ * (same objects, sizes and precision; every section's size is checked,
+ * BG_EINVAL on a mismatch).  Ring cursors and Poisson draws follow from the
+ * step counter, so run(T1); save; load into a rebuilt network; run(T2)
+ * equals run(T1 + T2).  bg_net_save/bg_net_load write and read a file. */
+BG_API int bg_net_state_bytes(bg_net *net, int64_t *bytes);
+BG_API int bg_net_save_state(bg_net *net, void *buf, int64_t cap,
+                             int64_t *written);
+BG_API int bg_net_load_state(bg_net *net, const void *buf, int64_t bytes);
+BG_API int bg_net_save(bg_net *net, const char *path);
+BG_API int bg_net_load(bg_net *net, const char *path);
+/* ---- failure detection (no counterpart in the reference, where a stalled
+ * or diverging simulation just runs on) -------------------------------------
+ * Polls of the persistent kernel's bounded inter-block wait before it gives
+ * up (default 2^22, a few seconds): every block then leaves its step loop,
+ * bg_net_run returns BG_ETIMEOUT with no kernel left running, and the
+ * network refuses further runs (BG_ESTATE).  Set before bg_net_prepare. */
+BG_API int bg_net_set_spin_limit(bg_net *net, int64_t polls);
+/* Test hook for the bounded waits: block `block` of the persistent kernel
+ * never publishes its step arrivals, so the other blocks' waits run out
+ * (-1, the default: off).  Set before bg_net_prepare. */
+BG_API int bg_net_debug_hold_arrival(bg_net *net, int32_t block);
+/* With enable = 1, every bg_net_run ends with a scan of all state
+ * variables; a NaN or infinity returns BG_ENUMERIC naming the group,
+ * variable and neuron, and the network refuses further runs. */
+BG_API int bg_net_set_check_finite(bg_net *net, int enable);
 /* ---- allocation-free entry point ------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory (code inside another framework's caching allocator, which owns the

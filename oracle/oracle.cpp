@@ -864,6 +864,94 @@ int or_net_stats(or_net *n, int64_t *steps, int64_t *launches, double *ms) {
     if (steps) *steps = n->nstep; if (launches) *launches = 0; if (ms) *ms = 0; return OR_OK;
 }
 
+}  /* extern "C" */
+
+/* Checkpoint / resume of the oracle's dynamic state (the engine's
+ * bg_net_save_state/bg_net_load_state; the reference pickles the network,
+ * network.py:652, utils/circular.py:249-269): step counter, states, spike
+ * histories, refractory bookkeeping, weights, rings and cursors, traces and
+ * their records, SpikeQueue rows, counters and monitor records, loaded into
+ * a network built the same way (sizes checked). */
+namespace {
+struct OW { std::vector<char> b;
+    void raw(const void *p, size_t k) { const char *c = (const char *)p; b.insert(b.end(), c, c + k); }
+    template <typename V> void val(const V &v) { raw(&v, sizeof(v)); }
+    template <typename V> void vec(const std::vector<V> &v) { val((uint64_t)v.size()); raw(v.data(), v.size() * sizeof(V)); } };
+struct OR_ { const char *p; size_t left; bool ok = true;
+    void raw(void *d, size_t k) { if (!ok || k > left) { ok = false; return; } std::memcpy(d, p, k); p += k; left -= k; }
+    template <typename V> void val(V &v) { raw(&v, sizeof(v)); }
+    template <typename V> void vec(std::vector<V> &v) { uint64_t k = 0; val(k); if (!ok || k * sizeof(V) > left) { ok = false; return; } v.resize(k); raw(v.data(), k * sizeof(V)); }
+    /* a vector whose size the network fixes */
+    template <typename V> void same(std::vector<V> &v) { const size_t want = v.size(); std::vector<V> t; vec(t); if (ok && t.size() != want) ok = false; if (ok) v.swap(t); } };
+template <typename IO> void or_visit(or_net *n, IO &io) {
+    for (auto &g : n->groups) {
+        io.same(g.S); io.same(g.next_allowed); io.same(g.last_spike); io.val(g.nspikes);
+        uint64_t d = g.hist.size(); io.val(d);
+        if (d != g.hist.size()) { io.ok = false; return; }
+        for (auto &h : g.hist) io.vec(h);
+    }
+    for (auto &c : n->conns) { io.same(c.w64); io.same(c.w32); io.same(c.ring); io.val(c.cur); io.val(c.events); }
+    for (auto &s : n->stdps) { io.same(s.A_pre); io.same(s.A_post); io.same(s.H_pre); io.same(s.H_post); io.val(s.cur); }
+    for (auto &y : n->syns) {
+        io.val(y.cur);
+        uint64_t L = y.X.size(); io.val(L);
+        if (L != y.X.size()) { io.ok = false; return; }
+        for (auto &x : y.X) io.vec(x);
+    }
+    for (auto &m : n->smons) { io.vec(m.steps); io.vec(m.idx); }
+    for (auto &m : n->stmons) { io.vec(m.vals); io.vec(m.steps); }
+}
+/* the writer has no size check: `same` is `vec` */
+struct OWv : OW { bool ok = true; template <typename V> void same(const std::vector<V> &v) { vec(v); } };
+const uint64_t kOrMagic = 0x31534f4e47425242ull;
+}
+
+extern "C" {
+
+int or_net_state_bytes(or_net *n, int64_t *bytes) {
+    if (!n || !bytes) return fail(OR_EINVAL, "state_bytes");
+    if (!n->prepared) { int st = or_net_prepare(n); if (st) return st; }
+    OWv w; w.val(kOrMagic); w.val(n->nstep); or_visit(n, w);
+    *bytes = (int64_t)w.b.size(); return OR_OK;
+}
+int or_net_save_state(or_net *n, void *buf, int64_t cap, int64_t *written) {
+    if (!n || (!buf && cap > 0)) return fail(OR_EINVAL, "save_state");
+    if (!n->prepared) { int st = or_net_prepare(n); if (st) return st; }
+    OWv w; w.val(kOrMagic); w.val(n->nstep); or_visit(n, w);
+    if ((int64_t)w.b.size() > cap) return fail(OR_EINVAL, "buffer too small for the state");
+    std::memcpy(buf, w.b.data(), w.b.size());
+    if (written) *written = (int64_t)w.b.size();
+    return OR_OK;
+}
+int or_net_load_state(or_net *n, const void *buf, int64_t bytes) {
+    if (!n || !buf || bytes < 0) return fail(OR_EINVAL, "load_state");
+    if (!n->prepared) { int st = or_net_prepare(n); if (st) return st; }
+    OR_ r{(const char *)buf, (size_t)bytes};
+    uint64_t magic = 0; int64_t nstep = 0;
+    r.val(magic); r.val(nstep);
+    if (!r.ok || magic != kOrMagic) return fail(OR_EINVAL, "not a saved network state");
+    or_visit(n, r);
+    if (!r.ok || r.left) return fail(OR_EINVAL, "state does not match this network");
+    n->nstep = nstep;
+    return OR_OK;
+}
+int or_net_save(or_net *n, const char *path) {
+    int64_t b = 0; int st = or_net_state_bytes(n, &b); if (st) return st;
+    std::vector<char> buf((size_t)b); int64_t w = 0;
+    st = or_net_save_state(n, buf.data(), b, &w); if (st) return st;
+    FILE *f = std::fopen(path, "wb"); if (!f) return fail(OR_EINVAL, "open");
+    const bool good = std::fwrite(buf.data(), 1, (size_t)w, f) == (size_t)w;
+    if (std::fclose(f) != 0 || !good) return fail(OR_EINVAL, "write");
+    return OR_OK;
+}
+int or_net_load(or_net *n, const char *path) {
+    FILE *f = std::fopen(path, "rb"); if (!f) return fail(OR_EINVAL, "open");
+    std::vector<char> buf; char tmp[1 << 16]; size_t k;
+    while ((k = std::fread(tmp, 1, sizeof(tmp), f)) > 0) buf.insert(buf.end(), tmp, tmp + k);
+    std::fclose(f);
+    return or_net_load_state(n, buf.data(), (int64_t)buf.size());
+}
+
 /* Uniform draw shared with the device Poisson source; exported so tests can
  * pin the stream against known answers. */
 double or_philox_uniform(uint64_t seed, int64_t step, int64_t i) { return philox_uniform(seed, step, i); }

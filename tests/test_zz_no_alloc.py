@@ -113,23 +113,28 @@ def test_noalloc_matches_network_engine_twice(gpu_table):
 
 
 @pytest.mark.gpu
-def test_noalloc_refuses_malformed_row_pointers(gpu_table):
-    """A decreasing or negative rowptr is refused with BG_EINVAL by the device
-    check that runs before any kernel walks the rows; the state is untouched."""
+def test_noalloc_refuses_malformed_rows(gpu_table):
+    """A decreasing or negative rowptr, a target beyond the group or a delay
+    at the ring depth is refused with BG_EINVAL by the device checks that
+    run before the step loop; the state is untouched."""
     import torch
     lib = gpu_table.lib
     _bind(lib)
     ne, exc, inh, d_exc, d_inh, S0 = _connectivity()
     A = np.eye(3)
-    for bad in ("decreasing", "negative"):
-        rp = exc[0].copy()
+    for bad in ("decreasing", "negative", "target", "delay"):
+        rp, cl, dl = exc[0].copy(), exc[1].copy(), d_exc.copy()
         if bad == "decreasing":
             rp[5], rp[6] = rp[6], rp[5]
-        else:
+        elif bad == "negative":
             rp[0] = -1
+        elif bad == "target":
+            cl[1000] = N                    # one target beyond the group
+        else:
+            dl[1000] = 51                   # ring depth 51: delays 0..50
         dev = {"ne": ne,
                "rowptr": [torch.from_numpy(rp).cuda(), torch.from_numpy(inh[0]).cuda()],
-               "cols": [torch.from_numpy(exc[1]).cuda(), torch.from_numpy(inh[1]).cuda()],
-               "delays": [torch.from_numpy(d_exc).cuda(), torch.from_numpy(d_inh).cuda()]}
+               "cols": [torch.from_numpy(cl).cuda(), torch.from_numpy(inh[1]).cuda()],
+               "delays": [torch.from_numpy(dl).cuda(), torch.from_numpy(d_inh).cuda()]}
         out, _ = _noalloc_run(lib, dev, S0, 10, A, np.zeros(3), expect=-1)
         assert np.array_equal(out, S0)
