@@ -411,6 +411,16 @@ class Runtime(object):
                                     ct.byref(mid)), "statemon_add")
         return mid.value
 
+    def spikemon_count(self, mid):
+        n = _i64()
+        self._c(self.t.spikemon_count(self.h, mid, ct.byref(n)), "spikemon_count")
+        return n.value
+
+    def statemon_count(self, mid):
+        n = _i64()
+        self._c(self.t.statemon_count(self.h, mid, ct.byref(n)), "statemon_count")
+        return n.value
+
     def spikemon_read(self, mid):
         n = _i64()
         self._c(self.t.spikemon_count(self.h, mid, ct.byref(n)), "spikemon_count")

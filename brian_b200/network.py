@@ -271,11 +271,19 @@ class Network(object):
         pending = self.__dict__.pop("_pending_state", None)
         if pending is not None:
             # a pickled network: its dynamic state (rings, histories, traces,
-            # counters) goes back into the rebuilt engine; the monitors keep
-            # their records on the Python side, so the engine's copies go
+            # counters, monitor records) goes back into the rebuilt engine;
+            # each monitor pickled its whole record, whose tail is what the
+            # engine held and now holds again, so that tail is dropped here
             rt.load_state(pending)
             for o, mid in b.mids.items():
-                rt.monitor_clear(mid)
+                if isinstance(o, SpikeMonitor):
+                    k = rt.spikemon_count(mid)
+                    if k:
+                        o._archived = tuple(x[:len(x) - k] for x in o._archived)
+                elif isinstance(o, StateMonitor):
+                    k = rt.statemon_count(mid)
+                    if k:
+                        o._archived = tuple(x[:len(x) - k] for x in o._archived)
         for o in b.objects:
             o._binding = b
         self._binding = b

