@@ -104,20 +104,27 @@ def cuba_scaled(inp, spike_monitor=False, record=None):
 
 
 def stdp_scaleup(seed=2024, nin=10000, nout=4096, gmax=0.01, rate_lo=5.0, rate_hi=25.0, spike_record=0,
-                 record=None, input_monitor=False):
+                 record=None, input_monitor=False, out_range=None):
     """The STDP scale-up network.  Returns a dict with the network and its
     objects: net, inputs, outputs, C (dense Connection), stdp, M (SpikeMonitor
     of the first `spike_record` outputs, or None), S (StateMonitor of v on
     the outputs `record`, or None), Mi (SpikeMonitor of the inputs when
-    asked), w0 (the initial weights, float64)."""
+    asked), w0 (the initial weights, float64).
+
+    out_range=(lo, hi) builds the shard of outputs [lo, hi): the same inputs
+    (the Poisson spikes are a function of (seed, step, index), so every
+    shard draws them alike) onto those outputs with their columns of the
+    full network's initial weights.  The outputs do not interact, so the
+    shards of a partition together run exactly the full network."""
     b = _b()
     eqs = b.Equations(STDP_EQS, taum=10 * ms, taue=5 * ms, Ee=0 * mV, vr=-60 * mV, El=-74 * mV)
     rng = np.random.Generator(np.random.PCG64(seed))
     rates = rng.uniform(rate_lo, rate_hi, nin)
     inputs = b.PoissonGroup(nin, rates=rates, seed=seed + 1)
-    outputs = b.NeuronGroup(nout, model=eqs, threshold=-54 * mV, reset=-60 * mV)
+    lo, hi = (0, nout) if out_range is None else out_range
+    outputs = b.NeuronGroup(hi - lo, model=eqs, threshold=-54 * mV, reset=-60 * mV)
     outputs.v = -60 * mV
-    w0 = rng.uniform(0, gmax, (nin, nout))
+    w0 = rng.uniform(0, gmax, (nin, nout))[:, lo:hi]
     C = b.Connection(inputs, outputs, "ge", structure="dense", dtype=np.float32)
     C.connect(W=w0)
     stdp = b.ExponentialSTDP(C, 20 * ms, 20 * ms, 0.01, -0.0105, wmax=gmax)
