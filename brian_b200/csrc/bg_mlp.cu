@@ -19,6 +19,7 @@
 // kernel (deterministic).
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
+#include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
 #include <cmath>
@@ -124,28 +125,6 @@ __global__ void __launch_bounds__(256) k_nll(const float *OUT, const float *Y, i
     }
 }
 
-// Adam on one parameter tensor [rows][cols] whose gradient is the sum of
-// `splits` partial slices; refreshes the bf16 copy and its transpose.
-__global__ void k_adam(float *W, float *m, float *v, const float *grad, int splits, int64_t split_stride, int rows,
-                       int cols, int rows_train, float lr, float b1, float b2, float eps, float c1, float c2,
-                       bf16 *Wb, bf16 *WbT) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (int64_t)rows * cols) return;
-    const int r = (int)(i / cols), c = (int)(i % cols);
-    if (r < rows_train) {
-        float g = 0.f;
-        for (int s = 0; s < splits; ++s) g += grad[s * split_stride + i];
-        const float mi = b1 * m[i] + (1.f - b1) * g;
-        const float vi = b2 * v[i] + (1.f - b2) * g * g;
-        m[i] = mi;
-        v[i] = vi;
-        W[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
-    }
-    const bf16 h = __float2bfloat16_rn(W[i]);
-    if (Wb) Wb[i] = h;
-    if (WbT) WbT[(int64_t)c * rows + r] = h;
-}
-
 __global__ void k_to_bf16(const float *W, int rows, int cols, bf16 *Wb, bf16 *WbT) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (int64_t)rows * cols) return;
@@ -153,6 +132,78 @@ __global__ void k_to_bf16(const float *W, int rows, int cols, bf16 *Wb, bf16 *Wb
     const bf16 h = __float2bfloat16_rn(W[i]);
     Wb[i] = h;
     if (WbT) WbT[(int64_t)c * rows + r] = h;
+}
+
+// Adam over every parameter tensor of the network in one launch: segment k
+// of the flat index space is tensor k (W0, b0, W1, b1, ...), whose gradient
+// is the sum of `splits` partial slices.  The step count t comes from device
+// memory (the step runs as a captured graph), c1 = 1 - b1^t, c2 = 1 - b2^t.
+struct AdamSeg {
+    float *P, *m, *v; const float *grad; int splits; int64_t split_stride; int rows, cols, rows_train;
+    bf16 *Pb, *PbT;
+};
+struct AdamAll {
+    AdamSeg seg[2 * kNLayer];
+    int64_t off[2 * kNLayer + 1];
+    const int64_t *step;
+    float lr, b1, b2, eps;
+};
+__global__ void k_adam_all(const AdamAll a) {
+    const int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i0 >= a.off[2 * kNLayer]) return;
+    int k = 0;
+#pragma unroll
+    for (int q = 1; q < 2 * kNLayer; ++q) k += i0 >= a.off[q] ? 1 : 0;
+    const AdamSeg &sg = a.seg[k];
+    const int64_t i = i0 - a.off[k];
+    const int r = (int)(i / sg.cols), c = (int)(i % sg.cols);
+    if (r < sg.rows_train) {
+        const float t = (float)*a.step;
+        const float c1 = 1.f - powf(a.b1, t), c2 = 1.f - powf(a.b2, t);
+        float g = 0.f;
+        for (int s = 0; s < sg.splits; ++s) g += sg.grad[s * sg.split_stride + i];
+        const float mi = a.b1 * sg.m[i] + (1.f - a.b1) * g;
+        const float vi = a.b2 * sg.v[i] + (1.f - a.b2) * g * g;
+        sg.m[i] = mi;
+        sg.v[i] = vi;
+        sg.P[i] -= a.lr * (mi / c1) / (sqrtf(vi / c2) + a.eps);
+    }
+    if (sg.Pb) {
+        const bf16 h = __float2bfloat16_rn(sg.P[i]);
+        sg.Pb[i] = h;
+        if (sg.PbT) sg.PbT[(int64_t)c * sg.rows + r] = h;
+    }
+}
+
+// One training step's bookkeeping: the batch index within the epoch and the
+// optimiser step, advanced after the step's kernels.
+__global__ void k_step_advance(int64_t *batch_index, int64_t *opt_step) {
+    *batch_index += 1;
+    *opt_step += 1;
+}
+
+// The epoch's batch order: rows sorted by a Philox draw keyed (seed, epoch, row).
+__global__ void k_perm_keys(uint64_t seed, int64_t epoch, int64_t n, unsigned long long *keys, int64_t *vals) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t c[4] = {(uint32_t)i, (uint32_t)((uint64_t)i >> 32), (uint32_t)epoch, (uint32_t)((uint64_t)epoch >> 32)};
+        bg_philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+        keys[i] = ((unsigned long long)c[0] << 32) | c[1];
+        vals[i] = i;
+    }
+}
+
+// Batch rows idx[base .. base+B) with base = B * batch_index (a device
+// counter, so the gather can sit in a captured graph).
+__global__ void k_gather_at(const float *Xall, const float *Yall, const int64_t *perm, const int64_t *batch_index,
+                            int B, int ydim, bf16 *X, bf16 *XT, float *Y) {
+    const int b = blockIdx.x;
+    const int64_t r = perm[*batch_index * B + b];
+    for (int j = threadIdx.x; j < kIn; j += blockDim.x) {
+        const bf16 v = __float2bfloat16_rn(Xall[r * kIn + j]);
+        X[(int64_t)b * kIn + j] = v;
+        XT[(int64_t)j * B + b] = v;
+    }
+    for (int j = threadIdx.x; j < ydim; j += blockDim.x) Y[(int64_t)b * ydim + j] = Yall[r * ydim + j];
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no
@@ -204,15 +255,41 @@ int launch_gemm_as(const umma::GemmArgs &g, int splits, cudaStream_t st, const C
     return BG_OK;
 }
 
-// TMA-fed stages when both operands allow a tensor map (16-byte aligned
-// rows, K a multiple of 8), else cp.async.
+int sm_count_mlp() {
+    static int n = 0;
+    if (!n) { int dev = 0; cudaGetDevice(&dev); cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev); if (n <= 0) n = 148; }
+    return n;
+}
+
+// The persistent warp-specialised kernel over all tiles of the product.
+template <int NT, int EPI>
+int launch_gemm_persistent(const umma::GemmArgs &g, int splits, cudaStream_t st, const CUtensorMap &ta,
+                           const CUtensorMap &tb) {
+    static bool attr_set = false;
+    constexpr size_t smem = umma::psmem_bytes<NT>();
+    if (!attr_set) {
+        MCK(cudaFuncSetAttribute(umma::k_gemm_p<NT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = true;
+    }
+    const int tiles_m = (g.M + umma::kM - 1) / umma::kM, tiles_n = (g.N + NT - 1) / NT;
+    const int ntiles = tiles_m * tiles_n * splits;
+    const int grid = std::max(1, std::min(ntiles, sm_count_mlp()));
+    umma::k_gemm_p<NT, EPI><<<grid, umma::kPThreads, smem, st>>>(g, ta, tb, tiles_m, tiles_n, splits);
+    MCK(cudaGetLastError());
+    return BG_OK;
+}
+
+// TMA-fed persistent kernel when both operands allow a tensor map (16-byte
+// aligned rows, K a multiple of 8) and every split has K-chunks, else the
+// one-tile-per-CTA kernel with cp.async stages.
 template <int NT, int EPI>
 int launch_gemm(const umma::GemmArgs &g, int splits, cudaStream_t st) {
     CUtensorMap ta, tb;
     memset(&ta, 0, sizeof ta);
     memset(&tb, 0, sizeof tb);
-    if (tile_map(&ta, g.A, g.M, g.K, g.lda, umma::kM) && tile_map(&tb, g.B, g.N, g.K, g.ldb, NT))
-        return launch_gemm_as<NT, EPI, true>(g, splits, st, ta, tb);
+    if (g.k_per_split >= umma::kKc && g.k_per_split % umma::kKc == 0 && (long long)g.k_per_split * splits == g.K &&
+        tile_map(&ta, g.A, g.M, g.K, g.lda, umma::kM) && tile_map(&tb, g.B, g.N, g.K, g.ldb, NT))
+        return launch_gemm_persistent<NT, EPI>(g, splits, st, ta, tb);
     return launch_gemm_as<NT, EPI, false>(g, splits, st, ta, tb);
 }
 
@@ -260,7 +337,15 @@ struct bg_mlp {
     float *W[kNLayer] = {}, *b[kNLayer] = {}, *mW[kNLayer] = {}, *vW[kNLayer] = {}, *mb[kNLayer] = {},
           *vb[kNLayer] = {};
     bf16 *Wb[kNLayer] = {}, *WbT[kNLayer] = {};
-    float *gW = nullptr;                  // weight-gradient scratch (largest layer x splits)
+    float *gW = nullptr;                  // weight-gradient scratch: per layer, kSplits partial slices
+    float *gWl[kNLayer] = {};             //   layer l's region of gW
+    int64_t *dBatchIdx = nullptr;         // device counters of a training step: batch within the epoch,
+    int64_t *dOptStep = nullptr;          //   optimiser step
+    // epoch order: Philox keys sorted with their row indices
+    unsigned long long *pkeys = nullptr, *pkeys_out = nullptr; int64_t *pvals = nullptr, *perm = nullptr;
+    void *sort_tmp = nullptr; size_t sort_tmp_bytes = 0;
+    // one training step captured as a graph (rebuilt when the batch size changes)
+    cudaGraphExec_t step_graph = nullptr; int graph_batch = 0; float graph_lr = 0.f;
     float *cs[kNLayer] = {};              // bias-gradient partials per layer [row blocks][512]
     int64_t step = 0;
     // batch buffers
@@ -278,6 +363,13 @@ namespace {
 
 int ensure_batch(bg_mlp *h, int B) {
     if (B == h->B) return BG_OK;
+    // the batch buffers move: a captured training step holds their addresses
+    if (h->step_graph) {
+        cudaStreamSynchronize(h->stream);
+        cudaGraphExecDestroy(h->step_graph);
+        h->step_graph = nullptr;
+        h->graph_batch = 0;
+    }
     int rc = 0;
     if ((rc = dalloc(&h->X, (size_t)B * kIn))) return rc;
     if ((rc = dalloc(&h->XT, (size_t)B * kIn))) return rc;
@@ -293,7 +385,7 @@ int ensure_batch(bg_mlp *h, int B) {
     if ((rc = dalloc(&h->Y, (size_t)B * h->ydim))) return rc;
     if ((rc = dalloc(&h->idx, (size_t)B))) return rc;
     for (int l = 0; l < kNLayer; ++l)
-        if ((rc = dalloc(&h->cs[l], (size_t)((B + 127) / 128) * kHid))) return rc;
+        if ((rc = dalloc(&h->cs[l], (size_t)((B + 31) / 32) * kHid))) return rc;
     h->B = B;
     return BG_OK;
 }
@@ -323,34 +415,29 @@ int forward(bg_mlp *h, int B) {
 
 // Bias-gradient partials of layer l: per-block column sums written by the
 // loss kernel (output layer, blocks of 256 rows, 64 columns) or by the
-// ReLU-gradient epilogue that produced G[l] (blocks of 128 rows).
+// ReLU-gradient epilogue that produced G[l] (blocks of 32 rows).
 void bias_partials(const bg_mlp *h, int l, int B, const float **p, int *nblk, int *ld) {
     *p = h->cs[l];
     if (l == kNLayer - 1) {
         *nblk = (B + 255) / 256;
         *ld = kOutPad;
     } else {
-        *nblk = (B + umma::kM - 1) / umma::kM;
+        *nblk = 4 * ((B + umma::kM - 1) / umma::kM);
         *ld = kHid;
     }
 }
 
-// backward from the loss gradient in h->dO / h->dOT; weight gradients of
-// layer l into h->gW (split slices), bias gradients from the column-sum
-// partials, then Adam
-int backward_and_update(bg_mlp *h, int B, float lr, bool update) {
+// backward from the loss gradient in h->dO / h->dOT: weight gradients of
+// layer l into its region of h->gW (kSplits partial slices over the batch),
+// bias gradients as the column-sum partials, and the input gradient of every
+// hidden layer (read against the weights before any update)
+int backward(bg_mlp *h, int B) {
     int rc = 0;
-    const int splits = B % (kSplits * umma::kKc) == 0 ? kSplits : 1;
+    const int splits = kSplits;
     const int kper = B / splits;
-    const int64_t slice = (int64_t)kHid * kHid;
-    // gradient of the layer input for layers 3, 2, 1 (G[l] = dZ of hidden layer l)
     const bf16 *gin = h->dO;
     const bf16 *ginT = h->dOT;
     int gK = kOutPad;
-    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
-    h->step += update ? 1 : 0;
-    const float c1 = 1.f - powf(b1, (float)std::max<int64_t>(h->step, 1));
-    const float c2 = 1.f - powf(b2, (float)std::max<int64_t>(h->step, 1));
     for (int l = 3; l >= 0; --l) {
         // dW_l = gin^T . input_l   (input_l = H[l-1] or X)
         const bf16 *inT = l > 0 ? h->HT[l - 1] : h->XT;
@@ -358,15 +445,15 @@ int backward_and_update(bg_mlp *h, int B, float lr, bool update) {
         {
             umma::GemmArgs g = gemm_args(ginT, B, inT, B, h->rows[l], nin, B, h->err);
             g.k_per_split = kper;
-            g.C = h->gW;
+            g.C = h->gWl[l];
             g.ldc = nin;
-            g.split_stride = slice;
+            g.split_stride = (int64_t)h->rows[l] * h->cols[l];
             if (nin == kIn) rc = launch_gemm<64, umma::EPI_F32>(g, splits, h->stream);
             else rc = launch_gemm<kNT, umma::EPI_F32>(g, splits, h->stream);
             if (rc) return rc;
         }
-        // gradient into the previous hidden layer (needs W_l before its
-        // update); its epilogue also sums the columns for layer l-1's bias
+        // gradient into the previous hidden layer; its epilogue also sums the
+        // columns for layer l-1's bias
         if (l > 0) {
             umma::GemmArgs g = gemm_args(gin, gK, h->WbT[l], h->rows[l], B, kHid, gK, h->err);
             g.act = h->H[l - 1];
@@ -378,27 +465,56 @@ int backward_and_update(bg_mlp *h, int B, float lr, bool update) {
             g.colsum = h->cs[l - 1];
             g.colsum_ld = kHid;
             if ((rc = launch_gemm<kNT, umma::EPI_DRELU_BF16>(g, 1, h->stream))) return rc;
-        }
-        if (update) {
-            const int rows_train = l == 3 ? 2 * h->ydim : h->rows[l];
-            const int64_t n = (int64_t)h->rows[l] * h->cols[l];
-            k_adam<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(
-                h->W[l], h->mW[l], h->vW[l], h->gW, splits, slice, h->rows[l], h->cols[l], rows_train, lr, b1, b2,
-                eps, c1, c2, h->Wb[l], h->WbT[l]);
-            const float *bp;
-            int nblk, ld;
-            bias_partials(h, l, B, &bp, &nblk, &ld);
-            k_adam<<<(unsigned)((h->rows[l] + 255) / 256), 256, 0, h->stream>>>(
-                h->b[l], h->mb[l], h->vb[l], bp, nblk, ld, h->rows[l], 1, rows_train, lr, b1, b2, eps, c1, c2,
-                nullptr, nullptr);
-            MCK(cudaGetLastError());
-        }
-        if (l > 0) {
             gin = h->G[l - 1];
             ginT = h->GT[l - 1];
             gK = kHid;
         }
     }
+    return BG_OK;
+}
+
+// Adam on every tensor in one launch (the step count is read on the device)
+int adam_all(bg_mlp *h, int B, float lr) {
+    AdamAll a;
+    memset(&a, 0, sizeof a);
+    int64_t off = 0;
+    for (int l = 0; l < kNLayer; ++l) {
+        const int rows_train = l == 3 ? 2 * h->ydim : h->rows[l];
+        AdamSeg &w = a.seg[2 * l];
+        w.P = h->W[l]; w.m = h->mW[l]; w.v = h->vW[l]; w.grad = h->gWl[l]; w.splits = kSplits;
+        w.split_stride = (int64_t)h->rows[l] * h->cols[l]; w.rows = h->rows[l]; w.cols = h->cols[l];
+        w.rows_train = rows_train; w.Pb = h->Wb[l]; w.PbT = h->WbT[l];
+        a.off[2 * l] = off;
+        off += (int64_t)h->rows[l] * h->cols[l];
+        const float *bp;
+        int nblk, ld;
+        bias_partials(h, l, B, &bp, &nblk, &ld);
+        AdamSeg &bb = a.seg[2 * l + 1];
+        bb.P = h->b[l]; bb.m = h->mb[l]; bb.v = h->vb[l]; bb.grad = bp; bb.splits = nblk; bb.split_stride = ld;
+        bb.rows = h->rows[l]; bb.cols = 1; bb.rows_train = rows_train;
+        a.off[2 * l + 1] = off;
+        off += h->rows[l];
+    }
+    a.off[2 * kNLayer] = off;
+    a.step = h->dOptStep;
+    a.lr = lr; a.b1 = 0.9f; a.b2 = 0.999f; a.eps = 1e-8f;
+    k_adam_all<<<(unsigned)((off + 255) / 256), 256, 0, h->stream>>>(a);
+    MCK(cudaGetLastError());
+    return BG_OK;
+}
+
+// one training step on batch `*dBatchIdx` of h->perm: gather, forward, loss,
+// backward, Adam, counters
+int train_step(bg_mlp *h, int B, float lr) {
+    k_gather_at<<<B, 64, 0, h->stream>>>(h->Xall, h->Yall, h->perm, h->dBatchIdx, B, h->ydim, h->X, h->XT, h->Y);
+    int rc = forward(h, B);
+    if (rc) return rc;
+    k_nll<<<(B + 255) / 256, 256, 0, h->stream>>>(h->OUT, h->Y, B, h->ydim, h->dO, h->dOT, h->cs[kNLayer - 1], h->loss);
+    if ((rc = backward(h, B))) return rc;
+    // Adam's step count t is the step being taken (1 for the first)
+    k_step_advance<<<1, 1, 0, h->stream>>>(h->dBatchIdx, h->dOptStep);
+    if ((rc = adam_all(h, B, lr))) return rc;
+    MCK(cudaGetLastError());
     return BG_OK;
 }
 
@@ -434,7 +550,16 @@ BG_API int bg_mlp_create(bg_mlp **out, int device, int ydim) {
         if (!rc) rc = dalloc(&h->Wb[l], n);
         if (!rc) rc = dalloc(&h->WbT[l], n);
     }
-    if (!rc) rc = dalloc(&h->gW, (size_t)kSplits * kHid * kHid);
+    {
+        size_t tot = 0;
+        for (int l = 0; l < kNLayer; ++l) tot += (size_t)kSplits * h->rows[l] * h->cols[l];
+        tot = std::max(tot, (size_t)kSplits * kHid * kHid);
+        if (!rc) rc = dalloc(&h->gW, tot);
+        size_t o = 0;
+        for (int l = 0; l < kNLayer && !rc; ++l) { h->gWl[l] = h->gW + o; o += (size_t)kSplits * h->rows[l] * h->cols[l]; }
+    }
+    if (!rc) rc = dalloc(&h->dBatchIdx, 1);
+    if (!rc) rc = dalloc(&h->dOptStep, 1);
     if (!rc) rc = dalloc(&h->loss, 1);
     if (rc) {
         bg_mlp_destroy(h);
@@ -456,6 +581,9 @@ BG_API int bg_mlp_destroy(bg_mlp *h) {
     dfree(h->X); dfree(h->XT); dfree(h->dO); dfree(h->dOT); dfree(h->OUT); dfree(h->Y); dfree(h->idx);
     for (int l = 0; l < kNLayer; ++l) dfree(h->cs[l]);
     dfree(h->gW); dfree(h->loss); dfree(h->err); dfree(h->Xall); dfree(h->Yall);
+    dfree(h->dBatchIdx); dfree(h->dOptStep); dfree(h->pkeys); dfree(h->pkeys_out); dfree(h->pvals); dfree(h->perm);
+    if (h->sort_tmp) cudaFree(h->sort_tmp);
+    if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return BG_OK;
@@ -474,6 +602,7 @@ BG_API int bg_mlp_set_params(bg_mlp *h, int layer, const float *W, const float *
     k_to_bf16<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->W[layer], h->rows[layer], h->cols[layer],
                                                                     h->Wb[layer], h->WbT[layer]);
     MCK(cudaGetLastError());
+    MCK(cudaMemsetAsync(h->dOptStep, 0, sizeof(int64_t), h->stream));
     MCK(cudaStreamSynchronize(h->stream));
     h->step = 0;
     return BG_OK;
@@ -531,6 +660,12 @@ BG_API int bg_mlp_last_forward_ms(bg_mlp *h, float *ms) {
 BG_API int bg_mlp_set_data(bg_mlp *h, const float *X, const float *Y, int64_t n) {
     if (!h || !X || !Y || n <= 0) return fail(BG_EINVAL, "mlp: bad training set");
     MCK(cudaSetDevice(h->device));
+    MCK(cudaStreamSynchronize(h->stream));
+    // the training set moves: the epoch-order buffers and the captured step
+    // (which holds its addresses) are rebuilt by the next bg_mlp_train
+    dfree(h->pkeys); dfree(h->pkeys_out); dfree(h->pvals); dfree(h->perm);
+    if (h->sort_tmp) { cudaFree(h->sort_tmp); h->sort_tmp = nullptr; h->sort_tmp_bytes = 0; }
+    if (h->step_graph) { cudaGraphExecDestroy(h->step_graph); h->step_graph = nullptr; h->graph_batch = 0; }
     int rc = dalloc(&h->Xall, (size_t)n * kIn);
     if (!rc) rc = dalloc(&h->Yall, (size_t)n * h->ydim);
     if (rc) return rc;
@@ -549,38 +684,56 @@ BG_API int bg_mlp_train(bg_mlp *h, int epochs, int batch, float lr, uint64_t see
     int rc = ensure_batch(h, batch);
     if (rc) return rc;
     const int64_t steps = h->nset / batch;
-    std::vector<int64_t> perm(h->nset);
+    // the epoch order buffers and the sort's scratch, kept for later calls
+    if (!h->perm) {
+        if ((rc = dalloc(&h->pkeys, (size_t)h->nset)) || (rc = dalloc(&h->pkeys_out, (size_t)h->nset)) ||
+            (rc = dalloc(&h->pvals, (size_t)h->nset)) || (rc = dalloc(&h->perm, (size_t)h->nset)))
+            return rc;
+        size_t bytes = 0;
+        MCK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, h->pkeys, h->pkeys_out, h->pvals, h->perm, (int)h->nset));
+        MCK(cudaMalloc(&h->sort_tmp, bytes));
+        h->sort_tmp_bytes = bytes;
+    }
     cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventRecord(e0, h->stream);
+    MCK(cudaEventCreate(&e0));
+    MCK(cudaEventCreate(&e1));
+    MCK(cudaEventRecord(e0, h->stream));
     for (int ep = 0; ep < epochs && !rc; ++ep) {
-        // epoch permutation from a Philox stream keyed (seed, epoch)
-        for (int64_t i = 0; i < h->nset; ++i) perm[i] = i;
-        for (int64_t i = h->nset - 1; i > 0; --i) {
-            const int64_t j = (int64_t)(bg_philox_uniform(seed, ep, i) * (double)(i + 1));
-            std::swap(perm[i], perm[std::min(j, i)]);
-        }
-        int64_t *dperm = nullptr;
-        if (cudaMalloc((void **)&dperm, (size_t)steps * batch * sizeof(int64_t)) != cudaSuccess) {
-            rc = fail(BG_ENOMEM, "mlp: cudaMalloc failed");
-            break;
-        }
-        cudaMemcpyAsync(dperm, perm.data(), (size_t)steps * batch * sizeof(int64_t), cudaMemcpyHostToDevice,
-                        h->stream);
-        cudaMemsetAsync(h->loss, 0, sizeof(float), h->stream);
+        // the epoch's order: rows sorted by Philox keys (seed, epoch, row)
+        k_perm_keys<<<(unsigned)std::min<int64_t>((h->nset + 255) / 256, 4096), 256, 0, h->stream>>>(
+            seed, ep, h->nset, h->pkeys, h->pvals);
+        MCK(cudaGetLastError());
+        MCK(cub::DeviceRadixSort::SortPairs(h->sort_tmp, h->sort_tmp_bytes, h->pkeys, h->pkeys_out, h->pvals, h->perm,
+                                            (int)h->nset, 0, 64, h->stream));
+        MCK(cudaMemsetAsync(h->loss, 0, sizeof(float), h->stream));
+        MCK(cudaMemsetAsync(h->dBatchIdx, 0, sizeof(int64_t), h->stream));
         for (int64_t s = 0; s < steps && !rc; ++s) {
-            k_gather<<<batch, 64, 0, h->stream>>>(h->Xall, h->Yall, dperm + s * batch, batch, h->ydim, h->X, h->XT,
-                                                h->Y);
-            if ((rc = forward(h, batch))) break;
-            k_nll<<<(batch + 255) / 256, 256, 0, h->stream>>>(h->OUT, h->Y, batch, h->ydim, h->dO, h->dOT,
-                                                               h->cs[kNLayer - 1], h->loss);
-            rc = backward_and_update(h, batch, lr, true);
+            if (h->step_graph && h->graph_batch == batch && h->graph_lr == lr) {
+                MCK(cudaGraphLaunch(h->step_graph, h->stream));
+            } else if (s == 0) {
+                // the first step runs directly (kernel attributes, tensor maps)
+                rc = train_step(h, batch, lr);
+            } else {
+                // capture one step and replay it for the rest of training
+                if (h->step_graph) { cudaGraphExecDestroy(h->step_graph); h->step_graph = nullptr; }
+                cudaGraph_t graph = nullptr;
+                MCK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+                rc = train_step(h, batch, lr);
+                cudaError_t ce = cudaStreamEndCapture(h->stream, &graph);
+                if (!rc && ce != cudaSuccess) rc = fail(BG_ECUDA, std::string("mlp: step capture: ") + cudaGetErrorString(ce));
+                if (!rc && cudaGraphInstantiate(&h->step_graph, graph, 0) != cudaSuccess)
+                    rc = fail(BG_ECUDA, "mlp: step graph instantiation failed");
+                if (graph) cudaGraphDestroy(graph);
+                if (rc) break;
+                h->graph_batch = batch;
+                h->graph_lr = lr;
+                MCK(cudaGraphLaunch(h->step_graph, h->stream));
+            }
         }
+        h->step += steps;
         float ls = 0;
         cudaMemcpyAsync(&ls, h->loss, sizeof(float), cudaMemcpyDeviceToHost, h->stream);
         cudaError_t e = cudaStreamSynchronize(h->stream);
-        cudaFree(dperm);
         if (!rc && e != cudaSuccess) rc = fail(BG_ECUDA, std::string("mlp: training failed: ") + cudaGetErrorString(e));
         if (!rc) rc = check_err(h);
         if (epoch_loss) epoch_loss[ep] = ls / (float)steps;

@@ -74,8 +74,8 @@ struct GemmArgs {
     const __nv_bfloat16 *act; // [M][ldact] for EPI_DRELU_BF16
     int ldact;
     int n_valid;              // columns >= n_valid are written as 0 (bf16 outs) / skipped (fp32)
-    float *colsum;            // EPI_DRELU_BF16: column sums of the bf16 result over each CTA's
-    int colsum_ld;            //   128 rows, at colsum[blockIdx.x * colsum_ld + col] (or null)
+    float *colsum;            // EPI_DRELU_BF16: column sums of the bf16 result over each 32-row
+    int colsum_ld;            //   quarter of a row tile, at colsum[(4 * row tile + quarter) * colsum_ld + col] (or null)
     int *err;                 // error flag (device)
 };
 
@@ -452,14 +452,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(const GemmArgs g, const __
             }
         }
         if (EPI == EPI_DRELU_BF16 && g.colsum) {
-            __syncthreads();
-            if (warp == 0) {
-                for (int c = lane; c < NT; c += 32) {
-                    const int col = n0 + c;
-                    if (col < g.N)
-                        g.colsum[(long long)blockIdx.x * g.colsum_ld + col] =
-                            ((red[c] + red[NT + c]) + red[2 * NT + c]) + red[3 * NT + c];
-                }
+            __syncwarp();
+            // this warp's 32-row column sums: row (4 blockIdx.x + warp) of colsum
+            for (int c = lane; c < NT; c += 32) {
+                const int col = n0 + c;
+                if (col < g.N) g.colsum[(long long)(4 * blockIdx.x + warp) * g.colsum_ld + col] = red[warp * NT + c];
             }
         }
     }
@@ -473,6 +470,283 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(const GemmArgs g, const __
 template <int NT>
 constexpr size_t smem_bytes() {
     return sizeof(Smem<NT>) + 1024;
+}
+
+// ---------------------------------------------------------------------------
+// Persistent, warp-specialised form of the same product (TMA operands only).
+// A grid of at most one CTA per SM walks the output tiles (consecutive CTAs
+// take consecutive row tiles of one column tile, so they share the B tile in
+// L2).  Six warps per CTA:
+//   warp 0  producer: one thread fills a kPStages-deep ring of operand
+//           stages with TMA boxes (full[s] armed with the expected bytes,
+//           refilled after empty[s], which the MMAs of the stage commit to);
+//   warp 1  MMA: one thread issues the four tcgen05.mma of each K-chunk into
+//           one of two TMEM accumulators (2 x NT columns) and commits the
+//           finished tile to acc_full[buf];
+//   warps 2-5  epilogue: tcgen05.ld of their 32-lane quarter, the fused
+//           epilogue, stores straight from registers (each thread writes 16
+//           consecutive columns of its row: whole 32-byte sectors; the
+//           transposed copy is one 64-byte run per column and warp), then
+//           acc_empty[buf] frees the accumulator.
+// So the epilogue of tile i runs while the MMAs of tile i+1 accumulate into
+// the other buffer, and TMEM allocation, barrier set-up and pipeline fill are
+// paid once per CTA instead of once per tile.  Every wait is bounded; a wait
+// that gives up marks the CTA failed, the roles leave their loops, the
+// producer waits for its boxes in flight, the MMA thread for its MMAs, and
+// the TMEM is released.
+constexpr int kPStages = 4;
+constexpr int kPThreads = 192;
+
+template <int NT>
+struct PSmem {
+    alignas(1024) unsigned char a[kPStages][kM * kKc * 2];
+    alignas(1024) unsigned char b[kPStages][NT * kKc * 2];
+    alignas(8) unsigned long long full[kPStages];
+    alignas(8) unsigned long long empty[kPStages];
+    alignas(8) unsigned long long acc_full[2];
+    alignas(8) unsigned long long acc_empty[2];
+    alignas(8) unsigned long long done;
+    float red[4][NT];          // per-quarter column sums (EPI_DRELU_BF16)
+    uint32_t tmem_base;
+    int failed;
+};
+
+template <int NT>
+constexpr size_t psmem_bytes() {
+    return sizeof(PSmem<NT>) + 1024;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
+
+// tile t -> (row tile, column tile, split): row tiles vary fastest
+__device__ __forceinline__ void tile_coords(int t, int tiles_m, int tiles_n, int &mt, int &nt, int &z) {
+    mt = t % tiles_m;
+    const int r = t / tiles_m;
+    nt = r % tiles_n;
+    z = r / tiles_n;
+}
+
+template <int NT, int EPI>
+__device__ __forceinline__ void p_epilogue_chunk(const GemmArgs &g, const float (&v)[16], int row, int n0, int cb,
+                                                 int ntile_m, int quarter, int lane, PSmem<NT> &sm, int z) {
+    constexpr bool kBF = (EPI == EPI_RELU_BF16 || EPI == EPI_DRELU_BF16);
+    const bool row_ok = row < g.M;
+    const int c0 = n0 + cb;
+    if (kBF) {
+        __nv_bfloat16 hv[16];
+        float act[16];
+        if (EPI == EPI_DRELU_BF16) {
+            if (row_ok) {
+                const __nv_bfloat16 *src = g.act + (long long)row * g.ldact + c0;
+                const bool vec = ((((uintptr_t)src) & 15) == 0) && c0 + 16 <= g.N;
+                if (vec) {
+                    uint4 u[2];
+                    u[0] = *reinterpret_cast<const uint4 *>(src);
+                    u[1] = *reinterpret_cast<const uint4 *>(src + 8);
+                    const __nv_bfloat16 *h = reinterpret_cast<const __nv_bfloat16 *>(u);
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) act[i] = __bfloat162float(h[i]);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) act[i] = c0 + i < g.N ? __bfloat162float(src[i]) : 0.f;
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) act[i] = 0.f;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const int col = c0 + i;
+            float x = v[i];
+            if (EPI == EPI_RELU_BF16) {
+                x = col < g.N ? x + __ldg(g.bias + col) : 0.f;
+                x = x > 0.f ? x : 0.f;
+            } else {
+                x = act[i] > 0.f ? x : 0.f;
+            }
+            if (col >= g.n_valid || col >= g.N || !row_ok) x = 0.f;
+            hv[i] = __float2bfloat16_rn(x);
+        }
+        if (row_ok) {
+            __nv_bfloat16 *d = g.H + (long long)row * g.ldh + c0;
+            if (((((uintptr_t)d) & 15) == 0) && c0 + 16 <= g.N) {
+                reinterpret_cast<uint4 *>(d)[0] = reinterpret_cast<const uint4 *>(hv)[0];
+                reinterpret_cast<uint4 *>(d)[1] = reinterpret_cast<const uint4 *>(hv)[1];
+            } else {
+                for (int i = 0; i < 16 && c0 + i < g.N; ++i) d[i] = hv[i];
+            }
+            if (g.HT)
+#pragma unroll
+                for (int i = 0; i < 16; ++i)
+                    if (c0 + i < g.N) g.HT[(long long)(c0 + i) * g.ldht + row] = hv[i];
+        }
+        if (EPI == EPI_DRELU_BF16 && g.colsum) {
+            // column sums of the bf16 results over the quarter's 32 rows
+            // (a fixed butterfly order, so the result is deterministic)
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                float s = __bfloat162float(hv[i]);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+                if (lane == 0) sm.red[quarter][cb + i] = s;
+            }
+        }
+    } else {
+        if (row_ok) {
+            const int limit = min(g.N, g.n_valid);
+            float o[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) o[i] = (EPI == EPI_BIAS_F32 && c0 + i < g.N) ? v[i] + __ldg(g.bias + c0 + i) : v[i];
+            float *d = g.C + (long long)z * g.split_stride + (long long)row * g.ldc + c0;
+            if (((((uintptr_t)d) & 15) == 0) && c0 + 16 <= limit) {
+#pragma unroll
+                for (int i = 0; i < 16; i += 4) reinterpret_cast<float4 *>(d)[i / 4] = make_float4(o[i], o[i + 1], o[i + 2], o[i + 3]);
+            } else {
+                for (int i = 0; i < 16 && c0 + i < limit; ++i) d[i] = o[i];
+            }
+        }
+    }
+}
+
+template <int NT, int EPI>
+__global__ void __launch_bounds__(kPThreads, 1) k_gemm_p(const GemmArgs g, const __grid_constant__ CUtensorMap ta,
+                                                        const __grid_constant__ CUtensorMap tb, int tiles_m,
+                                                        int tiles_n, int splits) {
+    extern __shared__ unsigned char smem_raw[];
+    PSmem<NT> &sm = *reinterpret_cast<PSmem<NT> *>((void *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023));
+    constexpr uint32_t kCols = 2 * NT < 32 ? 32 : 2 * NT;     // two accumulators, power of two
+    constexpr uint32_t idesc = idesc_bf16(kM, NT);
+    constexpr uint32_t kLboA = kM * 16, kLboB = NT * 16;
+    constexpr uint32_t kBytes = (kM + NT) * kKc * 2;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int ntiles = tiles_m * tiles_n * splits;
+    const int nk = g.k_per_split / kKc;
+
+    if (tid == 0) {
+        for (int s = 0; s < kPStages; ++s) {
+            mbar_init(smem_u32(&sm.full[s]), 1);
+            mbar_init(smem_u32(&sm.empty[s]), 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(smem_u32(&sm.acc_full[b]), 1);
+            mbar_init(smem_u32(&sm.acc_empty[b]), 4);
+        }
+        mbar_init(smem_u32(&sm.done), 1);
+        sm.failed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&sm.tmem_base)),
+                     "r"(kCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = sm.tmem_base;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---- producer
+            long long it = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+                int mt, nt, z;
+                tile_coords(t, tiles_m, tiles_n, mt, nt, z);
+                const int m0 = mt * kM, n0 = nt * NT, kbeg = z * g.k_per_split;
+                for (int c = 0; c < nk; ++c, ++it) {
+                    const int st = (int)(it % kPStages);
+                    const long long use = it / kPStages;
+                    if (use >= 1 && !mbar_wait(smem_u32(&sm.empty[st]), (uint32_t)((use - 1) & 1))) { ok = false; break; }
+                    if (*(volatile int *)&sm.failed) { ok = false; break; }
+                    const uint32_t fb = smem_u32(&sm.full[st]);
+                    mbar_expect_tx(fb, kBytes);
+                    const uint32_t a_addr = smem_u32(sm.a[st]), b_addr = smem_u32(sm.b[st]);
+                    const int kx = kbeg + c * kKc;
+#pragma unroll
+                    for (int q = 0; q < kKc / 8; ++q) {
+                        tma_load_2d(a_addr + q * kLboA, &ta, kx + q * 8, m0, fb);
+                        tma_load_2d(b_addr + q * kLboB, &tb, kx + q * 8, n0, fb);
+                    }
+                }
+            }
+            if (!ok) atomicExch(&sm.failed, 1);
+            // the last boxes issued into each stage have landed before the CTA leaves
+            for (long long j = (it > kPStages ? it - kPStages : 0); j < it; ++j)
+                mbar_wait(smem_u32(&sm.full[j % kPStages]), (uint32_t)((j / kPStages) & 1));
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---- MMA issue
+            long long it = 0;
+            int ti = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++ti) {
+                const int buf = ti & 1, use = ti >> 1;
+                if (use >= 1 && !mbar_wait(smem_u32(&sm.acc_empty[buf]), (uint32_t)((use - 1) & 1))) { ok = false; break; }
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                const uint32_t acc = tmem + (uint32_t)(buf * NT);
+                for (int c = 0; c < nk; ++c, ++it) {
+                    const int st = (int)(it % kPStages);
+                    if (!mbar_wait(smem_u32(&sm.full[st]), (uint32_t)((it / kPStages) & 1))) { ok = false; break; }
+                    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                    const uint32_t a_addr = smem_u32(sm.a[st]), b_addr = smem_u32(sm.b[st]);
+#pragma unroll
+                    for (int j = 0; j < kKc / 16; ++j)
+                        umma_bf16(acc, smem_desc(a_addr + j * 2 * kLboA, kLboA, 128),
+                                  smem_desc(b_addr + j * 2 * kLboB, kLboB, 128), idesc, (c > 0 || j > 0) ? 1u : 0u);
+                    umma_commit(smem_u32(&sm.empty[st]));
+                }
+                if (!ok) break;
+                umma_commit(smem_u32(&sm.acc_full[buf]));
+            }
+            if (!ok) atomicExch(&sm.failed, 1);
+            umma_commit(smem_u32(&sm.done));    // arrives once every MMA issued above has finished
+            if (!mbar_wait(smem_u32(&sm.done), 0u)) atomicExch(&sm.failed, 1);
+        }
+    } else {
+        // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31
+        const int quarter = warp & 3;
+        int ti = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++ti) {
+            const int buf = ti & 1, use = ti >> 1;
+            int mt, nt, z;
+            tile_coords(t, tiles_m, tiles_n, mt, nt, z);
+            const int m0 = mt * kM, n0 = nt * NT;
+            bool ok = mbar_wait(smem_u32(&sm.acc_full[buf]), (uint32_t)(use & 1));
+            ok = __all_sync(0xffffffffu, ok);
+            if (!ok || *(volatile int *)&sm.failed) { if (lane == 0) atomicExch(&sm.failed, 1); break; }
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const int row = m0 + quarter * 32 + lane;
+#pragma unroll 1
+            for (int cb = 0; cb < NT; cb += 16) {
+                float v[16];
+                tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * NT + cb), v);
+                p_epilogue_chunk<NT, EPI>(g, v, row, n0, cb, mt, quarter, lane, sm, z);
+            }
+            // the accumulator is free once every lane's loads are done
+            asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&sm.acc_empty[buf]));
+            if (EPI == EPI_DRELU_BF16 && g.colsum) {
+                // this quarter's 32-row column sums: row (4 mt + quarter) of colsum
+                __syncwarp();
+                for (int c = lane; c < NT; c += 32)
+                    if (n0 + c < g.N) g.colsum[(long long)(4 * mt + quarter) * g.colsum_ld + n0 + c] = sm.red[quarter][c];
+                __syncwarp();
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (sm.failed && tid == 0 && g.err) atomicExch(g.err, 1);
+    if (warp == 1) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kCols) : "memory");
+    }
 }
 
 }  // namespace umma
