@@ -26,6 +26,7 @@
 #include <cstdint>
 #include <cstring>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "bg_common.cuh"
@@ -73,6 +74,8 @@ __global__ void k_gather(const float *Xall, const float *Yall, const int64_t *id
 // bf16 gradients into colsum[blockIdx.x][64] (the output bias gradient).
 __global__ void __launch_bounds__(256) k_nll(const float *OUT, const float *Y, int B, int ydim, bf16 *dO, bf16 *dOT,
                                              float *colsum, float *loss_sum) {
+    umma::pdl_launch_dependents();
+    umma::pdl_wait();
     constexpr int kMaxY = kOutPad / 2;
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     __shared__ float red[8][kOutPad];
@@ -148,7 +151,9 @@ struct AdamAll {
     const int64_t *step;
     float lr, b1, b2, eps;
 };
-__global__ void k_adam_all(const AdamAll a) {
+__global__ void k_adam_all(const __grid_constant__ AdamAll a) {
+    umma::pdl_launch_dependents();
+    umma::pdl_wait();
     const int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i0 >= a.off[2 * kNLayer]) return;
     int k = 0;
@@ -178,6 +183,8 @@ __global__ void k_adam_all(const AdamAll a) {
 // One training step's bookkeeping: the batch index within the epoch and the
 // optimiser step, advanced after the step's kernels.
 __global__ void k_step_advance(int64_t *batch_index, int64_t *opt_step) {
+    umma::pdl_launch_dependents();
+    umma::pdl_wait();
     *batch_index += 1;
     *opt_step += 1;
 }
@@ -227,17 +234,19 @@ EncodeTiledFn encode_tiled() {
 }
 
 // 2-D map of a row-major bf16 matrix [rows][ld] over its first `cols`
-// columns, boxes of 8 columns x box_rows rows, zero fill past the edges.
-bool tile_map(CUtensorMap *m, const bf16 *base, int rows, int cols, int ld, int box_rows) {
+// columns, zero fill past the edges: boxes of 8 columns x box_rows rows
+// (no swizzle), or with sw128 of 64 columns (one 128-byte line) x box_rows
+// rows landing in the 128-byte swizzled layout.
+bool tile_map(CUtensorMap *m, const bf16 *base, int rows, int cols, int ld, int box_rows, bool sw128 = false) {
     EncodeTiledFn f = encode_tiled();
-    if (!f || ((uintptr_t)base & 15) || ((size_t)ld * 2) % 16 || cols % 8) return false;
+    if (!f || ((uintptr_t)base & 15) || ((size_t)ld * 2) % 16 || cols % (sw128 ? 64 : 8)) return false;
     const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
     const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
-    const cuuint32_t box[2] = {8, (cuuint32_t)box_rows};
+    const cuuint32_t box[2] = {sw128 ? 64u : 8u, (cuuint32_t)box_rows};
     const cuuint32_t estr[2] = {1, 1};
     return f(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void *)base, dims, strides, box, estr,
-             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+             CU_TENSOR_MAP_INTERLEAVE_NONE, sw128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 template <int NT, int EPI, bool TMA>
@@ -253,6 +262,25 @@ int launch_gemm_as(const umma::GemmArgs &g, int splits, cudaStream_t st, const C
     umma::k_gemm<NT, EPI, TMA><<<grid, umma::kThreads, smem, st>>>(g, ta, tb);
     MCK(cudaGetLastError());
     return BG_OK;
+}
+
+// Launch with programmatic stream serialization: the kernel may start while
+// the previous one in the stream finishes; it waits (griddepcontrol.wait)
+// before reading anything that one wrote.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args &&...args) {
+    cudaLaunchConfig_t cfg;
+    memset(&cfg, 0, sizeof cfg);
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 int sm_count_mlp() {
@@ -274,8 +302,8 @@ int launch_gemm_persistent(const umma::GemmArgs &g, int splits, cudaStream_t st,
     const int tiles_m = (g.M + umma::kM - 1) / umma::kM, tiles_n = (g.N + NT - 1) / NT;
     const int ntiles = tiles_m * tiles_n * splits;
     const int grid = std::max(1, std::min(ntiles, sm_count_mlp()));
-    umma::k_gemm_p<NT, EPI><<<grid, umma::kPThreads, smem, st>>>(g, ta, tb, tiles_m, tiles_n, splits);
-    MCK(cudaGetLastError());
+    MCK(launch_pdl(umma::k_gemm_p<NT, EPI>, dim3(grid), dim3(umma::kPThreads), smem, st, g, ta, tb, tiles_m, tiles_n,
+                   splits));
     return BG_OK;
 }
 
@@ -288,8 +316,10 @@ int launch_gemm(const umma::GemmArgs &g, int splits, cudaStream_t st) {
     memset(&ta, 0, sizeof ta);
     memset(&tb, 0, sizeof tb);
     if (g.k_per_split >= umma::kKc && g.k_per_split % umma::kKc == 0 && (long long)g.k_per_split * splits == g.K &&
-        tile_map(&ta, g.A, g.M, g.K, g.lda, umma::kM) && tile_map(&tb, g.B, g.N, g.K, g.ldb, NT))
+        tile_map(&ta, g.A, g.M, g.K, g.lda, umma::kM, true) && tile_map(&tb, g.B, g.N, g.K, g.ldb, NT, true))
         return launch_gemm_persistent<NT, EPI>(g, splits, st, ta, tb);
+    memset(&ta, 0, sizeof ta);
+    memset(&tb, 0, sizeof tb);
     return launch_gemm_as<NT, EPI, false>(g, splits, st, ta, tb);
 }
 
@@ -498,8 +528,7 @@ int adam_all(bg_mlp *h, int B, float lr) {
     a.off[2 * kNLayer] = off;
     a.step = h->dOptStep;
     a.lr = lr; a.b1 = 0.9f; a.b2 = 0.999f; a.eps = 1e-8f;
-    k_adam_all<<<(unsigned)((off + 255) / 256), 256, 0, h->stream>>>(a);
-    MCK(cudaGetLastError());
+    MCK(launch_pdl(k_adam_all, dim3((unsigned)((off + 255) / 256)), dim3(256), 0, h->stream, a));
     return BG_OK;
 }
 
@@ -509,10 +538,11 @@ int train_step(bg_mlp *h, int B, float lr) {
     k_gather_at<<<B, 64, 0, h->stream>>>(h->Xall, h->Yall, h->perm, h->dBatchIdx, B, h->ydim, h->X, h->XT, h->Y);
     int rc = forward(h, B);
     if (rc) return rc;
-    k_nll<<<(B + 255) / 256, 256, 0, h->stream>>>(h->OUT, h->Y, B, h->ydim, h->dO, h->dOT, h->cs[kNLayer - 1], h->loss);
+    MCK(launch_pdl(k_nll, dim3((B + 255) / 256), dim3(256), 0, h->stream, (const float *)h->OUT, (const float *)h->Y, B,
+                   h->ydim, h->dO, h->dOT, h->cs[kNLayer - 1], h->loss));
     if ((rc = backward(h, B))) return rc;
     // Adam's step count t is the step being taken (1 for the first)
-    k_step_advance<<<1, 1, 0, h->stream>>>(h->dBatchIdx, h->dOptStep);
+    MCK(launch_pdl(k_step_advance, dim3(1), dim3(1), 0, h->stream, h->dBatchIdx, h->dOptStep));
     if ((rc = adam_all(h, B, lr))) return rc;
     MCK(cudaGetLastError());
     return BG_OK;
@@ -828,10 +858,15 @@ BG_API int bg_mlp_gradients(bg_mlp *h, int batch, float *loss, float *const *dW,
 // fp32 out), K a multiple of 64; the tensor-core kernel of the network.
 BG_API int bg_gemm_bf16(int64_t M, int64_t N, int64_t K, const void *A, const void *B, float *C, void *stream) {
     if (M <= 0 || N <= 0 || K <= 0 || K % 64 != 0 || !A || !B || !C) return fail(BG_EINVAL, "gemm: bad shape");
-    int *err = nullptr;
-    MCK(cudaMalloc((void **)&err, sizeof(int)));
-    MCK(cudaMemset(err, 0, sizeof(int)));
+    // the error flag of the tensor-core waits: one per device, kept for the process
+    static int *flags[64] = {nullptr};
+    int dev = 0;
+    MCK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(BG_EINVAL, "gemm: device index");
+    if (!flags[dev]) MCK(cudaMalloc((void **)&flags[dev], sizeof(int)));
+    int *err = flags[dev];
     cudaStream_t st = (cudaStream_t)stream;
+    MCK(cudaMemsetAsync(err, 0, sizeof(int), st));
     umma::GemmArgs g = gemm_args((const bf16 *)A, (int)K, (const bf16 *)B, (int)K, (int)M, (int)N, (int)K, err);
     g.C = C;
     g.ldc = (int)N;
@@ -839,7 +874,6 @@ BG_API int bg_gemm_bf16(int64_t M, int64_t N, int64_t K, const void *A, const vo
     cudaError_t e = cudaStreamSynchronize(st);
     int ev = 0;
     cudaMemcpy(&ev, err, sizeof(int), cudaMemcpyDeviceToHost);
-    cudaFree(err);
     if (rc) return rc;
     if (e != cudaSuccess) return fail(BG_ECUDA, std::string("gemm: ") + cudaGetErrorString(e));
     if (ev) return fail(BG_ETIMEOUT, "gemm: a tensor-core wait gave up");

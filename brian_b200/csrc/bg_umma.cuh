@@ -92,6 +92,21 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo = kLBO
     return d;
 }
 
+// K-major tile in the 128-byte swizzled layout: each row's 64 bf16 of a
+// K-chunk are one 128-byte line, 8-row atoms of 1024 bytes (stride byte
+// offset), the 16-byte pieces of a line XOR-permuted by the row within the
+// atom.  The K-step of one MMA (16 elements) advances the start address by
+// 32 bytes inside the line; the tiles are 1024-byte aligned (base offset 0).
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1 << 16;                          // leading byte offset: unused for swizzled K-major
+    d |= (uint64_t)((1024u >> 4) & 0x3FFFu) << 32;   // stride byte offset: one 8-row atom
+    d |= (uint64_t)1 << 46;                          // sm100 descriptor version
+    d |= (uint64_t)2 << 61;                          // layout: 128-byte swizzle
+    return d;
+}
+
 __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
 }
@@ -164,6 +179,17 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// 16 columns of the warp's 32 TMEM lanes into registers, without waiting
+// (tcgen05.wait::ld before the registers are read)
+__device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
 }
 
 // Shared memory of one CTA: the stage ring, the mbarriers, the TMEM base.
@@ -473,11 +499,13 @@ constexpr size_t smem_bytes() {
 }
 
 // ---------------------------------------------------------------------------
-// Persistent, warp-specialised form of the same product (TMA operands only).
+// Persistent, warp-specialised form of the same product (TMA operands only,
+// stages in the 128-byte swizzled K-major layout: one TMA box per operand and
+// K-chunk instead of eight 16-byte-wide ones; 6-8 stages in flight).
 // A grid of at most one CTA per SM walks the output tiles (consecutive CTAs
 // take consecutive row tiles of one column tile, so they share the B tile in
 // L2).  Six warps per CTA:
-//   warp 0  producer: one thread fills a kPStages-deep ring of operand
+//   warp 0  producer: one thread fills a PStages-deep ring of operand
 //           stages with TMA boxes (full[s] armed with the expected bytes,
 //           refilled after empty[s], which the MMAs of the stage commit to);
 //   warp 1  MMA: one thread issues the four tcgen05.mma of each K-chunk into
@@ -494,15 +522,24 @@ constexpr size_t smem_bytes() {
 // that gives up marks the CTA failed, the roles leave their loops, the
 // producer waits for its boxes in flight, the MMA thread for its MMAs, and
 // the TMEM is released.
-constexpr int kPStages = 4;
 constexpr int kPThreads = 192;
+// operand stages in flight: as many as fit in 100 KB, so that the CTA of the
+// next product (launched early, programmatic dependent launch) fits beside it
+template <int NT> struct PStages { static constexpr int value = (100 * 1024) / ((kM + NT) * kKc * 2); };
+
+// Programmatic dependent launch: the kernel lets the next one in its stream
+// start launching, and waits for the previous one to finish (and its writes
+// to be visible) before touching global memory.
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
 
 template <int NT>
 struct PSmem {
-    alignas(1024) unsigned char a[kPStages][kM * kKc * 2];
-    alignas(1024) unsigned char b[kPStages][NT * kKc * 2];
-    alignas(8) unsigned long long full[kPStages];
-    alignas(8) unsigned long long empty[kPStages];
+    static constexpr int S = PStages<NT>::value;
+    alignas(1024) unsigned char a[S][kM * kKc * 2];
+    alignas(1024) unsigned char b[S][NT * kKc * 2];
+    alignas(8) unsigned long long full[S];
+    alignas(8) unsigned long long empty[S];
     alignas(8) unsigned long long acc_full[2];
     alignas(8) unsigned long long acc_empty[2];
     alignas(8) unsigned long long done;
@@ -528,9 +565,26 @@ __device__ __forceinline__ void tile_coords(int t, int tiles_m, int tiles_n, int
     z = r / tiles_n;
 }
 
+// The ReLU mask source of a DRELU epilogue, 16 columns of the thread's row
+// from c0 on (0 past the matrix), read before the accumulator is ready.
+__device__ __forceinline__ void p_load_act(const GemmArgs &g, int row, int c0, uint4 (&u)[2]) {
+    u[0] = make_uint4(0, 0, 0, 0);
+    u[1] = make_uint4(0, 0, 0, 0);
+    if (row >= g.M) return;
+    const __nv_bfloat16 *src = g.act + (long long)row * g.ldact + c0;
+    if (((((uintptr_t)src) & 15) == 0) && c0 + 16 <= g.N) {
+        u[0] = *reinterpret_cast<const uint4 *>(src);
+        u[1] = *reinterpret_cast<const uint4 *>(src + 8);
+    } else {
+        __nv_bfloat16 *h = reinterpret_cast<__nv_bfloat16 *>(u);
+        for (int i = 0; i < 16 && c0 + i < g.N; ++i) h[i] = src[i];
+    }
+}
+
 template <int NT, int EPI>
 __device__ __forceinline__ void p_epilogue_chunk(const GemmArgs &g, const float (&v)[16], int row, int n0, int cb,
-                                                 int ntile_m, int quarter, int lane, PSmem<NT> &sm, int z) {
+                                                 int ntile_m, int quarter, int lane, PSmem<NT> &sm, int z,
+                                                 const uint4 (&actu)[2]) {
     constexpr bool kBF = (EPI == EPI_RELU_BF16 || EPI == EPI_DRELU_BF16);
     const bool row_ok = row < g.M;
     const int c0 = n0 + cb;
@@ -538,24 +592,9 @@ __device__ __forceinline__ void p_epilogue_chunk(const GemmArgs &g, const float 
         __nv_bfloat16 hv[16];
         float act[16];
         if (EPI == EPI_DRELU_BF16) {
-            if (row_ok) {
-                const __nv_bfloat16 *src = g.act + (long long)row * g.ldact + c0;
-                const bool vec = ((((uintptr_t)src) & 15) == 0) && c0 + 16 <= g.N;
-                if (vec) {
-                    uint4 u[2];
-                    u[0] = *reinterpret_cast<const uint4 *>(src);
-                    u[1] = *reinterpret_cast<const uint4 *>(src + 8);
-                    const __nv_bfloat16 *h = reinterpret_cast<const __nv_bfloat16 *>(u);
+            const __nv_bfloat16 *h = reinterpret_cast<const __nv_bfloat16 *>(actu);
 #pragma unroll
-                    for (int i = 0; i < 16; ++i) act[i] = __bfloat162float(h[i]);
-                } else {
-#pragma unroll
-                    for (int i = 0; i < 16; ++i) act[i] = c0 + i < g.N ? __bfloat162float(src[i]) : 0.f;
-                }
-            } else {
-#pragma unroll
-                for (int i = 0; i < 16; ++i) act[i] = 0.f;
-            }
+            for (int i = 0; i < 16; ++i) act[i] = __bfloat162float(h[i]);
         }
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
@@ -619,11 +658,17 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_p(const GemmArgs g, const
     PSmem<NT> &sm = *reinterpret_cast<PSmem<NT> *>((void *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023));
     constexpr uint32_t kCols = 2 * NT < 32 ? 32 : 2 * NT;     // two accumulators, power of two
     constexpr uint32_t idesc = idesc_bf16(kM, NT);
-    constexpr uint32_t kLboA = kM * 16, kLboB = NT * 16;
     constexpr uint32_t kBytes = (kM + NT) * kKc * 2;
+    constexpr int kPStages = PSmem<NT>::S;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int ntiles = tiles_m * tiles_n * splits;
     const int nk = g.k_per_split / kKc;
+    pdl_launch_dependents();
+    if (tid == 0) {
+        // the tensor maps' descriptors into the TMA unit's cache ahead of the first box
+        asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&ta)) : "memory");
+        asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&tb)) : "memory");
+    }
 
     if (tid == 0) {
         for (int s = 0; s < kPStages; ++s) {
@@ -648,6 +693,8 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_p(const GemmArgs g, const
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     const uint32_t tmem = sm.tmem_base;
+    // set-up done: from here on the previous kernel's results are read
+    pdl_wait();
 
     if (warp == 0) {
         if (lane == 0) {
@@ -665,13 +712,10 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_p(const GemmArgs g, const
                     if (*(volatile int *)&sm.failed) { ok = false; break; }
                     const uint32_t fb = smem_u32(&sm.full[st]);
                     mbar_expect_tx(fb, kBytes);
-                    const uint32_t a_addr = smem_u32(sm.a[st]), b_addr = smem_u32(sm.b[st]);
                     const int kx = kbeg + c * kKc;
-#pragma unroll
-                    for (int q = 0; q < kKc / 8; ++q) {
-                        tma_load_2d(a_addr + q * kLboA, &ta, kx + q * 8, m0, fb);
-                        tma_load_2d(b_addr + q * kLboB, &tb, kx + q * 8, n0, fb);
-                    }
+                    // one box of 64 K-elements (a 128-byte line) x all tile rows per operand
+                    tma_load_2d(smem_u32(sm.a[st]), &ta, kx, m0, fb);
+                    tma_load_2d(smem_u32(sm.b[st]), &tb, kx, n0, fb);
                 }
             }
             if (!ok) atomicExch(&sm.failed, 1);
@@ -697,8 +741,8 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_p(const GemmArgs g, const
                     const uint32_t a_addr = smem_u32(sm.a[st]), b_addr = smem_u32(sm.b[st]);
 #pragma unroll
                     for (int j = 0; j < kKc / 16; ++j)
-                        umma_bf16(acc, smem_desc(a_addr + j * 2 * kLboA, kLboA, 128),
-                                  smem_desc(b_addr + j * 2 * kLboB, kLboB, 128), idesc, (c > 0 || j > 0) ? 1u : 0u);
+                        umma_bf16(acc, smem_desc_sw128(a_addr + j * 32), smem_desc_sw128(b_addr + j * 32), idesc,
+                                  (c > 0 || j > 0) ? 1u : 0u);
                     umma_commit(smem_u32(&sm.empty[st]));
                 }
                 if (!ok) break;
@@ -717,21 +761,33 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_p(const GemmArgs g, const
             int mt, nt, z;
             tile_coords(t, tiles_m, tiles_n, mt, nt, z);
             const int m0 = mt * kM, n0 = nt * NT;
+            const int row = m0 + quarter * 32 + lane;
+            // the mask source is read while the MMAs of the tile run
+            uint4 actu[NT / 16][2];
+            if (EPI == EPI_DRELU_BF16)
+#pragma unroll
+                for (int q = 0; q < NT / 16; ++q) p_load_act(g, row, n0 + 16 * q, actu[q]);
             bool ok = mbar_wait(smem_u32(&sm.acc_full[buf]), (uint32_t)(use & 1));
             ok = __all_sync(0xffffffffu, ok);
             if (!ok || *(volatile int *)&sm.failed) { if (lane == 0) atomicExch(&sm.failed, 1); break; }
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-            const int row = m0 + quarter * 32 + lane;
-#pragma unroll 1
-            for (int cb = 0; cb < NT; cb += 16) {
-                float v[16];
-                tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * NT + cb), v);
-                p_epilogue_chunk<NT, EPI>(g, v, row, n0, cb, mt, quarter, lane, sm, z);
-            }
-            // the accumulator is free once every lane's loads are done
+            // the whole row of the tile out of TMEM with one wait, and the
+            // accumulator handed back to the MMA warp before the stores
+            uint32_t raw[NT / 16][16];
+#pragma unroll
+            for (int q = 0; q < NT / 16; ++q)
+                tmem_ld16_nowait(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * NT + 16 * q), raw[q]);
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(&sm.acc_empty[buf]));
+#pragma unroll
+            for (int q = 0; q < NT / 16; ++q) {
+                float v[16];
+#pragma unroll
+                for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(raw[q][i]);
+                p_epilogue_chunk<NT, EPI>(g, v, row, n0, 16 * q, mt, quarter, lane, sm, z, actu[q]);
+            }
             if (EPI == EPI_DRELU_BF16 && g.colsum) {
                 // this quarter's 32-row column sums: row (4 mt + quarter) of colsum
                 __syncwarp();
