@@ -511,9 +511,17 @@ def synapses_case(seed, n=32768, indegree=160, sim_steps=2000, profile_steps=300
     idx = np.asarray(M._record()[1])[ev0:]
     events = int(outdeg[idx].sum())
     nnz = sum(len(S) for S in syns)
-    dms = sum(v for k, v in prof if k.startswith("syn_deliver"))
+    dms = sum(v for k, v in prof if k.startswith("syn_"))
+    event_path = any(k.startswith("syn_gather") for k, _ in prof)
     hits_per_step = events / sim_steps
-    alg = nnz * 4 + (n + 1) * 8 * 2 + n * 8 * 2 + hits_per_step * 8
+    # algorithmic bytes of the delivery: the pull reads every synapse word,
+    # the state and the column offsets, plus the terms of the hits; the event
+    # path reads the spike history words of the delay window, per event a
+    # target, a column position and a term and the bin entry written and read
+    if event_path:
+        alg = (n / 32) * 4 * 41 + hits_per_step * (4 + 4 + 8 + 12 + 12) + n * 8 * 2
+    else:
+        alg = nnz * 4 + (n + 1) * 8 * 2 + n * 8 * 2 + hits_per_step * 8
     peak, peak_src = peaks()
     # the oracle (single-threaded C restatement, SpikeQueue in host memory)
     # on the same network, a bounded sample of steps from the same state
@@ -537,6 +545,7 @@ def synapses_case(seed, n=32768, indegree=160, sim_steps=2000, profile_steps=300
             "spikes": int(len(idx)), "events": events, "device_ms": st["last_run_ms"], "wall_s": wall,
             "events_per_s": events / (st["last_run_ms"] * 1e-3), "us_per_step": st["last_run_ms"] * 1e3 / sim_steps,
             "launches_us": [(k, round(v * 1e3, 3)) for k, v in prof],
+            "delivery": "events" if event_path else "pull",
             "deliver_us_per_step": dms * 1e3, "deliver_alg_bytes": alg,
             "deliver_gbs": alg / (dms * 1e-3) / 1e9 if dms > 0 else None,
             "hbm_peak_gbs": peak, "peak_source": peak_src}
@@ -919,6 +928,7 @@ def main():
         # synapses workload, reported beside the headline
         if not args.no_synapses:
             side["synapses"] = guarded(synapses_case, args.seed)
+            side["synapses_262k"] = guarded(synapses_case, args.seed, 262144)
 
     if rank == 0:
         config = bench_config(args, n, int(len(inp["exc"][1]) + len(inp["inh"][1])), per, world)

@@ -75,6 +75,7 @@ ENGINE_ONLY = {
                         _vp, _i32, ct.c_int, _P(_i32)],
     "net_persistent_threads": [_vp, _P(_i32)],
     "net_set_spin_limit": [_vp, _i64],
+    "net_set_synapse_events": [_vp, ct.c_int],
     "import_device_ptr": [_vp, _vp, _i64, ct.c_int, _P(_i32)],
     "group_use_buffer": [_vp, _i32, _i32],
     "group_padded_size": [_vp, _i32, _P(_i64)],
@@ -192,7 +193,7 @@ class Runtime(object):
     """One network handle on a function table."""
 
     def __init__(self, table=None, device=0, precision=64, deterministic=True, dt=1e-4, persistent=True,
-                 spin_limit=None, check_finite=False):
+                 spin_limit=None, check_finite=False, synapse_events=None):
         self.t = table if table is not None else product_table()
         self.h = ct.c_void_p()
         self.precision = precision
@@ -204,6 +205,8 @@ class Runtime(object):
             self.t.check(self.t.net_set_spin_limit(self.h, int(spin_limit)), "net_set_spin_limit")
         if check_finite and hasattr(self.t, "net_set_check_finite"):
             self.t.check(self.t.net_set_check_finite(self.h, 1), "net_set_check_finite")
+        if synapse_events and hasattr(self.t, "net_set_synapse_events"):
+            self.t.check(self.t.net_set_synapse_events(self.h, 1), "net_set_synapse_events")
 
     def import_device_ptr(self, ptr, nbytes, precision):
         bid = _i32()

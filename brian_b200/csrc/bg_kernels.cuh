@@ -1053,11 +1053,16 @@ struct SynArgs {
     int nops, nslots;
     int slot_of[kSynMaxOps], sub[kSynMaxOps], slot_var[kSynMaxOps];
     double *S; int64_t npad;
+    const int *use_pull;            // event path present: [step parity] 1 = the pull delivers this step
     int last;
 };
 static __global__ void __launch_bounds__(kSynThreads) k_syn_deliver(const SynArgs a) {
     __shared__ uint32_t mask[kSynChunk / 32];
     const long long nstep = a.ctl->nstep;
+    if (a.use_pull && a.use_pull[nstep & 1] == 0) {   // the event bins deliver this step
+        bg_finish_step(a.ctl, a.last);
+        return;
+    }
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     constexpr int kWarps = kSynThreads / 32;
     const int64_t ntiles = (a.tn + kSynTile - 1) / kSynTile;
@@ -1137,6 +1142,190 @@ static __global__ void __launch_bounds__(kSynThreads) k_syn_deliver(const SynArg
             for (int s = 0; s < kSynMaxOps; ++s)
                 if (s < a.nslots) a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] = x[s];
         }
+    }
+    bg_finish_step(a.ctl, a.last);
+}
+
+// Event-driven Synapses delivery.  The events of step t are the synapses of
+// delay d of the sources that spiked at step t - d.  k_syn_gather walks the
+// spike-history words of those steps and appends each event to the bin of
+// its target's block of kSynBin targets, with a 64-bit key that sorts into
+// the queue order of the pull above: target, then delay descending, then
+// source, then the synapse's rank among the source's synapses of that delay
+// (synapse index order).  k_syn_bins gives each bin a block that sorts its
+// events by key in shared memory and applies every target's events in that
+// order -- the same additions in the same order as the pull, so the result
+// is bit for bit the same.  A step whose events overflow a bin (or whose
+// keys do not fit) is delivered by the pull's test instead, by the same
+// blocks (use_pull), so the path is exact whatever the activity.
+constexpr int kSynBin = 1024;          // targets per bin (one block)
+constexpr int kSynBinCap = 8192;       // events per bin and step
+struct SynEvArgs {
+    DevCtl *ctl;
+    const uint32_t *hist; int depth; int64_t nwords;
+    int64_t so, sn, tn; int dmax;
+    const int64_t *srcptr; const uint8_t *sd; const int32_t *stgt; const int32_t *sq;   // rows by source, (delay, synapse)
+    const int32_t *doff;            // [sn][dmax + 2]: start of each delay within a source's row (or null)
+    const int64_t *colptr; const uint32_t *word;                                         // the pull's columns
+    int *bin_cnt; unsigned long long *bin_key; int32_t *bin_q; int nbins;
+    int *use_pull;                  // [2] by step parity
+    const double *term; int64_t nsyn;
+    int nops, nslots;
+    int slot_of[kSynMaxOps], sub[kSynMaxOps], slot_var[kSynMaxOps];
+    double *S; int64_t npad; int64_t to;
+    int last;
+};
+
+static __global__ void __launch_bounds__(256) k_syn_gather(const SynEvArgs a) {
+    const long long nstep = a.ctl->nstep;
+    const int64_t w0 = a.so >> 5, w1 = (a.so + a.sn + 31) >> 5, nw = w1 - w0;
+    const int64_t total = nw * (int64_t)(a.dmax + 1);
+    const int row0 = (int)(nstep % a.depth);
+    int *flag = a.use_pull + (nstep & 1);
+    for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < total; x += (int64_t)gridDim.x * blockDim.x) {
+        const int d = (int)(x / nw);
+        const int64_t wi = w0 + (x - (int64_t)d * nw);
+        if (nstep < d) continue;
+        int row = row0 - d;
+        row += row < 0 ? a.depth : 0;
+        uint32_t word = masked_word(a.hist + (int64_t)row * a.nwords, wi, a.so, a.so + a.sn);
+        while (word) {
+            const int b = __ffs(word) - 1; word &= word - 1;
+            const int64_t i = (wi << 5) + b - a.so;
+            // the synapses of source i with delay d: a range of its row
+            int64_t r0, r1;
+            const int64_t lo = a.srcptr[i];
+            if (a.doff) {
+                const int32_t *o = a.doff + i * (int64_t)(a.dmax + 2) + d;
+                r0 = lo + o[0];
+                r1 = lo + o[1];
+            } else {
+                const int64_t hi = a.srcptr[i + 1];
+                int64_t l = lo, h = hi;
+                while (l < h) { const int64_t m = (l + h) >> 1; if (a.sd[m] < d) l = m + 1; else h = m; }
+                r0 = l;
+                h = hi;
+                while (l < h) { const int64_t m = (l + h) >> 1; if (a.sd[m] <= d) l = m + 1; else h = m; }
+                r1 = l;
+            }
+            if (r1 - r0 > 256) { atomicExch(flag, 1); continue; }
+            for (int64_t p = r0; p < r1; ++p) {
+                const int64_t j = a.stgt[p];
+                const int bin = (int)(j / kSynBin);
+                const int slot = atomicAdd(a.bin_cnt + bin, 1);
+                if (slot >= kSynBinCap) { atomicExch(flag, 1); continue; }
+                const int64_t e = (int64_t)bin * kSynBinCap + slot;
+                a.bin_key[e] = ((unsigned long long)j << 40) | ((unsigned long long)(255 - d) << 32) |
+                               ((unsigned long long)i << 8) | (unsigned long long)(p - r0);
+                a.bin_q[e] = a.sq[p];
+            }
+        }
+    }
+    bg_finish_step(a.ctl, a.last);
+}
+
+constexpr int kSynBinThreads = 1024;
+static __global__ void __launch_bounds__(kSynBinThreads) k_syn_bins(const SynEvArgs a) {
+    extern __shared__ unsigned char syn_smem[];
+    unsigned long long *key = reinterpret_cast<unsigned long long *>(syn_smem);
+    int32_t *qv = reinterpret_cast<int32_t *>(key + kSynBinCap);
+    const long long nstep = a.ctl->nstep;
+    const int bin = blockIdx.x, tid = threadIdx.x;
+    const int n = min(a.bin_cnt[bin], kSynBinCap);
+    const bool pull = a.use_pull[nstep & 1] != 0;
+    __syncthreads();   // every thread has read the bin's count before thread 0 clears it
+    if (pull) {
+        // a step whose events overflowed: every target of the bin walks its
+        // incoming synapses in queue order and applies those whose source
+        // spiked d steps ago (the pull's test, one target per thread)
+        const int64_t j = (int64_t)bin * kSynBin + tid;
+        if (j < a.tn) {
+            const int row0 = (int)(nstep % a.depth);
+            double x[kSynMaxOps];
+            bool any = false;
+#pragma unroll
+            for (int s = 0; s < kSynMaxOps; ++s)
+                x[s] = s < a.nslots ? a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] : 0.0;
+            for (int64_t q = a.colptr[j]; q < a.colptr[j + 1]; ++q) {
+                const uint32_t wd = a.word[q];
+                const int lag = (int)(wd >> 24) - 1;
+                if (lag < 0 || nstep < lag) continue;
+                const int64_t src = a.so + (int64_t)(wd & 0xFFFFFFu);
+                int row = row0 - lag;
+                row += row < 0 ? a.depth : 0;
+                if (!((a.hist[(int64_t)row * a.nwords + (src >> 5)] >> (src & 31)) & 1u)) continue;
+                any = true;
+#pragma unroll
+                for (int k = 0; k < kSynMaxOps; ++k) {
+                    if (k >= a.nops) break;
+                    const double t = a.term[(int64_t)k * a.nsyn + q];
+#pragma unroll
+                    for (int s = 0; s < kSynMaxOps; ++s)
+                        if (s == a.slot_of[k]) x[s] = a.sub[k] ? __dsub_rn(x[s], t) : __dadd_rn(x[s], t);
+                }
+            }
+            if (any) {
+#pragma unroll
+                for (int s = 0; s < kSynMaxOps; ++s)
+                    if (s < a.nslots) a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] = x[s];
+            }
+        }
+    } else if (n > 0) {
+        int m = 1;
+        while (m < n) m <<= 1;
+        for (int e = tid; e < m; e += kSynBinThreads) {
+            if (e < n) { key[e] = a.bin_key[(int64_t)bin * kSynBinCap + e]; qv[e] = a.bin_q[(int64_t)bin * kSynBinCap + e]; }
+            else { key[e] = ~0ull; qv[e] = 0; }
+        }
+        __syncthreads();
+        // bitonic sort of (key, q) by key (keys are distinct)
+        for (int k = 2; k <= m; k <<= 1) {
+            for (int jj = k >> 1; jj > 0; jj >>= 1) {
+                for (int e = tid; e < m; e += kSynBinThreads) {
+                    const int o = e ^ jj;
+                    if (o > e) {
+                        const bool up = (e & k) == 0;
+                        const unsigned long long ka = key[e], kb = key[o];
+                        if ((ka > kb) == up) {
+                            key[e] = kb; key[o] = ka;
+                            const int32_t t = qv[e]; qv[e] = qv[o]; qv[o] = t;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        // each target of the bin: its events, in key order
+        const int64_t j = (int64_t)bin * kSynBin + tid;
+        if (j < a.tn) {
+            const unsigned long long want = (unsigned long long)j;
+            int l = 0, h = n;
+            while (l < h) { const int mm = (l + h) >> 1; if ((key[mm] >> 40) < want) l = mm + 1; else h = mm; }
+            if (l < n && (key[l] >> 40) == want) {
+                double x[kSynMaxOps];
+#pragma unroll
+                for (int s = 0; s < kSynMaxOps; ++s)
+                    x[s] = s < a.nslots ? a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] : 0.0;
+                for (int e = l; e < n && (key[e] >> 40) == want; ++e) {
+                    const int64_t q = qv[e];
+#pragma unroll
+                    for (int k = 0; k < kSynMaxOps; ++k) {
+                        if (k >= a.nops) break;
+                        const double t = a.term[(int64_t)k * a.nsyn + q];
+#pragma unroll
+                        for (int s = 0; s < kSynMaxOps; ++s)
+                            if (s == a.slot_of[k]) x[s] = a.sub[k] ? __dsub_rn(x[s], t) : __dadd_rn(x[s], t);
+                    }
+                }
+#pragma unroll
+                for (int s = 0; s < kSynMaxOps; ++s)
+                    if (s < a.nslots) a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] = x[s];
+            }
+        }
+    }
+    if (tid == 0) {
+        a.bin_cnt[bin] = 0;                             // empty for the next step
+        if (bin == 0) a.use_pull[(nstep + 1) & 1] = 0;  // next step's flag (nobody reads it this step)
     }
     bg_finish_step(a.ctl, a.last);
 }

@@ -134,6 +134,14 @@ struct HSyn {
     std::vector<int32_t> op_var, op_sub;
     std::vector<int64_t> colptr, perm; std::vector<uint32_t> word; std::vector<double> terms;   // terms: [nops][nsyn], synapse order
     int64_t *dColptr = nullptr; uint32_t *dWord = nullptr; double *dTerm = nullptr;
+    // event path (rows by source): per source, its synapses by (delay, synapse
+    // index) with their target and column position; event bins and flags
+    bool events = false;
+    std::vector<int64_t> srcptr; std::vector<uint8_t> sd; std::vector<int32_t> stgt, sq;
+    int64_t *dSrcPtr = nullptr; uint8_t *dSd = nullptr; int32_t *dStgt = nullptr, *dSq = nullptr;
+    int *dBinCnt = nullptr; unsigned long long *dBinKey = nullptr; int32_t *dBinQ = nullptr; int *dUsePull = nullptr;
+    int32_t *dDoff = nullptr;           // per source, start of each delay in its row (when it fits 256 MB)
+    int nbins = 0;
 };
 struct HSpikeMon {
     int gid; int64_t origin, n; int delay;
@@ -184,6 +192,7 @@ struct bg_net {
     int hold_block = -1;                // test hook: a persistent block that never arrives
     int check_finite = 0;               // check the states for NaN/inf after every run
     bool failed = false;                // a device error stopped the network
+    int syn_events_forced = 0;          // Synapses: event path whatever the size (tests)
     std::vector<void *> allocs;
     struct Import { void *ptr; int64_t bytes; int dtype; };
     std::vector<Import> imports;        // borrowed device buffers (the caller owns and frees them)
@@ -538,6 +547,38 @@ int build_syn(bg_net *net, int yi) {
     a.S = (double *)gt.dS; a.npad = gt.npad;
     const int64_t ntiles = (y.tn + bg::kSynTile - 1) / bg::kSynTile;
     const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)sm_count() * 8));
+    if (y.events) {
+        // event path: gather, then the bins (which fall back to the pull's
+        // test for a step whose events overflowed)
+        bg::SynEvArgs e;
+        std::memset(&e, 0, sizeof(e));
+        e.ctl = net->dCtl; e.hist = gs.dHist; e.depth = gs.depth; e.nwords = gs.npad / 32;
+        e.so = y.so; e.sn = y.sn; e.tn = y.tn; e.dmax = y.dmax;
+        e.srcptr = y.dSrcPtr; e.sd = y.dSd; e.stgt = y.dStgt; e.sq = y.dSq; e.doff = y.dDoff;
+        e.colptr = y.dColptr; e.word = y.dWord;
+        e.bin_cnt = y.dBinCnt; e.bin_key = y.dBinKey; e.bin_q = y.dBinQ; e.nbins = y.nbins; e.use_pull = y.dUsePull;
+        e.term = y.dTerm; e.nsyn = y.nsyn; e.nops = a.nops; e.nslots = a.nslots;
+        for (int k = 0; k < bg::kSynMaxOps; ++k) { e.slot_of[k] = a.slot_of[k]; e.sub[k] = a.sub[k]; e.slot_var[k] = a.slot_var[k]; }
+        e.S = a.S; e.npad = a.npad; e.to = y.to;
+        a.use_pull = y.dUsePull;
+        const int64_t nw = (y.so + y.sn + 31) / 32 - y.so / 32;
+        const int64_t ggrid = std::max<int64_t>(1, std::min<int64_t>((nw * (y.dmax + 1) + 255) / 256, (int64_t)sm_count() * 8));
+        const size_t bsmem = (size_t)bg::kSynBinCap * (8 + 4);
+        cudaFuncSetAttribute(bg::k_syn_bins, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem);
+        net->item_names.push_back("syn_gather[y" + std::to_string(yi) + "]");
+        net->step_launches.push_back([e, ggrid](cudaStream_t st, int, int last) {
+            bg::SynEvArgs b = e; b.last = last;
+            bg::k_syn_gather<<<(unsigned)ggrid, 256, 0, st>>>(b);
+            return cudaGetLastError();
+        });
+        net->item_names.push_back("syn_bins[y" + std::to_string(yi) + "]");
+        net->step_launches.push_back([e, bsmem](cudaStream_t st, int, int last) {
+            bg::SynEvArgs b = e; b.last = last;
+            bg::k_syn_bins<<<(unsigned)b.nbins, bg::kSynBinThreads, bsmem, st>>>(b);
+            return cudaGetLastError();
+        });
+        return BG_OK;
+    }
     net->item_names.push_back("syn_deliver[y" + std::to_string(yi) + "]");
     net->step_launches.push_back([a, grid](cudaStream_t st, int, int last) {
         bg::SynArgs b = a; b.last = last;
@@ -1340,7 +1381,7 @@ int bg_synapses_add(bg_net *n, int32_t src_gid, int64_t src_origin, int64_t src_
     pass(src_n, [&](int64_t k) { return (int64_t)pre[k]; });
     pass(254, [&](int64_t k) { return (int64_t)(253 - delay[k]); });
     pass(tgt_n, [&](int64_t k) { return (int64_t)post[k]; });
-    y.perm.swap(cur);
+    y.perm = cur;
     y.colptr.assign(tgt_n + 1, 0);
     for (int64_t k = 0; k < nsyn; ++k) y.colptr[post[k] + 1]++;
     for (int64_t j = 0; j < tgt_n; ++j) y.colptr[j + 1] += y.colptr[j];
@@ -1350,6 +1391,25 @@ int bg_synapses_add(bg_net *n, int32_t src_gid, int64_t src_origin, int64_t src_
         y.word[p] = (uint32_t)pre[k] | ((uint32_t)(delay[k] + 1) << 24);
     }
     if (nops > 0 && nsyn > 0) y.terms.assign(terms, terms + (size_t)nops * nsyn);
+    // rows by source for the event path: synapses of a source by (delay,
+    // synapse index) -- two stable counting passes -- with their targets and
+    // column positions (the index of their terms)
+    y.events = tgt_n < (int64_t(1) << 24) && nsyn > 0 && nsyn < (int64_t(1) << 31);
+    if (y.events) {
+        std::vector<int64_t> colpos(nsyn);
+        for (int64_t p = 0; p < nsyn; ++p) colpos[y.perm[p]] = p;
+        for (int64_t k = 0; k < nsyn; ++k) cur[k] = k;
+        pass(254, [&](int64_t k) { return (int64_t)delay[k]; });
+        pass(src_n, [&](int64_t k) { return (int64_t)pre[k]; });
+        y.srcptr.assign(src_n + 1, 0);
+        for (int64_t k = 0; k < nsyn; ++k) y.srcptr[pre[k] + 1]++;
+        for (int64_t i = 0; i < src_n; ++i) y.srcptr[i + 1] += y.srcptr[i];
+        y.sd.resize(nsyn); y.stgt.resize(nsyn); y.sq.resize(nsyn);
+        for (int64_t p = 0; p < nsyn; ++p) {
+            const int64_t k = cur[p];
+            y.sd[p] = (uint8_t)delay[k]; y.stgt[p] = post[k]; y.sq[p] = (int32_t)colpos[k];
+        }
+    }
     n->syns.push_back(std::move(y));
     *sid = (int32_t)n->syns.size() - 1;
     return BG_OK;
@@ -1710,6 +1770,45 @@ static int prepare_impl(bg_net *n) {
             return fail(BG_ENOMEM, "synapses");
         int st = upload(n, y.dColptr, y.colptr.data(), (y.tn + 1) * 8); if (st) return st;
         if (y.nsyn) { st = upload(n, y.dWord, y.word.data(), y.nsyn * 4); if (st) return st; }
+        // the event path pays off once the pull's synapse words no longer
+        // stay in L2 (it reads every word every step); below that the pull
+        // is cheaper than the event path's extra launches
+        if (y.events) {
+            int dev = 0, l2 = 0;
+            cudaGetDevice(&dev);
+            if (cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev) != cudaSuccess) l2 = 0;
+            int64_t words = 0;
+            for (const auto &o : n->syns) words += o.nsyn;
+            if (!n->syn_events_forced && words * 4 <= (int64_t)l2 / 2) y.events = false;
+        }
+        if (y.events) {
+            y.nbins = (int)((y.tn + bg::kSynBin - 1) / bg::kSynBin);
+            if (n->alloc(&y.dSrcPtr, (y.sn + 1) * 8) != cudaSuccess || n->alloc(&y.dSd, y.nsyn) != cudaSuccess ||
+                n->alloc(&y.dStgt, y.nsyn * 4) != cudaSuccess || n->alloc(&y.dSq, y.nsyn * 4) != cudaSuccess ||
+                n->alloc(&y.dBinCnt, (size_t)y.nbins * 4) != cudaSuccess ||
+                n->alloc(&y.dBinKey, (size_t)y.nbins * bg::kSynBinCap * 8) != cudaSuccess ||
+                n->alloc(&y.dBinQ, (size_t)y.nbins * bg::kSynBinCap * 4) != cudaSuccess || n->alloc(&y.dUsePull, 8) != cudaSuccess)
+                return fail(BG_ENOMEM, "synapse events");
+            if ((st = upload(n, y.dSrcPtr, y.srcptr.data(), (y.sn + 1) * 8)) || (st = upload(n, y.dSd, y.sd.data(), y.nsyn)) ||
+                (st = upload(n, y.dStgt, y.stgt.data(), y.nsyn * 4)) || (st = upload(n, y.dSq, y.sq.data(), y.nsyn * 4)))
+                return st;
+            BG_CUDA(cudaMemsetAsync(y.dBinCnt, 0, (size_t)y.nbins * 4, n->stream));
+            BG_CUDA(cudaMemsetAsync(y.dUsePull, 0, 8, n->stream));
+            const int64_t dw = y.dmax + 2;
+            if (y.sn * dw * 4 <= ((int64_t)256 << 20)) {
+                std::vector<int32_t> doff((size_t)(y.sn * dw));
+                for (int64_t i = 0; i < y.sn; ++i) {
+                    const int64_t r0 = y.srcptr[i], r1 = y.srcptr[i + 1];
+                    int64_t p = r0;
+                    for (int d = 0; d < dw; ++d) {
+                        while (p < r1 && y.sd[p] < d) ++p;
+                        doff[i * dw + d] = (int32_t)(p - r0);
+                    }
+                }
+                if (n->alloc(&y.dDoff, doff.size() * 4) != cudaSuccess) return fail(BG_ENOMEM, "synapse delay offsets");
+                if ((st = upload(n, y.dDoff, doff.data(), doff.size() * 4))) return st;
+            }
+        }
     }
     for (size_t yi = 0; yi < n->syns.size(); ++yi) {
         int st = bg_synapses_set_terms_impl(n, (int)yi, nullptr); if (st) return st;
@@ -2135,6 +2234,13 @@ int bg_group_use_buffer(bg_net *n, int32_t gid, int32_t buf_id) {
 int bg_group_padded_size(bg_net *n, int32_t gid, int64_t *npad) {
     if (!gid_ok(n, gid) || !npad) return fail(BG_EINVAL, "bg_group_padded_size");
     *npad = n->groups[gid].npad;
+    return BG_OK;
+}
+
+int bg_net_set_synapse_events(bg_net *n, int mode) {
+    if (!n || mode < 0 || mode > 1) return fail(BG_EINVAL, "synapse events: 0 (by size) or 1 (always)");
+    if (n->prepared) return fail(BG_ESTATE, "set before prepare");
+    n->syn_events_forced = mode;
     return BG_OK;
 }
 

@@ -35,7 +35,7 @@ __all__ = ["Network", "MagicNetwork", "run", "reinit", "stop", "clear", "network
            "NetworkOperation", "engine", "set_global_preferences", "get_global_preference"]
 
 _PREFS = {"useweave": False, "precision": 64, "deterministic": True, "device": 0, "persistent": True,
-          "spin_limit": None, "check_finite": False}
+          "spin_limit": None, "check_finite": False, "synapse_events": None}
 _table_override = []
 
 
@@ -46,7 +46,9 @@ def set_global_preferences(**kw):
     512: allow it with that many threads per block), spin_limit (polls of a
     bounded inter-block wait before the run fails with BG_ETIMEOUT; None:
     the engine's default), check_finite (bool: every run ends with a scan of
-    the state variables and a NaN or infinity fails it with BG_ENUMERIC)."""
+    the state variables and a NaN or infinity fails it with BG_ENUMERIC),
+    synapse_events (True: Synapses always take the event path; None: the
+    engine picks it when the synapses exceed half of L2)."""
     _PREFS.update(kw)
 
 
@@ -89,7 +91,8 @@ class _Binding(object):
     def __init__(self, net, table, dt):
         self.rt = Runtime(table, device=_PREFS["device"], precision=_PREFS["precision"],
                           deterministic=_PREFS["deterministic"], dt=dt, persistent=_PREFS["persistent"],
-                          spin_limit=_PREFS["spin_limit"], check_finite=_PREFS["check_finite"])
+                          spin_limit=_PREFS["spin_limit"], check_finite=_PREFS["check_finite"],
+                          synapse_events=_PREFS["synapse_events"])
         self.gids = {}
         self.cids = {}
         self.sids = {}

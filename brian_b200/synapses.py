@@ -290,9 +290,13 @@ class Synapses(EngineBound):
         post_idx = _group_range(self.target if post is None else post, self.target)
         m = len(post_idx)
         ks = np.random.binomial(m, sparseness, size=len(pre_idx)).astype(np.int64)
-        rows = np.repeat(np.arange(len(pre_idx)), ks)
-        # k distinct targets per row: draw with replacement for all rows at
-        # once, then redraw the repeats within a row until none is left
+        # rows holding more than a quarter of the targets take a random
+        # permutation's prefix (redrawing repeats would take ~m log m rounds)
+        dense = ks > m // 4 if m else np.zeros(len(ks), dtype=bool)
+        kd = np.where(dense, 0, ks)
+        rows = np.repeat(np.arange(len(pre_idx)), kd)
+        # k distinct targets per sparse row: draw with replacement for all rows
+        # at once, then redraw the repeats within a row until none is left
         sel = np.random.randint(0, max(m, 1), size=len(rows)).astype(np.int64) if m else np.zeros(0, np.int64)
         while len(sel):
             key = rows * max(m, 1) + sel
@@ -303,6 +307,14 @@ class Synapses(EngineBound):
             if nd == 0:
                 break
             sel[dup] = np.random.randint(0, m, size=nd)
+        if dense.any():
+            parts_r, parts_s = [rows], [sel]
+            for r in np.nonzero(dense)[0]:
+                parts_r.append(np.full(ks[r], r, dtype=np.int64))
+                parts_s.append(np.argsort(np.random.random(m), kind="stable")[:ks[r]].astype(np.int64))
+            rows, sel = np.concatenate(parts_r), np.concatenate(parts_s)
+            order = np.argsort(rows, kind="stable")        # synapses created row by row
+            rows, sel = rows[order], sel[order]
         self._create(pre_idx[rows], post_idx[sel])
 
     def connect_one_to_one(self, pre=None, post=None):

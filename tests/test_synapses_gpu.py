@@ -35,17 +35,26 @@ def test_known_answers_gpu(gpu_table):
     np.testing.assert_array_equal(kat.kat_insertion_order(gpu_table), kat.expected_insertion_order())
 
 
+@pytest.fixture(params=[None, True], ids=["by-size", "events"])
+def delivery(request):
+    """The Synapses delivery the engine picks by size (the pull for these
+    networks), and the event path forced."""
+    b.set_global_preferences(synapse_events=request.param)
+    yield request.param
+    b.set_global_preferences(synapse_events=None)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("kw", [dict(), dict(runs=2), dict(two_statements=False, multi=False),
                                 dict(N=6000, p=0.01, steps=1500)])
-def test_synapses_bit_exact(oracle_table, gpu_table, kw):
+def test_synapses_bit_exact(oracle_table, gpu_table, kw, delivery):
     ref, gpu = _both(scenarios.synapses_cuba, oracle_table, **kw)
     assert len(ref["spk0.idx"]) > 100
     scenarios.compare(ref, gpu)
 
 
 @pytest.mark.gpu
-def test_synapse_weights_changed_between_runs(oracle_table, gpu_table):
+def test_synapse_weights_changed_between_runs(oracle_table, gpu_table, delivery):
     def fn():
         from brian_b200 import ms, mV
         G = b.NeuronGroup(300, model="dv/dt = -v/(10*ms) : volt", threshold=-50 * mV, reset=-60 * mV)
@@ -63,4 +72,30 @@ def test_synapse_weights_changed_between_runs(oracle_table, gpu_table):
         return scenarios._result(net, groups=[G], spikemons=[M], statemons=[St])
     ref, gpu = _both(fn, oracle_table)
     assert len(ref["spk0.idx"]) > 10
+    scenarios.compare(ref, gpu)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rate,sparseness,delay", [(200.0, 0.6, "rand() * 2*ms"), (40.0, 1.0, "1*ms")])
+def test_synapses_event_bins_and_pull_fallback(oracle_table, gpu_table, rate, sparseness, delay, delivery):
+    """Dense, busy synapses: some steps bring more events to a block of
+    targets than its bin holds (and, with one delay for all synapses, every
+    source has more than 256 synapses of one delay), so those steps are
+    delivered by the pull and the others by the event bins -- equal to the
+    oracle bit for bit either way."""
+    def fn():
+        from brian_b200 import ms, mV
+        G = b.NeuronGroup(1200, model="dv/dt = -v/(10*ms) : volt", threshold=5 * mV, reset=0 * mV)
+        src = b.PoissonGroup(400, rates=rate, seed=5)
+        S = b.Synapses(src, G, model="w : volt", pre="v += w")
+        S.connect_random(sparseness=sparseness)
+        S.w = "0.01*mV * (1 + (i % 7))"
+        S.delay = delay
+        M = b.SpikeMonitor(G)
+        St = b.StateMonitor(G, "v", record=[0, 700, 1199])
+        net = b.Network(src, G, S, M, St)
+        net.run(60 * ms)
+        return scenarios._result(net, groups=[G], spikemons=[M], statemons=[St])
+    ref, gpu = _both(fn, oracle_table)
+    assert len(ref["spk0.idx"]) > 100
     scenarios.compare(ref, gpu)
