@@ -325,6 +325,39 @@ def fitting_bench(args):
                      "longest_simulation_steps": st["max_steps"], "blocks_per_sm": int(bps),
                      "autotune_ms": [round(float(x), 3) for x in tune_ms]}
     prob.handle.close()
+    # the latency floor of an evaluation: the longest simulation's dependent
+    # chain of steps, timed alone (one warp of candidates on one 20 s input)
+    w1 = FitWorkload(ntargets=1, dur_min=20.0, dur_max=20.0, seed=args.seed + 2)
+    w1.build_targets()
+    p1 = FittingProblem(eqs, THRESHOLD, RESET, w1.targets, w1.inputs, DT, 32, precision="float",
+                        param_names=list(PARAMS))
+    X1 = np.array([np.exp(np.log(lo) + (np.log(hi) - np.log(lo)) * rng.random(p1.N))
+                   for lo, hi in (PRIOR[k] for k in PARAMS)])
+    fl = []
+    for _ in range(3):
+        p1.evaluate(X1)
+        fl.append(p1.handle.stats()["last_eval_ms"])
+    st1 = p1.handle.stats()
+    p1.handle.close()
+    floor_ms = float(np.median(fl)) * st["max_steps"] / max(1, st1["max_steps"])
+    # FP32 work per neuron-step of the adaptive LIF's Euler step (R*I - V,
+    # / tau (a multiply by the reciprocal), * dt, + V; Vt0 - Vt, / tau_t,
+    # * dt, + Vt; the threshold compare): about 10 operations, against the
+    # CUDA cores' FP32 peak (148 SMs x 128 lanes x 2 x the max SM clock)
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            mhz = float(json.load(f)["sm_max_mhz"])
+    except Exception:
+        mhz = 1965.0
+    import torch
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    fp32_peak = sms * 128 * 2 * mhz * 1e6
+    ops = 10.0
+    out["kernel"].update({"chain_floor_ms": floor_ms, "chain_floor_frac": floor_ms / float(np.median(evals)),
+                          "fp32_ops_per_neuron_step": ops,
+                          "fp32_tflops": st["neuron_steps"] * ops / (np.median(evals) * 1e-3) / 1e12,
+                          "fp32_peak_tflops": fp32_peak / 1e12,
+                          "fp32_frac": st["neuron_steps"] * ops / (np.median(evals) * 1e-3) / fp32_peak})
     # ---- the CPU restatement (numpy, one core) on a bounded sample of the
     # same simulations: 256 candidates of the first target, 2000 steps
     if not args.no_cpu:
@@ -395,6 +428,18 @@ def fitting_bench(args):
     out["speedup_t90"] = ratio(res["plain"]["t90_ms"], l90)
     out["speedup_t50"] = ratio(res["plain"]["t50_ms"], l50)
     out["speedup_t90_vs_plain_256"] = ratio(res["plain_256"]["t90_ms"], l90)
+    # the network's host-side time counted too (features and sampling as the
+    # wall clock saw them, not only their device time)
+    lw = l90 - res["learned"]["network_ms"] + res["learned"]["network_wall_ms"] if np.isfinite(l90) else float("nan")
+    out["speedup_t90_network_wall"] = ratio(res["plain"]["t90_ms"], lw)
+    # the one-off cost of the learned proposal: simulating the training pairs
+    # and training the network; counted into one fit, and the number of fits
+    # after which it has paid for itself
+    one_off = train_ms + sim_s * 1e3
+    out["one_off_ms"] = one_off
+    out["speedup_t90_incl_training"] = ratio(res["plain"]["t90_ms"], l90 + one_off) if np.isfinite(l90) else None
+    saved = res["plain"]["t90_ms"] - l90
+    out["break_even_fits"] = (one_off / saved) if (np.isfinite(saved) and saved > 0) else None
     return out
 
 
