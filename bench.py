@@ -599,6 +599,46 @@ def synapses_case(seed, n=32768, indegree=160, sim_steps=2000, profile_steps=300
 from brian_b200.statistics import precision_agreement as precision_report  # noqa: E402
 
 
+def _oracle_c1_replica(args):
+    """One CUBA-4000 run (1 s) on the single-threaded oracle in a worker
+    process; returns (events, start, end) timed after a common barrier."""
+    seed, barrier = args
+    sys.path.insert(0, ROOT)
+    import oracle
+    import brian_b200 as b
+    from brian_b200 import workloads
+    from brian_b200.network import engine
+    b.clear()
+    b.reinit_default_clock()
+    with engine(oracle.table()):
+        net, P, M, S = workloads.cuba4000(seed=seed)
+        net.prepare()
+        barrier.wait()
+        t0 = time.time()
+        net.run(10000 * DT)
+        t1 = time.time()
+        ev = int(net._binding.rt.counters(1, 2)[1].sum())
+    net._invalidate()
+    return ev, t0, t1
+
+
+def oracle_all_cores_c1(seed, procs):
+    """`procs` independent CUBA-4000 replicas on the oracle at once, one per
+    host core (spawned processes): total events / wall from the first start
+    to the last end."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as man:
+        bar = man.Barrier(procs)
+        with ctx.Pool(procs) as pool:
+            res = pool.map(_oracle_c1_replica, [(seed + k, bar) for k in range(procs)])
+    ev = sum(r[0] for r in res)
+    wall = max(r[2] for r in res) - min(r[1] for r in res)
+    return {"value": ev / wall, "unit": "events/s", "cores": procs, "kind": "port",
+            "sample": "%d independent CUBA-4000 replicas (1 s simulated each, seeds %d..%d) on the single-threaded "
+                      "C++ oracle, one per host core, %.1f s wall" % (procs, seed, seed + procs - 1, wall)}
+
+
 def cuba4000_bench(args):
     """The plain CUBA network (4000 LIF, p = 0.02, zero delay, FP64, 1 s,
     SpikeMonitor and the v trace of 10 neurons) on the GPU: device time per
@@ -648,6 +688,10 @@ def cuba4000_bench(args):
         out["cpu_baseline"] = {"value": ev / wall, "unit": "events/s", "cores": 1, "kind": "port",
                                "sample": "the whole run (1 s simulated) on the single-threaded C++ oracle"}
         out["spikes_equal_oracle"] = bool(same)
+        try:
+            out["cpu_all_cores"] = oracle_all_cores_c1(args.seed, max(1, os.cpu_count() or 1))
+        except Exception as e:
+            out["cpu_all_cores"] = {"error": "%s: %s" % (type(e).__name__, e)}
     return out
 
 
