@@ -665,7 +665,9 @@ def cuba4000_bench(args):
         if prec == 64:
             out.update({"device_ms": st["last_run_ms"], "us_per_step": st["last_run_ms"] * 1e3 / steps,
                         "events": ev, "events_per_s": ev / (st["last_run_ms"] * 1e-3),
-                        "spikes": int(len(recs[64][0][1])), "launches": int(st["launches"])})
+                        "spikes": int(len(recs[64][0][1])), "launches": int(st["launches"]),
+                        "path": "persistent kernel (%d threads/block)" % st["persistent_threads"]
+                        if st.get("persistent_threads") else "stepped launches"})
         else:
             out["fp32_us_per_step"] = st["last_run_ms"] * 1e3 / steps
         net._invalidate()

@@ -100,9 +100,10 @@ __global__ void k_indegree(const int32_t *cols, int64_t n, int32_t *deg) {
         atomicAdd(deg + cols[i], 1);
 }
 // persistent push words: target | delay << 24
+// (d null: every delay is zero)
 __global__ void k_pack_synapses(const int32_t *cols, const uint8_t *d, int64_t n, uint32_t *out) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        out[i] = (uint32_t)cols[i] | ((uint32_t)d[i] << 24);
+        out[i] = (uint32_t)cols[i] | ((uint32_t)(d ? d[i] : 0) << 24);
 }
 
 struct HConn {
@@ -115,6 +116,10 @@ struct HConn {
     uint16_t *dCRing = nullptr; int64_t tnp = 0; void *dTable = nullptr; int tablen = 0;   // count ring (shared weight)
     int64_t *dRow = nullptr; int32_t *dCols = nullptr; void *dW = nullptr; uint8_t *dD = nullptr; void *dRing = nullptr;
     uint32_t *dPacked = nullptr;       // persistent path: target | delay << 24 (count rings, targets < 2^24)
+    // persistent path, zero-delay Connection: its own count ring of dir_md
+    // rows and the table {0, w} (not part of the saved state: every launch
+    // ends with the ring delivered)
+    uint16_t *dDirRing = nullptr; void *dDirTable = nullptr; int dir_md = 0;
     int64_t *dColptr = nullptr, *dColk = nullptr; int32_t *dColsrc = nullptr;
     int64_t wcount() const { return dense ? sn * tn : nnz; }
 };
@@ -152,6 +157,7 @@ struct HStateMon {
     int gid; int var; std::vector<int32_t> idx; int timestep; long long start = 0;
     std::vector<int32_t> sorted, pos, blk_lo;
     int32_t *dIdx = nullptr, *dPos = nullptr, *dBlk = nullptr; void *dBuf = nullptr; long long *dRowBase = nullptr;
+    int32_t *dBlkP = nullptr;          // blk_lo for the persistent kernel's blocks
     int64_t cap_rows = 0; long long rows_done = 0;
     std::vector<double> vals; std::vector<int64_t> steps;
 };
@@ -853,31 +859,60 @@ int persist_threads(int64_t n, int nvar, int forced) {
 
 // The persistent path applies to one linear group (at most 4 variables, no
 // refractoriness, no Poisson/generator input) whose every connection is a
-// shared-weight DelayConnection from the group onto itself, with no monitors
-// and no plasticity -- the CUBA benchmark topology.
+// shared-weight DelayConnection or zero-delay Connection from the group onto
+// itself, with undelayed spike monitors, StateMonitors and no plasticity --
+// the CUBA benchmark topology.
 // Steps per persistent launch when spike monitors record: the spike words of
 // a launch are converted to records after it (32 KB per step at 262144
 // neurons), in step ranges that fit each monitor's record buffer.
 constexpr int64_t kPersistMonSteps = bg::kMonWordsThreads;
 
+// Largest in-degree of a connection, counted on the device from its uploaded columns.
+int max_indegree(bg_net *n, const HConn &c, int64_t *kmax) {
+    *kmax = 0;
+    if (c.nnz <= 0) return BG_OK;
+    int32_t *dDeg = nullptr;
+    BG_CUDA(cudaMalloc(&dDeg, c.tn * 4));
+    std::vector<int32_t> indeg(c.tn);
+    cudaError_t e = cudaMemsetAsync(dDeg, 0, c.tn * 4, n->stream);
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((c.nnz + 255) / 256, (int64_t)sm_count() * 8));
+    if (e == cudaSuccess) { k_indegree<<<grid, 256, 0, n->stream>>>(c.dCols, c.nnz, dDeg); e = cudaGetLastError(); }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(indeg.data(), dDeg, c.tn * 4, cudaMemcpyDeviceToHost, n->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(n->stream);
+    cudaFree(dDeg);
+    if (e != cudaSuccess) return fail(BG_ECUDA, std::string("in-degree: ") + cudaGetErrorString(e));
+    for (int32_t k : indeg) *kmax = std::max<int64_t>(*kmax, k);
+    return BG_OK;
+}
+
+// A zero-delay Connection of the group onto itself with one shared weight
+// and nothing else on it: the persistent kernel counts its events per target
+// in a ring and adds the weight once per event at delivery.
+bool persist_direct(const HConn &c) {
+    return !c.hetero && !c.dense && c.delay == 0 && c.mod_var < 0 && c.stdp < 0 && c.homogeneous && c.src == 0 &&
+           c.tgt == 0 && c.tn <= (1 << 24);
+}
+
 template <typename T>
 int build_persist(bg_net *net) {
     net->persist = nullptr;
-    if (net->groups.size() != 1 || !net->stmons.empty() || !net->stdps.empty() || !net->syns.empty()) return BG_OK;
+    if (net->groups.size() != 1 || !net->stdps.empty() || !net->syns.empty()) return BG_OK;
     for (const HSpikeMon &m : net->smons)
         if (m.gid != 0 || m.delay != 0) return BG_OK;
+    if ((int)net->stmons.size() > bg::kMaxRec) return BG_OK;
 
     const HGroup &g = net->groups[0];
     if (!g.linear || g.nvar < 1 || g.nvar > 4 || g.refr || g.period > 0) return BG_OK;
     if (g.generated() || g.emp_steps > 0) return BG_OK;
     if (g.thr_kind != BG_THR_CONST && g.thr_kind != BG_THR_VAR && g.thr_kind != BG_THR_NONE) return BG_OK;
     if (net->conns.empty() || (int)net->conns.size() > bg::kPersistMaxPush) return BG_OK;
-    if ((int)g.delivs.size() > bg::kPersistMaxDeliv) return BG_OK;
-    int min_d = 255;
+    int min_d = 255, ndirect = 0;
     for (const HConn &c : net->conns) {
+        if (persist_direct(c)) { ++ndirect; min_d = 0; continue; }
         if (!c.fused_push || c.src != 0 || c.tgt != 0) return BG_OK;
         for (uint8_t d : c.d) min_d = std::min<int>(min_d, d);
     }
+    if (ndirect + (int)g.delivs.size() > bg::kPersistMaxDeliv) return BG_OK;
     {
         int dev = 0, coop = 0;
         if (cudaGetDevice(&dev) != cudaSuccess) return BG_OK;
@@ -909,23 +944,56 @@ int build_persist(bg_net *net) {
     a.thr_kind = g.thr_kind; a.thr_var = g.thr_var; a.thr_var2 = g.thr_var2; a.thr_val = (T)g.thr_val;
     a.reset_kind = g.reset_kind; a.reset_var = g.reset_var; a.reset_var2 = g.reset_var2; a.reset_val = (T)g.reset_val;
     a.hist = g.dHist; a.depth = g.depth; a.nwords = g.npad / 32;
-    a.ndeliv = (int)g.delivs.size();
-    for (int k = 0; k < a.ndeliv; ++k) {
+    // zero-delay Connections: a count ring of 3 rows (a push of step t lands
+    // in row t mod 3, delivered at the top of step t+1; blocks are at most
+    // one step apart) and the table {0, w}
+    for (HConn &c : net->conns) {
+        if (!persist_direct(c) || c.dDirRing) continue;
+        int64_t kmax = 0;
+        int st = max_indegree(net, c, &kmax);
+        if (st) return st;
+        if (kmax >= 65535) return BG_OK;                     // 16-bit counts
+        c.dir_md = 3;
+        c.tnp = (c.tn + 1) & ~1ll;
+        if (net->alloc(&c.dDirRing, (size_t)c.dir_md * c.tnp * 2) != cudaSuccess ||
+            net->alloc(&c.dDirTable, 2 * sizeof(T)) != cudaSuccess)
+            return fail(BG_ENOMEM, "count ring");
+        BG_CUDA(cudaMemsetAsync(c.dDirRing, 0, (size_t)c.dir_md * c.tnp * 2, net->stream));
+        const double w0 = c.w_bits == 64 ? *(const double *)c.w.data() : (double)*(const float *)c.w.data();
+        const T tab[2] = {T(0), (T)w0};
+        st = upload(net, c.dDirTable, tab, sizeof(tab));
+        if (st) return st;
+        BG_CUDA(cudaStreamSynchronize(net->stream));
+    }
+    // deliveries in the order of the stepped path: the zero-delay
+    // Connections (propagated in the step's connection slot), then the
+    // DelayConnections' due rows
+    a.ndeliv = 0;
+    for (const HConn &c : net->conns) {
+        if (!persist_direct(c)) continue;
+        a.direct_mask |= 1u << a.ndeliv;
+        bg::Deliv<T> &dv = a.deliv[a.ndeliv++];
+        dv.ring = nullptr; dv.tn = c.tn; dv.to = c.to; dv.md = c.dir_md; dv.var = c.var;
+        dv.cring = c.dDirRing; dv.tnp = c.tnp; dv.table = (const T *)c.dDirTable; dv.tablen = 2;
+    }
+    for (int k = 0; k < (int)g.delivs.size(); ++k) {
         const HConn &c = net->conns[g.delivs[k]];
-        a.deliv[k].ring = (T *)c.dRing; a.deliv[k].tn = c.tn; a.deliv[k].to = c.to; a.deliv[k].md = c.md; a.deliv[k].var = c.var;
-        a.deliv[k].cring = c.dCRing; a.deliv[k].tnp = c.tnp; a.deliv[k].table = (const T *)c.dTable; a.deliv[k].tablen = c.tablen;
+        bg::Deliv<T> &dv = a.deliv[a.ndeliv++];
+        dv.ring = (T *)c.dRing; dv.tn = c.tn; dv.to = c.to; dv.md = c.md; dv.var = c.var;
+        dv.cring = c.dCRing; dv.tnp = c.tnp; dv.table = (const T *)c.dTable; dv.tablen = c.tablen;
     }
     a.npush = (int)net->conns.size();
     for (int p = 0; p < a.npush; ++p) {
         HConn &c = net->conns[p];
         bg::Push<T> &q = a.push[p];
-        q.ring = (T *)c.dRing; q.md = c.md; q.so = c.so; q.sn = c.sn; q.tn = c.tn;
+        const bool direct = persist_direct(c);
+        q.ring = (T *)c.dRing; q.md = direct ? c.dir_md : c.md; q.so = c.so; q.sn = c.sn; q.tn = c.tn;
         q.rowptr = c.dRow; q.cols = c.dCols; q.w = c.dW; q.w_bits = c.w_bits; q.d = c.dD;
         q.events = net->dCounters + net->groups.size() + p;
-        q.cring = c.dCRing; q.tnp = c.tnp;
+        q.cring = direct ? c.dDirRing : c.dCRing; q.tnp = c.tnp;
         // one word per synapse for the scatter: a single load (and a single
         // stream of cache lines and pages) per synapse instead of two
-        if (c.dCRing && c.tn <= (1 << 24) && c.nnz > 0 && c.dCols && c.dD) {
+        if (q.cring && c.tn <= (1 << 24) && c.nnz > 0 && c.dCols && (c.dD || direct)) {
             if (!c.dPacked) {
                 if (net->alloc(&c.dPacked, c.nnz * 4) != cudaSuccess) return fail(BG_ENOMEM, "packed synapses");
                 const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((c.nnz + 255) / 256, (int64_t)sm_count() * 8));
@@ -940,6 +1008,25 @@ int build_persist(bg_net *net) {
     a.lag = min_d >= 1 ? 2 : 1;
     a.spin_limit = net->spin_limit;
     a.hold_block = net->hold_block;
+    // StateMonitors: the recorded neurons of each persistent block (the
+    // monitor's sorted indices split at multiples of bn)
+    a.nrec = (int)net->stmons.size();
+    for (int k = 0; k < a.nrec; ++k) {
+        HStateMon &m = net->stmons[k];
+        if (!m.dBlkP) {
+            std::vector<int32_t> lo(blocks + 1, 0);
+            const int64_t w = (int64_t)m.sorted.size();
+            for (int64_t b = 0, e = 0; b <= blocks; ++b) {
+                while (e < w && m.sorted[e] < b * bn) ++e;
+                lo[b] = (int32_t)e;
+            }
+            if (net->alloc(&m.dBlkP, (blocks + 1) * 4) != cudaSuccess) return fail(BG_ENOMEM, "state monitor");
+            BG_CUDA(cudaMemcpy(m.dBlkP, lo.data(), (blocks + 1) * 4, cudaMemcpyHostToDevice));
+        }
+        bg::RecDev &r = a.rec[k];
+        r.var = m.var; r.nidx = (int)m.idx.size(); r.idx = m.dIdx; r.pos = m.dPos; r.blk_lo = m.dBlkP;
+        r.buf = m.dBuf; r.row_base = m.dRowBase; r.timestep = m.timestep; r.start = m.start;
+    }
     if (!net->smons.empty()) {
         // spike monitors: the kernel writes each step's spike words; the
         // monitor kernels turn a launch's words into records (one launch per
@@ -1650,20 +1737,7 @@ static int prepare_impl(bg_net *n) {
             // A row entry collects at most one event per synapse, so counts
             // stay below the largest in-degree.
             int64_t kmax = 0;
-            if (c.fused_push && c.homogeneous && c.nnz > 0) {
-                // largest in-degree, counted on the device from the uploaded columns
-                int32_t *dDeg = nullptr;
-                BG_CUDA(cudaMalloc(&dDeg, c.tn * 4));
-                std::vector<int32_t> indeg(c.tn);
-                cudaError_t e = cudaMemsetAsync(dDeg, 0, c.tn * 4, n->stream);
-                const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((c.nnz + 255) / 256, (int64_t)sm_count() * 8));
-                if (e == cudaSuccess) { k_indegree<<<grid, 256, 0, n->stream>>>(c.dCols, c.nnz, dDeg); e = cudaGetLastError(); }
-                if (e == cudaSuccess) e = cudaMemcpyAsync(indeg.data(), dDeg, c.tn * 4, cudaMemcpyDeviceToHost, n->stream);
-                if (e == cudaSuccess) e = cudaStreamSynchronize(n->stream);
-                cudaFree(dDeg);
-                if (e != cudaSuccess) return fail(BG_ECUDA, std::string("in-degree: ") + cudaGetErrorString(e));
-                for (int32_t k : indeg) kmax = std::max<int64_t>(kmax, k);
-            }
+            if (c.fused_push && c.homogeneous && c.nnz > 0) { st = max_indegree(n, c, &kmax); if (st) return st; }
             if (kmax > 0 && kmax < 65535) {
                 c.tablen = (int)kmax + 1;
                 c.tnp = (c.tn + 1) & ~1ll;
@@ -1894,7 +1968,8 @@ static int net_run_steps(bg_net *n, int64_t nsteps, int64_t cs0) {
         BG_CUDA(cudaMemcpyAsync(&n->dCtl->clock_off, &off0, 8, cudaMemcpyHostToDevice, n->stream));
         BG_CUDA(cudaEventRecord(n->ev0, n->stream));
         const bool mons = !n->smons.empty();
-        const int64_t chunk = mons ? kPersistMonSteps : (int64_t)1 << 20;
+        int64_t chunk = mons ? kPersistMonSteps : (int64_t)1 << 20;
+        if (!n->stmons.empty()) chunk = std::min<int64_t>(chunk, n->chunk_steps);   // rows of the monitor buffers
         std::vector<long long> cnt;
         for (int64_t done = 0; done < nsteps;) {
             const int64_t c = std::min(chunk, nsteps - done);
@@ -1934,6 +2009,8 @@ static int net_run_steps(bg_net *n, int64_t nsteps, int64_t cs0) {
                     }
                 }
             }
+            // the launch ran the 'end' slot of its last step
+            if (!n->stmons.empty()) { st = drain(n, cs0 + done, n->nstep - 1, off0); if (st) return st; }
             done += c;
         }
         BG_CUDA(cudaEventRecord(n->ev1, n->stream));

@@ -1,6 +1,7 @@
 // bg_persist.cuh -- one cooperative launch runs many steps of a single
-// linear group whose outgoing connections are DelayConnections on the
-// shared-weight (atomic) path: the CUBA topology of Brian's benchmarks.
+// linear group whose outgoing connections are shared-weight DelayConnections
+// or zero-delay Connections onto itself: the CUBA topology of Brian's
+// benchmarks (CUBA-4000 with its StateMonitor, CUBA-262k with delays).
 //
 // Each block owns TH x NPT neurons for the whole launch and keeps their state
 // in registers; the row pointers of those neurons are staged in shared memory
@@ -43,6 +44,12 @@ template <typename T> struct PersistArgs {
     int64_t mon_stride;         // words per step in mon_words
     unsigned int spin_limit;    // polls of a wait before it gives up (BG_DERR_TIMEOUT)
     int hold_block;             // test hook: this block never publishes its arrivals (-1: none)
+    // zero-delay Connections (connection.py:224-256): bit d set when delivery
+    // d adds the shared weight once per event, sv = sv + w, k times in a row
+    // (the reference's additions), instead of the k-fold sum of a ring entry
+    uint32_t direct_mask;
+    int nrec; RecDev rec[kMaxRec];   // StateMonitors of the group ('end' slot, after the resets);
+                                     // blk_lo holds the ranges of this kernel's blocks
 };
 
 __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int *p) {
@@ -109,6 +116,7 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
     __shared__ int64_t srow1[kPersistMaxPush][kPushBatch];      // first batch, per connection
     __shared__ int32_t spref1[kPersistMaxPush][kPushBatch + 1];
     __shared__ int nsp, abort_flag;
+    __shared__ T stash[BN];                      // StateMonitor values of the block's neurons
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int base = blockIdx.x * BN;               // neuron counts < 2^31
     const int nvalid = (int)min((int64_t)BN, a.n - (int64_t)base);
@@ -229,7 +237,19 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
             for (int d = 0; d < kPersistMaxDeliv; ++d) {
                 if (d >= a.ndeliv) break;
                 const Deliv<T> &dv = a.deliv[d];
-                if (dv.cring) {
+                if (dv.cring && ((a.direct_mask >> d) & 1u)) {
+                    // table[1] = 0 + w = w: one addition of the weight per event
+                    const T w = staged ? stab[toff[d] + 1] : __ldg(dv.table + 1);
+                    on_var<NV>(dv.var, [&](auto K) {
+                        constexpr int k = decltype(K)::value;
+#pragma unroll
+                        for (int u = 0; u < NPT; ++u) {
+                            const int c = cnt[d][u];
+                            if (c) crow[d][u * TH] = 0;
+                            for (int q = 0; q < c; ++q) s[u][k] = rn<T>::add(s[u][k], w);
+                        }
+                    });
+                } else if (dv.cring) {
                     T v[NPT];
 #pragma unroll
                     for (int u = 0; u < NPT; ++u) {
@@ -266,6 +286,20 @@ __global__ void __launch_bounds__(TH, TH <= 512 ? 2 : 1) k_persist(const Persist
 #pragma unroll
                 for (int u = 0; u < NPT; ++u)
                     if ((prev_spk >> u) & 1u) uset<T, NV>(s[u], a.reset_var, uget<T, NV>(s[u], a.reset_var2));
+            }
+            // StateMonitors ('end' slot, after the resets) of the step just
+            // finished: the block's recorded neurons through shared memory
+            for (int r = 0; r < a.nrec; ++r) {
+                const RecDev &m = a.rec[r];
+                const long long rel = (t - 1) - m.start;
+                if (rel < 0 || rel % m.timestep) continue;       // block-uniform
+#pragma unroll
+                for (int u = 0; u < NPT; ++u) stash[u * TH + tid] = uget<T, NV>(s[u], m.var);
+                __syncthreads();
+                const long long row = rel / m.timestep - *m.row_base;
+                const int e0 = m.blk_lo[blockIdx.x], e1 = m.blk_lo[blockIdx.x + 1];
+                for (int e = e0 + tid; e < e1; e += TH) ((T *)m.buf)[row * m.nidx + m.pos[e]] = stash[m.idx[e] - base];
+                __syncthreads();
             }
         }
         if (st == a.nsteps) break;

@@ -32,9 +32,13 @@ def _result(net, groups=(), spikemons=(), statemons=(), conns=(), stdps=()):
     return out
 
 
-def cuba(N=4000, steps=10000, seed=1, p=0.02, record=10, refractory=0.0, runs=1):
+def cuba(N=4000, steps=10000, seed=1, p=0.02, record=10, refractory=0.0, runs=1, timestep=1, persistent=True):
     """Config 1: CUBA-4000, FP64, zero delay (examples/misc/CUBA.py:25-74);
-    `runs` > 1 splits the steps into that many equal run() calls."""
+    `runs` > 1 splits the steps into that many equal run() calls; `record`
+    is the number of leading neurons whose v is recorded, or their list;
+    `timestep` the StateMonitor's recording period in steps.  Without
+    refractoriness the engine runs it in its persistent kernel unless
+    `persistent` is False."""
     taum, taue, taui = 20 * ms, 5 * ms, 10 * ms
     Vt, Vr, El = -50 * mV, -60 * mV, -49 * mV
     eqs = b.Equations("""
@@ -54,12 +58,20 @@ def cuba(N=4000, steps=10000, seed=1, p=0.02, record=10, refractory=0.0, runs=1)
     rng = np.random.Generator(np.random.PCG64(seed + 2))
     P.v = Vr + rng.random(N) * (Vt - Vr)
     M = b.SpikeMonitor(P)
-    S = b.StateMonitor(P, "v", record=list(range(record)))
+    S = b.StateMonitor(P, "v", record=list(range(record)) if np.isscalar(record) else list(record),
+                       timestep=timestep)
     net = b.Network(P, Ce, Ci, M, S)
     assert steps % runs == 0
-    for _ in range(runs):
-        net.run(steps // runs * 0.1 * ms)
-    return _result(net, groups=[P], spikemons=[M], statemons=[S])
+    prev = b.get_global_preference("persistent")
+    b.set_global_preferences(persistent=persistent)
+    try:
+        for _ in range(runs):
+            net.run(steps // runs * 0.1 * ms)
+    finally:
+        b.set_global_preferences(persistent=prev)
+    out = _result(net, groups=[P], spikemons=[M], statemons=[S])
+    out["persistent_threads"] = net.stats().get("persistent_threads", 0)
+    return out
 
 
 def cuba_delay(N=3000, indegree=100, steps=2000, seed=3, wdtype=np.float32, we=0.162e-2, wi=-0.9e-2,

@@ -10,7 +10,7 @@ from brian_b200 import ms, mV
 from brian_b200.connections import fixed_indegree_csr
 
 
-def _net(N=5000, persistent=True):
+def _net(N=5000):
     eqs = b.Equations("dv/dt=(ge+gi-(v-El))/taum : volt\ndge/dt=-ge/taue : volt\ndgi/dt=-gi/taui : volt",
                       taum=20 * ms, taue=5 * ms, taui=10 * ms, El=-49 * mV)
     P = b.NeuronGroup(N, model=eqs, threshold=-50 * mV, reset=-60 * mV)
@@ -24,22 +24,29 @@ def _net(N=5000, persistent=True):
         C.connect_csr(rowptr, cols, w, delay_steps=rng.integers(1, 51, size=len(cols)).astype(np.uint8))
         objs.append(C)
     P.v = -60 * mV + rng.random(N) * 10 * mV
-    if not persistent:
-        # a StateMonitor keeps the network on the per-step launches
-        objs.append(b.StateMonitor(P, "v", record=[0, 1]))
+    objs.append(b.StateMonitor(P, "v", record=[0, 1]))
     return b.Network(*objs), P
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("persistent", [True, False])
 def test_group_state_in_torch_tensor(gpu_table, persistent):
+    prev = b.get_global_preference("persistent")
+    b.set_global_preferences(persistent=persistent)
+    try:
+        _state_in_tensor(persistent)
+    finally:
+        b.set_global_preferences(persistent=prev)
+
+
+def _state_in_tensor(persistent):
     import torch
     N = 5000
     b.clear()
-    ref, Pr = _net(N, persistent)
+    ref, Pr = _net(N)
     ref.run(400 * 0.1 * ms)
     b.clear()
-    net, P = _net(N, persistent)
+    net, P = _net(N)
     buf = torch.zeros((3, P.padded_size()), dtype=torch.float64, device="cuda")
     P.use_device_buffer(buf)
     net.run(400 * 0.1 * ms)

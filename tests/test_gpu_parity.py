@@ -25,16 +25,36 @@ def _both(fn, oracle_table, **kw):
     return out
 
 
+def _pop_threads(*outs):
+    return [o.pop("persistent_threads") for o in outs]
+
+
 @pytest.mark.gpu
 def test_cuba4000_bit_exact(oracle_table, gpu_table):
+    """Zero-delay Connections, a SpikeMonitor and a StateMonitor of v: the
+    persistent kernel (4 blocks of 1024 neurons)."""
     ref, gpu = _both(scenarios.cuba, oracle_table, steps=10000)
+    assert _pop_threads(ref, gpu)[1] == 512
     assert len(ref["spk0.idx"]) > 10000
+    scenarios.compare(ref, gpu)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("persistent", [True, False])
+def test_cuba4000_split_runs_statemonitor_period(oracle_table, gpu_table, persistent):
+    """Three run() calls, recorded neurons in several blocks and out of
+    order, every third step: the persistent and the stepped path."""
+    ref, gpu = _both(scenarios.cuba, oracle_table, steps=2400, runs=3, timestep=3,
+                     record=[3999, 0, 1500, 1024, 2047, 7], persistent=persistent)
+    assert _pop_threads(ref, gpu)[1] == (512 if persistent else 0)
+    assert len(ref["st0.steps"]) == 800
     scenarios.compare(ref, gpu)
 
 
 @pytest.mark.gpu
 def test_cuba4000_refractory_bit_exact(oracle_table, gpu_table):
     ref, gpu = _both(scenarios.cuba, oracle_table, steps=3000, refractory=5 * b.ms)
+    assert _pop_threads(ref, gpu)[1] == 0            # refractoriness: the stepped path
     scenarios.compare(ref, gpu)
 
 
