@@ -116,6 +116,13 @@ ENGINE_ONLY = {
     "fit_pso_best": [_vp, _vp, _vp],
     "fit_pso_state": [_vp, _vp, _vp, _vp, _vp],
     "fit_stats": [_vp, _vp, ct.c_int],
+    "batch_create": [_vp, _i32, _P(_vp)],
+    "batch_free": [_vp],
+    "batch_run": [_vp, _vp, _vp],
+    "batch_set_shape": [_vp, _i32, _i32],
+    "batch_get_shape": [_vp, _P(_i32), _P(_i32), _P(_i32), _P(_i32)],
+    "batch_autotune": [_vp, _i32, _P(_dbl)],
+    "batch_stats": [_vp, _P(_i64), _P(_dbl)],
 }
 
 
@@ -781,3 +788,50 @@ def spike_features(trains_steps, inputs, dt, device=0):
     t.check(t.spike_features(int(device), len(trains_steps), _ptr(steps), _ptr(offs), _ptr(I), _ptr(ioff), len(I),
                              float(dt), _ptr(out)), "spike_features")
     return out
+
+
+class BatchRuntime(object):
+    """One bg_batch handle over the engine handles of several Runtimes."""
+
+    def __init__(self, runtimes):
+        self.t = runtimes[0].t
+        if not hasattr(self.t, "batch_create"):
+            raise EngineError("batches need the CUDA engine")
+        self.runtimes = list(runtimes)            # the handles must outlive the batch
+        hs = (_vp * len(runtimes))(*[r.h.value for r in runtimes])
+        self.h = ct.c_void_p()
+        self.t.check(self.t.batch_create(hs, len(runtimes), ct.byref(self.h)), "batch_create")
+
+    def run(self, nsteps, cs0):
+        nsteps = np.ascontiguousarray(nsteps, dtype=np.int64)
+        cs0 = np.ascontiguousarray(cs0, dtype=np.int64)
+        self.t.check(self.t.batch_run(self.h, _ptr(nsteps), _ptr(cs0)), "batch_run")
+
+    def set_shape(self, shape, lanes):
+        self.t.check(self.t.batch_set_shape(self.h, int(shape), int(lanes)), "batch_set_shape")
+
+    def shape(self):
+        v = [_i32() for _ in range(4)]
+        self.t.check(self.t.batch_get_shape(self.h, *[ct.byref(x) for x in v]), "batch_get_shape")
+        return dict(shape=v[0].value, threads=v[1].value, neurons_per_thread=v[2].value, lanes=v[3].value)
+
+    def autotune(self, steps):
+        ms = _dbl()
+        self.t.check(self.t.batch_autotune(self.h, int(steps), ct.byref(ms)), "batch_autotune")
+        return ms.value
+
+    def stats(self):
+        n, ms = _i64(), _dbl()
+        self.t.check(self.t.batch_stats(self.h, ct.byref(n), ct.byref(ms)), "batch_stats")
+        return {"launches": n.value, "last_run_ms": ms.value}
+
+    def close(self):
+        if self.h:
+            self.t.batch_free(self.h)
+            self.h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -19,6 +19,7 @@
 
 #include "bg_kernels.cuh"
 #include "bg_persist.cuh"
+#include "bg_batch.cuh"
 #include "bg_rtc.h"
 #include "../../include/brian_b200.h"
 
@@ -2435,6 +2436,508 @@ int bg_net_stats(bg_net *n, int64_t *steps, int64_t *launches, double *ms) {
     if (steps) *steps = n->nstep;
     if (launches) *launches = n->launches;
     if (ms) *ms = n->last_ms;
+    return BG_OK;
+}
+
+}  // extern "C"
+
+// ============================================================== batches
+// Independent networks in one launch of bg::k_batch, one block each.  The
+// batch works on the networks' own device state (group state, count rings,
+// counters, control block) and appends the monitor records of every launch
+// to the networks' host-side records, so each network reads and continues
+// as if it had run alone.
+struct bg_batch {
+    std::vector<bg_net *> nets;
+    int device = 0, precision = 64, nvar = 0, max_n = 0;
+    int shape = -1, lanes = 32;
+    size_t smem = 0;                       // dynamic shared memory per block (largest layout)
+    std::vector<int32_t> smem_ring[bg::kBatchMaxConn];   // per network: ring offsets (-1: global)
+    std::vector<int32_t> smem_rows[bg::kBatchMaxConn];
+    std::vector<int32_t> smem_sl, smem_stash;
+    std::vector<uint32_t *> packed[bg::kBatchMaxConn];   // target | delay << 24, per network and connection
+    // launch outputs and monitor regions (one region per network and monitor)
+    int32_t *dOut = nullptr, *dOrder = nullptr; void *dNets = nullptr;
+    std::vector<int64_t> sreg, rreg;       // region starts: spike records / state values, [net * max + k]
+    std::vector<int32_t> scap, rcap;       // region capacities (records / rows)
+    int32_t *dSIdx = nullptr, *dSStep = nullptr; void *dRows = nullptr;
+    int32_t *dCIdx = nullptr, *dCStep = nullptr; void *dCRows = nullptr;   // compacted copies
+    int64_t *dGather = nullptr; int64_t gather_cap = 0;                     // region starts, lengths, targets
+    int64_t nsrec = 0, nrval = 0;
+    std::vector<std::pair<uint16_t *, uint16_t *>> snap;   // global rings and their copies (autotuning)
+    std::vector<size_t> snap_bytes;
+    std::vector<void *> allocs;
+    cudaStream_t stream = nullptr; cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ms = 0; int64_t launches = 0;
+    template <typename P> cudaError_t alloc(P **p, size_t bytes) {
+        void *q = nullptr;
+        cudaError_t e = cudaMalloc(&q, bytes ? bytes : 16);
+        if (e == cudaSuccess) { allocs.push_back(q); *p = (P *)q; }
+        return e;
+    }
+    ~bg_batch() {
+        for (void *q : allocs) cudaFree(q);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+// copies the regions [src + soff[r], + len[r]) to dst + doff[r] (32-bit words)
+__global__ void k_batch_gather(const uint32_t *src, const int64_t *g, int nreg, uint32_t *dst) {
+    for (int r = blockIdx.x; r < nreg; r += gridDim.x) {
+        const int64_t so = g[r], len = g[nreg + r], dof = g[2 * nreg + r];
+        for (int64_t k = threadIdx.x; k < len; k += blockDim.x) dst[dof + k] = src[so + k];
+    }
+}
+
+bool batch_direct(const HConn &c) {
+    return !c.hetero && !c.dense && c.delay == 0 && c.mod_var < 0 && c.stdp < 0 && c.homogeneous && c.src == 0 && c.tgt == 0;
+}
+
+// Why a network cannot run in a batch ("" when it can).
+std::string batch_refusal(const bg_net *n) {
+    if (n->failed) return "the network stopped after a device error";
+    if (n->groups.size() != 1) return "a batched network has exactly one NeuronGroup";
+    const HGroup &g = n->groups[0];
+    if (!g.linear || g.nvar < 1 || g.nvar > 4) return "the group is not linear with 1-4 variables";
+    if (g.refr || g.period > 0 || g.emp_steps > 0 || g.generated()) return "refractoriness and generated models are not batched";
+    if (g.thr_kind != BG_THR_CONST && g.thr_kind != BG_THR_VAR && g.thr_kind != BG_THR_NONE) return "threshold kind";
+    if (g.reset_kind != BG_RESET_NONE && g.reset_kind != BG_RESET_CONST && g.reset_kind != BG_RESET_VAR) return "reset kind";
+    if (g.n > bg::kBatchMaxNeurons) return "more than 4096 neurons";
+    if (!n->stdps.empty() || !n->syns.empty()) return "STDP and Synapses are not batched";
+    if ((int)n->conns.size() > bg::kBatchMaxConn) return "more than 2 connections";
+    for (const HConn &c : n->conns) {
+        if (batch_direct(c)) continue;
+        if (!(c.hetero && c.fused_push && c.dCRing && c.homogeneous && c.src == 0 && c.tgt == 0))
+            return "a connection that is neither a zero-delay shared-weight Connection nor a shared-weight DelayConnection onto the group";
+    }
+    if ((int)n->smons.size() > bg::kBatchMaxSmon) return "more than 2 spike monitors";
+    for (const HSpikeMon &m : n->smons) if (m.gid != 0 || m.delay != 0) return "a delayed spike monitor";
+    if ((int)n->stmons.size() > bg::kBatchMaxRec) return "more than 4 StateMonitors";
+    return "";
+}
+
+template <typename T>
+void batch_image(bg_batch *b, const std::vector<int64_t> &nsteps, int dry, std::vector<bg::BatchNet<T>> &img) {
+    img.assign(b->nets.size(), bg::BatchNet<T>());
+    for (size_t i = 0; i < b->nets.size(); ++i) {
+        bg_net *n = b->nets[i];
+        const HGroup &g = n->groups[0];
+        bg::BatchNet<T> &N = img[i];
+        std::memset(&N, 0, sizeof(N));
+        const int nv = g.nvar;
+        for (int j = 0; j < nv; ++j) {
+            for (int k = 0; k < nv; ++k) {
+                N.A[j * nv + k] = (T)g.A[j * nv + k];
+                if (N.A[j * nv + k] != T(0)) N.anz |= 1ull << (j * nv + k);
+            }
+            N.C[j] = g.useC ? (T)g.C[j] : T(0);
+            if (N.C[j] != T(0)) N.cnz |= 1u << j;
+        }
+        N.thr_kind = g.thr_kind; N.thr_var = g.thr_var; N.thr_var2 = g.thr_var2; N.thr_val = (T)g.thr_val;
+        N.reset_kind = g.reset_kind; N.reset_var = g.reset_var; N.reset_var2 = g.reset_var2; N.reset_val = (T)g.reset_val;
+        N.S = (T *)g.dS; N.npad = g.npad; N.n = (int32_t)g.n;
+        N.nconn = (int32_t)n->conns.size();
+        for (int c = 0; c < N.nconn; ++c) {
+            const HConn &hc = n->conns[c];
+            bg::BatchConn<T> &q = N.conn[c];
+            q.so = (int32_t)hc.so; q.sn = (int32_t)hc.sn; q.to = (int32_t)hc.to; q.tn = (int32_t)hc.tn; q.var = hc.var;
+            q.direct = batch_direct(hc) ? 1 : 0;
+            q.md = q.direct ? 1 : hc.md;
+            q.tnp = (int32_t)((hc.tn + 1) & ~1ll);
+            q.smem_ring = b->smem_ring[c][i]; q.smem_rows = b->smem_rows[c][i];
+            const double w0 = hc.w_bits == 64 ? *(const double *)hc.w.data() : (double)*(const float *)hc.w.data();
+            q.w = (T)w0;
+            q.rowptr = hc.dRow; q.packed = b->packed[c][i];
+            q.ring = q.direct ? nullptr : hc.dCRing;
+        }
+        // deliveries: the Connections (the step's connection slot), then the
+        // DelayConnections' due rows, each in connection order
+        N.ndeliv = 0;
+        for (int pass = 0; pass < 2; ++pass)
+            for (int c = 0; c < N.nconn; ++c)
+                if ((N.conn[c].direct == 1) == (pass == 0)) N.deliv[N.ndeliv++] = c;
+        const int ms = bg::kBatchMaxSmon, mr = bg::kBatchMaxRec;
+        N.nsmon = (int32_t)n->smons.size();
+        for (int m = 0; m < N.nsmon; ++m) {
+            const HSpikeMon &h = n->smons[m];
+            bg::BatchSmon &M = N.smon[m];
+            M.origin = (int32_t)h.origin; M.n = (int32_t)h.n; M.cap = b->scap[i * ms + m];
+            M.idx = b->dSIdx + b->sreg[i * ms + m]; M.step = b->dSStep + b->sreg[i * ms + m];
+        }
+        N.nrec = (int32_t)n->stmons.size();
+        for (int r = 0; r < N.nrec; ++r) {
+            const HStateMon &h = n->stmons[r];
+            bg::BatchRec &R = N.rec[r];
+            R.var = h.var; R.nidx = (int32_t)h.idx.size(); R.timestep = h.timestep; R.cap_rows = b->rcap[i * mr + r];
+            R.start = h.start; R.row0 = h.rows_done; R.idx = h.dIdx; R.pos = h.dPos;
+            R.buf = (T *)b->dRows + b->rreg[i * mr + r];
+        }
+        N.smem_sl = b->smem_sl[i]; N.smem_stash = b->smem_stash[i];
+        N.ctl = n->dCtl; N.counters = n->dCounters;
+        N.t0 = n->nstep; N.nsteps = (int32_t)nsteps[i];
+        N.out = b->dOut + i * bg::kBatchOut;
+        (void)dry;
+    }
+}
+
+// One launch over every network with steps left; returns the steps each ran.
+template <typename T>
+int batch_launch(bg_batch *b, const std::vector<int64_t> &want, int dry, std::vector<int32_t> *ran, float *ms) {
+    std::vector<bg::BatchNet<T>> img;
+    batch_image<T>(b, want, dry, img);
+    // longest remaining runs first (their blocks start in the first wave)
+    std::vector<int32_t> order(b->nets.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = (int32_t)i;
+    std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return want[x] > want[y]; });
+    BG_CUDA(cudaMemcpyAsync(b->dNets, img.data(), img.size() * sizeof(img[0]), cudaMemcpyHostToDevice, b->stream));
+    BG_CUDA(cudaMemcpyAsync(b->dOrder, order.data(), order.size() * 4, cudaMemcpyHostToDevice, b->stream));
+    BG_CUDA(cudaEventRecord(b->ev0, b->stream));
+    cudaError_t e = bg_batch_launch(b->precision, b->nvar, b->shape, b->dNets, b->dOrder, (int)b->nets.size(), b->lanes,
+                                    dry, b->smem, b->stream);
+    if (e != cudaSuccess) return fail(BG_ECUDA, std::string("batch launch: ") + cudaGetErrorString(e));
+    BG_CUDA(cudaEventRecord(b->ev1, b->stream));
+    BG_CUDA(cudaEventSynchronize(b->ev1));
+    BG_CUDA(cudaEventElapsedTime(ms, b->ev0, b->ev1));
+    b->launches++;
+    if (ran) {
+        ran->assign(b->nets.size() * bg::kBatchOut, 0);
+        BG_CUDA(cudaMemcpy(ran->data(), b->dOut, ran->size() * 4, cudaMemcpyDeviceToHost));
+    }
+    return BG_OK;
+}
+
+// Monitor records of the last launch into the networks' host records.
+template <typename T>
+int batch_collect(bg_batch *b, const std::vector<int32_t> &out, const std::vector<int64_t> &t0,
+                  const std::vector<long long> &off) {
+    const int ms = bg::kBatchMaxSmon, mr = bg::kBatchMaxRec, K = bg::kBatchOut;
+    const size_t nn = b->nets.size();
+    // spike records: regions (start, length, target), gathered into one block
+    std::vector<int64_t> so, len, dof;
+    int64_t tot = 0;
+    for (size_t i = 0; i < nn; ++i)
+        for (int m = 0; m < (int)b->nets[i]->smons.size(); ++m) {
+            const int64_t c = out[i * K + 1 + m];
+            if (c > 0) { so.push_back(b->sreg[i * ms + m]); len.push_back(c); dof.push_back(tot); tot += c; }
+        }
+    auto gather = [&](const uint32_t *src, uint32_t *dst, const std::vector<int64_t> &a, const std::vector<int64_t> &l,
+                      const std::vector<int64_t> &d, int words) -> int {
+        const int nreg = (int)a.size();
+        if (!nreg) return BG_OK;
+        std::vector<int64_t> g(3 * nreg);
+        for (int r = 0; r < nreg; ++r) { g[r] = a[r] * words; g[nreg + r] = l[r] * words; g[2 * nreg + r] = d[r] * words; }
+        if (3 * nreg > b->gather_cap) return fail(BG_ESTATE, "batch gather table");
+        BG_CUDA(cudaMemcpyAsync(b->dGather, g.data(), g.size() * 8, cudaMemcpyHostToDevice, b->stream));
+        k_batch_gather<<<(unsigned)std::min(nreg, 4096), 256, 0, b->stream>>>(src, b->dGather, nreg, dst);
+        BG_CUDA(cudaGetLastError());
+        BG_CUDA(cudaStreamSynchronize(b->stream));
+        return BG_OK;
+    };
+    if (tot > 0) {
+        int st = gather((const uint32_t *)b->dSIdx, (uint32_t *)b->dCIdx, so, len, dof, 1); if (st) return st;
+        st = gather((const uint32_t *)b->dSStep, (uint32_t *)b->dCStep, so, len, dof, 1); if (st) return st;
+        std::vector<int32_t> idx(tot), stp(tot);
+        BG_CUDA(cudaMemcpy(idx.data(), b->dCIdx, tot * 4, cudaMemcpyDeviceToHost));
+        BG_CUDA(cudaMemcpy(stp.data(), b->dCStep, tot * 4, cudaMemcpyDeviceToHost));
+        int64_t p = 0;
+        for (size_t i = 0; i < nn; ++i)
+            for (int m = 0; m < (int)b->nets[i]->smons.size(); ++m) {
+                HSpikeMon &h = b->nets[i]->smons[m];
+                const int64_t c = out[i * K + 1 + m];
+                const long long cs = t0[i] + off[i];
+                for (int64_t k = 0; k < c; ++k, ++p) { h.idx.push_back(idx[p]); h.steps.push_back(cs + stp[p]); }
+            }
+    }
+    // state rows
+    so.clear(); len.clear(); dof.clear(); tot = 0;
+    for (size_t i = 0; i < nn; ++i)
+        for (int r = 0; r < (int)b->nets[i]->stmons.size(); ++r) {
+            const int64_t rows = out[i * K + 1 + ms + r], w = (int64_t)b->nets[i]->stmons[r].idx.size();
+            if (rows > 0 && w > 0) { so.push_back(b->rreg[i * mr + r]); len.push_back(rows * w); dof.push_back(tot); tot += rows * w; }
+        }
+    std::vector<T> vals(tot);
+    if (tot > 0) {
+        const int words = (int)(sizeof(T) / 4);
+        int st = gather((const uint32_t *)b->dRows, (uint32_t *)b->dCRows, so, len, dof, words); if (st) return st;
+        BG_CUDA(cudaMemcpy(vals.data(), b->dCRows, tot * sizeof(T), cudaMemcpyDeviceToHost));
+    }
+    int64_t p = 0;
+    for (size_t i = 0; i < nn; ++i)
+        for (int r = 0; r < (int)b->nets[i]->stmons.size(); ++r) {
+            HStateMon &h = b->nets[i]->stmons[r];
+            const int64_t rows = out[i * K + 1 + ms + r], w = (int64_t)h.idx.size();
+            for (int64_t q = 0; q < rows; ++q) {
+                for (int64_t j = 0; j < w; ++j) h.vals.push_back((double)vals[p++]);
+                const long long ps = h.start + (h.rows_done + q) * h.timestep;
+                h.steps.push_back(ps + off[i]);
+            }
+            h.rows_done += rows;
+        }
+    return BG_OK;
+}
+
+template <typename T>
+int batch_run_impl(bg_batch *b, const int64_t *nsteps, const int64_t *cs0) {
+    const size_t nn = b->nets.size();
+    std::vector<int64_t> left(nsteps, nsteps + nn), t0(nn);
+    std::vector<long long> off(nn);
+    for (size_t i = 0; i < nn; ++i) {
+        if (left[i] < 0) return fail(BG_EINVAL, "negative step count");
+        if (b->nets[i]->nstep + left[i] >= (1ll << 31) - 1) return fail(BG_EINVAL, "a network runs at most 2^31-1 steps");
+        off[i] = cs0[i] - b->nets[i]->nstep;
+    }
+    double total_ms = 0;
+    std::vector<int32_t> out;
+    for (;;) {
+        bool any = false;
+        for (size_t i = 0; i < nn; ++i) any |= left[i] > 0;
+        if (!any) break;
+        std::vector<int64_t> want(nn);
+        for (size_t i = 0; i < nn; ++i) { want[i] = std::min<int64_t>(left[i], (int64_t)1 << 30); t0[i] = b->nets[i]->nstep; }
+        float ms = 0;
+        int st = batch_launch<T>(b, want, 0, &out, &ms);
+        if (st) return st;
+        total_ms += ms;
+        bool progress = false;
+        for (size_t i = 0; i < nn; ++i) {
+            const int32_t ran = out[i * bg::kBatchOut];
+            if (ran < 0 || ran > want[i]) return fail(BG_ESTATE, "batch launch reported a bad step count");
+            progress |= ran > 0 || want[i] == 0;
+        }
+        st = batch_collect<T>(b, out, t0, off);
+        if (st) return st;
+        for (size_t i = 0; i < nn; ++i) {
+            const int32_t ran = out[i * bg::kBatchOut];
+            b->nets[i]->nstep += ran;
+            b->nets[i]->launches += want[i] > 0 ? 1 : 0;
+            left[i] -= ran;
+        }
+        if (!progress) return fail(BG_ESTATE, "batch launch made no progress");
+    }
+    // the networks' own monitor bookkeeping follows (a later run alone
+    // writes its rows after the ones taken here)
+    for (bg_net *n : b->nets) {
+        for (HStateMon &m : n->stmons) BG_CUDA(cudaMemcpy(m.dRowBase, &m.rows_done, 8, cudaMemcpyHostToDevice));
+        n->last_ms = total_ms;
+    }
+    b->last_ms = total_ms;
+    return BG_OK;
+}
+
+// Shapes whose blocks hold the largest network and whose instance takes the layout.
+std::vector<int> batch_shapes(bg_batch *b) {
+    std::vector<int> v;
+    for (int sh = 0; sh < bg::kBatchNumShapes; ++sh)
+        if (bg::kBatchShapes[sh].threads * bg::kBatchShapes[sh].npt >= b->max_n &&
+            bg_batch_prepare_shape(b->precision, b->nvar, sh, b->smem) > 0)
+            v.push_back(sh);
+    return v;
+}
+
+int batch_snapshot(bg_batch *b, bool restore) {
+    for (size_t k = 0; k < b->snap.size(); ++k) {
+        uint16_t *ring = b->snap[k].first, *copy = b->snap[k].second;
+        BG_CUDA(cudaMemcpyAsync(restore ? ring : copy, restore ? copy : ring, b->snap_bytes[k], cudaMemcpyDeviceToDevice, b->stream));
+    }
+    BG_CUDA(cudaStreamSynchronize(b->stream));
+    return BG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bg_batch_create(bg_net *const *nets, int32_t count, bg_batch **out) {
+    if (!nets || count <= 0 || !out) return fail(BG_EINVAL, "bg_batch_create");
+    *out = nullptr;
+    for (int32_t i = 0; i < count; ++i) {
+        if (!nets[i]) return fail(BG_EINVAL, "null network");
+        for (int32_t k = 0; k < i; ++k) if (nets[k] == nets[i]) return fail(BG_EINVAL, "a network appears twice in the batch");
+        if (nets[i]->device != nets[0]->device || nets[i]->precision != nets[0]->precision)
+            return fail(BG_EINVAL, "the networks of a batch share the device and the precision");
+        if (!nets[i]->prepared) { int st = bg_net_prepare(nets[i]); if (st) return st; }
+        const std::string why = batch_refusal(nets[i]);
+        if (!why.empty()) return fail(BG_ENOSYS, "network " + std::to_string(i) + ": " + why);
+        if (nets[i]->groups[0].nvar != nets[0]->groups[0].nvar) return fail(BG_EINVAL, "the networks of a batch share the number of state variables");
+    }
+    BG_CUDA(cudaSetDevice(nets[0]->device));
+    std::unique_ptr<bg_batch> b(new bg_batch());
+    b->nets.assign(nets, nets + count);
+    b->device = nets[0]->device; b->precision = nets[0]->precision; b->nvar = nets[0]->groups[0].nvar;
+    BG_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    BG_CUDA(cudaEventCreate(&b->ev0));
+    BG_CUDA(cudaEventCreate(&b->ev1));
+    const size_t ts = b->precision == 64 ? 8 : 4;
+    // shared-memory layout of each network (32-bit words): staged row starts,
+    // spike list, record stash, then the rings -- a Connection's single row
+    // always, a DelayConnection's rows while the block stays under the budget
+    const int64_t kBudget = 100 * 1024 / 4;
+    int64_t ntot_s = 0, ntot_w = 0;
+    for (bg_net *n : b->nets) { ntot_s += (int64_t)n->smons.size(); for (auto &m : n->stmons) ntot_w += (int64_t)m.idx.size(); }
+    for (int c = 0; c < bg::kBatchMaxConn; ++c) { b->smem_ring[c].assign(count, -1); b->smem_rows[c].assign(count, 0); b->packed[c].assign(count, nullptr); }
+    b->smem_sl.assign(count, 0); b->smem_stash.assign(count, 0);
+    b->sreg.assign((size_t)count * bg::kBatchMaxSmon, 0); b->scap.assign((size_t)count * bg::kBatchMaxSmon, 0);
+    b->rreg.assign((size_t)count * bg::kBatchMaxRec, 0); b->rcap.assign((size_t)count * bg::kBatchMaxRec, 0);
+    int64_t maxw = 0, nreg = 0;
+    const int64_t scap_all = std::max<int64_t>(1024, std::min<int64_t>(1 << 16, ((int64_t)1 << 25) / std::max<int64_t>(1, ntot_s)));
+    const int64_t rcap_all = std::max<int64_t>(1, std::min<int64_t>(4096, ((int64_t)1 << 25) / std::max<int64_t>(1, ntot_w)));
+    for (int32_t i = 0; i < count; ++i) {
+        bg_net *n = b->nets[i];
+        const HGroup &g = n->groups[0];
+        b->max_n = std::max<int>(b->max_n, (int)g.n);
+        int64_t w = 0;
+        for (size_t c = 0; c < n->conns.size(); ++c) {
+            HConn &hc = n->conns[c];
+            if (hc.rowptr[hc.sn] - hc.rowptr[0] >= ((int64_t)1 << 32)) return fail(BG_ENOSYS, "more than 2^32 synapses in one connection");
+            if (hc.tn > (1 << 24)) return fail(BG_ENOSYS, "target range above 2^24");
+            b->smem_rows[c][i] = (int32_t)w; w += hc.sn + 1;
+            // packed synapse words (delay 0 for a Connection)
+            uint32_t *pk = nullptr;
+            if (b->alloc(&pk, std::max<int64_t>(1, hc.nnz) * 4) != cudaSuccess) return fail(BG_ENOMEM, "batch synapses");
+            if (hc.nnz > 0) {
+                const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((hc.nnz + 255) / 256, (int64_t)sm_count() * 8));
+                k_pack_synapses<<<grid, 256, 0, b->stream>>>(hc.dCols, batch_direct(hc) ? nullptr : hc.dD, hc.nnz, pk);
+                BG_CUDA(cudaGetLastError());
+            }
+            b->packed[c][i] = pk;
+            if (batch_direct(hc)) {
+                int64_t kmax = 0;
+                int st = max_indegree(n, hc, &kmax);
+                if (st) return st;
+                if (kmax >= 65535) return fail(BG_ENOSYS, "in-degree above 65534 (16-bit counts)");
+            }
+        }
+        b->smem_sl[i] = (int32_t)w; w += g.n;
+        w = (w + 1) & ~1ll;                                   // 8-byte alignment of the stash
+        b->smem_stash[i] = (int32_t)w; w += n->stmons.empty() ? 0 : g.n * (int64_t)(ts / 4);
+        for (size_t c = 0; c < n->conns.size(); ++c) {        // Connections: one row
+            const HConn &hc = n->conns[c];
+            if (!batch_direct(hc)) continue;
+            b->smem_ring[c][i] = (int32_t)w; w += ((hc.tn + 1) & ~1ll) / 2;
+        }
+        for (size_t c = 0; c < n->conns.size(); ++c) {        // DelayConnections: md rows, if they fit
+            const HConn &hc = n->conns[c];
+            if (batch_direct(hc)) continue;
+            const int64_t rw = (int64_t)hc.md * hc.tnp / 2;
+            if (w + rw <= kBudget) { b->smem_ring[c][i] = (int32_t)w; w += rw; }
+            else {
+                uint16_t *copy = nullptr;
+                const size_t bytes = (size_t)hc.md * hc.tnp * 2;
+                if (b->alloc(&copy, bytes) != cudaSuccess) return fail(BG_ENOMEM, "batch ring copy");
+                b->snap.push_back({hc.dCRing, copy}); b->snap_bytes.push_back(bytes);
+            }
+        }
+        maxw = std::max(maxw, w);
+        for (size_t m = 0; m < n->smons.size(); ++m) {
+            b->sreg[i * bg::kBatchMaxSmon + m] = b->nsrec;
+            const int64_t cap = std::max<int64_t>(n->smons[m].n, scap_all);
+            b->scap[i * bg::kBatchMaxSmon + m] = (int32_t)cap;
+            b->nsrec += cap; ++nreg;
+        }
+        for (size_t r = 0; r < n->stmons.size(); ++r) {
+            b->rreg[i * bg::kBatchMaxRec + r] = b->nrval;
+            b->rcap[i * bg::kBatchMaxRec + r] = (int32_t)rcap_all;
+            b->nrval += rcap_all * (int64_t)n->stmons[r].idx.size(); ++nreg;
+        }
+    }
+    b->smem = (size_t)maxw * 4;
+    if (b->nsrec > ((int64_t)1 << 31) || b->nrval > ((int64_t)1 << 31)) return fail(BG_ENOSYS, "batch monitor buffers above 2^31 entries");
+    b->gather_cap = 3 * std::max<int64_t>(1, nreg);
+    if (b->alloc(&b->dNets, (size_t)count * std::max(sizeof(bg::BatchNet<double>), sizeof(bg::BatchNet<float>))) != cudaSuccess ||
+        b->alloc(&b->dOrder, (size_t)count * 4) != cudaSuccess ||
+        b->alloc(&b->dOut, (size_t)count * bg::kBatchOut * 4) != cudaSuccess ||
+        b->alloc(&b->dSIdx, std::max<int64_t>(1, b->nsrec) * 4) != cudaSuccess ||
+        b->alloc(&b->dSStep, std::max<int64_t>(1, b->nsrec) * 4) != cudaSuccess ||
+        b->alloc(&b->dCIdx, std::max<int64_t>(1, b->nsrec) * 4) != cudaSuccess ||
+        b->alloc(&b->dCStep, std::max<int64_t>(1, b->nsrec) * 4) != cudaSuccess ||
+        b->alloc(&b->dRows, std::max<int64_t>(1, b->nrval) * ts) != cudaSuccess ||
+        b->alloc(&b->dCRows, std::max<int64_t>(1, b->nrval) * ts) != cudaSuccess ||
+        b->alloc(&b->dGather, b->gather_cap * 8) != cudaSuccess)
+        return fail(BG_ENOMEM, "batch buffers");
+    BG_CUDA(cudaStreamSynchronize(b->stream));
+    // default shape: the most threads among the shapes that hold the largest network
+    std::vector<int> ok = batch_shapes(b.get());
+    if (ok.empty()) return fail(BG_ENOSYS, "no block shape takes the batch's shared-memory layout");
+    b->shape = ok.back();
+    for (int sh : ok) if (bg::kBatchShapes[sh].threads > bg::kBatchShapes[b->shape].threads) b->shape = sh;
+    b->lanes = 32;
+    // every network's earlier work is finished before the batch's stream uses its state
+    for (bg_net *n : b->nets) BG_CUDA(cudaStreamSynchronize(n->stream));
+    *out = b.release();
+    return BG_OK;
+}
+
+int bg_batch_free(bg_batch *b) {
+    if (!b) return fail(BG_EINVAL, "batch");
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->stream);
+    delete b;
+    return BG_OK;
+}
+
+int bg_batch_run(bg_batch *b, const int64_t *nsteps, const int64_t *cs0) {
+    if (!b || !nsteps || !cs0) return fail(BG_EINVAL, "bg_batch_run");
+    BG_CUDA(cudaSetDevice(b->device));
+    for (bg_net *n : b->nets) {
+        if (n->failed) return fail(BG_ESTATE, "a network of the batch stopped after a device error");
+        BG_CUDA(cudaStreamSynchronize(n->stream));
+    }
+    return b->precision == 64 ? batch_run_impl<double>(b, nsteps, cs0) : batch_run_impl<float>(b, nsteps, cs0);
+}
+
+int bg_batch_set_shape(bg_batch *b, int32_t shape, int32_t lanes) {
+    if (!b) return fail(BG_EINVAL, "batch");
+    if (lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32) return fail(BG_EINVAL, "lanes per spike row: 4, 8, 16 or 32");
+    std::vector<int> ok = batch_shapes(b);
+    if (std::find(ok.begin(), ok.end(), shape) == ok.end()) return fail(BG_EINVAL, "block shape does not hold the batch");
+    b->shape = shape; b->lanes = lanes;
+    return BG_OK;
+}
+
+int bg_batch_get_shape(bg_batch *b, int32_t *shape, int32_t *threads, int32_t *npt, int32_t *lanes) {
+    if (!b || b->shape < 0) return fail(BG_EINVAL, "batch");
+    if (shape) *shape = b->shape;
+    if (threads) *threads = bg::kBatchShapes[b->shape].threads;
+    if (npt) *npt = bg::kBatchShapes[b->shape].npt;
+    if (lanes) *lanes = b->lanes;
+    return BG_OK;
+}
+
+int bg_batch_autotune(bg_batch *b, int32_t steps, double *best_ms) {
+    if (!b || steps <= 0) return fail(BG_EINVAL, "bg_batch_autotune");
+    BG_CUDA(cudaSetDevice(b->device));
+    for (bg_net *n : b->nets) BG_CUDA(cudaStreamSynchronize(n->stream));
+    std::vector<int64_t> want(b->nets.size(), steps);
+    const int keep_shape = b->shape, keep_lanes = b->lanes;
+    double best = -1;
+    int bs = keep_shape, bl = keep_lanes;
+    int st = batch_snapshot(b, false);
+    if (st) return st;
+    for (int sh : batch_shapes(b)) {
+        for (int lanes : {4, 8, 16, 32}) {
+            b->shape = sh; b->lanes = lanes;
+            float ms = 0;
+            for (int rep = 0; rep < 2 && st == BG_OK; ++rep) {      // warm-up, then timed
+                st = b->precision == 64 ? batch_launch<double>(b, want, 1, nullptr, &ms) : batch_launch<float>(b, want, 1, nullptr, &ms);
+                if (st == BG_OK) st = batch_snapshot(b, true);      // dry runs still push into rings kept in global memory
+            }
+            if (st) { b->shape = keep_shape; b->lanes = keep_lanes; return st; }
+            if (best < 0 || ms < best) { best = ms; bs = sh; bl = lanes; }
+        }
+    }
+    b->shape = bs; b->lanes = bl;
+    if (best_ms) *best_ms = best;
+    return BG_OK;
+}
+
+int bg_batch_stats(bg_batch *b, int64_t *launches, double *ms) {
+    if (!b) return fail(BG_EINVAL, "batch");
+    if (launches) *launches = b->launches;
+    if (ms) *ms = b->last_ms;
     return BG_OK;
 }
 

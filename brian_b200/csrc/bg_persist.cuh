@@ -62,42 +62,6 @@ __device__ __forceinline__ void red_release_add(unsigned int *p, unsigned int v)
     asm volatile("red.release.gpu.global.add.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
 }
 
-// Block-uniform variable access without runtime-indexed register arrays:
-// `var` is a kernel parameter, so the switch is a uniform branch.
-template <typename T, int NV>
-__device__ __forceinline__ T uget(const T (&s)[NV], int var) {
-    switch (var) {
-    case 0: return s[0];
-    case 1: if (NV > 1) return s[NV > 1 ? 1 : 0]; break;
-    case 2: if (NV > 2) return s[NV > 2 ? 2 : 0]; break;
-    default: if (NV > 3) return s[NV > 3 ? 3 : 0]; break;
-    }
-    return T(0);
-}
-template <typename T, int NV>
-__device__ __forceinline__ void uset(T (&s)[NV], int var, T v) {
-    switch (var) {
-    case 0: s[0] = v; break;
-    case 1: if (NV > 1) s[NV > 1 ? 1 : 0] = v; break;
-    case 2: if (NV > 2) s[NV > 2 ? 2 : 0] = v; break;
-    default: if (NV > 3) s[NV > 3 ? 3 : 0] = v; break;
-    }
-}
-
-// Uniform dispatch on a state-variable index hoisted out of the per-neuron
-// loops: f receives the index as a compile-time constant, so the neuron loop
-// inside it indexes registers directly and the branch runs once per thread.
-template <int K> struct VarIdx { static constexpr int value = K; };
-template <int NV, typename F>
-__device__ __forceinline__ void on_var(int var, F &&f) {
-    switch (var) {
-    case 0: f(VarIdx<0>()); break;
-    case 1: if constexpr (NV > 1) f(VarIdx<1>()); break;
-    case 2: if constexpr (NV > 2) f(VarIdx<2>()); break;
-    default: if constexpr (NV > 3) f(VarIdx<3>()); break;
-    }
-}
-
 // DIAG: the host found A's nonzeros to be exactly its first row and its
 // diagonal, and C's to be at most its first entry (a potential driven by
 // decaying synaptic variables, as in CUBA), so the update needs no mask tests.

@@ -551,6 +551,40 @@ BG_API int bg_mlp_gradients(bg_mlp *h, int batch, float *loss, float *const *dW,
 BG_API int bg_gemm_bf16(int64_t M, int64_t N, int64_t K, const void *A, const void *B,
                         float *C, void *stream);
 
+/* ---- batches of independent networks ----------------------------------
+ * Many small networks simulated side by side in one kernel launch, one
+ * thread block per network (no counterpart in the reference, which runs one
+ * Network per process: network.py:403-430 is the step each block repeats).
+ * A network qualifies when it is what the persistent kernel runs -- one
+ * linear group of 1-4 variables and at most 4096 neurons, no
+ * refractoriness, at most 2 connections onto the group that are zero-delay
+ * shared-weight Connections or shared-weight DelayConnections, at most 2
+ * undelayed spike monitors and 4 StateMonitors, no STDP or Synapses -- and
+ * the networks of a batch share the device, the precision and the number of
+ * state variables.  Each network keeps its own parameters, connectivity,
+ * weights, thresholds and durations; its results are those of bg_net_run on
+ * it alone, bit for bit: its state, rings, counters and monitor records
+ * advance as if it had.  The networks (prepared by this call if needed) must
+ * outlive the batch and are not run alone while a batch call is in flight. */
+typedef struct bg_batch bg_batch;
+BG_API int bg_batch_create(bg_net *const *nets, int32_t count, bg_batch **out);
+BG_API int bg_batch_free(bg_batch *b);
+/* Runs network i for nsteps[i] steps (uneven durations allowed); cs0[i] is
+ * its clock step at the start (as for bg_net_run).  Monitor records are
+ * drained into the networks' host records between launches. */
+BG_API int bg_batch_run(bg_batch *b, const int64_t *nsteps, const int64_t *cs0);
+/* Block shape (an index into the kernel's shapes: 128x4, 256x4, 512x4,
+ * 512x8, 1024x4 threads x neurons per thread; the block must hold the
+ * largest network) and lanes per spike row in the push (4, 8, 16, 32). */
+BG_API int bg_batch_set_shape(bg_batch *b, int32_t shape, int32_t lanes);
+BG_API int bg_batch_get_shape(bg_batch *b, int32_t *shape, int32_t *threads, int32_t *npt, int32_t *lanes);
+/* Times `steps` steps of every valid (shape, lanes) pair on the batch
+ * without changing any network (state, rings and records are left as they
+ * were) and keeps the fastest; best_ms (nullable) is its time. */
+BG_API int bg_batch_autotune(bg_batch *b, int32_t steps, double *best_ms);
+/* Kernel launches so far and device time (ms) of the last bg_batch_run. */
+BG_API int bg_batch_stats(bg_batch *b, int64_t *launches, double *ms);
+
 #ifdef __cplusplus
 }
 #endif
