@@ -453,7 +453,10 @@ def profile_case(case, seed):
           batch 4096 (launch 12 of k_gemm is the 512 x 512 hidden layer of
           the second step).
     synapses: CUBA through Synapses (see synapses_case).
-    stdp: the STDP scale-up network, 300 steps."""
+    stdp: the STDP scale-up network, 300 steps.
+    batch: 148 CUBA-4000 networks in one NetworkBatch at the default shape
+          (1024 x 4, 32 lanes), 2000 steps, no autotuning: the first k_batch
+          launch covers steps 0..~1500 (the StateMonitor rows end it)."""
     rng = np.random.default_rng(seed)
     if case == "fit":
         from brian_b200.synthetic import (FitWorkload, adaptive_lif_equations, THRESHOLD, RESET, PARAMS,
@@ -491,6 +494,16 @@ def profile_case(case, seed):
         d["net"].run(300 * DT)
         sp, _ = d["net"]._binding.rt.counters(2, 1)
         print(json.dumps({"case": "stdp", "steps": 300, "input_spikes": int(sp[0]), "output_spikes": int(sp[1])}))
+    elif case == "batch":
+        import brian_b200 as b
+        from brian_b200 import workloads
+        built = [workloads.cuba4000(seed=seed + r) for r in range(148)]
+        batch = b.NetworkBatch([x[0] for x in built])
+        batch.run(2000 * DT)
+        st = batch.stats()
+        print(json.dumps({"case": "batch", "device_ms": st["last_run_ms"], "launches": st["launches"],
+                          "shape": batch.shape()}))
+        batch.close()
     else:
         raise SystemExit("unknown profile case %r" % case)
 
@@ -697,6 +710,54 @@ def cuba4000_bench(args):
     return out
 
 
+def cuba4000_batch_bench(args, replicas=148, steps=10000):
+    """`replicas` independent CUBA-4000 networks (seeds seed..seed+replicas-1,
+    each with its SpikeMonitor and v trace of 10 neurons, FP64, 1 s) in one
+    NetworkBatch: one block per network, block shape and lanes per spike row
+    autotuned first.  Aggregate synaptic events/s over the batch's device
+    time; the replica with the bench seed is compared with the same network
+    run alone through Network.run (spikes and v trace bit for bit)."""
+    import brian_b200 as b
+    from brian_b200 import workloads
+    b.set_global_preferences(precision=64)
+    b.clear()
+    b.reinit_default_clock()
+    t0 = time.perf_counter()
+    built = [workloads.cuba4000(seed=args.seed + r) for r in range(replicas)]
+    build_s = time.perf_counter() - t0
+    batch = b.NetworkBatch([x[0] for x in built])
+    t0 = time.perf_counter()
+    tune_ms = batch.autotune(200)
+    tune_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    batch.run(steps * DT)
+    wall_s = time.perf_counter() - t0
+    st = batch.stats()
+    ev = sum(int(x[0]._binding.rt.counters(1, 2)[1].sum()) for x in built)
+    spikes = sum(len(x[2]._record()[1]) for x in built)
+    rec0 = (tuple(a.copy() for a in built[0][2]._record()), built[0][3]._record()[1].copy())
+    shape = batch.shape()
+    batch.close()
+    for x in built:
+        x[0]._invalidate()
+    # the first replica alone
+    b.clear()
+    b.reinit_default_clock()
+    net, P, M, S = workloads.cuba4000(seed=args.seed)
+    net.run(steps * DT)
+    alone = (tuple(a.copy() for a in M._record()), S._record()[1].copy())
+    net._invalidate()
+    same = all(np.array_equal(x, y) for x, y in zip(rec0[0], alone[0])) and np.array_equal(rec0[1], alone[1])
+    dev_ms = st["last_run_ms"]
+    return {"workload": "%d independent CUBA-4000 networks (seeds %d..%d), 1 s each, SpikeMonitor + v of 10 neurons "
+                        "each, one NetworkBatch" % (replicas, args.seed, args.seed + replicas - 1),
+            "replicas": replicas, "events": ev, "spikes": spikes, "device_ms": dev_ms,
+            "events_per_s": ev / (dev_ms * 1e-3), "wall_ms": wall_s * 1e3, "events_per_s_wall": ev / wall_s,
+            "us_per_step": dev_ms * 1e3 / steps, "launches": st["launches"], "shape": shape,
+            "autotune_ms_200_steps": tune_ms, "autotune_wall_s": tune_s, "build_s": build_s,
+            "replica0_equal_single_run": bool(same)}
+
+
 def cuba262k_precision(args, inp, nsteps=2000):
     """CUBA-262k with FP32 state against FP64 (same network and initial
     state, spike monitor and v of 10 neurons, `nsteps` steps), and the FP32
@@ -883,7 +944,7 @@ def main():
     ap.add_argument("--fit-train", type=int, default=1 << 20)
     ap.add_argument("--fit-epochs", type=int, default=40)
     ap.add_argument("--fit-iters", type=int, default=40)
-    ap.add_argument("--profile-case", choices=["fit", "gemm", "synapses", "stdp"], default=None,
+    ap.add_argument("--profile-case", choices=["fit", "gemm", "synapses", "stdp", "batch"], default=None,
                     help="run one small case for a single-kernel ncu capture and exit")
     args = ap.parse_args()
     if args.profile_case:
@@ -1008,6 +1069,7 @@ def main():
     if rank == 0 and world == 1:
         if not args.no_cuba4000:
             side["cuba4000"] = guarded(cuba4000_bench, args)
+            side["cuba4000_batch"] = guarded(cuba4000_batch_bench, args)
         if not args.no_precision:
             side["precision_cuba262k"] = guarded(cuba262k_precision, args, inp)
         if not args.no_stdp:

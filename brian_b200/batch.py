@@ -83,8 +83,9 @@ class NetworkBatch(object):
         return ms
 
     def set_shape(self, shape, lanes=32):
-        """Block shape index (128x4, 256x4, 512x4, 512x8, 1024x4 threads x
-        neurons per thread) and lanes per spike row (4, 8, 16, 32)."""
+        """Block shape index (128x4, 256x4, 512x4, 512x8, 1024x4, 768x6
+        threads x neurons per thread) and lanes per spike row (4, 8, 16,
+        32)."""
         self._runtime().set_shape(shape, lanes)
         self._shape = (int(shape), int(lanes))
 

@@ -18,10 +18,11 @@ const void *batch_fn_shape(int shape) {
     case 2: return batch_fn<T, NV, 2>();
     case 3: return batch_fn<T, NV, 3>();
     case 4: return batch_fn<T, NV, 4>();
+    case 5: return batch_fn<T, NV, 5>();
     default: return nullptr;
     }
 }
-static_assert(bg::kBatchNumShapes == 5, "one case per shape");
+static_assert(bg::kBatchNumShapes == 6, "one case per shape");
 
 template <typename T>
 const void *batch_fn_nv(int nvar, int shape) {

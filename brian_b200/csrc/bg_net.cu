@@ -2454,7 +2454,7 @@ struct bg_batch {
     size_t smem = 0;                       // dynamic shared memory per block (largest layout)
     std::vector<int32_t> smem_ring[bg::kBatchMaxConn];   // per network: ring offsets (-1: global)
     std::vector<int32_t> smem_rows[bg::kBatchMaxConn];
-    std::vector<int32_t> smem_sl, smem_stash;
+    std::vector<int32_t> smem_pos;
     std::vector<uint32_t *> packed[bg::kBatchMaxConn];   // target | delay << 24, per network and connection
     // launch outputs and monitor regions (one region per network and monitor)
     int32_t *dOut = nullptr, *dOrder = nullptr; void *dNets = nullptr;
@@ -2517,6 +2517,11 @@ std::string batch_refusal(const bg_net *n) {
     if ((int)n->smons.size() > bg::kBatchMaxSmon) return "more than 2 spike monitors";
     for (const HSpikeMon &m : n->smons) if (m.gid != 0 || m.delay != 0) return "a delayed spike monitor";
     if ((int)n->stmons.size() > bg::kBatchMaxRec) return "more than 4 StateMonitors";
+    for (const HStateMon &m : n->stmons) {
+        if (m.gid != 0) return "a StateMonitor on another group";
+        for (size_t e = 1; e < m.sorted.size(); ++e)
+            if (m.sorted[e] == m.sorted[e - 1]) return "a StateMonitor that records a neuron twice";
+    }
     return "";
 }
 
@@ -2537,6 +2542,10 @@ void batch_image(bg_batch *b, const std::vector<int64_t> &nsteps, int dry, std::
             N.C[j] = g.useC ? (T)g.C[j] : T(0);
             if (N.C[j] != T(0)) N.cnz |= 1u << j;
         }
+        N.diag = (N.cnz & ~1u) == 0;
+        for (int j = 0; j < nv; ++j)
+            for (int k = 0; k < nv; ++k)
+                if ((((N.anz >> (j * nv + k)) & 1ull) != 0) != (j == 0 || j == k)) N.diag = 0;
         N.thr_kind = g.thr_kind; N.thr_var = g.thr_var; N.thr_var2 = g.thr_var2; N.thr_val = (T)g.thr_val;
         N.reset_kind = g.reset_kind; N.reset_var = g.reset_var; N.reset_var2 = g.reset_var2; N.reset_val = (T)g.reset_val;
         N.S = (T *)g.dS; N.npad = g.npad; N.n = (int32_t)g.n;
@@ -2546,7 +2555,7 @@ void batch_image(bg_batch *b, const std::vector<int64_t> &nsteps, int dry, std::
             bg::BatchConn<T> &q = N.conn[c];
             q.so = (int32_t)hc.so; q.sn = (int32_t)hc.sn; q.to = (int32_t)hc.to; q.tn = (int32_t)hc.tn; q.var = hc.var;
             q.direct = batch_direct(hc) ? 1 : 0;
-            q.md = q.direct ? 1 : hc.md;
+            q.md = q.direct ? 2 : hc.md;           // a Connection's row of step t (parity), pushed and delivered
             q.tnp = (int32_t)((hc.tn + 1) & ~1ll);
             q.smem_ring = b->smem_ring[c][i]; q.smem_rows = b->smem_rows[c][i];
             const double w0 = hc.w_bits == 64 ? *(const double *)hc.w.data() : (double)*(const float *)hc.w.data();
@@ -2576,7 +2585,7 @@ void batch_image(bg_batch *b, const std::vector<int64_t> &nsteps, int dry, std::
             R.start = h.start; R.row0 = h.rows_done; R.idx = h.dIdx; R.pos = h.dPos;
             R.buf = (T *)b->dRows + b->rreg[i * mr + r];
         }
-        N.smem_sl = b->smem_sl[i]; N.smem_stash = b->smem_stash[i];
+        N.smem_pos = b->smem_pos[i];
         N.ctl = n->dCtl; N.counters = n->dCounters;
         N.t0 = n->nstep; N.nsteps = (int32_t)nsteps[i];
         N.out = b->dOut + i * bg::kBatchOut;
@@ -2773,13 +2782,13 @@ int bg_batch_create(bg_net *const *nets, int32_t count, bg_batch **out) {
     BG_CUDA(cudaEventCreate(&b->ev1));
     const size_t ts = b->precision == 64 ? 8 : 4;
     // shared-memory layout of each network (32-bit words): staged row starts,
-    // spike list, record stash, then the rings -- a Connection's single row
+    // StateMonitor columns, then the rings -- a Connection's single row
     // always, a DelayConnection's rows while the block stays under the budget
     const int64_t kBudget = 100 * 1024 / 4;
     int64_t ntot_s = 0, ntot_w = 0;
     for (bg_net *n : b->nets) { ntot_s += (int64_t)n->smons.size(); for (auto &m : n->stmons) ntot_w += (int64_t)m.idx.size(); }
     for (int c = 0; c < bg::kBatchMaxConn; ++c) { b->smem_ring[c].assign(count, -1); b->smem_rows[c].assign(count, 0); b->packed[c].assign(count, nullptr); }
-    b->smem_sl.assign(count, 0); b->smem_stash.assign(count, 0);
+    b->smem_pos.assign(count, 0);
     b->sreg.assign((size_t)count * bg::kBatchMaxSmon, 0); b->scap.assign((size_t)count * bg::kBatchMaxSmon, 0);
     b->rreg.assign((size_t)count * bg::kBatchMaxRec, 0); b->rcap.assign((size_t)count * bg::kBatchMaxRec, 0);
     int64_t maxw = 0, nreg = 0;
@@ -2811,13 +2820,11 @@ int bg_batch_create(bg_net *const *nets, int32_t count, bg_batch **out) {
                 if (kmax >= 65535) return fail(BG_ENOSYS, "in-degree above 65534 (16-bit counts)");
             }
         }
-        b->smem_sl[i] = (int32_t)w; w += g.n;
-        w = (w + 1) & ~1ll;                                   // 8-byte alignment of the stash
-        b->smem_stash[i] = (int32_t)w; w += n->stmons.empty() ? 0 : g.n * (int64_t)(ts / 4);
-        for (size_t c = 0; c < n->conns.size(); ++c) {        // Connections: one row
+        b->smem_pos[i] = (int32_t)w; w += (int64_t)n->stmons.size() * ((g.n + 1) / 2);
+        for (size_t c = 0; c < n->conns.size(); ++c) {        // Connections: two rows (step parity)
             const HConn &hc = n->conns[c];
             if (!batch_direct(hc)) continue;
-            b->smem_ring[c][i] = (int32_t)w; w += ((hc.tn + 1) & ~1ll) / 2;
+            b->smem_ring[c][i] = (int32_t)w; w += (hc.tn + 1) & ~1ll;
         }
         for (size_t c = 0; c < n->conns.size(); ++c) {        // DelayConnections: md rows, if they fit
             const HConn &hc = n->conns[c];

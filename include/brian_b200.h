@@ -574,8 +574,8 @@ BG_API int bg_batch_free(bg_batch *b);
  * drained into the networks' host records between launches. */
 BG_API int bg_batch_run(bg_batch *b, const int64_t *nsteps, const int64_t *cs0);
 /* Block shape (an index into the kernel's shapes: 128x4, 256x4, 512x4,
- * 512x8, 1024x4 threads x neurons per thread; the block must hold the
- * largest network) and lanes per spike row in the push (4, 8, 16, 32). */
+ * 512x8, 1024x4, 768x6 threads x neurons per thread; the block must hold
+ * the largest network) and lanes per spike row in the push (4, 8, 16, 32). */
 BG_API int bg_batch_set_shape(bg_batch *b, int32_t shape, int32_t lanes);
 BG_API int bg_batch_get_shape(bg_batch *b, int32_t *shape, int32_t *threads, int32_t *npt, int32_t *lanes);
 /* Times `steps` steps of every valid (shape, lanes) pair on the batch

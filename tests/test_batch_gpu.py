@@ -115,7 +115,7 @@ def test_batch_uneven_durations_bit_exact(oracle_table, gpu_table):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("shape", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("shape", [0, 1, 2, 3, 4, 5])
 @pytest.mark.parametrize("lanes", [4, 32])
 def test_batch_every_shape_bit_exact(oracle_table, gpu_table, shape, lanes):
     specs = [dict(kind="cuba", n=500, seed=21, record=(1, 499)), dict(kind="delay", n=300, seed=22),
