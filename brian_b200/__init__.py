@@ -24,6 +24,7 @@ from .monitors import (SpikeMonitor, StateMonitor, RecentStateMonitor, ISIHistog
 from .network import (Network, MagicNetwork, run, reinit, stop, clear, network_operation, NetworkOperation,
                       set_global_preferences, get_global_preference)
 from .batch import NetworkBatch
+from .timedarray import TimedArray, TimedArraySetter, set_group_var_by_array
 from .statistics import firing_rate, CV, gamma_factor, get_gamma_factor, spike_triggered_average
 from .modelfitting import (GPUModelFitting, modelfitting, distributed_modelfitting, get_spikes, predict, print_table, PSO, GA, CMAES,
                            OptimizationResult, euler_scheme, rk2_scheme, exp_euler_scheme)

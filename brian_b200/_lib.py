@@ -31,6 +31,7 @@ SIGNATURES = {
     "group_set_refractory": [_vp, _i32, _dbl, _i32, ct.c_int, _dbl],
     "group_set_empirical": [_vp, _i32, _i32],
     "group_set_model": [_vp, _i32, _vp],
+    "group_set_timed_array": [_vp, _i32, ct.c_int, _i64, _i64, _vp, _i64, _i64, ct.c_int, _dbl, _dbl, _i64, _vp],
     "conn_add": [_vp, _i32, _i64, _i64, _i32, _i64, _i64, ct.c_int, _i64, _vp, _vp, _vp, ct.c_int,
                  _i32, _vp, _i32, ct.c_int, _P(_i32)],
     "conn_add_dense": [_vp, _i32, _i64, _i64, _i32, _i64, _i64, ct.c_int, _vp, ct.c_int, _i32, ct.c_int,
@@ -275,6 +276,13 @@ class Runtime(object):
         A = np.ascontiguousarray(A, dtype=np.float64)
         C = None if C is None else np.ascontiguousarray(C, dtype=np.float64)
         self._c(self.t.group_set_linear(self.h, gid, _ptr(A), _ptr(C)), "group_set_linear")
+
+    def group_set_timed_array(self, gid, var, origin, count, values, mode, t_init, adt, first_step, bp):
+        values = np.ascontiguousarray(values, dtype=np.float64)
+        bp = None if bp is None or len(bp) == 0 else np.ascontiguousarray(bp, dtype=np.int64)
+        self._c(self.t.group_set_timed_array(self.h, gid, int(var), int(origin), int(count), _ptr(values),
+                                             values.shape[0], values.shape[1], int(mode), float(t_init), float(adt),
+                                             int(first_step), _ptr(bp)), "group_set_timed_array")
 
     def group_set_threshold(self, gid, kind, var=0, value=0.0, var2=0):
         self._c(self.t.group_set_threshold(self.h, gid, kind, var, float(value), var2), "group_set_threshold")

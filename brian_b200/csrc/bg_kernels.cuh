@@ -71,6 +71,18 @@ struct RecDev {                        // StateMonitor recorded in this group
     void *buf; const long long *row_base; int timestep; long long start;
 };
 
+// TimedArraySetter (timedarray.py:238-303): at the start of a step, before
+// the update, S[var][origin + k] (k < count) takes row r of vals[nrows][ncols]
+// (ncols 1: one value for all).  mode 0 (array on a clock): r = rint((cs*dt -
+// t_init) / adt) clamped to the rows; mode 1 (explicit times): r = the number
+// of breakpoint steps bp[0..nrows-1) <= cs.  Nothing before clock step first.
+constexpr int kMaxSet = 4;
+template <typename T> struct SetDev {
+    int var, mode; int64_t origin, count, nrows, ncols;
+    double t_init, adt; long long first;
+    const T *vals; const int64_t *bp;
+};
+
 template <typename T> struct HeadArgs {
     DevCtl *ctl;
     T *S; int64_t n, npad; int nvar;
@@ -88,9 +100,25 @@ template <typename T> struct HeadArgs {
     int ndeliv; Deliv<T> deliv[kMaxDeliv];
     int nrec; RecDev rec[kMaxRec];
     int npush; Push<T> push[kMaxPush];
+    int nset; SetDev<T> set[kMaxSet];
     unsigned long long *spikes;    // running spike count of the group
     int tail, update, last;
 };
+
+// Row of a setter's array at clock step cs (the reference's
+// int(rint((t - t_init) / dt)) clamped, or the count of breakpoints <= cs).
+template <typename T>
+__device__ __forceinline__ int64_t setter_row(const SetDev<T> &st, long long cs, double dt) {
+    if (st.mode == 0) {
+        const double x = __ddiv_rn(__dsub_rn(__dmul_rn((double)cs, dt), st.t_init), st.adt);
+        if (!(x > 0.0)) return 0;
+        if (x >= (double)(st.nrows - 1)) return st.nrows - 1;
+        return (int64_t)rint(x);
+    }
+    int64_t lo = 0, hi = st.nrows - 1;                   // first breakpoint > cs
+    while (lo < hi) { const int64_t m = (lo + hi) >> 1; if (st.bp[m] <= cs) lo = m + 1; else hi = m; }
+    return lo;
+}
 
 // Row j of the exact linear update: ((0 + A[j][k0] s_k0) + A[j][k1] s_k1) +
 // ... over the nonzero coefficients (bit j*NV+k of anz), left to right, then
@@ -383,6 +411,19 @@ __device__ __forceinline__ void head_body(const HeadArgs<T> &a) {
     }
 
     if (a.update) {
+        // TimedArraySetters ('start' slot)
+        for (int q = 0; q < a.nset; ++q) {
+            const SetDev<T> &st = a.set[q];
+            if (cs < st.first) continue;                       // uniform
+            const int64_t r = setter_row<T>(st, cs, a.dt);
+            const T *row = st.vals + r * st.ncols;
+#pragma unroll
+            for (int u = 0; u < kNPT; ++u) {
+                const int64_t i = base + u * kHeadThreads + tid;
+                if (i >= st.origin && i < st.origin + st.count)
+                    set_var<T, NV>(s[u], st.var, row[st.ncols == 1 ? 0 : i - st.origin]);
+            }
+        }
         __shared__ uint32_t words[kBlockNeurons / 32];
         uint32_t nspk = 0;
 #pragma unroll

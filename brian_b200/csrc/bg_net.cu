@@ -53,6 +53,12 @@ struct HGroup {
     int64_t *dGenSteps = nullptr; int32_t *dGenIdx = nullptr;
     std::vector<int> delivs, recs;
     int emp_steps = 0;                  // EmpiricalThreshold window (steps), 0: off
+    struct Setter {                     // TimedArraySetter (see bg::SetDev)
+        int var, mode; int64_t origin, count, nrows, ncols; double t_init, adt; int64_t first;
+        std::vector<double> vals; std::vector<int64_t> bp;
+        void *dVals = nullptr; int64_t *dBp = nullptr;
+    };
+    std::vector<Setter> setters;
     // generated model (update / threshold / reset as C over s_<name>),
     // compiled with the head kernel by NVRTC at prepare
     std::vector<std::string> gen_names;
@@ -331,6 +337,13 @@ int build_group(bg_net *net, int gid) {
         q.rowptr = c.dRow; q.cols = c.dCols; q.w = c.dW; q.w_bits = c.w_bits; q.d = c.dD;
         q.events = net->dCounters + net->groups.size() + ci;
         q.cring = c.dCRing; q.tnp = c.tnp;
+    }
+    a.nset = (int)g.setters.size();
+    for (int k = 0; k < a.nset; ++k) {
+        const HGroup::Setter &h = g.setters[k];
+        bg::SetDev<T> &d = a.set[k];
+        d.var = h.var; d.mode = h.mode; d.origin = h.origin; d.count = h.count; d.nrows = h.nrows; d.ncols = h.ncols;
+        d.t_init = h.t_init; d.adt = h.adt; d.first = h.first; d.vals = (const T *)h.dVals; d.bp = h.dBp;
     }
     if ((int)g.recs.size() > bg::kMaxRec) return fail(BG_ENOSYS, "too many StateMonitors on one group");
     a.nrec = (int)g.recs.size();
@@ -904,7 +917,7 @@ int build_persist(bg_net *net) {
 
     const HGroup &g = net->groups[0];
     if (!g.linear || g.nvar < 1 || g.nvar > 4 || g.refr || g.period > 0) return BG_OK;
-    if (g.generated() || g.emp_steps > 0) return BG_OK;
+    if (g.generated() || g.emp_steps > 0 || !g.setters.empty()) return BG_OK;
     if (g.thr_kind != BG_THR_CONST && g.thr_kind != BG_THR_VAR && g.thr_kind != BG_THR_NONE) return BG_OK;
     if (net->conns.empty() || (int)net->conns.size() > bg::kPersistMaxPush) return BG_OK;
     int min_d = 255, ndirect = 0;
@@ -1139,6 +1152,32 @@ int bg_group_set_linear(bg_net *n, int32_t gid, const double *A, const double *C
     HGroup &g = n->groups[gid];
     g.linear = true; g.A.assign(A, A + g.nvar * g.nvar);
     g.useC = C != nullptr; if (C) g.C.assign(C, C + g.nvar);
+    return BG_OK;
+}
+
+int bg_group_set_timed_array(bg_net *n, int32_t gid, int var, int64_t origin, int64_t count, const double *values,
+                             int64_t nrows, int64_t ncols, int mode, double t_init, double adt, int64_t first_step,
+                             const int64_t *bp) {
+    if (!gid_ok(n, gid) || !values) return fail(BG_EINVAL, "bg_group_set_timed_array");
+    if (n->prepared) return fail(BG_ESTATE, "network already prepared");
+    HGroup &g = n->groups[gid];
+    if (var < 0 || var >= g.nvar) return fail(BG_EINVAL, "timed array: variable out of range");
+    if (origin < 0 || count < 1 || origin + count > g.n) return fail(BG_EINVAL, "timed array: neuron range");
+    if (nrows < 1 || (ncols != 1 && ncols != count)) return fail(BG_EINVAL, "timed array: shape is (T,) or (T, count)");
+    if (mode != 0 && mode != 1) return fail(BG_EINVAL, "timed array: mode 0 (clock) or 1 (times)");
+    if (mode == 0 && !(adt > 0) ) return fail(BG_EINVAL, "timed array: dt must be positive");
+    if (mode == 1 && nrows > 1 && !bp) return fail(BG_EINVAL, "timed array: breakpoints missing");
+    if ((int)g.setters.size() >= bg::kMaxSet) return fail(BG_ENOSYS, "more than 4 TimedArraySetters on one group");
+    HGroup::Setter h;
+    h.var = var; h.mode = mode; h.origin = origin; h.count = count; h.nrows = nrows; h.ncols = ncols;
+    h.t_init = t_init; h.adt = adt; h.first = first_step;
+    h.vals.assign(values, values + nrows * ncols);
+    if (mode == 1 && nrows > 1) {
+        h.bp.assign(bp, bp + (nrows - 1));
+        for (size_t k = 1; k < h.bp.size(); ++k)
+            if (h.bp[k] < h.bp[k - 1]) return fail(BG_EINVAL, "timed array: breakpoints must ascend");
+    }
+    g.setters.push_back(std::move(h));
     return BG_OK;
 }
 
@@ -1703,6 +1742,20 @@ static int prepare_impl(bg_net *n) {
         if (g.refr && n->alloc(&g.dNext, g.npad * 8) != cudaSuccess) return fail(BG_ENOMEM, "refractory");
         if ((g.period > 0 || g.emp_steps > 0) && n->alloc(&g.dLast, g.npad * 4) != cudaSuccess)
             return fail(BG_ENOMEM, "refractory");
+        for (auto &h : g.setters) {
+            const size_t nv = h.vals.size();
+            if (n->alloc(&h.dVals, nv * ts) != cudaSuccess || n->alloc(&h.dBp, std::max<size_t>(1, h.bp.size()) * 8) != cudaSuccess)
+                return fail(BG_ENOMEM, "timed array");
+            int st;
+            if (ts == 8) st = upload(n, h.dVals, h.vals.data(), nv * 8);
+            else {
+                std::vector<float> f(h.vals.begin(), h.vals.end());
+                st = upload(n, h.dVals, f.data(), nv * 4);
+                if (!st) BG_CUDA(cudaStreamSynchronize(n->stream));
+            }
+            if (st) return st;
+            if (!h.bp.empty()) { st = upload(n, h.dBp, h.bp.data(), h.bp.size() * 8); if (st) return st; }
+        }
         if (!g.gen_steps.empty()) {
             if (n->alloc(&g.dGenSteps, g.gen_steps.size() * 8) != cudaSuccess || n->alloc(&g.dGenIdx, g.gen_idx.size() * 4) != cudaSuccess)
                 return fail(BG_ENOMEM, "generator");
@@ -2504,6 +2557,7 @@ std::string batch_refusal(const bg_net *n) {
     const HGroup &g = n->groups[0];
     if (!g.linear || g.nvar < 1 || g.nvar > 4) return "the group is not linear with 1-4 variables";
     if (g.refr || g.period > 0 || g.emp_steps > 0 || g.generated()) return "refractoriness and generated models are not batched";
+    if (!g.setters.empty()) return "TimedArraySetters are not batched";
     if (g.thr_kind != BG_THR_CONST && g.thr_kind != BG_THR_VAR && g.thr_kind != BG_THR_NONE) return "threshold kind";
     if (g.reset_kind != BG_RESET_NONE && g.reset_kind != BG_RESET_CONST && g.reset_kind != BG_RESET_VAR) return "reset kind";
     if (g.n > bg::kBatchMaxNeurons) return "more than 4096 neurons";

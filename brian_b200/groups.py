@@ -137,6 +137,11 @@ class Refractoriness(Reset):
         self.state = state
 
 
+def _is_timed_array(value):
+    from .timedarray import TimedArray
+    return isinstance(value, TimedArray)
+
+
 # ------------------------------------------------------------ state arrays
 class StateArray(np.ndarray):
     """Array returned by ``G.v``: item assignment writes through to the group."""
@@ -201,12 +206,22 @@ class _GroupBase(EngineBound):
         owner = self.__dict__.get("_owner")
         if owner is not None and not name.startswith("_"):
             key = name[:-1] if name.endswith("_") else name
+            if key in owner.__dict__.get("var_index", {}) and _is_timed_array(value):
+                # G.x = TimedArray(...): a setter (neurongroup.py:645-652)
+                self.set_var_by_array(key, value)
+                return
             if key in owner.__dict__.get("var_index", {}):
                 var = owner.var_index[key]
                 vals = np.broadcast_to(np.asarray(value, dtype=np.float64), (self._n,))
                 self._write_var(var, vals)
                 return
         object.__setattr__(self, name, value)
+
+    def set_var_by_array(self, var, arr, times=None, clock=None, start=None, dt=None):
+        """Set `var` from a TimedArray at the start of every step
+        (neurongroup.py:731-735)."""
+        from .timedarray import set_group_var_by_array
+        return set_group_var_by_array(self, var, arr, times=times, clock=clock, start=start, dt=dt)
 
     def subgroup(self, N):
         if self._next_subgroup + N > self._n:
@@ -278,6 +293,7 @@ class NeuronGroup(_GroupBase):
         # nonlinear model, general string threshold/reset) can still be built:
         # GPUModelFitting takes its model.  Lowering it onto a network raises.
         self._fitting_only = None
+        self._setters = []                 # TimedArraySetters carried by the group
         self._level = level
         # integration scheme of a generated update (None: exact linear)
         self._scheme = None
@@ -437,6 +453,8 @@ class NeuronGroup(_GroupBase):
         if self.eqs is not None and self._names and self._scheme is None:
             A, C = linear_propagator(self.eqs, dt)
             rt.group_set_linear(gid, A, C)
+        for setter in self.__dict__.get("_setters", ()):
+            setter._lower(rt, gid, self, dt)
         th = self._threshold
         gen_thr = isinstance(th, StringThreshold)
         gen_reset = isinstance(self._reset, StringReset)

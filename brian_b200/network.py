@@ -29,6 +29,7 @@ from .connections import Connection, DelayConnection
 from .groups import NeuronGroup, Subgroup, _GroupBase
 from .monitors import SpikeMonitor, StateMonitor, MultiStateMonitor
 from .stdp import ExponentialSTDP, STDP
+from .timedarray import TimedArraySetter
 from .synapses import Synapses
 
 __all__ = ["Network", "MagicNetwork", "run", "reinit", "stop", "clear", "network_operation",
@@ -89,6 +90,7 @@ class _Binding(object):
     """Owns one engine handle and the id maps of the objects lowered onto it."""
 
     def __init__(self, net, table, dt):
+        self.net = net
         self.rt = Runtime(table, device=_PREFS["device"], precision=_PREFS["precision"],
                           deterministic=_PREFS["deterministic"], dt=dt, persistent=_PREFS["persistent"],
                           spin_limit=_PREFS["spin_limit"], check_finite=_PREFS["check_finite"],
@@ -187,6 +189,12 @@ class Network(object):
                 self.synapses.append(o)
             elif isinstance(o, MultiStateMonitor):
                 self.add(*o.contained_objects)
+                continue
+            elif isinstance(o, TimedArraySetter):
+                # an explicitly added setter rides with its group
+                owner = o.group._owner
+                if not any(o is x for x in owner._setters):
+                    owner._setters.append(o)
                 continue
             elif isinstance(o, NetworkOperation):
                 raise NotImplementedError("NetworkOperation objects are not supported on the engine")

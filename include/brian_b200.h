@@ -95,6 +95,18 @@ BG_API int bg_group_add(bg_net *net, int64_t n, int nvar, const double *S0,
  * columns without fused multiply-add. */
 BG_API int bg_group_set_linear(bg_net *net, int32_t gid, const double *A,
                         const double *C);
+/* TimedArraySetter (timedarray.py:238-303; TimedArray.__call__ 209-235):
+ * at the start of every step (clock step cs >= first_step), before the
+ * update, S[var][origin + k] for k < count takes row r of
+ * values[nrows][ncols] (ncols 1: the same value for all, else ncols =
+ * count).  mode 0, an array on a clock grid: r = rint((cs*dt - t_init) /
+ * adt) clamped to [0, nrows); mode 1, an array on explicit ascending times:
+ * r = the number of the nrows-1 breakpoint clock steps bp[] (ascending; bp[i-1]
+ * the first step whose time reaches times[i]) that are <= cs.  At most 4 per
+ * group; groups with one run on the per-step kernels. */
+BG_API int bg_group_set_timed_array(bg_net *net, int32_t gid, int var, int64_t origin, int64_t count,
+                                    const double *values, int64_t nrows, int64_t ncols, int mode,
+                                    double t_init, double adt, int64_t first_step, const int64_t *bp);
 /* Threshold / VariableThreshold (threshold.py:160-191, 373-396). */
 BG_API int bg_group_set_threshold(bg_net *net, int32_t gid, int kind, int var,
                            double value, int var2);

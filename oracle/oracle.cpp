@@ -99,6 +99,12 @@ struct Group {
     int32_t depth = 1;
     int64_t nspikes = 0;
     int32_t emp_steps = 0; std::vector<int64_t> last_spike;
+    /* TimedArraySetters (timedarray.py:238-303): see or_group_set_timed_array */
+    struct Setter {
+        int var, mode; int64_t origin, count, nrows, ncols; double t_init, adt; int64_t first;
+        std::vector<double> vals; std::vector<int64_t> bp;
+    };
+    std::vector<Setter> setters;
     /* generated model: one neuron at a time over S[var * n + i] */
     void (*gen_update)(double *, int64_t, int64_t, double) = nullptr;
     int (*gen_threshold)(const double *, int64_t, int64_t, double) = nullptr;
@@ -191,6 +197,41 @@ int or_group_set_linear(or_net *n, int32_t gid, const double *A, const double *C
     g.useC = C != nullptr; if (C) g.C.assign(C, C + m);
     return OR_OK;
 }
+/* TimedArraySetter: at the start of the step (before every group's update)
+ * S[var][origin + k] = values[r][ncols == 1 ? 0 : k] with r the row of
+ * TimedArray.__call__ (timedarray.py:209-235: int(rint((t - t_init)/dt))
+ * clamped) for an array on a clock (mode 0), or the row the setter's walk
+ * through ascending times reaches (timedarray.py:280-292: the last i with
+ * times[i] <= t), given as the clock steps bp[i-1] at which row i starts
+ * (mode 1). */
+int or_group_set_timed_array(or_net *n, int32_t gid, int var, int64_t origin, int64_t count, const double *values,
+                             int64_t nrows, int64_t ncols, int mode, double t_init, double adt, int64_t first_step,
+                             const int64_t *bp) {
+    if (!gid_ok(n, gid) || !values) return fail(OR_EINVAL, "set_timed_array");
+    Group &g = n->groups[gid];
+    if (var < 0 || var >= g.nvar || origin < 0 || count < 1 || origin + count > g.n || nrows < 1 ||
+        (ncols != 1 && ncols != count) || (mode != 0 && mode != 1) || (mode == 0 && !(adt > 0)) ||
+        (mode == 1 && nrows > 1 && !bp))
+        return fail(OR_EINVAL, "set_timed_array");
+    Group::Setter h;
+    h.var = var; h.mode = mode; h.origin = origin; h.count = count; h.nrows = nrows; h.ncols = ncols;
+    h.t_init = t_init; h.adt = adt; h.first = first_step;
+    h.vals.assign(values, values + nrows * ncols);
+    if (mode == 1 && nrows > 1) h.bp.assign(bp, bp + (nrows - 1));
+    g.setters.push_back(std::move(h));
+    return OR_OK;
+}
+
+static int64_t setter_row(const Group::Setter &h, int64_t cs, double dt) {
+    if (h.mode == 0) {
+        const double x = ((double)cs * dt - h.t_init) / h.adt;
+        if (!(x > 0.0)) return 0;
+        if (x >= (double)(h.nrows - 1)) return h.nrows - 1;
+        return (int64_t)std::nearbyint(x);      /* round half to even, as numpy.rint */
+    }
+    return (int64_t)(std::upper_bound(h.bp.begin(), h.bp.end(), cs) - h.bp.begin());
+}
+
 int or_group_set_threshold(or_net *n, int32_t gid, int kind, int var, double value, int var2) {
     if (!gid_ok(n, gid)) return fail(OR_EINVAL, "set_threshold");
     Group &g = n->groups[gid];
@@ -608,6 +649,14 @@ static void step(or_net *n, int64_t cs) {
     const double dt = n->dt;
     const double t = (double)cs * dt;
     std::vector<int32_t> spk;
+    /* ---- start slot: TimedArraySetters ---- */
+    for (auto &g : n->groups)
+        for (const auto &h : g.setters) {
+            if (cs < h.first) continue;
+            const double *row = &h.vals[(size_t)(setter_row(h, cs, dt) * h.ncols)];
+            double *sv = &g.S[(size_t)h.var * g.n + h.origin];
+            for (int64_t k = 0; k < h.count; ++k) sv[k] = row[h.ncols == 1 ? 0 : k];
+        }
     /* ---- groups slot ---- */
     for (size_t gi = 0; gi < n->groups.size(); ++gi) {
         Group &g = n->groups[gi];
