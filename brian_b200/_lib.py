@@ -109,6 +109,9 @@ ENGINE_ONLY = {
     "mlp_set_data": [_vp, _vp, _vp, _i64],
     "mlp_train": [_vp, ct.c_int, ct.c_int, ct.c_float, _u64, _vp, _P(ct.c_float)],
     "mlp_gradients": [_vp, ct.c_int, _P(ct.c_float), _vp, _vp],
+    "mlp_epoch_order": [_vp, _u64, _i64],
+    "mlp_step_gradients": [_vp, ct.c_int, _i64, _P(ct.c_float), _P(_vp), _P(_i64)],
+    "mlp_apply_gradients": [_vp, _vp, ct.c_float, ct.c_float],
     "gemm_bf16": [_i64, _i64, _i64, _vp, _vp, _vp, _vp],
     "fit_autotune": [_vp, _vp, _P(_i32), _vp],
     "fit_pso_init": [_vp, _i32, _vp, _vp, _vp, _dbl, _dbl, _dbl, _u64],
@@ -714,6 +717,23 @@ MLP_ROWS = (512, 512, 512, 64)
 MLP_COLS = (64, 512, 512, 512)
 
 
+class DeviceVector(object):
+    """A float32 vector in device memory owned by an engine handle, exposed
+    through __cuda_array_interface__ (torch.as_tensor(v, device="cuda")
+    gives a view of it, e.g. for an all-reduce)."""
+
+    def __init__(self, ptr, n, device=0):
+        self.ptr, self.n, self.device = int(ptr), int(n), int(device)
+
+    @property
+    def __cuda_array_interface__(self):
+        return {"shape": (self.n,), "typestr": "<f4", "data": (self.ptr, False), "version": 3, "strides": None}
+
+    def torch(self):
+        import torch
+        return torch.as_tensor(self, device="cuda:%d" % self.device)
+
+
 class MLPHandle(object):
     """The proposal network (bg_mlp_* in include/brian_b200.h)."""
 
@@ -721,6 +741,8 @@ class MLPHandle(object):
         self.t = table if table is not None else product_table()
         self.h = ct.c_void_p()
         self.ydim = ydim
+        self.device = int(device)
+        self.rows = 0
         self.t.check(self.t.mlp_create(ct.byref(self.h), int(device), int(ydim)), "mlp_create")
 
     def close(self):
@@ -764,6 +786,23 @@ class MLPHandle(object):
         X = np.ascontiguousarray(X, dtype=np.float32)
         Y = np.ascontiguousarray(Y, dtype=np.float32)
         self._c(self.t.mlp_set_data(self.h, _ptr(X), _ptr(Y), len(X)), "mlp_set_data")
+        self.rows = len(X)
+
+    # ---- data-parallel steps (bg_mlp_epoch_order / step_gradients / apply_gradients)
+    def epoch_order(self, seed, epoch):
+        self._c(self.t.mlp_epoch_order(self.h, int(seed) & ((1 << 64) - 1), int(epoch)), "mlp_epoch_order")
+
+    def step_gradients(self, batch, row0):
+        """Mean loss of rows [row0, row0+batch) of the epoch order and the
+        flat gradient, a DeviceVector into the handle."""
+        loss, p, n = ct.c_float(), _vp(), _i64()
+        self._c(self.t.mlp_step_gradients(self.h, int(batch), int(row0), ct.byref(loss), ct.byref(p), ct.byref(n)),
+                "mlp_step_gradients")
+        return loss.value, DeviceVector(p.value, n.value, self.device)
+
+    def apply_gradients(self, grad, lr, scale=1.0):
+        ptr = grad.ptr if isinstance(grad, DeviceVector) else int(grad)
+        self._c(self.t.mlp_apply_gradients(self.h, ct.c_void_p(ptr), float(lr), float(scale)), "mlp_apply_gradients")
 
     def train(self, epochs, batch, lr, seed):
         loss = np.zeros(max(1, epochs), dtype=np.float32)

@@ -150,6 +150,7 @@ struct AdamAll {
     int64_t off[2 * kNLayer + 1];
     const int64_t *step;
     float lr, b1, b2, eps;
+    float scale;                   // gradient multiplier (1: exact; 1/ranks after a summing all-reduce)
 };
 __global__ void k_adam_all(const __grid_constant__ AdamAll a) {
     umma::pdl_launch_dependents();
@@ -167,6 +168,7 @@ __global__ void k_adam_all(const __grid_constant__ AdamAll a) {
         const float c1 = 1.f - powf(a.b1, t), c2 = 1.f - powf(a.b2, t);
         float g = 0.f;
         for (int s = 0; s < sg.splits; ++s) g += sg.grad[s * sg.split_stride + i];
+        g *= a.scale;
         const float mi = a.b1 * sg.m[i] + (1.f - a.b1) * g;
         const float vi = a.b2 * sg.v[i] + (1.f - a.b2) * g * g;
         sg.m[i] = mi;
@@ -178,6 +180,23 @@ __global__ void k_adam_all(const __grid_constant__ AdamAll a) {
         sg.Pb[i] = h;
         if (sg.PbT) sg.PbT[(int64_t)c * sg.rows + r] = h;
     }
+}
+
+// The gradient of every tensor as one flat vector in the optimiser's segment
+// order (W0, b0, W1, b1, ...): each entry the sum of its partial slices in
+// the order Adam sums them, so an update from the flat vector (scale 1)
+// equals the fused one.  Data-parallel training all-reduces this vector.
+__global__ void k_grad_flat(const __grid_constant__ AdamAll a, float *flat) {
+    const int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i0 >= a.off[2 * kNLayer]) return;
+    int k = 0;
+#pragma unroll
+    for (int q = 1; q < 2 * kNLayer; ++q) k += i0 >= a.off[q] ? 1 : 0;
+    const AdamSeg &sg = a.seg[k];
+    const int64_t i = i0 - a.off[k];
+    float g = 0.f;
+    for (int s = 0; s < sg.splits; ++s) g += sg.grad[s * sg.split_stride + i];
+    flat[i0] = g;
 }
 
 // One training step's bookkeeping: the batch index within the epoch and the
@@ -387,6 +406,7 @@ struct bg_mlp {
     int64_t nset = 0;
     float *Xall = nullptr, *Yall = nullptr;
     float last_forward_ms = 0;
+    float *gflat = nullptr; int64_t nflat = 0;   // flat gradient (data-parallel steps)
 };
 
 namespace {
@@ -503,8 +523,9 @@ int backward(bg_mlp *h, int B) {
     return BG_OK;
 }
 
-// Adam on every tensor in one launch (the step count is read on the device)
-int adam_all(bg_mlp *h, int B, float lr) {
+// Adam's tensor descriptors: gradients from the partial slices of a batch
+// of B rows, or (flat != null) from a flat gradient vector
+AdamAll adam_desc(bg_mlp *h, int B, float lr, const float *flat, float scale) {
     AdamAll a;
     memset(&a, 0, sizeof a);
     int64_t off = 0;
@@ -527,7 +548,16 @@ int adam_all(bg_mlp *h, int B, float lr) {
     }
     a.off[2 * kNLayer] = off;
     a.step = h->dOptStep;
-    a.lr = lr; a.b1 = 0.9f; a.b2 = 0.999f; a.eps = 1e-8f;
+    a.lr = lr; a.b1 = 0.9f; a.b2 = 0.999f; a.eps = 1e-8f; a.scale = scale;
+    if (flat)
+        for (int k = 0; k < 2 * kNLayer; ++k) { a.seg[k].grad = flat + a.off[k]; a.seg[k].splits = 1; a.seg[k].split_stride = 0; }
+    return a;
+}
+
+// Adam on every tensor in one launch (the step count is read on the device)
+int adam_all(bg_mlp *h, int B, float lr, const float *flat = nullptr, float scale = 1.f) {
+    const AdamAll a = adam_desc(h, B, lr, flat, scale);
+    const int64_t off = a.off[2 * kNLayer];
     MCK(launch_pdl(k_adam_all, dim3((unsigned)((off + 255) / 256)), dim3(256), 0, h->stream, a));
     return BG_OK;
 }
@@ -545,6 +575,30 @@ int train_step(bg_mlp *h, int B, float lr) {
     MCK(launch_pdl(k_step_advance, dim3(1), dim3(1), 0, h->stream, h->dBatchIdx, h->dOptStep));
     if ((rc = adam_all(h, B, lr))) return rc;
     MCK(cudaGetLastError());
+    return BG_OK;
+}
+
+// the epoch order buffers and the sort's scratch, kept for later calls
+int ensure_perm(bg_mlp *h) {
+    if (h->perm) return BG_OK;
+    int rc;
+    if ((rc = dalloc(&h->pkeys, (size_t)h->nset)) || (rc = dalloc(&h->pkeys_out, (size_t)h->nset)) ||
+        (rc = dalloc(&h->pvals, (size_t)h->nset)) || (rc = dalloc(&h->perm, (size_t)h->nset)))
+        return rc;
+    size_t bytes = 0;
+    MCK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, h->pkeys, h->pkeys_out, h->pvals, h->perm, (int)h->nset));
+    MCK(cudaMalloc(&h->sort_tmp, bytes));
+    h->sort_tmp_bytes = bytes;
+    return BG_OK;
+}
+
+// the epoch's order: rows sorted by Philox keys (seed, epoch, row)
+int epoch_perm(bg_mlp *h, uint64_t seed, int64_t ep) {
+    k_perm_keys<<<(unsigned)std::min<int64_t>((h->nset + 255) / 256, 4096), 256, 0, h->stream>>>(
+        seed, ep, h->nset, h->pkeys, h->pvals);
+    MCK(cudaGetLastError());
+    MCK(cub::DeviceRadixSort::SortPairs(h->sort_tmp, h->sort_tmp_bytes, h->pkeys, h->pkeys_out, h->pvals, h->perm,
+                                        (int)h->nset, 0, 64, h->stream));
     return BG_OK;
 }
 
@@ -610,7 +664,7 @@ BG_API int bg_mlp_destroy(bg_mlp *h) {
     for (int l = 0; l < 3; ++l) { dfree(h->H[l]); dfree(h->HT[l]); dfree(h->G[l]); dfree(h->GT[l]); }
     dfree(h->X); dfree(h->XT); dfree(h->dO); dfree(h->dOT); dfree(h->OUT); dfree(h->Y); dfree(h->idx);
     for (int l = 0; l < kNLayer; ++l) dfree(h->cs[l]);
-    dfree(h->gW); dfree(h->loss); dfree(h->err); dfree(h->Xall); dfree(h->Yall);
+    dfree(h->gW); dfree(h->gflat); dfree(h->loss); dfree(h->err); dfree(h->Xall); dfree(h->Yall);
     dfree(h->dBatchIdx); dfree(h->dOptStep); dfree(h->pkeys); dfree(h->pkeys_out); dfree(h->pvals); dfree(h->perm);
     if (h->sort_tmp) cudaFree(h->sort_tmp);
     if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
@@ -714,27 +768,13 @@ BG_API int bg_mlp_train(bg_mlp *h, int epochs, int batch, float lr, uint64_t see
     int rc = ensure_batch(h, batch);
     if (rc) return rc;
     const int64_t steps = h->nset / batch;
-    // the epoch order buffers and the sort's scratch, kept for later calls
-    if (!h->perm) {
-        if ((rc = dalloc(&h->pkeys, (size_t)h->nset)) || (rc = dalloc(&h->pkeys_out, (size_t)h->nset)) ||
-            (rc = dalloc(&h->pvals, (size_t)h->nset)) || (rc = dalloc(&h->perm, (size_t)h->nset)))
-            return rc;
-        size_t bytes = 0;
-        MCK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, h->pkeys, h->pkeys_out, h->pvals, h->perm, (int)h->nset));
-        MCK(cudaMalloc(&h->sort_tmp, bytes));
-        h->sort_tmp_bytes = bytes;
-    }
+    if ((rc = ensure_perm(h))) return rc;
     cudaEvent_t e0, e1;
     MCK(cudaEventCreate(&e0));
     MCK(cudaEventCreate(&e1));
     MCK(cudaEventRecord(e0, h->stream));
     for (int ep = 0; ep < epochs && !rc; ++ep) {
-        // the epoch's order: rows sorted by Philox keys (seed, epoch, row)
-        k_perm_keys<<<(unsigned)std::min<int64_t>((h->nset + 255) / 256, 4096), 256, 0, h->stream>>>(
-            seed, ep, h->nset, h->pkeys, h->pvals);
-        MCK(cudaGetLastError());
-        MCK(cub::DeviceRadixSort::SortPairs(h->sort_tmp, h->sort_tmp_bytes, h->pkeys, h->pkeys_out, h->pvals, h->perm,
-                                            (int)h->nset, 0, 64, h->stream));
+        if ((rc = epoch_perm(h, seed, ep))) break;
         MCK(cudaMemsetAsync(h->loss, 0, sizeof(float), h->stream));
         MCK(cudaMemsetAsync(h->dBatchIdx, 0, sizeof(int64_t), h->stream));
         for (int64_t s = 0; s < steps && !rc; ++s) {
@@ -776,6 +816,63 @@ BG_API int bg_mlp_train(bg_mlp *h, int epochs, int batch, float lr, uint64_t see
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     return rc;
+}
+
+BG_API int bg_mlp_epoch_order(bg_mlp *h, uint64_t seed, int64_t epoch) {
+    if (!h || epoch < 0) return fail(BG_EINVAL, "mlp: bad epoch");
+    if (h->nset <= 0) return fail(BG_ESTATE, "mlp: no training set");
+    MCK(cudaSetDevice(h->device));
+    int rc = ensure_perm(h);
+    if (!rc) rc = epoch_perm(h, seed, epoch);
+    if (!rc) MCK(cudaStreamSynchronize(h->stream));
+    return rc;
+}
+
+BG_API int bg_mlp_step_gradients(bg_mlp *h, int batch, int64_t row0, float *loss, void **grad, int64_t *ngrad) {
+    if (!h || batch < 128 || batch % 128 != 0 || (batch / kSplits) % umma::kKc != 0)
+        return fail(BG_EINVAL, "mlp: batch must be a multiple of 512 (128 rows x 8 batch splits of 64)");
+    if (!h->perm) return fail(BG_ESTATE, "mlp: no epoch order (bg_mlp_epoch_order)");
+    if (row0 < 0 || row0 % batch != 0 || row0 + batch > h->nset) return fail(BG_EINVAL, "mlp: rows outside the epoch");
+    MCK(cudaSetDevice(h->device));
+    int rc = ensure_batch(h, batch);
+    if (rc) return rc;
+    const int64_t nflat = adam_desc(h, batch, 0.f, nullptr, 1.f).off[2 * kNLayer];
+    if (h->nflat != nflat) {
+        if ((rc = dalloc(&h->gflat, (size_t)nflat))) return rc;
+        h->nflat = nflat;
+    }
+    const int64_t bidx = row0 / batch;
+    MCK(cudaMemcpyAsync(h->dBatchIdx, &bidx, sizeof(int64_t), cudaMemcpyHostToDevice, h->stream));
+    MCK(cudaMemsetAsync(h->loss, 0, sizeof(float), h->stream));
+    k_gather_at<<<batch, 64, 0, h->stream>>>(h->Xall, h->Yall, h->perm, h->dBatchIdx, batch, h->ydim, h->X, h->XT, h->Y);
+    if ((rc = forward(h, batch))) return rc;
+    k_nll<<<(batch + 255) / 256, 256, 0, h->stream>>>(h->OUT, h->Y, batch, h->ydim, h->dO, h->dOT,
+                                                       h->cs[kNLayer - 1], h->loss);
+    if ((rc = backward(h, batch))) return rc;
+    const AdamAll a = adam_desc(h, batch, 0.f, nullptr, 1.f);
+    k_grad_flat<<<(unsigned)((nflat + 255) / 256), 256, 0, h->stream>>>(a, h->gflat);
+    MCK(cudaGetLastError());
+    float ls = 0;
+    MCK(cudaMemcpyAsync(&ls, h->loss, sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    MCK(cudaStreamSynchronize(h->stream));
+    if ((rc = check_err(h))) return rc;
+    if (loss) *loss = ls;
+    if (grad) *grad = h->gflat;
+    if (ngrad) *ngrad = nflat;
+    return BG_OK;
+}
+
+BG_API int bg_mlp_apply_gradients(bg_mlp *h, const void *grad, float lr, float scale) {
+    if (!h || !grad) return fail(BG_EINVAL, "mlp: no gradient");
+    if (!h->gflat || h->B <= 0) return fail(BG_ESTATE, "mlp: no step gradients yet");
+    MCK(cudaSetDevice(h->device));
+    // Adam's step count t is the step being taken (1 for the first)
+    MCK(launch_pdl(k_step_advance, dim3(1), dim3(1), 0, h->stream, h->dBatchIdx, h->dOptStep));
+    int rc = adam_all(h, h->B, lr, (const float *)grad, scale);
+    if (rc) return rc;
+    MCK(cudaStreamSynchronize(h->stream));
+    h->step += 1;
+    return BG_OK;
 }
 
 // One forward + backward on the first `n` rows of the training set (no

@@ -553,6 +553,20 @@ BG_API int bg_mlp_set_data(bg_mlp *h, const float *X, const float *Y, int64_t n)
  * [epochs] and gpu_ms (nullable) report the mean loss and device time. */
 BG_API int bg_mlp_train(bg_mlp *h, int epochs, int batch, float lr, uint64_t seed,
                         float *epoch_loss, float *gpu_ms);
+/* Data-parallel training (one bg_mlp per rank, the same training set and
+ * seed on every rank).  bg_mlp_epoch_order draws the epoch's row order
+ * (the order bg_mlp_train uses).  bg_mlp_step_gradients runs forward and
+ * backward on rows [row0, row0 + batch) of that order (row0 a multiple of
+ * batch; batch a multiple of 512) and returns the mean loss and the flat
+ * FP32 gradient of every tensor (W0, b0, W1, b1, ... row-major) as a device
+ * pointer into the handle (*ngrad floats, valid until the next call), for
+ * the caller's all-reduce.  bg_mlp_apply_gradients takes one Adam step from
+ * a device gradient of that layout multiplied by `scale` (1/ranks after a
+ * summing all-reduce).  With one rank these steps equal bg_mlp_train's bit
+ * for bit. */
+BG_API int bg_mlp_epoch_order(bg_mlp *h, uint64_t seed, int64_t epoch);
+BG_API int bg_mlp_step_gradients(bg_mlp *h, int batch, int64_t row0, float *loss, void **grad, int64_t *ngrad);
+BG_API int bg_mlp_apply_gradients(bg_mlp *h, const void *grad, float lr, float scale);
 /* Loss and gradients on the first `batch` training rows without an update
  * (dW[l] [rows][cols], db[l] [rows]; entries may be NULL). */
 BG_API int bg_mlp_gradients(bg_mlp *h, int batch, float *loss, float *const *dW,
