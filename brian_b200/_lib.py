@@ -42,6 +42,9 @@ SIGNATURES = {
     "synapses_add": [_vp, _i32, _i64, _i64, _i32, _i64, _i64, _i64, _vp, _vp, _vp, ct.c_int, _vp, _vp, _vp,
                      _P(_i32)],
     "synapses_set_terms": [_vp, _i32, _vp],
+    "synapses_set_code": [_vp, _i32, _i32, _vp, ct.c_char_p, ct.c_char_p, _i32, _vp, _i32, _vp, _i32, _vp],
+    "synapses_get_var": [_vp, _i32, _i32, _vp],
+    "synapses_set_var": [_vp, _i32, _i32, _vp],
     "stdp_set_update": [_vp, _i32, ct.c_int, ct.c_int, _dbl],
     "stdp_add_delayed": [_vp, _i32, _vp, _dbl, _dbl, _dbl, _dbl, ct.c_int, _i32, _i32, _vp, _vp, _P(_i32)],
     "stdp_get_traces": [_vp, _i32, _vp, _vp],
@@ -405,6 +408,23 @@ class Runtime(object):
                                     _ptr(pre), _ptr(post), _ptr(delay), len(op_var), _ptr(op_var), _ptr(op_sub),
                                     _ptr(terms), ct.byref(sid)), "synapses_add")
         return sid.value
+
+    def synapses_set_code(self, yid, sv, pre_code, post_code, slot_var, writes, pre_var):
+        sv = np.ascontiguousarray(sv, dtype=np.float64)
+        a = lambda v: np.ascontiguousarray(v, dtype=np.int32) if len(v) else None
+        sl, wr, pv = a(slot_var), a(writes), a(pre_var)
+        self._c(self.t.synapses_set_code(self.h, int(yid), int(sv.shape[0]), _ptr(sv) if sv.size else None,
+                                         pre_code.encode(), post_code.encode(), len(slot_var), _ptr(sl), len(writes),
+                                         _ptr(wr), len(pre_var), _ptr(pv)), "synapses_set_code")
+
+    def synapses_get_var(self, yid, k, n):
+        out = np.empty(n, dtype=np.float64)
+        self._c(self.t.synapses_get_var(self.h, int(yid), int(k), _ptr(out)), "synapses_get_var")
+        return out
+
+    def synapses_set_var(self, yid, k, values):
+        values = np.ascontiguousarray(values, dtype=np.float64)
+        self._c(self.t.synapses_set_var(self.h, int(yid), int(k), _ptr(values)), "synapses_set_var")
 
     def synapses_set_terms(self, sid, terms):
         terms = np.ascontiguousarray(terms, dtype=np.float64)

@@ -25,7 +25,7 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
 
 # Headers the network engine compiles again at run time (NVRTC) around a
 # generated model: embedded into bg_rtc_src.cu, which this script writes.
-RTC_HEADERS = ["bg_common.cuh", "bg_kernels.cuh"]
+RTC_HEADERS = ["bg_common.cuh", "bg_expfn.h", "bg_kernels.cuh"]
 RTC_OUT = os.path.join(CSRC, "bg_rtc_src.cu")
 
 

@@ -1223,6 +1223,110 @@ static __global__ void __launch_bounds__(kSynThreads) k_syn_deliver(const SynArg
     bg_finish_step(a.ctl, a.last);
 }
 
+// Synapses with code (plastic synapses, synapses.py:149-330, 400-510): per
+// synapse variables in column order, the presynaptic code run for each event
+// of a target in queue order (the reference's rounds over repeated targets
+// run the whole code for one event of each target per round, so a target
+// sees its events one by one in that order), then the postsynaptic code for
+// every synapse of a target that spiked in this step (the post queue is read
+// after the pre queues).  C is the generated policy: C::pre(x, sv, q, t, pre)
+// and C::post(x, sv, q, t) with x the target's variables (slots), sv the
+// synaptic arrays, q the synapse's column position, pre the source's
+// variables that the code reads.
+constexpr int kSynMaxVars = 8;
+struct SynCodeArgs {
+    DevCtl *ctl;
+    const uint32_t *hist; int depth; int64_t nwords;        // source group's spike history
+    const uint32_t *thist; int tdepth; int64_t tnwords;     // target group's (postsynaptic spikes)
+    int64_t so, to, tn;
+    const int64_t *colptr; const uint32_t *word;
+    double *sv[kSynMaxVars];
+    int nslots; int slot_var[kSynMaxOps];
+    double *S; int64_t npad;                                 // target group state
+    const double *Ssrc; int64_t snpad; int npre; int pre_var[kSynMaxOps];
+    double dt;
+    int has_post;
+    int last;
+};
+template <typename C>
+__device__ __forceinline__ void syn_code_body(const SynCodeArgs &a) {
+    __shared__ uint32_t mask[kSynChunk / 32];
+    const long long nstep = a.ctl->nstep;
+    const double t = (double)(nstep + a.ctl->clock_off) * a.dt;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    constexpr int kWarps = kSynThreads / 32;
+    const int64_t ntiles = (a.tn + kSynTile - 1) / kSynTile;
+    const int row0 = (int)(nstep % a.depth);
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int64_t j0 = tile * kSynTile, j1 = min(a.tn, j0 + kSynTile);
+        const int64_t P0 = a.colptr[j0], P1 = a.colptr[j1];
+        const int64_t j = j0 + tid;
+        const bool own = tid < kSynTile && j < j1;
+        const int64_t q0 = own ? a.colptr[j] : 0, q1 = own ? a.colptr[j + 1] : 0;
+        double x[kSynMaxOps];
+#pragma unroll
+        for (int s = 0; s < kSynMaxOps; ++s)
+            x[s] = (own && q0 < q1 && s < a.nslots) ? a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] : 0.0;
+        bool any = false;
+        for (int64_t c0 = P0; c0 < P1; c0 += kSynChunk) {
+            const int64_t c1 = min(P1, c0 + (int64_t)kSynChunk);
+            const int nw = (int)((c1 - c0 + 31) >> 5);
+            for (int w0 = wid; w0 < nw; w0 += kWarps) {
+                const int64_t p = c0 + (int64_t)w0 * 32 + lane;
+                const uint32_t wd = p < c1 ? a.word[p] : 0u;
+                const int lag = (int)(wd >> 24) - 1;
+                uint32_t hb = 0u;
+                if (lag >= 0 && nstep >= lag) {
+                    const int64_t src = a.so + (int64_t)(wd & 0xFFFFFFu);
+                    int row = row0 - lag;
+                    row += row < 0 ? a.depth : 0;
+                    hb = (a.hist[(int64_t)row * a.nwords + (src >> 5)] >> (src & 31)) & 1u;
+                }
+                const uint32_t m = __ballot_sync(0xffffffffu, hb != 0u);
+                if (lane == 0) mask[w0] = m;
+            }
+            __syncthreads();
+            if (own) {
+                const int64_t lo = max(q0, c0), hi = min(q1, c1);
+                for (int64_t p = lo; p < hi;) {
+                    const int w = (int)((p - c0) >> 5), b = (int)((p - c0) & 31);
+                    const int64_t wend = min(hi, c0 + (int64_t)(w + 1) * 32);
+                    uint32_t m = mask[w] >> b;
+                    const int nb = (int)(wend - p);
+                    if (nb < 32) m &= (1u << nb) - 1u;
+                    while (m) {
+                        const int l = __ffs(m) - 1; m &= m - 1;
+                        const int64_t q = p + l;
+                        any = true;
+                        double pv[kSynMaxOps];
+#pragma unroll
+                        for (int k = 0; k < kSynMaxOps; ++k) {
+                            pv[k] = 0.0;
+                            if (k < a.npre)
+                                pv[k] = a.Ssrc[(int64_t)a.pre_var[k] * a.snpad + a.so + (int64_t)(a.word[q] & 0xFFFFFFu)];
+                        }
+                        C::pre(x, a.sv, q, t, pv);
+                    }
+                    p = wend;
+                }
+            }
+            __syncthreads();
+        }
+        if (own && a.has_post && q0 < q1) {
+            const int64_t tj = a.to + j;
+            const int trow = (int)(nstep % a.tdepth);
+            if ((a.thist[(int64_t)trow * a.tnwords + (tj >> 5)] >> (tj & 31)) & 1u)
+                for (int64_t q = q0; q < q1; ++q) C::post(x, a.sv, q, t);
+        }
+        if (own && any) {
+#pragma unroll
+            for (int s = 0; s < kSynMaxOps; ++s)
+                if (s < a.nslots) a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] = x[s];
+        }
+    }
+    bg_finish_step(a.ctl, a.last);
+}
+
 // Event-driven Synapses delivery.  The events of step t are the synapses of
 // delay d of the sources that spiked at step t - d.  k_syn_gather walks the
 // spike-history words of those steps and appends each event to the bin of

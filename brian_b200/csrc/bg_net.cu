@@ -154,6 +154,13 @@ struct HSyn {
     int *dBinCnt = nullptr; unsigned long long *dBinKey = nullptr; int32_t *dBinQ = nullptr; int *dUsePull = nullptr;
     int32_t *dDoff = nullptr;           // per source, start of each delay in its row (when it fits 256 MB)
     int nbins = 0;
+    // synapses with code (bg_synapses_set_code): synaptic variables [nsv][nsyn]
+    // (synapse order on the host, column order on the device), the generated
+    // pre/post code, the target variables it uses (slots; `writes` those it
+    // assigns) and the source variables it reads
+    bool coded = false; int nsv = 0; std::vector<double> sv; double *dSv = nullptr;
+    std::string pre_code, post_code; std::vector<int32_t> slot_var, pre_var, writes;
+    cudaLibrary_t code_lib = nullptr; cudaKernel_t code_kernel = nullptr;
 };
 struct HSpikeMon {
     int gid; int64_t origin, n; int delay;
@@ -549,8 +556,66 @@ int build_stdp_post(bg_net *net, int sid) {
     return BG_OK;
 }
 
+// The generated kernel of a Synapses object with code: the policy struct
+// (pre and post bodies over X(slot), SV(var), PRE(k), T) around
+// bg::syn_code_body, compiled by NVRTC with the engine's kernel sources.
+int compile_syn_code(HSyn &y) {
+    if (y.code_kernel) return BG_OK;
+    std::string src = "#define BG_GENERATED_MODEL 1\n";
+    for (const char *const *p = kNetRtcSource; *p; ++p) src += *p;
+    src += "namespace bg {\nstruct SynCode {\n"
+           "#define X(s) x_[s]\n#define SV(k) sv_[k][q_]\n#define PRE(k) pre_[k]\n#define T t_\n"
+           "    static __device__ __forceinline__ void pre(double *x_, double *const *sv_, int64_t q_, double t_, const double *pre_) {\n"
+           "        (void)x_; (void)sv_; (void)q_; (void)t_; (void)pre_;\n" + y.pre_code + "\n    }\n"
+           "    static __device__ __forceinline__ void post(double *x_, double *const *sv_, int64_t q_, double t_) {\n"
+           "        (void)x_; (void)sv_; (void)q_; (void)t_;\n" + y.post_code + "\n    }\n"
+           "#undef X\n#undef SV\n#undef PRE\n#undef T\n};\n}  // namespace bg\n"
+           "extern \"C\" __global__ void __launch_bounds__(bg::kSynThreads) bg_syn_code(const bg::SynCodeArgs a) {\n"
+           "    bg::syn_code_body<bg::SynCode>(a);\n}\n";
+    std::vector<char> cubin;
+    std::string log;
+    int rc = bg_nvrtc_compile(src, &cubin, &log);
+    if (rc) return rc;
+    cudaError_t e = cudaLibraryLoadData(&y.code_lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
+    if (e == cudaSuccess) e = cudaLibraryGetKernel(&y.code_kernel, y.code_lib, "bg_syn_code");
+    if (e != cudaSuccess) return fail(BG_ECUDA, std::string("synaptic code kernel: ") + cudaGetErrorString(e));
+    return BG_OK;
+}
+
+int build_syn_code(bg_net *net, int yi) {
+    HSyn &y = net->syns[yi];
+    const HGroup &gs = net->groups[y.src];
+    HGroup &gt = net->groups[y.tgt];
+    int st = compile_syn_code(y);
+    if (st) return st;
+    bg::SynCodeArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.ctl = net->dCtl; a.hist = gs.dHist; a.depth = gs.depth; a.nwords = gs.npad / 32;
+    a.thist = gt.dHist; a.tdepth = gt.depth; a.tnwords = gt.npad / 32;
+    a.so = y.so; a.to = y.to; a.tn = y.tn; a.colptr = y.dColptr; a.word = y.dWord;
+    for (int v = 0; v < y.nsv; ++v) a.sv[v] = y.dSv + (size_t)v * y.nsyn;
+    a.nslots = (int)y.slot_var.size();
+    for (int k = 0; k < a.nslots; ++k) a.slot_var[k] = y.slot_var[k];
+    a.S = (double *)gt.dS; a.npad = gt.npad;
+    a.Ssrc = (const double *)gs.dS; a.snpad = gs.npad; a.npre = (int)y.pre_var.size();
+    for (int k = 0; k < a.npre; ++k) a.pre_var[k] = y.pre_var[k];
+    a.dt = net->dt;
+    a.has_post = y.post_code.empty() ? 0 : 1;
+    const int64_t ntiles = (y.tn + bg::kSynTile - 1) / bg::kSynTile;
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)sm_count() * 8));
+    const cudaKernel_t k = y.code_kernel;
+    net->item_names.push_back("syn_code[y" + std::to_string(yi) + "]");
+    net->step_launches.push_back([a, k, grid](cudaStream_t s, int, int last) {
+        bg::SynCodeArgs b = a; b.last = last;
+        void *args[] = {(void *)&b};
+        return cudaLaunchKernel((const void *)k, dim3(grid), dim3(bg::kSynThreads), args, 0, s);
+    });
+    return BG_OK;
+}
+
 int build_syn(bg_net *net, int yi) {
     HSyn &y = net->syns[yi];
+    if (y.coded) return build_syn_code(net, yi);
     const HGroup &gs = net->groups[y.src];
     HGroup &gt = net->groups[y.tgt];
     bg::SynArgs a;
@@ -1542,6 +1607,54 @@ int bg_synapses_add(bg_net *n, int32_t src_gid, int64_t src_origin, int64_t src_
     return BG_OK;
 }
 
+int bg_synapses_set_code(bg_net *n, int32_t yid, int32_t nsv, const double *sv, const char *pre_code,
+                         const char *post_code, int32_t nslots, const int32_t *slot_var, int32_t nwrites,
+                         const int32_t *writes, int32_t npre, const int32_t *pre_var) {
+    if (!n || yid < 0 || yid >= (int32_t)n->syns.size() || nsv < 0 || nsv > bg::kSynMaxVars || nslots < 0 ||
+        nslots > bg::kSynMaxOps || npre < 0 || npre > bg::kSynMaxOps || nwrites < 0 || nwrites > nslots ||
+        (nslots && !slot_var) || (npre && !pre_var) || (nwrites && !writes))
+        return fail(BG_EINVAL, "bg_synapses_set_code");
+    if (n->prepared) return fail(BG_ESTATE, "network already prepared");
+    HSyn &y = n->syns[yid];
+    if (y.nops) return fail(BG_EINVAL, "Synapses with code take no separate statements");
+    const HGroup &gs = n->groups[y.src], &gt = n->groups[y.tgt];
+    for (int k = 0; k < nslots; ++k) if (slot_var[k] < 0 || slot_var[k] >= gt.nvar) return fail(BG_EINVAL, "target variable");
+    for (int k = 0; k < nwrites; ++k) if (writes[k] < 0 || writes[k] >= gt.nvar) return fail(BG_EINVAL, "target variable");
+    for (int k = 0; k < npre; ++k) if (pre_var[k] < 0 || pre_var[k] >= gs.nvar) return fail(BG_EINVAL, "source variable");
+    y.coded = true; y.nsv = nsv;
+    if (sv) y.sv.assign(sv, sv + (size_t)nsv * y.nsyn);
+    else y.sv.assign((size_t)nsv * y.nsyn, 0.0);
+    y.pre_code = pre_code ? pre_code : ""; y.post_code = post_code ? post_code : "";
+    y.slot_var.assign(slot_var, slot_var + nslots); y.writes.assign(writes, writes + nwrites);
+    y.pre_var.assign(pre_var, pre_var + npre);
+    return BG_OK;
+}
+
+int bg_synapses_get_var(bg_net *n, int32_t yid, int32_t k, double *out) {
+    if (!n || yid < 0 || yid >= (int32_t)n->syns.size() || !out) return fail(BG_EINVAL, "bg_synapses_get_var");
+    HSyn &y = n->syns[yid];
+    if (!y.coded || k < 0 || k >= y.nsv) return fail(BG_EINVAL, "synaptic variable");
+    if (!n->prepared || y.nsyn == 0) { std::copy(y.sv.begin() + (size_t)k * y.nsyn, y.sv.begin() + (size_t)(k + 1) * y.nsyn, out); return BG_OK; }
+    std::vector<double> col(y.nsyn);
+    BG_CUDA(cudaStreamSynchronize(n->stream));
+    BG_CUDA(cudaMemcpy(col.data(), y.dSv + (size_t)k * y.nsyn, y.nsyn * 8, cudaMemcpyDeviceToHost));
+    for (int64_t p = 0; p < y.nsyn; ++p) out[y.perm[p]] = col[p];
+    return BG_OK;
+}
+
+int bg_synapses_set_var(bg_net *n, int32_t yid, int32_t k, const double *in) {
+    if (!n || yid < 0 || yid >= (int32_t)n->syns.size() || !in) return fail(BG_EINVAL, "bg_synapses_set_var");
+    HSyn &y = n->syns[yid];
+    if (!y.coded || k < 0 || k >= y.nsv) return fail(BG_EINVAL, "synaptic variable");
+    std::copy(in, in + y.nsyn, y.sv.begin() + (size_t)k * y.nsyn);
+    if (!n->prepared || y.nsyn == 0) return BG_OK;
+    std::vector<double> col(y.nsyn);
+    for (int64_t p = 0; p < y.nsyn; ++p) col[p] = in[y.perm[p]];
+    BG_CUDA(cudaStreamSynchronize(n->stream));
+    BG_CUDA(cudaMemcpy(y.dSv + (size_t)k * y.nsyn, col.data(), y.nsyn * 8, cudaMemcpyHostToDevice));
+    return BG_OK;
+}
+
 // Upload the statements' terms in column order (from `terms` in synapse
 // order, or from the stored copy when null).
 static int bg_synapses_set_terms_impl(bg_net *n, int yi, const double *terms) {
@@ -1715,10 +1828,14 @@ static int prepare_impl(bg_net *n) {
     // head kernel, after the Synapses kernel: refuse targets fed by both
     for (const auto &y : n->syns)
         for (const auto &c : n->conns)
-            if (c.hetero && c.tgt == y.tgt && c.to < y.to + y.tn && y.to < c.to + c.tn)
+            if (c.hetero && c.tgt == y.tgt && c.to < y.to + y.tn && y.to < c.to + c.tn) {
                 for (int v : y.op_var)
                     if (v == c.var)
                         return fail(BG_ENOSYS, "a variable fed by both a DelayConnection and Synapses");
+                for (int v : y.writes)
+                    if (v == c.var)
+                        return fail(BG_ENOSYS, "a variable fed by both a DelayConnection and Synapses");
+            }
     // chunk length bounded by monitor buffer sizes
     int64_t chunk = kChunkSteps;
     for (auto &m : n->smons) chunk = std::min<int64_t>(chunk, std::max<int64_t>(kGraphSteps, (int64_t)(1 << 25) / std::max<int64_t>(1, m.n)));
@@ -1898,6 +2015,16 @@ static int prepare_impl(bg_net *n) {
             return fail(BG_ENOMEM, "synapses");
         int st = upload(n, y.dColptr, y.colptr.data(), (y.tn + 1) * 8); if (st) return st;
         if (y.nsyn) { st = upload(n, y.dWord, y.word.data(), y.nsyn * 4); if (st) return st; }
+        if (y.coded) {
+            y.events = false;                   // the code runs on the pull's per-target walk
+            if (n->alloc(&y.dSv, std::max<int64_t>(1, (int64_t)y.nsv * y.nsyn) * 8) != cudaSuccess)
+                return fail(BG_ENOMEM, "synaptic variables");
+            std::vector<double> col((size_t)y.nsv * y.nsyn);
+            for (int v = 0; v < y.nsv; ++v)
+                for (int64_t p = 0; p < y.nsyn; ++p) col[(size_t)v * y.nsyn + p] = y.sv[(size_t)v * y.nsyn + y.perm[p]];
+            if (!col.empty()) { st = upload(n, y.dSv, col.data(), col.size() * 8); if (st) return st; }
+            BG_CUDA(cudaStreamSynchronize(n->stream));
+        }
         // the event path pays off once the pull's synapse words no longer
         // stay in L2 (it reads every word every step); below that the pull
         // is cheaper than the event path's extra launches
@@ -2231,6 +2358,7 @@ template <typename F> void visit_state(bg_net *n, F &&f) {
         f.devbuf(st.delayed ? st.dHpre : nullptr, st.delayed ? (size_t)st.hlen * c.sn * 8 : 0, "trace records");
         f.devbuf(st.delayed ? st.dHpost : nullptr, st.delayed ? (size_t)st.hlen * c.tn * 8 : 0, "trace records");
     }
+    for (auto &y : n->syns) f.devbuf(y.coded ? y.dSv : nullptr, y.coded ? (size_t)y.nsv * y.nsyn * 8 : 0, "synaptic variables");
     for (auto &m : n->smons) { f.hostvec(m.steps); f.hostvec(m.idx); }
     for (auto &m : n->stmons) { f.hostvec(m.vals); f.hostvec(m.steps); f.hostval(m.rows_done); }
 }

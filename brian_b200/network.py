@@ -117,6 +117,12 @@ class _Binding(object):
     def write_synapse_terms(self, y, terms):
         self.rt.synapses_set_terms(self.yids[y], terms)
 
+    def read_synapse_var(self, y, k):
+        return self.rt.synapses_get_var(self.yids[y], k, len(y))
+
+    def write_synapse_var(self, y, k, values):
+        self.rt.synapses_set_var(self.yids[y], k, values)
+
     def read_traces(self, s):
         return self.rt.stdp_get_traces(self.sids[s], len(s.C.source), len(s.C.target))
 
@@ -144,6 +150,7 @@ class _Binding(object):
                 o._traces()
                 o._binding = None
             elif isinstance(o, Synapses):
+                o._sync_vars()
                 o._binding = None
             elif isinstance(o, (SpikeMonitor, StateMonitor)):
                 o._archive()

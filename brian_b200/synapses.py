@@ -1,15 +1,25 @@
-"""Synapses (synapses/synapses.py:43-1058 of Brian 1.4.4) with static
-synaptic variables and presynaptic code that adds to postsynaptic variables.
+"""Synapses (synapses/synapses.py:43-1058 of Brian 1.4.4).
 
 What runs on the engine:
 
-* ``model``: declarations of static synaptic variables (``w : 1``,
-  ``w : volt``); synaptic differential equations and event-driven code
-  raise NotImplementedError.
-* ``pre``: one code string whose lines are ``x += e`` or ``x -= e`` with
-  ``x`` a variable of the target group (optionally ``x_post``) and ``e`` a
-  synaptic variable, a constant, a product of both or its negation.
-  ``post`` code and lists of ``pre`` codes raise NotImplementedError.
+* ``model``: static synaptic variables (``w : 1``, ``w : volt``) and
+  event-driven linear equations (``dApre/dt = -Apre/taupre : 1
+  (event-driven)``, any ``a*x + b`` with constant a, b), whose exact
+  solution is applied at each event before the code, with ``lastupdate``
+  set to t after it (synapses.py:179-187, 257-296).  Clock-driven synaptic
+  equations raise NotImplementedError.
+* ``pre``: one code string.  Lines ``x += e`` / ``x -= e`` adding a
+  synaptic variable, a constant or their product to a postsynaptic
+  variable run on the engine's static kernels; anything else (assignments
+  and ``+= -= *= /=`` of synaptic or postsynaptic variables, expressions
+  with ``clip``, ``exp``, ``abs``, ``sqrt``, ``t``, ``x_pre`` reads) is
+  compiled into a generated kernel, which runs the whole code for each
+  event of a target in queue order.
+* ``post``: one code string changing synaptic variables, run for every
+  synapse of a target that spiked in the step, after the presynaptic
+  events (the post queue, delay 0).  Lists of several codes raise
+  NotImplementedError, as do postsynaptic codes that change neuron
+  variables.
 * Synapse creation as the reference's ``S[i, j] = True | int | float |
   'condition'`` (synapses.py:583-723), ``connect_random`` and
   ``connect_one_to_one``; synapse indices are allocated in the same order
@@ -29,7 +39,9 @@ by the engine (it adds the connection's due row after the Synapses, the
 reference before).  The reference applies repeated targets
 in rounds over numpy's default (unstable) argsort (synapses.py:502-516),
 which orders ties by numpy's sort implementation; queue order is the order
-a stable sort gives.
+a stable sort gives.  ``exp`` in generated synaptic code is the engine's
+own ``bg_exp`` (csrc/bg_expfn.h), the same operations on the GPU and in
+the CPU restatement, within one ulp of the C library's exp.
 """
 import ast
 import re
@@ -41,6 +53,16 @@ from ._lib import EngineBound
 from .groups import NeuronGroup, Subgroup
 
 __all__ = ["Synapses"]
+
+
+def _split(code):
+    """Statements of a code string, one per line or ';'."""
+    out = []
+    for ln in code.replace(";", "\n").split("\n"):
+        ln = ln.split("#", 1)[0].strip()
+        if ln:
+            out.append(ln)
+    return out
 
 
 def _flat(code):
@@ -89,7 +111,12 @@ class _SynapticVariable(object):
         self._S, self._name = S, name
 
     def _get(self):
-        return self._S._vars[self._name]
+        S = self._S
+        b = S.__dict__.get("_binding")
+        if b is not None and S._coded:
+            # a variable the synaptic code changes lives on the engine
+            S._vars[self._name] = b.read_synapse_var(S, S._names.index(self._name))
+        return S._vars[self._name]
 
     def __array__(self, dtype=None, copy=None):
         a = self._get()
@@ -106,8 +133,9 @@ class _SynapticVariable(object):
         idx = S._synapse_index(key)
         if isinstance(value, str):
             value = S._eval_string(value, idx)
+        self._get()
         S._vars[self._name][idx] = np.asarray(value, dtype=np.float64)
-        S._changed()
+        S._changed(var=self._name)
 
 
 class _SynapticDelay(_SynapticVariable):
@@ -133,8 +161,10 @@ class Synapses(EngineBound):
         target = target or source
         if source.clock is not target.clock:
             raise ValueError("Source and target groups must have the same clock")
-        if post is not None:
-            raise NotImplementedError("postsynaptic code of Synapses is not run by the engine")
+        if isinstance(post, (list, tuple)):
+            if len(post) != 1:
+                raise NotImplementedError("several postsynaptic codes are not run by the engine")
+            post = post[0]
         if isinstance(pre, (list, tuple)):
             if len(pre) != 1:
                 raise NotImplementedError("several presynaptic codes are not run by the engine")
@@ -148,32 +178,199 @@ class Synapses(EngineBound):
         ns = _caller_namespace(level)
         if code_namespace:
             ns.update(code_namespace)
-        self._names = self._parse_model(model or "")
+        self._names, self._ed = self._parse_model(model or "", ns)
+        # lastupdate (synapses.py:179-187): with event-driven variables or
+        # when a code names it; set to t after each pre and post code
+        uses_lu = re.search(r"\blastupdate\b", (pre or "") + "\n" + (post or "")) is not None
+        if self._ed or uses_lu:
+            self._names.append("lastupdate")
         for n in self._names:
             self._vars[n] = np.zeros(0)
         self.presynaptic = np.zeros(0, dtype=np.int64)
         self.postsynaptic = np.zeros(0, dtype=np.int64)
         self._delay = np.zeros(0, dtype=np.int16)
-        self._ops = self._parse_pre(pre or "", ns)
+        self._coded = bool(post) or bool(self._ed) or uses_lu
+        self._ops = []
+        if not self._coded:
+            try:
+                self._ops = self._parse_pre(pre or "", ns)
+            except NotImplementedError:
+                self._coded = True
+        self._code = self._generate(pre or "", post or "", ns) if self._coded else None
         self._binding = None
         self._iscompressed = False
 
     # ---------------------------------------------------------------- model
-    def _parse_model(self, model):
-        names = []
+    def _parse_model(self, model, ns):
+        """Static variables ('w : unit') and event-driven linear equations
+        ('dx/dt = a*x + b : unit (event-driven)', a and b constants), whose
+        exact solution is applied at each event (synapses.py:257-296):
+        x = -b/a + exp(a (t - lastupdate)) (x + b/a), or x + b (t -
+        lastupdate) for a = 0.  Returns the names and [(name, a, b)]."""
+        names, ed = [], []
         for line in _flat(model):
             line = line.split("#")[0].strip()
             if not line:
                 continue
+            m = re.match(r"^d(\w+)\s*/\s*dt\s*=\s*(.+?)\s*:\s*([^()]*?)\s*\(\s*event-driven\s*\)\s*$", line)
+            if m:
+                var, rhs = m.group(1), m.group(2)
+                ed.append((var,) + self._affine(var, rhs, ns, line))
+                names.append(var)
+                continue
             m = re.match(r"^(\w+)\s*:\s*[\w\s\*/\.]+$", line)
             if not m or "=" in line:
-                raise NotImplementedError("only static synaptic variables ('w : unit') are run by the engine: %r"
-                                          % line)
+                raise NotImplementedError("synaptic equations other than static variables and event-driven "
+                                          "linear equations are not run by the engine: %r" % line)
             names.append(m.group(1))
         for n in names:
             if n in ("delay", "delay_pre", "delay_post", "lastupdate"):
                 raise NotImplementedError("synaptic variable %r" % n)
-        return names
+        return names, ed
+
+    @staticmethod
+    def _affine(var, rhs, ns, line):
+        """(a, b) of rhs = a*var + b, from rhs at var = 0 and var = 1 (the
+        reference's AffineFunction test, synapses.py:262-273)."""
+        tree = ast.parse(rhs, mode="eval")
+        env = {}
+        for node in ast.walk(tree):
+            if isinstance(node, ast.Name) and node.id != var:
+                v = ns.get(node.id)
+                if not (np.isscalar(v) and isinstance(v, (int, float, np.integer, np.floating))):
+                    raise TypeError("Cannot turn equation for %s into event-driven code: %r" % (var, line))
+                env[node.id] = float(v)
+        code = compile(tree, "<event-driven>", "eval")
+        f = lambda x: float(eval(code, {"__builtins__": {}}, dict(env, **{var: x})))
+        b = f(0.0)
+        a = f(1.0) - b
+        if abs(f(2.0) - (2.0 * a + b)) > 1e-9 * max(1.0, abs(a), abs(b)):
+            raise TypeError("Cannot turn equation for %s into event-driven code: %r" % (var, line))
+        return a, b
+
+    def _generate(self, pre, post, ns):
+        """C bodies of the pre and post codes for the engine (over X(slot),
+        SV(var), PRE(k), T): the event-driven updates, the code's
+        statements in order, then lastupdate = t.  Returns (pre, post,
+        target variables of the slots, the written ones, source
+        variables)."""
+        from .codegen import _Emitter, CodegenError
+        tvars = self.target._owner.var_index
+        svars = self.source._owner.var_index
+        slots, writes, pres = [], [], []
+
+        def slot(var):
+            if var not in slots:
+                if len(slots) == 4:
+                    raise NotImplementedError("synaptic code using more than four postsynaptic variables")
+                slots.append(var)
+            return "X(%d)" % slots.index(var)
+
+        def pre_slot(var):
+            if var not in pres:
+                if len(pres) == 4:
+                    raise NotImplementedError("synaptic code reading more than four presynaptic variables")
+                pres.append(var)
+            return "PRE(%d)" % pres.index(var)
+
+        def resolve(name):
+            if name in self._names:
+                return "SV(%d)" % self._names.index(name)
+            if name == "t":
+                return "T"
+            if name.endswith("_post") and name[:-5] in tvars and isinstance(name[:-5], str):
+                return slot(name[:-5])
+            if name.endswith("_pre") and name[:-4] in svars and isinstance(name[:-4], str):
+                return pre_slot(name[:-4])
+            if name in tvars and isinstance(name, str):
+                return slot(name)
+            return None
+
+        class _SynEmitter(_Emitter):
+            def expr(self, node):
+                if isinstance(node, ast.Call) and isinstance(node.func, ast.Name) and not node.keywords:
+                    f, args = node.func.id, node.args
+                    if f == "clip" and len(args) == 3:
+                        return "bg_clip(%s, %s, %s)" % tuple(self.expr(x) for x in args)
+                    if f == "exp" and len(args) == 1:
+                        return "bg_exp(%s)" % self.expr(args[0])
+                    if f in ("abs", "fabs") and len(args) == 1:
+                        return "fabs(%s)" % self.expr(args[0])
+                    if f == "sqrt" and len(args) == 1:
+                        return "sqrt(%s)" % self.expr(args[0])
+                    raise CodegenError("function %r in synaptic code" % f)
+                return _Emitter.expr(self, node)
+
+            def power(self, node):
+                out = _Emitter.power(self, node)
+                if out.startswith("pow("):
+                    raise CodegenError("powers other than 2, 1, 0.5 and -1 in synaptic code")
+                return out
+
+        def emitter(code):
+            names = {}
+            for line in _split(code):
+                for node in ast.walk(ast.parse(line, mode="exec")):
+                    if isinstance(node, ast.Name):
+                        c = resolve(node.id)
+                        if c is not None:
+                            names[node.id] = c
+            return _SynEmitter("double", names, ns)
+
+        def body(code, is_post):
+            em = emitter(code)
+            out = []
+            lu = self._names.index("lastupdate") if "lastupdate" in self._names else None
+            for var, a, b in self._ed:
+                v = "SV(%d)" % self._names.index(var)
+                dt_ = "(T - SV(%d))" % lu
+                if a == 0.0:
+                    out.append("%s = (%s + (%s * %s));" % (v, v, em.literal(b), dt_))
+                elif b == 0.0:
+                    out.append("%s = (%s * bg_exp((%s * %s)));" % (v, v, em.literal(a), dt_))
+                else:
+                    out.append("%s = (%s + (bg_exp((%s * %s)) * (%s + %s)));"
+                               % (v, em.literal(-b / a), em.literal(a), dt_, v, em.literal(b / a)))
+            for line in _split(code):
+                st = ast.parse(line, mode="exec").body
+                if len(st) != 1:
+                    raise NotImplementedError("synaptic statement %r" % line)
+                st = st[0]
+                if isinstance(st, ast.Assign) and len(st.targets) == 1 and isinstance(st.targets[0], ast.Name):
+                    name, value = st.targets[0].id, None
+                elif isinstance(st, ast.AugAssign) and isinstance(st.target, ast.Name):
+                    name, value = st.target.id, st.op
+                else:
+                    raise NotImplementedError("synaptic statement %r" % line)
+                if name.endswith("_pre") and name[:-4] in svars:
+                    raise ValueError('The synaptic code "%s" changes the value of a pre-synaptic variable.' % line)
+                lhs = resolve(name)
+                if lhs is None or lhs == "T" or lhs.startswith("PRE"):
+                    raise NotImplementedError("synaptic code assigns %r: %r" % (name, line))
+                if lhs.startswith("X("):
+                    if is_post:
+                        raise NotImplementedError("postsynaptic code that changes a neuron variable: %r" % line)
+                    var = tvars[name[:-5] if name.endswith("_post") else name]
+                    if var not in writes:
+                        writes.append(var)
+                try:
+                    rhs = em.expr(st.value)
+                except CodegenError as e:
+                    raise NotImplementedError("synaptic code %r: %s" % (line, e))
+                if value is None:
+                    out.append("%s = %s;" % (lhs, rhs))
+                else:
+                    ops = {ast.Add: "+", ast.Sub: "-", ast.Mult: "*", ast.Div: "/"}
+                    if type(value) not in ops:
+                        raise NotImplementedError("synaptic statement %r" % line)
+                    out.append("%s = (%s %s %s);" % (lhs, lhs, ops[type(value)], rhs))
+            if lu is not None:
+                out.append("SV(%d) = T;" % lu)
+            return "\n".join("        " + x for x in out)
+
+        pre_c = body(pre, False)
+        post_c = body(post, True) if post.strip() else ""
+        return pre_c, post_c, [int(tvars[v]) for v in slots], [int(w) for w in writes], [int(svars[v]) for v in pres]
 
     def _parse_pre(self, pre, ns):
         """Lines 'x += e' / 'x -= e' -> (target var index, subtract, synaptic
@@ -441,13 +638,29 @@ class Synapses(EngineBound):
             object.__setattr__(self, name, value)
 
     # ------------------------------------------------------------- lowering
-    def _changed(self, delays=False):
+    def _changed(self, delays=False, var=None):
         b = self.__dict__.get("_binding")
         if b is None:
             return
         if delays:
             raise NotImplementedError("changing synapses or delays after the first run is not supported")
+        if self._coded:
+            if var is not None:
+                b.write_synapse_var(self, self._names.index(var), self._vars[var])
+            return
         b.write_synapse_terms(self, self._terms())
+
+    def _sync_vars(self):
+        """Synaptic variables the engine holds, into the host copies."""
+        b = self.__dict__.get("_binding")
+        if b is not None and self._coded:
+            for k, n in enumerate(self._names):
+                self._vars[n] = b.read_synapse_var(self, k)
+
+    def _host_state(self, d):
+        if self._coded:
+            self._sync_vars()
+            d["_vars"] = {n: v.copy() for n, v in self._vars.items()}
 
     def _terms(self):
         """Per statement and synapse, the value added or subtracted:
@@ -479,6 +692,15 @@ class Synapses(EngineBound):
         self._queue_check()
         src, tgt = self.source._owner, self.target._owner
         ops = self._ops
+        if self._coded:
+            sid = rt.synapses_add(gids[src], self.source._origin, len(self.source), gids[tgt], self.target._origin,
+                                  len(self.target), self.presynaptic, self.postsynaptic, self._delay, [], [],
+                                  np.zeros((0, len(self))))
+            pre_c, post_c, slots, writes, pres = self._code
+            sv = np.array([self._vars[n] for n in self._names], dtype=np.float64).reshape(len(self._names), len(self))
+            rt.synapses_set_code(sid, sv, pre_c, post_c, slots, writes, pres)
+            self._iscompressed = True
+            return sid
         sid = rt.synapses_add(gids[src], self.source._origin, len(self.source), gids[tgt], self.target._origin,
                               len(self.target), self.presynaptic, self.postsynaptic, self._delay,
                               [o[0] for o in ops], [1 if o[1] else 0 for o in ops], self._terms())

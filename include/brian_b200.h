@@ -200,6 +200,23 @@ BG_API int bg_synapses_add(bg_net *net, int32_t src_gid, int64_t src_origin,
 /* New statement terms ([nops][nsyn], synapse order), e.g. after S.w[:] = ...
  * (synapticvariable.py __setitem__) between runs. */
 BG_API int bg_synapses_set_terms(bg_net *net, int32_t sid, const double *terms);
+/* Synapses with code (synapses.py:149-330, 400-510): nsv synaptic
+ * variables (initial values sv[nsv][nsyn], synapse order; NULL: zeros), a
+ * presynaptic code run for every event of a target in queue order and a
+ * postsynaptic code run for every synapse of a target that spiked in the
+ * step, after the events (the post queue, delay 0), both in the 'synapses'
+ * slot.  The codes are C statement lists over X(s) (target variable
+ * slot_var[s]), SV(k) (synaptic variable k), PRE(k) (source variable
+ * pre_var[k], read only), T (the time), bg_exp and bg_clip (identical on
+ * the GPU and in the CPU restatement); `writes` lists the target variables
+ * the codes assign.  Replaces the statement terms of bg_synapses_add (nops
+ * must be 0); before prepare. */
+BG_API int bg_synapses_set_code(bg_net *net, int32_t sid, int32_t nsv, const double *sv, const char *pre_code,
+                                const char *post_code, int32_t nslots, const int32_t *slot_var, int32_t nwrites,
+                                const int32_t *writes, int32_t npre, const int32_t *pre_var);
+/* Synaptic variable k of a Synapses with code, in synapse order. */
+BG_API int bg_synapses_get_var(bg_net *net, int32_t sid, int32_t k, double *out);
+BG_API int bg_synapses_set_var(bg_net *net, int32_t sid, int32_t k, const double *in);
 
 /* ExponentialSTDP on a sparse DelayConnection (stdp.py:296-368, replacing
  * the STDPUpdater / DelayedSTDPUpdater pair and the two RecentStateMonitors

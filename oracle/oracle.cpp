@@ -149,6 +149,13 @@ struct Syn {
     int nops; std::vector<int32_t> op_var, op_sub; std::vector<double> terms;   /* [nops][nsyn] */
     std::vector<std::vector<int32_t>> syn_of_pre;                               /* ascending */
     int32_t L = 1; int64_t cur = 0; std::vector<std::vector<int32_t>> X;
+    /* synapses with code (or_synapses_set_code): synaptic variables
+     * [nsv][nsyn] in synapse order, the compiled pre/post codes, the target
+     * variables they use (slots) and the source variables they read */
+    bool coded = false; int nsv = 0; std::vector<double> sv;
+    std::vector<int32_t> slot_var, pre_var; std::vector<std::vector<int32_t>> syn_of_post;
+    void (*sc_pre)(double *, double *const *, int64_t, double, const double *) = nullptr;
+    void (*sc_post)(double *, double *const *, int64_t, double) = nullptr;
 };
 struct SpikeMon { int32_t gid; int64_t origin, n; int32_t delay; std::vector<int64_t> steps; std::vector<int32_t> idx; };
 struct StateMon { int32_t gid; int var; std::vector<int32_t> idx; int32_t timestep; int64_t start;
@@ -481,11 +488,100 @@ int or_synapses_set_terms(or_net *n, int32_t sid, const double *terms) {
     std::copy(terms, terms + (size_t)y.nops * y.nsyn, y.terms.begin());
     return OR_OK;
 }
+/* Synapses with code: the codes are C statements over X(s), SV(k), PRE(k)
+ * and T (the engine compiles the same text for the GPU), compiled here with
+ * gcc (no contraction) next to the library and loaded.  bg_exp / bg_clip
+ * come from the engine's bg_expfn.h so both sides run the same operations. */
+int or_synapses_set_code(or_net *n, int32_t sid, int32_t nsv, const double *sv, const char *pre_code,
+                         const char *post_code, int32_t nslots, const int32_t *slot_var, int32_t nwrites,
+                         const int32_t *writes, int32_t npre, const int32_t *pre_var) {
+    (void)writes;
+    if (!n || sid < 0 || sid >= (int32_t)n->syns.size() || nsv < 0 || nsv > 8 || nslots < 0 || nslots > 4 ||
+        npre < 0 || npre > 4 || nwrites < 0 || nwrites > nslots)
+        return fail(OR_EINVAL, "synapses_set_code");
+    if (n->prepared) return fail(OR_ESTATE, "network already prepared");
+    Syn &y = n->syns[sid];
+    if (y.nops) return fail(OR_EINVAL, "Synapses with code take no separate statements");
+    y.coded = true; y.nsv = nsv;
+    if (sv) y.sv.assign(sv, sv + (size_t)nsv * y.nsyn); else y.sv.assign((size_t)nsv * y.nsyn, 0.0);
+    y.slot_var.assign(slot_var, slot_var + nslots); y.pre_var.assign(pre_var, pre_var + npre);
+    y.syn_of_post.assign(y.tn, std::vector<int32_t>());
+    for (int64_t k = 0; k < y.nsyn; ++k) y.syn_of_post[y.post[k]].push_back((int32_t)k);
+    Dl_info info;
+    if (!dladdr((void *)&or_synapses_set_code, &info) || !info.dli_fname) return fail(OR_ESTATE, "dladdr");
+    std::string here = info.dli_fname;
+    here = here.substr(0, here.find_last_of('/'));
+    const std::string dir = here + "/_ref/gen";
+    std::string c = "#include <math.h>\n#include <stdint.h>\n#include \"" + here + "/../brian_b200/csrc/bg_expfn.h\"\n"
+                    "#define X(s) x_[s]\n#define SV(k) sv_[k][q_]\n#define PRE(k) pre_[k]\n#define T t_\n"
+                    "void sc_pre(double *x_, double *const *sv_, int64_t q_, double t_, const double *pre_) {\n"
+                    "    (void)x_; (void)sv_; (void)q_; (void)t_; (void)pre_;\n" + std::string(pre_code ? pre_code : "") +
+                    "\n}\nvoid sc_post(double *x_, double *const *sv_, int64_t q_, double t_) {\n"
+                    "    (void)x_; (void)sv_; (void)q_; (void)t_;\n" + std::string(post_code ? post_code : "") + "\n}\n";
+    static int counter = 0;
+    const std::string stem = dir + "/syn_" + std::to_string((long long)getpid_or()) + "_" + std::to_string(counter++);
+    if (std::system(("mkdir -p '" + dir + "'").c_str()) != 0) return fail(OR_ESTATE, "mkdir " + dir);
+    FILE *f = std::fopen((stem + ".c").c_str(), "w");
+    if (!f) return fail(OR_ESTATE, "cannot write " + stem + ".c");
+    std::fputs(c.c_str(), f);
+    std::fclose(f);
+    const std::string cmd = "gcc -O2 -ffp-contract=off -fno-fast-math -shared -fPIC -w -o '" + stem + ".so' '" + stem + ".c' -lm";
+    if (std::system(cmd.c_str()) != 0) return fail(OR_ESTATE, "gcc failed on the synaptic code: " + stem + ".c");
+    void *h = dlopen((stem + ".so").c_str(), RTLD_NOW | RTLD_LOCAL);
+    std::remove((stem + ".c").c_str());
+    std::remove((stem + ".so").c_str());
+    if (!h) return fail(OR_ESTATE, std::string("dlopen: ") + dlerror());
+    y.sc_pre = (void (*)(double *, double *const *, int64_t, double, const double *))dlsym(h, "sc_pre");
+    y.sc_post = (void (*)(double *, double *const *, int64_t, double))dlsym(h, "sc_post");
+    if (!y.sc_pre || !y.sc_post) return fail(OR_ESTATE, "synaptic code symbols");
+    if (!post_code || !*post_code) y.sc_post = nullptr;
+    return OR_OK;
+}
+int or_synapses_get_var(or_net *n, int32_t sid, int32_t k, double *out) {
+    if (!n || sid < 0 || sid >= (int32_t)n->syns.size() || !out) return fail(OR_EINVAL, "synapses_get_var");
+    const Syn &y = n->syns[sid];
+    if (!y.coded || k < 0 || k >= y.nsv) return fail(OR_EINVAL, "synaptic variable");
+    std::copy(y.sv.begin() + (size_t)k * y.nsyn, y.sv.begin() + (size_t)(k + 1) * y.nsyn, out);
+    return OR_OK;
+}
+int or_synapses_set_var(or_net *n, int32_t sid, int32_t k, const double *in) {
+    if (!n || sid < 0 || sid >= (int32_t)n->syns.size() || !in) return fail(OR_EINVAL, "synapses_set_var");
+    Syn &y = n->syns[sid];
+    if (!y.coded || k < 0 || k >= y.nsv) return fail(OR_EINVAL, "synaptic variable");
+    std::copy(in, in + y.nsyn, y.sv.begin() + (size_t)k * y.nsyn);
+    return OR_OK;
+}
+
 /* Synapses.update (synapses.py:808-827) in the 'synapses' slot: the events
- * of this step, in queue order, applied statement by statement; then next(). */
-static void synapses_deliver(or_net *n) {
+ * of this step, in queue order, applied statement by statement (with code:
+ * the whole presynaptic code per event, a target's events in queue order,
+ * then the postsynaptic code for each synapse of a target that spiked in
+ * this step); then next(). */
+static void synapses_deliver(or_net *n, double t) {
     for (auto &y : n->syns) {
         Group &g = n->groups[y.tgt];
+        if (y.coded) {
+            const Group &gs = n->groups[y.src];
+            std::vector<double *> svp(8, nullptr);
+            for (int v = 0; v < y.nsv; ++v) svp[v] = &y.sv[(size_t)v * y.nsyn];
+            double x[4] = {0, 0, 0, 0}, pv[4] = {0, 0, 0, 0};
+            for (int32_t e : y.X[y.cur]) {
+                const int64_t j = y.to + y.post[e];
+                for (size_t s2 = 0; s2 < y.slot_var.size(); ++s2) x[s2] = g.S[(size_t)y.slot_var[s2] * g.n + j];
+                for (size_t k = 0; k < y.pre_var.size(); ++k) pv[k] = gs.S[(size_t)y.pre_var[k] * gs.n + y.so + y.pre[e]];
+                y.sc_pre(x, svp.data(), e, t, pv);
+                for (size_t s2 = 0; s2 < y.slot_var.size(); ++s2) g.S[(size_t)y.slot_var[s2] * g.n + j] = x[s2];
+            }
+            if (y.sc_post)
+                for (int32_t i : g.hist[0]) {
+                    if (i < y.to || i >= y.to + y.tn) continue;
+                    for (size_t s2 = 0; s2 < y.slot_var.size(); ++s2) x[s2] = g.S[(size_t)y.slot_var[s2] * g.n + i];
+                    for (int32_t e : y.syn_of_post[i - y.to]) y.sc_post(x, svp.data(), e, t);
+                }
+            y.X[y.cur].clear();
+            y.cur = (y.cur + 1) % y.L;
+            continue;
+        }
         for (int32_t e : y.X[y.cur]) {
             const int64_t j = y.to + y.post[e];
             for (int k = 0; k < y.nops; ++k) {
@@ -850,7 +946,7 @@ static void step(or_net *n, int64_t cs) {
         c.cur = (c.cur + 1) % c.md;
     }
     /* ---- synapses ---- */
-    synapses_deliver(n);
+    synapses_deliver(n, t);
     /* ---- resets ---- */
     for (auto &g : n->groups) {
         const int64_t N = g.n;
@@ -946,6 +1042,7 @@ template <typename IO> void or_visit(or_net *n, IO &io) {
         uint64_t L = y.X.size(); io.val(L);
         if (L != y.X.size()) { io.ok = false; return; }
         for (auto &x : y.X) io.vec(x);
+        io.same(y.sv);
     }
     for (auto &m : n->smons) { io.vec(m.steps); io.vec(m.idx); }
     for (auto &m : n->stmons) { io.vec(m.vals); io.vec(m.steps); }

@@ -138,7 +138,7 @@ def test_unsupported_forms():
     _fresh()
     G = b.NeuronGroup(5, model="v : 1")
     with pytest.raises(NotImplementedError):
-        b.Synapses(G, G, model="w : 1", pre="v += w", post="w += 1")
+        b.Synapses(G, G, model="w : 1", pre="v += w", post="v_post += w")
     with pytest.raises(NotImplementedError):
         b.Synapses(G, G, model="dw/dt = -w/(5*ms) : 1", pre="v += w")
     with pytest.raises(ValueError):
