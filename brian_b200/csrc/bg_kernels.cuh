@@ -1271,19 +1271,27 @@ __device__ __forceinline__ void syn_code_body(const SynCodeArgs &a) {
         for (int64_t c0 = P0; c0 < P1; c0 += kSynChunk) {
             const int64_t c1 = min(P1, c0 + (int64_t)kSynChunk);
             const int nw = (int)((c1 - c0 + 31) >> 5);
-            for (int w0 = wid; w0 < nw; w0 += kWarps) {
-                const int64_t p = c0 + (int64_t)w0 * 32 + lane;
-                const uint32_t wd = p < c1 ? a.word[p] : 0u;
-                const int lag = (int)(wd >> 24) - 1;
-                uint32_t hb = 0u;
-                if (lag >= 0 && nstep >= lag) {
-                    const int64_t src = a.so + (int64_t)(wd & 0xFFFFFFu);
-                    int row = row0 - lag;
-                    row += row < 0 ? a.depth : 0;
-                    hb = (a.hist[(int64_t)row * a.nwords + (src >> 5)] >> (src & 31)) & 1u;
+            // hit bits of the chunk's synapses: kSynUnroll words in flight per warp
+            for (int w0 = wid; w0 < nw; w0 += kWarps * kSynUnroll) {
+                uint32_t wd[kSynUnroll];
+#pragma unroll
+                for (int u = 0; u < kSynUnroll; ++u) {
+                    const int64_t p = c0 + (int64_t)(w0 + u * kWarps) * 32 + lane;
+                    wd[u] = (w0 + u * kWarps < nw && p < c1) ? a.word[p] : 0u;
                 }
-                const uint32_t m = __ballot_sync(0xffffffffu, hb != 0u);
-                if (lane == 0) mask[w0] = m;
+#pragma unroll
+                for (int u = 0; u < kSynUnroll; ++u) {
+                    const int lag = (int)(wd[u] >> 24) - 1;
+                    uint32_t hb = 0u;
+                    if (lag >= 0 && nstep >= lag) {
+                        const int64_t src = a.so + (int64_t)(wd[u] & 0xFFFFFFu);
+                        int row = row0 - lag;
+                        row += row < 0 ? a.depth : 0;
+                        hb = (a.hist[(int64_t)row * a.nwords + (src >> 5)] >> (src & 31)) & 1u;
+                    }
+                    const uint32_t m = __ballot_sync(0xffffffffu, hb != 0u);
+                    if (lane == 0 && w0 + u * kWarps < nw) mask[w0 + u * kWarps] = m;
+                }
             }
             __syncthreads();
             if (own) {
