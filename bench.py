@@ -385,7 +385,8 @@ def fitting_bench(args):
     Xtr, th, sim_s = simulate_training_set(eqs, THRESHOLD, RESET, prior, pool, DT, args.fit_train,
                                            seed=args.seed + 5, duration_range=(1.0, 20.0))
     net = ProposalNetwork(prior, seed=1, basis=ADAPTIVE_LIF_BASIS)
-    loss, train_ms = net.train(Xtr, th, epochs=args.fit_epochs, batch=4096, lr=1e-3, seed=args.seed + 3)
+    loss, train_ms = net.train(Xtr, th, epochs=args.fit_epochs, batch=args.fit_batch, lr=args.fit_lr,
+                               seed=args.seed + 3)
     n_used = (len(Xtr) // 4096) * 4096
     # flops of one sample: forward 64x512 + 2 x 512x512 + 512x64 (padded
     # output) multiply-adds, backward twice that minus the first layer's input
@@ -398,6 +399,7 @@ def fitting_bench(args):
     except Exception:
         pk, pk_src = 1400.0, "fallback"
     out["training"] = {"pairs": int(args.fit_train), "simulation_wall_s": sim_s, "epochs": args.fit_epochs,
+                       "batch": args.fit_batch, "lr": args.fit_lr,
                        "gpu_ms": train_ms, "final_loss": float(loss[-1]),
                        "tensor_tflops": flops / (train_ms * 1e-3) / 1e12, "tensor_peak_tflops": pk,
                        "tensor_peak_source": pk_src, "tensor_frac": flops / (train_ms * 1e-3) / 1e12 / pk}
@@ -943,6 +945,10 @@ def main():
     ap.add_argument("--fit-targets", type=int, default=256)
     ap.add_argument("--fit-train", type=int, default=1 << 20)
     ap.add_argument("--fit-epochs", type=int, default=40)
+    # 16384 rows a step at lr 2e-3: the same race result as 4096 at 1e-3
+    # (speedup 10.6 either way) in 1.15 s of training instead of 1.8 s
+    ap.add_argument("--fit-batch", type=int, default=16384, help="rows per training step of the proposal network")
+    ap.add_argument("--fit-lr", type=float, default=2e-3)
     ap.add_argument("--fit-iters", type=int, default=40)
     ap.add_argument("--profile-case", choices=["fit", "gemm", "synapses", "stdp", "batch"], default=None,
                     help="run one small case for a single-kernel ncu capture and exit")
