@@ -1365,16 +1365,31 @@ struct SynEvArgs {
     int last;
 };
 
-static __global__ void __launch_bounds__(256) k_syn_gather(const SynEvArgs a) {
-    const long long nstep = a.ctl->nstep;
+// Events of several Synapses objects gathered and applied by the same two
+// launches (objects whose targets' variables do not overlap, so their
+// order does not matter): object k owns gather items [item0[k],
+// item0[k+1]) and bins [bin0[k], bin0[k+1]).
+constexpr int kSynEvMerge = 4;
+struct SynEvGroup {
+    int nobj;
+    SynEvArgs o[kSynEvMerge];
+    int64_t item0[kSynEvMerge + 1];
+    int bin0[kSynEvMerge + 1];
+    DevCtl *ctl;
+    int last;
+};
+
+// gather item x = d * nw + word of one object: the spiking sources of step
+// t - d in that history word and their synapses of delay d, into the bins
+__device__ __forceinline__ void syn_gather_item(const SynEvArgs &a, long long nstep, int64_t x) {
     const int64_t w0 = a.so >> 5, w1 = (a.so + a.sn + 31) >> 5, nw = w1 - w0;
-    const int64_t total = nw * (int64_t)(a.dmax + 1);
     const int row0 = (int)(nstep % a.depth);
     int *flag = a.use_pull + (nstep & 1);
-    for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < total; x += (int64_t)gridDim.x * blockDim.x) {
-        const int d = (int)(x / nw);
+    {
+        // (items per object < 2^31: 32-bit division)
+        const int d = (int)((uint32_t)x / (uint32_t)nw);
         const int64_t wi = w0 + (x - (int64_t)d * nw);
-        if (nstep < d) continue;
+        if (nstep < d) return;
         int row = row0 - d;
         row += row < 0 ? a.depth : 0;
         uint32_t word = masked_word(a.hist + (int64_t)row * a.nwords, wi, a.so, a.so + a.sn);
@@ -1410,16 +1425,29 @@ static __global__ void __launch_bounds__(256) k_syn_gather(const SynEvArgs a) {
             }
         }
     }
-    bg_finish_step(a.ctl, a.last);
+}
+
+static __global__ void __launch_bounds__(256) k_syn_gather(const __grid_constant__ SynEvGroup g) {
+    const long long nstep = g.ctl->nstep;
+    const int64_t total = g.item0[g.nobj];
+    for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < total; x += (int64_t)gridDim.x * blockDim.x) {
+        int k = 0;
+        while (k + 1 < g.nobj && x >= g.item0[k + 1]) ++k;
+        syn_gather_item(g.o[k], nstep, x - g.item0[k]);
+    }
+    bg_finish_step(g.ctl, g.last);
 }
 
 constexpr int kSynBinThreads = 1024;
-static __global__ void __launch_bounds__(kSynBinThreads) k_syn_bins(const SynEvArgs a) {
+constexpr int kSynSegMax = 64;                          // events of one target per step sorted by its thread
+static_assert(kSynBin == kSynBinThreads, "one thread per target of a bin");
+// one bin of one object: its events sorted by key and applied per target in
+// key order, or the pull's test for a step whose events overflowed
+__device__ __forceinline__ void syn_bins_block(const SynEvArgs &a, long long nstep, int bin) {
     extern __shared__ unsigned char syn_smem[];
     unsigned long long *key = reinterpret_cast<unsigned long long *>(syn_smem);
     int32_t *qv = reinterpret_cast<int32_t *>(key + kSynBinCap);
-    const long long nstep = a.ctl->nstep;
-    const int bin = blockIdx.x, tid = threadIdx.x;
+    const int tid = threadIdx.x;
     const int n = min(a.bin_cnt[bin], kSynBinCap);
     const bool pull = a.use_pull[nstep & 1] != 0;
     __syncthreads();   // every thread has read the bin's count before thread 0 clears it
@@ -1460,6 +1488,75 @@ static __global__ void __launch_bounds__(kSynBinThreads) k_syn_bins(const SynEvA
             }
         }
     } else if (n > 0) {
+        // events per target of the bin (a counting sort by target): each
+        // target's events go to its own segment, which its thread then
+        // orders by key (insertion sort: a target's events in one step are
+        // few); a bin with a target of more than kSynSegMax events takes the
+        // bitonic sort of the whole bin instead
+        __shared__ int tcnt[kSynBin];
+        __shared__ int wsum[kSynBinThreads / 32], maxc;
+        const int lane = tid & 31, warp = tid >> 5;
+        tcnt[tid] = 0;
+        if (tid == 0) maxc = 0;
+        __syncthreads();
+        for (int e = tid; e < n; e += kSynBinThreads)
+            atomicAdd(&tcnt[(int)((a.bin_key[(int64_t)bin * kSynBinCap + e] >> 40) - (unsigned long long)bin * kSynBin)], 1);
+        __syncthreads();
+        const int c = tcnt[tid];
+        if (c) atomicMax(&maxc, c);
+        int incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) { const int v = __shfl_up_sync(0xffffffffu, incl, o); if (lane >= o) incl += v; }
+        if (lane == 31) wsum[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            int v = wsum[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) { const int u = __shfl_up_sync(0xffffffffu, v, o); if (lane >= o) v += u; }
+            wsum[lane] = v;
+        }
+        __syncthreads();
+        const int beg = (warp ? wsum[warp - 1] : 0) + incl - c;
+        if (maxc <= kSynSegMax) {                       // uniform
+            tcnt[tid] = beg;                            // the segment's fill cursor
+            __syncthreads();
+            for (int e = tid; e < n; e += kSynBinThreads) {
+                const unsigned long long k = a.bin_key[(int64_t)bin * kSynBinCap + e];
+                const int pos = atomicAdd(&tcnt[(int)((k >> 40) - (unsigned long long)bin * kSynBin)], 1);
+                key[pos] = k;
+                qv[pos] = a.bin_q[(int64_t)bin * kSynBinCap + e];
+            }
+            __syncthreads();
+            const int64_t j = (int64_t)bin * kSynBin + tid;
+            if (c && j < a.tn) {
+                for (int u = beg + 1; u < beg + c; ++u) {
+                    const unsigned long long kk = key[u];
+                    const int32_t qq = qv[u];
+                    int w = u - 1;
+                    while (w >= beg && key[w] > kk) { key[w + 1] = key[w]; qv[w + 1] = qv[w]; --w; }
+                    key[w + 1] = kk;
+                    qv[w + 1] = qq;
+                }
+                double x[kSynMaxOps];
+#pragma unroll
+                for (int s = 0; s < kSynMaxOps; ++s)
+                    x[s] = s < a.nslots ? a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] : 0.0;
+                for (int e = beg; e < beg + c; ++e) {
+                    const int64_t q = qv[e];
+#pragma unroll
+                    for (int k = 0; k < kSynMaxOps; ++k) {
+                        if (k >= a.nops) break;
+                        const double t = a.term[(int64_t)k * a.nsyn + q];
+#pragma unroll
+                        for (int s = 0; s < kSynMaxOps; ++s)
+                            if (s == a.slot_of[k]) x[s] = a.sub[k] ? __dsub_rn(x[s], t) : __dadd_rn(x[s], t);
+                    }
+                }
+#pragma unroll
+                for (int s = 0; s < kSynMaxOps; ++s)
+                    if (s < a.nslots) a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] = x[s];
+            }
+        } else {
         int m = 1;
         while (m < n) m <<= 1;
         for (int e = tid; e < m; e += kSynBinThreads) {
@@ -1511,12 +1608,19 @@ static __global__ void __launch_bounds__(kSynBinThreads) k_syn_bins(const SynEvA
                     if (s < a.nslots) a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] = x[s];
             }
         }
+        }
     }
     if (tid == 0) {
         a.bin_cnt[bin] = 0;                             // empty for the next step
         if (bin == 0) a.use_pull[(nstep + 1) & 1] = 0;  // next step's flag (nobody reads it this step)
     }
-    bg_finish_step(a.ctl, a.last);
+}
+
+static __global__ void __launch_bounds__(kSynBinThreads) k_syn_bins(const __grid_constant__ SynEvGroup g) {
+    int k = 0;
+    while (k + 1 < g.nobj && (int)blockIdx.x >= g.bin0[k + 1]) ++k;
+    syn_bins_block(g.o[k], g.ctl->nstep, (int)blockIdx.x - g.bin0[k]);
+    bg_finish_step(g.ctl, g.last);
 }
 
 // SpikeMonitor (monitor.py:156-166): one block appends the step's spikes in

@@ -582,6 +582,75 @@ int compile_syn_code(HSyn &y) {
     return BG_OK;
 }
 
+// The event path's arguments of Synapses object yi.
+bg::SynEvArgs syn_ev_args(bg_net *net, int yi) {
+    HSyn &y = net->syns[yi];
+    const HGroup &gs = net->groups[y.src];
+    HGroup &gt = net->groups[y.tgt];
+    bg::SynEvArgs e;
+    std::memset(&e, 0, sizeof(e));
+    e.ctl = net->dCtl; e.hist = gs.dHist; e.depth = gs.depth; e.nwords = gs.npad / 32;
+    e.so = y.so; e.sn = y.sn; e.tn = y.tn; e.dmax = y.dmax;
+    e.srcptr = y.dSrcPtr; e.sd = y.dSd; e.stgt = y.dStgt; e.sq = y.dSq; e.doff = y.dDoff;
+    e.colptr = y.dColptr; e.word = y.dWord;
+    e.bin_cnt = y.dBinCnt; e.bin_key = y.dBinKey; e.bin_q = y.dBinQ; e.nbins = y.nbins; e.use_pull = y.dUsePull;
+    e.term = y.dTerm; e.nsyn = y.nsyn; e.nops = y.nops;
+    for (int k = 0; k < y.nops; ++k) {
+        int sl = -1;
+        for (int q = 0; q < e.nslots; ++q) if (e.slot_var[q] == y.op_var[k]) sl = q;
+        if (sl < 0) { sl = e.nslots++; e.slot_var[sl] = y.op_var[k]; }
+        e.slot_of[k] = sl; e.sub[k] = y.op_sub[k];
+    }
+    e.S = (double *)gt.dS; e.npad = gt.npad; e.to = y.to;
+    return e;
+}
+
+// Event path of the Synapses objects `ids` (consecutive in the schedule,
+// targets' variables disjoint): one gather launch over all their (delay,
+// history word) items, then one launch over all their bins (which fall back
+// to the pull's test for an object whose events overflowed in a step).
+int build_syn_events(bg_net *net, const std::vector<int> &ids) {
+    bg::SynEvGroup g;
+    std::memset(&g, 0, sizeof(g));
+    g.nobj = (int)ids.size(); g.ctl = net->dCtl;
+    std::string tag;
+    for (int k = 0; k < g.nobj; ++k) {
+        const HSyn &y = net->syns[ids[k]];
+        g.o[k] = syn_ev_args(net, ids[k]);
+        const int64_t nw = (y.so + y.sn + 31) / 32 - y.so / 32;
+        g.item0[k + 1] = g.item0[k] + nw * (y.dmax + 1);
+        if (nw * (y.dmax + 1) >= ((int64_t)1 << 31)) return fail(BG_ENOSYS, "Synapses event path: too many (delay, word) items");
+        g.bin0[k + 1] = g.bin0[k] + y.nbins;
+        tag += (k ? ",y" : "y") + std::to_string(ids[k]);
+    }
+    const int64_t ggrid = std::max<int64_t>(1, std::min<int64_t>((g.item0[g.nobj] + 255) / 256, (int64_t)sm_count() * 8));
+    const size_t bsmem = (size_t)bg::kSynBinCap * (8 + 4);
+    cudaFuncSetAttribute(bg::k_syn_bins, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem);
+    net->item_names.push_back("syn_gather[" + tag + "]");
+    net->step_launches.push_back([g, ggrid](cudaStream_t st, int, int last) {
+        bg::SynEvGroup b = g; b.last = last;
+        bg::k_syn_gather<<<(unsigned)ggrid, 256, 0, st>>>(b);
+        return cudaGetLastError();
+    });
+    net->item_names.push_back("syn_bins[" + tag + "]");
+    net->step_launches.push_back([g, bsmem](cudaStream_t st, int, int last) {
+        bg::SynEvGroup b = g; b.last = last;
+        bg::k_syn_bins<<<(unsigned)b.bin0[b.nobj], bg::kSynBinThreads, bsmem, st>>>(b);
+        return cudaGetLastError();
+    });
+    return BG_OK;
+}
+
+// Whether Synapses objects a and b may apply their events in either order:
+// no target variable on overlapping target ranges is written by both.
+bool syn_disjoint(const HSyn &a, const HSyn &b) {
+    if (a.tgt != b.tgt || a.to >= b.to + b.tn || b.to >= a.to + a.tn) return true;
+    for (int u : a.op_var)
+        for (int v : b.op_var)
+            if (u == v) return false;
+    return true;
+}
+
 int build_syn_code(bg_net *net, int yi) {
     HSyn &y = net->syns[yi];
     const HGroup &gs = net->groups[y.src];
@@ -632,38 +701,7 @@ int build_syn(bg_net *net, int yi) {
     a.S = (double *)gt.dS; a.npad = gt.npad;
     const int64_t ntiles = (y.tn + bg::kSynTile - 1) / bg::kSynTile;
     const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)sm_count() * 8));
-    if (y.events) {
-        // event path: gather, then the bins (which fall back to the pull's
-        // test for a step whose events overflowed)
-        bg::SynEvArgs e;
-        std::memset(&e, 0, sizeof(e));
-        e.ctl = net->dCtl; e.hist = gs.dHist; e.depth = gs.depth; e.nwords = gs.npad / 32;
-        e.so = y.so; e.sn = y.sn; e.tn = y.tn; e.dmax = y.dmax;
-        e.srcptr = y.dSrcPtr; e.sd = y.dSd; e.stgt = y.dStgt; e.sq = y.dSq; e.doff = y.dDoff;
-        e.colptr = y.dColptr; e.word = y.dWord;
-        e.bin_cnt = y.dBinCnt; e.bin_key = y.dBinKey; e.bin_q = y.dBinQ; e.nbins = y.nbins; e.use_pull = y.dUsePull;
-        e.term = y.dTerm; e.nsyn = y.nsyn; e.nops = a.nops; e.nslots = a.nslots;
-        for (int k = 0; k < bg::kSynMaxOps; ++k) { e.slot_of[k] = a.slot_of[k]; e.sub[k] = a.sub[k]; e.slot_var[k] = a.slot_var[k]; }
-        e.S = a.S; e.npad = a.npad; e.to = y.to;
-        a.use_pull = y.dUsePull;
-        const int64_t nw = (y.so + y.sn + 31) / 32 - y.so / 32;
-        const int64_t ggrid = std::max<int64_t>(1, std::min<int64_t>((nw * (y.dmax + 1) + 255) / 256, (int64_t)sm_count() * 8));
-        const size_t bsmem = (size_t)bg::kSynBinCap * (8 + 4);
-        cudaFuncSetAttribute(bg::k_syn_bins, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem);
-        net->item_names.push_back("syn_gather[y" + std::to_string(yi) + "]");
-        net->step_launches.push_back([e, ggrid](cudaStream_t st, int, int last) {
-            bg::SynEvArgs b = e; b.last = last;
-            bg::k_syn_gather<<<(unsigned)ggrid, 256, 0, st>>>(b);
-            return cudaGetLastError();
-        });
-        net->item_names.push_back("syn_bins[y" + std::to_string(yi) + "]");
-        net->step_launches.push_back([e, bsmem](cudaStream_t st, int, int last) {
-            bg::SynEvArgs b = e; b.last = last;
-            bg::k_syn_bins<<<(unsigned)b.nbins, bg::kSynBinThreads, bsmem, st>>>(b);
-            return cudaGetLastError();
-        });
-        return BG_OK;
-    }
+    if (y.events) return build_syn_events(net, {yi});
     net->item_names.push_back("syn_deliver[y" + std::to_string(yi) + "]");
     net->step_launches.push_back([a, grid](cudaStream_t st, int, int last) {
         bg::SynArgs b = a; b.last = last;
@@ -2094,7 +2132,21 @@ static int prepare_impl(bg_net *n) {
     // the 'synapses' slot: after the connections, before the resets
     // (DelayConnection rows and resets of this step run in the next step's
     // head kernel, so a target variable fed by both is refused at prepare)
-    for (size_t yi = 0; yi < n->syns.size(); ++yi) { st = build_syn(n, (int)yi); if (st) return st; }
+    // consecutive event-path objects with disjoint targets share their launches
+    for (size_t yi = 0; yi < n->syns.size();) {
+        if (!n->syns[yi].events || n->syns[yi].coded) { st = build_syn(n, (int)yi); if (st) return st; ++yi; continue; }
+        std::vector<int> grp{(int)yi};
+        size_t yj = yi + 1;
+        while (yj < n->syns.size() && (int)grp.size() < bg::kSynEvMerge && n->syns[yj].events && !n->syns[yj].coded) {
+            bool ok = true;
+            for (int k : grp) ok = ok && syn_disjoint(n->syns[k], n->syns[yj]);
+            if (!ok) break;
+            grp.push_back((int)yj++);
+        }
+        st = build_syn_events(n, grp);
+        if (st) return st;
+        yi = yj;
+    }
     if (n->step_launches.empty()) return fail(BG_EINVAL, "empty network");
     if (n->allow_persist) st = n->precision == 64 ? build_persist<double>(n) : build_persist<float>(n);
     if (st) return st;
