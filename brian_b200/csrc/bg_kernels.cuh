@@ -1413,15 +1413,28 @@ __device__ __forceinline__ void syn_gather_item(const SynEvArgs &a, long long ns
                 r1 = l;
             }
             if (r1 - r0 > 256) { atomicExch(flag, 1); continue; }
-            for (int64_t p = r0; p < r1; ++p) {
-                const int64_t j = a.stgt[p];
-                const int bin = (int)(j / kSynBin);
-                const int slot = atomicAdd(a.bin_cnt + bin, 1);
-                if (slot >= kSynBinCap) { atomicExch(flag, 1); continue; }
-                const int64_t e = (int64_t)bin * kSynBinCap + slot;
-                a.bin_key[e] = ((unsigned long long)j << 40) | ((unsigned long long)(255 - d) << 32) |
-                               ((unsigned long long)i << 8) | (unsigned long long)(p - r0);
-                a.bin_q[e] = a.sq[p];
+            // eight synapses at a time: their targets loaded, then their bin
+            // slots taken, then their events written (one memory round trip
+            // per stage instead of per synapse)
+            for (int64_t p0 = r0; p0 < r1; p0 += 8) {
+                const int m = r1 - p0 < 8 ? (int)(r1 - p0) : 8;
+                int32_t tg[8], qs[8], slot[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (u < m) { tg[u] = __ldg(a.stgt + p0 + u); qs[u] = __ldg(a.sq + p0 + u); }
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (u < m) slot[u] = atomicAdd(a.bin_cnt + tg[u] / kSynBin, 1);
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    if (u >= m) break;
+                    if (slot[u] >= kSynBinCap) { atomicExch(flag, 1); continue; }
+                    const int64_t j = tg[u];
+                    const int64_t e = (j / kSynBin) * kSynBinCap + slot[u];
+                    a.bin_key[e] = ((unsigned long long)j << 40) | ((unsigned long long)(255 - d) << 32) |
+                                   ((unsigned long long)i << 8) | (unsigned long long)(p0 + u - r0);
+                    a.bin_q[e] = qs[u];
+                }
             }
         }
     }
@@ -1496,11 +1509,18 @@ __device__ __forceinline__ void syn_bins_block(const SynEvArgs &a, long long nst
         __shared__ int tcnt[kSynBin];
         __shared__ int wsum[kSynBinThreads / 32], maxc;
         const int lane = tid & 31, warp = tid >> 5;
+        // the bin's first kSynBinThreads events stay in registers between
+        // the count and the placement
+        const int64_t e0 = (int64_t)bin * kSynBinCap;
+        unsigned long long k0 = 0;
+        int32_t q0 = 0;
+        if (tid < n) { k0 = a.bin_key[e0 + tid]; q0 = a.bin_q[e0 + tid]; }
         tcnt[tid] = 0;
         if (tid == 0) maxc = 0;
         __syncthreads();
-        for (int e = tid; e < n; e += kSynBinThreads)
-            atomicAdd(&tcnt[(int)((a.bin_key[(int64_t)bin * kSynBinCap + e] >> 40) - (unsigned long long)bin * kSynBin)], 1);
+        if (tid < n) atomicAdd(&tcnt[(int)((k0 >> 40) - (unsigned long long)bin * kSynBin)], 1);
+        for (int e = tid + kSynBinThreads; e < n; e += kSynBinThreads)
+            atomicAdd(&tcnt[(int)((a.bin_key[e0 + e] >> 40) - (unsigned long long)bin * kSynBin)], 1);
         __syncthreads();
         const int c = tcnt[tid];
         if (c) atomicMax(&maxc, c);
@@ -1520,11 +1540,16 @@ __device__ __forceinline__ void syn_bins_block(const SynEvArgs &a, long long nst
         if (maxc <= kSynSegMax) {                       // uniform
             tcnt[tid] = beg;                            // the segment's fill cursor
             __syncthreads();
-            for (int e = tid; e < n; e += kSynBinThreads) {
-                const unsigned long long k = a.bin_key[(int64_t)bin * kSynBinCap + e];
+            if (tid < n) {
+                const int pos = atomicAdd(&tcnt[(int)((k0 >> 40) - (unsigned long long)bin * kSynBin)], 1);
+                key[pos] = k0;
+                qv[pos] = q0;
+            }
+            for (int e = tid + kSynBinThreads; e < n; e += kSynBinThreads) {
+                const unsigned long long k = a.bin_key[e0 + e];
                 const int pos = atomicAdd(&tcnt[(int)((k >> 40) - (unsigned long long)bin * kSynBin)], 1);
                 key[pos] = k;
-                qv[pos] = a.bin_q[(int64_t)bin * kSynBinCap + e];
+                qv[pos] = a.bin_q[e0 + e];
             }
             __syncthreads();
             const int64_t j = (int64_t)bin * kSynBin + tid;
@@ -1616,7 +1641,7 @@ __device__ __forceinline__ void syn_bins_block(const SynEvArgs &a, long long nst
     }
 }
 
-static __global__ void __launch_bounds__(kSynBinThreads) k_syn_bins(const __grid_constant__ SynEvGroup g) {
+static __global__ void __launch_bounds__(kSynBinThreads, 2) k_syn_bins(const __grid_constant__ SynEvGroup g) {
     int k = 0;
     while (k + 1 < g.nobj && (int)blockIdx.x >= g.bin0[k + 1]) ++k;
     syn_bins_block(g.o[k], g.ctl->nstep, (int)blockIdx.x - g.bin0[k]);
@@ -1624,7 +1649,10 @@ static __global__ void __launch_bounds__(kSynBinThreads) k_syn_bins(const __grid
 }
 
 // SpikeMonitor (monitor.py:156-166): one block appends the step's spikes in
-// ascending order.
+// ascending order.  A pass covers kMonThreads * kMonWords history words: they
+// are loaded at once (coalesced, into shared memory), thread t then owns the
+// kMonWords consecutive words from t * kMonWords, and one block-wide prefix
+// sum of the threads' spike counts gives every spike its slot.
 struct MonArgs {
     DevCtl *ctl;
     const uint32_t *hist; int depth; int64_t nwords; int delay;
@@ -1634,35 +1662,62 @@ struct MonArgs {
     int last;
 };
 constexpr int kMonThreads = 1024;
+constexpr int kMonWords = 8;
 static __global__ void __launch_bounds__(kMonThreads) k_spikemon(const MonArgs a) {
-    __shared__ int wcnt[kMonThreads / 32 + 1];
+    __shared__ uint32_t sw[kMonThreads * kMonWords + kMonThreads * kMonWords / 32];   // one pad word per 32: no bank conflicts either way
+    __shared__ int wcnt[kMonThreads / 32];
     const long long nstep = a.ctl->nstep;
     if (nstep >= a.delay && blockIdx.x == 0) {
         const long long cs = nstep + a.ctl->clock_off;
+        const int32_t srel = (int32_t)(cs - *a.step_base);
         const uint32_t *H = a.hist + (int64_t)((int)(nstep - a.delay) % a.depth) * a.nwords;
         const int64_t end = a.origin + a.n;
         const int64_t w0 = a.origin >> 5, w1 = (end + 31) >> 5;
         long long base = *a.cnt;
-        const int tid = threadIdx.x;
-        for (int64_t cw = w0; cw < w1; cw += kMonThreads) {
-            const int64_t wi = cw + tid;
-            uint32_t word = wi < w1 ? masked_word(H, wi, a.origin, end) : 0u;
-            const int pc = __popc(word);
+        const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+        for (int64_t cw = w0; cw < w1; cw += kMonThreads * kMonWords) {
+#pragma unroll
+            for (int u = 0; u < kMonWords; ++u) {
+                const int e = u * kMonThreads + tid;
+                const int64_t wi = cw + e;
+                sw[e + (e >> 5)] = wi < w1 ? masked_word(H, wi, a.origin, end) : 0u;
+            }
+            __syncthreads();
+            uint32_t wd[kMonWords];
+            int pc = 0;
+#pragma unroll
+            for (int u = 0; u < kMonWords; ++u) {
+                const int e = tid * kMonWords + u;
+                wd[u] = sw[e + (e >> 5)];
+                pc += __popc(wd[u]);
+            }
             int incl = pc;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) { int v = __shfl_up_sync(0xffffffffu, incl, o); if ((tid & 31) >= o) incl += v; }
-            if ((tid & 31) == 31) wcnt[tid >> 5] = incl;
+            for (int o = 1; o < 32; o <<= 1) { const int v = __shfl_up_sync(0xffffffffu, incl, o); if (lane >= o) incl += v; }
+            if (lane == 31) wcnt[warp] = incl;
             __syncthreads();
-            if (tid == 0) { int s = 0; for (int q = 0; q < kMonThreads / 32; ++q) { int v = wcnt[q]; wcnt[q] = s; s += v; } wcnt[kMonThreads / 32] = s; }
-            __syncthreads();
-            long long o = base + wcnt[tid >> 5] + incl - pc;
-            while (word) {
-                const int b = __ffs(word) - 1; word &= word - 1;
-                if (o < a.cap) { a.idx[o] = (int32_t)(((wi << 5) + b) - a.origin); a.steps[o] = (int32_t)(cs - *a.step_base); }
-                else bg_raise(a.ctl, BG_DERR_MONITOR_OVERFLOW, o);
-                ++o;
+            int wpre = 0, tot = 0;
+            {
+                const int v = wcnt[lane];
+                int sc = v;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) { const int x = __shfl_up_sync(0xffffffffu, sc, o); if (lane >= o) sc += x; }
+                wpre = __shfl_sync(0xffffffffu, sc - v, warp);
+                tot = __shfl_sync(0xffffffffu, sc, 31);
             }
-            base += wcnt[kMonThreads / 32];
+            long long o = base + wpre + incl - pc;
+#pragma unroll
+            for (int u = 0; u < kMonWords; ++u) {
+                uint32_t word = wd[u];
+                const int64_t wi = cw + tid * kMonWords + u;
+                while (word) {
+                    const int b = __ffs(word) - 1; word &= word - 1;
+                    if (o < a.cap) { a.idx[o] = (int32_t)(((wi << 5) + b) - a.origin); a.steps[o] = srel; }
+                    else bg_raise(a.ctl, BG_DERR_MONITOR_OVERFLOW, o);
+                    ++o;
+                }
+            }
+            base += tot;
             __syncthreads();
         }
         if (tid == 0) *a.cnt = base;
