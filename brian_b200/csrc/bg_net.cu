@@ -203,6 +203,13 @@ struct bg_net {
     unsigned long long *dCounters = nullptr; // [groups] spikes, then [conns] events
     std::vector<Launch> finalize_launches; // tail-only head kernels
     cudaGraphExec_t gexec = nullptr;
+    // step launches [side0, side1) (the SpikeMonitors, right after the group
+    // kernels) only read the spike history the group kernels wrote: in the
+    // step graph they run on a side stream beside the launches after them
+    // and join before the step's last launch (the one that advances the step)
+    size_t side0 = 0, side1 = 0;
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     // persistent single-launch path (see bg_persist.cuh); empty when the
     // network does not have its shape
     std::function<cudaError_t(cudaStream_t, int nsteps)> persist;
@@ -1232,6 +1239,9 @@ int bg_net_destroy(bg_net *n) {
     for (void *p : n->allocs) cudaFree(p);
     if (n->ev0) cudaEventDestroy(n->ev0);
     if (n->ev1) cudaEventDestroy(n->ev1);
+    if (n->ev_fork) cudaEventDestroy(n->ev_fork);
+    if (n->ev_join) cudaEventDestroy(n->ev_join);
+    if (n->side) cudaStreamDestroy(n->side);
     if (n->stream) cudaStreamDestroy(n->stream);
     delete n;
     return BG_OK;
@@ -2117,11 +2127,13 @@ static int prepare_impl(bg_net *n) {
         st = n->precision == 64 ? build_group<double>(n, (int)gi) : build_group<float>(n, (int)gi);
         if (st) return st;
     }
+    const size_t nhead = n->step_launches.size();
+    std::vector<size_t> mon_launch;
     for (size_t si = 0; si < n->stdps.size(); ++si) { st = build_decay(n, (int)si); if (st) return st; }
     for (const Item &it : n->items) {
         switch (it.kind) {
         case IT_CONN: st = n->precision == 64 ? build_conn<double>(n, it.id) : build_conn<float>(n, it.id); break;
-        case IT_SPIKEMON: st = build_spikemon(n, it.id); break;
+        case IT_SPIKEMON: mon_launch.push_back(n->step_launches.size()); st = build_spikemon(n, it.id); break;
         // STDP keeps FP64 traces and weight arithmetic on both paths (the
         // FP32 path moves the neuron state and the propagation to FP32)
         case IT_STDP_PRE: st = build_stdp_pre(n, it.id); break;
@@ -2148,6 +2160,22 @@ static int prepare_impl(bg_net *n) {
         yi = yj;
     }
     if (n->step_launches.empty()) return fail(BG_EINVAL, "empty network");
+    {
+        // SpikeMonitors move to right after the group kernels (they read
+        // nothing but the spike history, which only the group kernels write)
+        std::vector<Launch> L;
+        std::vector<std::string> names;
+        std::vector<char> is_mon(n->step_launches.size(), 0);
+        for (size_t i : mon_launch) is_mon[i] = 1;
+        for (size_t i = 0; i < nhead; ++i) { L.push_back(n->step_launches[i]); names.push_back(n->item_names[i]); }
+        for (size_t i : mon_launch) { L.push_back(n->step_launches[i]); names.push_back(n->item_names[i]); }
+        for (size_t i = nhead; i < n->step_launches.size(); ++i)
+            if (!is_mon[i]) { L.push_back(n->step_launches[i]); names.push_back(n->item_names[i]); }
+        n->step_launches.swap(L);
+        n->item_names.swap(names);
+        n->side0 = nhead;
+        n->side1 = nhead + mon_launch.size();
+    }
     if (n->allow_persist) st = n->precision == 64 ? build_persist<double>(n) : build_persist<float>(n);
     if (st) return st;
     BG_CUDA(cudaStreamSynchronize(n->stream));
@@ -2165,12 +2193,39 @@ static int launch_step(bg_net *n, int tail) {
     return BG_OK;
 }
 
+// one step into the graph being captured, the side launches on the side
+// stream (forked after the group kernels, joined before the last launch)
+static int capture_step_forked(bg_net *n) {
+    const size_t k = n->step_launches.size();
+    for (size_t i = 0; i < k; ++i) {
+        cudaStream_t st = n->stream;
+        if (i == n->side0) {
+            BG_CUDA(cudaEventRecord(n->ev_fork, n->stream));
+            BG_CUDA(cudaStreamWaitEvent(n->side, n->ev_fork, 0));
+        }
+        if (i >= n->side0 && i < n->side1) st = n->side;
+        if (i == n->side1) BG_CUDA(cudaEventRecord(n->ev_join, n->side));
+        if (i + 1 == k) BG_CUDA(cudaStreamWaitEvent(n->stream, n->ev_join, 0));
+        cudaError_t e = n->step_launches[i](st, 1, i + 1 == k);
+        if (e != cudaSuccess) return fail(BG_ECUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    }
+    n->launches += (int64_t)k;
+    return BG_OK;
+}
+
 static int ensure_graph(bg_net *n) {
     if (n->gexec) return BG_OK;
+    // the side launches fork only when a launch follows them
+    const bool fork = n->side1 > n->side0 && n->side1 < n->step_launches.size();
+    if (fork && !n->side) {
+        BG_CUDA(cudaStreamCreateWithFlags(&n->side, cudaStreamNonBlocking));
+        BG_CUDA(cudaEventCreateWithFlags(&n->ev_fork, cudaEventDisableTiming));
+        BG_CUDA(cudaEventCreateWithFlags(&n->ev_join, cudaEventDisableTiming));
+    }
     cudaGraph_t graph;
     BG_CUDA(cudaStreamBeginCapture(n->stream, cudaStreamCaptureModeThreadLocal));
     int st = BG_OK;
-    for (int s = 0; s < kGraphSteps && st == BG_OK; ++s) st = launch_step(n, 1);
+    for (int s = 0; s < kGraphSteps && st == BG_OK; ++s) st = fork ? capture_step_forked(n) : launch_step(n, 1);
     cudaError_t e = cudaStreamEndCapture(n->stream, &graph);
     n->launches -= (int64_t)kGraphSteps * (int64_t)n->step_launches.size();
     if (st) return st;
