@@ -1336,19 +1336,23 @@ __device__ __forceinline__ void syn_code_body(const SynCodeArgs &a) {
 }
 
 // Event-driven Synapses delivery.  The events of step t are the synapses of
-// delay d of the sources that spiked at step t - d.  k_syn_gather walks the
-// spike-history words of those steps and appends each event to the bin of
-// its target's block of kSynBin targets, with a 64-bit key that sorts into
-// the queue order of the pull above: target, then delay descending, then
-// source, then the synapse's rank among the source's synapses of that delay
-// (synapse index order).  k_syn_bins gives each bin a block that sorts its
-// events by key in shared memory and applies every target's events in that
-// order -- the same additions in the same order as the pull, so the result
-// is bit for bit the same.  A step whose events overflow a bin (or whose
-// keys do not fit) is delivered by the pull's test instead, by the same
-// blocks (use_pull), so the path is exact whatever the activity.
+// delay d of the sources that spiked at step t - d.  Each object keeps a
+// ring of spike lists, one row per step (the sources that spiked then, in
+// no particular order).  k_syn_gather appends this step's spikes to the
+// ring (from the spike-history words) and walks, for every delay d >= 1,
+// the list of step t - d (the delay-0 synapses come straight from the
+// words), appending each event to the bin of its target's block of kSynBin
+// targets, with a 64-bit key that sorts into the queue order of the pull
+// above: target, then delay descending, then source, then the synapse's
+// rank among the source's synapses of that delay (synapse index order).
+// k_syn_bins gives each bin a block that sorts its events by key in shared
+// memory and applies every target's events in that order -- the same
+// additions in the same order as the pull, so the result is bit for bit the
+// same.  A step whose events overflow a bin (or whose keys do not fit) is
+// delivered by the pull's test instead, by the same blocks (use_pull), so
+// the path is exact whatever the activity.
 constexpr int kSynBin = 1024;          // targets per bin (one block)
-constexpr int kSynBinCap = 8192;       // events per bin and step
+constexpr int kSynBinCap = 4096;       // events per bin and step
 struct SynEvArgs {
     DevCtl *ctl;
     const uint32_t *hist; int depth; int64_t nwords;
@@ -1358,6 +1362,10 @@ struct SynEvArgs {
     const int64_t *colptr; const uint32_t *word;                                         // the pull's columns
     int *bin_cnt; unsigned long long *bin_key; int32_t *bin_q; int nbins;
     int *use_pull;                  // [2] by step parity
+    // spike lists: row (step % sdepth) holds scnt[row] source indices; with
+    // sdepth >= dmax + 2 the row a step fills, the row it clears (the next
+    // step's) and the rows it reads (steps t-1 .. t-dmax) are all different
+    int32_t *slist; int *scnt; int sdepth;
     const double *term; int64_t nsyn;
     int nops, nslots;
     int slot_of[kSynMaxOps], sub[kSynMaxOps], slot_var[kSynMaxOps];
@@ -1367,95 +1375,173 @@ struct SynEvArgs {
 
 // Events of several Synapses objects gathered and applied by the same two
 // launches (objects whose targets' variables do not overlap, so their
-// order does not matter): object k owns gather items [item0[k],
-// item0[k+1]) and bins [bin0[k], bin0[k+1]).
+// order does not matter).  Gather: blocks [0, npair * nparts) walk the
+// spike lists, (object, delay) pair p = block / nparts (object k owns pairs
+// [pair0[k], pair0[k+1]), delays 1 .. dmax), each list split over nparts
+// blocks; the blocks after them walk the history words of this step,
+// object k owning words [item0[k], item0[k+1]).  Bins: object k owns bins
+// [bin0[k], bin0[k+1]).
 constexpr int kSynEvMerge = 4;
 struct SynEvGroup {
     int nobj;
     SynEvArgs o[kSynEvMerge];
     int64_t item0[kSynEvMerge + 1];
+    int pair0[kSynEvMerge + 1];
+    int nparts;
     int bin0[kSynEvMerge + 1];
     DevCtl *ctl;
     int last;
 };
 
-// gather item x = d * nw + word of one object: the spiking sources of step
-// t - d in that history word and their synapses of delay d, into the bins
-__device__ __forceinline__ void syn_gather_item(const SynEvArgs &a, long long nstep, int64_t x) {
-    const int64_t w0 = a.so >> 5, w1 = (a.so + a.sn + 31) >> 5, nw = w1 - w0;
-    const int row0 = (int)(nstep % a.depth);
-    int *flag = a.use_pull + (nstep & 1);
-    {
-        // (items per object < 2^31: 32-bit division)
-        const int d = (int)((uint32_t)x / (uint32_t)nw);
-        const int64_t wi = w0 + (x - (int64_t)d * nw);
-        if (nstep < d) return;
-        int row = row0 - d;
-        row += row < 0 ? a.depth : 0;
-        uint32_t word = masked_word(a.hist + (int64_t)row * a.nwords, wi, a.so, a.so + a.sn);
-        while (word) {
-            const int b = __ffs(word) - 1; word &= word - 1;
-            const int64_t i = (wi << 5) + b - a.so;
-            // the synapses of source i with delay d: a range of its row
-            int64_t r0, r1;
-            const int64_t lo = a.srcptr[i];
-            if (a.doff) {
-                const int32_t *o = a.doff + i * (int64_t)(a.dmax + 2) + d;
-                r0 = lo + o[0];
-                r1 = lo + o[1];
-            } else {
-                const int64_t hi = a.srcptr[i + 1];
-                int64_t l = lo, h = hi;
-                while (l < h) { const int64_t m = (l + h) >> 1; if (a.sd[m] < d) l = m + 1; else h = m; }
-                r0 = l;
-                h = hi;
-                while (l < h) { const int64_t m = (l + h) >> 1; if (a.sd[m] <= d) l = m + 1; else h = m; }
-                r1 = l;
-            }
-            if (r1 - r0 > 256) { atomicExch(flag, 1); continue; }
-            // eight synapses at a time: their targets loaded, then their bin
-            // slots taken, then their events written (one memory round trip
-            // per stage instead of per synapse)
-            for (int64_t p0 = r0; p0 < r1; p0 += 8) {
-                const int m = r1 - p0 < 8 ? (int)(r1 - p0) : 8;
-                int32_t tg[8], qs[8], slot[8];
+// the synapses of source i (relative to the object's source range) with
+// delay d: rows [r0, r1) of the by-source arrays
+__device__ __forceinline__ void syn_src_range(const SynEvArgs &a, int64_t i, int d, int64_t &r0, int64_t &r1) {
+    const int64_t lo = __ldg(a.srcptr + i);
+    if (a.doff) {
+        const int32_t *o = a.doff + i * (int64_t)(a.dmax + 2) + d;
+        r0 = lo + __ldg(o);
+        r1 = lo + __ldg(o + 1);
+    } else {
+        const int64_t hi = __ldg(a.srcptr + i + 1);
+        int64_t l = lo, h = hi;
+        while (l < h) { const int64_t m = (l + h) >> 1; if (a.sd[m] < d) l = m + 1; else h = m; }
+        r0 = l;
+        h = hi;
+        while (l < h) { const int64_t m = (l + h) >> 1; if (a.sd[m] <= d) l = m + 1; else h = m; }
+        r1 = l;
+    }
+}
+
+// the events of source i's synapses of delay d, into the bins
+__device__ __forceinline__ void syn_push_events(const SynEvArgs &a, int64_t i, int d, int *flag) {
+    int64_t r0, r1;
+    syn_src_range(a, i, d, r0, r1);
+    if (r1 - r0 > 256) { atomicExch(flag, 1); return; }
+    // eight synapses at a time: their targets loaded, then their bin slots
+    // taken, then their events written (one memory round trip per stage
+    // instead of per synapse)
+    for (int64_t p0 = r0; p0 < r1; p0 += 8) {
+        const int m = r1 - p0 < 8 ? (int)(r1 - p0) : 8;
+        int32_t tg[8], qs[8], slot[8];
 #pragma unroll
-                for (int u = 0; u < 8; ++u)
-                    if (u < m) { tg[u] = __ldg(a.stgt + p0 + u); qs[u] = __ldg(a.sq + p0 + u); }
+        for (int u = 0; u < 8; ++u)
+            if (u < m) { tg[u] = __ldg(a.stgt + p0 + u); qs[u] = __ldg(a.sq + p0 + u); }
 #pragma unroll
-                for (int u = 0; u < 8; ++u)
-                    if (u < m) slot[u] = atomicAdd(a.bin_cnt + tg[u] / kSynBin, 1);
+        for (int u = 0; u < 8; ++u)
+            if (u < m) slot[u] = atomicAdd(a.bin_cnt + tg[u] / kSynBin, 1);
 #pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    if (u >= m) break;
-                    if (slot[u] >= kSynBinCap) { atomicExch(flag, 1); continue; }
-                    const int64_t j = tg[u];
-                    const int64_t e = (j / kSynBin) * kSynBinCap + slot[u];
-                    a.bin_key[e] = ((unsigned long long)j << 40) | ((unsigned long long)(255 - d) << 32) |
-                                   ((unsigned long long)i << 8) | (unsigned long long)(p0 + u - r0);
-                    a.bin_q[e] = qs[u];
-                }
-            }
+        for (int u = 0; u < 8; ++u) {
+            if (u >= m) break;
+            if (slot[u] >= kSynBinCap) { atomicExch(flag, 1); continue; }
+            const int64_t j = tg[u];
+            const int64_t e = (j / kSynBin) * kSynBinCap + slot[u];
+            a.bin_key[e] = ((unsigned long long)j << 40) | ((unsigned long long)(255 - d) << 32) |
+                           ((unsigned long long)i << 8) | (unsigned long long)(p0 + u - r0);
+            a.bin_q[e] = qs[u];
         }
+    }
+}
+
+// history word x (of the object's source range) of step nstep: its spikes
+// appended to the step's list, and their delay-0 events
+__device__ __forceinline__ void syn_gather_word(const SynEvArgs &a, long long nstep, int64_t x) {
+    const int64_t wi = (a.so >> 5) + x;
+    uint32_t word = masked_word(a.hist + (int64_t)(nstep % a.depth) * a.nwords, wi, a.so, a.so + a.sn);
+    if (!word) return;
+    const int row = (int)(nstep % a.sdepth);
+    int pos = atomicAdd(a.scnt + row, __popc(word));
+    int32_t *L = a.slist + (int64_t)row * a.sn;
+    int *flag = a.use_pull + (nstep & 1);
+    while (word) {
+        const int b = __ffs(word) - 1; word &= word - 1;
+        const int64_t i = (wi << 5) + b - a.so;
+        L[pos++] = (int32_t)i;
+        syn_push_events(a, i, 0, flag);
     }
 }
 
 static __global__ void __launch_bounds__(256) k_syn_gather(const __grid_constant__ SynEvGroup g) {
     const long long nstep = g.ctl->nstep;
-    const int64_t total = g.item0[g.nobj];
-    for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < total; x += (int64_t)gridDim.x * blockDim.x) {
+    const int nlist = g.pair0[g.nobj] * g.nparts;
+    if (blockIdx.x == 0 && threadIdx.x < g.nobj) {
+        // the next step's list row starts empty (no one reads it this step)
+        const SynEvArgs &a = g.o[threadIdx.x];
+        a.scnt[(nstep + 1) % a.sdepth] = 0;
+    }
+    if ((int)blockIdx.x < nlist) {
+        const int pair = (int)blockIdx.x / g.nparts, part = (int)blockIdx.x % g.nparts;
         int k = 0;
-        while (k + 1 < g.nobj && x >= g.item0[k + 1]) ++k;
-        syn_gather_item(g.o[k], nstep, x - g.item0[k]);
+        while (k + 1 < g.nobj && pair >= g.pair0[k + 1]) ++k;
+        const SynEvArgs &a = g.o[k];
+        const int d = 1 + pair - g.pair0[k];
+        const int row = (int)((nstep - d + a.sdepth) % a.sdepth);
+        const int cnt = nstep < d ? 0 : a.scnt[row];
+        const int32_t *L = a.slist + (int64_t)row * a.sn;
+        int *flag = a.use_pull + (nstep & 1);
+        for (int e = part * blockDim.x + threadIdx.x; e < cnt; e += g.nparts * blockDim.x)
+            syn_push_events(a, L[e], d, flag);
+    } else {
+        const int64_t total = g.item0[g.nobj];
+        for (int64_t x = ((int64_t)blockIdx.x - nlist) * blockDim.x + threadIdx.x; x < total;
+             x += (int64_t)(gridDim.x - nlist) * blockDim.x) {
+            int k = 0;
+            while (k + 1 < g.nobj && x >= g.item0[k + 1]) ++k;
+            syn_gather_word(g.o[k], nstep, x - g.item0[k]);
+        }
     }
     bg_finish_step(g.ctl, g.last);
 }
 
-constexpr int kSynBinThreads = 1024;
+// The spike lists of steps t-1 .. t-dmax rebuilt from the spike history
+// (before a run whose history did not come from the gather: a new or
+// reinitialised network, a loaded state); the rows' counts are zero.
+static __global__ void __launch_bounds__(256) k_syn_lists(const SynEvArgs a) {
+    const long long nstep = a.ctl->nstep;
+    const int64_t w0 = a.so >> 5, nw = ((a.so + a.sn + 31) >> 5) - w0;
+    for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < nw * a.dmax; x += (int64_t)gridDim.x * blockDim.x) {
+        const int d = 1 + (int)(x / nw);
+        const int64_t wi = w0 + x % nw;
+        if (nstep < d) continue;
+        uint32_t word = masked_word(a.hist + (int64_t)((nstep - d) % a.depth) * a.nwords, wi, a.so, a.so + a.sn);
+        if (!word) continue;
+        const int row = (int)((nstep - d) % a.sdepth);
+        int pos = atomicAdd(a.scnt + row, __popc(word));
+        while (word) {
+            const int b = __ffs(word) - 1; word &= word - 1;
+            a.slist[(int64_t)row * a.sn + pos++] = (int32_t)((wi << 5) + b - a.so);
+        }
+    }
+}
+
+constexpr int kSynBinThreads = 512;
+constexpr int kSynTPT = kSynBin / kSynBinThreads;       // targets per thread (consecutive)
 constexpr int kSynSegMax = 64;                          // events of one target per step sorted by its thread
-static_assert(kSynBin == kSynBinThreads, "one thread per target of a bin");
+static_assert(kSynTPT == 2, "two targets per thread of a bin block");
+
+// a target's variables plus its events (x holds its slots)
+__device__ __forceinline__ void syn_apply_terms(const SynEvArgs &a, double (&x)[kSynMaxOps], int64_t q) {
+#pragma unroll
+    for (int k = 0; k < kSynMaxOps; ++k) {
+        if (k >= a.nops) break;
+        const double t = a.term[(int64_t)k * a.nsyn + q];
+#pragma unroll
+        for (int s = 0; s < kSynMaxOps; ++s)
+            if (s == a.slot_of[k]) x[s] = a.sub[k] ? __dsub_rn(x[s], t) : __dadd_rn(x[s], t);
+    }
+}
+__device__ __forceinline__ void syn_load_slots(const SynEvArgs &a, int64_t j, double (&x)[kSynMaxOps]) {
+#pragma unroll
+    for (int s = 0; s < kSynMaxOps; ++s) x[s] = s < a.nslots ? a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] : 0.0;
+}
+__device__ __forceinline__ void syn_store_slots(const SynEvArgs &a, int64_t j, const double (&x)[kSynMaxOps]) {
+#pragma unroll
+    for (int s = 0; s < kSynMaxOps; ++s)
+        if (s < a.nslots) a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] = x[s];
+}
+
 // one bin of one object: its events sorted by key and applied per target in
-// key order, or the pull's test for a step whose events overflowed
+// key order, or the pull's test for a step whose events overflowed.  Thread
+// t serves targets kSynTPT*t .. kSynTPT*t + kSynTPT - 1 of the bin.
 __device__ __forceinline__ void syn_bins_block(const SynEvArgs &a, long long nstep, int bin) {
     extern __shared__ unsigned char syn_smem[];
     unsigned long long *key = reinterpret_cast<unsigned long long *>(syn_smem);
@@ -1463,19 +1549,19 @@ __device__ __forceinline__ void syn_bins_block(const SynEvArgs &a, long long nst
     const int tid = threadIdx.x;
     const int n = min(a.bin_cnt[bin], kSynBinCap);
     const bool pull = a.use_pull[nstep & 1] != 0;
+    const int64_t j0 = (int64_t)bin * kSynBin + kSynTPT * tid;        // this thread's first target
     __syncthreads();   // every thread has read the bin's count before thread 0 clears it
     if (pull) {
         // a step whose events overflowed: every target of the bin walks its
         // incoming synapses in queue order and applies those whose source
-        // spiked d steps ago (the pull's test, one target per thread)
-        const int64_t j = (int64_t)bin * kSynBin + tid;
-        if (j < a.tn) {
-            const int row0 = (int)(nstep % a.depth);
+        // spiked d steps ago (the pull's test)
+        const int row0 = (int)(nstep % a.depth);
+        for (int u = 0; u < kSynTPT; ++u) {
+            const int64_t j = j0 + u;
+            if (j >= a.tn) break;
             double x[kSynMaxOps];
+            syn_load_slots(a, j, x);
             bool any = false;
-#pragma unroll
-            for (int s = 0; s < kSynMaxOps; ++s)
-                x[s] = s < a.nslots ? a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] : 0.0;
             for (int64_t q = a.colptr[j]; q < a.colptr[j + 1]; ++q) {
                 const uint32_t wd = a.word[q];
                 const int lag = (int)(wd >> 24) - 1;
@@ -1485,20 +1571,9 @@ __device__ __forceinline__ void syn_bins_block(const SynEvArgs &a, long long nst
                 row += row < 0 ? a.depth : 0;
                 if (!((a.hist[(int64_t)row * a.nwords + (src >> 5)] >> (src & 31)) & 1u)) continue;
                 any = true;
-#pragma unroll
-                for (int k = 0; k < kSynMaxOps; ++k) {
-                    if (k >= a.nops) break;
-                    const double t = a.term[(int64_t)k * a.nsyn + q];
-#pragma unroll
-                    for (int s = 0; s < kSynMaxOps; ++s)
-                        if (s == a.slot_of[k]) x[s] = a.sub[k] ? __dsub_rn(x[s], t) : __dadd_rn(x[s], t);
-                }
+                syn_apply_terms(a, x, q);
             }
-            if (any) {
-#pragma unroll
-                for (int s = 0; s < kSynMaxOps; ++s)
-                    if (s < a.nslots) a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] = x[s];
-            }
+            if (any) syn_store_slots(a, j, x);
         }
     } else if (n > 0) {
         // events per target of the bin (a counting sort by target): each
@@ -1515,30 +1590,37 @@ __device__ __forceinline__ void syn_bins_block(const SynEvArgs &a, long long nst
         unsigned long long k0 = 0;
         int32_t q0 = 0;
         if (tid < n) { k0 = a.bin_key[e0 + tid]; q0 = a.bin_q[e0 + tid]; }
-        tcnt[tid] = 0;
+#pragma unroll
+        for (int u = 0; u < kSynTPT; ++u) tcnt[kSynTPT * tid + u] = 0;
         if (tid == 0) maxc = 0;
         __syncthreads();
         if (tid < n) atomicAdd(&tcnt[(int)((k0 >> 40) - (unsigned long long)bin * kSynBin)], 1);
         for (int e = tid + kSynBinThreads; e < n; e += kSynBinThreads)
             atomicAdd(&tcnt[(int)((a.bin_key[e0 + e] >> 40) - (unsigned long long)bin * kSynBin)], 1);
         __syncthreads();
-        const int c = tcnt[tid];
-        if (c) atomicMax(&maxc, c);
+        int cu[kSynTPT], c = 0, cmax = 0;
+#pragma unroll
+        for (int u = 0; u < kSynTPT; ++u) { cu[u] = tcnt[kSynTPT * tid + u]; c += cu[u]; cmax = max(cmax, cu[u]); }
+        if (cmax) atomicMax(&maxc, cmax);
         int incl = c;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) { const int v = __shfl_up_sync(0xffffffffu, incl, o); if (lane >= o) incl += v; }
         if (lane == 31) wsum[warp] = incl;
         __syncthreads();
         if (warp == 0) {
-            int v = wsum[lane];
+            int v = lane < kSynBinThreads / 32 ? wsum[lane] : 0;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) { const int u = __shfl_up_sync(0xffffffffu, v, o); if (lane >= o) v += u; }
-            wsum[lane] = v;
+            if (lane < kSynBinThreads / 32) wsum[lane] = v;
         }
         __syncthreads();
         const int beg = (warp ? wsum[warp - 1] : 0) + incl - c;
         if (maxc <= kSynSegMax) {                       // uniform
-            tcnt[tid] = beg;                            // the segment's fill cursor
+            {
+                int b = beg;                            // the segments' fill cursors
+#pragma unroll
+                for (int u = 0; u < kSynTPT; ++u) { tcnt[kSynTPT * tid + u] = b; b += cu[u]; }
+            }
             __syncthreads();
             if (tid < n) {
                 const int pos = atomicAdd(&tcnt[(int)((k0 >> 40) - (unsigned long long)bin * kSynBin)], 1);
@@ -1552,87 +1634,64 @@ __device__ __forceinline__ void syn_bins_block(const SynEvArgs &a, long long nst
                 qv[pos] = a.bin_q[e0 + e];
             }
             __syncthreads();
-            const int64_t j = (int64_t)bin * kSynBin + tid;
-            if (c && j < a.tn) {
-                for (int u = beg + 1; u < beg + c; ++u) {
-                    const unsigned long long kk = key[u];
-                    const int32_t qq = qv[u];
-                    int w = u - 1;
-                    while (w >= beg && key[w] > kk) { key[w + 1] = key[w]; qv[w + 1] = qv[w]; --w; }
-                    key[w + 1] = kk;
-                    qv[w + 1] = qq;
-                }
-                double x[kSynMaxOps];
+            int sb = beg;
 #pragma unroll
-                for (int s = 0; s < kSynMaxOps; ++s)
-                    x[s] = s < a.nslots ? a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] : 0.0;
-                for (int e = beg; e < beg + c; ++e) {
-                    const int64_t q = qv[e];
-#pragma unroll
-                    for (int k = 0; k < kSynMaxOps; ++k) {
-                        if (k >= a.nops) break;
-                        const double t = a.term[(int64_t)k * a.nsyn + q];
-#pragma unroll
-                        for (int s = 0; s < kSynMaxOps; ++s)
-                            if (s == a.slot_of[k]) x[s] = a.sub[k] ? __dsub_rn(x[s], t) : __dadd_rn(x[s], t);
+            for (int u = 0; u < kSynTPT; ++u) {
+                const int64_t j = j0 + u;
+                const int cc = cu[u];
+                if (cc && j < a.tn) {
+                    for (int v = sb + 1; v < sb + cc; ++v) {
+                        const unsigned long long kk = key[v];
+                        const int32_t qq = qv[v];
+                        int w = v - 1;
+                        while (w >= sb && key[w] > kk) { key[w + 1] = key[w]; qv[w + 1] = qv[w]; --w; }
+                        key[w + 1] = kk;
+                        qv[w + 1] = qq;
                     }
+                    double x[kSynMaxOps];
+                    syn_load_slots(a, j, x);
+                    for (int e = sb; e < sb + cc; ++e) syn_apply_terms(a, x, qv[e]);
+                    syn_store_slots(a, j, x);
                 }
-#pragma unroll
-                for (int s = 0; s < kSynMaxOps; ++s)
-                    if (s < a.nslots) a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] = x[s];
+                sb += cc;
             }
         } else {
-        int m = 1;
-        while (m < n) m <<= 1;
-        for (int e = tid; e < m; e += kSynBinThreads) {
-            if (e < n) { key[e] = a.bin_key[(int64_t)bin * kSynBinCap + e]; qv[e] = a.bin_q[(int64_t)bin * kSynBinCap + e]; }
-            else { key[e] = ~0ull; qv[e] = 0; }
-        }
-        __syncthreads();
-        // bitonic sort of (key, q) by key (keys are distinct)
-        for (int k = 2; k <= m; k <<= 1) {
-            for (int jj = k >> 1; jj > 0; jj >>= 1) {
-                for (int e = tid; e < m; e += kSynBinThreads) {
-                    const int o = e ^ jj;
-                    if (o > e) {
-                        const bool up = (e & k) == 0;
-                        const unsigned long long ka = key[e], kb = key[o];
-                        if ((ka > kb) == up) {
-                            key[e] = kb; key[o] = ka;
-                            const int32_t t = qv[e]; qv[e] = qv[o]; qv[o] = t;
+            int m = 1;
+            while (m < n) m <<= 1;
+            for (int e = tid; e < m; e += kSynBinThreads) {
+                if (e < n) { key[e] = a.bin_key[e0 + e]; qv[e] = a.bin_q[e0 + e]; }
+                else { key[e] = ~0ull; qv[e] = 0; }
+            }
+            __syncthreads();
+            // bitonic sort of (key, q) by key (keys are distinct)
+            for (int k = 2; k <= m; k <<= 1) {
+                for (int jj = k >> 1; jj > 0; jj >>= 1) {
+                    for (int e = tid; e < m; e += kSynBinThreads) {
+                        const int o = e ^ jj;
+                        if (o > e) {
+                            const bool up = (e & k) == 0;
+                            const unsigned long long ka = key[e], kb = key[o];
+                            if ((ka > kb) == up) {
+                                key[e] = kb; key[o] = ka;
+                                const int32_t t = qv[e]; qv[e] = qv[o]; qv[o] = t;
+                            }
                         }
                     }
+                    __syncthreads();
                 }
-                __syncthreads();
             }
-        }
-        // each target of the bin: its events, in key order
-        const int64_t j = (int64_t)bin * kSynBin + tid;
-        if (j < a.tn) {
-            const unsigned long long want = (unsigned long long)j;
-            int l = 0, h = n;
-            while (l < h) { const int mm = (l + h) >> 1; if ((key[mm] >> 40) < want) l = mm + 1; else h = mm; }
-            if (l < n && (key[l] >> 40) == want) {
+            // each target of the thread: its events, in key order
+            for (int u = 0; u < kSynTPT; ++u) {
+                const int64_t j = j0 + u;
+                if (j >= a.tn || !cu[u]) continue;
+                const unsigned long long want = (unsigned long long)j;
+                int l = 0, h = n;
+                while (l < h) { const int mm = (l + h) >> 1; if ((key[mm] >> 40) < want) l = mm + 1; else h = mm; }
                 double x[kSynMaxOps];
-#pragma unroll
-                for (int s = 0; s < kSynMaxOps; ++s)
-                    x[s] = s < a.nslots ? a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] : 0.0;
-                for (int e = l; e < n && (key[e] >> 40) == want; ++e) {
-                    const int64_t q = qv[e];
-#pragma unroll
-                    for (int k = 0; k < kSynMaxOps; ++k) {
-                        if (k >= a.nops) break;
-                        const double t = a.term[(int64_t)k * a.nsyn + q];
-#pragma unroll
-                        for (int s = 0; s < kSynMaxOps; ++s)
-                            if (s == a.slot_of[k]) x[s] = a.sub[k] ? __dsub_rn(x[s], t) : __dadd_rn(x[s], t);
-                    }
-                }
-#pragma unroll
-                for (int s = 0; s < kSynMaxOps; ++s)
-                    if (s < a.nslots) a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] = x[s];
+                syn_load_slots(a, j, x);
+                for (int e = l; e < n && (key[e] >> 40) == want; ++e) syn_apply_terms(a, x, qv[e]);
+                syn_store_slots(a, j, x);
             }
-        }
         }
     }
     if (tid == 0) {
@@ -1641,7 +1700,7 @@ __device__ __forceinline__ void syn_bins_block(const SynEvArgs &a, long long nst
     }
 }
 
-static __global__ void __launch_bounds__(kSynBinThreads, 2) k_syn_bins(const __grid_constant__ SynEvGroup g) {
+static __global__ void __launch_bounds__(kSynBinThreads, 4) k_syn_bins(const __grid_constant__ SynEvGroup g) {
     int k = 0;
     while (k + 1 < g.nobj && (int)blockIdx.x >= g.bin0[k + 1]) ++k;
     syn_bins_block(g.o[k], g.ctl->nstep, (int)blockIdx.x - g.bin0[k]);

@@ -154,6 +154,7 @@ struct HSyn {
     int *dBinCnt = nullptr; unsigned long long *dBinKey = nullptr; int32_t *dBinQ = nullptr; int *dUsePull = nullptr;
     int32_t *dDoff = nullptr;           // per source, start of each delay in its row (when it fits 256 MB)
     int nbins = 0;
+    int32_t *dSlist = nullptr; int *dScnt = nullptr; int sdepth = 0;   // spike lists of the last sdepth steps
     // synapses with code (bg_synapses_set_code): synaptic variables [nsv][nsyn]
     // (synapse order on the host, column order on the device), the generated
     // pre/post code, the target variables it uses (slots; `writes` those it
@@ -220,6 +221,7 @@ struct bg_net {
     int check_finite = 0;               // check the states for NaN/inf after every run
     bool failed = false;                // a device error stopped the network
     int syn_events_forced = 0;          // Synapses: event path whatever the size (tests)
+    bool syn_lists_stale = true;        // Synapses spike lists to rebuild from the history before the next step
     std::vector<void *> allocs;
     struct Import { void *ptr; int64_t bytes; int dtype; };
     std::vector<Import> imports;        // borrowed device buffers (the caller owns and frees them)
@@ -601,6 +603,7 @@ bg::SynEvArgs syn_ev_args(bg_net *net, int yi) {
     e.srcptr = y.dSrcPtr; e.sd = y.dSd; e.stgt = y.dStgt; e.sq = y.dSq; e.doff = y.dDoff;
     e.colptr = y.dColptr; e.word = y.dWord;
     e.bin_cnt = y.dBinCnt; e.bin_key = y.dBinKey; e.bin_q = y.dBinQ; e.nbins = y.nbins; e.use_pull = y.dUsePull;
+    e.slist = y.dSlist; e.scnt = y.dScnt; e.sdepth = y.sdepth;
     e.term = y.dTerm; e.nsyn = y.nsyn; e.nops = y.nops;
     for (int k = 0; k < y.nops; ++k) {
         int sl = -1;
@@ -625,12 +628,18 @@ int build_syn_events(bg_net *net, const std::vector<int> &ids) {
         const HSyn &y = net->syns[ids[k]];
         g.o[k] = syn_ev_args(net, ids[k]);
         const int64_t nw = (y.so + y.sn + 31) / 32 - y.so / 32;
-        g.item0[k + 1] = g.item0[k] + nw * (y.dmax + 1);
-        if (nw * (y.dmax + 1) >= ((int64_t)1 << 31)) return fail(BG_ENOSYS, "Synapses event path: too many (delay, word) items");
+        g.item0[k + 1] = g.item0[k] + nw;
+        g.pair0[k + 1] = g.pair0[k] + y.dmax;
         g.bin0[k + 1] = g.bin0[k] + y.nbins;
         tag += (k ? ",y" : "y") + std::to_string(ids[k]);
     }
-    const int64_t ggrid = std::max<int64_t>(1, std::min<int64_t>((g.item0[g.nobj] + 255) / 256, (int64_t)sm_count() * 8));
+    // every (object, delay) list split over nparts blocks (about four list
+    // blocks per SM in all), then the blocks of this step's history words
+    const int npair = g.pair0[g.nobj];
+    g.nparts = npair ? std::max(1, sm_count() * 4 / npair) : 1;
+    const int64_t ggrid = (int64_t)npair * g.nparts +
+                          std::max<int64_t>(1, std::min<int64_t>((g.item0[g.nobj] + 255) / 256, (int64_t)sm_count() * 4));
+    if (ggrid >= ((int64_t)1 << 31)) return fail(BG_ENOSYS, "Synapses event path: too many gather blocks");
     const size_t bsmem = (size_t)bg::kSynBinCap * (8 + 4);
     cudaFuncSetAttribute(bg::k_syn_bins, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem);
     net->item_names.push_back("syn_gather[" + tag + "]");
@@ -809,6 +818,7 @@ int upload_state(bg_net *net, HGroup &g, int var, const double *in) {
 }
 
 int reset_dynamic(bg_net *net) {
+    net->syn_lists_stale = true;
     for (auto &g : net->groups) {
         BG_CUDA(cudaMemsetAsync(g.dHist, 0, (size_t)g.depth * (g.npad / 32) * 4, net->stream));
         if (g.dNext) {
@@ -2083,6 +2093,8 @@ static int prepare_impl(bg_net *n) {
             int64_t words = 0;
             for (const auto &o : n->syns) words += o.nsyn;
             if (!n->syn_events_forced && words * 4 <= (int64_t)l2 / 2) y.events = false;
+            // the spike lists hold every source for dmax + 2 steps
+            if ((int64_t)(y.dmax + 2) * y.sn * 4 > ((int64_t)1 << 30)) y.events = false;
         }
         if (y.events) {
             y.nbins = (int)((y.tn + bg::kSynBin - 1) / bg::kSynBin);
@@ -2092,6 +2104,11 @@ static int prepare_impl(bg_net *n) {
                 n->alloc(&y.dBinKey, (size_t)y.nbins * bg::kSynBinCap * 8) != cudaSuccess ||
                 n->alloc(&y.dBinQ, (size_t)y.nbins * bg::kSynBinCap * 4) != cudaSuccess || n->alloc(&y.dUsePull, 8) != cudaSuccess)
                 return fail(BG_ENOMEM, "synapse events");
+            y.sdepth = y.dmax + 2;
+            if (n->alloc(&y.dSlist, (size_t)y.sdepth * std::max<int64_t>(1, y.sn) * 4) != cudaSuccess ||
+                n->alloc(&y.dScnt, (size_t)y.sdepth * 4) != cudaSuccess)
+                return fail(BG_ENOMEM, "synapse spike lists");
+            BG_CUDA(cudaMemsetAsync(y.dScnt, 0, (size_t)y.sdepth * 4, n->stream));
             if ((st = upload(n, y.dSrcPtr, y.srcptr.data(), (y.sn + 1) * 8)) || (st = upload(n, y.dSd, y.sd.data(), y.nsyn)) ||
                 (st = upload(n, y.dStgt, y.stgt.data(), y.nsyn * 4)) || (st = upload(n, y.dSq, y.sq.data(), y.nsyn * 4)))
                 return st;
@@ -2180,6 +2197,26 @@ static int prepare_impl(bg_net *n) {
     if (st) return st;
     BG_CUDA(cudaStreamSynchronize(n->stream));
     n->prepared = true;
+    return BG_OK;
+}
+
+// The event path's spike lists of the last dmax steps, rebuilt from the
+// spike history when it did not come from the gather launches.
+static int refresh_syn_lists(bg_net *n) {
+    if (!n->syn_lists_stale) return BG_OK;
+    for (size_t yi = 0; yi < n->syns.size(); ++yi) {
+        const HSyn &y = n->syns[yi];
+        if (!y.events || y.coded || !y.dScnt) continue;
+        BG_CUDA(cudaMemsetAsync(y.dScnt, 0, (size_t)y.sdepth * 4, n->stream));
+        if (y.dmax == 0) continue;
+        const bg::SynEvArgs a = syn_ev_args(n, (int)yi);
+        const int64_t nw = (y.so + y.sn + 31) / 32 - y.so / 32;
+        const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((nw * y.dmax + 255) / 256, (int64_t)sm_count() * 8));
+        bg::k_syn_lists<<<(unsigned)grid, 256, 0, n->stream>>>(a);
+        BG_CUDA(cudaGetLastError());
+        n->launches += 1;
+    }
+    n->syn_lists_stale = false;
     return BG_OK;
 }
 
@@ -2310,6 +2347,7 @@ static int net_run_steps(bg_net *n, int64_t nsteps, int64_t cs0) {
     }
     int st = ensure_graph(n);
     if (st) return st;
+    if ((st = refresh_syn_lists(n))) return st;
     long long off = cs0 - n->nstep;
     BG_CUDA(cudaMemcpyAsync(&n->dCtl->clock_off, &off, 8, cudaMemcpyHostToDevice, n->stream));
     BG_CUDA(cudaStreamSynchronize(n->stream));
@@ -2540,6 +2578,7 @@ int bg_net_load_state(bg_net *n, const void *buf, int64_t bytes) {
     if (!ok) { n->failed = true; return fail(BG_EINVAL, r.err + "; the network must be rebuilt"); }
     if (r.left) { n->failed = true; return fail(BG_EINVAL, "state has trailing bytes; the network must be rebuilt"); }
     n->nstep = nstep;
+    n->syn_lists_stale = true;
     long long ns = nstep;
     BG_CUDA(cudaMemcpy(&n->dCtl->nstep, &ns, 8, cudaMemcpyHostToDevice));
     for (auto &m : n->stmons) BG_CUDA(cudaMemcpy(m.dRowBase, &m.rows_done, 8, cudaMemcpyHostToDevice));
@@ -2681,6 +2720,8 @@ int bg_net_profile(bg_net *n, int64_t nsteps, int64_t cs0, double *ms, int64_t c
     }
     const size_t k = n->step_launches.size();
     *nitems = (int64_t)k;
+    int st0 = refresh_syn_lists(n);
+    if (st0) return st0;
     long long off = cs0 - n->nstep;
     BG_CUDA(cudaMemcpyAsync(&n->dCtl->clock_off, &off, 8, cudaMemcpyHostToDevice, n->stream));
     std::vector<cudaEvent_t> ev(k + 1);

@@ -137,3 +137,40 @@ def test_state_refused_by_another_network(oracle_table):
         with pytest.raises(Exception):
             other._binding.rt.load_state(blob)
         other._invalidate()
+
+
+def _synapses():
+    np.random.seed(21)                      # connect_random and rand() draw from numpy's global generator
+    G = b.NeuronGroup(300, model="dv/dt = -v/(10*ms) : volt", threshold=5 * mV, reset=0 * mV)
+    src = b.PoissonGroup(200, rates=120.0, seed=3)
+    S = b.Synapses(src, G, model="w : volt", pre="v += w")
+    S.connect_random(sparseness=0.2)
+    S.w = "0.2*mV * (1 + (i % 3))"
+    S.delay = "rand() * 3*ms"
+    return b.Network(src, G, S, b.SpikeMonitor(G), b.StateMonitor(G, "v", record=[0, 7]))
+
+
+@pytest.mark.parametrize("events", [None, True], ids=["by-size", "events"])
+def test_checkpoint_synapses_oracle(oracle_table, events):
+    b.set_global_preferences(synapse_events=events)
+    try:
+        whole, resumed = checkpoint_roundtrip(_synapses, 213, 190, oracle_table)
+    finally:
+        b.set_global_preferences(synapse_events=None)
+    assert len(whole["spk3"][1]) > 100
+    _equal(whole, resumed)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("events", [None, True], ids=["by-size", "events"])
+def test_checkpoint_synapses_gpu(gpu_table, events):
+    """Synapses with delays up to 3 ms resumed 21.3 ms into the run: the
+    event path rebuilds the spike lists of the last 30 steps from the loaded
+    spike history."""
+    b.set_global_preferences(synapse_events=events)
+    try:
+        whole, resumed = checkpoint_roundtrip(_synapses, 213, 190)
+    finally:
+        b.set_global_preferences(synapse_events=None)
+    assert len(whole["spk3"][1]) > 100
+    _equal(whole, resumed)
