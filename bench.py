@@ -455,6 +455,7 @@ def profile_case(case, seed):
           batch 4096 (launch 12 of k_gemm is the 512 x 512 hidden layer of
           the second step).
     synapses: CUBA through Synapses (see synapses_case).
+    synapses_262k: the same at 262 144 neurons (the event path), 300 steps.
     stdp: the STDP scale-up network, 300 steps.
     batch: 148 CUBA-4000 networks in one NetworkBatch at the default shape
           (1024 x 4, 32 lanes), 2000 steps, no autotuning: the first k_batch
@@ -487,6 +488,13 @@ def profile_case(case, seed):
         print(json.dumps({"case": "gemm", "train_ms": ms, "steps": n // 4096, "loss": float(loss[0])}))
     elif case == "synapses":
         print(json.dumps(synapses_case(seed)))
+    elif case == "synapses_262k":
+        # the event path at 262 144 neurons without a monitor, 300 steps:
+        # each step launches the group kernel, k_syn_gather and k_syn_bins
+        net, _, _, _ = synapses_network(seed, 262144, 160, False)
+        net.run(300 * DT)
+        st = net._binding.rt.stats()
+        print(json.dumps({"case": "synapses_262k", "steps": 300, "us_per_step": st["last_run_ms"] * 1e3 / 300}))
     elif case == "stdp":
         # the STDP scale-up network (164 MB of weights) for 300 steps: the
         # outputs fire on about half the steps from step ~100 on, so launches
@@ -510,6 +518,45 @@ def profile_case(case, seed):
         raise SystemExit("unknown profile case %r" % case)
 
 
+def synapses_network(seed, n, indegree, monitor):
+    """CUBA through Synapses (see synapses_case): returns (net, syns, outdeg, M)."""
+    import brian_b200 as b
+    from brian_b200 import ms, mV
+    from brian_b200._lib import fixed_indegree_csr_native
+
+    rng = np.random.default_rng(seed)
+    b.clear()
+    b.reinit_default_clock()
+    eqs = b.Equations("""
+    dv/dt  = (ge+gi-(v-El))/taum : volt
+    dge/dt = -ge/taue : volt
+    dgi/dt = -gi/taui : volt
+    """, taum=20 * ms, taue=5 * ms, taui=10 * ms, El=-49 * mV)
+    P = b.NeuronGroup(n, model=eqs, threshold=-50 * mV, reset=-60 * mV)
+    ne = int(0.8 * n)
+    Pe, Pi = P.subgroup(ne), P.subgroup(n - ne)
+    syns, outdeg = [], np.zeros(n, dtype=np.int64)
+    for src, cnt, k, w, var, off in ((Pe, ne, int(0.8 * indegree), 1.62 * 80 / indegree * mV, "ge", 0),
+                                     (Pi, n - ne, indegree - int(0.8 * indegree), 9 * 80 / indegree * mV, "gi",
+                                      ne)):
+        S = b.Synapses(src, P, model="w : volt", pre="%s %s= w" % (var, "+" if var == "ge" else "-"))
+        rowptr, cols = fixed_indegree_csr_native(cnt, n, k, seed + off)
+        S.create_synapses(np.repeat(np.arange(cnt), np.diff(rowptr)), cols)
+        S.w = w * (0.5 + rng.random(len(S)))
+        S.delay = rng.random(len(S)) * 4 * ms
+        outdeg[off:off + cnt] = np.diff(rowptr)
+        syns.append(S)
+    P.v = -60 * mV + rng.random(n) * 10 * mV
+    objs = [P] + syns
+    M = None
+    if monitor:
+        M = b.SpikeMonitor(P)
+        objs.append(M)
+    net = b.Network(*objs)
+    net.prepare()
+    return net, syns, outdeg, M
+
+
 def synapses_case(seed, n=32768, indegree=160, sim_steps=2000, profile_steps=300):
     """CUBA through Synapses: n LIF neurons, fixed in-degree (80 % exc, 20 %
     inh) built with create_synapses, per-synapse weights, float delays
@@ -519,48 +566,11 @@ def synapses_case(seed, n=32768, indegree=160, sim_steps=2000, profile_steps=300
     delivery kernel's algorithmic bytes per launch (every incoming synapse
     word tested, the targets' state, the terms of the hits) against its
     mean duration."""
-    import brian_b200 as b
-    from brian_b200 import ms, mV
-    from brian_b200._lib import fixed_indegree_csr_native
-
-    def build(monitor):
-        rng = np.random.default_rng(seed)
-        b.clear()
-        b.reinit_default_clock()
-        eqs = b.Equations("""
-        dv/dt  = (ge+gi-(v-El))/taum : volt
-        dge/dt = -ge/taue : volt
-        dgi/dt = -gi/taui : volt
-        """, taum=20 * ms, taue=5 * ms, taui=10 * ms, El=-49 * mV)
-        P = b.NeuronGroup(n, model=eqs, threshold=-50 * mV, reset=-60 * mV)
-        ne = int(0.8 * n)
-        Pe, Pi = P.subgroup(ne), P.subgroup(n - ne)
-        syns, outdeg = [], np.zeros(n, dtype=np.int64)
-        for src, cnt, k, w, var, off in ((Pe, ne, int(0.8 * indegree), 1.62 * 80 / indegree * mV, "ge", 0),
-                                         (Pi, n - ne, indegree - int(0.8 * indegree), 9 * 80 / indegree * mV, "gi",
-                                          ne)):
-            S = b.Synapses(src, P, model="w : volt", pre="%s %s= w" % (var, "+" if var == "ge" else "-"))
-            rowptr, cols = fixed_indegree_csr_native(cnt, n, k, seed + off)
-            S.create_synapses(np.repeat(np.arange(cnt), np.diff(rowptr)), cols)
-            S.w = w * (0.5 + rng.random(len(S)))
-            S.delay = rng.random(len(S)) * 4 * ms
-            outdeg[off:off + cnt] = np.diff(rowptr)
-            syns.append(S)
-        P.v = -60 * mV + rng.random(n) * 10 * mV
-        objs = [P] + syns
-        M = None
-        if monitor:
-            M = b.SpikeMonitor(P)
-            objs.append(M)
-        net = b.Network(*objs)
-        net.prepare()
-        return net, syns, outdeg, M
-
-    net, syns, outdeg, _ = build(False)
+    net, syns, outdeg, _ = synapses_network(seed, n, indegree, False)
     rt = net._binding.rt
     net.run(100 * DT)
     prof = rt.profile(profile_steps, net.clock.step)
-    net, syns, outdeg, M = build(True)
+    net, syns, outdeg, M = synapses_network(seed, n, indegree, True)
     rt = net._binding.rt
     net.run(100 * DT)
     ev0 = len(M._record()[1])
@@ -571,13 +581,16 @@ def synapses_case(seed, n=32768, indegree=160, sim_steps=2000, profile_steps=300
     idx = np.asarray(M._record()[1])[ev0:]
     events = int(outdeg[idx].sum())
     nnz = sum(len(S) for S in syns)
-    dms = sum(v for k, v in prof if k.startswith("syn_"))
-    event_path = any(k.startswith("syn_gather") for k, _ in prof)
+    # the persistent kernel for Synapses is one item (the whole step)
+    persistent = any(k.startswith("persist") for k, _ in prof)
+    dms = sum(v for k, v in prof if k.startswith("syn_") or k.startswith("persist"))
+    event_path = persistent or any(k.startswith("syn_gather") for k, _ in prof)
     hits_per_step = events / sim_steps
     # algorithmic bytes of the delivery: the pull reads every synapse word,
     # the state and the column offsets, plus the terms of the hits; the event
     # path reads the spike history words of the delay window, per event a
     # target, a column position and a term and the bin entry written and read
+    # (the persistent kernel's time also covers the group update)
     if event_path:
         alg = (n / 32) * 4 * 41 + hits_per_step * (4 + 4 + 8 + 12 + 12) + n * 8 * 2
     else:
@@ -589,7 +602,7 @@ def synapses_case(seed, n=32768, indegree=160, sim_steps=2000, profile_steps=300
     from brian_b200.network import engine
     cpu_steps = 2000
     with engine(oracle.table()):
-        cnet, _, _, cM = build(True)
+        cnet, _, _, cM = synapses_network(seed, n, indegree, True)
         cnet.run(100 * DT)
         c0 = len(cM._record()[1])
         t1 = time.perf_counter()
@@ -605,7 +618,7 @@ def synapses_case(seed, n=32768, indegree=160, sim_steps=2000, profile_steps=300
             "spikes": int(len(idx)), "events": events, "device_ms": st["last_run_ms"], "wall_s": wall,
             "events_per_s": events / (st["last_run_ms"] * 1e-3), "us_per_step": st["last_run_ms"] * 1e3 / sim_steps,
             "launches_us": [(k, round(v * 1e3, 3)) for k, v in prof],
-            "delivery": "events" if event_path else "pull",
+            "delivery": ("events, persistent kernel" if persistent else "events") if event_path else "pull",
             "deliver_us_per_step": dms * 1e3, "deliver_alg_bytes": alg,
             "deliver_gbs": alg / (dms * 1e-3) / 1e9 if dms > 0 else None,
             "hbm_peak_gbs": peak, "peak_source": peak_src}
@@ -950,7 +963,7 @@ def main():
     ap.add_argument("--fit-batch", type=int, default=16384, help="rows per training step of the proposal network")
     ap.add_argument("--fit-lr", type=float, default=2e-3)
     ap.add_argument("--fit-iters", type=int, default=40)
-    ap.add_argument("--profile-case", choices=["fit", "gemm", "synapses", "stdp", "batch"], default=None,
+    ap.add_argument("--profile-case", choices=["fit", "gemm", "synapses", "synapses_262k", "stdp", "batch"], default=None,
                     help="run one small case for a single-kernel ncu capture and exit")
     args = ap.parse_args()
     if args.profile_case:

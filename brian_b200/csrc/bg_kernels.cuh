@@ -1412,8 +1412,10 @@ __device__ __forceinline__ void syn_src_range(const SynEvArgs &a, int64_t i, int
     }
 }
 
-// the events of source i's synapses of delay d, into the bins
-__device__ __forceinline__ void syn_push_events(const SynEvArgs &a, int64_t i, int d, int *flag) {
+// the events of source i's synapses of delay d, into the bins (bin_cnt,
+// bin_key, bin_q: the object's bins or one parity of them)
+__device__ __forceinline__ void syn_push_events(const SynEvArgs &a, int64_t i, int d, int *flag, int *bin_cnt,
+                                                unsigned long long *bin_key, int32_t *bin_q) {
     int64_t r0, r1;
     syn_src_range(a, i, d, r0, r1);
     if (r1 - r0 > 256) { atomicExch(flag, 1); return; }
@@ -1428,16 +1430,16 @@ __device__ __forceinline__ void syn_push_events(const SynEvArgs &a, int64_t i, i
             if (u < m) { tg[u] = __ldg(a.stgt + p0 + u); qs[u] = __ldg(a.sq + p0 + u); }
 #pragma unroll
         for (int u = 0; u < 8; ++u)
-            if (u < m) slot[u] = atomicAdd(a.bin_cnt + tg[u] / kSynBin, 1);
+            if (u < m) slot[u] = atomicAdd(bin_cnt + tg[u] / kSynBin, 1);
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
             if (u >= m) break;
             if (slot[u] >= kSynBinCap) { atomicExch(flag, 1); continue; }
             const int64_t j = tg[u];
             const int64_t e = (j / kSynBin) * kSynBinCap + slot[u];
-            a.bin_key[e] = ((unsigned long long)j << 40) | ((unsigned long long)(255 - d) << 32) |
-                           ((unsigned long long)i << 8) | (unsigned long long)(p0 + u - r0);
-            a.bin_q[e] = qs[u];
+            bin_key[e] = ((unsigned long long)j << 40) | ((unsigned long long)(255 - d) << 32) |
+                         ((unsigned long long)i << 8) | (unsigned long long)(p0 + u - r0);
+            bin_q[e] = qs[u];
         }
     }
 }
@@ -1456,7 +1458,7 @@ __device__ __forceinline__ void syn_gather_word(const SynEvArgs &a, long long ns
         const int b = __ffs(word) - 1; word &= word - 1;
         const int64_t i = (wi << 5) + b - a.so;
         L[pos++] = (int32_t)i;
-        syn_push_events(a, i, 0, flag);
+        syn_push_events(a, i, 0, flag, a.bin_cnt, a.bin_key, a.bin_q);
     }
 }
 
@@ -1479,7 +1481,7 @@ static __global__ void __launch_bounds__(256) k_syn_gather(const __grid_constant
         const int32_t *L = a.slist + (int64_t)row * a.sn;
         int *flag = a.use_pull + (nstep & 1);
         for (int e = part * blockDim.x + threadIdx.x; e < cnt; e += g.nparts * blockDim.x)
-            syn_push_events(a, L[e], d, flag);
+            syn_push_events(a, L[e], d, flag, a.bin_cnt, a.bin_key, a.bin_q);
     } else {
         const int64_t total = g.item0[g.nobj];
         for (int64_t x = ((int64_t)blockIdx.x - nlist) * blockDim.x + threadIdx.x; x < total;
@@ -1514,53 +1516,34 @@ static __global__ void __launch_bounds__(256) k_syn_lists(const SynEvArgs a) {
 }
 
 constexpr int kSynBinThreads = 512;
-constexpr int kSynTPT = kSynBin / kSynBinThreads;       // targets per thread (consecutive)
+constexpr int kSynTPT = kSynBin / kSynBinThreads;       // targets per thread
 constexpr int kSynSegMax = 64;                          // events of one target per step sorted by its thread
 static_assert(kSynTPT == 2, "two targets per thread of a bin block");
 
-// a target's variables plus its events (x holds its slots)
-__device__ __forceinline__ void syn_apply_terms(const SynEvArgs &a, double (&x)[kSynMaxOps], int64_t q) {
-#pragma unroll
-    for (int k = 0; k < kSynMaxOps; ++k) {
-        if (k >= a.nops) break;
-        const double t = a.term[(int64_t)k * a.nsyn + q];
-#pragma unroll
-        for (int s = 0; s < kSynMaxOps; ++s)
-            if (s == a.slot_of[k]) x[s] = a.sub[k] ? __dsub_rn(x[s], t) : __dadd_rn(x[s], t);
-    }
-}
-__device__ __forceinline__ void syn_load_slots(const SynEvArgs &a, int64_t j, double (&x)[kSynMaxOps]) {
-#pragma unroll
-    for (int s = 0; s < kSynMaxOps; ++s) x[s] = s < a.nslots ? a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] : 0.0;
-}
-__device__ __forceinline__ void syn_store_slots(const SynEvArgs &a, int64_t j, const double (&x)[kSynMaxOps]) {
-#pragma unroll
-    for (int s = 0; s < kSynMaxOps; ++s)
-        if (s < a.nslots) a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] = x[s];
-}
-
-// one bin of one object: its events sorted by key and applied per target in
-// key order, or the pull's test for a step whose events overflowed.  Thread
-// t serves targets kSynTPT*t .. kSynTPT*t + kSynTPT - 1 of the bin.
-__device__ __forceinline__ void syn_bins_block(const SynEvArgs &a, long long nstep, int bin) {
+// The events of one bin (step nstep, n events in gkey/gq) applied per target
+// in key order -- the pull's order -- or, when `pull` (the step overflowed),
+// the pull's test for every target of the bin.  Thread t serves the bin's
+// targets t and t + kSynBinThreads (u = 0, 1): f.begin(u, j) before the
+// first event of its target u (bin target index j), f.add(u, q) per event
+// (synapse column q), f.end(u, j) after the last.  The block's
+// kSynBinThreads threads all call it (it synchronises); dynamic shared memory
+// holds kSynBinCap keys and positions.
+template <class F>
+__device__ __forceinline__ void syn_bin_apply(const SynEvArgs &a, long long nstep, int bin, bool pull, int n,
+                                              const unsigned long long *gkey, const int32_t *gq, F &f) {
     extern __shared__ unsigned char syn_smem[];
     unsigned long long *key = reinterpret_cast<unsigned long long *>(syn_smem);
     int32_t *qv = reinterpret_cast<int32_t *>(key + kSynBinCap);
     const int tid = threadIdx.x;
-    const int n = min(a.bin_cnt[bin], kSynBinCap);
-    const bool pull = a.use_pull[nstep & 1] != 0;
-    const int64_t j0 = (int64_t)bin * kSynBin + kSynTPT * tid;        // this thread's first target
-    __syncthreads();   // every thread has read the bin's count before thread 0 clears it
+    const int64_t jb = (int64_t)bin * kSynBin;                  // the bin's first target
     if (pull) {
-        // a step whose events overflowed: every target of the bin walks its
-        // incoming synapses in queue order and applies those whose source
-        // spiked d steps ago (the pull's test)
+        // every target of the bin walks its incoming synapses in queue order
+        // and applies those whose source spiked d steps ago (the pull's test)
         const int row0 = (int)(nstep % a.depth);
+#pragma unroll
         for (int u = 0; u < kSynTPT; ++u) {
-            const int64_t j = j0 + u;
-            if (j >= a.tn) break;
-            double x[kSynMaxOps];
-            syn_load_slots(a, j, x);
+            const int64_t j = jb + u * kSynBinThreads + tid;
+            if (j >= a.tn) continue;
             bool any = false;
             for (int64_t q = a.colptr[j]; q < a.colptr[j + 1]; ++q) {
                 const uint32_t wd = a.word[q];
@@ -1569,132 +1552,168 @@ __device__ __forceinline__ void syn_bins_block(const SynEvArgs &a, long long nst
                 const int64_t src = a.so + (int64_t)(wd & 0xFFFFFFu);
                 int row = row0 - lag;
                 row += row < 0 ? a.depth : 0;
-                if (!((a.hist[(int64_t)row * a.nwords + (src >> 5)] >> (src & 31)) & 1u)) continue;
+                if (!((__ldcg(a.hist + (int64_t)row * a.nwords + (src >> 5)) >> (src & 31)) & 1u)) continue;
+                if (!any) f.begin(u, j);
                 any = true;
-                syn_apply_terms(a, x, q);
+                f.add(u, q);
             }
-            if (any) syn_store_slots(a, j, x);
+            if (any) f.end(u, j);
         }
-    } else if (n > 0) {
-        // events per target of the bin (a counting sort by target): each
-        // target's events go to its own segment, which its thread then
-        // orders by key (insertion sort: a target's events in one step are
-        // few); a bin with a target of more than kSynSegMax events takes the
-        // bitonic sort of the whole bin instead
-        __shared__ int tcnt[kSynBin];
-        __shared__ int wsum[kSynBinThreads / 32], maxc;
-        const int lane = tid & 31, warp = tid >> 5;
-        // the bin's first kSynBinThreads events stay in registers between
-        // the count and the placement
-        const int64_t e0 = (int64_t)bin * kSynBinCap;
-        unsigned long long k0 = 0;
-        int32_t q0 = 0;
-        if (tid < n) { k0 = a.bin_key[e0 + tid]; q0 = a.bin_q[e0 + tid]; }
+        return;
+    }
+    if (n <= 0) return;
+    // events per target (a counting sort by target): each target's events go
+    // to its own segment, which its thread then orders by key (insertion
+    // sort: a target's events in one step are few); a bin with a target of
+    // more than kSynSegMax events takes the bitonic sort of the whole bin
+    __shared__ int tcnt[kSynBin];
+    __shared__ int wsum[kSynBinThreads / 32], maxc;
+    const int lane = tid & 31, warp = tid >> 5;
+    // the bin's first kSynBinThreads events stay in registers between the
+    // count and the placement
+    unsigned long long k0 = 0;
+    int32_t q0 = 0;
+    if (tid < n) { k0 = __ldcg(gkey + tid); q0 = __ldcg(gq + tid); }
 #pragma unroll
-        for (int u = 0; u < kSynTPT; ++u) tcnt[kSynTPT * tid + u] = 0;
-        if (tid == 0) maxc = 0;
-        __syncthreads();
-        if (tid < n) atomicAdd(&tcnt[(int)((k0 >> 40) - (unsigned long long)bin * kSynBin)], 1);
-        for (int e = tid + kSynBinThreads; e < n; e += kSynBinThreads)
-            atomicAdd(&tcnt[(int)((a.bin_key[e0 + e] >> 40) - (unsigned long long)bin * kSynBin)], 1);
-        __syncthreads();
-        int cu[kSynTPT], c = 0, cmax = 0;
+    for (int u = 0; u < kSynTPT; ++u) tcnt[u * kSynBinThreads + tid] = 0;
+    if (tid == 0) maxc = 0;
+    __syncthreads();
+    if (tid < n) atomicAdd(&tcnt[(int)((k0 >> 40) - (unsigned long long)jb)], 1);
+    for (int e = tid + kSynBinThreads; e < n; e += kSynBinThreads)
+        atomicAdd(&tcnt[(int)((__ldcg(gkey + e) >> 40) - (unsigned long long)jb)], 1);
+    __syncthreads();
+    int cu[kSynTPT], c = 0, cmax = 0;
 #pragma unroll
-        for (int u = 0; u < kSynTPT; ++u) { cu[u] = tcnt[kSynTPT * tid + u]; c += cu[u]; cmax = max(cmax, cu[u]); }
-        if (cmax) atomicMax(&maxc, cmax);
-        int incl = c;
+    for (int u = 0; u < kSynTPT; ++u) { cu[u] = tcnt[u * kSynBinThreads + tid]; c += cu[u]; cmax = max(cmax, cu[u]); }
+    if (cmax) atomicMax(&maxc, cmax);
+    int incl = c;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) { const int v = __shfl_up_sync(0xffffffffu, incl, o); if (lane >= o) incl += v; }
-        if (lane == 31) wsum[warp] = incl;
-        __syncthreads();
-        if (warp == 0) {
-            int v = lane < kSynBinThreads / 32 ? wsum[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) { const int v = __shfl_up_sync(0xffffffffu, incl, o); if (lane >= o) incl += v; }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        int v = lane < kSynBinThreads / 32 ? wsum[lane] : 0;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) { const int u = __shfl_up_sync(0xffffffffu, v, o); if (lane >= o) v += u; }
-            if (lane < kSynBinThreads / 32) wsum[lane] = v;
+        for (int o = 1; o < 32; o <<= 1) { const int u = __shfl_up_sync(0xffffffffu, v, o); if (lane >= o) v += u; }
+        if (lane < kSynBinThreads / 32) wsum[lane] = v;
+    }
+    __syncthreads();
+    const int beg = (warp ? wsum[warp - 1] : 0) + incl - c;    // the thread's segments, u = 0 then 1
+    if (maxc <= kSynSegMax) {                                    // uniform
+        {
+            int b = beg;                                         // the segments' fill cursors
+#pragma unroll
+            for (int u = 0; u < kSynTPT; ++u) { tcnt[u * kSynBinThreads + tid] = b; b += cu[u]; }
         }
         __syncthreads();
-        const int beg = (warp ? wsum[warp - 1] : 0) + incl - c;
-        if (maxc <= kSynSegMax) {                       // uniform
-            {
-                int b = beg;                            // the segments' fill cursors
+        if (tid < n) {
+            const int pos = atomicAdd(&tcnt[(int)((k0 >> 40) - (unsigned long long)jb)], 1);
+            key[pos] = k0;
+            qv[pos] = q0;
+        }
+        for (int e = tid + kSynBinThreads; e < n; e += kSynBinThreads) {
+            const unsigned long long k = __ldcg(gkey + e);
+            const int pos = atomicAdd(&tcnt[(int)((k >> 40) - (unsigned long long)jb)], 1);
+            key[pos] = k;
+            qv[pos] = __ldcg(gq + e);
+        }
+        __syncthreads();
+        int sb = beg;
 #pragma unroll
-                for (int u = 0; u < kSynTPT; ++u) { tcnt[kSynTPT * tid + u] = b; b += cu[u]; }
-            }
-            __syncthreads();
-            if (tid < n) {
-                const int pos = atomicAdd(&tcnt[(int)((k0 >> 40) - (unsigned long long)bin * kSynBin)], 1);
-                key[pos] = k0;
-                qv[pos] = q0;
-            }
-            for (int e = tid + kSynBinThreads; e < n; e += kSynBinThreads) {
-                const unsigned long long k = a.bin_key[e0 + e];
-                const int pos = atomicAdd(&tcnt[(int)((k >> 40) - (unsigned long long)bin * kSynBin)], 1);
-                key[pos] = k;
-                qv[pos] = a.bin_q[e0 + e];
-            }
-            __syncthreads();
-            int sb = beg;
-#pragma unroll
-            for (int u = 0; u < kSynTPT; ++u) {
-                const int64_t j = j0 + u;
-                const int cc = cu[u];
-                if (cc && j < a.tn) {
-                    for (int v = sb + 1; v < sb + cc; ++v) {
-                        const unsigned long long kk = key[v];
-                        const int32_t qq = qv[v];
-                        int w = v - 1;
-                        while (w >= sb && key[w] > kk) { key[w + 1] = key[w]; qv[w + 1] = qv[w]; --w; }
-                        key[w + 1] = kk;
-                        qv[w + 1] = qq;
-                    }
-                    double x[kSynMaxOps];
-                    syn_load_slots(a, j, x);
-                    for (int e = sb; e < sb + cc; ++e) syn_apply_terms(a, x, qv[e]);
-                    syn_store_slots(a, j, x);
+        for (int u = 0; u < kSynTPT; ++u) {
+            const int64_t j = jb + u * kSynBinThreads + tid;
+            const int cc = cu[u];
+            if (cc && j < a.tn) {
+                for (int v = sb + 1; v < sb + cc; ++v) {
+                    const unsigned long long kk = key[v];
+                    const int32_t qq = qv[v];
+                    int w = v - 1;
+                    while (w >= sb && key[w] > kk) { key[w + 1] = key[w]; qv[w + 1] = qv[w]; --w; }
+                    key[w + 1] = kk;
+                    qv[w + 1] = qq;
                 }
-                sb += cc;
+                f.begin(u, j);
+                for (int e = sb; e < sb + cc; ++e) f.add(u, qv[e]);
+                f.end(u, j);
             }
-        } else {
-            int m = 1;
-            while (m < n) m <<= 1;
-            for (int e = tid; e < m; e += kSynBinThreads) {
-                if (e < n) { key[e] = a.bin_key[e0 + e]; qv[e] = a.bin_q[e0 + e]; }
-                else { key[e] = ~0ull; qv[e] = 0; }
-            }
-            __syncthreads();
-            // bitonic sort of (key, q) by key (keys are distinct)
-            for (int k = 2; k <= m; k <<= 1) {
-                for (int jj = k >> 1; jj > 0; jj >>= 1) {
-                    for (int e = tid; e < m; e += kSynBinThreads) {
-                        const int o = e ^ jj;
-                        if (o > e) {
-                            const bool up = (e & k) == 0;
-                            const unsigned long long ka = key[e], kb = key[o];
-                            if ((ka > kb) == up) {
-                                key[e] = kb; key[o] = ka;
-                                const int32_t t = qv[e]; qv[e] = qv[o]; qv[o] = t;
-                            }
+            sb += cc;
+        }
+    } else {
+        int m = 1;
+        while (m < n) m <<= 1;
+        for (int e = tid; e < m; e += kSynBinThreads) {
+            if (e < n) { key[e] = __ldcg(gkey + e); qv[e] = __ldcg(gq + e); }
+            else { key[e] = ~0ull; qv[e] = 0; }
+        }
+        __syncthreads();
+        // bitonic sort of (key, q) by key (keys are distinct)
+        for (int k = 2; k <= m; k <<= 1) {
+            for (int jj = k >> 1; jj > 0; jj >>= 1) {
+                for (int e = tid; e < m; e += kSynBinThreads) {
+                    const int o = e ^ jj;
+                    if (o > e) {
+                        const bool up = (e & k) == 0;
+                        const unsigned long long ka = key[e], kb = key[o];
+                        if ((ka > kb) == up) {
+                            key[e] = kb; key[o] = ka;
+                            const int32_t t = qv[e]; qv[e] = qv[o]; qv[o] = t;
                         }
                     }
-                    __syncthreads();
                 }
-            }
-            // each target of the thread: its events, in key order
-            for (int u = 0; u < kSynTPT; ++u) {
-                const int64_t j = j0 + u;
-                if (j >= a.tn || !cu[u]) continue;
-                const unsigned long long want = (unsigned long long)j;
-                int l = 0, h = n;
-                while (l < h) { const int mm = (l + h) >> 1; if ((key[mm] >> 40) < want) l = mm + 1; else h = mm; }
-                double x[kSynMaxOps];
-                syn_load_slots(a, j, x);
-                for (int e = l; e < n && (key[e] >> 40) == want; ++e) syn_apply_terms(a, x, qv[e]);
-                syn_store_slots(a, j, x);
+                __syncthreads();
             }
         }
+        // each target of the thread: its events, in key order
+#pragma unroll
+        for (int u = 0; u < kSynTPT; ++u) {
+            const int64_t j = jb + u * kSynBinThreads + tid;
+            if (j >= a.tn || !cu[u]) continue;
+            const unsigned long long want = (unsigned long long)j;
+            int l = 0, h = n;
+            while (l < h) { const int mm = (l + h) >> 1; if ((key[mm] >> 40) < want) l = mm + 1; else h = mm; }
+            f.begin(u, j);
+            for (int e = l; e < n && (key[e] >> 40) == want; ++e) f.add(u, qv[e]);
+            f.end(u, j);
+        }
     }
-    if (tid == 0) {
+    __syncthreads();                                             // shared memory free for the next bin
+}
+
+// the stepped path's target access: the target's slots loaded from the
+// group state, the statements applied, stored back
+struct SynSlotsF {
+    const SynEvArgs &a;
+    double x[kSynTPT][kSynMaxOps];
+    __device__ void begin(int u, int64_t j) {
+#pragma unroll
+        for (int s = 0; s < kSynMaxOps; ++s) x[u][s] = s < a.nslots ? a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] : 0.0;
+    }
+    __device__ void add(int u, int64_t q) {
+#pragma unroll
+        for (int k = 0; k < kSynMaxOps; ++k) {
+            if (k >= a.nops) break;
+            const double t = a.term[(int64_t)k * a.nsyn + q];
+#pragma unroll
+            for (int s = 0; s < kSynMaxOps; ++s)
+                if (s == a.slot_of[k]) x[u][s] = a.sub[k] ? __dsub_rn(x[u][s], t) : __dadd_rn(x[u][s], t);
+        }
+    }
+    __device__ void end(int u, int64_t j) {
+#pragma unroll
+        for (int s = 0; s < kSynMaxOps; ++s)
+            if (s < a.nslots) a.S[(int64_t)a.slot_var[s] * a.npad + a.to + j] = x[u][s];
+    }
+};
+
+// one bin of one object on the stepped path, then the bin emptied for the
+// next step
+__device__ __forceinline__ void syn_bins_block(const SynEvArgs &a, long long nstep, int bin) {
+    const int n = min(a.bin_cnt[bin], kSynBinCap);
+    const bool pull = a.use_pull[nstep & 1] != 0;
+    __syncthreads();   // every thread has read the bin's count before thread 0 clears it
+    SynSlotsF f{a};
+    syn_bin_apply(a, nstep, bin, pull, n, a.bin_key + (int64_t)bin * kSynBinCap, a.bin_q + (int64_t)bin * kSynBinCap, f);
+    if (threadIdx.x == 0) {
         a.bin_cnt[bin] = 0;                             // empty for the next step
         if (bin == 0) a.use_pull[(nstep + 1) & 1] = 0;  // next step's flag (nobody reads it this step)
     }

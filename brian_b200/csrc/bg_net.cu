@@ -19,6 +19,7 @@
 
 #include "bg_kernels.cuh"
 #include "bg_persist.cuh"
+#include "bg_synpersist.cuh"
 #include "bg_batch.cuh"
 #include "bg_rtc.h"
 #include "../../include/brian_b200.h"
@@ -155,6 +156,7 @@ struct HSyn {
     int32_t *dDoff = nullptr;           // per source, start of each delay in its row (when it fits 256 MB)
     int nbins = 0;
     int32_t *dSlist = nullptr; int *dScnt = nullptr; int sdepth = 0;   // spike lists of the last sdepth steps
+    double *dTermSrc = nullptr;         // persistent kernel: the statement's term per synapse, by-source order
     // synapses with code (bg_synapses_set_code): synaptic variables [nsv][nsyn]
     // (synapse order on the host, column order on the device), the generated
     // pre/post code, the target variables it uses (slots; `writes` those it
@@ -215,6 +217,8 @@ struct bg_net {
     // network does not have its shape
     std::function<cudaError_t(cudaStream_t, int nsteps)> persist;
     unsigned int *dArrived = nullptr;
+    int *dUsePull3 = nullptr;           // Synapses persistent kernel: overflow flags by step mod 3
+    int *dPBinCnt = nullptr; unsigned long long *dPBinKey = nullptr; double *dPBinT = nullptr;   //   and its bins
     int64_t launches = 0; double last_ms = 0;
     unsigned int spin_limit = BG_SPIN_LIMIT;   // polls of a bounded inter-block wait
     int hold_block = -1;                // test hook: a persistent block that never arrives
@@ -1191,6 +1195,159 @@ int build_persist(bg_net *net) {
     return BG_OK;
 }
 
+// The persistent kernel's copy of a Synapses object's terms in by-source
+// order (its one statement), from the column-order terms on the device.
+int refresh_term_src(bg_net *net, const HSyn &y) {
+    if (!y.dTermSrc || y.nsyn == 0) return BG_OK;
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((y.nsyn + 255) / 256, (int64_t)sm_count() * 8));
+    bg::k_syn_term_src<<<grid, 256, 0, net->stream>>>(y.dSq, y.dTerm, y.nsyn, y.dTermSrc);
+    BG_CUDA(cudaGetLastError());
+    BG_CUDA(cudaStreamSynchronize(net->stream));
+    return BG_OK;
+}
+
+// The persistent kernel of CUBA through Synapses (bg_synpersist.cuh): one
+// linear FP64 group whose event-path Synapses (static variables, additive
+// statements) all connect it to itself, bins aligned with the kernel's
+// 1024-neuron blocks, every block co-resident.  Otherwise the stepped path.
+int build_syn_persist(bg_net *net) {
+    net->persist = nullptr;
+    if (net->groups.size() != 1 || !net->conns.empty() || !net->stdps.empty() || net->syns.empty()) return BG_OK;
+    if (net->precision != 64 || (int)net->syns.size() > bg::kSynEvMerge) return BG_OK;
+    for (const HSyn &y : net->syns) {
+        if (!y.events || y.coded || y.src != 0 || y.tgt != 0 || y.to % bg::kSynBin != 0 || !y.dScnt) return BG_OK;
+        // one statement; one target range for all (the bins are shared, the
+        // key holds target * 4 + object below 2^24); sources below 2^24
+        if (y.nops != 1 || y.to != net->syns[0].to || y.tn != net->syns[0].tn) return BG_OK;
+        if (y.tn > ((int64_t)1 << 22) || y.sn >= ((int64_t)1 << 24)) return BG_OK;
+    }
+    for (const HSpikeMon &m : net->smons)
+        if (m.gid != 0 || m.delay != 0) return BG_OK;
+    if ((int)net->stmons.size() > bg::kMaxRec) return BG_OK;
+    const HGroup &g = net->groups[0];
+    if (!g.linear || g.nvar < 1 || g.nvar > 4 || g.refr || g.period > 0) return BG_OK;
+    if (g.generated() || g.emp_steps > 0 || !g.setters.empty()) return BG_OK;
+    if (g.thr_kind != BG_THR_CONST && g.thr_kind != BG_THR_VAR && g.thr_kind != BG_THR_NONE) return BG_OK;
+    {
+        int dev = 0, coop = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) return BG_OK;
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+        if (!coop) return BG_OK;
+    }
+    const int64_t blocks = (g.n + bg::kSPBn - 1) / bg::kSPBn;
+    const size_t smem = (size_t)bg::kSynBinCap * (8 + 8);
+    const void *kern[4][2] = {{(const void *)bg::k_syn_persist<1, false>, (const void *)bg::k_syn_persist<1, true>},
+                              {(const void *)bg::k_syn_persist<2, false>, (const void *)bg::k_syn_persist<2, true>},
+                              {(const void *)bg::k_syn_persist<3, false>, (const void *)bg::k_syn_persist<3, true>},
+                              {(const void *)bg::k_syn_persist<4, false>, (const void *)bg::k_syn_persist<4, true>}};
+    int64_t slots = -1;
+    for (int d = 0; d < 2; ++d) {
+        const void *k = kern[g.nvar - 1][d];
+        int per_sm = 0;
+        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, bg::kSPTh, smem) != cudaSuccess) {
+            cudaGetLastError();
+            return BG_OK;
+        }
+        const int64_t sl = (int64_t)per_sm * sm_count();
+        slots = slots < 0 ? sl : std::min(slots, sl);
+    }
+    if (blocks > slots) return BG_OK;
+    if (!net->dArrived && net->alloc(&net->dArrived, 64) != cudaSuccess) return fail(BG_ENOMEM, "arrival counter");
+    if (!net->dUsePull3) {
+        if (net->alloc(&net->dUsePull3, 16) != cudaSuccess) return fail(BG_ENOMEM, "overflow flags");
+        BG_CUDA(cudaMemsetAsync(net->dUsePull3, 0, 16, net->stream));
+    }
+    bg::SynPersistArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.ctl = net->dCtl; a.S = (double *)g.dS; a.n = g.n; a.npad = g.npad;
+    for (int j = 0; j < g.nvar; ++j) {
+        for (int k = 0; k < g.nvar; ++k) {
+            a.A[j * g.nvar + k] = g.A[j * g.nvar + k];
+            if (a.A[j * g.nvar + k] != 0) a.anz |= 1ull << (j * g.nvar + k);
+        }
+        a.C[j] = g.useC ? g.C[j] : 0.0;
+        if (a.C[j] != 0) a.cnz |= 1u << j;
+    }
+    a.thr_kind = g.thr_kind; a.thr_var = g.thr_var; a.thr_var2 = g.thr_var2; a.thr_val = g.thr_val;
+    a.reset_kind = g.reset_kind; a.reset_var = g.reset_var; a.reset_var2 = g.reset_var2; a.reset_val = g.reset_val;
+    a.hist = g.dHist; a.depth = g.depth; a.nwords = g.npad / 32;
+    a.nobj = (int)net->syns.size();
+    const HSyn &y0 = net->syns[0];
+    a.nbins = y0.nbins; a.blk0 = (int)(y0.to / bg::kSynBin); a.tn = y0.tn;
+    if (!net->dPBinCnt) {
+        if (net->alloc(&net->dPBinCnt, (size_t)2 * a.nbins * 4) != cudaSuccess ||
+            net->alloc(&net->dPBinKey, (size_t)2 * a.nbins * bg::kSynBinCap * 8) != cudaSuccess ||
+            net->alloc(&net->dPBinT, (size_t)2 * a.nbins * bg::kSynBinCap * 8) != cudaSuccess)
+            return fail(BG_ENOMEM, "synapse event bins");
+        BG_CUDA(cudaMemsetAsync(net->dPBinCnt, 0, (size_t)2 * a.nbins * 4, net->stream));
+    }
+    a.bin_cnt = net->dPBinCnt; a.bin_key = net->dPBinKey; a.bin_t = net->dPBinT;
+    for (int k = 0; k < a.nobj; ++k) {
+        HSyn &y = net->syns[k];
+        if (!y.dTermSrc) {
+            if (net->alloc(&y.dTermSrc, (size_t)std::max<int64_t>(1, y.nsyn) * 8) != cudaSuccess)
+                return fail(BG_ENOMEM, "synapse terms by source");
+            int st = refresh_term_src(net, y);
+            if (st) return st;
+        }
+        bg::SynPersistObj &o = a.o[k];
+        o.e = syn_ev_args(net, k);
+        o.term_src = y.dTermSrc;
+        o.var = y.op_var[0]; o.sub = y.op_sub[0];
+        a.pair0[k + 1] = a.pair0[k] + y.dmax;
+    }
+    const int npair = a.pair0[a.nobj];
+    a.nparts = npair ? std::max<int>(1, (int)(blocks / npair)) : 1;
+    a.use_pull = net->dUsePull3;
+    a.spikes = net->dCounters;
+    a.arrived = net->dArrived;
+    a.spin_limit = net->spin_limit;
+    a.nrec = (int)net->stmons.size();
+    for (int k = 0; k < a.nrec; ++k) {
+        HStateMon &m = net->stmons[k];
+        if (!m.dBlkP) {
+            std::vector<int32_t> lo(blocks + 1, 0);
+            const int64_t w = (int64_t)m.sorted.size();
+            for (int64_t b = 0, e = 0; b <= blocks; ++b) {
+                while (e < w && m.sorted[e] < b * bg::kSPBn) ++e;
+                lo[b] = (int32_t)e;
+            }
+            if (net->alloc(&m.dBlkP, (blocks + 1) * 4) != cudaSuccess) return fail(BG_ENOMEM, "state monitor");
+            BG_CUDA(cudaMemcpy(m.dBlkP, lo.data(), (blocks + 1) * 4, cudaMemcpyHostToDevice));
+        }
+        bg::RecDev &r = a.rec[k];
+        r.var = m.var; r.nidx = (int)m.idx.size(); r.idx = m.dIdx; r.pos = m.dPos; r.blk_lo = m.dBlkP;
+        r.buf = m.dBuf; r.row_base = m.dRowBase; r.timestep = m.timestep; r.start = m.start;
+    }
+    if (!net->smons.empty()) {
+        a.mon_stride = g.npad / 32;
+        if (!net->dMonWords &&
+            (net->alloc(&net->dMonWords, (size_t)kPersistMonSteps * a.mon_stride * 4) != cudaSuccess ||
+             net->alloc(&net->dMonOff, (size_t)kPersistMonSteps * 8) != cudaSuccess))
+            return fail(BG_ENOMEM, "spike words");
+        a.mon_words = net->dMonWords;
+    }
+    bool diag = (a.cnz & ~1u) == 0;
+    for (int j = 0; j < g.nvar; ++j)
+        for (int k = 0; k < g.nvar; ++k)
+            if ((((a.anz >> (j * g.nvar + k)) & 1ull) != 0) != (j == 0 || j == k)) diag = false;
+    const void *k = kern[g.nvar - 1][diag ? 1 : 0];
+    unsigned int *arr = net->dArrived;
+    int *flags = net->dUsePull3;
+    net->persist_used = bg::kSPTh;
+    net->persist = [a, blocks, k, smem, arr, flags](cudaStream_t s, int nsteps) {
+        cudaError_t e = cudaMemsetAsync(arr, 0, 64, s);
+        if (e != cudaSuccess) return e;
+        e = cudaMemsetAsync(flags, 0, 16, s);
+        if (e != cudaSuccess) return e;
+        bg::SynPersistArgs b = a; b.nsteps = nsteps;
+        void *args[] = {(void *)&b};
+        return cudaLaunchCooperativeKernel(k, dim3((unsigned)blocks), dim3(bg::kSPTh), args, smem, s);
+    };
+    return BG_OK;
+}
+
 // Runs nsteps with the persistent kernel (one launch) and advances the step
 // counter on the host and device.
 int run_persist(bg_net *n, int64_t nsteps) {
@@ -1724,7 +1881,7 @@ static int bg_synapses_set_terms_impl(bg_net *n, int yi, const double *terms) {
         for (int64_t p = 0; p < y.nsyn; ++p) col[(size_t)k * y.nsyn + p] = y.terms[(size_t)k * y.nsyn + y.perm[p]];
     BG_CUDA(cudaStreamSynchronize(n->stream));
     BG_CUDA(cudaMemcpy(y.dTerm, col.data(), col.size() * 8, cudaMemcpyHostToDevice));
-    return BG_OK;
+    return refresh_term_src(n, y);
 }
 
 int bg_synapses_set_terms(bg_net *n, int32_t sid, const double *terms) {
@@ -2194,6 +2351,7 @@ static int prepare_impl(bg_net *n) {
         n->side1 = nhead + mon_launch.size();
     }
     if (n->allow_persist) st = n->precision == 64 ? build_persist<double>(n) : build_persist<float>(n);
+    if (!st && n->allow_persist && !n->persist) st = build_syn_persist(n);
     if (st) return st;
     BG_CUDA(cudaStreamSynchronize(n->stream));
     n->prepared = true;
@@ -2289,6 +2447,8 @@ static int net_run_steps(bg_net *n, int64_t nsteps, int64_t cs0) {
     if (n->nstep + nsteps >= (1ll << 31) - 1) return fail(BG_EINVAL, "a network runs at most 2^31-1 steps");
     BG_CUDA(cudaSetDevice(n->device));
     if (n->persist) {
+        int st0 = refresh_syn_lists(n);
+        if (st0) return st0;
         long long off0 = cs0 - n->nstep;
         BG_CUDA(cudaMemcpyAsync(&n->dCtl->clock_off, &off0, 8, cudaMemcpyHostToDevice, n->stream));
         BG_CUDA(cudaEventRecord(n->ev0, n->stream));
@@ -2704,6 +2864,8 @@ int bg_net_profile(bg_net *n, int64_t nsteps, int64_t cs0, double *ms, int64_t c
         return fail(BG_ENOSYS, "profiling runs networks without monitors");
     BG_CUDA(cudaSetDevice(n->device));
     if (n->persist) {
+        int st0 = refresh_syn_lists(n);
+        if (st0) return st0;
         *nitems = 1;
         cudaEvent_t e0, e1;
         BG_CUDA(cudaEventCreate(&e0)); BG_CUDA(cudaEventCreate(&e1));

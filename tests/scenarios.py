@@ -355,10 +355,13 @@ def stdp_delay(Nin=400, Nout=40, steps=3000, seed=9, p=0.5, wdtype=np.float64, i
     return res
 
 
-def synapses_cuba(N=2000, steps=2000, seed=11, p=0.02, runs=1, two_statements=True, multi=True):
+def synapses_cuba(N=2000, steps=2000, seed=11, p=0.02, runs=1, two_statements=True, multi=True,
+                  report_persistent=False):
     """CUBA through Synapses: excitatory and inhibitory subgroups onto the
     whole group with per-synapse weights and float delays (0-4 ms); the
-    excitatory code has two statements; some pairs get two synapses."""
+    excitatory code has two statements; some pairs get two synapses.
+    `report_persistent` adds the threads per block of the engine's
+    persistent kernel (0: the stepped path ran)."""
     taum, taue, taui = 20 * ms, 5 * ms, 10 * ms
     Vt, Vr, El = -50 * mV, -60 * mV, -49 * mV
     eqs = b.Equations("""
@@ -387,7 +390,10 @@ def synapses_cuba(N=2000, steps=2000, seed=11, p=0.02, runs=1, two_statements=Tr
     net = b.Network(P, Se, Si, M, S)
     for _ in range(runs):
         net.run(steps * 0.1 * ms / runs)
-    return _result(net, groups=[P], spikemons=[M], statemons=[S])
+    out = _result(net, groups=[P], spikemons=[M], statemons=[S])
+    if report_persistent:
+        out["persistent_threads"] = net.stats().get("persistent_threads", 0)
+    return out
 
 
 def kitchen_sink(steps=400, seed=7):

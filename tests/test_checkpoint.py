@@ -174,3 +174,39 @@ def test_checkpoint_synapses_gpu(gpu_table, events):
         b.set_global_preferences(synapse_events=None)
     assert len(whole["spk3"][1]) > 100
     _equal(whole, resumed)
+
+
+def _synapses_self():
+    """CUBA through Synapses onto its own group (the engine's persistent
+    kernel for Synapses when the event path is forced)."""
+    np.random.seed(5)
+    eqs = b.Equations("dv/dt=(ge+gi-(v-El))/taum : volt\ndge/dt=-ge/taue : volt\ndgi/dt=-gi/taui : volt",
+                      taum=20 * ms, taue=5 * ms, taui=10 * ms, El=-49 * mV)
+    N = 2500
+    P = b.NeuronGroup(N, model=eqs, threshold=-50 * mV, reset=-60 * mV)
+    Pe, Pi = P.subgroup(2000), P.subgroup(500)
+    rng = np.random.Generator(np.random.PCG64(6))
+    Se = b.Synapses(Pe, P, model="w : volt", pre="ge += w", max_delay=5 * ms)
+    Si = b.Synapses(Pi, P, model="w : volt", pre="gi -= w")
+    Se.connect_random(sparseness=0.02)
+    Si.connect_random(sparseness=0.02)
+    Se.w = 1.62 * mV * (0.5 + rng.random(len(Se)))
+    Si.w = 9 * mV * (0.5 + rng.random(len(Si)))
+    Se.delay = rng.random(len(Se)) * 4 * ms
+    Si.delay = rng.random(len(Si)) * 4 * ms
+    P.v = -60 * mV + rng.random(N) * 10 * mV
+    return b.Network(P, Se, Si, b.SpikeMonitor(P), b.StateMonitor(P, "v", record=[0, 1, N - 1]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("events", [None, True], ids=["by-size", "events"])
+def test_checkpoint_synapses_self_gpu(gpu_table, events):
+    """One group with Synapses onto itself (with the event path forced: the
+    persistent kernel for Synapses), resumed mid-run from a saved state."""
+    b.set_global_preferences(synapse_events=events)
+    try:
+        whole, resumed = checkpoint_roundtrip(_synapses_self, 237, 180)
+    finally:
+        b.set_global_preferences(synapse_events=None)
+    assert len(whole["spk3"][1]) > 100
+    _equal(whole, resumed)

@@ -99,3 +99,21 @@ def test_synapses_event_bins_and_pull_fallback(oracle_table, gpu_table, rate, sp
     ref, gpu = _both(fn, oracle_table)
     assert len(ref["spk0.idx"]) > 100
     scenarios.compare(ref, gpu)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kw", [dict(), dict(runs=3, steps=2400), dict(multi=False, N=5000, p=0.01, steps=1200),
+                                dict(multi=False, N=40000, p=0.001, steps=600)])
+def test_synapses_persistent_kernel(oracle_table, gpu_table, kw):
+    """One group with Synapses onto itself (one statement each) on the event
+    path runs in the persistent kernel for Synapses (one launch per run, one
+    grid-wide wait per step): spikes, states and the StateMonitor equal the
+    oracle's."""
+    b.set_global_preferences(synapse_events=True)
+    try:
+        ref, gpu = _both(scenarios.synapses_cuba, oracle_table, report_persistent=True, two_statements=False, **kw)
+    finally:
+        b.set_global_preferences(synapse_events=None)
+    assert ref.pop("persistent_threads") == 0 and gpu.pop("persistent_threads") > 0
+    assert len(ref["spk0.idx"]) > 100
+    scenarios.compare(ref, gpu)
