@@ -36,6 +36,7 @@ constexpr int kSPTh = kSynBinThreads;            // threads per block
 constexpr int kSPNpt = kSynTPT;                  // neurons per thread
 constexpr int kSPBn = kSPTh * kSPNpt;            // neurons per block
 static_assert(kSPBn == kSynBin, "a block's neurons are one bin of targets");
+constexpr int kSynSub = 4;                       // threads per listed source on the spike lists
 
 struct SynPersistObj {
     SynEvArgs e;                                 // lists, rows by source, pull columns, terms
@@ -66,31 +67,33 @@ struct SynPersistArgs {
 };
 
 // the events of source i's synapses of delay d of object k into the bins of
-// one parity: key and term
-__device__ __forceinline__ void synp_push(const SynPersistObj &ob, int k, int64_t i, int d, int *flag, int *cnt,
-                                          unsigned long long *key, double *tv) {
+// one parity (key and term): this thread's share, synapses sub, sub + nsub,
+// ... of the source's row of that delay, four at a time (loads, then slots,
+// then stores)
+__device__ __forceinline__ void synp_push(const SynPersistObj &ob, int k, int64_t i, int d, int sub, int nsub,
+                                          int *flag, int *cnt, unsigned long long *key, double *tv) {
     const SynEvArgs &a = ob.e;
     int64_t r0, r1;
     syn_src_range(a, i, d, r0, r1);
-    if (r1 - r0 > 256) { atomicExch(flag, 1); return; }
-    for (int64_t p0 = r0; p0 < r1; p0 += 4) {
-        const int m = r1 - p0 < 4 ? (int)(r1 - p0) : 4;
+    if (r1 - r0 > 256) { if (sub == 0) atomicExch(flag, 1); return; }
+    for (int64_t p0 = r0 + sub; p0 < r1; p0 += 4 * nsub) {
         int32_t tg[4], slot[4];
         double tt[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u)
-            if (u < m) { tg[u] = __ldg(a.stgt + p0 + u); tt[u] = __ldg(ob.term_src + p0 + u); }
+            if (p0 + u * nsub < r1) { tg[u] = __ldg(a.stgt + p0 + u * nsub); tt[u] = __ldg(ob.term_src + p0 + u * nsub); }
 #pragma unroll
         for (int u = 0; u < 4; ++u)
-            if (u < m) slot[u] = atomicAdd(cnt + tg[u] / kSynBin, 1);
+            if (p0 + u * nsub < r1) slot[u] = atomicAdd(cnt + tg[u] / kSynBin, 1);
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            if (u >= m) break;
+            const int64_t p = p0 + u * nsub;
+            if (p >= r1) break;
             if (slot[u] >= kSynBinCap) { atomicExch(flag, 1); continue; }
             const int64_t j = tg[u];
             const int64_t e = (j / kSynBin) * kSynBinCap + slot[u];
             key[e] = ((unsigned long long)(j * 4 + k) << 40) | ((unsigned long long)(255 - d) << 32) |
-                     ((unsigned long long)i << 8) | (unsigned long long)(p0 + u - r0);
+                     ((unsigned long long)i << 8) | (unsigned long long)(p - r0);
             tv[e] = tt[u];
         }
     }
@@ -356,7 +359,7 @@ __global__ void __launch_bounds__(kSPTh, 2) k_syn_persist(const __grid_constant_
                 const int row = (int)(t % e.sdepth);
                 const int pos = atomicAdd(e.scnt + row, __popc(word));   // used after the pushes
                 for (uint32_t wv = word; wv; wv &= wv - 1)
-                    synp_push(ob, k, wb + (__ffs(wv) - 1) - e.so, 0, flag, bcnt, bkey, bt);
+                    synp_push(ob, k, wb + (__ffs(wv) - 1) - e.so, 0, 0, 1, flag, bcnt, bkey, bt);
                 int32_t *L = e.slist + (int64_t)row * e.sn + pos;
                 for (uint32_t wv = word; wv; wv &= wv - 1) *L++ = (int32_t)(wb + (__ffs(wv) - 1) - e.so);
             }
@@ -372,11 +375,12 @@ __global__ void __launch_bounds__(kSPTh, 2) k_syn_persist(const __grid_constant_
                 if (t < d) continue;
                 const int row = (int)((t - d) % e.sdepth);
                 const int32_t *L = e.slist + (int64_t)row * e.sn;
-                const int q0 = part * nl + tid;
+                // kSynSub threads per listed source, each with a share of its synapses
+                const int q0 = (part * nl + tid) / kSynSub, sub = tid % kSynSub;
                 const int32_t first = q0 < e.sn ? __ldcg(L + q0) : 0;   // loaded beside the count
                 const int cnt = __ldcg(e.scnt + row);
-                for (int q = q0; q < cnt; q += a.nparts * nl)
-                    synp_push(ob, k, q == q0 ? first : __ldcg(L + q), d, flag, bcnt, bkey, bt);
+                for (int q = q0; q < cnt; q += a.nparts * nl / kSynSub)
+                    synp_push(ob, k, q == q0 ? first : __ldcg(L + q), d, sub, kSynSub, flag, bcnt, bkey, bt);
             }
         }
         // ---- arrive at step t; wait for every block's arrival
