@@ -455,7 +455,10 @@ def profile_case(case, seed):
           batch 4096 (launch 12 of k_gemm is the 512 x 512 hidden layer of
           the second step).
     synapses: CUBA through Synapses (see synapses_case).
-    synapses_262k: the same at 262 144 neurons (the event path), 300 steps.
+    synapses_262k: the same at 262 144 neurons (the event path: the
+          persistent kernel for Synapses), 300 steps.
+    synapses_262k_stepped: the same on the stepped path (group kernel,
+          k_syn_gather, k_syn_bins per step).
     stdp: the STDP scale-up network, 300 steps.
     batch: 148 CUBA-4000 networks in one NetworkBatch at the default shape
           (1024 x 4, 32 lanes), 2000 steps, no autotuning: the first k_batch
@@ -488,13 +491,20 @@ def profile_case(case, seed):
         print(json.dumps({"case": "gemm", "train_ms": ms, "steps": n // 4096, "loss": float(loss[0])}))
     elif case == "synapses":
         print(json.dumps(synapses_case(seed)))
-    elif case == "synapses_262k":
-        # the event path at 262 144 neurons without a monitor, 300 steps:
-        # each step launches the group kernel, k_syn_gather and k_syn_bins
-        net, _, _, _ = synapses_network(seed, 262144, 160, False)
-        net.run(300 * DT)
+    elif case in ("synapses_262k", "synapses_262k_stepped"):
+        # the event path at 262 144 neurons without a monitor, 300 steps: one
+        # launch of k_syn_persist, or (stepped) per step the group kernel,
+        # k_syn_gather and k_syn_bins
+        import brian_b200 as b
+        prev = b.get_global_preference("persistent")
+        b.set_global_preferences(persistent=case == "synapses_262k")
+        try:
+            net, _, _, _ = synapses_network(seed, 262144, 160, False)
+            net.run(300 * DT)
+        finally:
+            b.set_global_preferences(persistent=prev)
         st = net._binding.rt.stats()
-        print(json.dumps({"case": "synapses_262k", "steps": 300, "us_per_step": st["last_run_ms"] * 1e3 / 300}))
+        print(json.dumps({"case": case, "steps": 300, "us_per_step": st["last_run_ms"] * 1e3 / 300}))
     elif case == "stdp":
         # the STDP scale-up network (164 MB of weights) for 300 steps: the
         # outputs fire on about half the steps from step ~100 on, so launches
@@ -963,7 +973,7 @@ def main():
     ap.add_argument("--fit-batch", type=int, default=16384, help="rows per training step of the proposal network")
     ap.add_argument("--fit-lr", type=float, default=2e-3)
     ap.add_argument("--fit-iters", type=int, default=40)
-    ap.add_argument("--profile-case", choices=["fit", "gemm", "synapses", "synapses_262k", "stdp", "batch"], default=None,
+    ap.add_argument("--profile-case", choices=["fit", "gemm", "synapses", "synapses_262k", "synapses_262k_stepped", "stdp", "batch"], default=None,
                     help="run one small case for a single-kernel ncu capture and exit")
     args = ap.parse_args()
     if args.profile_case:

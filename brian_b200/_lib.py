@@ -219,8 +219,8 @@ class Runtime(object):
             self.t.check(self.t.net_set_spin_limit(self.h, int(spin_limit)), "net_set_spin_limit")
         if check_finite and hasattr(self.t, "net_set_check_finite"):
             self.t.check(self.t.net_set_check_finite(self.h, 1), "net_set_check_finite")
-        if synapse_events and hasattr(self.t, "net_set_synapse_events"):
-            self.t.check(self.t.net_set_synapse_events(self.h, 1), "net_set_synapse_events")
+        if synapse_events is not None and hasattr(self.t, "net_set_synapse_events"):
+            self.t.check(self.t.net_set_synapse_events(self.h, 1 if synapse_events else 2), "net_set_synapse_events")
 
     def import_device_ptr(self, ptr, nbytes, precision):
         bid = _i32()

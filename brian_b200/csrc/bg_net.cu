@@ -1210,24 +1210,36 @@ int refresh_term_src(bg_net *net, const HSyn &y) {
 // linear FP64 group whose event-path Synapses (static variables, additive
 // statements) all connect it to itself, bins aligned with the kernel's
 // 1024-neuron blocks, every block co-resident.  Otherwise the stepped path.
-int build_syn_persist(bg_net *net) {
-    net->persist = nullptr;
-    if (net->groups.size() != 1 || !net->conns.empty() || !net->stdps.empty() || net->syns.empty()) return BG_OK;
-    if (net->precision != 64 || (int)net->syns.size() > bg::kSynEvMerge) return BG_OK;
+// Whether the network has the shape of the persistent kernel for Synapses
+// (device limits aside): one linear FP64 group, Synapses only, each with one
+// statement, onto the group itself, one target range starting at a bin
+// boundary; monitors of that group.
+bool syn_persist_shape(const bg_net *net) {
+    if (!net->allow_persist) return false;
+    if (net->groups.size() != 1 || !net->conns.empty() || !net->stdps.empty() || net->syns.empty()) return false;
+    if (net->precision != 64 || (int)net->syns.size() > bg::kSynEvMerge) return false;
     for (const HSyn &y : net->syns) {
-        if (!y.events || y.coded || y.src != 0 || y.tgt != 0 || y.to % bg::kSynBin != 0 || !y.dScnt) return BG_OK;
+        if (y.coded || y.src != 0 || y.tgt != 0 || y.to % bg::kSynBin != 0) return false;
         // one statement; one target range for all (the bins are shared, the
         // key holds target * 4 + object below 2^24); sources below 2^24
-        if (y.nops != 1 || y.to != net->syns[0].to || y.tn != net->syns[0].tn) return BG_OK;
-        if (y.tn > ((int64_t)1 << 22) || y.sn >= ((int64_t)1 << 24)) return BG_OK;
+        if (y.nops != 1 || y.to != net->syns[0].to || y.tn != net->syns[0].tn) return false;
+        if (y.tn > ((int64_t)1 << 22) || y.sn >= ((int64_t)1 << 24)) return false;
     }
     for (const HSpikeMon &m : net->smons)
-        if (m.gid != 0 || m.delay != 0) return BG_OK;
-    if ((int)net->stmons.size() > bg::kMaxRec) return BG_OK;
+        if (m.gid != 0 || m.delay != 0) return false;
+    if ((int)net->stmons.size() > bg::kMaxRec) return false;
     const HGroup &g = net->groups[0];
-    if (!g.linear || g.nvar < 1 || g.nvar > 4 || g.refr || g.period > 0) return BG_OK;
-    if (g.generated() || g.emp_steps > 0 || !g.setters.empty()) return BG_OK;
-    if (g.thr_kind != BG_THR_CONST && g.thr_kind != BG_THR_VAR && g.thr_kind != BG_THR_NONE) return BG_OK;
+    if (!g.linear || g.nvar < 1 || g.nvar > 4 || g.refr || g.period > 0) return false;
+    if (g.generated() || g.emp_steps > 0 || !g.setters.empty()) return false;
+    return g.thr_kind == BG_THR_CONST || g.thr_kind == BG_THR_VAR || g.thr_kind == BG_THR_NONE;
+}
+
+int build_syn_persist(bg_net *net) {
+    net->persist = nullptr;
+    if (!syn_persist_shape(net)) return BG_OK;
+    for (const HSyn &y : net->syns)
+        if (!y.events || !y.dScnt) return BG_OK;
+    const HGroup &g = net->groups[0];
     {
         int dev = 0, coop = 0;
         if (cudaGetDevice(&dev) != cudaSuccess) return BG_OK;
@@ -2242,17 +2254,19 @@ static int prepare_impl(bg_net *n) {
         }
         // the event path pays off once the pull's synapse words no longer
         // stay in L2 (it reads every word every step); below that the pull
-        // is cheaper than the event path's extra launches
-        if (y.events) {
+        // is cheaper than the event path's extra launches -- unless the
+        // network runs in the persistent kernel for Synapses (no launches)
+        if (n->syn_events_forced == 2) y.events = false;
+        if (y.events && !syn_persist_shape(n)) {
             int dev = 0, l2 = 0;
             cudaGetDevice(&dev);
             if (cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev) != cudaSuccess) l2 = 0;
             int64_t words = 0;
             for (const auto &o : n->syns) words += o.nsyn;
             if (!n->syn_events_forced && words * 4 <= (int64_t)l2 / 2) y.events = false;
-            // the spike lists hold every source for dmax + 2 steps
-            if ((int64_t)(y.dmax + 2) * y.sn * 4 > ((int64_t)1 << 30)) y.events = false;
         }
+        // the spike lists hold every source for dmax + 2 steps
+        if (y.events && (int64_t)(y.dmax + 2) * y.sn * 4 > ((int64_t)1 << 30)) y.events = false;
         if (y.events) {
             y.nbins = (int)((y.tn + bg::kSynBin - 1) / bg::kSynBin);
             if (n->alloc(&y.dSrcPtr, (y.sn + 1) * 8) != cudaSuccess || n->alloc(&y.dSd, y.nsyn) != cudaSuccess ||
@@ -2803,7 +2817,7 @@ int bg_group_padded_size(bg_net *n, int32_t gid, int64_t *npad) {
 }
 
 int bg_net_set_synapse_events(bg_net *n, int mode) {
-    if (!n || mode < 0 || mode > 1) return fail(BG_EINVAL, "synapse events: 0 (by size) or 1 (always)");
+    if (!n || mode < 0 || mode > 2) return fail(BG_EINVAL, "synapse events: 0 (by size), 1 (always) or 2 (never)");
     if (n->prepared) return fail(BG_ESTATE, "set before prepare");
     n->syn_events_forced = mode;
     return BG_OK;

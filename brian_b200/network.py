@@ -48,8 +48,9 @@ def set_global_preferences(**kw):
     bounded inter-block wait before the run fails with BG_ETIMEOUT; None:
     the engine's default), check_finite (bool: every run ends with a scan of
     the state variables and a NaN or infinity fails it with BG_ENUMERIC),
-    synapse_events (True: Synapses always take the event path; None: the
-    engine picks it when the synapses exceed half of L2)."""
+    synapse_events (True: Synapses always take the event path; False:
+    never; None: the engine picks it when the synapses exceed half of L2
+    or the network has the shape of its persistent kernel for Synapses)."""
     _PREFS.update(kw)
 
 

@@ -327,11 +327,13 @@ BG_API int bg_import_device_ptr(bg_net *net, void *ptr, int64_t bytes,
  * before bg_net_prepare. */
 BG_API int bg_group_use_buffer(bg_net *net, int32_t gid, int32_t buf_id);
 BG_API int bg_group_padded_size(bg_net *net, int32_t gid, int64_t *npad);
-/* Synapses delivery: the event path (the events of the spiking sources,
- * binned by target block and applied in queue order) is taken when the
- * synapse words exceed half of L2, the pull over every synapse otherwise;
- * mode 1 takes the event path whatever the size.  Both give identical
- * results.  Set before bg_net_prepare. */
+/* Synapses delivery: mode 0 (default) takes the event path (the events of
+ * the spiking sources, binned by target block and applied in queue order)
+ * when the synapse words exceed half of L2 or the network has the shape of
+ * the persistent kernel for Synapses (one linear group, its Synapses onto
+ * itself with one statement each), the pull over every synapse otherwise;
+ * mode 1 takes the event path whatever the size, mode 2 the pull.  All give
+ * identical results.  Set before bg_net_prepare. */
 BG_API int bg_net_set_synapse_events(bg_net *net, int mode);
 /* ---- checkpoint / resume (Network.__reduce__, network.py:652;
  * SpikeContainer.__reduce__, utils/circular.py:249-269;

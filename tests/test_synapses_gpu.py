@@ -35,10 +35,11 @@ def test_known_answers_gpu(gpu_table):
     np.testing.assert_array_equal(kat.kat_insertion_order(gpu_table), kat.expected_insertion_order())
 
 
-@pytest.fixture(params=[None, True], ids=["by-size", "events"])
+@pytest.fixture(params=[None, True, False], ids=["by-size", "events", "pull"])
 def delivery(request):
-    """The Synapses delivery the engine picks by size (the pull for these
-    networks), and the event path forced."""
+    """The Synapses delivery the engine picks by size (the pull for most of
+    these networks, the persistent kernel for Synapses for those of its
+    shape), the event path forced, and the pull forced."""
     b.set_global_preferences(synapse_events=request.param)
     yield request.param
     b.set_global_preferences(synapse_events=None)
