@@ -162,7 +162,7 @@ __global__ void k_adam_all(const __grid_constant__ AdamAll a) {
     for (int q = 1; q < 2 * kNLayer; ++q) k += i0 >= a.off[q] ? 1 : 0;
     const AdamSeg &sg = a.seg[k];
     const int64_t i = i0 - a.off[k];
-    const int r = (int)(i / sg.cols), c = (int)(i % sg.cols);
+    const int r = (int)(i / sg.cols);
     if (r < sg.rows_train) {
         const float t = (float)*a.step;
         const float c1 = 1.f - powf(a.b1, t), c2 = 1.f - powf(a.b2, t);
@@ -175,10 +175,71 @@ __global__ void k_adam_all(const __grid_constant__ AdamAll a) {
         sg.v[i] = vi;
         sg.P[i] -= a.lr * (mi / c1) / (sqrtf(vi / c2) + a.eps);
     }
-    if (sg.Pb) {
-        const bf16 h = __float2bfloat16_rn(sg.P[i]);
-        sg.Pb[i] = h;
-        if (sg.PbT) sg.PbT[(int64_t)c * sg.rows + r] = h;
+    if (sg.Pb) sg.Pb[i] = __float2bfloat16_rn(sg.P[i]);   // the transposed copy: k_transpose_all
+}
+
+// The transposed bf16 copies of the updated weights (PbT[c][r] = Pb[r][c]),
+// 32 x 32 tiles through shared memory so that both the reads and the writes
+// are coalesced; block b is a tile of the first segments with a PbT.
+__global__ void __launch_bounds__(256) k_transpose_all(const __grid_constant__ AdamAll a) {
+    umma::pdl_launch_dependents();
+    umma::pdl_wait();
+    __shared__ bf16 tile[32][33];
+    int b = blockIdx.x, k = 0;
+    for (; k < 2 * kNLayer; ++k) {
+        const AdamSeg &sg = a.seg[k];
+        if (!sg.PbT) continue;
+        const int nt = ((sg.rows + 31) / 32) * ((sg.cols + 31) / 32);
+        if (b < nt) break;
+        b -= nt;
+    }
+    if (k == 2 * kNLayer) return;
+    const AdamSeg &sg = a.seg[k];
+    const int tcols = (sg.cols + 31) / 32;
+    const int r0 = (b / tcols) * 32, c0 = (b % tcols) * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+#pragma unroll
+    for (int j = 0; j < 32; j += 8) {
+        const int r = r0 + ty + j, c = c0 + tx;
+        if (r < sg.rows && c < sg.cols) tile[ty + j][tx] = sg.Pb[(int64_t)r * sg.cols + c];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 32; j += 8) {
+        const int c = c0 + ty + j, r = r0 + tx;
+        if (r < sg.rows && c < sg.cols) sg.PbT[(int64_t)c * sg.rows + r] = tile[tx][ty + j];
+    }
+}
+
+// The bias gradients, each the sum of its layer's column-sum partials (one
+// per 32 or 256 batch rows), in one fixed order: block b sums 32 columns of
+// one layer, warp w the partials w, w + 8, ... of them (coalesced rows), and
+// warp 0 adds the eight warp sums in warp order.
+struct BiasRed {
+    const float *p[kNLayer]; int nblk[kNLayer], ld[kNLayer], rows[kNLayer];
+    int blk0[kNLayer + 1];          // first block of each layer
+    float *out;                     // [kNLayer][kHid]
+};
+__global__ void __launch_bounds__(256) k_bias_reduce(const __grid_constant__ BiasRed r) {
+    umma::pdl_launch_dependents();
+    umma::pdl_wait();
+    __shared__ float red[8][32];
+    int l = 0;
+    while (l + 1 < kNLayer && (int)blockIdx.x >= r.blk0[l + 1]) ++l;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int i = ((int)blockIdx.x - r.blk0[l]) * 32 + lane;
+    float g = 0.f;
+    if (i < r.rows[l]) {
+#pragma unroll 8
+        for (int s = warp; s < r.nblk[l]; s += 8) g += r.p[l][(int64_t)s * r.ld[l] + i];
+    }
+    red[warp][lane] = g;
+    __syncthreads();
+    if (warp == 0 && i < r.rows[l]) {
+        float t = red[0][lane];
+#pragma unroll
+        for (int w = 1; w < 8; ++w) t += red[w][lane];
+        r.out[l * kHid + i] = t;
     }
 }
 
@@ -396,6 +457,7 @@ struct bg_mlp {
     // one training step captured as a graph (rebuilt when the batch size changes)
     cudaGraphExec_t step_graph = nullptr; int graph_batch = 0; float graph_lr = 0.f;
     float *cs[kNLayer] = {};              // bias-gradient partials per layer [row blocks][512]
+    float *gbias = nullptr;               // their sums, [kNLayer][512]
     int64_t step = 0;
     // batch buffers
     int B = 0;
@@ -436,6 +498,7 @@ int ensure_batch(bg_mlp *h, int B) {
     if ((rc = dalloc(&h->idx, (size_t)B))) return rc;
     for (int l = 0; l < kNLayer; ++l)
         if ((rc = dalloc(&h->cs[l], (size_t)((B + 31) / 32) * kHid))) return rc;
+    if (!h->gbias && (rc = dalloc(&h->gbias, (size_t)kNLayer * kHid))) return rc;
     h->B = B;
     return BG_OK;
 }
@@ -475,6 +538,23 @@ void bias_partials(const bg_mlp *h, int l, int B, const float **p, int *nblk, in
         *nblk = 4 * ((B + umma::kM - 1) / umma::kM);
         *ld = kHid;
     }
+}
+
+// the bias gradients' sums (k_bias_reduce) for Adam and the flat gradient
+int reduce_bias(bg_mlp *h, int B, bool pdl) {
+    BiasRed r;
+    memset(&r, 0, sizeof r);
+    for (int l = 0; l < kNLayer; ++l) {
+        bias_partials(h, l, B, &r.p[l], &r.nblk[l], &r.ld[l]);
+        r.rows[l] = h->rows[l];
+        r.blk0[l + 1] = r.blk0[l] + (r.rows[l] + 31) / 32;
+    }
+    r.out = h->gbias;
+    const dim3 grid((unsigned)r.blk0[kNLayer]), block(256);
+    if (pdl) MCK(launch_pdl(k_bias_reduce, grid, block, 0, h->stream, r));
+    else k_bias_reduce<<<grid, block, 0, h->stream>>>(r);
+    MCK(cudaGetLastError());
+    return BG_OK;
 }
 
 // backward from the loss gradient in h->dO / h->dOT: weight gradients of
@@ -537,11 +617,9 @@ AdamAll adam_desc(bg_mlp *h, int B, float lr, const float *flat, float scale) {
         w.rows_train = rows_train; w.Pb = h->Wb[l]; w.PbT = h->WbT[l];
         a.off[2 * l] = off;
         off += (int64_t)h->rows[l] * h->cols[l];
-        const float *bp;
-        int nblk, ld;
-        bias_partials(h, l, B, &bp, &nblk, &ld);
         AdamSeg &bb = a.seg[2 * l + 1];
-        bb.P = h->b[l]; bb.m = h->mb[l]; bb.v = h->vb[l]; bb.grad = bp; bb.splits = nblk; bb.split_stride = ld;
+        bb.P = h->b[l]; bb.m = h->mb[l]; bb.v = h->vb[l];
+        bb.grad = h->gbias + (int64_t)l * kHid; bb.splits = 1; bb.split_stride = 0;   // k_bias_reduce's sums
         bb.rows = h->rows[l]; bb.cols = 1; bb.rows_train = rows_train;
         a.off[2 * l + 1] = off;
         off += h->rows[l];
@@ -559,6 +637,10 @@ int adam_all(bg_mlp *h, int B, float lr, const float *flat = nullptr, float scal
     const AdamAll a = adam_desc(h, B, lr, flat, scale);
     const int64_t off = a.off[2 * kNLayer];
     MCK(launch_pdl(k_adam_all, dim3((unsigned)((off + 255) / 256)), dim3(256), 0, h->stream, a));
+    int tiles = 0;
+    for (int k = 0; k < 2 * kNLayer; ++k)
+        if (a.seg[k].PbT) tiles += ((a.seg[k].rows + 31) / 32) * ((a.seg[k].cols + 31) / 32);
+    if (tiles) MCK(launch_pdl(k_transpose_all, dim3((unsigned)tiles), dim3(32, 8), 0, h->stream, a));
     return BG_OK;
 }
 
@@ -571,6 +653,7 @@ int train_step(bg_mlp *h, int B, float lr) {
     MCK(launch_pdl(k_nll, dim3((B + 255) / 256), dim3(256), 0, h->stream, (const float *)h->OUT, (const float *)h->Y, B,
                    h->ydim, h->dO, h->dOT, h->cs[kNLayer - 1], h->loss));
     if ((rc = backward(h, B))) return rc;
+    if ((rc = reduce_bias(h, B, true))) return rc;
     // Adam's step count t is the step being taken (1 for the first)
     MCK(launch_pdl(k_step_advance, dim3(1), dim3(1), 0, h->stream, h->dBatchIdx, h->dOptStep));
     if ((rc = adam_all(h, B, lr))) return rc;
@@ -849,6 +932,7 @@ BG_API int bg_mlp_step_gradients(bg_mlp *h, int batch, int64_t row0, float *loss
     k_nll<<<(batch + 255) / 256, 256, 0, h->stream>>>(h->OUT, h->Y, batch, h->ydim, h->dO, h->dOT,
                                                        h->cs[kNLayer - 1], h->loss);
     if ((rc = backward(h, batch))) return rc;
+    if ((rc = reduce_bias(h, batch, false))) return rc;
     const AdamAll a = adam_desc(h, batch, 0.f, nullptr, 1.f);
     k_grad_flat<<<(unsigned)((nflat + 255) / 256), 256, 0, h->stream>>>(a, h->gflat);
     MCK(cudaGetLastError());

@@ -525,7 +525,7 @@ constexpr size_t smem_bytes() {
 constexpr int kPThreads = 192;
 // operand stages in flight: as many as fit in 100 KB, so that the CTA of the
 // next product (launched early, programmatic dependent launch) fits beside it
-template <int NT> struct PStages { static constexpr int value = (100 * 1024) / ((kM + NT) * kKc * 2); };
+template <int NT> struct PStages { static constexpr int value = (192 * 1024) / ((kM + NT) * kKc * 2); };
 
 // Programmatic dependent launch: the kernel lets the next one in its stream
 // start launching, and waits for the previous one to finish (and its writes

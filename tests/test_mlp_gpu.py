@@ -134,3 +134,30 @@ def test_learned_proposals_beat_plain_swarm():
     assert l["first_evaluation_reached"] > p["first_evaluation_reached"]
     assert l["t50_ms"] < p["t50_ms"]
     assert l["reached"] >= p["reached"]
+
+
+def test_step_gradients_match_gradients():
+    """The flat gradient of one training step (the data-parallel path: the
+    weight partials and the bias gradients summed on the device) over a set
+    that is exactly one batch equals the gradients of the same rows taken in
+    another order, segment by segment (W0, b0, W1, b1, ...)."""
+    import torch
+    h, P, rng = _net(3)
+    n = 4096
+    X = rng.standard_normal((n, 64)).astype(np.float32)
+    Y = rng.uniform(-1, 1, (n, 5)).astype(np.float32)
+    h.set_data(X, Y)
+    loss, dW, db = h.gradients(n)
+    h.epoch_order(5, 0)
+    loss2, g = h.step_gradients(n, 0)
+    flat = g.torch().cpu().numpy()
+    assert abs(loss - loss2) <= 1e-4 * abs(loss)
+    o = 0
+    for l in range(4):
+        for want in (dW[l].ravel(), db[l]):
+            got = flat[o:o + want.size]
+            o += want.size
+            err = np.linalg.norm(got - want) / max(np.linalg.norm(want), 1e-30)
+            assert err < 1e-3, (l, want.size, err)
+    assert o == flat.size
+    h.close()
