@@ -1145,7 +1145,7 @@ static __global__ void __launch_bounds__(kSynThreads) k_syn_deliver(const SynArg
     const int64_t ntiles = (a.tn + kSynTile - 1) / kSynTile;
     // history row of step nstep - lag: (nstep mod depth) - lag, wrapped once
     // (lag <= depth - 1); no 64-bit modulo per synapse
-    const int row0 = (int)(nstep % a.depth);
+    const int row0 = (int)nstep % a.depth;
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int64_t j0 = tile * kSynTile, j1 = min(a.tn, j0 + kSynTile);
         const int64_t P0 = a.colptr[j0], P1 = a.colptr[j1];
@@ -1256,7 +1256,7 @@ __device__ __forceinline__ void syn_code_body(const SynCodeArgs &a) {
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     constexpr int kWarps = kSynThreads / 32;
     const int64_t ntiles = (a.tn + kSynTile - 1) / kSynTile;
-    const int row0 = (int)(nstep % a.depth);
+    const int row0 = (int)nstep % a.depth;
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int64_t j0 = tile * kSynTile, j1 = min(a.tn, j0 + kSynTile);
         const int64_t P0 = a.colptr[j0], P1 = a.colptr[j1];
@@ -1322,7 +1322,7 @@ __device__ __forceinline__ void syn_code_body(const SynCodeArgs &a) {
         }
         if (own && a.has_post && q0 < q1) {
             const int64_t tj = a.to + j;
-            const int trow = (int)(nstep % a.tdepth);
+            const int trow = (int)nstep % a.tdepth;
             if ((a.thist[(int64_t)trow * a.tnwords + (tj >> 5)] >> (tj & 31)) & 1u)
                 for (int64_t q = q0; q < q1; ++q) C::post(x, a.sv, q, t);
         }
@@ -1448,9 +1448,9 @@ __device__ __forceinline__ void syn_push_events(const SynEvArgs &a, int64_t i, i
 // appended to the step's list, and their delay-0 events
 __device__ __forceinline__ void syn_gather_word(const SynEvArgs &a, long long nstep, int64_t x) {
     const int64_t wi = (a.so >> 5) + x;
-    uint32_t word = masked_word(a.hist + (int64_t)(nstep % a.depth) * a.nwords, wi, a.so, a.so + a.sn);
+    uint32_t word = masked_word(a.hist + (int64_t)((int)nstep % a.depth) * a.nwords, wi, a.so, a.so + a.sn);
     if (!word) return;
-    const int row = (int)(nstep % a.sdepth);
+    const int row = (int)nstep % a.sdepth;
     int pos = atomicAdd(a.scnt + row, __popc(word));
     int32_t *L = a.slist + (int64_t)row * a.sn;
     int *flag = a.use_pull + (nstep & 1);
@@ -1468,7 +1468,7 @@ static __global__ void __launch_bounds__(256) k_syn_gather(const __grid_constant
     if (blockIdx.x == 0 && threadIdx.x < g.nobj) {
         // the next step's list row starts empty (no one reads it this step)
         const SynEvArgs &a = g.o[threadIdx.x];
-        a.scnt[(nstep + 1) % a.sdepth] = 0;
+        a.scnt[((int)nstep + 1) % a.sdepth] = 0;
     }
     if ((int)blockIdx.x < nlist) {
         const int pair = (int)blockIdx.x / g.nparts, part = (int)blockIdx.x % g.nparts;
@@ -1476,7 +1476,7 @@ static __global__ void __launch_bounds__(256) k_syn_gather(const __grid_constant
         while (k + 1 < g.nobj && pair >= g.pair0[k + 1]) ++k;
         const SynEvArgs &a = g.o[k];
         const int d = 1 + pair - g.pair0[k];
-        const int row = (int)((nstep - d + a.sdepth) % a.sdepth);
+        const int row = ((int)nstep - d + a.sdepth) % a.sdepth;
         const int cnt = nstep < d ? 0 : a.scnt[row];
         const int32_t *L = a.slist + (int64_t)row * a.sn;
         int *flag = a.use_pull + (nstep & 1);
@@ -1504,7 +1504,7 @@ static __global__ void __launch_bounds__(256) k_syn_lists(const SynEvArgs a) {
         const int d = 1 + (int)(x / nw);
         const int64_t wi = w0 + x % nw;
         if (nstep < d) continue;
-        uint32_t word = masked_word(a.hist + (int64_t)((nstep - d) % a.depth) * a.nwords, wi, a.so, a.so + a.sn);
+        uint32_t word = masked_word(a.hist + (int64_t)(((int)nstep - d) % a.depth) * a.nwords, wi, a.so, a.so + a.sn);
         if (!word) continue;
         const int row = (int)((nstep - d) % a.sdepth);
         int pos = atomicAdd(a.scnt + row, __popc(word));
@@ -1539,7 +1539,7 @@ __device__ __forceinline__ void syn_bin_apply(const SynEvArgs &a, long long nste
     if (pull) {
         // every target of the bin walks its incoming synapses in queue order
         // and applies those whose source spiked d steps ago (the pull's test)
-        const int row0 = (int)(nstep % a.depth);
+        const int row0 = (int)nstep % a.depth;
 #pragma unroll
         for (int u = 0; u < kSynTPT; ++u) {
             const int64_t j = jb + u * kSynBinThreads + tid;

@@ -130,7 +130,7 @@ __device__ __forceinline__ void synp_bins(const SynPersistArgs &a, long long t, 
     const int n = min(__ldcg(cnt), kSynBinCap);
     if (pull) {
         // the pull's test for every target of the bin, object by object
-        const int row0 = (int)(t % a.depth);
+        const int row0 = (int)t % a.depth;
 #pragma unroll
         for (int u = 0; u < kSPNpt; ++u) {
             const int64_t j = jb + u * kSPTh + tid;
@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(kSPTh, 2) k_syn_persist(const __grid_constant_
     const int base = blockIdx.x * kSPBn;         // neuron counts < 2^31
     const int nvalid = (int)min((int64_t)kSPBn, a.n - (int64_t)base);
     const unsigned int G = gridDim.x;
-    const long long t0 = a.ctl->nstep;
+    const long long t0 = a.ctl->nstep;          // step counters are below 2^31 (checked by the host)
     const int nl = kSPTh - 32 * a.nobj;          // threads on the spike lists; the rest on this step's words
     if (tid == 0) abort_flag = 0;
     double s[kSPNpt][NV];
@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(kSPTh, 2) k_syn_persist(const __grid_constant_
             if (lane == 0) {
                 const int w = u * (kSPTh / 32) + warp;
                 words[w] = ball;
-                a.hist[(int64_t)(t % a.depth) * a.nwords + (base >> 5) + w] = ball;
+                a.hist[(int64_t)((int)t % a.depth) * a.nwords + (base >> 5) + w] = ball;
                 if (a.mon_words) a.mon_words[(int64_t)st * a.mon_stride + (base >> 5) + w] = ball;
                 my_spikes += __popc(ball);
             }
@@ -337,11 +337,11 @@ __global__ void __launch_bounds__(kSPTh, 2) k_syn_persist(const __grid_constant_
         if (blockIdx.x == 0) {
             if (tid < a.nobj) {
                 const SynEvArgs &e = a.o[tid].e;
-                e.scnt[(t + 1) % e.sdepth] = 0;              // step t+1's list starts empty
+                e.scnt[((int)t + 1) % e.sdepth] = 0;              // step t+1's list starts empty
             }
-            if (tid == 32) a.use_pull[(t + 1) % 3] = 0;     // step t+1's overflow flag (last read in C(t-2))
+            if (tid == 32) a.use_pull[((int)t + 1) % 3] = 0;     // step t+1's overflow flag (last read in C(t-2))
         }
-        int *flag = a.use_pull + (int)(t % 3);
+        int *flag = a.use_pull + (int)t % 3;
         int *bcnt = a.bin_cnt + (int64_t)par * a.nbins;
         unsigned long long *bkey = a.bin_key + (int64_t)par * a.nbins * kSynBinCap;
         double *bt = a.bin_t + (int64_t)par * a.nbins * kSynBinCap;
@@ -356,7 +356,7 @@ __global__ void __launch_bounds__(kSPTh, 2) k_syn_persist(const __grid_constant_
             if (wb < e.so) { const int sh = (int)(e.so - wb); word = sh >= 32 ? 0u : (word & (0xffffffffu << sh)); }
             if (wb + 32 > e.so + e.sn) { const int keep = (int)(e.so + e.sn - wb); word = keep <= 0 ? 0u : (keep >= 32 ? word : (word & ((1u << keep) - 1u))); }
             if (word) {
-                const int row = (int)(t % e.sdepth);
+                const int row = (int)t % e.sdepth;
                 const int pos = atomicAdd(e.scnt + row, __popc(word));   // used after the pushes
                 for (uint32_t wv = word; wv; wv &= wv - 1)
                     synp_push(ob, k, wb + (__ffs(wv) - 1) - e.so, 0, 0, 1, flag, bcnt, bkey, bt);
@@ -373,7 +373,7 @@ __global__ void __launch_bounds__(kSPTh, 2) k_syn_persist(const __grid_constant_
                 const SynEvArgs &e = ob.e;
                 const int d = 1 + pair - a.pair0[k];
                 if (t < d) continue;
-                const int row = (int)((t - d) % e.sdepth);
+                const int row = ((int)t - d) % e.sdepth;
                 const int32_t *L = e.slist + (int64_t)row * e.sn;
                 // kSynSub threads per listed source, each with a share of its synapses
                 const int q0 = (part * nl + tid) / kSynSub, sub = tid % kSynSub;
