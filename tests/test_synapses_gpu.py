@@ -118,3 +118,33 @@ def test_synapses_persistent_kernel(oracle_table, gpu_table, kw):
     assert ref.pop("persistent_threads") == 0 and gpu.pop("persistent_threads") > 0
     assert len(ref["spk0.idx"]) > 100
     scenarios.compare(ref, gpu)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("delay", ["1*ms", "rand() * 2*ms"])
+def test_synapses_persistent_overflow(oracle_table, gpu_table, delay):
+    """The persistent kernel for Synapses on a dense, busy network onto
+    itself: every source has 750 synapses, so with one delay a source has
+    more than 256 synapses of that delay, and with random delays a step's
+    events exceed what a bin holds; those steps are delivered by the pull's
+    test inside the same launch.  Spikes, states and the StateMonitor equal
+    the oracle's."""
+    def fn():
+        from brian_b200 import ms, mV
+        G = b.NeuronGroup(1500, model="dv/dt = (20*mV - v)/(10*ms) : volt", threshold=10 * mV, reset=0 * mV)
+        G.v = np.random.rand(1500) * 10 * mV
+        S = b.Synapses(G, G, model="w : volt", pre="v += w")
+        S.connect_random(sparseness=0.5)
+        S.w = "0.002*mV * (1 + (i % 7))"
+        S.delay = delay
+        M = b.SpikeMonitor(G)
+        St = b.StateMonitor(G, "v", record=[0, 700, 1499])
+        net = b.Network(G, S, M, St)
+        net.run(30 * ms)
+        out = scenarios._result(net, groups=[G], spikemons=[M], statemons=[St])
+        out["persistent_threads"] = net.stats().get("persistent_threads", 0)
+        return out
+    ref, gpu = _both(fn, oracle_table)
+    assert ref.pop("persistent_threads") == 0 and gpu.pop("persistent_threads") > 0
+    assert len(ref["spk0.idx"]) > 10000
+    scenarios.compare(ref, gpu)
