@@ -1315,6 +1315,7 @@ int build_syn_persist(bg_net *net) {
     a.spikes = net->dCounters;
     a.arrived = net->dArrived;
     a.spin_limit = net->spin_limit;
+    a.hold_block = net->hold_block;
     a.nrec = (int)net->stmons.size();
     for (int k = 0; k < a.nrec; ++k) {
         HStateMon &m = net->stmons[k];

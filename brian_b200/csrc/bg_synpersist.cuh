@@ -63,6 +63,7 @@ struct SynPersistArgs {
     int nsteps;
     uint32_t *mon_words; int64_t mon_stride;     // spike monitors: the words of each step of the launch
     unsigned int spin_limit;
+    int hold_block;                              // test hook: this block never publishes its arrivals (-1: none)
     int nrec; RecDev rec[kMaxRec];               // StateMonitors; blk_lo holds this kernel's block ranges
 };
 
@@ -385,7 +386,7 @@ __global__ void __launch_bounds__(kSPTh, 2) k_syn_persist(const __grid_constant_
         }
         // ---- arrive at step t; wait for every block's arrival
         __syncthreads();
-        if (tid == 0) red_release_add(a.arrived + (st & 3), 1u);
+        if (tid == 0 && (int)blockIdx.x != a.hold_block) red_release_add(a.arrived + (st & 3), 1u);
         if (tid == 32) {
             const unsigned int *ctr = a.arrived + (st & 3);
             const unsigned int target = (unsigned int)((st >> 2) + 1) * G;

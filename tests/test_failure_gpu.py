@@ -119,3 +119,45 @@ def test_connection_rows_refused(gpu_table, bad):
         net.run(10 * 0.1 * ms)
     if isinstance(e.value, EngineError):
         assert e.value.code == BG_EINVAL, e.value
+
+
+@pytest.mark.gpu
+def test_bounded_wait_runs_out_synapses(oracle_table, gpu_table):
+    """The same for the persistent kernel for Synapses: one block holds back
+    its arrivals, every wait runs out, the run fails with BG_ETIMEOUT and
+    the device runs the next network bit for bit like the oracle."""
+    b.set_global_preferences(spin_limit=20000)
+    try:
+        b.clear()
+        b.reinit_default_clock()
+        np.random.seed(1234)
+        P = b.NeuronGroup(6000, model="dv/dt = (20*mV - v)/(10*ms) : volt", threshold=10 * mV, reset=0 * mV)
+        P.v = np.random.rand(6000) * 10 * mV
+        S = b.Synapses(P, P, model="w : volt", pre="v += w")
+        S.connect_random(sparseness=0.01)
+        S.w = 0.01 * mV
+        S.delay = "rand() * 2*ms"
+        net = b.Network(P, S)
+        net.prepare(configure=lambda rt: rt.debug_hold_arrival(2))
+        assert net.stats()["persistent_threads"] > 0
+        with pytest.raises(EngineError) as e:
+            net.run(100 * 0.1 * ms)
+        assert e.value.code == BG_ETIMEOUT, e.value
+        with pytest.raises(EngineError) as e:
+            net.run(10 * 0.1 * ms)
+        assert e.value.code == BG_ESTATE
+        net._invalidate()
+    finally:
+        b.set_global_preferences(spin_limit=None)
+    out = []
+    for tab in (oracle_table, None):
+        b.clear()
+        b.reinit_default_clock()
+        np.random.seed(1234)
+        if tab is None:
+            out.append(scenarios.synapses_cuba(two_statements=False, steps=500, report_persistent=True))
+        else:
+            with engine(tab):
+                out.append(scenarios.synapses_cuba(two_statements=False, steps=500, report_persistent=True))
+    assert out[0].pop("persistent_threads") == 0 and out[1].pop("persistent_threads") > 0
+    scenarios.compare(out[0], out[1])
