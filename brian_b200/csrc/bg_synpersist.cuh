@@ -254,7 +254,7 @@ __device__ __forceinline__ void synp_bins(const SynPersistArgs &a, long long t, 
 template <int NV, bool DIAG>
 __global__ void __launch_bounds__(kSPTh, 2) k_syn_persist(const __grid_constant__ SynPersistArgs a) {
     __shared__ uint32_t words[kSPBn / 32];
-    __shared__ int abort_flag;
+    __shared__ int abort_flag, pull_s;
     __shared__ double stash[kSPBn];              // StateMonitor values of the block's neurons
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int base = blockIdx.x * kSPBn;         // neuron counts < 2^31
@@ -395,11 +395,14 @@ __global__ void __launch_bounds__(kSPTh, 2) k_syn_persist(const __grid_constant_
                 if (++it > a.spin_limit) { abort_flag = 1; bg_raise(a.ctl, BG_DERR_TIMEOUT, t); break; }
                 __nanosleep(32);
             }
+            // the step's overflow flag, read once per block (every warp of
+            // every block reading one address queues at one L2 slice)
+            pull_s = __ldcg(flag);
         }
         __syncthreads();
         if (abort_flag) break;
         // ---- C(t): this block's bin, then the resets of step t
-        synp_bins<NV>(a, t, par, __ldcg(flag) != 0, s);
+        synp_bins<NV>(a, t, par, pull_s != 0, s);
         if (a.reset_kind == 1) {
 #pragma unroll
             for (int u = 0; u < kSPNpt; ++u)
