@@ -522,7 +522,7 @@ constexpr size_t smem_bytes() {
 // that gives up marks the CTA failed, the roles leave their loops, the
 // producer waits for its boxes in flight, the MMA thread for its MMAs, and
 // the TMEM is released.
-constexpr int kPThreads = 192;
+constexpr int kPThreads = 320;          // producer, MMA, eight epilogue warps (two per TMEM lane quarter)
 // operand stages in flight: as many as fit in 100 KB, so that the CTA of the
 // next product (launched early, programmatic dependent launch) fits beside it
 template <int NT> struct PStages { static constexpr int value = (192 * 1024) / ((kM + NT) * kKc * 2); };
@@ -660,6 +660,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_p(const GemmArgs g, const
     constexpr uint32_t idesc = idesc_bf16(kM, NT);
     constexpr uint32_t kBytes = (kM + NT) * kKc * 2;
     constexpr int kPStages = PSmem<NT>::S;
+    static_assert(NT % 32 == 0, "two epilogue warps per lane quarter split the columns in halves of 16-column chunks");
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int ntiles = tiles_m * tiles_n * splits;
     const int nk = g.k_per_split / kKc;
@@ -677,7 +678,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_p(const GemmArgs g, const
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(smem_u32(&sm.acc_full[b]), 1);
-            mbar_init(smem_u32(&sm.acc_empty[b]), 4);
+            mbar_init(smem_u32(&sm.acc_empty[b]), 8);
         }
         mbar_init(smem_u32(&sm.done), 1);
         sm.failed = 0;
@@ -753,8 +754,10 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_p(const GemmArgs g, const
             if (!mbar_wait(smem_u32(&sm.done), 0u)) atomicExch(&sm.failed, 1);
         }
     } else {
-        // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31
-        const int quarter = warp & 3;
+        // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31, the
+        // columns of its half (warps 2-5 the first, 6-9 the second)
+        const int quarter = warp & 3, half = (warp - 2) >> 2;
+        constexpr int kQ = NT / 32;                              // 16-column chunks per half
         int ti = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++ti) {
             const int buf = ti & 1, use = ti >> 1;
@@ -763,35 +766,35 @@ __global__ void __launch_bounds__(kPThreads, 1) k_gemm_p(const GemmArgs g, const
             const int m0 = mt * kM, n0 = nt * NT;
             const int row = m0 + quarter * 32 + lane;
             // the mask source is read while the MMAs of the tile run
-            uint4 actu[NT / 16][2];
+            uint4 actu[kQ][2];
             if (EPI == EPI_DRELU_BF16)
 #pragma unroll
-                for (int q = 0; q < NT / 16; ++q) p_load_act(g, row, n0 + 16 * q, actu[q]);
+                for (int q = 0; q < kQ; ++q) p_load_act(g, row, n0 + 16 * (half * kQ + q), actu[q]);
             bool ok = mbar_wait(smem_u32(&sm.acc_full[buf]), (uint32_t)(use & 1));
             ok = __all_sync(0xffffffffu, ok);
             if (!ok || *(volatile int *)&sm.failed) { if (lane == 0) atomicExch(&sm.failed, 1); break; }
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
             // the whole row of the tile out of TMEM with one wait, and the
             // accumulator handed back to the MMA warp before the stores
-            uint32_t raw[NT / 16][16];
+            uint32_t raw[kQ][16];
 #pragma unroll
-            for (int q = 0; q < NT / 16; ++q)
-                tmem_ld16_nowait(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * NT + 16 * q), raw[q]);
+            for (int q = 0; q < kQ; ++q)
+                tmem_ld16_nowait(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * NT + 16 * (half * kQ + q)), raw[q]);
             asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(&sm.acc_empty[buf]));
 #pragma unroll
-            for (int q = 0; q < NT / 16; ++q) {
+            for (int q = 0; q < kQ; ++q) {
                 float v[16];
 #pragma unroll
                 for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(raw[q][i]);
-                p_epilogue_chunk<NT, EPI>(g, v, row, n0, 16 * q, mt, quarter, lane, sm, z, actu[q]);
+                p_epilogue_chunk<NT, EPI>(g, v, row, n0, 16 * (half * kQ + q), mt, quarter, lane, sm, z, actu[q]);
             }
             if (EPI == EPI_DRELU_BF16 && g.colsum) {
                 // this quarter's 32-row column sums: row (4 mt + quarter) of colsum
                 __syncwarp();
-                for (int c = lane; c < NT; c += 32)
+                for (int c = half * (NT / 2) + lane; c < (half + 1) * (NT / 2); c += 32)
                     if (n0 + c < g.N) g.colsum[(long long)(4 * mt + quarter) * g.colsum_ld + n0 + c] = sm.red[quarter][c];
                 __syncwarp();
             }
